@@ -1,0 +1,224 @@
+"""Python bindings of the C ABI (include/deme_b200.h).
+
+``Solver`` drives the CUDA library through ``deme_*``.  ``HandleSolver`` is the same wrapper over any library
+that exports the ABI's entry points under another prefix; tests use it to run the C oracle and the reference
+kernels compiled for the CPU with identical calls.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _capi as capi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libdeme_b200.so")
+_lib = None
+
+
+def load_product_library(path: str = LIB_PATH) -> C.CDLL:
+    """Load the CUDA product library; fails loudly if it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise RuntimeError(f"CUDA extension not built: {path} is missing (run __graft_entry__.build())")
+        lib = capi.load_library(path)
+        capi.bind(lib, "deme_")
+        lib.deme_get_error.restype = C.c_char_p
+        lib.deme_get_error.argtypes = [C.c_void_p]
+        lib.deme_status_string.restype = C.c_char_p
+        lib.deme_status_string.argtypes = [C.c_int32]
+        lib.deme_get_num_contacts.restype = C.c_int32
+        lib.deme_get_num_contacts.argtypes = [C.c_void_p, C.POINTER(C.c_uint32)]
+        lib.deme_create.restype = C.c_int32
+        lib.deme_create.argtypes = [C.POINTER(capi.SimParams), C.POINTER(capi.Scene), C.POINTER(C.c_void_p)]
+        lib.deme_sync.restype = C.c_int32
+        lib.deme_sync.argtypes = [C.c_void_p]
+        lib.deme_kinetic_energy.restype = C.c_int32
+        lib.deme_kinetic_energy.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        lib.deme_get_time.restype = C.c_int32
+        lib.deme_get_time.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+        lib.deme_set_force_model.restype = C.c_int32
+        lib.deme_set_force_model.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_char_p), C.c_int32]
+        lib.deme_abi_version.restype = C.c_int32
+        _lib = lib
+    return _lib
+
+
+class DemeError(RuntimeError):
+    pass
+
+
+class HandleSolver:
+    """Wrapper over a library exporting the ABI under ``prefix`` (``orc_`` or ``ref_``)."""
+
+    def __init__(self, lib: C.CDLL, prefix: str, built, threads: int | None = None):
+        self.lib = lib
+        self.prefix = prefix
+        self.built = built
+        capi.bind(lib, prefix)
+        if threads is not None and hasattr(lib, prefix + "set_threads"):
+            getattr(lib, prefix + "set_threads")(threads)
+        scene, self._keep = built.scene_struct()
+        self._params = built.params
+        self.h = self._create(scene)
+        self.nO = built.counts["o"]
+        self.nS = built.counts["s"]
+        self.nW = built.params.n_contact_wildcards
+
+    def _fn(self, name):
+        return getattr(self.lib, self.prefix + name)
+
+    def _create(self, scene):
+        h = self._fn("create")(C.byref(self._params), C.byref(scene))
+        if not h:
+            raise DemeError(f"{self.prefix}create failed")
+        return h
+
+    def _check(self, st, what):
+        if st != capi.DEME_OK:
+            raise DemeError(f"{self.prefix}{what}: {capi.STATUS_NAMES.get(st, st)}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._fn("destroy")(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- steps ---
+    def detect_contacts(self):
+        self._check(self._fn("detect_contacts")(self.h), "detect_contacts")
+
+    def compute_forces(self):
+        self._check(self._fn("compute_forces")(self.h), "compute_forces")
+
+    def integrate(self):
+        self._check(self._fn("integrate")(self.h), "integrate")
+
+    def step(self, n: int = 1):
+        self._check(self._fn("step")(self.h, n), "step")
+
+    def sync(self):
+        pass
+
+    # --- transfer ---
+    def num_contacts(self) -> int:
+        return int(self._fn("num_contacts")(self.h))
+
+    def state(self) -> dict:
+        out = {name: np.zeros(self.nO, dt) for name, dt in capi.STATE_FIELDS}
+        st, keep = capi.state_struct(out)
+        self._check(self._fn("download_state")(self.h, C.byref(st)), "download_state")
+        return out
+
+    def set_state(self, arrays: dict):
+        arrays = {k: np.ascontiguousarray(v, dtype=dict(capi.STATE_FIELDS)[k]) for k, v in arrays.items()}
+        st, keep = capi.state_struct(arrays)
+        self._check(self._fn("upload_state")(self.h, C.byref(st)), "upload_state")
+
+    def contacts(self) -> dict:
+        n = self.num_contacts()
+        cap = max(n, 1)
+        d = dict(idA=np.zeros(cap, np.uint32), idB=np.zeros(cap, np.uint32), type=np.zeros(cap, np.uint8),
+                 mapping=np.zeros(cap, np.uint32), wildcards=np.zeros((max(self.nW, 1), cap), np.float32))
+        c = capi.Contacts(cap, 0, capi.ptr(d["idA"]), capi.ptr(d["idB"]), capi.ptr(d["type"]),
+                          capi.ptr(d["mapping"]), capi.ptr(d["wildcards"]))
+        self._check(self._fn("download_contacts")(self.h, C.byref(c)), "download_contacts")
+        n = c.n_contacts
+        return dict(idA=d["idA"][:n], idB=d["idB"][:n], type=d["type"][:n], mapping=d["mapping"][:n],
+                    wildcards=d["wildcards"][:self.nW, :n])
+
+    def set_contacts(self, d: dict):
+        n = len(d["idA"])
+        cap = max(n, 1)
+        idA = np.zeros(cap, np.uint32)
+        idB = np.zeros(cap, np.uint32)
+        tp = np.zeros(cap, np.uint8)
+        wc = np.zeros((max(self.nW, 1), cap), np.float32)
+        idA[:n] = d["idA"]
+        idB[:n] = d["idB"]
+        tp[:n] = d["type"]
+        if self.nW and d.get("wildcards") is not None:
+            wc[:self.nW, :n] = d["wildcards"]
+        c = capi.Contacts(cap, n, capi.ptr(idA), capi.ptr(idB), capi.ptr(tp), None, capi.ptr(wc))
+        self._check(self._fn("upload_contacts")(self.h, C.byref(c)), "upload_contacts")
+
+    def contact_forces(self) -> dict:
+        n = self.num_contacts()
+        cap = max(n, 1)
+        d = {k: np.zeros((cap, 3), np.float32) for k in ("force", "torque_only_force", "cpA", "cpB")}
+        c = capi.ContactForces(cap, 0, capi.ptr(d["force"]), capi.ptr(d["torque_only_force"]), capi.ptr(d["cpA"]),
+                               capi.ptr(d["cpB"]))
+        self._check(self._fn("download_contact_forces")(self.h, C.byref(c)), "download_contact_forces")
+        return {k: v[:c.n_contacts] for k, v in d.items()}
+
+    def bin_assignment(self, with_pairs: bool = True) -> dict:
+        nb = np.zeros(max(self.nS, 1), np.uint16)
+        na = np.zeros(max(self.nS, 1), np.uint8)
+        npairs = C.c_uint32(0)
+        self._check(self._fn("bin_assignment")(self.h, capi.ptr(nb), capi.ptr(na), 0, None, None, C.byref(npairs)),
+                    "bin_assignment")
+        out = dict(n_bins=nb[:self.nS], n_anal=na[:self.nS], n_pairs=int(npairs.value))
+        if with_pairs:
+            cap = max(int(npairs.value), 1)
+            bins = np.zeros(cap, np.uint32)
+            sph = np.zeros(cap, np.uint32)
+            self._check(self._fn("bin_assignment")(self.h, None, None, cap, capi.ptr(bins), capi.ptr(sph),
+                                                   C.byref(npairs)), "bin_assignment")
+            out["bins"] = bins[:npairs.value]
+            out["spheres"] = sph[:npairs.value]
+        return out
+
+    def kinetic_energy(self) -> float:
+        return float(self._fn("kinetic_energy")(self.h))
+
+
+class Solver(HandleSolver):
+    """The CUDA product path (``deme_*``)."""
+
+    def __init__(self, built, lib_path: str = LIB_PATH):
+        lib = load_product_library(lib_path)
+        self.lib = lib
+        self.prefix = "deme_"
+        self.built = built
+        scene, self._keep = built.scene_struct()
+        self._params = built.params
+        h = C.c_void_p()
+        st = lib.deme_create(C.byref(self._params), C.byref(scene), C.byref(h))
+        if st != capi.DEME_OK:
+            raise DemeError(f"deme_create: {capi.STATUS_NAMES.get(st, st)}")
+        self.h = h.value
+        self.nO = built.counts["o"]
+        self.nS = built.counts["s"]
+        self.nW = built.params.n_contact_wildcards
+
+    def _check(self, st, what):
+        if st != capi.DEME_OK:
+            msg = self.lib.deme_get_error(self.h)
+            raise DemeError(f"deme_{what}: {capi.STATUS_NAMES.get(st, st)}: {msg.decode() if msg else ''}")
+
+    def num_contacts(self) -> int:
+        n = C.c_uint32(0)
+        self._check(self.lib.deme_get_num_contacts(self.h, C.byref(n)), "get_num_contacts")
+        return int(n.value)
+
+    def sync(self):
+        self._check(self.lib.deme_sync(self.h), "sync")
+
+    def kinetic_energy(self) -> float:
+        ke = C.c_double(0)
+        self._check(self.lib.deme_kinetic_energy(self.h, C.byref(ke)), "kinetic_energy")
+        return float(ke.value)
+
+    def set_force_model(self, src: str | None, wildcards=()):
+        names = (C.c_char_p * max(len(wildcards), 1))(*[w.encode() for w in wildcards])
+        self._check(self.lib.deme_set_force_model(self.h, src.encode() if src else None, names, len(wildcards)),
+                    "set_force_model")
+        self.nW = len(wildcards) if src else self._params.n_contact_wildcards

@@ -1,0 +1,201 @@
+"""Seeded synthetic scenes for the benchmark configurations and the parity tests.
+
+Scene sizes and materials follow the benchmark configurations of this project (settling box, rotating drum,
+hopper, column collapse).  Geometry that does not fit as literally specified is resized as recorded in the
+``info`` of each scene (the design notes give the reasoning).  Generators use numpy's PCG64 with an explicit
+seed, so every scene is reproducible bit for bit.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import _capi as capi
+from .scene import SceneBuilder
+
+f32 = np.float32
+
+
+def sphere_mass(r: float, rho: float) -> float:
+    return 4.0 / 3.0 * math.pi * r**3 * rho
+
+
+def random_quaternions(rng, n):
+    """Uniform random unit quaternions (Shoemake), rows (w, x, y, z)."""
+    u1, u2, u3 = rng.random(n), rng.random(n), rng.random(n)
+    q = np.stack([np.sqrt(1 - u1) * np.sin(2 * np.pi * u2), np.sqrt(1 - u1) * np.cos(2 * np.pi * u2),
+                  np.sqrt(u1) * np.sin(2 * np.pi * u3), np.sqrt(u1) * np.cos(2 * np.pi * u3)], axis=1)
+    return q[:, [3, 0, 1, 2]].astype(f32)
+
+
+def settling_box(n: int = 10000, r: float = 5e-3, rho: float = 2600.0, box=(0.2, 0.2, 0.4), spacing: float = 2.2,
+                 jitter: float = 0.1, seed: int = 1, dt: float = 1e-5, per_layer: int | None = None,
+                 vel_scale: float = 0.0, ang_scale: float = 0.0):
+    """Settling box: monodisperse spheres on a jittered cubic lattice inside a box of 6 planes.
+
+    A lattice of spacing 2.2 r holds 18 x 18 sites per layer in a 0.2 m box; 10,000 spheres then need 31 layers
+    (0.34 m), so the lattice is filled from the floor up instead of only the lower half.
+    """
+    rng = np.random.default_rng(seed)
+    s = SceneBuilder()
+    s.InstructBoxDomainDimension(*box)
+    s.SetCoordSysOrigin("center")
+    mat = s.LoadMaterial({"E": 1e7, "nu": 0.3, "CoR": 0.5, "mu": 0.5, "Crr": 0.0})
+    s.InstructBoxDomainBoundingBC("all", mat)
+    m = sphere_mass(r, rho)
+    t = s.LoadSphereType(m, r, mat)
+    a = spacing * r
+    nx = int(box[0] // a) if per_layer is None else per_layer
+    ny = int(box[1] // a) if per_layer is None else per_layer
+    nz = int(math.ceil(n / (nx * ny)))
+    lbf = -np.asarray(box) / 2
+    x0 = lbf[0] + (box[0] - nx * a) / 2 + a / 2
+    y0 = lbf[1] + (box[1] - ny * a) / 2 + a / 2
+    z0 = lbf[2] + a / 2
+    idx = np.arange(n)
+    pos = np.stack([x0 + (idx % nx) * a, y0 + ((idx // nx) % ny) * a, z0 + (idx // (nx * ny)) * a], axis=1)
+    pos += rng.uniform(-jitter * r, jitter * r, size=pos.shape)
+    b = s.AddClumps(t, pos.astype(f32))
+    if vel_scale:
+        b.SetVel(rng.normal(0, vel_scale, size=(n, 3)).astype(f32))
+    if ang_scale:
+        b.SetAngVel(rng.normal(0, ang_scale, size=(n, 3)).astype(f32))
+    s.SetInitTimeStep(dt)
+    s.SetGravitationalAcceleration((0, 0, -9.81))
+    s.SetInitBinSize(2.0 * r)
+    built = s.Initialize()
+    built.info.update(workload="settling_box", n_layers=nz, per_layer=(nx, ny), seed=seed)
+    return built
+
+
+def triangle_template(rng, r_nom: float, rho: float, n_mc: int = 20000):
+    """Three-sphere triangular clump: radii U[0.8, 1.2] r_nom, centres 0.6 r from the clump centroid.
+
+    Mass, centre of mass and principal moments are integrated by Monte Carlo over the union of the spheres;
+    relative positions are re-centred on the centre of mass, and the clump frame is taken as principal
+    (the in-plane symmetric layout makes the products of inertia small; they are dropped).
+    """
+    radii = rng.uniform(0.8, 1.2, 3) * r_nom
+    ang = np.array([0.0, 2 * np.pi / 3, 4 * np.pi / 3])
+    centers = np.stack([0.6 * radii * np.cos(ang), 0.6 * radii * np.sin(ang), np.zeros(3)], axis=1)
+    lo = (centers - radii[:, None]).min(0)
+    hi = (centers + radii[:, None]).max(0)
+    pts = lo + (hi - lo) * rng.random((n_mc, 3))
+    inside = np.zeros(n_mc, bool)
+    for c, r in zip(centers, radii):
+        inside |= ((pts - c) ** 2).sum(1) <= r * r
+    vol = np.prod(hi - lo) * inside.mean()
+    p = pts[inside]
+    com = p.mean(0)
+    d = p - com
+    mass = rho * vol
+    I = mass * np.array([(d[:, 1] ** 2 + d[:, 2] ** 2).mean(), (d[:, 0] ** 2 + d[:, 2] ** 2).mean(),
+                         (d[:, 0] ** 2 + d[:, 1] ** 2).mean()])
+    return radii.astype(f32), (centers - com).astype(f32), float(mass), I.astype(f32), float(vol)
+
+
+def drum(n_clumps: int = 1_000_000, r_nom: float = 2e-3, rho: float = 2500.0, n_templates: int = 64,
+         fill: float = 0.30, packing: float = 0.6, rpm: float = 20.0, dt: float = 5e-6, seed: int = 2,
+         shell: bool = False):
+    """Rotating drum of three-sphere clumps (analytical cylinder + two end planes, prescribed rotation).
+
+    One million clumps of about 8e-8 m^3 do not fit a 30 % fill of an R = 0.25 m, L = 0.3 m drum, so the drum is
+    scaled (same L / R ratio) until the clumps at ``packing`` bulk density fill ``fill`` of its volume.
+    Clumps start on a jittered lattice in the lower part of the drum with random orientations.
+    """
+    rng = np.random.default_rng(seed)
+    tmpl = [triangle_template(rng, r_nom, rho) for _ in range(n_templates)]
+    vol_clump = float(np.mean([t[4] for t in tmpl]))
+    bulk = n_clumps * vol_clump / packing
+    # drum volume V = pi R^2 L with L = 1.2 R
+    R = (bulk / fill / (math.pi * 1.2)) ** (1.0 / 3.0)
+    L = 1.2 * R
+    s = SceneBuilder()
+    margin = 4 * r_nom
+    box = (2 * R + 2 * margin, L + 2 * margin, 2 * R + 2 * margin)
+    s.InstructBoxDomainDimension(*box)
+    s.SetCoordSysOrigin("center")
+    mat = s.LoadMaterial({"E": 5e7, "nu": 0.3, "CoR": 0.3, "mu": 0.4, "Crr": 0.02})
+    ts = [s.LoadClumpType(t[2], t[3], t[0], t[1], mat) for t in tmpl]
+    # lattice of clump centres inside the drum's lower region
+    a = 2.4 * 1.2 * r_nom * 1.25
+    xs = np.arange(-R + a, R - a, a)
+    ys = np.arange(-L / 2 + a, L / 2 - a, a)
+    zs = np.arange(-R + a, R - a, a)
+    X, Y, Z = np.meshgrid(xs, ys, zs, indexing="ij")
+    P = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+    inside = P[:, 0] ** 2 + P[:, 2] ** 2 <= (R - a) ** 2
+    P = P[inside]
+    P = P[np.argsort(P[:, 2], kind="stable")]
+    if len(P) < n_clumps:
+        raise ValueError(f"lattice holds {len(P)} clumps, {n_clumps} requested")
+    P = P[:n_clumps] + rng.uniform(-0.05 * a, 0.05 * a, size=(n_clumps, 3))
+    types = rng.integers(0, n_templates, n_clumps)
+    b = s.AddClumps(types, P.astype(f32))
+    b.SetOriQ(random_quaternions(rng, n_clumps))
+    drum_fam = 10
+    d = s.AddExternalObject()
+    d.AddCylinder((0, 0, 0), (0, 1, 0), R, mat)
+    d.AddPlane((0, -L / 2, 0), (0, 1, 0), mat)
+    d.AddPlane((0, L / 2, 0), (0, -1, 0), mat)
+    d.SetFamily(drum_fam)
+    omega = rpm * 2 * math.pi / 60.0
+    s.SetFamilyPrescribedLinVel(drum_fam, "0", "0", "0")
+    s.SetFamilyPrescribedAngVel(drum_fam, "0", repr(float(f32(omega))), "0")
+    s.SetInitTimeStep(dt)
+    s.SetGravitationalAcceleration((0, 0, -9.81))
+    built = s.Initialize()
+    built.info.update(workload="drum", R=R, L=L, n_templates=n_templates, omega=omega, seed=seed,
+                      vol_clump=vol_clump, n_clumps=n_clumps)
+    return built
+
+
+def packed_clumps(n_clumps: int = 600, r: float = 4e-3, spacing: float = 1.55, seed: int = 3, three: bool = True,
+                  vel_scale: float = 0.05, ang_scale: float = 5.0, dt: float = 1e-5, beta: float = 0.0,
+                  families: bool = False):
+    """Small dense scene for parity tests: overlapping clumps with random poses, velocities and spin, in a box of
+    planes, so that one step exercises every branch of the force model."""
+    rng = np.random.default_rng(seed)
+    s = SceneBuilder()
+    side = (n_clumps ** (1 / 3) + 1) * spacing * 2 * r
+    s.InstructBoxDomainDimension(side, side, side)
+    s.SetCoordSysOrigin("center")
+    mA = s.LoadMaterial({"E": 1e7, "nu": 0.3, "CoR": 0.5, "mu": 0.5, "Crr": 0.05})
+    mB = s.LoadMaterial({"E": 5e7, "nu": 0.25, "CoR": 0.3, "mu": 0.4, "Crr": 0.0})
+    s.InstructBoxDomainBoundingBC("all", mB)
+    tmpls = []
+    for k in range(4):
+        if three:
+            radii = rng.uniform(0.8, 1.2, 3) * r
+            ang = np.array([0, 2 * np.pi / 3, 4 * np.pi / 3]) + k
+            rel = np.stack([0.6 * radii * np.cos(ang), 0.6 * radii * np.sin(ang), np.zeros(3)], 1)
+            m = sphere_mass(r, 2500) * 2.4
+            tmpls.append(s.LoadClumpType(m, (m * r * r * 0.5, m * r * r * 0.55, m * r * r * 0.6), radii, rel,
+                                         [mA, mB, mA]))
+        else:
+            rr = r * (0.9 + 0.05 * k)
+            tmpls.append(s.LoadSphereType(sphere_mass(rr, 2500), rr, [mA, mB][k % 2]))
+    n_side = int(math.ceil(n_clumps ** (1 / 3)))
+    a = spacing * 2 * r * (1.0 if three else 0.62)
+    g = np.arange(n_side) * a
+    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+    P = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)[:n_clumps]
+    P = P - P.mean(0) + rng.uniform(-0.15 * r, 0.15 * r, size=P.shape)
+    types = rng.integers(0, 4, n_clumps)
+    b = s.AddClumps(types, P.astype(f32))
+    b.SetOriQ(random_quaternions(rng, n_clumps))
+    b.SetVel(rng.normal(0, vel_scale, (n_clumps, 3)).astype(f32))
+    b.SetAngVel(rng.normal(0, ang_scale, (n_clumps, 3)).astype(f32))
+    if families:
+        fam = rng.integers(0, 3, n_clumps)
+        b.SetFamilies(fam)
+        s.DisableContactBetweenFamilies(1, 2)
+        s.SetFamilyPrescribedLinVel(2, "0", "0", "-0.01")
+    s.SetInitTimeStep(dt)
+    s.SetGravitationalAcceleration((0, 0, -9.81))
+    if beta:
+        s.SetExpandFactor(beta)
+    built = s.Initialize()
+    built.info.update(workload="packed_clumps", seed=seed)
+    return built

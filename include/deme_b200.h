@@ -1,0 +1,291 @@
+/*
+ * deme_b200.h -- C ABI of the B200-native DEM-Engine hot path.
+ *
+ * The reference solver (DEM-Engine, `deme::DEMSolver`, src/DEM/API.h:44-887) has no C ABI: its kernels are
+ * reachable only through the C++ class and its two worker threads (kT: contact detection, dT: dynamics).
+ * This header is the drop-in boundary for that per-step path.  Each entry point names the reference
+ * interface it replaces.  The C++ `deme::DEMSolver` facade in dem-engine-sbel_b200/csrc/solver/ is
+ * written on top of these calls and keeps the reference's method names.
+ *
+ * Conventions
+ *   - plain C structs of host pointers plus counts; caller-owned host buffers, solver-owned device buffers;
+ *   - every entry point returns a deme_status; nothing throws and no kernel traps;
+ *   - one handle per host thread (not re-entrant);
+ *   - ID widths and array layouts follow src/DEM/VariableTypes.h:11-49 and src/DEM/Defines.h:154-383.
+ */
+#ifndef DEME_B200_H
+#define DEME_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DEME_B200_ABI_VERSION 1
+
+/* Status codes (the reference throws std::runtime_error instead: src/DEM/Structs.h:129-141, src/core/utils/GpuError.h:13-27). */
+typedef enum {
+    DEME_OK = 0,
+    DEME_ERR_INVALID = 1,     /* bad argument or inconsistent scene */
+    DEME_ERR_CUDA = 2,        /* CUDA runtime error; the handle should be destroyed */
+    DEME_ERR_OOM = 3,         /* device allocation failed */
+    DEME_ERR_OVERFLOW = 4,    /* a device-side capacity check failed (reported, never trapped) */
+    DEME_ERR_NVRTC = 5,       /* the user force model did not compile */
+    DEME_ERR_TIMEOUT = 6,     /* a bounded device wait gave up */
+    DEME_ERR_STATE = 7,       /* call made in the wrong lifecycle state */
+    DEME_ERR_NO_DEVICE = 8    /* no CUDA device is visible */
+} deme_status;
+
+/* Contact types (src/DEM/Defines.h:63-67).  Cylinder and cone are additions of this build. */
+#define DEME_NOT_A_CONTACT 0
+#define DEME_SPHERE_SPHERE_CONTACT 1
+#define DEME_SPHERE_MESH_CONTACT 2
+#define DEME_SPHERE_PLANE_CONTACT 3
+#define DEME_SPHERE_PLATE_CONTACT 4
+#define DEME_SPHERE_CYLINDER_CONTACT 5
+#define DEME_SPHERE_CONE_CONTACT 6
+
+/* Analytical component types (src/DEM/Defines.h:60-61, plus the two new shapes). */
+#define DEME_ANAL_PLANE 0
+#define DEME_ANAL_PLATE 1
+#define DEME_ANAL_CYLINDER 2
+#define DEME_ANAL_CONE 3
+
+/* Integrators (src/DEM/Defines.h:106, TIME_INTEGRATOR). */
+#define DEME_INTEGRATOR_FORWARD_EULER 0
+#define DEME_INTEGRATOR_CENTERED_DIFFERENCE 1
+#define DEME_INTEGRATOR_EXTENDED_TAYLOR 2
+
+/* NULL_MAPPING_PARTNER (src/DEM/Defines.h:80-81).  The reference's expression `(1 << 31) + (1 << 31 - 1)` parses as
+ * (1 << 31) + (1 << 30) because `-` binds tighter than `<<`, so its value is 0xC0000000, kept here bit for bit. */
+#define DEME_NULL_MAPPING_PARTNER 0xC0000000u
+/* Family-mask table size.  The reference sizes it (255*256)/2 = 32640 (src/DEM/APIPrivate.cpp:588) but indexes up to
+ * 32895 for family 255 (src/kernel/DEMHelperKernels.cu:51-56); this build stores 32896 entries, tail = allow. */
+#define DEME_NUM_FAMILY_MASK 32896
+#define DEME_NUM_FAMILIES 256
+#define DEME_RESERVED_FAMILY 255
+#define DEME_MAX_WILDCARDS 8
+
+/* Simulation parameters: the fields of deme::DEMSimParams (src/DEM/Defines.h:154-211) plus the two JIT literals.
+ * `l_kernel` and `voxel_size_kernel` are the values the reference's kernels see: it substitutes `_l_` and
+ * `_voxelSize_` as std::fixed 17-decimal text (src/DEM/APIPrivate.cpp:1358-1359, src/DEM/HostSideHelpers.hpp:396-401),
+ * while host-side initial encoding uses the exact doubles `l` and `voxel_size` (src/DEM/dT.cpp:572-575). */
+typedef struct {
+    uint8_t nvXp2, nvYp2, nvZp2, pad0;
+    uint32_t nbX, nbY, nbZ;
+    double l;
+    double voxel_size;
+    double l_kernel;
+    double voxel_size_kernel;
+    double bin_size;
+    float lbf[3];
+    float G[3];
+    float h;          /* time step (float, as DEMSimParams::h) */
+    float beta;       /* contact-detection expand factor (DEMSimParams::beta) */
+    int32_t integrator;
+    int32_t cd_update_freq;  /* 0: contact detection every step (src/DEM/API.h:82, SetCDUpdateFreq) */
+    int32_t n_contact_wildcards; /* 4 for the built-in Hertz-Mindlin model, 0 for frictionless */
+    int32_t pad1;
+} deme_sim_params;
+
+/* Per-family prescription.  The reference jitifies these as C expression strings
+ * (src/DEM/APIPrivate.cpp:1005-1048); this struct carries the constant-valued form.  `has_*` marks the
+ * components the user prescribed ("none" in the reference leaves a component free). */
+typedef struct {
+    uint8_t used;
+    uint8_t lin_vel_prescribed;
+    uint8_t rot_vel_prescribed;
+    uint8_t lin_pos_prescribed;
+    uint8_t rot_pos_prescribed;
+    uint8_t has_vel[3];
+    uint8_t has_omg[3];
+    uint8_t has_pos[3];
+    uint8_t pad[4];
+    float vel[3];
+    float omg[3];
+    double pos[3];
+} deme_family_prescription;
+
+/* Scene: the flattened arrays dT/kT receive at Initialize (src/DEM/dT.cpp:480-640), as host pointers. */
+typedef struct {
+    uint32_t n_owners;
+    uint32_t n_spheres;
+    uint32_t n_anal;
+    uint32_t n_materials;
+    /* owners (clumps first, then analytical owners: src/DEM/dT.cpp:622-640) */
+    const uint64_t* voxel;
+    const uint16_t* locX;
+    const uint16_t* locY;
+    const uint16_t* locZ;
+    const float* oriQw;
+    const float* oriQx;
+    const float* oriQy;
+    const float* oriQz;
+    const float* vX;
+    const float* vY;
+    const float* vZ;
+    const float* omgX;
+    const float* omgY;
+    const float* omgZ;
+    const uint8_t* family;
+    const float* mass;
+    const float* mmiXX;
+    const float* mmiYY;
+    const float* mmiZZ;
+    /* spheres (flattened clump components: ClumpCompAcqStratAllFlatten.cu) */
+    const uint32_t* sphere_owner;
+    const float* relX;
+    const float* relY;
+    const float* relZ;
+    const float* radius;
+    const uint8_t* sphere_material;
+    /* analytical components (AnalyticalCompDefJitify.cu) */
+    const uint8_t* anal_type;
+    const uint32_t* anal_owner;
+    const uint8_t* anal_normal;
+    const uint8_t* anal_material;
+    const float* anal_relX;
+    const float* anal_relY;
+    const float* anal_relZ;
+    const float* anal_rotX;
+    const float* anal_rotY;
+    const float* anal_rotZ;
+    const float* anal_size1;
+    const float* anal_size2;
+    const float* anal_size3;
+    const float* anal_mass;
+    /* materials (keys E, nu, CoR, mu, Crr: src/DEM/AuxClasses.cpp:222) */
+    const float* mat_E;
+    const float* mat_nu;
+    const float* mat_CoR;
+    const float* mat_mu;
+    const float* mat_Crr;
+    /* families */
+    const uint8_t* family_masks;                        /* DEME_NUM_FAMILY_MASK entries, 1 = prevent contact */
+    const deme_family_prescription* prescriptions;      /* DEME_NUM_FAMILIES entries */
+} deme_scene;
+
+/* Mutable owner state (download/upload).  Any pointer may be NULL to skip that array. */
+typedef struct {
+    uint64_t* voxel;
+    uint16_t* locX;
+    uint16_t* locY;
+    uint16_t* locZ;
+    float* oriQw;
+    float* oriQx;
+    float* oriQy;
+    float* oriQz;
+    float* vX;
+    float* vY;
+    float* vZ;
+    float* omgX;
+    float* omgY;
+    float* omgZ;
+    float* aX;
+    float* aY;
+    float* aZ;
+    float* alphaX;
+    float* alphaY;
+    float* alphaZ;
+    uint8_t* family;
+} deme_state;
+
+/* Contact list (kT product, src/DEM/Defines.h:242-245).  Order: sorted by idA; inside one idA, sphere--analytical
+ * contacts first (ascending component id), then sphere--sphere contacts (ascending idB).  The reference sorts by idA
+ * only, so its in-segment order is a permutation of this one. */
+typedef struct {
+    uint32_t capacity;       /* elements available in each caller array (in) */
+    uint32_t n_contacts;     /* contacts in the list (out) */
+    uint32_t* idA;
+    uint32_t* idB;
+    uint8_t* type;
+    uint32_t* mapping;       /* index into the previous list, or DEME_NULL_MAPPING_PARTNER */
+    float* wildcards;        /* n_contact_wildcards x capacity, row-major by wildcard (may be NULL) */
+} deme_contacts;
+
+/* Per-contact dT outputs (contactForces, contactTorque_convToForce, contactPointGeometryA/B in DEMDataDT). */
+typedef struct {
+    uint32_t capacity;
+    uint32_t n_contacts;
+    float* force;            /* 3 x n, interleaved xyz */
+    float* torque_only_force;
+    float* cpA;
+    float* cpB;
+} deme_contact_forces;
+
+typedef struct deme_handle deme_handle;
+
+/* Version and error text. */
+int32_t deme_abi_version(void);
+const char* deme_status_string(int32_t status);
+
+/* Create a solver on the current CUDA device and upload the scene.
+ * Replaces DEMSolver::Initialize -> allocateGPUArrays/initializeGPUArrays (src/DEM/APIPublic.cpp:659-693,
+ * src/DEM/APIPrivate.cpp:760-818). */
+int32_t deme_create(const deme_sim_params* params, const deme_scene* scene, deme_handle** out);
+void deme_destroy(deme_handle* h);
+/* Last error message of this handle (static storage, valid until the next call on it). */
+const char* deme_get_error(deme_handle* h);
+
+/* Force model.  src == NULL selects the built-in frictional Hertz-Mindlin model (FullHertzianForceModel.cu);
+ * otherwise `src` is a user force-model snippet compiled with NVRTC into the force-kernel template, with the
+ * given per-contact wildcard names (DefineContactForceModel, src/DEM/APIPublic.cpp:116-121;
+ * DEMForceModel::SetPerContactWildcards, src/DEM/AuxClasses.cpp:256-266). */
+int32_t deme_set_force_model(deme_handle* h, const char* src, const char* const* wildcard_names, int32_t n_wildcards);
+
+/* Contact detection on the current state (kT: contactDetection, src/algorithms/DEMCubContactDetection.cu:39-397),
+ * including the history map against the previous list and the wildcard remap
+ * (dT::migratePersistentContacts, src/DEM/dT.cpp:1258-1347). */
+int32_t deme_detect_contacts(deme_handle* h);
+/* Forces and their collection onto owners for the current contact list (dT::calculateForces,
+ * src/DEM/dT.cpp:1349-1422, collectContactForces, src/algorithms/DEMCubForceCollection.cu:20-158). */
+int32_t deme_compute_forces(deme_handle* h);
+/* Owner integration (integrateOwners, src/kernel/DEMIntegrationKernels.cu:170-179). */
+int32_t deme_integrate(deme_handle* h);
+/* n full steps (contact detection every cd_update_freq steps, forces, integration), as DoDynamics
+ * (src/DEM/APIPublic.cpp:871-892) driven by DoStepDynamics. */
+int32_t deme_step(deme_handle* h, int32_t n_steps);
+/* Block until all work of this handle is done. */
+int32_t deme_sync(deme_handle* h);
+
+/* State and contact transfer (GetOwner* / SetOwner*, src/DEM/API.h:196-214; WriteContactFile, API.h:324). */
+int32_t deme_download_state(deme_handle* h, deme_state* out);
+int32_t deme_upload_state(deme_handle* h, const deme_state* in);
+int32_t deme_get_num_contacts(deme_handle* h, uint32_t* n);
+int32_t deme_download_contacts(deme_handle* h, deme_contacts* out);
+/* Replace the current contact list and its wildcards (history); mapping is ignored.  Used to inject identical
+ * kT products into dT for parity checks. */
+int32_t deme_upload_contacts(deme_handle* h, const deme_contacts* in);
+int32_t deme_download_contact_forces(deme_handle* h, deme_contact_forces* out);
+
+/* Streams: kT (contact detection) and dT (dynamics) work queues; NULL restores the handle's own streams.
+ * The two workers of the reference are host threads with one stream each (src/core/utils/GpuManager.cpp:8-32). */
+int32_t deme_set_streams(deme_handle* h, void* kT_stream, void* dT_stream);
+
+/* Simulation time advanced so far and step counter. */
+int32_t deme_get_time(deme_handle* h, double* t, int64_t* steps);
+/* Sum of 0.5 m v^2 + 0.5 I omega^2 over clump owners (DEMOwnerQueryKernels.cu:10-37 computes the per-owner term;
+ * the reference's GetTotalKineticEnergy returns 0, src/DEM/dT.cpp:154-171). */
+int32_t deme_kinetic_energy(deme_handle* h, double* ke);
+
+/* Bin assignment of the reference (getNumberOfBinsEachSphereTouches / populateBinSphereTouchingPairs, radix sort
+ * by bin: src/kernel/DEMBinSphereKernels.cu:12-230, src/algorithms/DEMCubContactDetection.cu:59-129) on the current
+ * state.  Fills per-sphere bin counts and, if pair arrays are given with enough capacity, the (bin, sphere) pairs
+ * sorted by bin (stable).  *n_pairs receives the pair count. */
+int32_t deme_bin_assignment(deme_handle* h, uint16_t* n_bins_per_sphere, uint8_t* n_anal_per_sphere,
+                            uint32_t pair_capacity, uint32_t* bin_ids, uint32_t* sphere_ids, uint32_t* n_pairs);
+
+/* Stable radix sort of (key, value) u32 pairs held in device memory (project-written onesweep sort; replaces
+ * cub::DeviceRadixSort::SortPairs, src/algorithms/DEMCubWrappers.cu:43-59).  Sorts bits [0, key_bits). */
+int32_t deme_radix_sort_pairs_device(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                                     uint32_t* vals_out, uint32_t n, int32_t key_bits, void* scratch,
+                                     size_t scratch_bytes, void* stream);
+size_t deme_radix_sort_scratch_bytes(uint32_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DEME_B200_H */
