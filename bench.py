@@ -1,0 +1,348 @@
+#!/usr/bin/env python
+"""Benchmark: M sphere-steps/s of the DEM hot path on the rotating-drum workload (1M three-sphere clumps, 3M
+spheres, analytical cylinder + two end planes, 20 rpm), one full step = contact detection + fused Hertz-Mindlin
+forces + integration.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--clumps M]
+
+N > 1 runs under torchrun (one process per GPU); every rank advances its own independent drum (replicas only: one
+scene does not shard), value = all ranks' sphere-steps / max-over-ranks device time.
+
+Timing: W untimed steps, then K steps bracketed by a barrier and torch.cuda.synchronize(), timed with CUDA events
+recorded on the stream the library launches on.  The owner/sphere/contact arrays (several hundred MB) exceed the
+126 MB L2, so no explicit flush is done.  A second short pass brackets every kernel with events to get the
+per-kernel durations that give the roofline of the dominant kernel; an e2e pass goes through the C ABI with a
+pinned host-to-device update of the drum's prescribed rotation and a device-to-host read of the kinetic energy
+every step.
+
+--impl reference times the CPU implementation of the same method (the C oracle with OpenMP on all host cores;
+the reference itself has no CPU solver and cannot express the analytical cylinder) on a bounded sample of the
+drum workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "dem-engine-sbel_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "M sphere-steps/s"
+UNIT = "M sphere-steps/s"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms",
+                                          "200", "-i", str(self.index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except Exception:
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def algorithmic_bytes(kernel: str, nS: int, nO: int, nC: int, n_cells: int) -> float:
+    """Compulsory HBM bytes of one launch (every array element read or written once per use, SoA)."""
+    if kernel == "force":
+        # per contact: idA, idB, type (9 B) + history read and write (32 B); per sphere: relPos+radius, owner,
+        # material (21 B); per owner: voxel, loc, quat, vel+mass, omega, MOI (80 B) + accumulators (32 B)
+        return 41.0 * nC + 21.0 * nS + 112.0 * nO
+    if kernel == "pair_count":
+        # per sphere: ID-order posF, exact position, owner, radius (60 B) + cell-order posF, id (20 B) + count (4 B);
+        # the cell table once
+        return 84.0 * nS + 4.0 * n_cells
+    if kernel == "pair_emit":
+        return 84.0 * nS + 4.0 * n_cells + 9.0 * nC + 4.0 * nS
+    if kernel == "integrate":
+        return 160.0 * nO
+    if kernel == "sort_onesweep":
+        return 16.0 * nS
+    if kernel == "sphere_prep":
+        return (21.0 + 4.0) * nS + 30.0 * nO + (24 + 16 + 8 + 1) * nS
+    if kernel == "history":
+        return (9.0 + 16.0 + 4.0) * nC + 9.0 * nC + 16.0 * nC
+    return 0.0
+
+
+def build_drum(n_clumps: int, seed: int):
+    from deme_b200 import workloads
+    return workloads.drum(n_clumps=n_clumps, seed=seed)
+
+
+def run_reference(args):
+    """CPU implementation of the same method (the C oracle, OpenMP on all host cores) on a bounded sample."""
+    from deme_b200 import HandleSolver, capi
+    lib_path = os.path.join(ROOT, "oracle", "_build", "libdeme_oracle.so")
+    if not os.path.exists(lib_path):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+    cores = os.cpu_count() or 1
+    n_clumps = min(args.clumps, args.ref_clumps)
+    built = build_drum(n_clumps, seed=1)
+    orc = HandleSolver(capi.load_library(lib_path), "orc_", built, threads=cores)
+    w = max(1, min(args.warmup, 2))
+    k = max(1, min(args.steps, args.ref_steps))
+    orc.step(w)
+    t0 = time.perf_counter()
+    orc.step(k)
+    dt = time.perf_counter() - t0
+    v = built.n_spheres * k / dt / 1e6
+    sample = (f"drum generator with {n_clumps} clumps ({built.n_spheres} spheres), {k} timed steps after {w} warm-up "
+              f"steps, C oracle (OpenMP)")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": k,
+            "warmup": w, "ms_per_step": dt / k * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 forces, f64 positions, integer voxels", "data": "synthetic (seeded)",
+            "config": {"workload": "rotating drum, three-sphere clumps (sample)", "n_clumps": n_clumps,
+                       "n_spheres": built.n_spheres},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_sample(args):
+    from deme_b200 import HandleSolver, capi
+    lib_path = os.path.join(ROOT, "oracle", "_build", "libdeme_oracle.so")
+    if not os.path.exists(lib_path):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+    cores = os.cpu_count() or 1
+    n_clumps = min(args.clumps, args.ref_clumps)
+    built = build_drum(n_clumps, seed=1)
+    orc = HandleSolver(capi.load_library(lib_path), "orc_", built, threads=cores)
+    orc.step(1)
+    k = max(1, args.ref_steps)
+    t0 = time.perf_counter()
+    orc.step(k)
+    dt = time.perf_counter() - t0
+    return {"value": built.n_spheres * k / dt / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"C oracle (OpenMP, {cores} threads) on the drum generator with {n_clumps} clumps "
+                      f"({built.n_spheres} spheres), {k} steps after 1 warm-up step"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--clumps", type=int, default=1_000_000)
+    ap.add_argument("--ref-clumps", type=int, default=100_000)
+    ap.add_argument("--ref-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return
+
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from deme_b200 import Solver, capi
+    from deme_b200 import solver as solver_mod
+
+    built = build_drum(args.clumps, seed=2 + rank)
+    s = Solver(built)
+    lib = s.lib
+    lib.deme_launch_count.restype = C.c_int64
+    lib.deme_kernel_timing.argtypes = [C.c_int32]
+    lib.deme_kernel_times.argtypes = [C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_double),
+                                      C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
+    lib.deme_set_streams.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.deme_set_family_prescription.argtypes = [C.c_void_p, C.c_int32, C.POINTER(capi.FamilyPrescription)]
+    stream = torch.cuda.Stream()
+    lib.deme_set_streams(s.h, C.c_void_p(stream.cuda_stream), C.c_void_p(stream.cuda_stream))
+
+    # ---- warm-up ----
+    s.step(args.warmup)
+    s.sync()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+
+    # ---- timed region ----
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    n0 = lib.deme_launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    s.step(args.steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = lib.deme_launch_count() - n0
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    nC = s.num_contacts()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    ms_max = float(t.item())
+    value = world * built.n_spheres * args.steps / (ms_max / 1e3) / 1e6
+
+    # ---- per-kernel device times (roofline of the dominant kernel) ----
+    k_steps = min(args.steps, 5)
+    lib.deme_kernel_timing(1)
+    s.step(k_steps)
+    s.sync()
+    names = (C.c_char_p * 32)()
+    tot = (C.c_double * 32)()
+    cnt = (C.c_int64 * 32)()
+    nk = C.c_int32(0)
+    lib.deme_kernel_times(32, names, tot, cnt, C.byref(nk))
+    lib.deme_kernel_timing(0)
+    kernels = {names[i].decode(): (tot[i], cnt[i]) for i in range(nk.value) if cnt[i] > 0}
+    dominant = max(kernels, key=lambda k: kernels[k][0])
+    d_ms, d_cnt = kernels[dominant]
+    n_cells = int(s_grid_cells(built))
+    bytes_per_launch = algorithmic_bytes(dominant, built.n_spheres, built.n_owners, s.num_contacts(), n_cells)
+    avg_s = d_ms / d_cnt / 1e3
+    peak, peak_kind = peaks()
+    achieved = bytes_per_launch / avg_s / 1e9 if avg_s > 0 else 0.0
+    traffic = read_traffic(dominant, built.n_spheres, s.num_contacts())
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_s * 1e3,
+                "kernel_ms_per_step": {k: v[0] / k_steps for k, v in kernels.items()}}
+
+    # ---- e2e through the C ABI with host buffers ----
+    drum_fam = 10
+    presc = capi.FamilyPrescription()
+    base = built.prescriptions[drum_fam]
+    C.memmove(C.byref(presc), C.byref(base), C.sizeof(presc))
+    ke = C.c_double(0.0)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        lib.deme_set_family_prescription(s.h, drum_fam, C.byref(presc))
+        s.step(1)
+        ke_val = s.kinetic_energy()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * built.n_spheres * args.steps / float(te.item()) / 1e6
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(args)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 forces/velocities, f64 positions on integer voxels",
+            "data": "synthetic (seeded drum generator)",
+            "config": {"workload": "rotating drum: 1M three-sphere clumps (3M spheres), analytical cylinder + 2 end "
+                                   "planes, 20 rpm, dt 5e-6, CD every step" if args.clumps == 1_000_000 else
+                       f"rotating drum: {args.clumps} three-sphere clumps",
+                       "n_clumps": built.info["n_clumps"], "n_spheres": built.n_spheres,
+                       "n_contacts": nC, "drum_R_m": built.info["R"], "drum_L_m": built.info["L"],
+                       "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+            "roofline": roofline, "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": C.sizeof(capi.FamilyPrescription),
+                    "d2h_bytes_per_step": 8},
+            "gpu_launches": int(launches), "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def s_grid_cells(built):
+    """Cells of the contact search grid (same rule as the library: cell >= max(bin, CD diameter))."""
+    import math
+    p = built.params
+    r = built.arrays["radius"].max() + p.beta
+    cs = max(p.bin_size, 2.0 * float(r)) * (1.0 + 1e-6)
+    n = 1
+    for a in range(3):
+        n *= math.ceil(p.domain[a] / cs) + 1
+    return n
+
+
+def read_traffic(kernel, nS, nC):
+    """DRAM bytes per launch of ``kernel`` from the committed ncu summary, scaled to this launch's size."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)[kernel]
+        scale = (nC / d["n_contacts"]) if d.get("per") == "contact" else (nS / d["n_spheres"])
+        return d["dram_bytes_per_launch"] * scale
+    except Exception:
+        return None
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,902 @@
+// capi.cu -- the solver handle behind the C ABI (include/deme_b200.h).
+//
+// One handle owns all device arrays of one scene on one GPU.  The reference keeps the same data in managed
+// vectors of its two worker threads (src/DEM/dT.h:88-247, src/DEM/kT.h) and copies it between them every step;
+// here kT and dT share one HBM address space, so the kT product is a double-buffered contact list whose roles
+// swap by pointer, and nothing is copied between the halves.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/deme_b200.h"
+#include "kernels.cuh"
+#include "primitives.cuh"
+
+using namespace deme_b200;
+
+namespace {
+
+struct ContactBuf {
+    uint32_t cap = 0;
+    uint32_t* idA = nullptr;
+    uint32_t* idB = nullptr;
+    uint8_t* type = nullptr;
+    float4* hist = nullptr;
+    uint32_t* mapping = nullptr;
+    uint32_t* off = nullptr;  // nS + 1, allocated once
+    ContactView view() const { return ContactView{idA, idB, type, hist, mapping, off}; }
+};
+
+}  // namespace
+
+struct deme_handle {
+    std::string err;
+    int device = 0;
+    cudaStream_t st_dt = nullptr, st_kt = nullptr;
+    cudaStream_t own_dt = nullptr, own_kt = nullptr;
+    deme_sim_params params{};
+    SimConsts k{};
+    uint32_t nO = 0, nS = 0, nA = 0, nM = 0, nClumps = 0;
+    int nW = 0;
+    // scene and state
+    uint64_t* voxel = nullptr;
+    ushort4* loc = nullptr;
+    float4* quat = nullptr;
+    float4* vel = nullptr;
+    float4* omg = nullptr;
+    float4* moi = nullptr;
+    float4* acc = nullptr;
+    float4* alpha = nullptr;
+    float4* sph = nullptr;
+    uint32_t* sOwner = nullptr;
+    uint8_t* sMat = nullptr;
+    uint8_t* masks = nullptr;
+    float* mat = nullptr;  // 5 x nM
+    AnalRaw* analRaw = nullptr;
+    AnalPlaced* analPlaced = nullptr;
+    Prescription* presc = nullptr;
+    // contact detection
+    CDView cd{};
+    uint32_t nCells = 0;
+    int cellBits = 0;
+    ContactBuf lists[2];
+    int cur = 0;
+    uint32_t nContacts = 0;
+    // per-contact outputs
+    bool keepOutputs = false;
+    uint32_t outCap = 0;
+    ContactOutputs outs{nullptr, nullptr, nullptr, nullptr};
+    bool outsValid = false;
+    // scratch
+    void* scratch = nullptr;
+    size_t scratchBytes = 0;
+    uint32_t* dTotal = nullptr;
+    uint32_t* hTotal = nullptr;
+    uint32_t* dErr = nullptr;
+    uint32_t* hErr = nullptr;
+    double* dKE = nullptr;
+    double* hKE = nullptr;
+    Prescription* hPresc = nullptr;
+    double t = 0.0;
+    int64_t steps = 0;
+    std::vector<void*> allocs;
+
+    StateView state_view() const {
+        StateView s;
+        s.voxel = voxel;
+        s.loc = loc;
+        s.quat = quat;
+        s.vel = vel;
+        s.omg = omg;
+        s.moi = moi;
+        s.acc = acc;
+        s.alpha = alpha;
+        s.sph = sph;
+        s.sOwner = sOwner;
+        s.sMat = sMat;
+        s.masks = masks;
+        s.mat = MaterialTable{mat, mat + nM, mat + 2 * nM, mat + 3 * nM, mat + 4 * nM};
+        s.anal = analPlaced;
+        s.nA = nA;
+        s.presc = presc;
+        return s;
+    }
+};
+
+#define CUDA_TRY(h, expr)                                                                        \
+    do {                                                                                         \
+        cudaError_t e_ = (expr);                                                                 \
+        if (e_ != cudaSuccess) {                                                                 \
+            (h)->err = std::string(#expr) + ": " + cudaGetErrorString(e_);                       \
+            return e_ == cudaErrorMemoryAllocation ? DEME_ERR_OOM : DEME_ERR_CUDA;               \
+        }                                                                                        \
+    } while (0)
+
+static int32_t dalloc(deme_handle* h, void** p, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        h->err = std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e);
+        return DEME_ERR_OOM;
+    }
+    h->allocs.push_back(*p);
+    return DEME_OK;
+}
+template <typename T>
+static int32_t dalloc_n(deme_handle* h, T** p, size_t n) {
+    return dalloc(h, reinterpret_cast<void**>(p), n * sizeof(T));
+}
+static void dfree(deme_handle* h, void* p) {
+    if (!p) return;
+    auto it = std::find(h->allocs.begin(), h->allocs.end(), p);
+    if (it != h->allocs.end()) h->allocs.erase(it);
+    cudaFree(p);
+}
+
+#define TRY(expr)                      \
+    do {                               \
+        int32_t s_ = (expr);           \
+        if (s_ != DEME_OK) return s_;  \
+    } while (0)
+
+static int32_t check_launch(deme_handle* h, const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        h->err = std::string(what) + ": " + cudaGetErrorString(e);
+        return DEME_ERR_CUDA;
+    }
+    return DEME_OK;
+}
+
+static int32_t read_device_errors(deme_handle* h) {
+    CUDA_TRY(h, cudaMemcpyAsync(h->hErr, h->dErr, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->st_dt));
+    CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
+    if (*h->hErr) {
+        uint32_t e = *h->hErr;
+        h->err = "device error word 0x" + std::to_string(e) +
+                 ((e & ERR_SORT_LOOKBACK_TIMEOUT) ? " (radix sort look-back timed out)" : "") +
+                 ((e & ERR_CONTACT_CAPACITY) ? " (contact capacity exceeded)" : "") +
+                 ((e & ERR_SEGMENT_TOO_LONG) ? " (contact segment mismatch)" : "");
+        *h->hErr = 0;
+        cudaMemsetAsync(h->dErr, 0, sizeof(uint32_t), h->st_dt);
+        return (e & ERR_SORT_LOOKBACK_TIMEOUT) ? DEME_ERR_TIMEOUT : DEME_ERR_OVERFLOW;
+    }
+    return DEME_OK;
+}
+
+static int32_t ensure_scratch(deme_handle* h, size_t bytes) {
+    if (bytes <= h->scratchBytes) return DEME_OK;
+    dfree(h, h->scratch);
+    h->scratch = nullptr;
+    h->scratchBytes = 0;
+    TRY(dalloc(h, &h->scratch, bytes));
+    h->scratchBytes = bytes;
+    return DEME_OK;
+}
+
+static int32_t ensure_list(deme_handle* h, ContactBuf& b, uint32_t n) {
+    if (n <= b.cap) return DEME_OK;
+    uint32_t cap = std::max<uint32_t>(1024u, (uint32_t)std::min<uint64_t>(0xFFFFFFF0ull, (uint64_t)n * 5 / 4 + 64));
+    dfree(h, b.idA);
+    dfree(h, b.idB);
+    dfree(h, b.type);
+    dfree(h, b.hist);
+    dfree(h, b.mapping);
+    b.idA = b.idB = b.mapping = nullptr;
+    b.type = nullptr;
+    b.hist = nullptr;
+    b.cap = 0;
+    TRY(dalloc_n(h, &b.idA, cap));
+    TRY(dalloc_n(h, &b.idB, cap));
+    TRY(dalloc_n(h, &b.type, cap));
+    TRY(dalloc_n(h, &b.hist, cap));
+    TRY(dalloc_n(h, &b.mapping, cap));
+    b.cap = cap;
+    return DEME_OK;
+}
+
+static int32_t ensure_outputs(deme_handle* h, uint32_t n) {
+    if (n <= h->outCap) return DEME_OK;
+    uint32_t cap = std::max<uint32_t>(1024u, n + n / 4);
+    dfree(h, h->outs.F);
+    dfree(h, h->outs.TOF);
+    dfree(h, h->outs.CPA);
+    dfree(h, h->outs.CPB);
+    h->outs = ContactOutputs{nullptr, nullptr, nullptr, nullptr};
+    h->outCap = 0;
+    TRY(dalloc_n(h, &h->outs.F, cap));
+    TRY(dalloc_n(h, &h->outs.TOF, cap));
+    TRY(dalloc_n(h, &h->outs.CPA, cap));
+    TRY(dalloc_n(h, &h->outs.CPB, cap));
+    h->outCap = cap;
+    return DEME_OK;
+}
+
+extern "C" {
+
+int32_t deme_abi_version(void) { return DEME_B200_ABI_VERSION; }
+
+const char* deme_status_string(int32_t s) {
+    switch (s) {
+        case DEME_OK: return "DEME_OK";
+        case DEME_ERR_INVALID: return "DEME_ERR_INVALID";
+        case DEME_ERR_CUDA: return "DEME_ERR_CUDA";
+        case DEME_ERR_OOM: return "DEME_ERR_OOM";
+        case DEME_ERR_OVERFLOW: return "DEME_ERR_OVERFLOW";
+        case DEME_ERR_NVRTC: return "DEME_ERR_NVRTC";
+        case DEME_ERR_TIMEOUT: return "DEME_ERR_TIMEOUT";
+        case DEME_ERR_STATE: return "DEME_ERR_STATE";
+        case DEME_ERR_NO_DEVICE: return "DEME_ERR_NO_DEVICE";
+        default: return "unknown";
+    }
+}
+
+const char* deme_get_error(deme_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_scene* s) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        h->err = "no CUDA device";
+        return DEME_ERR_NO_DEVICE;
+    }
+    CUDA_TRY(h, cudaGetDevice(&h->device));
+    h->params = *p;
+    h->nO = s->n_owners;
+    h->nS = s->n_spheres;
+    h->nA = s->n_anal;
+    h->nM = s->n_materials;
+    h->nW = p->n_contact_wildcards;
+    if (h->nW != 0 && h->nW != 4) {
+        h->err = "the built-in models use 0 or 4 contact wildcards";
+        return DEME_ERR_INVALID;
+    }
+    if (h->nA > 255) {
+        h->err = "at most 255 analytical components";
+        return DEME_ERR_INVALID;
+    }
+    const uint32_t nO = h->nO, nS = h->nS, nA = h->nA, nM = h->nM;
+    // clumps are the owners referenced by spheres; analytical owners follow them
+    uint32_t nClumps = 0;
+    for (uint32_t i = 0; i < nS; i++) nClumps = std::max(nClumps, s->sphere_owner[i] + 1);
+    for (uint32_t i = 0; i < nA; i++)
+        if (s->anal_owner[i] < nClumps || s->anal_owner[i] >= nO) {
+            h->err = "analytical owners must follow the clump owners";
+            return DEME_ERR_INVALID;
+        }
+    for (uint32_t i = 0; i < nS; i++)
+        if (s->sphere_owner[i] >= nO || s->sphere_material[i] >= std::max(nM, 1u)) {
+            h->err = "sphere owner or material out of range";
+            return DEME_ERR_INVALID;
+        }
+    for (uint32_t i = 1; i < nS; i++)
+        if (s->sphere_owner[i] < s->sphere_owner[i - 1]) {
+            h->err = "spheres must be grouped by owner in ascending owner order";
+            return DEME_ERR_INVALID;
+        }
+    h->nClumps = nClumps;
+    CUDA_TRY(h, cudaStreamCreateWithFlags(&h->own_dt, cudaStreamNonBlocking));
+    CUDA_TRY(h, cudaStreamCreateWithFlags(&h->own_kt, cudaStreamNonBlocking));
+    h->st_dt = h->own_dt;
+    h->st_kt = h->own_kt;
+
+    // ---- constants and the contact search grid ----
+    SimConsts& k = h->k;
+    k.nvXp2 = p->nvXp2;
+    k.nvYp2 = p->nvYp2;
+    k.l_kernel = p->l_kernel;
+    k.voxel_kernel = p->voxel_size_kernel;
+    k.bin_size = p->bin_size;
+    k.nbX = p->nbX;
+    k.nbY = p->nbY;
+    k.nbZ = p->nbZ;
+    k.beta = p->beta;
+    k.h = p->h;
+    k.G[0] = p->G[0];
+    k.G[1] = p->G[1];
+    k.G[2] = p->G[2];
+    k.integrator = p->integrator;
+    k.n_spheres = nS;
+    k.n_owners = nO;
+    k.n_anal = nA;
+    float rmax = 0.f;
+    for (uint32_t i = 0; i < nS; i++) {
+        float r = s->radius[i];
+        r += p->beta;
+        rmax = std::max(rmax, r);
+    }
+    k.r_max_cd = rmax;
+    const double world[3] = {p->voxel_size * std::ldexp(1.0, p->nvXp2), p->voxel_size * std::ldexp(1.0, p->nvYp2),
+                             p->voxel_size * std::ldexp(1.0, p->nvZp2)};
+    const double wmax = std::max(world[0], std::max(world[1], world[2]));
+    k.prefilter_abs = (float)(4e-7 * wmax + 1e-9);
+    double dom[3];
+    for (int a = 0; a < 3; a++) dom[a] = p->domain[a] > 0.f ? (double)p->domain[a] : world[a];
+    double cs = std::max(p->bin_size, 2.0 * (double)rmax) * (1.0 + 1e-6);
+    if (!(cs > 0.0)) cs = 1.0;
+    auto ncell = [&](double c, double d) { return (uint64_t)std::ceil(d / c) + 1; };
+    while (ncell(cs, dom[0]) * ncell(cs, dom[1]) * ncell(cs, dom[2]) > (1ull << 26)) cs *= 1.25;
+    k.cell_size = cs;
+    k.gx = (uint32_t)ncell(cs, dom[0]);
+    k.gy = (uint32_t)ncell(cs, dom[1]);
+    k.gz = (uint32_t)ncell(cs, dom[2]);
+    h->nCells = k.gx * k.gy * k.gz;
+    h->cellBits = 1;
+    while ((1ull << h->cellBits) < h->nCells) h->cellBits++;
+
+    // ---- device arrays ----
+    TRY(dalloc_n(h, &h->voxel, nO));
+    TRY(dalloc_n(h, &h->loc, nO));
+    TRY(dalloc_n(h, &h->quat, nO));
+    TRY(dalloc_n(h, &h->vel, nO));
+    TRY(dalloc_n(h, &h->omg, nO));
+    TRY(dalloc_n(h, &h->moi, nO));
+    TRY(dalloc_n(h, &h->acc, nO));
+    TRY(dalloc_n(h, &h->alpha, nO));
+    TRY(dalloc_n(h, &h->sph, nS));
+    TRY(dalloc_n(h, &h->sOwner, nS));
+    TRY(dalloc_n(h, &h->sMat, nS));
+    TRY(dalloc_n(h, &h->masks, DEME_NUM_FAMILY_MASK));
+    TRY(dalloc_n(h, &h->mat, 5 * std::max(nM, 1u)));
+    TRY(dalloc_n(h, &h->analRaw, std::max(nA, 1u)));
+    TRY(dalloc_n(h, &h->analPlaced, std::max(nA, 1u)));
+    TRY(dalloc_n(h, &h->presc, DEME_NUM_FAMILIES));
+    {
+        std::vector<ushort4> loc(nO);
+        std::vector<float4> quat(nO), vel(nO), omg(nO), moi(nO);
+        for (uint32_t o = 0; o < nO; o++) {
+            loc[o] = make_ushort4(s->locX[o], s->locY[o], s->locZ[o], s->family[o]);
+            quat[o] = make_float4(s->oriQw[o], s->oriQx[o], s->oriQy[o], s->oriQz[o]);
+            vel[o] = make_float4(s->vX[o], s->vY[o], s->vZ[o], s->mass[o]);
+            omg[o] = make_float4(s->omgX[o], s->omgY[o], s->omgZ[o], 0.f);
+            moi[o] = make_float4(s->mmiXX[o], s->mmiYY[o], s->mmiZZ[o], 0.f);
+        }
+        CUDA_TRY(h, cudaMemcpy(h->voxel, s->voxel, nO * sizeof(uint64_t), cudaMemcpyHostToDevice));
+        CUDA_TRY(h, cudaMemcpy(h->loc, loc.data(), nO * sizeof(ushort4), cudaMemcpyHostToDevice));
+        CUDA_TRY(h, cudaMemcpy(h->quat, quat.data(), nO * sizeof(float4), cudaMemcpyHostToDevice));
+        CUDA_TRY(h, cudaMemcpy(h->vel, vel.data(), nO * sizeof(float4), cudaMemcpyHostToDevice));
+        CUDA_TRY(h, cudaMemcpy(h->omg, omg.data(), nO * sizeof(float4), cudaMemcpyHostToDevice));
+        CUDA_TRY(h, cudaMemcpy(h->moi, moi.data(), nO * sizeof(float4), cudaMemcpyHostToDevice));
+        CUDA_TRY(h, cudaMemset(h->acc, 0, nO * sizeof(float4)));
+        CUDA_TRY(h, cudaMemset(h->alpha, 0, nO * sizeof(float4)));
+        std::vector<float4> sph(nS);
+        for (uint32_t i = 0; i < nS; i++) sph[i] = make_float4(s->relX[i], s->relY[i], s->relZ[i], s->radius[i]);
+        CUDA_TRY(h, cudaMemcpy(h->sph, sph.data(), nS * sizeof(float4), cudaMemcpyHostToDevice));
+        CUDA_TRY(h, cudaMemcpy(h->sOwner, s->sphere_owner, nS * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        CUDA_TRY(h, cudaMemcpy(h->sMat, s->sphere_material, nS, cudaMemcpyHostToDevice));
+        std::vector<uint8_t> masks(DEME_NUM_FAMILY_MASK, 0);
+        if (s->family_masks) std::memcpy(masks.data(), s->family_masks, DEME_NUM_FAMILY_MASK);
+        CUDA_TRY(h, cudaMemcpy(h->masks, masks.data(), DEME_NUM_FAMILY_MASK, cudaMemcpyHostToDevice));
+        std::vector<float> mat(5 * std::max(nM, 1u), 0.f);
+        for (uint32_t m = 0; m < nM; m++) {
+            mat[m] = s->mat_E[m];
+            mat[nM + m] = s->mat_nu[m];
+            mat[2 * nM + m] = s->mat_CoR[m];
+            mat[3 * nM + m] = s->mat_mu[m];
+            mat[4 * nM + m] = s->mat_Crr[m];
+        }
+        CUDA_TRY(h, cudaMemcpy(h->mat, mat.data(), mat.size() * sizeof(float), cudaMemcpyHostToDevice));
+        std::vector<AnalRaw> raw(std::max(nA, 1u));
+        for (uint32_t a = 0; a < nA; a++) {
+            AnalRaw r{};
+            r.relX = s->anal_relX[a];
+            r.relY = s->anal_relY[a];
+            r.relZ = s->anal_relZ[a];
+            r.rotX = s->anal_rotX[a];
+            r.rotY = s->anal_rotY[a];
+            r.rotZ = s->anal_rotZ[a];
+            r.size1 = s->anal_size1[a];
+            r.size2 = s->anal_size2[a];
+            r.size3 = s->anal_size3[a];
+            r.mass = s->anal_mass[a];
+            r.owner = s->anal_owner[a];
+            r.type = s->anal_type[a];
+            r.normal = s->anal_normal[a];
+            r.material = s->anal_material[a];
+            // cone wall: sin and cos of the half angle, computed once on the host
+            r.c1 = std::sin((double)r.size1);
+            r.c2 = std::cos((double)r.size1);
+            if (r.material >= std::max(nM, 1u)) {
+                h->err = "analytical material out of range";
+                return DEME_ERR_INVALID;
+            }
+            raw[a] = r;
+        }
+        CUDA_TRY(h, cudaMemcpy(h->analRaw, raw.data(), raw.size() * sizeof(AnalRaw), cudaMemcpyHostToDevice));
+        std::vector<Prescription> pr(DEME_NUM_FAMILIES);
+        for (int f = 0; f < DEME_NUM_FAMILIES; f++) {
+            Prescription q{};
+            if (s->prescriptions) {
+                const deme_family_prescription& src = s->prescriptions[f];
+                q.used = src.used;
+                q.lin_vel = src.lin_vel_prescribed;
+                q.rot_vel = src.rot_vel_prescribed;
+                q.lin_pos = src.lin_pos_prescribed;
+                q.rot_pos = src.rot_pos_prescribed;
+                for (int c = 0; c < 3; c++) {
+                    q.has_vel[c] = src.has_vel[c];
+                    q.has_omg[c] = src.has_omg[c];
+                    q.has_pos[c] = src.has_pos[c];
+                    q.vel[c] = src.vel[c];
+                    q.omg[c] = src.omg[c];
+                    q.pos[c] = src.pos[c];
+                }
+            }
+            pr[f] = q;
+        }
+        CUDA_TRY(h, cudaMemcpy(h->presc, pr.data(), pr.size() * sizeof(Prescription), cudaMemcpyHostToDevice));
+    }
+    // ---- contact-detection work arrays ----
+    CDView& cd = h->cd;
+    TRY(dalloc_n(h, &cd.pX, nS));
+    TRY(dalloc_n(h, &cd.pY, nS));
+    TRY(dalloc_n(h, &cd.pZ, nS));
+    TRY(dalloc_n(h, &cd.posF, nS));
+    TRY(dalloc_n(h, &cd.posFSorted, nS));
+    TRY(dalloc_n(h, &cd.cellKey, nS));
+    TRY(dalloc_n(h, &cd.idSeq, nS));
+    TRY(dalloc_n(h, &cd.keySorted, nS));
+    TRY(dalloc_n(h, &cd.idSorted, nS));
+    TRY(dalloc_n(h, &cd.cellCount, (size_t)h->nCells + 1));
+    TRY(dalloc_n(h, &cd.cellStart, (size_t)h->nCells + 1));
+    TRY(dalloc_n(h, &cd.nAnal, nS));
+    TRY(dalloc_n(h, &cd.cnt, (size_t)nS + 1));
+    for (int b = 0; b < 2; b++) {
+        TRY(dalloc_n(h, &h->lists[b].off, (size_t)nS + 1));
+        CUDA_TRY(h, cudaMemset(h->lists[b].off, 0, ((size_t)nS + 1) * sizeof(uint32_t)));
+        TRY(ensure_list(h, h->lists[b], std::max<uint32_t>(1024u, 4u * nS)));
+    }
+    TRY(ensure_scratch(h, std::max(radix_sort_scratch_bytes(nS), scan_scratch_bytes(std::max(h->nCells + 1, nS + 1)))));
+    TRY(dalloc_n(h, &h->dTotal, 4));
+    TRY(dalloc_n(h, &h->dErr, 4));
+    TRY(dalloc_n(h, &h->dKE, 2));
+    CUDA_TRY(h, cudaMemset(h->dErr, 0, 4 * sizeof(uint32_t)));
+    CUDA_TRY(h, cudaMallocHost(&h->hTotal, 4 * sizeof(uint32_t)));
+    CUDA_TRY(h, cudaMallocHost(&h->hErr, 4 * sizeof(uint32_t)));
+    CUDA_TRY(h, cudaMallocHost(&h->hKE, 2 * sizeof(double)));
+    *h->hErr = 0;
+    CUDA_TRY(h, cudaDeviceSynchronize());
+    return DEME_OK;
+}
+
+int32_t deme_create(const deme_sim_params* params, const deme_scene* scene, deme_handle** out) {
+    if (!params || !scene || !out) return DEME_ERR_INVALID;
+    *out = nullptr;
+    deme_handle* h = new deme_handle();
+    int32_t st = create_impl(h, params, scene);
+    if (st != DEME_OK) {
+        // keep the handle so the caller can read the message; it owns no live work
+        *out = h;
+        return st;
+    }
+    *out = h;
+    return DEME_OK;
+}
+
+void deme_destroy(deme_handle* h) {
+    if (!h) return;
+    if (h->own_dt) cudaStreamSynchronize(h->own_dt);
+    if (h->own_kt) cudaStreamSynchronize(h->own_kt);
+    for (void* p : h->allocs) cudaFree(p);
+    h->allocs.clear();
+    if (h->hTotal) cudaFreeHost(h->hTotal);
+    if (h->hErr) cudaFreeHost(h->hErr);
+    if (h->hKE) cudaFreeHost(h->hKE);
+    if (h->hPresc) cudaFreeHost(h->hPresc);
+    if (h->own_dt) cudaStreamDestroy(h->own_dt);
+    if (h->own_kt) cudaStreamDestroy(h->own_kt);
+    delete h;
+}
+
+int32_t deme_set_force_model(deme_handle* h, const char* src, const char* const* names, int32_t n) {
+    if (!h) return DEME_ERR_INVALID;
+    if (src == nullptr) return DEME_OK;
+    h->err = "custom force models need the NVRTC front end, which this build does not include yet";
+    return DEME_ERR_NVRTC;
+}
+
+int32_t deme_set_streams(deme_handle* h, void* kT_stream, void* dT_stream) {
+    if (!h) return DEME_ERR_INVALID;
+    h->st_kt = kT_stream ? (cudaStream_t)kT_stream : h->own_kt;
+    h->st_dt = dT_stream ? (cudaStream_t)dT_stream : h->own_dt;
+    return DEME_OK;
+}
+
+int32_t deme_keep_contact_forces(deme_handle* h, int32_t enable) {
+    if (!h) return DEME_ERR_INVALID;
+    h->keepOutputs = enable != 0;
+    return DEME_OK;
+}
+
+// ---------------------------------------------------------------------------------------------------- kT ----
+int32_t deme_detect_contacts(deme_handle* h) {
+    if (!h) return DEME_ERR_INVALID;
+    cudaStream_t st = h->st_dt;
+    const SimConsts& k = h->k;
+    StateView s = h->state_view();
+    CDView& cd = h->cd;
+    launch_place_anal(k, s, h->analRaw, h->analPlaced, h->nA, st);
+    CUDA_TRY(h, cudaMemsetAsync(cd.cellCount, 0, ((size_t)h->nCells + 1) * sizeof(uint32_t), st));
+    launch_sphere_prep(k, s, cd, st);
+    exclusive_scan_u32(cd.cellCount, h->nCells + 1, cd.cellStart, nullptr, h->scratch, st);
+    radix_sort_pairs(cd.cellKey, cd.idSeq, cd.keySorted, cd.idSorted, h->nS, h->cellBits, h->scratch, h->dErr, st);
+    launch_gather_sorted(k, cd, st);
+    launch_pair_count(k, s, cd, st);
+    TRY(check_launch(h, "contact count"));
+    const int nxt = h->cur ^ 1;
+    ContactBuf& nb = h->lists[nxt];
+    ContactBuf& pb = h->lists[h->cur];
+    exclusive_scan_u32(cd.cnt, h->nS + 1, nb.off, h->dTotal, h->scratch, st);
+    CUDA_TRY(h, cudaMemcpyAsync(h->hTotal, h->dTotal, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    const uint32_t n = *h->hTotal;
+    TRY(ensure_list(h, nb, n));
+    launch_pair_emit(k, s, cd, nb.view(), nb.cap, h->dErr, st);
+    launch_history(k, nb.view(), pb.view(), n, h->nW > 0, st);
+    TRY(check_launch(h, "contact emit"));
+    h->cur = nxt;
+    h->nContacts = n;
+    h->outsValid = false;
+    return read_device_errors(h);
+}
+
+// ---------------------------------------------------------------------------------------------------- dT ----
+int32_t deme_compute_forces(deme_handle* h) {
+    if (!h) return DEME_ERR_INVALID;
+    cudaStream_t st = h->st_dt;
+    const SimConsts& k = h->k;
+    StateView s = h->state_view();
+    launch_place_anal(k, s, h->analRaw, h->analPlaced, h->nA, st);
+    // prepareForceArrays (src/kernel/DEMPrepForceKernels.cu:23-31): accumulators start from zero every step
+    CUDA_TRY(h, cudaMemsetAsync(h->acc, 0, h->nO * sizeof(float4), st));
+    CUDA_TRY(h, cudaMemsetAsync(h->alpha, 0, h->nO * sizeof(float4), st));
+    const ContactBuf& c = h->lists[h->cur];
+    const ContactOutputs* out = nullptr;
+    if (h->keepOutputs) {
+        TRY(ensure_outputs(h, h->nContacts));
+        out = &h->outs;
+    }
+    launch_force(k, s, c.view(), h->nContacts, h->nW > 0, out, st);
+    TRY(check_launch(h, "force"));
+    h->outsValid = out != nullptr;
+    return DEME_OK;
+}
+
+int32_t deme_integrate(deme_handle* h) {
+    if (!h) return DEME_ERR_INVALID;
+    cudaStream_t st = h->st_dt;
+    launch_integrate(h->k, h->state_view(), st);
+    TRY(check_launch(h, "integrate"));
+    h->t += (double)h->k.h;
+    h->steps++;
+    return DEME_OK;
+}
+
+int32_t deme_step(deme_handle* h, int32_t n_steps) {
+    if (!h) return DEME_ERR_INVALID;
+    for (int32_t i = 0; i < n_steps; i++) {
+        const int f = h->params.cd_update_freq;
+        if (f <= 0 || (h->steps % f) == 0) TRY(deme_detect_contacts(h));
+        TRY(deme_compute_forces(h));
+        TRY(deme_integrate(h));
+    }
+    return check_launch(h, "step");
+}
+
+int32_t deme_sync(deme_handle* h) {
+    if (!h) return DEME_ERR_INVALID;
+    CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
+    CUDA_TRY(h, cudaStreamSynchronize(h->st_kt));
+    return read_device_errors(h);
+}
+
+// ---------------------------------------------------------------------------------------------- transfer ----
+int32_t deme_download_state(deme_handle* h, deme_state* o) {
+    if (!h || !o) return DEME_ERR_INVALID;
+    const uint32_t n = h->nO;
+    CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
+    std::vector<ushort4> loc(n);
+    std::vector<float4> q(n), v(n), w(n), a(n), al(n);
+    CUDA_TRY(h, cudaMemcpy(loc.data(), h->loc, n * sizeof(ushort4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(q.data(), h->quat, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(v.data(), h->vel, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(w.data(), h->omg, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(a.data(), h->acc, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(al.data(), h->alpha, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    if (o->voxel) CUDA_TRY(h, cudaMemcpy(o->voxel, h->voxel, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < n; i++) {
+        if (o->locX) o->locX[i] = loc[i].x;
+        if (o->locY) o->locY[i] = loc[i].y;
+        if (o->locZ) o->locZ[i] = loc[i].z;
+        if (o->family) o->family[i] = (uint8_t)loc[i].w;
+        if (o->oriQw) o->oriQw[i] = q[i].x;
+        if (o->oriQx) o->oriQx[i] = q[i].y;
+        if (o->oriQy) o->oriQy[i] = q[i].z;
+        if (o->oriQz) o->oriQz[i] = q[i].w;
+        if (o->vX) o->vX[i] = v[i].x;
+        if (o->vY) o->vY[i] = v[i].y;
+        if (o->vZ) o->vZ[i] = v[i].z;
+        if (o->omgX) o->omgX[i] = w[i].x;
+        if (o->omgY) o->omgY[i] = w[i].y;
+        if (o->omgZ) o->omgZ[i] = w[i].z;
+        if (o->aX) o->aX[i] = a[i].x;
+        if (o->aY) o->aY[i] = a[i].y;
+        if (o->aZ) o->aZ[i] = a[i].z;
+        if (o->alphaX) o->alphaX[i] = al[i].x;
+        if (o->alphaY) o->alphaY[i] = al[i].y;
+        if (o->alphaZ) o->alphaZ[i] = al[i].z;
+    }
+    return DEME_OK;
+}
+
+int32_t deme_upload_state(deme_handle* h, const deme_state* s) {
+    if (!h || !s) return DEME_ERR_INVALID;
+    const uint32_t n = h->nO;
+    CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
+    std::vector<ushort4> loc(n);
+    std::vector<float4> q(n), v(n), w(n), a(n), al(n);
+    CUDA_TRY(h, cudaMemcpy(loc.data(), h->loc, n * sizeof(ushort4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(q.data(), h->quat, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(v.data(), h->vel, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(w.data(), h->omg, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(a.data(), h->acc, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(al.data(), h->alpha, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < n; i++) {
+        if (s->locX) loc[i].x = s->locX[i];
+        if (s->locY) loc[i].y = s->locY[i];
+        if (s->locZ) loc[i].z = s->locZ[i];
+        if (s->family) loc[i].w = s->family[i];
+        if (s->oriQw) q[i].x = s->oriQw[i];
+        if (s->oriQx) q[i].y = s->oriQx[i];
+        if (s->oriQy) q[i].z = s->oriQy[i];
+        if (s->oriQz) q[i].w = s->oriQz[i];
+        if (s->vX) v[i].x = s->vX[i];
+        if (s->vY) v[i].y = s->vY[i];
+        if (s->vZ) v[i].z = s->vZ[i];
+        if (s->omgX) w[i].x = s->omgX[i];
+        if (s->omgY) w[i].y = s->omgY[i];
+        if (s->omgZ) w[i].z = s->omgZ[i];
+        if (s->aX) a[i].x = s->aX[i];
+        if (s->aY) a[i].y = s->aY[i];
+        if (s->aZ) a[i].z = s->aZ[i];
+        if (s->alphaX) al[i].x = s->alphaX[i];
+        if (s->alphaY) al[i].y = s->alphaY[i];
+        if (s->alphaZ) al[i].z = s->alphaZ[i];
+    }
+    if (s->voxel) CUDA_TRY(h, cudaMemcpy(h->voxel, s->voxel, n * sizeof(uint64_t), cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(h->loc, loc.data(), n * sizeof(ushort4), cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(h->quat, q.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(h->vel, v.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(h->omg, w.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(h->acc, a.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(h->alpha, al.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    return DEME_OK;
+}
+
+int32_t deme_get_num_contacts(deme_handle* h, uint32_t* n) {
+    if (!h || !n) return DEME_ERR_INVALID;
+    *n = h->nContacts;
+    return DEME_OK;
+}
+
+int32_t deme_download_contacts(deme_handle* h, deme_contacts* o) {
+    if (!h || !o) return DEME_ERR_INVALID;
+    const uint32_t n = h->nContacts;
+    o->n_contacts = n;
+    if (o->capacity < n) return DEME_ERR_OVERFLOW;
+    CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
+    const ContactBuf& c = h->lists[h->cur];
+    if (n == 0) return DEME_OK;
+    if (o->idA) CUDA_TRY(h, cudaMemcpy(o->idA, c.idA, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (o->idB) CUDA_TRY(h, cudaMemcpy(o->idB, c.idB, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (o->type) CUDA_TRY(h, cudaMemcpy(o->type, c.type, n, cudaMemcpyDeviceToHost));
+    if (o->mapping) CUDA_TRY(h, cudaMemcpy(o->mapping, c.mapping, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (o->wildcards && h->nW > 0) {
+        std::vector<float4> hw(n);
+        CUDA_TRY(h, cudaMemcpy(hw.data(), c.hist, n * sizeof(float4), cudaMemcpyDeviceToHost));
+        for (uint32_t i = 0; i < n; i++) {
+            o->wildcards[i] = hw[i].x;
+            o->wildcards[(size_t)o->capacity + i] = hw[i].y;
+            o->wildcards[2 * (size_t)o->capacity + i] = hw[i].z;
+            o->wildcards[3 * (size_t)o->capacity + i] = hw[i].w;
+        }
+    }
+    return DEME_OK;
+}
+
+int32_t deme_upload_contacts(deme_handle* h, const deme_contacts* in) {
+    if (!h || !in) return DEME_ERR_INVALID;
+    const uint32_t n = in->n_contacts;
+    for (uint32_t i = 0; i < n; i++) {
+        const bool ss = in->type[i] == DEME_SPHERE_SPHERE_CONTACT;
+        if (in->idA[i] >= h->nS || (ss && in->idB[i] >= h->nS) || (!ss && in->idB[i] >= h->nA)) {
+            h->err = "contact ids out of range";
+            return DEME_ERR_INVALID;
+        }
+    }
+    // canonical order: (idA, group, idB), group 0 = sphere--analytical
+    std::vector<uint32_t> perm(n);
+    std::iota(perm.begin(), perm.end(), 0u);
+    std::stable_sort(perm.begin(), perm.end(), [&](uint32_t a, uint32_t b) {
+        const uint32_t ga = in->type[a] == DEME_SPHERE_SPHERE_CONTACT, gb = in->type[b] == DEME_SPHERE_SPHERE_CONTACT;
+        if (in->idA[a] != in->idA[b]) return in->idA[a] < in->idA[b];
+        if (ga != gb) return ga < gb;
+        return in->idB[a] < in->idB[b];
+    });
+    std::vector<uint32_t> A(n), B(n), off(h->nS + 1, 0);
+    std::vector<uint8_t> T(n);
+    std::vector<float4> hw(n, make_float4(0.f, 0.f, 0.f, 0.f));
+    for (uint32_t i = 0; i < n; i++) {
+        const uint32_t j = perm[i];
+        A[i] = in->idA[j];
+        B[i] = in->idB[j];
+        T[i] = in->type[j];
+        if (in->wildcards && h->nW > 0)
+            hw[i] = make_float4(in->wildcards[j], in->wildcards[(size_t)in->capacity + j],
+                                in->wildcards[2 * (size_t)in->capacity + j], in->wildcards[3 * (size_t)in->capacity + j]);
+        off[A[i] + 1]++;
+    }
+    for (uint32_t s = 0; s < h->nS; s++) off[s + 1] += off[s];
+    CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
+    ContactBuf& c = h->lists[h->cur];
+    TRY(ensure_list(h, c, n));
+    if (n) {
+        CUDA_TRY(h, cudaMemcpy(c.idA, A.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        CUDA_TRY(h, cudaMemcpy(c.idB, B.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        CUDA_TRY(h, cudaMemcpy(c.type, T.data(), n, cudaMemcpyHostToDevice));
+        CUDA_TRY(h, cudaMemcpy(c.hist, hw.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+        std::vector<uint32_t> nul(n, DEME_NULL_MAPPING_PARTNER);
+        CUDA_TRY(h, cudaMemcpy(c.mapping, nul.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    }
+    CUDA_TRY(h, cudaMemcpy(c.off, off.data(), off.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    h->nContacts = n;
+    h->outsValid = false;
+    return DEME_OK;
+}
+
+int32_t deme_download_contact_forces(deme_handle* h, deme_contact_forces* o) {
+    if (!h || !o) return DEME_ERR_INVALID;
+    const uint32_t n = h->nContacts;
+    o->n_contacts = n;
+    if (o->capacity < n) return DEME_ERR_OVERFLOW;
+    if (!h->outsValid) {
+        h->err = "per-contact forces were not kept: call deme_keep_contact_forces(h, 1) before deme_compute_forces";
+        return DEME_ERR_STATE;
+    }
+    CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
+    std::vector<float4> tmp(n);
+    float* dst[4] = {o->force, o->torque_only_force, o->cpA, o->cpB};
+    float4* src[4] = {h->outs.F, h->outs.TOF, h->outs.CPA, h->outs.CPB};
+    for (int a = 0; a < 4; a++) {
+        if (!dst[a] || n == 0) continue;
+        CUDA_TRY(h, cudaMemcpy(tmp.data(), src[a], n * sizeof(float4), cudaMemcpyDeviceToHost));
+        for (uint32_t i = 0; i < n; i++) {
+            dst[a][3 * (size_t)i] = tmp[i].x;
+            dst[a][3 * (size_t)i + 1] = tmp[i].y;
+            dst[a][3 * (size_t)i + 2] = tmp[i].z;
+        }
+    }
+    return DEME_OK;
+}
+
+int32_t deme_set_family_prescription(deme_handle* h, int32_t family, const deme_family_prescription* src) {
+    if (!h || !src || family < 0 || family >= DEME_NUM_FAMILIES) return DEME_ERR_INVALID;
+    if (!h->hPresc) CUDA_TRY(h, cudaMallocHost(&h->hPresc, sizeof(Prescription)));
+    CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));  // the staging buffer may still feed an earlier copy
+    Prescription& q = *h->hPresc;
+    q = Prescription{};
+    q.used = src->used;
+    q.lin_vel = src->lin_vel_prescribed;
+    q.rot_vel = src->rot_vel_prescribed;
+    q.lin_pos = src->lin_pos_prescribed;
+    q.rot_pos = src->rot_pos_prescribed;
+    for (int c = 0; c < 3; c++) {
+        q.has_vel[c] = src->has_vel[c];
+        q.has_omg[c] = src->has_omg[c];
+        q.has_pos[c] = src->has_pos[c];
+        q.vel[c] = src->vel[c];
+        q.omg[c] = src->omg[c];
+        q.pos[c] = src->pos[c];
+    }
+    CUDA_TRY(h, cudaMemcpyAsync(h->presc + family, h->hPresc, sizeof(Prescription), cudaMemcpyHostToDevice, h->st_dt));
+    return DEME_OK;
+}
+
+int32_t deme_get_time(deme_handle* h, double* t, int64_t* steps) {
+    if (!h) return DEME_ERR_INVALID;
+    if (t) *t = h->t;
+    if (steps) *steps = h->steps;
+    return DEME_OK;
+}
+
+int32_t deme_kinetic_energy(deme_handle* h, double* ke) {
+    if (!h || !ke) return DEME_ERR_INVALID;
+    launch_kinetic_energy(h->k, h->state_view(), h->nClumps, h->dKE, h->st_dt);
+    CUDA_TRY(h, cudaMemcpyAsync(h->hKE, h->dKE, sizeof(double), cudaMemcpyDeviceToHost, h->st_dt));
+    CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
+    *ke = *h->hKE;
+    return DEME_OK;
+}
+
+int32_t deme_bin_assignment(deme_handle* h, uint16_t* n_bins, uint8_t* n_anal, uint32_t pair_capacity,
+                            uint32_t* bin_ids, uint32_t* sphere_ids, uint32_t* n_pairs) {
+    if (!h) return DEME_ERR_INVALID;
+    cudaStream_t st = h->st_dt;
+    const uint32_t nS = h->nS;
+    StateView s = h->state_view();
+    launch_place_anal(h->k, s, h->analRaw, h->analPlaced, h->nA, st);
+    uint16_t* dNb = nullptr;
+    uint8_t* dNa = nullptr;
+    uint32_t* dOff = nullptr;
+    TRY(dalloc_n(h, &dNb, nS + 1));
+    TRY(dalloc_n(h, &dNa, nS + 1));
+    TRY(dalloc_n(h, &dOff, nS + 1));
+    int32_t rc = DEME_OK;
+    do {
+        launch_bin_count(h->k, s, dNb, dNa, st);
+        exclusive_scan_u16(dNb, nS, dOff, h->dTotal, h->scratch, st);
+        if (cudaMemcpyAsync(h->hTotal, h->dTotal, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            h->err = "bin assignment count failed";
+            rc = DEME_ERR_CUDA;
+            break;
+        }
+        const uint32_t P = nS ? *h->hTotal : 0;
+        if (n_pairs) *n_pairs = P;
+        if (n_bins && nS) cudaMemcpy(n_bins, dNb, nS * sizeof(uint16_t), cudaMemcpyDeviceToHost);
+        if (n_anal && nS) cudaMemcpy(n_anal, dNa, nS, cudaMemcpyDeviceToHost);
+        if (!bin_ids || !sphere_ids) break;
+        if (pair_capacity < P) {
+            rc = DEME_ERR_OVERFLOW;
+            break;
+        }
+        uint32_t *kb = nullptr, *vb = nullptr, *ko = nullptr, *vo = nullptr;
+        void* sc = nullptr;
+        if ((rc = dalloc_n(h, &kb, P + 1)) || (rc = dalloc_n(h, &vb, P + 1)) || (rc = dalloc_n(h, &ko, P + 1)) ||
+            (rc = dalloc_n(h, &vo, P + 1)) || (rc = dalloc(h, &sc, radix_sort_scratch_bytes(P))))
+            break;
+        launch_bin_emit(h->k, s, dOff, kb, vb, st);
+        int bits = 1;
+        const uint64_t nb = (uint64_t)h->k.nbX * h->k.nbY * h->k.nbZ;
+        while (bits < 32 && (1ull << bits) < nb) bits++;
+        radix_sort_pairs(kb, vb, ko, vo, P, bits, sc, h->dErr, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) {
+            h->err = "bin assignment sort failed";
+            rc = DEME_ERR_CUDA;
+        } else if (P) {
+            cudaMemcpy(bin_ids, ko, P * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+            cudaMemcpy(sphere_ids, vo, P * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+        }
+        dfree(h, kb);
+        dfree(h, vb);
+        dfree(h, ko);
+        dfree(h, vo);
+        dfree(h, sc);
+    } while (0);
+    dfree(h, dNb);
+    dfree(h, dNa);
+    dfree(h, dOff);
+    if (rc != DEME_OK) return rc;
+    return read_device_errors(h);
+}
+
+int32_t deme_radix_sort_pairs_device(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                                     uint32_t* vals_out, uint32_t n, int32_t key_bits, void* scratch,
+                                     size_t scratch_bytes, void* stream) {
+    if (scratch_bytes < radix_sort_scratch_bytes(n) + 16) return DEME_ERR_INVALID;
+    // the error word lives at the end of the caller's scratch
+    uint32_t* err = reinterpret_cast<uint32_t*>(static_cast<uint8_t*>(scratch) + radix_sort_scratch_bytes(n));
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaMemsetAsync(err, 0, sizeof(uint32_t), st);
+    radix_sort_pairs(keys_in, vals_in, keys_out, vals_out, n, key_bits, scratch, err, st);
+    return cudaGetLastError() == cudaSuccess ? DEME_OK : DEME_ERR_CUDA;
+}
+
+size_t deme_radix_sort_scratch_bytes(uint32_t n) { return radix_sort_scratch_bytes(n) + 16; }
+
+}  // extern "C"

@@ -1,0 +1,247 @@
+// device_common.cuh -- shared device helpers of the B200 DEM hot path.
+//
+// The arithmetic restates the reference's device helpers operation by operation (paths relative to the
+// reference's src/): voxel <-> position codec (kernel/DEMHelperKernels.cu:66-135), quaternion rotation (:137-148),
+// sphere-sphere and sphere-entity overlap tests (:195-264, :356-445) and the bin id of a point (:266-273).
+// The library is compiled with --fmad=false so every multiply and add rounds on its own, like the CPU oracle,
+// and float-to-integer conversions are written as explicit saturating helpers (PTX cvt semantics).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/deme_b200.h"
+
+namespace deme_b200 {
+
+constexpr double kTinyFloat = 1e-12;
+constexpr double kHugeFloat = 1e15;
+// src/DEM/Defines.h:30-35
+constexpr double kTwoOverThree = 0.666666666666667;
+constexpr double kFourOverThree = 1.333333333333333;
+constexpr double kFiveOverThree = 1.666666666666667;
+constexpr double kTwoTimesSqrtFiveOverSix = 1.825741858350554;
+constexpr double kPi = 3.1415926535897932385;
+constexpr double kPiSquared = 9.869604401089358;
+
+// Owner state lives in HBM as packed structure-of-arrays so that one owner is read with a few wide loads:
+//   pos   : uint64 voxel id + ushort4 (locX, locY, locZ, family)
+//   quat  : float4 (w, x, y, z)
+//   vel   : float4 (vx, vy, vz, mass)
+//   omg   : float4 (wx, wy, wz, 0)
+//   moi   : float4 (Ixx, Iyy, Izz, 0)
+// Spheres: float4 (relX, relY, relZ, radius), uint32 owner, uint8 material.
+struct SimConsts {
+    uint32_t nvXp2, nvYp2;
+    double l_kernel, voxel_kernel;
+    double bin_size;
+    uint32_t nbX, nbY, nbZ;
+    float beta;
+    float h;
+    float G[3];
+    int integrator;
+    uint32_t n_spheres, n_owners, n_anal;
+    // contact-detection search grid (positions relative to the LBF corner)
+    double cell_size;
+    uint32_t gx, gy, gz;
+    float r_max_cd;      // largest CD radius (radius + beta)
+    float prefilter_abs; // absolute slack of the float pre-filter
+};
+
+// Per-family prescription (constant-valued form of the reference's jitified strings).
+struct Prescription {
+    uint8_t used, lin_vel, rot_vel, lin_pos, rot_pos;
+    uint8_t has_vel[3], has_omg[3], has_pos[3];
+    float vel[3];
+    float omg[3];
+    double pos[3];
+};
+
+// Analytical component, placed in the world for the current state (owner pose applied).
+struct AnalPlaced {
+    double x, y, z;        // component reference point (double)
+    float dx, dy, dz;      // rotated direction (plane normal / axis)
+    uint32_t owner;
+    uint8_t type, normal, material, pad;
+    float mass;
+    double size1, c1, c2, umin, umax;  // cylinder radius / cone (sin, cos, axial range)
+};
+
+// ---------------- saturating conversions (cvt.rzi semantics, NaN -> 0) ----------------
+__host__ __device__ __forceinline__ uint32_t sat_u32(double x) {
+    if (!(x > 0.0)) return 0u;
+    if (x >= 4294967296.0) return 0xFFFFFFFFu;
+    return (uint32_t)x;
+}
+__host__ __device__ __forceinline__ uint64_t sat_u64(double x) {
+    if (!(x > 0.0)) return 0ull;
+    if (x >= 18446744073709551616.0) return ~0ull;
+    return (uint64_t)x;
+}
+__host__ __device__ __forceinline__ uint16_t sat_u16(double x) {
+    if (!(x > 0.0)) return 0u;
+    if (x >= 65536.0) return 65535u;
+    return (uint16_t)x;
+}
+
+// ---------------- position codec ----------------
+// voxelIDToPosition (DEMHelperKernels.cu:93-110)
+__device__ __forceinline__ void voxel_to_pos(const SimConsts& k, uint64_t id, uint32_t sx, uint32_t sy, uint32_t sz,
+                                             double& X, double& Y, double& Z) {
+    uint64_t vx = id & ((1ull << k.nvXp2) - 1ull);
+    uint64_t vy = (id >> k.nvXp2) & ((1ull << k.nvYp2) - 1ull);
+    uint64_t vz = id >> (k.nvXp2 + k.nvYp2);
+    X = __dadd_rn(__dmul_rn((double)vx, k.voxel_kernel), __dmul_rn((double)sx, k.l_kernel));
+    Y = __dadd_rn(__dmul_rn((double)vy, k.voxel_kernel), __dmul_rn((double)sy, k.l_kernel));
+    Z = __dadd_rn(__dmul_rn((double)vz, k.voxel_kernel), __dmul_rn((double)sz, k.l_kernel));
+}
+// positionToVoxelID (DEMHelperKernels.cu:113-135)
+__device__ __forceinline__ void pos_to_voxel(const SimConsts& k, double X, double Y, double Z, uint64_t& id,
+                                             uint16_t& sx, uint16_t& sy, uint16_t& sz) {
+    const double vs = k.voxel_kernel, l = k.l_kernel;
+    uint64_t nx = sat_u64(X / vs), ny = sat_u64(Y / vs), nz = sat_u64(Z / vs);
+    sx = sat_u16((X - __dmul_rn((double)nx, vs)) / l);
+    sy = sat_u16((Y - __dmul_rn((double)ny, vs)) / l);
+    sz = sat_u16((Z - __dmul_rn((double)nz, vs)) / l);
+    id = nx + (ny << k.nvXp2) + (nz << (k.nvXp2 + k.nvYp2));
+}
+
+// applyOriQToVector3<float, float> (DEMHelperKernels.cu:137-148)
+__device__ __forceinline__ void rot_f(float& X, float& Y, float& Z, float w, float x, float y, float z) {
+    const float ox = X, oy = Y, oz = Z;
+    X = (2.0f * (w * w + x * x) - 1.0f) * ox + (2.0f * (x * y - w * z)) * oy + (2.0f * (x * z + w * y)) * oz;
+    Y = (2.0f * (x * y + w * z)) * ox + (2.0f * (w * w + y * y) - 1.0f) * oy + (2.0f * (y * z - w * x)) * oz;
+    Z = (2.0f * (x * z - w * y)) * ox + (2.0f * (y * z + w * x)) * oy + (2.0f * (w * w + z * z) - 1.0f) * oz;
+}
+
+// locateMaskPair (DEMHelperKernels.cu:51-56)
+__device__ __forceinline__ uint32_t mask_index(uint32_t i, uint32_t j) {
+    if (i > j) {
+        uint32_t t = i;
+        i = j;
+        j = t;
+    }
+    return (1u + j) * j / 2u + i;
+}
+
+// normalizeVector3<float> (DEMHelperKernels.cu:156-166)
+__device__ __forceinline__ void normalize_f(float& x, float& y, float& z) {
+    const float m = sqrtf(x * x + y * y + z * z);
+    x /= m;
+    y /= m;
+    z /= m;
+}
+
+// Bin index range covered by a sphere along one axis (DEMBinSphereKernels.cu:52-64, 163-175).
+__device__ __forceinline__ void bin_range(double p, double rD, double bs, uint32_t& lo, uint32_t& hi) {
+    const double b = p / bs, span = rD / bs;
+    lo = sat_u32(b - span);
+    hi = sat_u32(b + span);
+}
+
+// Signed gap and wall normal of the cylinder / cone components (no reference counterpart; same conventions as the
+// reference plane).  Returns false where the normal is undefined or the cone wall does not exist.
+__device__ __forceinline__ bool curved_gap(const AnalPlaced& a, double xA, double yA, double zA, double& gap,
+                                           double& nx, double& ny, double& nz) {
+    const double ax = (double)a.dx, ay = (double)a.dy, az = (double)a.dz;
+    const double vx = xA - a.x, vy = yA - a.y, vz = zA - a.z;
+    const double t = vx * ax + vy * ay + vz * az;
+    const double wx = vx - t * ax, wy = vy - t * ay, wz = vz - t * az;
+    const double rho = sqrt(wx * wx + wy * wy + wz * wz);
+    if (!(rho > 0.0)) return false;
+    const double ux = wx / rho, uy = wy / rho, uz = wz / rho;
+    if (a.type == DEME_ANAL_CYLINDER) {
+        if (a.normal) {
+            gap = rho - a.size1;
+            nx = ux;
+            ny = uy;
+            nz = uz;
+        } else {
+            gap = a.size1 - rho;
+            nx = -ux;
+            ny = -uy;
+            nz = -uz;
+        }
+        return true;
+    }
+    const double s = t * a.c2 + rho * a.c1;
+    const double uc = s * a.c2;
+    if (uc < a.umin || uc > a.umax) return false;
+    const double g = t * a.c1 - rho * a.c2;
+    const double gx = a.c1 * ax - a.c2 * ux, gy = a.c1 * ay - a.c2 * uy, gz = a.c1 * az - a.c2 * uz;
+    if (a.normal) {
+        gap = -g;
+        nx = -gx;
+        ny = -gy;
+        nz = -gz;
+    } else {
+        gap = g;
+        nx = gx;
+        ny = gy;
+        nz = gz;
+    }
+    return true;
+}
+
+// checkSphereEntityOverlap, contact-detection form (DEMHelperKernels.cu:356-391)
+__device__ __forceinline__ int anal_overlap_cd(const AnalPlaced& a, double xA, double yA, double zA, double radA,
+                                               float beta4) {
+    if (a.type == DEME_ANAL_PLANE) {
+        const double px = xA - a.x, py = yA - a.y, pz = zA - a.z;
+        const double dist = px * (double)a.dx + py * (double)a.dy + pz * (double)a.dz;
+        if (dist > radA + (double)beta4) return DEME_NOT_A_CONTACT;
+        return DEME_SPHERE_PLANE_CONTACT;
+    }
+    if (a.type == DEME_ANAL_CYLINDER || a.type == DEME_ANAL_CONE) {
+        double gap, nx, ny, nz;
+        if (!curved_gap(a, xA, yA, zA, gap, nx, ny, nz)) return DEME_NOT_A_CONTACT;
+        if (gap > radA + (double)beta4) return DEME_NOT_A_CONTACT;
+        return a.type == DEME_ANAL_CYLINDER ? DEME_SPHERE_CYLINDER_CONTACT : DEME_SPHERE_CONE_CONTACT;
+    }
+    return DEME_NOT_A_CONTACT;
+}
+
+// checkSphereEntityOverlap, dynamics form with contact point and normal (DEMHelperKernels.cu:394-445)
+__device__ __forceinline__ int anal_overlap_dt(const AnalPlaced& a, double xA, double yA, double zA, double radA,
+                                               double& CPX, double& CPY, double& CPZ, float& nX, float& nY, float& nZ,
+                                               double& depth) {
+    if (a.type == DEME_ANAL_PLANE) {
+        const double px = xA - a.x, py = yA - a.y, pz = zA - a.z;
+        const double ddx = (double)a.dx, ddy = (double)a.dy, ddz = (double)a.dz;
+        const double dist = px * ddx + py * ddy + pz * ddz;
+        const double od = (radA + 0.0 - dist) / 2.0;
+        if (od < 0.0) return DEME_NOT_A_CONTACT;
+        depth = od;
+        CPX = xA - ddx * (dist + od);
+        CPY = yA - ddy * (dist + od);
+        CPZ = zA - ddz * (dist + od);
+        nX = (float)ddx;
+        nY = (float)ddy;
+        nZ = (float)ddz;
+        return DEME_SPHERE_PLANE_CONTACT;
+    }
+    if (a.type == DEME_ANAL_CYLINDER || a.type == DEME_ANAL_CONE) {
+        double gap, nx, ny, nz;
+        if (!curved_gap(a, xA, yA, zA, gap, nx, ny, nz)) return DEME_NOT_A_CONTACT;
+        const double od = (radA + 0.0 - gap) / 2.0;
+        if (od < 0.0) return DEME_NOT_A_CONTACT;
+        depth = od;
+        CPX = xA - nx * (gap + od);
+        CPY = yA - ny * (gap + od);
+        CPZ = zA - nz * (gap + od);
+        nX = (float)nx;
+        nY = (float)ny;
+        nZ = (float)nz;
+        return a.type == DEME_ANAL_CYLINDER ? DEME_SPHERE_CYLINDER_CONTACT : DEME_SPHERE_CONE_CONTACT;
+    }
+    return DEME_NOT_A_CONTACT;
+}
+
+// Device error word bits (read by the host once per step; kernels never trap).
+enum : uint32_t {
+    ERR_CONTACT_CAPACITY = 1u << 0,
+    ERR_SORT_LOOKBACK_TIMEOUT = 1u << 1,
+    ERR_SCAN_LOOKBACK_TIMEOUT = 1u << 2,
+    ERR_SEGMENT_TOO_LONG = 1u << 3,
+};
+
+}  // namespace deme_b200

@@ -1,0 +1,138 @@
+// force_model_hertz.cuh -- the built-in frictional Hertz-Mindlin contact model, restated operation by operation
+// from the reference (src/kernel/DEMCustomizablePolicies/FullHertzianForceModel.cu:1-124 with
+// matProxy2ContactParam, src/kernel/DEMHelperKernels.cu:316-339).  Every float/double promotion of the reference
+// expression is written out explicitly so the result does not depend on compiler contraction.
+//
+// Inputs are the names the reference exposes to a force model; `force`, `torque_only_force` and the four contact
+// wildcards (delta_tan_x/y/z, delta_time) are read-write.
+#pragma once
+#include "device_common.cuh"
+
+namespace deme_b200 {
+
+struct ContactGeom {
+    float3 B2A;          // unit normal from B to A
+    double overlapDepth;
+    float3 locCPA, locCPB;
+    float ARadius, BRadius, AOwnerMass, BOwnerMass;
+    float4 AoriQ, BoriQ;  // (w, x, y, z)
+    float3 ALinVel, BLinVel, ARotVel, BRotVel;
+    uint32_t matA, matB;
+};
+
+struct MaterialTable {
+    const float* E;
+    const float* nu;
+    const float* CoR;
+    const float* mu;
+    const float* Crr;
+};
+
+__device__ __forceinline__ void hertz_mindlin(const ContactGeom& g, const MaterialTable& m, float ts, float3& force,
+                                              float3& torque_only_force, float& delta_tan_x, float& delta_tan_y,
+                                              float& delta_tan_z, float& delta_time) {
+    // material proxies
+    float E_cnt, G_cnt, CoR_cnt, mu_cnt, Crr_cnt;
+    {
+        const float E_A = m.E[g.matA], nu_A = m.nu[g.matA], CoR_A = m.CoR[g.matA], mu_A = m.mu[g.matA],
+                    Crr_A = m.Crr[g.matA];
+        const float E_B = m.E[g.matB], nu_B = m.nu[g.matB], CoR_B = m.CoR[g.matB], mu_B = m.mu[g.matB],
+                    Crr_B = m.Crr[g.matB];
+        const float invE =
+            (float)((1. - (double)(nu_A * nu_A)) / (double)E_A + (1. - (double)(nu_B * nu_B)) / (double)E_B);
+        E_cnt = (float)(1. / (double)invE);
+        const float invG = (float)(2. * (2. - (double)nu_A) * (1. + (double)nu_A) / (double)E_A +
+                                   2. * (2. - (double)nu_B) * (1. + (double)nu_B) / (double)E_B);
+        G_cnt = (float)(1. / (double)invG);
+        CoR_cnt = CoR_A < CoR_B ? CoR_A : CoR_B;
+        mu_cnt = mu_A > mu_B ? mu_A : mu_B;
+        Crr_cnt = Crr_A > Crr_B ? Crr_A : Crr_B;
+    }
+    // rotational velocity of the contact point, mapped to the global frame
+    float rAx = g.ARotVel.y * g.locCPA.z - g.ARotVel.z * g.locCPA.y;
+    float rAy = g.ARotVel.z * g.locCPA.x - g.ARotVel.x * g.locCPA.z;
+    float rAz = g.ARotVel.x * g.locCPA.y - g.ARotVel.y * g.locCPA.x;
+    float rBx = g.BRotVel.y * g.locCPB.z - g.BRotVel.z * g.locCPB.y;
+    float rBy = g.BRotVel.z * g.locCPB.x - g.BRotVel.x * g.locCPB.z;
+    float rBz = g.BRotVel.x * g.locCPB.y - g.BRotVel.y * g.locCPB.x;
+    rot_f(rAx, rAy, rAz, g.AoriQ.x, g.AoriQ.y, g.AoriQ.z, g.AoriQ.w);
+    rot_f(rBx, rBy, rBz, g.BoriQ.x, g.BoriQ.y, g.BoriQ.z, g.BoriQ.w);
+    const float nX = g.B2A.x, nY = g.B2A.y, nZ = g.B2A.z;
+    // normal part and history update
+    const float vx = (g.ALinVel.x + rAx) - (g.BLinVel.x + rBx);
+    const float vy = (g.ALinVel.y + rAy) - (g.BLinVel.y + rBy);
+    const float vz = (g.ALinVel.z + rAz) - (g.BLinVel.z + rBz);
+    const float proj = vx * nX + vy * nY + vz * nZ;
+    const float vtx = vx - proj * nX, vty = vy - proj * nY, vtz = vz - proj * nZ;
+    float dtx = delta_tan_x + ts * vtx, dty = delta_tan_y + ts * vty, dtz = delta_tan_z + ts * vtz;
+    const float dproj = dtx * nX + dty * nY + dtz * nZ;
+    dtx -= dproj * nX;
+    dty -= dproj * nY;
+    dtz -= dproj * nZ;
+    delta_time += ts;
+    const float mass_eff = (g.AOwnerMass * g.BOwnerMass) / (g.AOwnerMass + g.BOwnerMass);
+    const float sqrt_Rd = (float)sqrt(g.overlapDepth * (double)(g.ARadius * g.BRadius) /
+                                      (double)(g.ARadius + g.BRadius));
+    const float Sn = (float)(2. * (double)E_cnt * (double)sqrt_Rd);
+    const float loge = (float)(((double)CoR_cnt < kTinyFloat) ? log(kTinyFloat) : (double)logf(CoR_cnt));
+    const float beta = (float)((double)loge / sqrt((double)(loge * loge) + kPiSquared));
+    const float k_n = (float)(kTwoOverThree * (double)Sn);
+    const float gamma_n = (float)(kTwoTimesSqrtFiveOverSix * (double)beta * (double)sqrtf(Sn * mass_eff));
+    const float scal = (float)((double)k_n * g.overlapDepth + (double)(gamma_n * proj));
+    force.x += scal * nX;
+    force.y += scal * nY;
+    force.z += scal * nZ;
+    // rolling resistance
+    if ((double)Crr_cnt > 0.0) {
+        bool add_rr = true;
+        const float R_eff = sqrtf((g.ARadius * g.BRadius) / (g.ARadius + g.BRadius));
+        const float kn_simple = (float)(kFourOverThree * (double)E_cnt * (double)sqrtf(R_eff));
+        const float gn_simple =
+            -2.f * sqrtf((float)(kFiveOverThree * (double)mass_eff * (double)E_cnt)) * beta * powf(R_eff, 0.25f);
+        const float d_coeff = gn_simple / (2.f * sqrtf(kn_simple * mass_eff));
+        if ((double)d_coeff < 1.0) {
+            const float t_coll = (float)(kPi * (double)sqrtf(mass_eff / (kn_simple * (1.f - d_coeff * d_coeff))));
+            if (delta_time <= t_coll) add_rr = false;
+        }
+        if (add_rr) {
+            const float vrx = rBx - rAx, vry = rBy - rAy, vrz = rBz - rAz;
+            const float vmag = sqrtf(vrx * vrx + vry * vry + vrz * vrz);
+            if ((double)vmag > kTinyFloat) {
+                const float s = Crr_cnt * sqrtf(force.x * force.x + force.y * force.y + force.z * force.z);
+                torque_only_force.x = (vrx / vmag) * s;
+                torque_only_force.y = (vry / vmag) * s;
+                torque_only_force.z = (vrz / vmag) * s;
+            }
+        }
+    }
+    // tangential part with Coulomb cap
+    if ((double)mu_cnt > 0.0) {
+        const float kt = (float)(8. * (double)G_cnt * (double)sqrt_Rd);
+        const float gt = (float)(-kTwoTimesSqrtFiveOverSix * (double)beta * (double)sqrtf(mass_eff * kt));
+        const float nkt = -kt;
+        float tfx = nkt * dtx - gt * vtx, tfy = nkt * dty - gt * vty, tfz = nkt * dtz - gt * vtz;
+        const float ft = sqrtf(tfx * tfx + tfy * tfy + tfz * tfz);
+        if ((double)ft > kTinyFloat) {
+            const float ft_max = sqrtf(force.x * force.x + force.y * force.y + force.z * force.z) * mu_cnt;
+            if (ft > ft_max) {
+                const float r = ft_max / ft;
+                tfx = r * tfx;
+                tfy = r * tfy;
+                tfz = r * tfz;
+                dtx = (tfx + gt * vtx) / nkt;
+                dty = (tfy + gt * vty) / nkt;
+                dtz = (tfz + gt * vtz) / nkt;
+            }
+        } else {
+            tfx = tfy = tfz = 0.f;
+        }
+        force.x += tfx;
+        force.y += tfy;
+        force.z += tfz;
+    }
+    delta_tan_x = dtx;
+    delta_tan_y = dty;
+    delta_tan_z = dtz;
+}
+
+}  // namespace deme_b200

@@ -1,0 +1,714 @@
+// kernels.cu -- per-step kernels of the B200 DEM hot path.
+//
+// Contact detection (kT).  The reference assigns every sphere to all bins its expanded radius touches, sorts the
+// (bin, sphere) pairs and tests all pairs inside each bin, keeping a pair only in the bin that holds its contact
+// point (src/algorithms/DEMCubContactDetection.cu:39-233, src/kernel/DEMBinSphereKernels.cu,
+// src/kernel/DEMContactKernels_Blockwise.cu).  That reports the pair (A < B) exactly when
+//     owner(A) != owner(B), the family mask allows it, the double-precision overlap test of the expanded radii
+//     passes, and bin(CP) lies in bin_range(A) and in bin_range(B) on every axis.
+// This file enumerates candidates differently -- each sphere is sorted once into a home cell of a search grid
+// whose cells are at least one expanded diameter wide, and each sphere A scans the cells its neighbours can live
+// in -- and then evaluates that same predicate with the reference's arithmetic.  The contact set is therefore the
+// reference's, while the bin-pair list (about 8-30 pairs per sphere) and its 32-bit radix sort disappear.  Output
+// is written directly in canonical order: grouped by A (ascending), sphere--analytical contacts first, then
+// sphere--sphere contacts by ascending B.
+//
+// Dynamics (dT).  One fused kernel per contact: pose gather, overlap re-test, Hertz-Mindlin, history update and
+// accumulation of the owners' linear and angular accelerations (the reference's calculateContactForces +
+// collectContactForces, src/kernel/DEMCalcForceKernels.cu:14-179, src/algorithms/DEMCubForceCollection.cu:20-158).
+// Contacts sharing owner(A) are adjacent, so the A side is reduced inside the warp before one vector atomic per
+// segment; the B side uses one float4 atomic per contact.  One kernel per owner integrates
+// (src/kernel/DEMIntegrationKernels.cu:46-179) and clears the accumulators for the next step.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "kernels.cuh"
+#include "profiler.cuh"
+
+namespace deme_b200 {
+
+static inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+// Sphere centre in double (owner position + rotated relative position), DEMBinSphereKernels.cu:39-51.
+__device__ __forceinline__ void sphere_center(const SimConsts& k, const StateView& s, uint32_t sid, uint32_t& owner,
+                                              float4& sp, double& X, double& Y, double& Z) {
+    owner = s.sOwner[sid];
+    sp = s.sph[sid];
+    const uint64_t v = s.voxel[owner];
+    const ushort4 l = s.loc[owner];
+    const float4 q = s.quat[owner];
+    double ox, oy, oz;
+    voxel_to_pos(k, v, l.x, l.y, l.z, ox, oy, oz);
+    float rx = sp.x, ry = sp.y, rz = sp.z;
+    rot_f(rx, ry, rz, q.x, q.y, q.z, q.w);
+    X = ox + (double)rx;
+    Y = oy + (double)ry;
+    Z = oz + (double)rz;
+}
+
+// ------------------------------------------------------------------------------------------------------------
+__global__ void k_place_anal(SimConsts k, StateView s, const AnalRaw* raw, AnalPlaced* placed, uint32_t nA) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nA) return;
+    const AnalRaw r = raw[i];
+    const uint32_t o = r.owner;
+    const ushort4 l = s.loc[o];
+    const float4 q = s.quat[o];
+    double ox, oy, oz;
+    voxel_to_pos(k, s.voxel[o], l.x, l.y, l.z, ox, oy, oz);
+    float rx = r.relX, ry = r.relY, rz = r.relZ, dx = r.rotX, dy = r.rotY, dz = r.rotZ;
+    rot_f(rx, ry, rz, q.x, q.y, q.z, q.w);
+    rot_f(dx, dy, dz, q.x, q.y, q.z, q.w);
+    AnalPlaced a;
+    a.x = ox + (double)rx;
+    a.y = oy + (double)ry;
+    a.z = oz + (double)rz;
+    a.dx = dx;
+    a.dy = dy;
+    a.dz = dz;
+    a.owner = o;
+    a.type = r.type;
+    a.normal = r.normal;
+    a.material = r.material;
+    a.pad = 0;
+    a.mass = r.mass;
+    a.size1 = (double)r.size1;
+    a.c1 = r.c1;
+    a.c2 = r.c2;
+    a.umin = (double)r.size2;
+    a.umax = (double)r.size3;
+    placed[i] = a;
+}
+
+void launch_place_anal(const SimConsts& k, const StateView& s, const AnalRaw* raw, AnalPlaced* placed, uint32_t nA,
+                       cudaStream_t st) {
+    if (!(nA)) return;
+    ProfScope prof_(KID_PLACE_ANAL, st);
+    if (nA) k_place_anal<<<blocks_for(nA, 64), 64, 0, st>>>(k, s, raw, placed, nA);
+}
+
+// ------------------------------------------------------------------------------------------------------------
+// Per sphere: exact position, CD radius, home cell, analytical-contact count
+// (getNumberOfBinsEachSphereTouches's analytical loop, DEMBinSphereKernels.cu:72-113).
+__global__ void __launch_bounds__(256) k_sphere_prep(SimConsts k, StateView s, CDView cd) {
+    const uint32_t sid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sid >= k.n_spheres) return;
+    uint32_t owner;
+    float4 sp;
+    double X, Y, Z;
+    sphere_center(k, s, sid, owner, sp, X, Y, Z);
+    cd.pX[sid] = X;
+    cd.pY[sid] = Y;
+    cd.pZ[sid] = Z;
+    float rf = sp.w;
+    rf += k.beta;
+    cd.posF[sid] = make_float4((float)X, (float)Y, (float)Z, rf);
+    const uint32_t cx = min(sat_u32(X / k.cell_size), k.gx - 1);
+    const uint32_t cy = min(sat_u32(Y / k.cell_size), k.gy - 1);
+    const uint32_t cz = min(sat_u32(Z / k.cell_size), k.gz - 1);
+    const uint32_t key = cx + k.gx * (cy + k.gy * cz);
+    cd.cellKey[sid] = key;
+    cd.idSeq[sid] = sid;
+    atomicAdd(&cd.cellCount[key], 1u);
+    // sphere--analytical contacts (expanded radius in double, entity margin beta)
+    double rD = (double)sp.w;
+    rD += (double)k.beta;
+    const uint32_t fam = s.loc[owner].w;
+    uint32_t c = 0;
+    for (uint32_t a = 0; a < s.nA; a++) {
+        const AnalPlaced ap = s.anal[a];
+        if (s.masks[mask_index(fam, s.loc[ap.owner].w)] != 0) continue;
+        if (anal_overlap_cd(ap, X, Y, Z, rD, k.beta) != DEME_NOT_A_CONTACT) c++;
+    }
+    cd.nAnal[sid] = (uint8_t)c;
+}
+
+void launch_sphere_prep(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st) {
+    if (!(k.n_spheres)) return;
+    ProfScope prof_(KID_SPHERE_PREP, st);
+    if (k.n_spheres) k_sphere_prep<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
+}
+
+__global__ void k_gather_sorted(uint32_t n, const float4* __restrict__ posF, const uint32_t* __restrict__ idSorted,
+                                float4* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = posF[idSorted[i]];
+}
+
+void launch_gather_sorted(const SimConsts& k, const CDView& cd, cudaStream_t st) {
+    if (!(k.n_spheres)) return;
+    ProfScope prof_(KID_GATHER, st);
+    if (k.n_spheres) k_gather_sorted<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k.n_spheres, cd.posF, cd.idSorted,
+                                                                                     cd.posFSorted);
+}
+
+// The reference's pair predicate for A < B (see the file comment).  Returns true when the pair is a contact.
+__device__ __forceinline__ bool pair_is_contact(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t A,
+                                                uint32_t B, uint32_t oA, uint32_t famA, float rfA, double xa,
+                                                double ya, double za, const uint32_t loA[3], const uint32_t hiA[3],
+                                                float rfB) {
+    const uint32_t oB = s.sOwner[B];
+    if (oA == oB) return false;
+    if (s.masks[mask_index(famA, s.loc[oB].w)] != 0) return false;
+    const double xb = cd.pX[B], yb = cd.pY[B], zb = cd.pZ[B];
+    // checkSpheresOverlap<double>, DEMHelperKernels.cu:195-222
+    const double radA = (double)rfA, radB = (double)rfB;
+    const double d2 = (xa - xb) * (xa - xb) + (ya - yb) * (ya - yb) + (za - zb) * (za - zb);
+    if (d2 > (radA + radB) * (radA + radB)) return false;
+    float nx = (float)(xa - xb), ny = (float)(ya - yb), nz = (float)(za - zb);
+    normalize_f(nx, ny, nz);
+    const double half = (radA + radB - sqrt(d2)) / 2.0;
+    const double cpx = xb + (radB - half) * (double)nx;
+    const double cpy = yb + (radB - half) * (double)ny;
+    const double cpz = zb + (radB - half) * (double)nz;
+    // getPointBinID, DEMHelperKernels.cu:266-273, tested per axis against both spheres' bin ranges
+    const uint32_t bx = sat_u32(cpx / k.bin_size), by = sat_u32(cpy / k.bin_size), bz = sat_u32(cpz / k.bin_size);
+    if (bx < loA[0] || bx > hiA[0] || by < loA[1] || by > hiA[1] || bz < loA[2] || bz > hiA[2]) return false;
+    const float4 spB = s.sph[B];
+    double rDB = (double)spB.w;
+    rDB += (double)k.beta;
+    uint32_t lo, hi;
+    bin_range(xb, rDB, k.bin_size, lo, hi);
+    if (bx < lo || bx > hi) return false;
+    bin_range(yb, rDB, k.bin_size, lo, hi);
+    if (by < lo || by > hi) return false;
+    bin_range(zb, rDB, k.bin_size, lo, hi);
+    if (bz < lo || bz > hi) return false;
+    return true;
+}
+
+// Enumerate the candidates of sphere A: spheres B > A whose home cell lies in the cells A's neighbours can occupy.
+template <bool kEmit>
+__device__ __forceinline__ uint32_t scan_neighbours(const SimConsts& k, const StateView& s, const CDView& cd,
+                                                    uint32_t A, uint32_t* outB, uint32_t cap_left) {
+    const float4 fA = cd.posF[A];
+    const double xa = cd.pX[A], ya = cd.pY[A], za = cd.pZ[A];
+    const uint32_t oA = s.sOwner[A];
+    const uint32_t famA = s.loc[oA].w;
+    const float4 spA = s.sph[A];
+    double rDA = (double)spA.w;
+    rDA += (double)k.beta;
+    uint32_t loA[3], hiA[3];
+    bin_range(xa, rDA, k.bin_size, loA[0], hiA[0]);
+    bin_range(ya, rDA, k.bin_size, loA[1], hiA[1]);
+    bin_range(za, rDA, k.bin_size, loA[2], hiA[2]);
+    const double reach = (double)fA.w + (double)k.r_max_cd + (double)k.prefilter_abs;
+    const uint32_t x0 = min(sat_u32((xa - reach) / k.cell_size), k.gx - 1);
+    const uint32_t x1 = min(sat_u32((xa + reach) / k.cell_size), k.gx - 1);
+    const uint32_t y0 = min(sat_u32((ya - reach) / k.cell_size), k.gy - 1);
+    const uint32_t y1 = min(sat_u32((ya + reach) / k.cell_size), k.gy - 1);
+    const uint32_t z0 = min(sat_u32((za - reach) / k.cell_size), k.gz - 1);
+    const uint32_t z1 = min(sat_u32((za + reach) / k.cell_size), k.gz - 1);
+    uint32_t count = 0;
+    for (uint32_t cz = z0; cz <= z1; cz++) {
+        for (uint32_t cy = y0; cy <= y1; cy++) {
+            const uint32_t rowBase = k.gx * (cy + k.gy * cz);
+            // cells x0..x1 of one row are contiguous in the sorted order
+            const uint32_t j0 = cd.cellStart[rowBase + x0];
+            const uint32_t j1 = cd.cellStart[rowBase + x1 + 1];
+            for (uint32_t j = j0; j < j1; j++) {
+                const uint32_t B = cd.idSorted[j];
+                if (B <= A) continue;
+                const float4 fB = cd.posFSorted[j];
+                const float dx = fA.x - fB.x, dy = fA.y - fB.y, dz = fA.z - fB.z;
+                const float lim = (fA.w + fB.w) * 1.00001f + k.prefilter_abs;
+                if (dx * dx + dy * dy + dz * dz > lim * lim) continue;
+                if (!pair_is_contact(k, s, cd, A, B, oA, famA, fA.w, xa, ya, za, loA, hiA, fB.w)) continue;
+                if (kEmit) {
+                    if (count < cap_left) outB[count] = B;
+                }
+                count++;
+            }
+        }
+    }
+    return count;
+}
+
+__global__ void __launch_bounds__(256) k_pair_count(SimConsts k, StateView s, CDView cd) {
+    const uint32_t A = blockIdx.x * blockDim.x + threadIdx.x;
+    if (A >= k.n_spheres) return;
+    const uint32_t n = scan_neighbours<false>(k, s, cd, A, nullptr, 0);
+    cd.cnt[A] = n + cd.nAnal[A];
+}
+
+void launch_pair_count(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st) {
+    if (!(k.n_spheres)) return;
+    ProfScope prof_(KID_PAIR_COUNT, st);
+    if (k.n_spheres) k_pair_count<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
+}
+
+__global__ void __launch_bounds__(256) k_pair_emit(SimConsts k, StateView s, CDView cd, ContactView c, uint32_t cap,
+                                                   uint32_t* err) {
+    const uint32_t A = blockIdx.x * blockDim.x + threadIdx.x;
+    if (A >= k.n_spheres) return;
+    const uint32_t begin = c.off[A], end = c.off[A + 1];
+    if (end > cap) {
+        atomicOr(err, ERR_CONTACT_CAPACITY);
+        return;
+    }
+    uint32_t w = begin;
+    // sphere--analytical contacts first, ascending component id (populateBinSphereTouchingPairs, :186-228)
+    const uint32_t nAn = cd.nAnal[A];
+    if (nAn) {
+        const double X = cd.pX[A], Y = cd.pY[A], Z = cd.pZ[A];
+        const float4 sp = s.sph[A];
+        double rD = (double)sp.w;
+        rD += (double)k.beta;
+        const uint32_t fam = s.loc[s.sOwner[A]].w;
+        for (uint32_t a = 0; a < s.nA && w < end; a++) {
+            const AnalPlaced ap = s.anal[a];
+            if (s.masks[mask_index(fam, s.loc[ap.owner].w)] != 0) continue;
+            const int t = anal_overlap_cd(ap, X, Y, Z, rD, k.beta);
+            if (t != DEME_NOT_A_CONTACT) {
+                c.idA[w] = A;
+                c.idB[w] = a;
+                c.type[w] = (uint8_t)t;
+                w++;
+            }
+        }
+    }
+    // sphere--sphere contacts, then sorted by idB (insertion sort of the short segment)
+    const uint32_t ssBegin = w;
+    const uint32_t n = scan_neighbours<true>(k, s, cd, A, c.idB + ssBegin, end - ssBegin);
+    if (ssBegin + n != end) atomicOr(err, ERR_SEGMENT_TOO_LONG);
+    const uint32_t m = min(n, end - ssBegin);
+    uint32_t* seg = c.idB + ssBegin;
+    for (uint32_t i = 1; i < m; i++) {
+        const uint32_t v = seg[i];
+        uint32_t j = i;
+        while (j > 0 && seg[j - 1] > v) {
+            seg[j] = seg[j - 1];
+            j--;
+        }
+        seg[j] = v;
+    }
+    for (uint32_t i = 0; i < m; i++) {
+        c.idA[ssBegin + i] = A;
+        c.type[ssBegin + i] = DEME_SPHERE_SPHERE_CONTACT;
+    }
+}
+
+void launch_pair_emit(const SimConsts& k, const StateView& s, const CDView& cd, const ContactView& c, uint32_t cap,
+                      uint32_t* err, cudaStream_t st) {
+    if (!(k.n_spheres)) return;
+    ProfScope prof_(KID_PAIR_EMIT, st);
+    if (k.n_spheres) k_pair_emit<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd, c, cap, err);
+}
+
+// ------------------------------------------------------------------------------------------------------------
+// History map and wildcard remap: for each new contact, find (idB, type) in A's segment of the previous list
+// (buildPersistentMap, src/kernel/DEMHistoryMappingKernels.cu:16-60; rearrangeContactWildcards,
+// src/kernel/DEMPrepForceKernels.cu:93-115).  Segments of both lists are sorted by (group, idB), group 0 being the
+// sphere--analytical contacts, so a binary search finds the unique partner.
+__global__ void __launch_bounds__(256) k_history(uint32_t n, ContactView cur, ContactView prev, bool has_hist) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t A = cur.idA[i], B = cur.idB[i];
+    const uint8_t t = cur.type[i];
+    const uint64_t key = ((uint64_t)(t == DEME_SPHERE_SPHERE_CONTACT ? 1u : 0u) << 32) | B;
+    uint32_t lo = prev.off[A], hi = prev.off[A + 1];
+    uint32_t partner = DEME_NULL_MAPPING_PARTNER;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        const uint8_t tm = prev.type[mid];
+        const uint64_t km = ((uint64_t)(tm == DEME_SPHERE_SPHERE_CONTACT ? 1u : 0u) << 32) | prev.idB[mid];
+        if (km < key) {
+            lo = mid + 1;
+        } else {
+            hi = mid;
+        }
+    }
+    if (lo < prev.off[A + 1] && prev.idB[lo] == B && prev.type[lo] == t) partner = lo;
+    cur.mapping[i] = partner;
+    if (has_hist) cur.hist[i] = partner == DEME_NULL_MAPPING_PARTNER ? make_float4(0.f, 0.f, 0.f, 0.f) : prev.hist[partner];
+}
+
+void launch_history(const SimConsts& k, const ContactView& cur, const ContactView& prev, uint32_t n, bool has_hist,
+                    cudaStream_t st) {
+    if (!(n)) return;
+    ProfScope prof_(KID_HISTORY, st);
+    if (n) k_history<<<blocks_for(n, 256), 256, 0, st>>>(n, cur, prev, has_hist);
+}
+
+__global__ void k_count_by_sphere(const uint32_t* idA, uint32_t n, uint32_t* cnt) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) atomicAdd(&cnt[idA[i]], 1u);
+}
+void launch_count_by_sphere(const uint32_t* idA, uint32_t n, uint32_t* cnt, cudaStream_t st) {
+    if (!(n)) return;
+    ProfScope prof_(KID_OTHER, st);
+    if (n) k_count_by_sphere<<<blocks_for(n, 256), 256, 0, st>>>(idA, n, cnt);
+}
+
+// ------------------------------------------------------------------------------------------------------------
+// Fused force + collection kernel.
+template <bool kStore>
+__global__ void __launch_bounds__(256) k_force(SimConsts k, StateView s, ContactView c, uint32_t n, bool has_hist,
+                                               ContactOutputs out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n;
+    uint32_t oA = 0xFFFFFFFFu, oB = 0xFFFFFFFFu;
+    bool bSphere = false;
+    float3 F = make_float3(0.f, 0.f, 0.f), T = make_float3(0.f, 0.f, 0.f);
+    float3 cpA = make_float3(0.f, 0.f, 0.f), cpB = make_float3(0.f, 0.f, 0.f);
+    float4 qA = make_float4(1.f, 0.f, 0.f, 0.f), qB = qA;
+    float mA = 1.f, mB = 1.f;
+    bool active = false;
+    if (valid) {
+        const uint32_t sA = c.idA[i];
+        const uint32_t bId = c.idB[i];
+        int ct = c.type[i];
+        float4 hw = has_hist ? c.hist[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        ContactGeom g;
+        // body A (always a sphere)
+        oA = s.sOwner[sA];
+        const float4 spA = s.sph[sA];
+        const ushort4 lA = s.loc[oA];
+        qA = s.quat[oA];
+        const float4 vA = s.vel[oA];
+        const float4 wA = s.omg[oA];
+        double AOx, AOy, AOz;
+        voxel_to_pos(k, s.voxel[oA], lA.x, lA.y, lA.z, AOx, AOy, AOz);
+        float rx = spA.x, ry = spA.y, rz = spA.z;
+        rot_f(rx, ry, rz, qA.x, qA.y, qA.z, qA.w);
+        const double Ax = AOx + (double)rx, Ay = AOy + (double)ry, Az = AOz + (double)rz;
+        g.ARadius = spA.w;
+        g.AOwnerMass = vA.w;
+        g.matA = s.sMat[sA];
+        g.ALinVel = make_float3(vA.x, vA.y, vA.z);
+        g.ARotVel = make_float3(wA.x, wA.y, wA.z);
+        mA = vA.w;
+        double BOx, BOy, BOz, CPx = 0, CPy = 0, CPz = 0, depth = 0;
+        float nX = 0, nY = 0, nZ = 0;
+        if (ct == DEME_SPHERE_SPHERE_CONTACT) {
+            bSphere = true;
+            oB = s.sOwner[bId];
+            const float4 spB = s.sph[bId];
+            const ushort4 lB = s.loc[oB];
+            qB = s.quat[oB];
+            const float4 vB = s.vel[oB];
+            const float4 wB = s.omg[oB];
+            voxel_to_pos(k, s.voxel[oB], lB.x, lB.y, lB.z, BOx, BOy, BOz);
+            float bx = spB.x, by = spB.y, bz = spB.z;
+            rot_f(bx, by, bz, qB.x, qB.y, qB.z, qB.w);
+            const double Bx = BOx + (double)bx, By = BOy + (double)by, Bz = BOz + (double)bz;
+            g.BRadius = spB.w;
+            g.BOwnerMass = vB.w;
+            g.matB = s.sMat[bId];
+            g.BLinVel = make_float3(vB.x, vB.y, vB.z);
+            g.BRotVel = make_float3(wB.x, wB.y, wB.z);
+            mB = vB.w;
+            // checkSpheresOverlap<double, float>, DEMHelperKernels.cu:233-264
+            const double radA = (double)g.ARadius, radB = (double)g.BRadius;
+            const double d2 = (Ax - Bx) * (Ax - Bx) + (Ay - By) * (Ay - By) + (Az - Bz) * (Az - Bz);
+            if (d2 > (radA + radB) * (radA + radB)) {
+                ct = DEME_NOT_A_CONTACT;
+            } else {
+                nX = (float)(Ax - Bx);
+                nY = (float)(Ay - By);
+                nZ = (float)(Az - Bz);
+                normalize_f(nX, nY, nZ);
+                depth = radA + radB - sqrt(d2);
+                CPx = Bx + (radB - depth / 2.0) * (double)nX;
+                CPy = By + (radB - depth / 2.0) * (double)nY;
+                CPz = Bz + (radB - depth / 2.0) * (double)nZ;
+            }
+        } else {
+            const AnalPlaced a = s.anal[bId];
+            oB = a.owner;
+            const ushort4 lB = s.loc[oB];
+            qB = s.quat[oB];
+            const float4 vB = s.vel[oB];
+            const float4 wB = s.omg[oB];
+            voxel_to_pos(k, s.voxel[oB], lB.x, lB.y, lB.z, BOx, BOy, BOz);
+            g.BRadius = (float)kHugeFloat;
+            g.BOwnerMass = a.mass;
+            g.matB = a.material;
+            g.BLinVel = make_float3(vB.x, vB.y, vB.z);
+            g.BRotVel = make_float3(wB.x, wB.y, wB.z);
+            ct = anal_overlap_dt(a, Ax, Ay, Az, (double)g.ARadius, CPx, CPy, CPz, nX, nY, nZ, depth);
+        }
+        if (ct != DEME_NOT_A_CONTACT) {
+            active = true;
+            float cax = (float)(CPx - AOx), cay = (float)(CPy - AOy), caz = (float)(CPz - AOz);
+            float cbx = (float)(CPx - BOx), cby = (float)(CPy - BOy), cbz = (float)(CPz - BOz);
+            rot_f(cax, cay, caz, qA.x, -qA.y, -qA.z, -qA.w);
+            rot_f(cbx, cby, cbz, qB.x, -qB.y, -qB.z, -qB.w);
+            cpA = make_float3(cax, cay, caz);
+            cpB = make_float3(cbx, cby, cbz);
+            g.B2A = make_float3(nX, nY, nZ);
+            g.overlapDepth = depth;
+            g.locCPA = cpA;
+            g.locCPB = cpB;
+            g.AoriQ = qA;
+            g.BoriQ = qB;
+            hertz_mindlin(g, s.mat, k.h, F, T, hw.x, hw.y, hw.z, hw.w);
+        } else {
+            hw = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        if (has_hist) c.hist[i] = hw;
+        if (kStore) {
+            out.F[i] = make_float4(F.x, F.y, F.z, 0.f);
+            out.TOF[i] = make_float4(T.x, T.y, T.z, 0.f);
+            out.CPA[i] = make_float4(cpA.x, cpA.y, cpA.z, 0.f);
+            out.CPB[i] = make_float4(cpB.x, cpB.y, cpB.z, 0.f);
+        }
+    }
+    // owner contributions (forceToAcc / forceToAngAcc, src/kernel/DEMCollectForceKernels.cu:68-120)
+    float4 aA = make_float4(0.f, 0.f, 0.f, 0.f), alA = aA, aB = aA, alB = aA;
+    if (active) {
+        const float4 mi = s.moi[oA];
+        aA = make_float4((F.x * 1.f) / mA, (F.y * 1.f) / mA, (F.z * 1.f) / mA, 0.f);
+        float gx = (F.x + T.x) * 1.f, gy = (F.y + T.y) * 1.f, gz = (F.z + T.z) * 1.f;
+        rot_f(gx, gy, gz, qA.x, -qA.y, -qA.z, -qA.w);
+        alA = make_float4((cpA.y * gz - cpA.z * gy) / mi.x, (cpA.z * gx - cpA.x * gz) / mi.y,
+                          (cpA.x * gy - cpA.y * gx) / mi.z, 0.f);
+        if (bSphere) {
+            const float4 mj = s.moi[oB];
+            aB = make_float4((F.x * -1.f) / mB, (F.y * -1.f) / mB, (F.z * -1.f) / mB, 0.f);
+            float hx = (F.x + T.x) * -1.f, hy = (F.y + T.y) * -1.f, hz = (F.z + T.z) * -1.f;
+            rot_f(hx, hy, hz, qB.x, -qB.y, -qB.z, -qB.w);
+            alB = make_float4((cpB.y * hz - cpB.z * hy) / mj.x, (cpB.z * hx - cpB.x * hz) / mj.y,
+                              (cpB.x * hy - cpB.y * hx) / mj.z, 0.f);
+        }
+    }
+    // A side: contacts of one owner are adjacent (sorted by sphere id; a clump's spheres have consecutive ids).
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t key = valid ? oA : 0xFFFFFFFFu;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t k2 = __shfl_down_sync(0xffffffffu, key, off);
+        const float x0 = __shfl_down_sync(0xffffffffu, aA.x, off);
+        const float x1 = __shfl_down_sync(0xffffffffu, aA.y, off);
+        const float x2 = __shfl_down_sync(0xffffffffu, aA.z, off);
+        const float y0 = __shfl_down_sync(0xffffffffu, alA.x, off);
+        const float y1 = __shfl_down_sync(0xffffffffu, alA.y, off);
+        const float y2 = __shfl_down_sync(0xffffffffu, alA.z, off);
+        if (lane + off < 32 && k2 == key) {
+            aA.x += x0;
+            aA.y += x1;
+            aA.z += x2;
+            alA.x += y0;
+            alA.y += y1;
+            alA.z += y2;
+        }
+    }
+    const uint32_t prevKey = __shfl_up_sync(0xffffffffu, key, 1);
+    const bool head = (lane == 0) || (prevKey != key);
+    if (head && key != 0xFFFFFFFFu) {
+        atomicAdd(&s.acc[key], aA);
+        atomicAdd(&s.alpha[key], alA);
+    }
+    if (active && bSphere) {
+        atomicAdd(&s.acc[oB], aB);
+        atomicAdd(&s.alpha[oB], alB);
+    }
+}
+
+void launch_force(const SimConsts& k, const StateView& s, const ContactView& c, uint32_t n, bool has_hist,
+                  const ContactOutputs* out, cudaStream_t st) {
+    if (!(n)) return;
+    ProfScope prof_(KID_FORCE, st);
+    if (!n) return;
+    if (out)
+        k_force<true><<<blocks_for(n, 256), 256, 0, st>>>(k, s, c, n, has_hist, *out);
+    else
+        k_force<false><<<blocks_for(n, 256), 256, 0, st>>>(k, s, c, n, has_hist, ContactOutputs{});
+}
+
+// ------------------------------------------------------------------------------------------------------------
+// integrateOwners (src/kernel/DEMIntegrationKernels.cu:46-179) with the constant prescription table.
+__global__ void __launch_bounds__(256) k_integrate(SimConsts k, StateView s) {
+    const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= k.n_owners) return;
+    ushort4 l = s.loc[o];
+    const Prescription pr = s.presc[l.w];
+    float4 v = s.vel[o];
+    float4 w = s.omg[o];
+    const float4 a = s.acc[o];
+    const float4 al = s.alpha[o];
+    const float ovx = v.x, ovy = v.y, ovz = v.z, owx = w.x, owy = w.y, owz = w.z;
+    bool linV = false, rotV = false, linP = false, rotP = false;
+    if (pr.used) {
+        if (pr.has_vel[0]) v.x = pr.vel[0];
+        if (pr.has_vel[1]) v.y = pr.vel[1];
+        if (pr.has_vel[2]) v.z = pr.vel[2];
+        if (pr.has_omg[0]) w.x = pr.omg[0];
+        if (pr.has_omg[1]) w.y = pr.omg[1];
+        if (pr.has_omg[2]) w.z = pr.omg[2];
+        linV = pr.lin_vel;
+        rotV = pr.rot_vel;
+    }
+    const float h = k.h;
+    float ux = 0.f, uy = 0.f, uz = 0.f, qx = 0.f, qy = 0.f, qz = 0.f;
+    if (!linV) {
+        ux = (a.x + k.G[0]) * h;
+        uy = (a.y + k.G[1]) * h;
+        uz = (a.z + k.G[2]) * h;
+        v.x += ux;
+        v.y += uy;
+        v.z += uz;
+    }
+    if (!rotV) {
+        qx = al.x * h;
+        qy = al.y * h;
+        qz = al.z * h;
+        w.x += qx;
+        w.y += qy;
+        w.z += qz;
+    }
+    float px, py, pz, rx, ry, rz;
+    if (k.integrator == DEME_INTEGRATOR_FORWARD_EULER) {
+        px = ovx; py = ovy; pz = ovz;
+        rx = owx; ry = owy; rz = owz;
+    } else if (k.integrator == DEME_INTEGRATOR_CENTERED_DIFFERENCE) {
+        px = ovx + ux; py = ovy + uy; pz = ovz + uz;
+        rx = owx + qx; ry = owy + qy; rz = owz + qz;
+    } else {
+        px = ovx + ux * 0.5f; py = ovy + uy * 0.5f; pz = ovz + uz * 0.5f;
+        rx = owx + qx * 0.5f; ry = owy + qy * 0.5f; rz = owz + qz * 0.5f;
+    }
+    double X, Y, Z;
+    uint64_t vox = s.voxel[o];
+    voxel_to_pos(k, vox, l.x, l.y, l.z, X, Y, Z);
+    if (pr.used) {
+        if (pr.has_pos[0]) X = pr.pos[0];
+        if (pr.has_pos[1]) Y = pr.pos[1];
+        if (pr.has_pos[2]) Z = pr.pos[2];
+        linP = pr.lin_pos;
+        rotP = pr.rot_pos;
+    }
+    if (!linP) {
+        X += (double)px * (double)h;
+        Y += (double)py * (double)h;
+        Z += (double)pz * (double)h;
+    }
+    uint16_t sx, sy, sz;
+    pos_to_voxel(k, X, Y, Z, vox, sx, sy, sz);
+    l.x = sx;
+    l.y = sy;
+    l.z = sz;
+    float4 q = s.quat[o];
+    if (!rotP) {
+        double q0 = 1.0, q1 = rx, q2 = ry, q3 = rz;
+        const double len = sqrt(q1 * q1 + q2 * q2 + q3 * q3);
+        const double theta = 0.5 * (double)h * len;
+        if (len > 0) {
+            q0 = cos(theta);
+            const double sn = sin(theta) / len;
+            q1 *= sn;
+            q2 *= sn;
+            q3 *= sn;
+        }
+        const float a1 = q.x, b1 = q.y, c1 = q.z, d1 = q.w;
+        const float a2 = (float)q0, b2 = (float)q1, c2 = (float)q2, d2 = (float)q3;
+        q.x = a1 * a2 - b1 * b2 - c1 * c2 - d1 * d2;
+        q.y = a1 * b2 + b1 * a2 + c1 * d2 - d1 * c2;
+        q.z = a1 * c2 - b1 * d2 + c1 * a2 + d1 * b2;
+        q.w = a1 * d2 + b1 * c2 - c1 * b2 + d1 * a2;
+    }
+    s.vel[o] = v;
+    s.omg[o] = w;
+    s.voxel[o] = vox;
+    s.loc[o] = l;
+    s.quat[o] = q;
+}
+
+void launch_integrate(const SimConsts& k, const StateView& s, cudaStream_t st) {
+    if (!(k.n_owners)) return;
+    ProfScope prof_(KID_INTEGRATE, st);
+    if (k.n_owners) k_integrate<<<blocks_for(k.n_owners, 256), 256, 0, st>>>(k, s);
+}
+
+// Kinetic energy of clump owners: per-owner term of DEMOwnerQueryKernels.cu:10-37, summed in double.
+__global__ void k_kinetic_energy(SimConsts k, StateView s, uint32_t nClumps, double* out) {
+    __shared__ double sh[32];
+    const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    if (o < nClumps) {
+        const float4 v = s.vel[o], w = s.omg[o], I = s.moi[o];
+        const double v2 = (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z;
+        const double r2 = (double)I.x * w.x * w.x + (double)I.y * w.y * w.y + (double)I.z * w.z * w.z;
+        e = 0.5 * (double)v.w * v2 + 0.5 * r2;
+    }
+    for (int off = 16; off > 0; off >>= 1) e += __shfl_down_sync(0xffffffffu, e, off);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = e;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        e = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+        for (int off = 16; off > 0; off >>= 1) e += __shfl_down_sync(0xffffffffu, e, off);
+        if (threadIdx.x == 0) atomicAdd(out, e);
+    }
+}
+
+void launch_kinetic_energy(const SimConsts& k, const StateView& s, uint32_t n_clumps, double* out, cudaStream_t st) {
+    if (!(true)) return;
+    ProfScope prof_(KID_OTHER, st);
+    cudaMemsetAsync(out, 0, sizeof(double), st);
+    if (n_clumps) k_kinetic_energy<<<blocks_for(n_clumps, 256), 256, 0, st>>>(k, s, n_clumps, out);
+}
+
+// ------------------------------------------------------------------------------------------------------------
+// Reference bin assignment (getNumberOfBinsEachSphereTouches / populateBinSphereTouchingPairs): parity path only.
+__global__ void k_bin_count(SimConsts k, StateView s, uint16_t* nBins, uint8_t* nAnal) {
+    const uint32_t sid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sid >= k.n_spheres) return;
+    uint32_t owner;
+    float4 sp;
+    double X, Y, Z;
+    sphere_center(k, s, sid, owner, sp, X, Y, Z);
+    double rD = (double)sp.w;
+    rD += (double)k.beta;
+    uint32_t lo[3], hi[3];
+    bin_range(X, rD, k.bin_size, lo[0], hi[0]);
+    bin_range(Y, rD, k.bin_size, lo[1], hi[1]);
+    bin_range(Z, rD, k.bin_size, lo[2], hi[2]);
+    const uint16_t nx = (uint16_t)(hi[0] - lo[0] + 1u), ny = (uint16_t)(hi[1] - lo[1] + 1u),
+                   nz = (uint16_t)(hi[2] - lo[2] + 1u);
+    nBins[sid] = (uint16_t)((int)nx * (int)ny * (int)nz);
+    const uint32_t fam = s.loc[owner].w;
+    uint32_t c = 0;
+    for (uint32_t a = 0; a < s.nA; a++) {
+        const AnalPlaced ap = s.anal[a];
+        if (s.masks[mask_index(fam, s.loc[ap.owner].w)] != 0) continue;
+        if (anal_overlap_cd(ap, X, Y, Z, rD, k.beta) != DEME_NOT_A_CONTACT) c++;
+    }
+    nAnal[sid] = (uint8_t)c;
+}
+
+__global__ void k_bin_emit(SimConsts k, StateView s, const uint32_t* off, uint32_t* bins, uint32_t* sph) {
+    const uint32_t sid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sid >= k.n_spheres) return;
+    uint32_t owner;
+    float4 sp;
+    double X, Y, Z;
+    sphere_center(k, s, sid, owner, sp, X, Y, Z);
+    double rD = (double)sp.w;
+    rD += (double)k.beta;
+    uint32_t lo[3], hi[3];
+    bin_range(X, rD, k.bin_size, lo[0], hi[0]);
+    bin_range(Y, rD, k.bin_size, lo[1], hi[1]);
+    bin_range(Z, rD, k.bin_size, lo[2], hi[2]);
+    uint32_t w = off[sid];
+    for (uint32_t kk = lo[2]; kk <= hi[2]; kk++)
+        for (uint32_t j = lo[1]; j <= hi[1]; j++)
+            for (uint32_t i = lo[0]; i <= hi[0]; i++) {
+                bins[w] = i + j * k.nbX + kk * k.nbX * k.nbY;
+                sph[w] = sid;
+                w++;
+            }
+}
+
+void launch_bin_count(const SimConsts& k, const StateView& s, uint16_t* nBins, uint8_t* nAnal, cudaStream_t st) {
+    if (!(k.n_spheres)) return;
+    ProfScope prof_(KID_OTHER, st);
+    if (k.n_spheres) k_bin_count<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, nBins, nAnal);
+}
+void launch_bin_emit(const SimConsts& k, const StateView& s, const uint32_t* off, uint32_t* bins, uint32_t* sph,
+                     cudaStream_t st) {
+    if (!(k.n_spheres)) return;
+    ProfScope prof_(KID_OTHER, st);
+    if (k.n_spheres) k_bin_emit<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, off, bins, sph);
+}
+
+}  // namespace deme_b200

@@ -1,0 +1,93 @@
+// kernels.cuh -- device data views and host launchers of the per-step kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "device_common.cuh"
+#include "force_model_hertz.cuh"
+
+namespace deme_b200 {
+
+// Owner and sphere arrays in HBM (layout documented in device_common.cuh).
+struct StateView {
+    uint64_t* voxel;
+    ushort4* loc;   // (locX, locY, locZ, family)
+    float4* quat;   // (w, x, y, z)
+    float4* vel;    // (vx, vy, vz, mass)
+    float4* omg;    // (wx, wy, wz, 0)
+    const float4* moi;
+    float4* acc;    // force accumulators (a)
+    float4* alpha;  // torque accumulators (alpha)
+    const float4* sph;  // (relX, relY, relZ, radius)
+    const uint32_t* sOwner;
+    const uint8_t* sMat;
+    const uint8_t* masks;
+    MaterialTable mat;
+    const AnalPlaced* anal;
+    uint32_t nA;
+    const Prescription* presc;  // DEME_NUM_FAMILIES entries
+};
+
+// Raw analytical component description (scene constants).
+struct AnalRaw {
+    float relX, relY, relZ, rotX, rotY, rotZ, size1, size2, size3, mass;
+    uint32_t owner;
+    uint8_t type, normal, material, pad;
+    double c1, c2;
+};
+
+// Contact-detection work arrays.
+struct CDView {
+    double* pX;
+    double* pY;
+    double* pZ;
+    float4* posF;        // ID order: (x, y, z, CD radius)
+    float4* posFSorted;  // cell order
+    uint32_t* cellKey;
+    uint32_t* idSeq;
+    uint32_t* keySorted;
+    uint32_t* idSorted;
+    uint32_t* cellCount;  // nCells + 1
+    uint32_t* cellStart;  // nCells + 1
+    uint8_t* nAnal;
+    uint32_t* cnt;
+};
+
+// One contact list (kT product) with its history wildcards.
+struct ContactView {
+    uint32_t* idA;
+    uint32_t* idB;
+    uint8_t* type;
+    float4* hist;       // (delta_tan_x, delta_tan_y, delta_tan_z, delta_time)
+    uint32_t* mapping;
+    uint32_t* off;      // CSR offsets by sphere (nS + 1)
+};
+
+struct ContactOutputs {
+    float4* F;
+    float4* TOF;
+    float4* CPA;
+    float4* CPB;
+};
+
+void launch_place_anal(const SimConsts& k, const StateView& s, const AnalRaw* raw, AnalPlaced* placed, uint32_t nA,
+                       cudaStream_t st);
+void launch_sphere_prep(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
+void launch_gather_sorted(const SimConsts& k, const CDView& cd, cudaStream_t st);
+void launch_pair_count(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
+void launch_pair_emit(const SimConsts& k, const StateView& s, const CDView& cd, const ContactView& c, uint32_t cap,
+                      uint32_t* err, cudaStream_t st);
+void launch_history(const SimConsts& k, const ContactView& cur, const ContactView& prev, uint32_t n, bool has_hist,
+                    cudaStream_t st);
+void launch_count_by_sphere(const uint32_t* idA, uint32_t n, uint32_t* cnt, cudaStream_t st);
+void launch_force(const SimConsts& k, const StateView& s, const ContactView& c, uint32_t n, bool has_hist,
+                  const ContactOutputs* out, cudaStream_t st);
+void launch_integrate(const SimConsts& k, const StateView& s, cudaStream_t st);
+void launch_kinetic_energy(const SimConsts& k, const StateView& s, uint32_t n_clumps, double* out, cudaStream_t st);
+
+// Reference bin assignment (parity path).
+void launch_bin_count(const SimConsts& k, const StateView& s, uint16_t* nBins, uint8_t* nAnal, cudaStream_t st);
+void launch_bin_emit(const SimConsts& k, const StateView& s, const uint32_t* off, uint32_t* bins, uint32_t* sph,
+                     cudaStream_t st);
+
+}  // namespace deme_b200

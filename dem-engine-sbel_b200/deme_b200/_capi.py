@@ -62,6 +62,8 @@ class SimParams(C.Structure):
         ("cd_update_freq", C.c_int32),
         ("n_contact_wildcards", C.c_int32),
         ("pad1", C.c_int32),
+        ("domain", C.c_float * 3),
+        ("pad2", C.c_float),
     ]
 
 

@@ -545,6 +545,7 @@ class SceneBuilder:
         p.integrator = self.integrator
         p.cd_update_freq = self.update_freq
         p.n_contact_wildcards = self.n_wildcards
+        p.domain[:] = [float(v) for v in self.box]
 
         arrays = dict(voxel=vox, locX=lx, locY=ly, locZ=lz, oriQw=oriQw, oriQx=oriQx, oriQy=oriQy, oriQz=oriQz,
                       vX=vX, vY=vY, vZ=vZ, omgX=wX, omgY=wY, omgZ=wZ, family=family, mass=mass,

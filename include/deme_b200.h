@@ -88,6 +88,8 @@ typedef struct {
     int32_t cd_update_freq;  /* 0: contact detection every step (src/DEM/API.h:82, SetCDUpdateFreq) */
     int32_t n_contact_wildcards; /* 4 for the built-in Hertz-Mindlin model, 0 for frictionless */
     int32_t pad1;
+    float domain[3];  /* user-instructed domain size (InstructBoxDomainDimension); bounds the contact search grid */
+    float pad2;
 } deme_sim_params;
 
 /* Per-family prescription.  The reference jitifies these as C expression strings
@@ -259,10 +261,25 @@ int32_t deme_download_contacts(deme_handle* h, deme_contacts* out);
  * kT products into dT for parity checks. */
 int32_t deme_upload_contacts(deme_handle* h, const deme_contacts* in);
 int32_t deme_download_contact_forces(deme_handle* h, deme_contact_forces* out);
+/* Keep the per-contact force, torque-only force and local contact points of the next deme_compute_forces calls so
+ * deme_download_contact_forces can return them (the fused hot path does not store them by default). */
+int32_t deme_keep_contact_forces(deme_handle* h, int32_t enable);
 
 /* Streams: kT (contact detection) and dT (dynamics) work queues; NULL restores the handle's own streams.
  * The two workers of the reference are host threads with one stream each (src/core/utils/GpuManager.cpp:8-32). */
 int32_t deme_set_streams(deme_handle* h, void* kT_stream, void* dT_stream);
+
+/* Change one family's prescription between steps (the constant-valued form of SetFamilyPrescribedLinVel /
+ * SetFamilyPrescribedAngVel / SetFamilyFixed, src/DEM/APIPublic.cpp:145-252, which the reference can only change by
+ * re-jitifying).  The value is staged through pinned memory and applied in stream order. */
+int32_t deme_set_family_prescription(deme_handle* h, int32_t family, const deme_family_prescription* p);
+
+/* Instrumentation.  deme_launch_count: kernels launched by this library in this process.  deme_kernel_timing(1)
+ * brackets every launch with CUDA events on its stream; deme_kernel_times sums them per kernel name.  (The reference
+ * keeps host wall-clock timers per phase instead: src/DEM/kT.h:179-181, src/DEM/dT.h:253-255.) */
+int64_t deme_launch_count(void);
+int32_t deme_kernel_timing(int32_t enable);
+int32_t deme_kernel_times(int32_t cap, const char** names, double* total_ms, int64_t* launches, int32_t* n_out);
 
 /* Simulation time advanced so far and step counter. */
 int32_t deme_get_time(deme_handle* h, double* t, int64_t* steps);

@@ -1,0 +1,111 @@
+"""Shared test helpers: library loading, canonical contact order and comparisons.
+
+The oracle (oracle/) is only ever used here as the checker.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "dem-engine-sbel_b200")
+for p in (PKG, ROOT):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+from deme_b200 import capi, HandleSolver, Solver, workloads  # noqa: E402
+
+ORACLE_LIB = os.path.join(ROOT, "oracle", "_build", "libdeme_oracle.so")
+
+
+def oracle_lib():
+    if not os.path.exists(ORACLE_LIB):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+    return capi.load_library(ORACLE_LIB)
+
+
+def oracle(built, threads=4):
+    return HandleSolver(oracle_lib(), "orc_", built, threads=threads)
+
+
+def reference_available() -> bool:
+    from oracle import ref_build
+    return ref_build.available()
+
+
+def reference(built, threads=4):
+    from oracle import ref_build
+    lib = ref_build.build(built)
+    return HandleSolver(capi.load_library(lib), "ref_", built, threads=threads)
+
+
+def canonical_order(c: dict) -> np.ndarray:
+    """Permutation putting a contact list in (idA, group, idB) order, group 0 = sphere--analytical."""
+    grp = (c["type"] == capi.SPHERE_SPHERE_CONTACT).astype(np.int64)
+    return np.lexsort((c["idB"].astype(np.int64), grp, c["idA"].astype(np.int64)))
+
+
+def canonical(c: dict) -> dict:
+    p = canonical_order(c)
+    out = {k: (v[..., p] if k == "wildcards" else v[p]) for k, v in c.items() if k != "mapping"}
+    out["perm"] = p
+    return out
+
+
+def partner_keys(c: dict, prev: dict) -> np.ndarray:
+    """For each contact, the (idA, idB, type) key of its history partner in ``prev`` (-1 when new)."""
+    keys = np.full((len(c["idA"]), 3), -1, np.int64)
+    m = c["mapping"]
+    ok = m != capi.NULL_MAPPING_PARTNER
+    mi = m[ok].astype(np.int64)
+    keys[ok, 0] = prev["idA"][mi]
+    keys[ok, 1] = prev["idB"][mi]
+    keys[ok, 2] = prev["type"][mi]
+    return keys
+
+
+def contact_key(c: dict) -> np.ndarray:
+    return np.stack([c["idA"].astype(np.int64), c["idB"].astype(np.int64), c["type"].astype(np.int64)], 1)
+
+
+def rel_err(a, b, floor):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.max(np.abs(a - b) / (np.abs(b) + floor)) if a.size else 0.0
+
+
+def positions(built, st):
+    return built.decode_positions(st)
+
+
+GOLDEN_DIR = os.path.join(ROOT, "tests", "golden")
+GOLDEN = ["clumps_planes", "spheres_families", "settle_small"]
+
+
+class _Built:
+    """A BuiltScene rebuilt from a golden fixture."""
+
+    def __init__(self, rec):
+        from deme_b200.scene import BuiltScene
+        p = capi.SimParams()
+        for name, _ in capi.SimParams._fields_:
+            v = rec["param_" + name]
+            if v.ndim:
+                getattr(p, name)[:] = list(v)
+            else:
+                setattr(p, name, v.item())
+        presc = (capi.FamilyPrescription * capi.NUM_FAMILIES).from_buffer_copy(rec["presc"].tobytes())
+        arrays = {k[len("scene_"):]: rec[k] for k in rec.files if k.startswith("scene_")}
+        o, s, a, m = (int(x) for x in rec["counts"])
+        self.inner = BuiltScene(p, arrays, dict(o=o, s=s, a=a, m=m), presc, {})
+
+    def __getattr__(self, k):
+        return getattr(self.inner, k)
+
+
+def load_golden(name):
+    rec = np.load(os.path.join(GOLDEN_DIR, name + ".npz"))
+    return _Built(rec).inner, rec
