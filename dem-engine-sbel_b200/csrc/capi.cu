@@ -83,6 +83,8 @@ struct deme_handle {
     double* dKE = nullptr;
     double* hKE = nullptr;
     Prescription* hPresc = nullptr;
+    float* analPartial = nullptr;
+    size_t analPartialCap = 0;
     double t = 0.0;
     int64_t steps = 0;
     std::vector<void*> allocs;
@@ -159,12 +161,17 @@ static int32_t read_device_errors(deme_handle* h) {
     CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
     if (*h->hErr) {
         uint32_t e = *h->hErr;
-        h->err = "device error word 0x" + std::to_string(e) +
+        uint32_t w[4] = {0, 0, 0, 0};
+        cudaMemcpy(w, h->dErr, sizeof(w), cudaMemcpyDeviceToHost);
+        h->err = "device error word " + std::to_string(e) +
                  ((e & ERR_SORT_LOOKBACK_TIMEOUT) ? " (radix sort look-back timed out)" : "") +
                  ((e & ERR_CONTACT_CAPACITY) ? " (contact capacity exceeded)" : "") +
-                 ((e & ERR_SEGMENT_TOO_LONG) ? " (contact segment mismatch)" : "");
+                 ((e & ERR_SEGMENT_TOO_LONG) ? " (contact segment mismatch)" : "") +
+                 ((e & ERR_INDEX) ? " (index out of range at site " + std::to_string(w[1]) + ": " +
+                                        std::to_string(w[2]) + " >= " + std::to_string(w[3]) + ")"
+                                  : "");
         *h->hErr = 0;
-        cudaMemsetAsync(h->dErr, 0, sizeof(uint32_t), h->st_dt);
+        cudaMemsetAsync(h->dErr, 0, 4 * sizeof(uint32_t), h->st_dt);
         return (e & ERR_SORT_LOOKBACK_TIMEOUT) ? DEME_ERR_TIMEOUT : DEME_ERR_OVERFLOW;
     }
     return DEME_OK;
@@ -254,6 +261,10 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
     h->nW = p->n_contact_wildcards;
     if (h->nW != 0 && h->nW != 4) {
         h->err = "the built-in models use 0 or 4 contact wildcards";
+        return DEME_ERR_INVALID;
+    }
+    if ((int)p->nvXp2 + (int)p->nvYp2 + (int)p->nvZp2 > 64) {
+        h->err = "voxel bits nvXp2 + nvYp2 + nvZp2 exceed 64: voxel ids would wrap";
         return DEME_ERR_INVALID;
     }
     if (h->nA > 255) {
@@ -446,6 +457,8 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
     TRY(dalloc_n(h, &cd.cellStart, (size_t)h->nCells + 1));
     TRY(dalloc_n(h, &cd.nAnal, nS));
     TRY(dalloc_n(h, &cd.cnt, (size_t)nS + 1));
+    // cnt[nS] stays 0 so the scan over nS + 1 entries leaves the total in off[nS]
+    CUDA_TRY(h, cudaMemset(cd.cnt, 0, ((size_t)nS + 1) * sizeof(uint32_t)));
     for (int b = 0; b < 2; b++) {
         TRY(dalloc_n(h, &h->lists[b].off, (size_t)nS + 1));
         CUDA_TRY(h, cudaMemset(h->lists[b].off, 0, ((size_t)nS + 1) * sizeof(uint32_t)));
@@ -454,6 +467,7 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
     TRY(ensure_scratch(h, std::max(radix_sort_scratch_bytes(nS), scan_scratch_bytes(std::max(h->nCells + 1, nS + 1)))));
     TRY(dalloc_n(h, &h->dTotal, 4));
     TRY(dalloc_n(h, &h->dErr, 4));
+    h->k.err = h->dErr;
     TRY(dalloc_n(h, &h->dKE, 2));
     CUDA_TRY(h, cudaMemset(h->dErr, 0, 4 * sizeof(uint32_t)));
     CUDA_TRY(h, cudaMallocHost(&h->hTotal, 4 * sizeof(uint32_t)));
@@ -537,7 +551,7 @@ int32_t deme_detect_contacts(deme_handle* h) {
     const uint32_t n = *h->hTotal;
     TRY(ensure_list(h, nb, n));
     launch_pair_emit(k, s, cd, nb.view(), nb.cap, h->dErr, st);
-    launch_history(k, nb.view(), pb.view(), n, h->nW > 0, st);
+    launch_history(k, nb.view(), pb.view(), n, h->nContacts, h->nW > 0, st);
     TRY(check_launch(h, "contact emit"));
     h->cur = nxt;
     h->nContacts = n;
@@ -561,7 +575,19 @@ int32_t deme_compute_forces(deme_handle* h) {
         TRY(ensure_outputs(h, h->nContacts));
         out = &h->outs;
     }
-    launch_force(k, s, c.view(), h->nContacts, h->nW > 0, out, st);
+    AnalAccum aa{nullptr, h->nClumps, h->nO - h->nClumps};
+    if (aa.nAO) {
+        const size_t need = (size_t)force_blocks(std::max(h->nContacts, 1u)) * 6u * aa.nAO;
+        if (need > h->analPartialCap) {
+            dfree(h, h->analPartial);
+            h->analPartial = nullptr;
+            h->analPartialCap = 0;
+            TRY(dalloc_n(h, &h->analPartial, need + need / 4 + 64));
+            h->analPartialCap = need + need / 4 + 64;
+        }
+        aa.partial = h->analPartial;
+    }
+    launch_force(k, s, c.view(), h->nContacts, h->nW > 0, out, aa, st);
     TRY(check_launch(h, "force"));
     h->outsValid = out != nullptr;
     return DEME_OK;
@@ -804,6 +830,13 @@ int32_t deme_set_family_prescription(deme_handle* h, int32_t family, const deme_
         q.pos[c] = src->pos[c];
     }
     CUDA_TRY(h, cudaMemcpyAsync(h->presc + family, h->hPresc, sizeof(Prescription), cudaMemcpyHostToDevice, h->st_dt));
+    return DEME_OK;
+}
+
+int32_t deme_set_time_step(deme_handle* h, float h_step) {
+    if (!h || !(h_step > 0.f)) return DEME_ERR_INVALID;
+    h->params.h = h_step;
+    h->k.h = h_step;
     return DEME_OK;
 }
 

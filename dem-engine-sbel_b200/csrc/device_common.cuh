@@ -45,6 +45,7 @@ struct SimConsts {
     uint32_t gx, gy, gz;
     float r_max_cd;      // largest CD radius (radius + beta)
     float prefilter_abs; // absolute slack of the float pre-filter
+    uint32_t* err;       // device error block (4 words), see index_ok
 };
 
 // Per-family prescription (constant-valued form of the reference's jitified strings).
@@ -242,6 +243,18 @@ enum : uint32_t {
     ERR_SORT_LOOKBACK_TIMEOUT = 1u << 1,
     ERR_SCAN_LOOKBACK_TIMEOUT = 1u << 2,
     ERR_SEGMENT_TOO_LONG = 1u << 3,
+    ERR_INDEX = 1u << 4,
 };
+
+// Index self-check: an out-of-range index sets ERR_INDEX, records (site, index, limit) of the first offender in
+// err[1..3] and the caller skips the access.  err points to the handle's 4-word device error block.
+__device__ __forceinline__ bool index_ok(uint32_t* err, uint32_t site, uint64_t idx, uint64_t limit) {
+    if (idx < limit) return true;
+    if (atomicOr(err, ERR_INDEX) & ERR_INDEX) return false;
+    err[1] = site;
+    err[2] = (uint32_t)idx;
+    err[3] = (uint32_t)limit;
+    return false;
+}
 
 }  // namespace deme_b200

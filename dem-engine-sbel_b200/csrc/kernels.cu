@@ -130,16 +130,19 @@ void launch_sphere_prep(const SimConsts& k, const StateView& s, const CDView& cd
 }
 
 __global__ void k_gather_sorted(uint32_t n, const float4* __restrict__ posF, const uint32_t* __restrict__ idSorted,
-                                float4* __restrict__ out) {
+                                float4* __restrict__ out, uint32_t* err) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = posF[idSorted[i]];
+    if (i < n) {
+        const uint32_t j = idSorted[i];
+        if (index_ok(err, 1, j, n)) out[i] = posF[j];
+    }
 }
 
 void launch_gather_sorted(const SimConsts& k, const CDView& cd, cudaStream_t st) {
     if (!(k.n_spheres)) return;
     ProfScope prof_(KID_GATHER, st);
     if (k.n_spheres) k_gather_sorted<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k.n_spheres, cd.posF, cd.idSorted,
-                                                                                     cd.posFSorted);
+                                                                                     cd.posFSorted, k.err);
 }
 
 // The reference's pair predicate for A < B (see the file comment).  Returns true when the pair is a contact.
@@ -205,10 +208,12 @@ __device__ __forceinline__ uint32_t scan_neighbours(const SimConsts& k, const St
             const uint32_t rowBase = k.gx * (cy + k.gy * cz);
             // cells x0..x1 of one row are contiguous in the sorted order
             const uint32_t j0 = cd.cellStart[rowBase + x0];
-            const uint32_t j1 = cd.cellStart[rowBase + x1 + 1];
+            uint32_t j1 = cd.cellStart[rowBase + x1 + 1];
+            if (!index_ok(k.err, 2, j1, (uint64_t)k.n_spheres + 1)) j1 = j0;
             for (uint32_t j = j0; j < j1; j++) {
                 const uint32_t B = cd.idSorted[j];
                 if (B <= A) continue;
+                if (!index_ok(k.err, 3, B, k.n_spheres)) continue;
                 const float4 fB = cd.posFSorted[j];
                 const float dx = fA.x - fB.x, dy = fA.y - fB.y, dz = fA.z - fB.z;
                 const float lim = (fA.w + fB.w) * 1.00001f + k.prefilter_abs;
@@ -260,6 +265,7 @@ __global__ void __launch_bounds__(256) k_pair_emit(SimConsts k, StateView s, CDV
             if (s.masks[mask_index(fam, s.loc[ap.owner].w)] != 0) continue;
             const int t = anal_overlap_cd(ap, X, Y, Z, rD, k.beta);
             if (t != DEME_NOT_A_CONTACT) {
+                if (!index_ok(k.err, 4, w, cap)) break;
                 c.idA[w] = A;
                 c.idB[w] = a;
                 c.type[w] = (uint8_t)t;
@@ -300,13 +306,20 @@ void launch_pair_emit(const SimConsts& k, const StateView& s, const CDView& cd, 
 // (buildPersistentMap, src/kernel/DEMHistoryMappingKernels.cu:16-60; rearrangeContactWildcards,
 // src/kernel/DEMPrepForceKernels.cu:93-115).  Segments of both lists are sorted by (group, idB), group 0 being the
 // sphere--analytical contacts, so a binary search finds the unique partner.
-__global__ void __launch_bounds__(256) k_history(uint32_t n, ContactView cur, ContactView prev, bool has_hist) {
+__global__ void __launch_bounds__(256) k_history(uint32_t n, ContactView cur, ContactView prev, bool has_hist,
+                                                 uint32_t nS, uint32_t prevN, uint32_t* err) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t A = cur.idA[i], B = cur.idB[i];
     const uint8_t t = cur.type[i];
     const uint64_t key = ((uint64_t)(t == DEME_SPHERE_SPHERE_CONTACT ? 1u : 0u) << 32) | B;
+    if (!index_ok(err, 5, A, nS)) return;
     uint32_t lo = prev.off[A], hi = prev.off[A + 1];
+    if (!index_ok(err, 6, hi, (uint64_t)prevN + 1) || lo > hi) {
+        cur.mapping[i] = DEME_NULL_MAPPING_PARTNER;
+        if (has_hist) cur.hist[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
     uint32_t partner = DEME_NULL_MAPPING_PARTNER;
     while (lo < hi) {
         const uint32_t mid = (lo + hi) >> 1;
@@ -319,15 +332,16 @@ __global__ void __launch_bounds__(256) k_history(uint32_t n, ContactView cur, Co
         }
     }
     if (lo < prev.off[A + 1] && prev.idB[lo] == B && prev.type[lo] == t) partner = lo;
+    if (partner != DEME_NULL_MAPPING_PARTNER && !index_ok(err, 7, partner, prevN)) partner = DEME_NULL_MAPPING_PARTNER;
     cur.mapping[i] = partner;
     if (has_hist) cur.hist[i] = partner == DEME_NULL_MAPPING_PARTNER ? make_float4(0.f, 0.f, 0.f, 0.f) : prev.hist[partner];
 }
 
-void launch_history(const SimConsts& k, const ContactView& cur, const ContactView& prev, uint32_t n, bool has_hist,
-                    cudaStream_t st) {
+void launch_history(const SimConsts& k, const ContactView& cur, const ContactView& prev, uint32_t n, uint32_t prevN,
+                    bool has_hist, cudaStream_t st) {
     if (!(n)) return;
     ProfScope prof_(KID_HISTORY, st);
-    if (n) k_history<<<blocks_for(n, 256), 256, 0, st>>>(n, cur, prev, has_hist);
+    k_history<<<blocks_for(n, 256), 256, 0, st>>>(n, cur, prev, has_hist, k.n_spheres, prevN, k.err);
 }
 
 __global__ void k_count_by_sphere(const uint32_t* idA, uint32_t n, uint32_t* cnt) {
@@ -344,7 +358,11 @@ void launch_count_by_sphere(const uint32_t* idA, uint32_t n, uint32_t* cnt, cuda
 // Fused force + collection kernel.
 template <bool kStore>
 __global__ void __launch_bounds__(256) k_force(SimConsts k, StateView s, ContactView c, uint32_t n, bool has_hist,
-                                               ContactOutputs out) {
+                                               ContactOutputs out, AnalAccum aa) {
+    // analytical owners (walls) collect their reactions block-locally, then one fixed-order reduction
+    extern __shared__ float s_anal[];  // 6 floats per analytical owner
+    for (uint32_t t = threadIdx.x; t < 6u * aa.nAO; t += blockDim.x) s_anal[t] = 0.f;
+    if (aa.nAO) __syncthreads();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = i < n;
     uint32_t oA = 0xFFFFFFFFu, oB = 0xFFFFFFFFu;
@@ -354,7 +372,14 @@ __global__ void __launch_bounds__(256) k_force(SimConsts k, StateView s, Contact
     float4 qA = make_float4(1.f, 0.f, 0.f, 0.f), qB = qA;
     float mA = 1.f, mB = 1.f;
     bool active = false;
+    bool ids_ok = valid;
     if (valid) {
+        const int ct0 = c.type[i];
+        ids_ok = index_ok(k.err, 8, c.idA[i], k.n_spheres) &&
+                 index_ok(k.err, 9, c.idB[i], ct0 == DEME_SPHERE_SPHERE_CONTACT ? k.n_spheres : k.n_anal) &&
+                 index_ok(k.err, 10, ct0 == DEME_SPHERE_SPHERE_CONTACT || ct0 >= 3 ? 0 : 1, 1);
+    }
+    if (ids_ok) {
         const uint32_t sA = c.idA[i];
         const uint32_t bId = c.idB[i];
         int ct = c.type[i];
@@ -458,13 +483,15 @@ __global__ void __launch_bounds__(256) k_force(SimConsts k, StateView s, Contact
     float4 aA = make_float4(0.f, 0.f, 0.f, 0.f), alA = aA, aB = aA, alB = aA;
     if (active) {
         const float4 mi = s.moi[oA];
+        const bool bOwnerCounts = bSphere || aa.nAO;
         aA = make_float4((F.x * 1.f) / mA, (F.y * 1.f) / mA, (F.z * 1.f) / mA, 0.f);
         float gx = (F.x + T.x) * 1.f, gy = (F.y + T.y) * 1.f, gz = (F.z + T.z) * 1.f;
         rot_f(gx, gy, gz, qA.x, -qA.y, -qA.z, -qA.w);
         alA = make_float4((cpA.y * gz - cpA.z * gy) / mi.x, (cpA.z * gx - cpA.x * gz) / mi.y,
                           (cpA.x * gy - cpA.y * gx) / mi.z, 0.f);
-        if (bSphere) {
+        if (bOwnerCounts) {
             const float4 mj = s.moi[oB];
+            if (!bSphere) mB = s.vel[oB].w;  // owner mass of the analytical object (massOwnerBody)
             aB = make_float4((F.x * -1.f) / mB, (F.y * -1.f) / mB, (F.z * -1.f) / mB, 0.f);
             float hx = (F.x + T.x) * -1.f, hy = (F.y + T.y) * -1.f, hz = (F.z + T.z) * -1.f;
             rot_f(hx, hy, hz, qB.x, -qB.y, -qB.z, -qB.w);
@@ -474,7 +501,7 @@ __global__ void __launch_bounds__(256) k_force(SimConsts k, StateView s, Contact
     }
     // A side: contacts of one owner are adjacent (sorted by sphere id; a clump's spheres have consecutive ids).
     const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t key = valid ? oA : 0xFFFFFFFFu;
+    const uint32_t key = ids_ok ? oA : 0xFFFFFFFFu;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
         const uint32_t k2 = __shfl_down_sync(0xffffffffu, key, off);
@@ -503,18 +530,60 @@ __global__ void __launch_bounds__(256) k_force(SimConsts k, StateView s, Contact
         atomicAdd(&s.acc[oB], aB);
         atomicAdd(&s.alpha[oB], alB);
     }
+    if (aa.nAO) {
+        if (active && !bSphere && index_ok(k.err, 11, oB - aa.nClumps, aa.nAO)) {
+            float* slot = s_anal + 6u * (oB - aa.nClumps);
+            atomicAdd(slot + 0, aB.x);
+            atomicAdd(slot + 1, aB.y);
+            atomicAdd(slot + 2, aB.z);
+            atomicAdd(slot + 3, alB.x);
+            atomicAdd(slot + 4, alB.y);
+            atomicAdd(slot + 5, alB.z);
+        }
+        __syncthreads();
+        for (uint32_t t = threadIdx.x; t < 6u * aa.nAO; t += blockDim.x)
+            aa.partial[(size_t)blockIdx.x * 6u * aa.nAO + t] = s_anal[t];
+    }
+}
+
+// Sum the per-block partials of each analytical owner in block order (deterministic) into its accumulators.
+__global__ void k_anal_reduce(AnalAccum aa, uint32_t nBlocks, float4* acc, float4* alpha) {
+    __shared__ float sh[256];
+    const uint32_t slot = blockIdx.x / 6u, comp = blockIdx.x % 6u;
+    float v = 0.f;
+    for (uint32_t b = threadIdx.x; b < nBlocks; b += blockDim.x) v += aa.partial[(size_t)b * 6u * aa.nAO + 6u * slot + comp];
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (uint32_t w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const uint32_t o = aa.nClumps + slot;
+        float* dst = comp < 3 ? &acc[o].x : &alpha[o].x;
+        dst[comp % 3] = sh[0];
+    }
 }
 
 void launch_force(const SimConsts& k, const StateView& s, const ContactView& c, uint32_t n, bool has_hist,
-                  const ContactOutputs* out, cudaStream_t st) {
+                  const ContactOutputs* out, const AnalAccum& aa, cudaStream_t st) {
     if (!(n)) return;
-    ProfScope prof_(KID_FORCE, st);
-    if (!n) return;
-    if (out)
-        k_force<true><<<blocks_for(n, 256), 256, 0, st>>>(k, s, c, n, has_hist, *out);
-    else
-        k_force<false><<<blocks_for(n, 256), 256, 0, st>>>(k, s, c, n, has_hist, ContactOutputs{});
+    const uint32_t nb = blocks_for(n, 256);
+    const size_t smem = 6u * aa.nAO * sizeof(float);
+    {
+        ProfScope prof_(KID_FORCE, st);
+        if (out)
+            k_force<true><<<nb, 256, smem, st>>>(k, s, c, n, has_hist, *out, aa);
+        else
+            k_force<false><<<nb, 256, smem, st>>>(k, s, c, n, has_hist, ContactOutputs{}, aa);
+    }
+    if (aa.nAO) {
+        ProfScope prof_(KID_OTHER, st);
+        k_anal_reduce<<<6u * aa.nAO, 256, 0, st>>>(aa, nb, s.acc, s.alpha);
+    }
 }
+
+uint32_t force_blocks(uint32_t n) { return blocks_for(n, 256); }
 
 // ------------------------------------------------------------------------------------------------------------
 // integrateOwners (src/kernel/DEMIntegrationKernels.cu:46-179) with the constant prescription table.

@@ -63,6 +63,13 @@ struct ContactView {
     uint32_t* off;      // CSR offsets by sphere (nS + 1)
 };
 
+// Reactions on analytical owners (walls): block partials, reduced in fixed order.
+struct AnalAccum {
+    float* partial;     // blocks x nAO x 6
+    uint32_t nClumps;   // analytical owners are [nClumps, nClumps + nAO)
+    uint32_t nAO;
+};
+
 struct ContactOutputs {
     float4* F;
     float4* TOF;
@@ -77,11 +84,12 @@ void launch_gather_sorted(const SimConsts& k, const CDView& cd, cudaStream_t st)
 void launch_pair_count(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
 void launch_pair_emit(const SimConsts& k, const StateView& s, const CDView& cd, const ContactView& c, uint32_t cap,
                       uint32_t* err, cudaStream_t st);
-void launch_history(const SimConsts& k, const ContactView& cur, const ContactView& prev, uint32_t n, bool has_hist,
-                    cudaStream_t st);
+void launch_history(const SimConsts& k, const ContactView& cur, const ContactView& prev, uint32_t n, uint32_t prevN,
+                    bool has_hist, cudaStream_t st);
 void launch_count_by_sphere(const uint32_t* idA, uint32_t n, uint32_t* cnt, cudaStream_t st);
 void launch_force(const SimConsts& k, const StateView& s, const ContactView& c, uint32_t n, bool has_hist,
-                  const ContactOutputs* out, cudaStream_t st);
+                  const ContactOutputs* out, const AnalAccum& aa, cudaStream_t st);
+uint32_t force_blocks(uint32_t n);
 void launch_integrate(const SimConsts& k, const StateView& s, cudaStream_t st);
 void launch_kinetic_energy(const SimConsts& k, const StateView& s, uint32_t n_clumps, double* out, cudaStream_t st);
 

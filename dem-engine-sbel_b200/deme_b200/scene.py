@@ -377,6 +377,12 @@ class SceneBuilder:
                 b1 += 1
             left -= 1
         bits = [b3, b2, b1]
+        if sum(bits) > 64:
+            # The reference's split (APIPrivate.cpp:267-281) subtracts the second-place extra bits once but gives
+            # them to both larger axes, so it overshoots 64 bits whenever that extra is non-zero; the top bits of
+            # the voxel id then wrap and positions jump.  Refuse such domains instead of corrupting positions.
+            raise ValueError(f"domain {list(map(float, self.box))} needs {sum(bits)} voxel bits (> 64) under the "
+                             "reference's bit split; use a domain whose two smaller sides are within a factor sqrt(2)")
         if self.dir_exact is not None:
             raise NotImplementedError("exact-direction world sizing")
         ls = [float(size321[i]) / 2.0**16 / 2.0**bits[i] for i in range(3)]

@@ -193,7 +193,11 @@ class Solver(HandleSolver):
         h = C.c_void_p()
         st = lib.deme_create(C.byref(self._params), C.byref(scene), C.byref(h))
         if st != capi.DEME_OK:
-            raise DemeError(f"deme_create: {capi.STATUS_NAMES.get(st, st)}")
+            msg = lib.deme_get_error(h.value) if h.value else b""
+            if h.value:
+                lib.deme_destroy(h.value)
+            self.h = None
+            raise DemeError(f"deme_create: {capi.STATUS_NAMES.get(st, st)}: {msg.decode() if msg else ''}")
         self.h = h.value
         self.nO = built.counts["o"]
         self.nS = built.counts["s"]
@@ -216,6 +220,18 @@ class Solver(HandleSolver):
         ke = C.c_double(0)
         self._check(self.lib.deme_kinetic_energy(self.h, C.byref(ke)), "kinetic_energy")
         return float(ke.value)
+
+    def set_time_step(self, h: float):
+        self.lib.deme_set_time_step.argtypes = [C.c_void_p, C.c_float]
+        self._check(self.lib.deme_set_time_step(self.h, h), "set_time_step")
+
+    def set_streams(self, kt_stream: int | None, dt_stream: int | None):
+        self.lib.deme_set_streams.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        self._check(self.lib.deme_set_streams(self.h, kt_stream, dt_stream), "set_streams")
+
+    def keep_contact_forces(self, enable: bool = True):
+        self.lib.deme_keep_contact_forces.argtypes = [C.c_void_p, C.c_int32]
+        self._check(self.lib.deme_keep_contact_forces(self.h, int(enable)), "keep_contact_forces")
 
     def set_force_model(self, src: str | None, wildcards=()):
         names = (C.c_char_p * max(len(wildcards), 1))(*[w.encode() for w in wildcards])

@@ -102,7 +102,7 @@ def drum(n_clumps: int = 1_000_000, r_nom: float = 2e-3, rho: float = 2500.0, n_
 
     One million clumps of about 8e-8 m^3 do not fit a 30 % fill of an R = 0.25 m, L = 0.3 m drum, so the drum is
     scaled (same L / R ratio) until the clumps at ``packing`` bulk density fill ``fill`` of its volume.
-    Clumps start on a jittered lattice in the lower part of the drum with random orientations.
+    Clumps start on a loose lattice in the lower part of the drum with random orientations.
     """
     rng = np.random.default_rng(seed)
     tmpl = [triangle_template(rng, r_nom, rho) for _ in range(n_templates)]
@@ -113,24 +113,32 @@ def drum(n_clumps: int = 1_000_000, r_nom: float = 2e-3, rho: float = 2500.0, n_
     L = 1.2 * R
     s = SceneBuilder()
     margin = 4 * r_nom
-    box = (2 * R + 2 * margin, L + 2 * margin, 2 * R + 2 * margin)
+    # cubic domain, as in the reference's drum demo: the reference's voxel bit split overshoots 64 bits when the
+    # two smaller sides differ by more than sqrt(2)
+    side = 2 * R + 2 * margin
+    box = (side, side, side)
     s.InstructBoxDomainDimension(*box)
     s.SetCoordSysOrigin("center")
     mat = s.LoadMaterial({"E": 5e7, "nu": 0.3, "CoR": 0.3, "mu": 0.4, "Crr": 0.02})
     ts = [s.LoadClumpType(t[2], t[3], t[0], t[1], mat) for t in tmpl]
-    # lattice of clump centres inside the drum's lower region
-    a = 2.4 * 1.2 * r_nom * 1.25
-    xs = np.arange(-R + a, R - a, a)
-    ys = np.arange(-L / 2 + a, L / 2 - a, a)
-    zs = np.arange(-R + a, R - a, a)
-    X, Y, Z = np.meshgrid(xs, ys, zs, indexing="ij")
-    P = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
-    inside = P[:, 0] ** 2 + P[:, 2] ** 2 <= (R - a) ** 2
+    # Clump centres on a hexagonal close-packed lattice of non-overlapping bounding spheres (the reference's drum
+    # demo likewise starts from a grid sampler with spacing above the clump size), filled from the bottom of the
+    # drum; the bed settles under gravity before measurements (bench.py).
+    reach = float(max(np.max(np.linalg.norm(t[1], axis=1) + t[0]) for t in tmpl))
+    a = 2.0 * reach * 1.02
+    dy, dz = a * math.sqrt(3.0) / 2.0, a * math.sqrt(2.0 / 3.0)
+    nx, ny, nz = int(2 * R / a) + 2, int(L / dy) + 2, int(2 * R / dz) + 2
+    K, J, I = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    px = -R + I * a + np.where((J + K) % 2 == 0, 0.0, a / 2)
+    py = -L / 2 + J * dy + np.where(K % 2 == 0, 0.0, dy / 3)
+    pz = -R + K * dz
+    P = np.stack([px.ravel(), py.ravel(), pz.ravel()], axis=1)
+    inside = (P[:, 0] ** 2 + P[:, 2] ** 2 <= (R - reach * 1.05) ** 2) & (np.abs(P[:, 1]) <= L / 2 - reach * 1.05)
     P = P[inside]
     P = P[np.argsort(P[:, 2], kind="stable")]
     if len(P) < n_clumps:
         raise ValueError(f"lattice holds {len(P)} clumps, {n_clumps} requested")
-    P = P[:n_clumps] + rng.uniform(-0.05 * a, 0.05 * a, size=(n_clumps, 3))
+    P = P[:n_clumps]
     types = rng.integers(0, n_templates, n_clumps)
     b = s.AddClumps(types, P.astype(f32))
     b.SetOriQ(random_quaternions(rng, n_clumps))
@@ -147,7 +155,7 @@ def drum(n_clumps: int = 1_000_000, r_nom: float = 2e-3, rho: float = 2500.0, n_
     s.SetGravitationalAcceleration((0, 0, -9.81))
     built = s.Initialize()
     built.info.update(workload="drum", R=R, L=L, n_templates=n_templates, omega=omega, seed=seed,
-                      vol_clump=vol_clump, n_clumps=n_clumps)
+                      vol_clump=vol_clump, n_clumps=n_clumps, lattice_spacing=a, clump_reach=reach)
     return built
 
 

@@ -281,6 +281,9 @@ int64_t deme_launch_count(void);
 int32_t deme_kernel_timing(int32_t enable);
 int32_t deme_kernel_times(int32_t cap, const char** names, double* total_ms, int64_t* launches, int32_t* n_out);
 
+/* Change the time step between steps (SetInitTimeStep followed by UpdateSimParams, src/DEM/API.h:61, 399). */
+int32_t deme_set_time_step(deme_handle* h, float h_step);
+
 /* Simulation time advanced so far and step counter. */
 int32_t deme_get_time(deme_handle* h, double* t, int64_t* steps);
 /* Sum of 0.5 m v^2 + 0.5 I omega^2 over clump owners (DEMOwnerQueryKernels.cu:10-37 computes the per-owner term;

@@ -24,7 +24,12 @@ ORACLE_LIB = os.path.join(ROOT, "oracle", "_build", "libdeme_oracle.so")
 def oracle_lib():
     if not os.path.exists(ORACLE_LIB):
         subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
-    return capi.load_library(ORACLE_LIB)
+    try:
+        return capi.load_library(ORACLE_LIB)
+    except OSError:
+        # prebuilt with an OpenMP runtime this machine lacks: rebuild without it
+        subprocess.check_call(["make", "-s", "-B", "-C", os.path.join(ROOT, "oracle")])
+        return capi.load_library(ORACLE_LIB)
 
 
 def oracle(built, threads=4):

@@ -43,7 +43,7 @@ def owner_scale(built, c, f):
         f["torque_only_force"].astype(np.float64), axis=1)
     lin = np.zeros(nO)
     np.add.at(lin, oA, Fm)
-    np.add.at(lin, oB[ss], Fm[ss])
+    np.add.at(lin, oB, Fm)
     return lin / a["mass"].astype(np.float64)
 
 
