@@ -103,12 +103,13 @@ def algorithmic_bytes(kernel: str, nS: int, nO: int, nC: int, n_cells: int) -> f
         # per contact: idA, idB, type (9 B) + history read and write (32 B); per sphere: relPos+radius, owner,
         # material (21 B); per owner: voxel, loc, quat, vel+mass, omega, MOI (80 B) + accumulators (32 B)
         return 41.0 * nC + 21.0 * nS + 112.0 * nO
-    if kernel == "pair_count":
-        # per sphere: ID-order posF, exact position, owner, radius (60 B) + cell-order posF, id (20 B) + count (4 B);
-        # the cell table once
-        return 84.0 * nS + 4.0 * n_cells
-    if kernel == "pair_emit":
-        return 84.0 * nS + 4.0 * n_cells + 9.0 * nC + 4.0 * nS
+    if kernel == "pair_find":
+        # per sphere: cell-order position+radius and id (20 B), exact position, owner, radius (44 B), count and
+        # list start (8 B); the cell table once; partner ids written once (4 B per sphere-sphere contact)
+        return 72.0 * nS + 4.0 * n_cells + 4.0 * nC
+    if kernel == "pair_assemble":
+        # per sphere: offsets, counts, list start (16 B); partner ids read (4 B) and idA, idB, type written (9 B)
+        return 16.0 * nS + 13.0 * nC
     if kernel == "integrate":
         return 160.0 * nO
     if kernel == "sort_onesweep":
@@ -176,7 +177,7 @@ def cpu_baseline_sample(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--clumps", type=int, default=1_000_000)
@@ -241,7 +242,9 @@ def main():
     s.sync()
     prep_s = time.perf_counter() - t_prep
 
-    # ---- warm-up ----
+    # ---- warm-up (the clock sampler starts here so it has samples when the timed region is short) ----
+    sampler = ClockSampler(local_rank)
+    sampler.start()
     s.step(args.warmup)
     s.sync()
     torch.cuda.synchronize()
@@ -249,8 +252,6 @@ def main():
         dist.barrier()
 
     # ---- timed region ----
-    sampler = ClockSampler(local_rank)
-    sampler.start()
     n0 = lib.deme_launch_count()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)

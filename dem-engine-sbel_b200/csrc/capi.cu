@@ -65,6 +65,7 @@ struct deme_handle {
     CDView cd{};
     uint32_t nCells = 0;
     int cellBits = 0;
+    uint32_t candCap = 0;
     ContactBuf lists[2];
     int cur = 0;
     uint32_t nContacts = 0;
@@ -205,6 +206,17 @@ static int32_t ensure_list(deme_handle* h, ContactBuf& b, uint32_t n) {
     TRY(dalloc_n(h, &b.hist, cap));
     TRY(dalloc_n(h, &b.mapping, cap));
     b.cap = cap;
+    return DEME_OK;
+}
+
+static int32_t ensure_cand(deme_handle* h, uint32_t n) {
+    if (n <= h->candCap) return DEME_OK;
+    const uint32_t cap = std::max<uint32_t>(1024u, (uint32_t)std::min<uint64_t>(0xFFFFFFF0ull, (uint64_t)n * 5 / 4 + 64));
+    dfree(h, h->cd.candTemp);
+    h->cd.candTemp = nullptr;
+    h->candCap = 0;
+    TRY(dalloc_n(h, &h->cd.candTemp, cap));
+    h->candCap = cap;
     return DEME_OK;
 }
 
@@ -449,6 +461,10 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
     TRY(dalloc_n(h, &cd.pZ, nS));
     TRY(dalloc_n(h, &cd.posF, nS));
     TRY(dalloc_n(h, &cd.posFSorted, nS));
+    TRY(dalloc_n(h, &cd.pXs, nS));
+    TRY(dalloc_n(h, &cd.pYs, nS));
+    TRY(dalloc_n(h, &cd.pZs, nS));
+    TRY(dalloc_n(h, &cd.metaS, nS));
     TRY(dalloc_n(h, &cd.cellKey, nS));
     TRY(dalloc_n(h, &cd.idSeq, nS));
     TRY(dalloc_n(h, &cd.keySorted, nS));
@@ -459,6 +475,10 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
     TRY(dalloc_n(h, &cd.cnt, (size_t)nS + 1));
     // cnt[nS] stays 0 so the scan over nS + 1 entries leaves the total in off[nS]
     CUDA_TRY(h, cudaMemset(cd.cnt, 0, ((size_t)nS + 1) * sizeof(uint32_t)));
+    TRY(dalloc_n(h, &cd.candStart, nS + 1));
+    TRY(dalloc_n(h, &cd.ovf, nS + 1));
+    TRY(dalloc_n(h, &cd.counters, 4));
+    TRY(ensure_cand(h, std::max<uint32_t>(1024u, 2u * nS)));
     for (int b = 0; b < 2; b++) {
         TRY(dalloc_n(h, &h->lists[b].off, (size_t)nS + 1));
         CUDA_TRY(h, cudaMemset(h->lists[b].off, 0, ((size_t)nS + 1) * sizeof(uint32_t)));
@@ -539,20 +559,30 @@ int32_t deme_detect_contacts(deme_handle* h) {
     launch_sphere_prep(k, s, cd, st);
     exclusive_scan_u32(cd.cellCount, h->nCells + 1, cd.cellStart, nullptr, h->scratch, st);
     radix_sort_pairs(cd.cellKey, cd.idSeq, cd.keySorted, cd.idSorted, h->nS, h->cellBits, h->scratch, h->dErr, st);
-    launch_gather_sorted(k, cd, st);
-    launch_pair_count(k, s, cd, st);
-    TRY(check_launch(h, "contact count"));
+    launch_gather_sorted(k, s, cd, st);
     const int nxt = h->cur ^ 1;
     ContactBuf& nb = h->lists[nxt];
     ContactBuf& pb = h->lists[h->cur];
-    exclusive_scan_u32(cd.cnt, h->nS + 1, nb.off, h->dTotal, h->scratch, st);
-    CUDA_TRY(h, cudaMemcpyAsync(h->hTotal, h->dTotal, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(h, cudaStreamSynchronize(st));
-    const uint32_t n = *h->hTotal;
+    uint32_t n = 0, nOvf = 0;
+    for (int attempt = 0; attempt < 2; attempt++) {
+        CUDA_TRY(h, cudaMemsetAsync(cd.counters, 0, 2 * sizeof(uint32_t), st));
+        launch_pair_find(k, s, cd, h->candCap, st);
+        TRY(check_launch(h, "contact search"));
+        exclusive_scan_u32(cd.cnt, h->nS + 1, nb.off, h->dTotal, h->scratch, st);
+        CUDA_TRY(h, cudaMemcpyAsync(h->hTotal + 1, cd.counters, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(h, cudaMemcpyAsync(h->hTotal, h->dTotal, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(h, cudaStreamSynchronize(st));
+        n = h->hTotal[0];
+        nOvf = h->hTotal[2];
+        if (h->hTotal[1] <= h->candCap) break;
+        // the partner list outgrew its buffer: grow and search again
+        TRY(ensure_cand(h, h->hTotal[1]));
+    }
+    launch_pair_overflow(k, s, cd, nOvf, h->candCap, st);
     TRY(ensure_list(h, nb, n));
-    launch_pair_emit(k, s, cd, nb.view(), nb.cap, h->dErr, st);
+    launch_pair_assemble(k, s, cd, nb.view(), nb.cap, st);
     launch_history(k, nb.view(), pb.view(), n, h->nContacts, h->nW > 0, st);
-    TRY(check_launch(h, "contact emit"));
+    TRY(check_launch(h, "contact assembly"));
     h->cur = nxt;
     h->nContacts = n;
     h->outsValid = false;

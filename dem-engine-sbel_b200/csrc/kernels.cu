@@ -129,31 +129,40 @@ void launch_sphere_prep(const SimConsts& k, const StateView& s, const CDView& cd
     if (k.n_spheres) k_sphere_prep<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
 }
 
-__global__ void k_gather_sorted(uint32_t n, const float4* __restrict__ posF, const uint32_t* __restrict__ idSorted,
-                                float4* __restrict__ out, uint32_t* err) {
+// Cell-order copies of everything the contact search reads, so that a warp (neighbouring cells) reads contiguous
+// memory: position + id for the pre-filter, exact position and (owner, radius, family) for the exact test.
+__global__ void k_gather_sorted(SimConsts k, StateView s, CDView cd) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) {
-        const uint32_t j = idSorted[i];
-        if (index_ok(err, 1, j, n)) out[i] = posF[j];
-    }
+    if (i >= k.n_spheres) return;
+    const uint32_t j = cd.idSorted[i];
+    if (!index_ok(k.err, 1, j, k.n_spheres)) return;
+    const float4 p = cd.posF[j];
+    cd.posFSorted[i] = make_float4(p.x, p.y, p.z, __uint_as_float(j));
+    cd.pXs[i] = cd.pX[j];
+    cd.pYs[i] = cd.pY[j];
+    cd.pZs[i] = cd.pZ[j];
+    const uint32_t o = s.sOwner[j];
+    cd.metaS[i] = make_uint4(o, __float_as_uint(s.sph[j].w), s.loc[o].w, 0u);
 }
 
-void launch_gather_sorted(const SimConsts& k, const CDView& cd, cudaStream_t st) {
+void launch_gather_sorted(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st) {
     if (!(k.n_spheres)) return;
     ProfScope prof_(KID_GATHER, st);
-    if (k.n_spheres) k_gather_sorted<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k.n_spheres, cd.posF, cd.idSorted,
-                                                                                     cd.posFSorted, k.err);
+    k_gather_sorted<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
 }
 
-// The reference's pair predicate for A < B (see the file comment).  Returns true when the pair is a contact.
-__device__ __forceinline__ bool pair_is_contact(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t A,
-                                                uint32_t B, uint32_t oA, uint32_t famA, float rfA, double xa,
-                                                double ya, double za, const uint32_t loA[3], const uint32_t hiA[3],
-                                                float rfB) {
-    const uint32_t oB = s.sOwner[B];
+// The reference's pair predicate for A < B (see the file comment), B given by its cell-order index j.
+__device__ __forceinline__ bool pair_is_contact(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t j,
+                                                uint32_t oA, uint32_t famA, float rfA, double xa, double ya, double za,
+                                                const uint32_t loA[3], const uint32_t hiA[3]) {
+    const uint4 mB = cd.metaS[j];
+    const uint32_t oB = mB.x;
     if (oA == oB) return false;
-    if (s.masks[mask_index(famA, s.loc[oB].w)] != 0) return false;
-    const double xb = cd.pX[B], yb = cd.pY[B], zb = cd.pZ[B];
+    if (s.masks[mask_index(famA, mB.z)] != 0) return false;
+    const float rB = __uint_as_float(mB.y);
+    float rfB = rB;
+    rfB += k.beta;
+    const double xb = cd.pXs[j], yb = cd.pYs[j], zb = cd.pZs[j];
     // checkSpheresOverlap<double>, DEMHelperKernels.cu:195-222
     const double radA = (double)rfA, radB = (double)rfB;
     const double d2 = (xa - xb) * (xa - xb) + (ya - yb) * (ya - yb) + (za - zb) * (za - zb);
@@ -167,8 +176,7 @@ __device__ __forceinline__ bool pair_is_contact(const SimConsts& k, const StateV
     // getPointBinID, DEMHelperKernels.cu:266-273, tested per axis against both spheres' bin ranges
     const uint32_t bx = sat_u32(cpx / k.bin_size), by = sat_u32(cpy / k.bin_size), bz = sat_u32(cpz / k.bin_size);
     if (bx < loA[0] || bx > hiA[0] || by < loA[1] || by > hiA[1] || bz < loA[2] || bz > hiA[2]) return false;
-    const float4 spB = s.sph[B];
-    double rDB = (double)spB.w;
+    double rDB = (double)rB;
     rDB += (double)k.beta;
     uint32_t lo, hi;
     bin_range(xb, rDB, k.bin_size, lo, hi);
@@ -180,48 +188,54 @@ __device__ __forceinline__ bool pair_is_contact(const SimConsts& k, const StateV
     return true;
 }
 
-// Enumerate the candidates of sphere A: spheres B > A whose home cell lies in the cells A's neighbours can occupy.
-template <bool kEmit>
+// Enumerate the contacts (B > A) of sphere A among the spheres whose home cells lie where A's neighbours can live.
+// The first kSlots partners are stored in buf (dynamic indexing keeps buf in local memory, which L1 caches); the
+// return value counts all of them.
+constexpr uint32_t kSlots = 16;
+
 __device__ __forceinline__ uint32_t scan_neighbours(const SimConsts& k, const StateView& s, const CDView& cd,
-                                                    uint32_t A, uint32_t* outB, uint32_t cap_left) {
-    const float4 fA = cd.posF[A];
-    const double xa = cd.pX[A], ya = cd.pY[A], za = cd.pZ[A];
-    const uint32_t oA = s.sOwner[A];
-    const uint32_t famA = s.loc[oA].w;
-    const float4 spA = s.sph[A];
-    double rDA = (double)spA.w;
+                                                    uint32_t iA, uint32_t* buf, uint32_t buf_cap) {
+    const float4 fA = cd.posFSorted[iA];
+    const uint32_t A = __float_as_uint(fA.w);
+    const double xa = cd.pXs[iA], ya = cd.pYs[iA], za = cd.pZs[iA];
+    const uint4 mA = cd.metaS[iA];
+    const uint32_t oA = mA.x, famA = mA.z;
+    const float rA = __uint_as_float(mA.y);
+    float rfA = rA;
+    rfA += k.beta;
+    double rDA = (double)rA;
     rDA += (double)k.beta;
     uint32_t loA[3], hiA[3];
     bin_range(xa, rDA, k.bin_size, loA[0], hiA[0]);
     bin_range(ya, rDA, k.bin_size, loA[1], hiA[1]);
     bin_range(za, rDA, k.bin_size, loA[2], hiA[2]);
-    const double reach = (double)fA.w + (double)k.r_max_cd + (double)k.prefilter_abs;
+    const double reach = (double)rfA + (double)k.r_max_cd + (double)k.prefilter_abs;
     const uint32_t x0 = min(sat_u32((xa - reach) / k.cell_size), k.gx - 1);
     const uint32_t x1 = min(sat_u32((xa + reach) / k.cell_size), k.gx - 1);
     const uint32_t y0 = min(sat_u32((ya - reach) / k.cell_size), k.gy - 1);
     const uint32_t y1 = min(sat_u32((ya + reach) / k.cell_size), k.gy - 1);
     const uint32_t z0 = min(sat_u32((za - reach) / k.cell_size), k.gz - 1);
     const uint32_t z1 = min(sat_u32((za + reach) / k.cell_size), k.gz - 1);
+    // conservative float pre-filter against the largest CD radius (the exact test follows in double)
+    const float lim = (rfA + k.r_max_cd) * 1.00001f + k.prefilter_abs;
+    const float lim2 = lim * lim;
     uint32_t count = 0;
     for (uint32_t cz = z0; cz <= z1; cz++) {
         for (uint32_t cy = y0; cy <= y1; cy++) {
             const uint32_t rowBase = k.gx * (cy + k.gy * cz);
             // cells x0..x1 of one row are contiguous in the sorted order
-            const uint32_t j0 = cd.cellStart[rowBase + x0];
-            uint32_t j1 = cd.cellStart[rowBase + x1 + 1];
+            const uint32_t j0 = __ldg(cd.cellStart + rowBase + x0);
+            uint32_t j1 = __ldg(cd.cellStart + rowBase + x1 + 1);
             if (!index_ok(k.err, 2, j1, (uint64_t)k.n_spheres + 1)) j1 = j0;
+#pragma unroll 4
             for (uint32_t j = j0; j < j1; j++) {
-                const uint32_t B = cd.idSorted[j];
-                if (B <= A) continue;
-                if (!index_ok(k.err, 3, B, k.n_spheres)) continue;
-                const float4 fB = cd.posFSorted[j];
+                const float4 fB = __ldg(cd.posFSorted + j);
                 const float dx = fA.x - fB.x, dy = fA.y - fB.y, dz = fA.z - fB.z;
-                const float lim = (fA.w + fB.w) * 1.00001f + k.prefilter_abs;
-                if (dx * dx + dy * dy + dz * dz > lim * lim) continue;
-                if (!pair_is_contact(k, s, cd, A, B, oA, famA, fA.w, xa, ya, za, loA, hiA, fB.w)) continue;
-                if (kEmit) {
-                    if (count < cap_left) outB[count] = B;
-                }
+                if (dx * dx + dy * dy + dz * dz > lim2) continue;
+                const uint32_t B = __float_as_uint(fB.w);
+                if (B <= A) continue;
+                if (!pair_is_contact(k, s, cd, j, oA, famA, rfA, xa, ya, za, loA, hiA)) continue;
+                if (count < buf_cap) buf[count] = B;
                 count++;
             }
         }
@@ -229,30 +243,192 @@ __device__ __forceinline__ uint32_t scan_neighbours(const SimConsts& k, const St
     return count;
 }
 
-__global__ void __launch_bounds__(256) k_pair_count(SimConsts k, StateView s, CDView cd) {
-    const uint32_t A = blockIdx.x * blockDim.x + threadIdx.x;
-    if (A >= k.n_spheres) return;
-    const uint32_t n = scan_neighbours<false>(k, s, cd, A, nullptr, 0);
-    cd.cnt[A] = n + cd.nAnal[A];
+// One search pass, threads in cell order (a warp shares neighbour cells), in three phases per warp:
+//   1. each lane runs the cheap float pre-filter over its candidate cells and keeps the survivors' cell-order
+//      indices (a lane that fills its survivor list tests the extra ones itself);
+//   2. the warp pools all survivors in shared memory (prefix sum over lanes), so that
+//   3. all 32 lanes run the double-precision reference predicate on pooled (sphere, candidate) pairs, instead of
+//      the whole warp stepping through the expensive path whenever any one lane has a survivor.
+// Partners land in a per-lane shared list; each sphere's list then goes to the temporary partner list at a
+// warp-aggregated offset, and spheres with more than kSlots partners are queued for a re-scan.
+constexpr uint32_t kSurv = 16;
+constexpr uint32_t kFindWarps = 4;
+
+struct SphereCtx {
+    double x, y, z;
+    uint32_t lo[3], hi[3];
+    uint32_t owner, fam, A;
+    float rf;
+};
+
+__device__ __forceinline__ void load_ctx(const SimConsts& k, const CDView& cd, uint32_t iA, SphereCtx& c, float4& fA) {
+    fA = cd.posFSorted[iA];
+    c.A = __float_as_uint(fA.w);
+    c.x = cd.pXs[iA];
+    c.y = cd.pYs[iA];
+    c.z = cd.pZs[iA];
+    const uint4 mA = cd.metaS[iA];
+    c.owner = mA.x;
+    c.fam = mA.z;
+    const float rA = __uint_as_float(mA.y);
+    float rf = rA;
+    rf += k.beta;
+    c.rf = rf;
+    double rD = (double)rA;
+    rD += (double)k.beta;
+    bin_range(c.x, rD, k.bin_size, c.lo[0], c.hi[0]);
+    bin_range(c.y, rD, k.bin_size, c.lo[1], c.hi[1]);
+    bin_range(c.z, rD, k.bin_size, c.lo[2], c.hi[2]);
 }
 
-void launch_pair_count(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st) {
+__global__ void __launch_bounds__(kFindWarps * 32) k_pair_find(SimConsts k, StateView s, CDView cd, uint32_t tempCap) {
+    __shared__ uint32_t s_pre[kFindWarps][33];             // survivor prefix over lanes
+    __shared__ uint32_t s_j[kFindWarps][32 * kSurv];       // pooled survivors (cell-order index)
+    __shared__ SphereCtx s_ctx[kFindWarps][32];
+    __shared__ uint32_t s_res[kFindWarps][32][kSlots];
+    __shared__ uint32_t s_resCnt[kFindWarps][32];
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool valid = i < k.n_spheres;
+    s_resCnt[w][lane] = 0;
+    uint32_t surv[kSurv];
+    uint32_t nSurv = 0;
+    SphereCtx c;
+    c.A = 0xFFFFFFFFu;
+    if (valid) {
+        float4 fA;
+        load_ctx(k, cd, i, c, fA);
+        if (!index_ok(k.err, 12, c.A, k.n_spheres)) {
+            valid = false;
+            c.A = 0xFFFFFFFFu;
+        } else {
+            s_ctx[w][lane] = c;
+            const double reach = (double)c.rf + (double)k.r_max_cd + (double)k.prefilter_abs;
+            const uint32_t x0 = min(sat_u32((c.x - reach) / k.cell_size), k.gx - 1);
+            const uint32_t x1 = min(sat_u32((c.x + reach) / k.cell_size), k.gx - 1);
+            const uint32_t y0 = min(sat_u32((c.y - reach) / k.cell_size), k.gy - 1);
+            const uint32_t y1 = min(sat_u32((c.y + reach) / k.cell_size), k.gy - 1);
+            const uint32_t z0 = min(sat_u32((c.z - reach) / k.cell_size), k.gz - 1);
+            const uint32_t z1 = min(sat_u32((c.z + reach) / k.cell_size), k.gz - 1);
+            const float lim = (c.rf + k.r_max_cd) * 1.00001f + k.prefilter_abs;
+            const float lim2 = lim * lim;
+            for (uint32_t cz = z0; cz <= z1; cz++) {
+                for (uint32_t cy = y0; cy <= y1; cy++) {
+                    const uint32_t rowBase = k.gx * (cy + k.gy * cz);
+                    const uint32_t j0 = __ldg(cd.cellStart + rowBase + x0);
+                    uint32_t j1 = __ldg(cd.cellStart + rowBase + x1 + 1);
+                    if (!index_ok(k.err, 2, j1, (uint64_t)k.n_spheres + 1)) j1 = j0;
+                    for (uint32_t j = j0; j < j1; j++) {
+                        const float4 fB = __ldg(cd.posFSorted + j);
+                        const float dx = fA.x - fB.x, dy = fA.y - fB.y, dz = fA.z - fB.z;
+                        if (dx * dx + dy * dy + dz * dz > lim2) continue;
+                        if (__float_as_uint(fB.w) <= c.A) continue;
+                        if (nSurv < kSurv) {
+                            surv[nSurv++] = j;
+                        } else if (pair_is_contact(k, s, cd, j, c.owner, c.fam, c.rf, c.x, c.y, c.z, c.lo, c.hi)) {
+                            // survivor list full: test in place
+                            const uint32_t r = atomicAdd(&s_resCnt[w][lane], 1u);
+                            if (r < kSlots) s_res[w][lane][r] = __float_as_uint(fB.w);
+                        }
+                    }
+                }
+            }
+        }
+    }
+    // pool the survivors of the warp
+    uint32_t incl = nSurv;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= (uint32_t)off) incl += y;
+    }
+    const uint32_t totalSurv = __shfl_sync(0xffffffffu, incl, 31);
+    const uint32_t sbase = incl - nSurv;
+    s_pre[w][lane + 1] = incl;
+    if (lane == 0) s_pre[w][0] = 0;
+    for (uint32_t q = 0; q < nSurv; q++) s_j[w][sbase + q] = surv[q];
+    __syncwarp();
+    // exact reference predicate on pooled pairs, all lanes busy
+    for (uint32_t p = lane; p < totalSurv; p += 32) {
+        uint32_t L = 0;  // owning lane: last lane whose prefix is <= p
+#pragma unroll
+        for (uint32_t step = 16; step > 0; step >>= 1)
+            if (s_pre[w][L + step] <= p) L += step;
+        const uint32_t j = s_j[w][p];
+        const SphereCtx& a = s_ctx[w][L];
+        if (pair_is_contact(k, s, cd, j, a.owner, a.fam, a.rf, a.x, a.y, a.z, a.lo, a.hi)) {
+            const uint32_t r = atomicAdd(&s_resCnt[w][L], 1u);
+            if (r < kSlots) s_res[w][L][r] = __float_as_uint(cd.posFSorted[j].w);
+        }
+    }
+    __syncwarp();
+    const uint32_t n = valid ? s_resCnt[w][lane] : 0u;
+    // warp-aggregated allocation in the temporary partner list
+    uint32_t inc2 = n;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc2, off);
+        if (lane >= (uint32_t)off) inc2 += y;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, inc2, 31);
+    uint32_t base = 0;
+    if (lane == 31 && total) base = atomicAdd(&cd.counters[0], total);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    if (!valid) return;
+    const uint32_t A = c.A;
+    const uint32_t start = base + inc2 - n;
+    cd.cnt[A] = n + cd.nAnal[A];
+    cd.candStart[A] = start;
+    if (n && start + n <= tempCap) {
+        const uint32_t m = min(n, kSlots);
+        for (uint32_t t = 0; t < m; t++) cd.candTemp[start + t] = s_res[w][lane][t];
+        if (n > kSlots) {
+            const uint32_t o = atomicAdd(&cd.counters[1], 1u);
+            cd.ovf[o] = i;  // cell-order index of the sphere
+        }
+    }
+}
+
+void launch_pair_find(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st) {
     if (!(k.n_spheres)) return;
     ProfScope prof_(KID_PAIR_COUNT, st);
-    if (k.n_spheres) k_pair_count<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
+    k_pair_find<<<blocks_for(k.n_spheres, kFindWarps * 32), kFindWarps * 32, 0, st>>>(k, s, cd, tempCap);
 }
 
-__global__ void __launch_bounds__(256) k_pair_emit(SimConsts k, StateView s, CDView cd, ContactView c, uint32_t cap,
-                                                   uint32_t* err) {
+// Re-scan of the spheres with more partners than kSlots, writing the full list in place.
+__global__ void __launch_bounds__(128) k_pair_overflow(SimConsts k, StateView s, CDView cd, uint32_t nOvf,
+                                                       uint32_t tempCap) {
+    const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= nOvf) return;
+    const uint32_t iA = cd.ovf[o];
+    if (!index_ok(k.err, 13, iA, k.n_spheres)) return;
+    const uint32_t A = __float_as_uint(cd.posFSorted[iA].w);
+    const uint32_t start = cd.candStart[A];
+    const uint32_t n = cd.cnt[A] - cd.nAnal[A];
+    if (!index_ok(k.err, 14, (uint64_t)start + n, (uint64_t)tempCap + 1)) return;
+    const uint32_t got = scan_neighbours(k, s, cd, iA, cd.candTemp + start, n);
+    if (got != n) atomicOr(k.err, ERR_SEGMENT_TOO_LONG);
+}
+
+void launch_pair_overflow(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t nOvf, uint32_t tempCap,
+                          cudaStream_t st) {
+    if (!nOvf) return;
+    ProfScope prof_(KID_PAIR_COUNT, st);
+    k_pair_overflow<<<blocks_for(nOvf, 128), 128, 0, st>>>(k, s, cd, nOvf, tempCap);
+}
+
+// Writes the canonical list: per sphere A (ID order), its sphere--analytical contacts by component id
+// (populateBinSphereTouchingPairs, DEMBinSphereKernels.cu:186-228), then its sphere partners by ascending id.
+__global__ void __launch_bounds__(256) k_pair_assemble(SimConsts k, StateView s, CDView cd, ContactView c,
+                                                       uint32_t cap) {
     const uint32_t A = blockIdx.x * blockDim.x + threadIdx.x;
     if (A >= k.n_spheres) return;
     const uint32_t begin = c.off[A], end = c.off[A + 1];
     if (end > cap) {
-        atomicOr(err, ERR_CONTACT_CAPACITY);
+        atomicOr(k.err, ERR_CONTACT_CAPACITY);
         return;
     }
     uint32_t w = begin;
-    // sphere--analytical contacts first, ascending component id (populateBinSphereTouchingPairs, :186-228)
     const uint32_t nAn = cd.nAnal[A];
     if (nAn) {
         const double X = cd.pX[A], Y = cd.pY[A], Z = cd.pZ[A];
@@ -265,7 +441,6 @@ __global__ void __launch_bounds__(256) k_pair_emit(SimConsts k, StateView s, CDV
             if (s.masks[mask_index(fam, s.loc[ap.owner].w)] != 0) continue;
             const int t = anal_overlap_cd(ap, X, Y, Z, rD, k.beta);
             if (t != DEME_NOT_A_CONTACT) {
-                if (!index_ok(k.err, 4, w, cap)) break;
                 c.idA[w] = A;
                 c.idB[w] = a;
                 c.type[w] = (uint8_t)t;
@@ -273,14 +448,11 @@ __global__ void __launch_bounds__(256) k_pair_emit(SimConsts k, StateView s, CDV
             }
         }
     }
-    // sphere--sphere contacts, then sorted by idB (insertion sort of the short segment)
-    const uint32_t ssBegin = w;
-    const uint32_t n = scan_neighbours<true>(k, s, cd, A, c.idB + ssBegin, end - ssBegin);
-    if (ssBegin + n != end) atomicOr(err, ERR_SEGMENT_TOO_LONG);
-    const uint32_t m = min(n, end - ssBegin);
-    uint32_t* seg = c.idB + ssBegin;
-    for (uint32_t i = 1; i < m; i++) {
-        const uint32_t v = seg[i];
+    const uint32_t n = end - w;
+    const uint32_t* src = cd.candTemp + cd.candStart[A];
+    uint32_t* seg = c.idB + w;
+    for (uint32_t i = 0; i < n; i++) {
+        const uint32_t v = src[i];
         uint32_t j = i;
         while (j > 0 && seg[j - 1] > v) {
             seg[j] = seg[j - 1];
@@ -288,17 +460,17 @@ __global__ void __launch_bounds__(256) k_pair_emit(SimConsts k, StateView s, CDV
         }
         seg[j] = v;
     }
-    for (uint32_t i = 0; i < m; i++) {
-        c.idA[ssBegin + i] = A;
-        c.type[ssBegin + i] = DEME_SPHERE_SPHERE_CONTACT;
+    for (uint32_t i = 0; i < n; i++) {
+        c.idA[w + i] = A;
+        c.type[w + i] = DEME_SPHERE_SPHERE_CONTACT;
     }
 }
 
-void launch_pair_emit(const SimConsts& k, const StateView& s, const CDView& cd, const ContactView& c, uint32_t cap,
-                      uint32_t* err, cudaStream_t st) {
+void launch_pair_assemble(const SimConsts& k, const StateView& s, const CDView& cd, const ContactView& c, uint32_t cap,
+                          cudaStream_t st) {
     if (!(k.n_spheres)) return;
     ProfScope prof_(KID_PAIR_EMIT, st);
-    if (k.n_spheres) k_pair_emit<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd, c, cap, err);
+    k_pair_assemble<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd, c, cap);
 }
 
 // ------------------------------------------------------------------------------------------------------------

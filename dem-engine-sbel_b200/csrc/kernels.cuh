@@ -42,7 +42,11 @@ struct CDView {
     double* pY;
     double* pZ;
     float4* posF;        // ID order: (x, y, z, CD radius)
-    float4* posFSorted;  // cell order
+    float4* posFSorted;  // cell order: (x, y, z, sphere id bits)
+    double* pXs;         // cell order: exact position
+    double* pYs;
+    double* pZs;
+    uint4* metaS;        // cell order: (owner, radius bits, family, 0)
     uint32_t* cellKey;
     uint32_t* idSeq;
     uint32_t* keySorted;
@@ -51,6 +55,10 @@ struct CDView {
     uint32_t* cellStart;  // nCells + 1
     uint8_t* nAnal;
     uint32_t* cnt;
+    uint32_t* candStart;  // per sphere: first partner in candTemp
+    uint32_t* candTemp;   // partners of all spheres, one run per sphere
+    uint32_t* ovf;        // spheres with more partners than the search keeps in registers
+    uint32_t* counters;   // [0] partners appended, [1] overflow spheres
 };
 
 // One contact list (kT product) with its history wildcards.
@@ -80,10 +88,12 @@ struct ContactOutputs {
 void launch_place_anal(const SimConsts& k, const StateView& s, const AnalRaw* raw, AnalPlaced* placed, uint32_t nA,
                        cudaStream_t st);
 void launch_sphere_prep(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
-void launch_gather_sorted(const SimConsts& k, const CDView& cd, cudaStream_t st);
-void launch_pair_count(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
-void launch_pair_emit(const SimConsts& k, const StateView& s, const CDView& cd, const ContactView& c, uint32_t cap,
-                      uint32_t* err, cudaStream_t st);
+void launch_gather_sorted(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
+void launch_pair_find(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st);
+void launch_pair_overflow(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t nOvf, uint32_t tempCap,
+                          cudaStream_t st);
+void launch_pair_assemble(const SimConsts& k, const StateView& s, const CDView& cd, const ContactView& c, uint32_t cap,
+                          cudaStream_t st);
 void launch_history(const SimConsts& k, const ContactView& cur, const ContactView& prev, uint32_t n, uint32_t prevN,
                     bool has_hist, cudaStream_t st);
 void launch_count_by_sphere(const uint32_t* idA, uint32_t n, uint32_t* cnt, cudaStream_t st);
