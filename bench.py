@@ -188,7 +188,12 @@ def main():
                     help="untimed preparation: steps at --settle-dt that let the loose lattice fall into a bed")
     ap.add_argument("--settle-dt", type=float, default=2e-5)
     ap.add_argument("--calm-steps", type=int, default=1000, help="untimed steps at the workload's dt after settling")
+    ap.add_argument("--save-state", default=None, help="write the prepared state and contact history to this .npz")
+    ap.add_argument("--load-state", default=None, help="start from a state written by --save-state (no settling)")
     args = ap.parse_args()
+    if args.load_state:
+        args.settle_steps = 0
+        args.calm_steps = 0
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -225,6 +230,11 @@ def main():
     # ---- scene preparation (untimed): let the loose lattice settle into a bed ----
     t_prep = time.perf_counter()
     dt_work = float(built.params.h)
+    if args.load_state:
+        import numpy as np
+        z = np.load(args.load_state)
+        s.set_state({k[3:]: z[k] for k in z.files if k.startswith("st_")})
+        s.set_contacts({k[2:]: z[k] for k in z.files if k.startswith("c_")})
     if args.settle_steps > 0:
         s.set_time_step(args.settle_dt)
         done = 0
@@ -241,6 +251,12 @@ def main():
         s.step(args.calm_steps)
     s.sync()
     prep_s = time.perf_counter() - t_prep
+    if args.save_state and rank == 0:
+        import numpy as np
+        st = s.state()
+        c = s.contacts()
+        np.savez(args.save_state, **{"st_" + k: v for k, v in st.items() if not k.startswith("a")},
+                 **{"c_" + k: c[k] for k in ("idA", "idB", "type", "wildcards")})
 
     # ---- warm-up (the clock sampler starts here so it has samples when the timed region is short) ----
     sampler = ClockSampler(local_rank)

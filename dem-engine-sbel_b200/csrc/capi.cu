@@ -275,6 +275,10 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
         h->err = "the built-in models use 0 or 4 contact wildcards";
         return DEME_ERR_INVALID;
     }
+    if (p->nbX > 65535u || p->nbY > 65535u || p->nbZ > 65535u) {
+        h->err = "more than 65535 bins along an axis: enlarge the bin size";
+        return DEME_ERR_INVALID;
+    }
     if ((int)p->nvXp2 + (int)p->nvYp2 + (int)p->nvZp2 > 64) {
         h->err = "voxel bits nvXp2 + nvYp2 + nvZp2 exceed 64: voxel ids would wrap";
         return DEME_ERR_INVALID;
@@ -465,6 +469,7 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
     TRY(dalloc_n(h, &cd.pYs, nS));
     TRY(dalloc_n(h, &cd.pZs, nS));
     TRY(dalloc_n(h, &cd.metaS, nS));
+    TRY(dalloc_n(h, &cd.rngS, nS));
     TRY(dalloc_n(h, &cd.cellKey, nS));
     TRY(dalloc_n(h, &cd.idSeq, nS));
     TRY(dalloc_n(h, &cd.keySorted, nS));
@@ -563,22 +568,21 @@ int32_t deme_detect_contacts(deme_handle* h) {
     const int nxt = h->cur ^ 1;
     ContactBuf& nb = h->lists[nxt];
     ContactBuf& pb = h->lists[h->cur];
-    uint32_t n = 0, nOvf = 0;
+    uint32_t n = 0;
     for (int attempt = 0; attempt < 2; attempt++) {
         CUDA_TRY(h, cudaMemsetAsync(cd.counters, 0, 2 * sizeof(uint32_t), st));
         launch_pair_find(k, s, cd, h->candCap, st);
+        launch_pair_overflow(k, s, cd, h->candCap, st);
         TRY(check_launch(h, "contact search"));
         exclusive_scan_u32(cd.cnt, h->nS + 1, nb.off, h->dTotal, h->scratch, st);
         CUDA_TRY(h, cudaMemcpyAsync(h->hTotal + 1, cd.counters, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         CUDA_TRY(h, cudaMemcpyAsync(h->hTotal, h->dTotal, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         CUDA_TRY(h, cudaStreamSynchronize(st));
         n = h->hTotal[0];
-        nOvf = h->hTotal[2];
         if (h->hTotal[1] <= h->candCap) break;
         // the partner list outgrew its buffer: grow and search again
         TRY(ensure_cand(h, h->hTotal[1]));
     }
-    launch_pair_overflow(k, s, cd, nOvf, h->candCap, st);
     TRY(ensure_list(h, nb, n));
     launch_pair_assemble(k, s, cd, nb.view(), nb.cap, st);
     launch_history(k, nb.view(), pb.view(), n, h->nContacts, h->nW > 0, st);

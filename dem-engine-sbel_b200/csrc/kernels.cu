@@ -129,6 +129,14 @@ void launch_sphere_prep(const SimConsts& k, const StateView& s, const CDView& cd
     if (k.n_spheres) k_sphere_prep<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
 }
 
+__device__ __forceinline__ uint4 pack_ranges(const uint32_t lo[3], const uint32_t hi[3]) {
+    return make_uint4(min(lo[0], 65535u) | (min(hi[0], 65535u) << 16), min(lo[1], 65535u) | (min(hi[1], 65535u) << 16),
+                      min(lo[2], 65535u) | (min(hi[2], 65535u) << 16), 0u);
+}
+__device__ __forceinline__ bool in_range(uint32_t b, uint32_t packed) {
+    return b >= (packed & 0xFFFFu) && b <= (packed >> 16);
+}
+
 // Cell-order copies of everything the contact search reads, so that a warp (neighbouring cells) reads contiguous
 // memory: position + id for the pre-filter, exact position and (owner, radius, family) for the exact test.
 __global__ void k_gather_sorted(SimConsts k, StateView s, CDView cd) {
@@ -142,7 +150,16 @@ __global__ void k_gather_sorted(SimConsts k, StateView s, CDView cd) {
     cd.pYs[i] = cd.pY[j];
     cd.pZs[i] = cd.pZ[j];
     const uint32_t o = s.sOwner[j];
-    cd.metaS[i] = make_uint4(o, __float_as_uint(s.sph[j].w), s.loc[o].w, 0u);
+    const float r = s.sph[j].w;
+    cd.metaS[i] = make_uint4(o, __float_as_uint(r), s.loc[o].w, 0u);
+    // bin ranges of the expanded sphere (reference arithmetic), packed 16 bits per bound
+    double rD = (double)r;
+    rD += (double)k.beta;
+    uint32_t lo[3], hi[3];
+    bin_range(cd.pX[j], rD, k.bin_size, lo[0], hi[0]);
+    bin_range(cd.pY[j], rD, k.bin_size, lo[1], hi[1]);
+    bin_range(cd.pZ[j], rD, k.bin_size, lo[2], hi[2]);
+    cd.rngS[i] = pack_ranges(lo, hi);
 }
 
 void launch_gather_sorted(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st) {
@@ -151,16 +168,16 @@ void launch_gather_sorted(const SimConsts& k, const StateView& s, const CDView& 
     k_gather_sorted<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
 }
 
-// The reference's pair predicate for A < B (see the file comment), B given by its cell-order index j.
+// The reference's pair predicate for A < B (see the file comment), B given by its cell-order index j; rngA holds
+// A's packed bin ranges.
 __device__ __forceinline__ bool pair_is_contact(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t j,
                                                 uint32_t oA, uint32_t famA, float rfA, double xa, double ya, double za,
-                                                const uint32_t loA[3], const uint32_t hiA[3]) {
+                                                uint4 rngA) {
     const uint4 mB = cd.metaS[j];
     const uint32_t oB = mB.x;
     if (oA == oB) return false;
     if (s.masks[mask_index(famA, mB.z)] != 0) return false;
-    const float rB = __uint_as_float(mB.y);
-    float rfB = rB;
+    float rfB = __uint_as_float(mB.y);
     rfB += k.beta;
     const double xb = cd.pXs[j], yb = cd.pYs[j], zb = cd.pZs[j];
     // checkSpheresOverlap<double>, DEMHelperKernels.cu:195-222
@@ -175,17 +192,9 @@ __device__ __forceinline__ bool pair_is_contact(const SimConsts& k, const StateV
     const double cpz = zb + (radB - half) * (double)nz;
     // getPointBinID, DEMHelperKernels.cu:266-273, tested per axis against both spheres' bin ranges
     const uint32_t bx = sat_u32(cpx / k.bin_size), by = sat_u32(cpy / k.bin_size), bz = sat_u32(cpz / k.bin_size);
-    if (bx < loA[0] || bx > hiA[0] || by < loA[1] || by > hiA[1] || bz < loA[2] || bz > hiA[2]) return false;
-    double rDB = (double)rB;
-    rDB += (double)k.beta;
-    uint32_t lo, hi;
-    bin_range(xb, rDB, k.bin_size, lo, hi);
-    if (bx < lo || bx > hi) return false;
-    bin_range(yb, rDB, k.bin_size, lo, hi);
-    if (by < lo || by > hi) return false;
-    bin_range(zb, rDB, k.bin_size, lo, hi);
-    if (bz < lo || bz > hi) return false;
-    return true;
+    if (!in_range(bx, rngA.x) || !in_range(by, rngA.y) || !in_range(bz, rngA.z)) return false;
+    const uint4 rngB = cd.rngS[j];
+    return in_range(bx, rngB.x) && in_range(by, rngB.y) && in_range(bz, rngB.z);
 }
 
 // Enumerate the contacts (B > A) of sphere A among the spheres whose home cells lie where A's neighbours can live.
@@ -194,21 +203,14 @@ __device__ __forceinline__ bool pair_is_contact(const SimConsts& k, const StateV
 constexpr uint32_t kSlots = 16;
 
 __device__ __forceinline__ uint32_t scan_neighbours(const SimConsts& k, const StateView& s, const CDView& cd,
-                                                    uint32_t iA, uint32_t* buf, uint32_t buf_cap) {
+                                                    uint32_t iA, uint32_t* out, uint32_t out_cap) {
     const float4 fA = cd.posFSorted[iA];
     const uint32_t A = __float_as_uint(fA.w);
     const double xa = cd.pXs[iA], ya = cd.pYs[iA], za = cd.pZs[iA];
     const uint4 mA = cd.metaS[iA];
-    const uint32_t oA = mA.x, famA = mA.z;
-    const float rA = __uint_as_float(mA.y);
-    float rfA = rA;
+    float rfA = __uint_as_float(mA.y);
     rfA += k.beta;
-    double rDA = (double)rA;
-    rDA += (double)k.beta;
-    uint32_t loA[3], hiA[3];
-    bin_range(xa, rDA, k.bin_size, loA[0], hiA[0]);
-    bin_range(ya, rDA, k.bin_size, loA[1], hiA[1]);
-    bin_range(za, rDA, k.bin_size, loA[2], hiA[2]);
+    const uint4 rngA = cd.rngS[iA];
     const double reach = (double)rfA + (double)k.r_max_cd + (double)k.prefilter_abs;
     const uint32_t x0 = min(sat_u32((xa - reach) / k.cell_size), k.gx - 1);
     const uint32_t x1 = min(sat_u32((xa + reach) / k.cell_size), k.gx - 1);
@@ -216,26 +218,23 @@ __device__ __forceinline__ uint32_t scan_neighbours(const SimConsts& k, const St
     const uint32_t y1 = min(sat_u32((ya + reach) / k.cell_size), k.gy - 1);
     const uint32_t z0 = min(sat_u32((za - reach) / k.cell_size), k.gz - 1);
     const uint32_t z1 = min(sat_u32((za + reach) / k.cell_size), k.gz - 1);
-    // conservative float pre-filter against the largest CD radius (the exact test follows in double)
     const float lim = (rfA + k.r_max_cd) * 1.00001f + k.prefilter_abs;
     const float lim2 = lim * lim;
     uint32_t count = 0;
     for (uint32_t cz = z0; cz <= z1; cz++) {
         for (uint32_t cy = y0; cy <= y1; cy++) {
             const uint32_t rowBase = k.gx * (cy + k.gy * cz);
-            // cells x0..x1 of one row are contiguous in the sorted order
-            const uint32_t j0 = __ldg(cd.cellStart + rowBase + x0);
-            uint32_t j1 = __ldg(cd.cellStart + rowBase + x1 + 1);
+            const uint32_t j0 = cd.cellStart[rowBase + x0];
+            uint32_t j1 = cd.cellStart[rowBase + x1 + 1];
             if (!index_ok(k.err, 2, j1, (uint64_t)k.n_spheres + 1)) j1 = j0;
-#pragma unroll 4
             for (uint32_t j = j0; j < j1; j++) {
-                const float4 fB = __ldg(cd.posFSorted + j);
+                const float4 fB = cd.posFSorted[j];
                 const float dx = fA.x - fB.x, dy = fA.y - fB.y, dz = fA.z - fB.z;
                 if (dx * dx + dy * dy + dz * dz > lim2) continue;
                 const uint32_t B = __float_as_uint(fB.w);
                 if (B <= A) continue;
-                if (!pair_is_contact(k, s, cd, j, oA, famA, rfA, xa, ya, za, loA, hiA)) continue;
-                if (count < buf_cap) buf[count] = B;
+                if (!pair_is_contact(k, s, cd, j, mA.x, mA.z, rfA, xa, ya, za, rngA)) continue;
+                if (count < out_cap) out[count] = B;
                 count++;
             }
         }
@@ -256,32 +255,13 @@ constexpr uint32_t kFindWarps = 4;
 
 struct SphereCtx {
     double x, y, z;
-    uint32_t lo[3], hi[3];
+    uint4 rng;
     uint32_t owner, fam, A;
     float rf;
 };
 
-__device__ __forceinline__ void load_ctx(const SimConsts& k, const CDView& cd, uint32_t iA, SphereCtx& c, float4& fA) {
-    fA = cd.posFSorted[iA];
-    c.A = __float_as_uint(fA.w);
-    c.x = cd.pXs[iA];
-    c.y = cd.pYs[iA];
-    c.z = cd.pZs[iA];
-    const uint4 mA = cd.metaS[iA];
-    c.owner = mA.x;
-    c.fam = mA.z;
-    const float rA = __uint_as_float(mA.y);
-    float rf = rA;
-    rf += k.beta;
-    c.rf = rf;
-    double rD = (double)rA;
-    rD += (double)k.beta;
-    bin_range(c.x, rD, k.bin_size, c.lo[0], c.hi[0]);
-    bin_range(c.y, rD, k.bin_size, c.lo[1], c.hi[1]);
-    bin_range(c.z, rD, k.bin_size, c.lo[2], c.hi[2]);
-}
-
-__global__ void __launch_bounds__(kFindWarps * 32) k_pair_find(SimConsts k, StateView s, CDView cd, uint32_t tempCap) {
+__global__ void __launch_bounds__(kFindWarps * 32, 8) k_pair_find(SimConsts k, StateView s, CDView cd,
+                                                                  uint32_t tempCap) {
     __shared__ uint32_t s_pre[kFindWarps][33];             // survivor prefix over lanes
     __shared__ uint32_t s_j[kFindWarps][32 * kSurv];       // pooled survivors (cell-order index)
     __shared__ SphereCtx s_ctx[kFindWarps][32];
@@ -293,24 +273,34 @@ __global__ void __launch_bounds__(kFindWarps * 32) k_pair_find(SimConsts k, Stat
     s_resCnt[w][lane] = 0;
     uint32_t surv[kSurv];
     uint32_t nSurv = 0;
-    SphereCtx c;
-    c.A = 0xFFFFFFFFu;
+    uint32_t A = 0xFFFFFFFFu;
     if (valid) {
-        float4 fA;
-        load_ctx(k, cd, i, c, fA);
-        if (!index_ok(k.err, 12, c.A, k.n_spheres)) {
+        const float4 fA = cd.posFSorted[i];
+        A = __float_as_uint(fA.w);
+        if (!index_ok(k.err, 12, A, k.n_spheres)) {
             valid = false;
-            c.A = 0xFFFFFFFFu;
         } else {
+            SphereCtx c;
+            c.A = A;
+            c.x = cd.pXs[i];
+            c.y = cd.pYs[i];
+            c.z = cd.pZs[i];
+            const uint4 mA = cd.metaS[i];
+            c.owner = mA.x;
+            c.fam = mA.z;
+            float rf = __uint_as_float(mA.y);
+            rf += k.beta;
+            c.rf = rf;
+            c.rng = cd.rngS[i];
             s_ctx[w][lane] = c;
-            const double reach = (double)c.rf + (double)k.r_max_cd + (double)k.prefilter_abs;
+            const double reach = (double)rf + (double)k.r_max_cd + (double)k.prefilter_abs;
             const uint32_t x0 = min(sat_u32((c.x - reach) / k.cell_size), k.gx - 1);
             const uint32_t x1 = min(sat_u32((c.x + reach) / k.cell_size), k.gx - 1);
             const uint32_t y0 = min(sat_u32((c.y - reach) / k.cell_size), k.gy - 1);
             const uint32_t y1 = min(sat_u32((c.y + reach) / k.cell_size), k.gy - 1);
             const uint32_t z0 = min(sat_u32((c.z - reach) / k.cell_size), k.gz - 1);
             const uint32_t z1 = min(sat_u32((c.z + reach) / k.cell_size), k.gz - 1);
-            const float lim = (c.rf + k.r_max_cd) * 1.00001f + k.prefilter_abs;
+            const float lim = (rf + k.r_max_cd) * 1.00001f + k.prefilter_abs;
             const float lim2 = lim * lim;
             for (uint32_t cz = z0; cz <= z1; cz++) {
                 for (uint32_t cy = y0; cy <= y1; cy++) {
@@ -321,32 +311,30 @@ __global__ void __launch_bounds__(kFindWarps * 32) k_pair_find(SimConsts k, Stat
                     for (uint32_t j = j0; j < j1; j++) {
                         const float4 fB = __ldg(cd.posFSorted + j);
                         const float dx = fA.x - fB.x, dy = fA.y - fB.y, dz = fA.z - fB.z;
-                        if (dx * dx + dy * dy + dz * dz > lim2) continue;
-                        if (__float_as_uint(fB.w) <= c.A) continue;
-                        if (nSurv < kSurv) {
-                            surv[nSurv++] = j;
-                        } else if (pair_is_contact(k, s, cd, j, c.owner, c.fam, c.rf, c.x, c.y, c.z, c.lo, c.hi)) {
-                            // survivor list full: test in place
-                            const uint32_t r = atomicAdd(&s_resCnt[w][lane], 1u);
-                            if (r < kSlots) s_res[w][lane][r] = __float_as_uint(fB.w);
+                        const bool keep = (dx * dx + dy * dy + dz * dz <= lim2) & (__float_as_uint(fB.w) > A);
+                        if (keep) {
+                            if (nSurv < kSurv) surv[nSurv] = j;
+                            nSurv++;
                         }
                     }
                 }
             }
         }
     }
-    // pool the survivors of the warp
-    uint32_t incl = nSurv;
+    // a lane with more survivors than it can pool is re-scanned by k_pair_overflow
+    const bool ovf = valid && nSurv > kSurv;
+    const uint32_t pool = (valid && !ovf) ? nSurv : 0u;
+    uint32_t incl = pool;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
         const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
         if (lane >= (uint32_t)off) incl += y;
     }
     const uint32_t totalSurv = __shfl_sync(0xffffffffu, incl, 31);
-    const uint32_t sbase = incl - nSurv;
+    const uint32_t sbase = incl - pool;
     s_pre[w][lane + 1] = incl;
     if (lane == 0) s_pre[w][0] = 0;
-    for (uint32_t q = 0; q < nSurv; q++) s_j[w][sbase + q] = surv[q];
+    for (uint32_t q = 0; q < pool; q++) s_j[w][sbase + q] = surv[q];
     __syncwarp();
     // exact reference predicate on pooled pairs, all lanes busy
     for (uint32_t p = lane; p < totalSurv; p += 32) {
@@ -356,13 +344,14 @@ __global__ void __launch_bounds__(kFindWarps * 32) k_pair_find(SimConsts k, Stat
             if (s_pre[w][L + step] <= p) L += step;
         const uint32_t j = s_j[w][p];
         const SphereCtx& a = s_ctx[w][L];
-        if (pair_is_contact(k, s, cd, j, a.owner, a.fam, a.rf, a.x, a.y, a.z, a.lo, a.hi)) {
+        if (pair_is_contact(k, s, cd, j, a.owner, a.fam, a.rf, a.x, a.y, a.z, a.rng)) {
             const uint32_t r = atomicAdd(&s_resCnt[w][L], 1u);
-            if (r < kSlots) s_res[w][L][r] = __float_as_uint(cd.posFSorted[j].w);
+            if (r < kSlots) s_res[w][L][r] = __float_as_uint(__ldg(cd.posFSorted + j).w);
         }
     }
     __syncwarp();
-    const uint32_t n = valid ? s_resCnt[w][lane] : 0u;
+    const bool ovf2 = ovf || (valid && s_resCnt[w][lane] > kSlots);
+    const uint32_t n = (valid && !ovf2) ? s_resCnt[w][lane] : 0u;
     // warp-aggregated allocation in the temporary partner list
     uint32_t inc2 = n;
 #pragma unroll
@@ -375,18 +364,16 @@ __global__ void __launch_bounds__(kFindWarps * 32) k_pair_find(SimConsts k, Stat
     if (lane == 31 && total) base = atomicAdd(&cd.counters[0], total);
     base = __shfl_sync(0xffffffffu, base, 31);
     if (!valid) return;
-    const uint32_t A = c.A;
+    if (ovf2) {
+        const uint32_t o = atomicAdd(&cd.counters[1], 1u);
+        cd.ovf[o] = i;  // cell-order index; k_pair_overflow writes cnt and the list
+        return;
+    }
     const uint32_t start = base + inc2 - n;
     cd.cnt[A] = n + cd.nAnal[A];
     cd.candStart[A] = start;
-    if (n && start + n <= tempCap) {
-        const uint32_t m = min(n, kSlots);
-        for (uint32_t t = 0; t < m; t++) cd.candTemp[start + t] = s_res[w][lane][t];
-        if (n > kSlots) {
-            const uint32_t o = atomicAdd(&cd.counters[1], 1u);
-            cd.ovf[o] = i;  // cell-order index of the sphere
-        }
-    }
+    if (start + n <= tempCap)
+        for (uint32_t t = 0; t < n; t++) cd.candTemp[start + t] = s_res[w][lane][t];
 }
 
 void launch_pair_find(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st) {
@@ -395,26 +382,29 @@ void launch_pair_find(const SimConsts& k, const StateView& s, const CDView& cd, 
     k_pair_find<<<blocks_for(k.n_spheres, kFindWarps * 32), kFindWarps * 32, 0, st>>>(k, s, cd, tempCap);
 }
 
-// Re-scan of the spheres with more partners than kSlots, writing the full list in place.
-__global__ void __launch_bounds__(128) k_pair_overflow(SimConsts k, StateView s, CDView cd, uint32_t nOvf,
-                                                       uint32_t tempCap) {
-    const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= nOvf) return;
-    const uint32_t iA = cd.ovf[o];
-    if (!index_ok(k.err, 13, iA, k.n_spheres)) return;
-    const uint32_t A = __float_as_uint(cd.posFSorted[iA].w);
-    const uint32_t start = cd.candStart[A];
-    const uint32_t n = cd.cnt[A] - cd.nAnal[A];
-    if (!index_ok(k.err, 14, (uint64_t)start + n, (uint64_t)tempCap + 1)) return;
-    const uint32_t got = scan_neighbours(k, s, cd, iA, cd.candTemp + start, n);
-    if (got != n) atomicOr(k.err, ERR_SEGMENT_TOO_LONG);
+// Spheres the pooled search could not hold: full per-thread search, counted first, then written to a freshly
+// allocated run of the temporary list.  Grid-stride over the device-side overflow count (no host round trip).
+__global__ void __launch_bounds__(128) k_pair_overflow(SimConsts k, StateView s, CDView cd, uint32_t tempCap) {
+    const uint32_t nOvf = *((volatile uint32_t*)&cd.counters[1]);
+    for (uint32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < nOvf; o += gridDim.x * blockDim.x) {
+        const uint32_t iA = cd.ovf[o];
+        if (!index_ok(k.err, 13, iA, k.n_spheres)) continue;
+        const uint32_t A = __float_as_uint(cd.posFSorted[iA].w);
+        const uint32_t n = scan_neighbours(k, s, cd, iA, nullptr, 0);
+        const uint32_t start = atomicAdd(&cd.counters[0], n);
+        cd.cnt[A] = n + cd.nAnal[A];
+        cd.candStart[A] = start;
+        if ((uint64_t)start + n <= tempCap) {
+            const uint32_t got = scan_neighbours(k, s, cd, iA, cd.candTemp + start, n);
+            if (got != n) atomicOr(k.err, ERR_SEGMENT_TOO_LONG);
+        }
+    }
 }
 
-void launch_pair_overflow(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t nOvf, uint32_t tempCap,
-                          cudaStream_t st) {
-    if (!nOvf) return;
+void launch_pair_overflow(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st) {
+    if (!(k.n_spheres)) return;
     ProfScope prof_(KID_PAIR_COUNT, st);
-    k_pair_overflow<<<blocks_for(nOvf, 128), 128, 0, st>>>(k, s, cd, nOvf, tempCap);
+    k_pair_overflow<<<148, 128, 0, st>>>(k, s, cd, tempCap);
 }
 
 // Writes the canonical list: per sphere A (ID order), its sphere--analytical contacts by component id
@@ -529,7 +519,7 @@ void launch_count_by_sphere(const uint32_t* idA, uint32_t n, uint32_t* cnt, cuda
 // ------------------------------------------------------------------------------------------------------------
 // Fused force + collection kernel.
 template <bool kStore>
-__global__ void __launch_bounds__(256) k_force(SimConsts k, StateView s, ContactView c, uint32_t n, bool has_hist,
+__global__ void __launch_bounds__(256, 3) k_force(SimConsts k, StateView s, ContactView c, uint32_t n, bool has_hist,
                                                ContactOutputs out, AnalAccum aa) {
     // analytical owners (walls) collect their reactions block-locally, then one fixed-order reduction
     extern __shared__ float s_anal[];  // 6 floats per analytical owner

@@ -47,6 +47,7 @@ struct CDView {
     double* pYs;
     double* pZs;
     uint4* metaS;        // cell order: (owner, radius bits, family, 0)
+    uint4* rngS;         // cell order: bin ranges of the expanded sphere, (lo | hi << 16) per axis
     uint32_t* cellKey;
     uint32_t* idSeq;
     uint32_t* keySorted;
@@ -90,8 +91,7 @@ void launch_place_anal(const SimConsts& k, const StateView& s, const AnalRaw* ra
 void launch_sphere_prep(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
 void launch_gather_sorted(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
 void launch_pair_find(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st);
-void launch_pair_overflow(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t nOvf, uint32_t tempCap,
-                          cudaStream_t st);
+void launch_pair_overflow(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st);
 void launch_pair_assemble(const SimConsts& k, const StateView& s, const CDView& cd, const ContactView& c, uint32_t cap,
                           cudaStream_t st);
 void launch_history(const SimConsts& k, const ContactView& cur, const ContactView& prev, uint32_t n, uint32_t prevN,
