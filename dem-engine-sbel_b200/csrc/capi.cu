@@ -71,6 +71,7 @@ struct deme_handle {
     uint32_t nContacts = 0;
     // per-contact outputs
     bool keepOutputs = false;
+    bool useOnesweep = false;  // sort spheres by cell with the multi-pass onesweep instead of the counting sort
     uint32_t outCap = 0;
     ContactOutputs outs{nullptr, nullptr, nullptr, nullptr};
     bool outsValid = false;
@@ -546,6 +547,12 @@ int32_t deme_set_streams(deme_handle* h, void* kT_stream, void* dT_stream) {
     return DEME_OK;
 }
 
+int32_t deme_set_cell_sort(deme_handle* h, int32_t onesweep) {
+    if (!h) return DEME_ERR_INVALID;
+    h->useOnesweep = onesweep != 0;
+    return DEME_OK;
+}
+
 int32_t deme_keep_contact_forces(deme_handle* h, int32_t enable) {
     if (!h) return DEME_ERR_INVALID;
     h->keepOutputs = enable != 0;
@@ -563,7 +570,10 @@ int32_t deme_detect_contacts(deme_handle* h) {
     CUDA_TRY(h, cudaMemsetAsync(cd.cellCount, 0, ((size_t)h->nCells + 1) * sizeof(uint32_t), st));
     launch_sphere_prep(k, s, cd, st);
     exclusive_scan_u32(cd.cellCount, h->nCells + 1, cd.cellStart, nullptr, h->scratch, st);
-    radix_sort_pairs(cd.cellKey, cd.idSeq, cd.keySorted, cd.idSorted, h->nS, h->cellBits, h->scratch, h->dErr, st);
+    if (h->useOnesweep)
+        radix_sort_pairs(cd.cellKey, cd.idSeq, cd.keySorted, cd.idSorted, h->nS, h->cellBits, h->scratch, h->dErr, st);
+    else
+        launch_cell_scatter(k, cd, st);
     launch_gather_sorted(k, s, cd, st);
     const int nxt = h->cur ^ 1;
     ContactBuf& nb = h->lists[nxt];

@@ -162,6 +162,26 @@ __global__ void k_gather_sorted(SimConsts k, StateView s, CDView cd) {
     cd.rngS[i] = pack_ranges(lo, hi);
 }
 
+// Counting sort of the spheres by home cell (a radix sort whose single digit spans the cell range): the histogram
+// was taken in k_sphere_prep and scanned into cellStart; each sphere takes a slot of its cell by decrementing the
+// cell's count.  The order inside a cell is not defined, which the search does not depend on (partner lists are
+// sorted when the contact list is assembled).
+__global__ void k_cell_scatter(uint32_t n, const uint32_t* __restrict__ cellKey, const uint32_t* __restrict__ cellStart,
+                               uint32_t* cellCount, uint32_t* idSorted) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const uint32_t key = cellKey[s];
+    const uint32_t slot = cellStart[key] + atomicSub(&cellCount[key], 1u) - 1u;
+    idSorted[slot] = s;
+}
+
+void launch_cell_scatter(const SimConsts& k, const CDView& cd, cudaStream_t st) {
+    if (!(k.n_spheres)) return;
+    ProfScope prof_(KID_CELL_SCATTER, st);
+    k_cell_scatter<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k.n_spheres, cd.cellKey, cd.cellStart, cd.cellCount,
+                                                                  cd.idSorted);
+}
+
 void launch_gather_sorted(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st) {
     if (!(k.n_spheres)) return;
     ProfScope prof_(KID_GATHER, st);
@@ -403,7 +423,7 @@ __global__ void __launch_bounds__(128) k_pair_overflow(SimConsts k, StateView s,
 
 void launch_pair_overflow(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st) {
     if (!(k.n_spheres)) return;
-    ProfScope prof_(KID_PAIR_COUNT, st);
+    ProfScope prof_(KID_PAIR_OVERFLOW, st);
     k_pair_overflow<<<148, 128, 0, st>>>(k, s, cd, tempCap);
 }
 

@@ -49,16 +49,46 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s
     return warp_prefix + x - v;
 }
 
+// Loads kScanItems consecutive values of one thread; full u32 tiles use 16-byte vector loads.
+template <typename T>
+__device__ __forceinline__ void load_items(const T* in, uint32_t n, size_t base, uint32_t (&v)[kScanItems]) {
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+        size_t idx = base + i;
+        v[i] = idx < n ? (uint32_t)in[idx] : 0u;
+    }
+}
+template <>
+__device__ __forceinline__ void load_items<uint32_t>(const uint32_t* in, uint32_t n, size_t base,
+                                                     uint32_t (&v)[kScanItems]) {
+    if (base + kScanItems <= n && ((reinterpret_cast<uintptr_t>(in + base) & 15u) == 0)) {
+        const uint4* p = reinterpret_cast<const uint4*>(in + base);
+#pragma unroll
+        for (int q = 0; q < kScanItems / 4; q++) {
+            const uint4 t = __ldg(p + q);
+            v[4 * q] = t.x;
+            v[4 * q + 1] = t.y;
+            v[4 * q + 2] = t.z;
+            v[4 * q + 3] = t.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < kScanItems; i++) {
+            size_t idx = base + i;
+            v[i] = idx < n ? in[idx] : 0u;
+        }
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kScanThreads) scan_reduce_kernel(const T* in, uint32_t n, uint32_t* block_sums) {
     __shared__ uint32_t sh[kScanThreads / 32];
     const size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    load_items<T>(in, n, base, v);
     uint32_t s = 0;
 #pragma unroll
-    for (int i = 0; i < kScanItems; i++) {
-        size_t idx = base + i;
-        if (idx < n) s += (uint32_t)in[idx];
-    }
+    for (int i = 0; i < kScanItems; i++) s += v[i];
     uint32_t total;
     block_exclusive_scan<T>(s, sh, total);
     if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
@@ -70,20 +100,34 @@ __global__ void __launch_bounds__(kScanThreads) scan_down_kernel(const T* in, ui
     __shared__ uint32_t sh[kScanThreads / 32];
     const size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
+    load_items<T>(in, n, base, v);
     uint32_t s = 0;
 #pragma unroll
-    for (int i = 0; i < kScanItems; i++) {
-        size_t idx = base + i;
-        v[i] = idx < n ? (uint32_t)in[idx] : 0u;
-        s += v[i];
-    }
+    for (int i = 0; i < kScanItems; i++) s += v[i];
     uint32_t total;
     uint32_t run = block_exclusive_scan<T>(s, sh, total) + (block_offsets ? block_offsets[blockIdx.x] : 0u);
+    if (base + kScanItems <= n && ((reinterpret_cast<uintptr_t>(out + base) & 15u) == 0)) {
+        uint4* p = reinterpret_cast<uint4*>(out + base);
 #pragma unroll
-    for (int i = 0; i < kScanItems; i++) {
-        size_t idx = base + i;
-        if (idx < n) out[idx] = run;
-        run += v[i];
+        for (int q = 0; q < kScanItems / 4; q++) {
+            uint4 t;
+            t.x = run;
+            run += v[4 * q];
+            t.y = run;
+            run += v[4 * q + 1];
+            t.z = run;
+            run += v[4 * q + 2];
+            t.w = run;
+            run += v[4 * q + 3];
+            p[q] = t;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < kScanItems; i++) {
+            size_t idx = base + i;
+            if (idx < n) out[idx] = run;
+            run += v[i];
+        }
     }
     // the last tile writes out[n] (total) when asked
     if (total_out && blockIdx.x == gridDim.x - 1 && threadIdx.x == kScanThreads - 1) *total_out = run;

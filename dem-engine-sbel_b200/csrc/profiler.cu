@@ -19,7 +19,7 @@ std::vector<cudaEvent_t> g_open;
 double g_ms[KID_COUNT];
 int64_t g_cnt[KID_COUNT];
 const char* g_names[KID_COUNT] = {"place_anal", "sphere_prep", "scan",    "sort_histogram", "sort_onesweep",
-                                  "gather_sorted", "pair_find", "pair_assemble", "history",        "force",
+                                  "gather_sorted", "pair_find", "pair_assemble", "pair_overflow", "cell_scatter", "history",        "force",
                                   "integrate",  "other"};
 }  // namespace
 

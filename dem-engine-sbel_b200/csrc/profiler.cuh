@@ -17,6 +17,8 @@ enum KernelId : int {
     KID_GATHER,
     KID_PAIR_COUNT,
     KID_PAIR_EMIT,
+    KID_PAIR_OVERFLOW,
+    KID_CELL_SCATTER,
     KID_HISTORY,
     KID_FORCE,
     KID_INTEGRATE,

@@ -264,6 +264,9 @@ int32_t deme_download_contact_forces(deme_handle* h, deme_contact_forces* out);
 /* Keep the per-contact force, torque-only force and local contact points of the next deme_compute_forces calls so
  * deme_download_contact_forces can return them (the fused hot path does not store them by default). */
 int32_t deme_keep_contact_forces(deme_handle* h, int32_t enable);
+/* How contact detection orders spheres by search cell: 0 (default) a one-pass counting sort (a radix sort whose single
+ * digit spans the cell range), 1 the multi-pass onesweep radix sort.  Both give the same contact list. */
+int32_t deme_set_cell_sort(deme_handle* h, int32_t onesweep);
 
 /* Streams: kT (contact detection) and dT (dynamics) work queues; NULL restores the handle's own streams.
  * The two workers of the reference are host threads with one stream each (src/core/utils/GpuManager.cpp:8-32). */

@@ -182,3 +182,20 @@ def test_gpu_empty_and_sparse_scenes():
     o.step(1)
     st, so = g.state(), o.state()
     np.testing.assert_allclose(st["vZ"], so["vZ"], rtol=1e-6)
+
+
+def test_cell_sort_variants_agree():
+    """The counting sort (default) and the onesweep radix sort order spheres differently inside a cell; the contact
+    list and its history must not depend on it."""
+    import ctypes as C
+    built = workloads.packed_clumps(n_clumps=500, seed=41, spacing=1.3)
+    lists = []
+    for onesweep in (0, 1):
+        g = gpu_solver(built, keep=False)
+        g.lib.deme_set_cell_sort.argtypes = [C.c_void_p, C.c_int32]
+        g.lib.deme_set_cell_sort(g.h, onesweep)
+        for _ in range(3):
+            g.step(1)
+        lists.append(g.contacts())
+    for k in ("idA", "idB", "type", "mapping"):
+        np.testing.assert_array_equal(lists[0][k], lists[1][k], err_msg=k)
