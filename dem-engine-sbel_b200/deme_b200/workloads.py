@@ -97,12 +97,14 @@ def triangle_template(rng, r_nom: float, rho: float, n_mc: int = 20000):
 
 def drum(n_clumps: int = 1_000_000, r_nom: float = 2e-3, rho: float = 2500.0, n_templates: int = 64,
          fill: float = 0.30, packing: float = 0.6, rpm: float = 20.0, dt: float = 5e-6, seed: int = 2,
-         shell: bool = False):
+         shell: bool = False, spacing: float = 1.02):
     """Rotating drum of three-sphere clumps (analytical cylinder + two end planes, prescribed rotation).
 
     One million clumps of about 8e-8 m^3 do not fit a 30 % fill of an R = 0.25 m, L = 0.3 m drum, so the drum is
     scaled (same L / R ratio) until the clumps at ``packing`` bulk density fill ``fill`` of its volume.
-    Clumps start on a loose lattice in the lower part of the drum with random orientations.
+    Clumps start on a loose lattice in the lower part of the drum with random orientations.  ``spacing`` is the
+    lattice pitch over the clump's bounding diameter: above 1 no two clumps touch; below 1 neighbouring clumps
+    interpenetrate, which gives a dense bed without settling (used to size CPU samples).
     """
     rng = np.random.default_rng(seed)
     tmpl = [triangle_template(rng, r_nom, rho) for _ in range(n_templates)]
@@ -125,7 +127,7 @@ def drum(n_clumps: int = 1_000_000, r_nom: float = 2e-3, rho: float = 2500.0, n_
     # demo likewise starts from a grid sampler with spacing above the clump size), filled from the bottom of the
     # drum; the bed settles under gravity before measurements (bench.py).
     reach = float(max(np.max(np.linalg.norm(t[1], axis=1) + t[0]) for t in tmpl))
-    a = 2.0 * reach * 1.02
+    a = 2.0 * reach * spacing
     dy, dz = a * math.sqrt(3.0) / 2.0, a * math.sqrt(2.0 / 3.0)
     nx, ny, nz = int(2 * R / a) + 2, int(L / dy) + 2, int(2 * R / dz) + 2
     K, J, I = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
