@@ -253,6 +253,7 @@ const char* deme_status_string(int32_t s) {
         case DEME_ERR_TIMEOUT: return "DEME_ERR_TIMEOUT";
         case DEME_ERR_STATE: return "DEME_ERR_STATE";
         case DEME_ERR_NO_DEVICE: return "DEME_ERR_NO_DEVICE";
+        case DEME_ERR_TOO_LARGE: return "DEME_ERR_TOO_LARGE";
         default: return "unknown";
     }
 }

@@ -23,6 +23,7 @@ STATUS_NAMES = {
     6: "DEME_ERR_TIMEOUT",
     7: "DEME_ERR_STATE",
     8: "DEME_ERR_NO_DEVICE",
+    9: "DEME_ERR_TOO_LARGE",
 }
 
 NOT_A_CONTACT = 0

@@ -35,7 +35,8 @@ typedef enum {
     DEME_ERR_NVRTC = 5,       /* the user force model did not compile */
     DEME_ERR_TIMEOUT = 6,     /* a bounded device wait gave up */
     DEME_ERR_STATE = 7,       /* call made in the wrong lifecycle state */
-    DEME_ERR_NO_DEVICE = 8    /* no CUDA device is visible */
+    DEME_ERR_NO_DEVICE = 8,   /* no CUDA device is visible */
+    DEME_ERR_TOO_LARGE = 9    /* input larger than a fixed capacity (nothing was launched) */
 } deme_status;
 
 /* Contact types (src/DEM/Defines.h:63-67).  Cylinder and cone are additions of this build. */
@@ -306,6 +307,22 @@ int32_t deme_radix_sort_pairs_device(const uint32_t* keys_in, const uint32_t* va
                                      uint32_t* vals_out, uint32_t n, int32_t key_bits, void* scratch,
                                      size_t scratch_bytes, void* stream);
 size_t deme_radix_sort_scratch_bytes(uint32_t n);
+
+/* Largest n deme_radix_sort_pairs_static accepts. */
+#define DEME_SORT_STATIC_MAX_N 1048576u
+
+/* The same stable sort for callers that cannot allocate device memory; it has no counterpart in the reference.
+ * It allocates nothing: its scratch is a fixed 8.5 MiB __device__ array inside this library, which every GPU that
+ * loads the library holds until the process exits.  The caller passes device inputs and outputs (outputs must not
+ * alias inputs); nothing needs to be zeroed beforehand, each call clears what its kernels read on `stream`.
+ * - n > DEME_SORT_STATIC_MAX_N returns DEME_ERR_TOO_LARGE and launches nothing; key_bits outside [0, 32] returns
+ *   DEME_ERR_INVALID.
+ * - The first call on each device (with that device current) looks up the scratch address; make it before any
+ *   stream capture.  A first call on a capturing stream returns DEME_ERR_STATE.
+ * - All calls on one device share the scratch: calls that overlap in time (other streams, other threads) race and
+ *   corrupt each other's results.  Serialise them, e.g. one stream per device. */
+int32_t deme_radix_sort_pairs_static(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                                     uint32_t* vals_out, uint32_t n, int32_t key_bits, void* stream);
 
 #ifdef __cplusplus
 }
