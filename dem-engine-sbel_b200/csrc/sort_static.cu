@@ -1,8 +1,14 @@
 // sort_static.cu -- deme_radix_sort_pairs_static: the onesweep radix sort of primitives.cu for callers that cannot
-// allocate device memory.  Its scratch (histograms, tile look-back flags, alternate key/value buffers, error word)
-// is one file-scope __device__ array, so every device that loads this library holds kStaticSortScratchBytes until
-// the process exits.  The array's device address is looked up once per device, on the first call made with that
-// device current; nothing here calls cudaMalloc/cudaFree or any allocating library routine.
+// allocate device memory.  Two kinds of caller are meant: code embedded in a host application that has already
+// reserved the GPU's memory for its own pool (a coupled fluid solver driving the DEM step, or a framework whose
+// caching allocator owns the HBM), where a cudaMalloc fails or splits that pool; and per-step code that must not
+// call cudaMalloc/cudaFree because they synchronise the device and stall the work queued on other streams.
+// Its scratch (histograms, tile look-back flags, alternate key/value buffers, error word) is one file-scope
+// __device__ array, so every device that loads this library holds kStaticSortScratchBytes until the process
+// exits.  Host code cannot use the array's name as a device pointer (on the host it names a stand-in object), so
+// its device address is looked up with cudaGetSymbolAddress once per device, on the first call made with that
+// device current, and passed to the kernels.  Nothing here calls cudaMalloc/cudaFree or any allocating library
+// routine.
 #include <mutex>
 
 #include "../../include/deme_b200.h"

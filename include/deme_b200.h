@@ -312,6 +312,9 @@ size_t deme_radix_sort_scratch_bytes(uint32_t n);
 #define DEME_SORT_STATIC_MAX_N 1048576u
 
 /* The same stable sort for callers that cannot allocate device memory; it has no counterpart in the reference.
+ * Such callers are, for example, a host application that has reserved the GPU's memory for its own pool (a coupled
+ * fluid solver, or a framework whose caching allocator owns the HBM), or per-step code that must not call
+ * cudaMalloc because it synchronises the device.
  * It allocates nothing: its scratch is a fixed 8.5 MiB __device__ array inside this library, which every GPU that
  * loads the library holds until the process exits.  The caller passes device inputs and outputs (outputs must not
  * alias inputs); nothing needs to be zeroed beforehand, each call clears what its kernels read on `stream`.

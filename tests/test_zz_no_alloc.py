@@ -1,5 +1,7 @@
 """deme_radix_sort_pairs_static, the sort whose scratch is a fixed __device__ array of the library (no device
-allocation in the call), against deme_radix_sort_pairs_device on the same inputs.
+allocation in the call), against deme_radix_sort_pairs_device on the same inputs.  It exists for callers that
+cannot allocate: a host application whose own memory pool already holds the GPU's memory, or per-step code that
+must not synchronise the device with a cudaMalloc.
 
 This file is collected last so that it also runs after every other GPU test in the same process; it must pass
 alone in a fresh process too (the first call does the per-device set-up)."""
