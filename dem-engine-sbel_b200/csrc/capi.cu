@@ -351,6 +351,7 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
     auto ncell = [&](double c, double d) { return (uint64_t)std::ceil(d / c) + 1; };
     while (ncell(cs, dom[0]) * ncell(cs, dom[1]) * ncell(cs, dom[2]) > (1ull << 26)) cs *= 1.25;
     k.cell_size = cs;
+    k.inv_cell = 1.0 / cs;
     k.gx = (uint32_t)ncell(cs, dom[0]);
     k.gy = (uint32_t)ncell(cs, dom[1]);
     k.gz = (uint32_t)ncell(cs, dom[2]);
@@ -482,7 +483,6 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
     TRY(dalloc_n(h, &cd.cnt, (size_t)nS + 1));
     // cnt[nS] stays 0 so the scan over nS + 1 entries leaves the total in off[nS]
     CUDA_TRY(h, cudaMemset(cd.cnt, 0, ((size_t)nS + 1) * sizeof(uint32_t)));
-    TRY(dalloc_n(h, &cd.candStart, nS + 1));
     TRY(dalloc_n(h, &cd.ovf, nS + 1));
     TRY(dalloc_n(h, &cd.counters, 4));
     TRY(ensure_cand(h, std::max<uint32_t>(1024u, 2u * nS)));
@@ -582,6 +582,7 @@ int32_t deme_detect_contacts(deme_handle* h) {
     uint32_t n = 0;
     for (int attempt = 0; attempt < 2; attempt++) {
         CUDA_TRY(h, cudaMemsetAsync(cd.counters, 0, 2 * sizeof(uint32_t), st));
+        if (attempt) launch_cnt_init(k, cd, st);
         launch_pair_find(k, s, cd, h->candCap, st);
         launch_pair_overflow(k, s, cd, h->candCap, st);
         TRY(check_launch(h, "contact search"));
@@ -591,10 +592,15 @@ int32_t deme_detect_contacts(deme_handle* h) {
         CUDA_TRY(h, cudaStreamSynchronize(st));
         n = h->hTotal[0];
         if (h->hTotal[1] <= h->candCap) break;
-        // the partner list outgrew its buffer: grow and search again
+        // the pair list outgrew its buffer: grow and search again
         TRY(ensure_cand(h, h->hTotal[1]));
     }
+    if (h->hTotal[1] > h->candCap) {
+        h->err = "contact search: pair list still over capacity after growing";
+        return DEME_ERR_OVERFLOW;
+    }
     TRY(ensure_list(h, nb, n));
+    launch_pair_scatter(k, cd, nb.view(), h->hTotal[1], nb.cap, st);
     launch_pair_assemble(k, s, cd, nb.view(), nb.cap, st);
     launch_history(k, nb.view(), pb.view(), n, h->nContacts, h->nW > 0, st);
     TRY(check_launch(h, "contact assembly"));

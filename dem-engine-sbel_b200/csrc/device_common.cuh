@@ -42,6 +42,7 @@ struct SimConsts {
     uint32_t n_spheres, n_owners, n_anal;
     // contact-detection search grid (positions relative to the LBF corner)
     double cell_size;
+    double inv_cell;     // 1 / cell_size
     uint32_t gx, gy, gz;
     float r_max_cd;      // largest CD radius (radius + beta)
     float prefilter_abs; // absolute slack of the float pre-filter
@@ -72,6 +73,11 @@ __host__ __device__ __forceinline__ uint32_t sat_u32(double x) {
     if (!(x > 0.0)) return 0u;
     if (x >= 4294967296.0) return 0xFFFFFFFFu;
     return (uint32_t)x;
+}
+
+// Search-grid cell coordinate of x (clamped to the grid).  Monotone in x, which is all the search relies on.
+__device__ __forceinline__ uint32_t cell_of(double x, double inv_cell, uint32_t g) {
+    return min(sat_u32(x * inv_cell), g - 1u);
 }
 __host__ __device__ __forceinline__ uint64_t sat_u64(double x) {
     if (!(x > 0.0)) return 0ull;

@@ -7,11 +7,12 @@
 //     owner(A) != owner(B), the family mask allows it, the double-precision overlap test of the expanded radii
 //     passes, and bin(CP) lies in bin_range(A) and in bin_range(B) on every axis.
 // This file enumerates candidates differently -- each sphere is sorted once into a home cell of a search grid
-// whose cells are at least one expanded diameter wide, and each sphere A scans the cells its neighbours can live
-// in -- and then evaluates that same predicate with the reference's arithmetic.  The contact set is therefore the
-// reference's, while the bin-pair list (about 8-30 pairs per sphere) and its 32-bit radix sort disappear.  Output
-// is written directly in canonical order: grouped by A (ascending), sphere--analytical contacts first, then
-// sphere--sphere contacts by ascending B.
+// whose cells are at least one expanded diameter wide, and each sphere scans the forward half (in cell order) of
+// the cells its neighbours can live in, so every pair is tested once -- and then evaluates that same predicate
+// with the reference's arithmetic.  The contact set is therefore the reference's, while the bin-pair list (about
+// 8-30 pairs per sphere) and its 32-bit radix sort disappear.  Found pairs are counted per A, scanned into
+// segments and placed; the list is then in canonical order: grouped by A (ascending), sphere--analytical contacts
+// first, then sphere--sphere contacts by ascending B.
 //
 // Dynamics (dT).  One fused kernel per contact: pose gather, overlap re-test, Hertz-Mindlin, history update and
 // accumulation of the owners' linear and angular accelerations (the reference's calculateContactForces +
@@ -103,9 +104,9 @@ __global__ void __launch_bounds__(256) k_sphere_prep(SimConsts k, StateView s, C
     float rf = sp.w;
     rf += k.beta;
     cd.posF[sid] = make_float4((float)X, (float)Y, (float)Z, rf);
-    const uint32_t cx = min(sat_u32(X / k.cell_size), k.gx - 1);
-    const uint32_t cy = min(sat_u32(Y / k.cell_size), k.gy - 1);
-    const uint32_t cz = min(sat_u32(Z / k.cell_size), k.gz - 1);
+    const uint32_t cx = cell_of(X, k.inv_cell, k.gx);
+    const uint32_t cy = cell_of(Y, k.inv_cell, k.gy);
+    const uint32_t cz = cell_of(Z, k.inv_cell, k.gz);
     const uint32_t key = cx + k.gx * (cy + k.gy * cz);
     cd.cellKey[sid] = key;
     cd.idSeq[sid] = sid;
@@ -121,6 +122,7 @@ __global__ void __launch_bounds__(256) k_sphere_prep(SimConsts k, StateView s, C
         if (anal_overlap_cd(ap, X, Y, Z, rD, k.beta) != DEME_NOT_A_CONTACT) c++;
     }
     cd.nAnal[sid] = (uint8_t)c;
+    cd.cnt[sid] = c;  // the pair search adds the sphere partners for which this sphere is A
 }
 
 void launch_sphere_prep(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st) {
@@ -188,160 +190,154 @@ void launch_gather_sorted(const SimConsts& k, const StateView& s, const CDView& 
     k_gather_sorted<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
 }
 
-// The reference's pair predicate for A < B (see the file comment), B given by its cell-order index j; rngA holds
-// A's packed bin ranges.
-__device__ __forceinline__ bool pair_is_contact(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t j,
-                                                uint32_t oA, uint32_t famA, float rfA, double xa, double ya, double za,
-                                                uint4 rngA) {
-    const uint4 mB = cd.metaS[j];
-    const uint32_t oB = mB.x;
-    if (oA == oB) return false;
-    if (s.masks[mask_index(famA, mB.z)] != 0) return false;
-    float rfB = __uint_as_float(mB.y);
-    rfB += k.beta;
-    const double xb = cd.pXs[j], yb = cd.pYs[j], zb = cd.pZs[j];
-    // checkSpheresOverlap<double>, DEMHelperKernels.cu:195-222
-    const double radA = (double)rfA, radB = (double)rfB;
-    const double d2 = (xa - xb) * (xa - xb) + (ya - yb) * (ya - yb) + (za - zb) * (za - zb);
-    if (d2 > (radA + radB) * (radA + radB)) return false;
-    float nx = (float)(xa - xb), ny = (float)(ya - yb), nz = (float)(za - zb);
-    normalize_f(nx, ny, nz);
-    const double half = (radA + radB - sqrt(d2)) / 2.0;
-    const double cpx = xb + (radB - half) * (double)nx;
-    const double cpy = yb + (radB - half) * (double)ny;
-    const double cpz = zb + (radB - half) * (double)nz;
-    // getPointBinID, DEMHelperKernels.cu:266-273, tested per axis against both spheres' bin ranges
-    const uint32_t bx = sat_u32(cpx / k.bin_size), by = sat_u32(cpy / k.bin_size), bz = sat_u32(cpz / k.bin_size);
-    if (!in_range(bx, rngA.x) || !in_range(by, rngA.y) || !in_range(bz, rngA.z)) return false;
-    const uint4 rngB = cd.rngS[j];
-    return in_range(bx, rngB.x) && in_range(by, rngB.y) && in_range(bz, rngB.z);
+// One sphere as the exact pair test sees it (cell-order records).
+struct SphRec {
+    double x, y, z;
+    uint4 rng;  // bin ranges of the expanded sphere, packed 16 bits per bound
+    uint32_t owner, fam, id;
+    float rf;  // expanded radius (radius + beta) in float, as the reference forms it
+};
+
+__device__ __forceinline__ SphRec load_rec(const SimConsts& k, const CDView& cd, uint32_t j) {
+    SphRec r;
+    r.x = cd.pXs[j];
+    r.y = cd.pYs[j];
+    r.z = cd.pZs[j];
+    const uint4 m = cd.metaS[j];
+    r.owner = m.x;
+    r.fam = m.z;
+    float rf = __uint_as_float(m.y);
+    rf += k.beta;
+    r.rf = rf;
+    r.rng = cd.rngS[j];
+    r.id = __float_as_uint(__ldg(&cd.posFSorted[j].w));
+    return r;
 }
 
-// Enumerate the contacts (B > A) of sphere A among the spheres whose home cells lie where A's neighbours can live.
-// The first kSlots partners are stored in buf (dynamic indexing keeps buf in local memory, which L1 caches); the
-// return value counts all of them.
-constexpr uint32_t kSlots = 16;
+// The reference's pair predicate (see the file comment) with a.id < b.id: the roles matter, because the contact
+// point is formed from B's side exactly as the reference forms it.
+__device__ __forceinline__ bool pair_exact(const SimConsts& k, const StateView& s, const SphRec& a, const SphRec& b) {
+    if (a.owner == b.owner) return false;
+    if (s.masks[mask_index(a.fam, b.fam)] != 0) return false;
+    // checkSpheresOverlap<double>, DEMHelperKernels.cu:195-222
+    const double radA = (double)a.rf, radB = (double)b.rf;
+    const double d2 = (a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y) + (a.z - b.z) * (a.z - b.z);
+    if (d2 > (radA + radB) * (radA + radB)) return false;
+    float nx = (float)(a.x - b.x), ny = (float)(a.y - b.y), nz = (float)(a.z - b.z);
+    normalize_f(nx, ny, nz);
+    const double half = (radA + radB - sqrt(d2)) / 2.0;
+    const double cpx = b.x + (radB - half) * (double)nx;
+    const double cpy = b.y + (radB - half) * (double)ny;
+    const double cpz = b.z + (radB - half) * (double)nz;
+    // getPointBinID, DEMHelperKernels.cu:266-273, tested per axis against both spheres' bin ranges
+    const uint32_t bx = sat_u32(cpx / k.bin_size), by = sat_u32(cpy / k.bin_size), bz = sat_u32(cpz / k.bin_size);
+    return in_range(bx, a.rng.x) && in_range(by, a.rng.y) && in_range(bz, a.rng.z) && in_range(bx, b.rng.x) &&
+           in_range(by, b.rng.y) && in_range(bz, b.rng.z);
+}
 
-__device__ __forceinline__ uint32_t scan_neighbours(const SimConsts& k, const StateView& s, const CDView& cd,
-                                                    uint32_t iA, uint32_t* out, uint32_t out_cap) {
-    const float4 fA = cd.posFSorted[iA];
-    const uint32_t A = __float_as_uint(fA.w);
-    const double xa = cd.pXs[iA], ya = cd.pYs[iA], za = cd.pZs[iA];
-    const uint4 mA = cd.metaS[iA];
-    float rfA = __uint_as_float(mA.y);
-    rfA += k.beta;
-    const uint4 rngA = cd.rngS[iA];
-    const double reach = (double)rfA + (double)k.r_max_cd + (double)k.prefilter_abs;
-    const uint32_t x0 = min(sat_u32((xa - reach) / k.cell_size), k.gx - 1);
-    const uint32_t x1 = min(sat_u32((xa + reach) / k.cell_size), k.gx - 1);
-    const uint32_t y0 = min(sat_u32((ya - reach) / k.cell_size), k.gy - 1);
-    const uint32_t y1 = min(sat_u32((ya + reach) / k.cell_size), k.gy - 1);
-    const uint32_t z0 = min(sat_u32((za - reach) / k.cell_size), k.gz - 1);
-    const uint32_t z1 = min(sat_u32((za + reach) / k.cell_size), k.gz - 1);
-    const float lim = (rfA + k.r_max_cd) * 1.00001f + k.prefilter_abs;
-    const float lim2 = lim * lim;
-    uint32_t count = 0;
-    for (uint32_t cz = z0; cz <= z1; cz++) {
-        for (uint32_t cy = y0; cy <= y1; cy++) {
+// Cells the neighbours of a sphere can live in.  Cell coordinates come from cell_of (a multiply by the
+// reciprocal cell size); the search grid is this file's own construct, so only monotonicity matters: a sphere
+// within `reach` of x has its home cell inside [cell_of(x - reach), cell_of(x + reach)].
+struct SearchBox {
+    uint32_t x0, x1, y0, y1, z0, z1, cy, cz;
+};
+
+__device__ __forceinline__ SearchBox search_box(const SimConsts& k, double x, double y, double z, float rf) {
+    const double reach = (double)rf + (double)k.r_max_cd + (double)k.prefilter_abs;
+    SearchBox b;
+    b.x0 = cell_of(x - reach, k.inv_cell, k.gx);
+    b.x1 = cell_of(x + reach, k.inv_cell, k.gx);
+    b.y0 = cell_of(y - reach, k.inv_cell, k.gy);
+    b.y1 = cell_of(y + reach, k.inv_cell, k.gy);
+    b.z0 = cell_of(z - reach, k.inv_cell, k.gz);
+    b.z1 = cell_of(z + reach, k.inv_cell, k.gz);
+    b.cy = cell_of(y, k.inv_cell, k.gy);
+    b.cz = cell_of(z, k.inv_cell, k.gz);
+    return b;
+}
+
+// Visits every candidate j of sphere i (cell-order index) in the FORWARD half of its neighbourhood: rows of cells
+// after i's own row in cell order (all of their cells in the box), and in i's own row the spheres after i.  Every
+// unordered pair of spheres within reach is visited exactly once, by the sphere that comes first in cell order.
+// `visit(j)` receives the cell-order index of each candidate that passes the float pre-filter.
+template <typename Visit>
+__device__ __forceinline__ void for_each_forward_candidate(const SimConsts& k, const CDView& cd, uint32_t i,
+                                                           const float4 fA, const SearchBox& b, float lim2,
+                                                           Visit visit) {
+    for (uint32_t cz = max(b.z0, b.cz); cz <= b.z1; cz++) {
+        for (uint32_t cy = (cz == b.cz) ? max(b.y0, b.cy) : b.y0; cy <= b.y1; cy++) {
             const uint32_t rowBase = k.gx * (cy + k.gy * cz);
-            const uint32_t j0 = cd.cellStart[rowBase + x0];
-            uint32_t j1 = cd.cellStart[rowBase + x1 + 1];
+            const bool own = (cz == b.cz) && (cy == b.cy);
+            const uint32_t j0 = own ? i + 1u : __ldg(cd.cellStart + rowBase + b.x0);
+            uint32_t j1 = __ldg(cd.cellStart + rowBase + b.x1 + 1);
             if (!index_ok(k.err, 2, j1, (uint64_t)k.n_spheres + 1)) j1 = j0;
             for (uint32_t j = j0; j < j1; j++) {
-                const float4 fB = cd.posFSorted[j];
+                const float4 fB = __ldg(cd.posFSorted + j);
                 const float dx = fA.x - fB.x, dy = fA.y - fB.y, dz = fA.z - fB.z;
-                if (dx * dx + dy * dy + dz * dz > lim2) continue;
-                const uint32_t B = __float_as_uint(fB.w);
-                if (B <= A) continue;
-                if (!pair_is_contact(k, s, cd, j, mA.x, mA.z, rfA, xa, ya, za, rngA)) continue;
-                if (count < out_cap) out[count] = B;
-                count++;
+                // explicit fused multiply-adds: the pre-filter only has to be conservative, its margin covers them
+                const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
+                if (d2 <= lim2) visit(j);
             }
         }
     }
-    return count;
+}
+
+__device__ __forceinline__ float prefilter_lim2(const SimConsts& k, float rf) {
+    const float lim = (rf + k.r_max_cd) * 1.00001f + k.prefilter_abs;
+    return lim * lim;
+}
+
+// Appends found pairs (A, B) to the temporary list with one atomic per warp and counts them on A.  All 32 lanes
+// of the warp call it together.
+__device__ __forceinline__ void append_pairs(const CDView& cd, bool hit, uint32_t A, uint32_t B, uint32_t tempCap) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t m = __ballot_sync(0xffffffffu, hit);
+    if (!m) return;
+    const uint32_t leader = __ffs(m) - 1u;
+    uint32_t start = 0;
+    if (lane == leader) start = atomicAdd(&cd.counters[0], (uint32_t)__popc(m));
+    start = __shfl_sync(0xffffffffu, start, leader);
+    if (hit) {
+        const uint32_t pos = start + __popc(m & ((1u << lane) - 1u));
+        if (pos < tempCap) cd.candTemp[pos] = make_uint2(A, B);
+        atomicAdd(&cd.cnt[A], 1u);
+    }
 }
 
 // One search pass, threads in cell order (a warp shares neighbour cells), in three phases per warp:
-//   1. each lane runs the cheap float pre-filter over its candidate cells and keeps the survivors' cell-order
-//      indices (a lane that fills its survivor list tests the extra ones itself);
-//   2. the warp pools all survivors in shared memory (prefix sum over lanes), so that
+//   1. each lane runs the cheap float pre-filter over the forward half of its neighbourhood and keeps the
+//      survivors' cell-order indices in shared memory;
+//   2. the warp pools all survivors (prefix sum over lanes), so that
 //   3. all 32 lanes run the double-precision reference predicate on pooled (sphere, candidate) pairs, instead of
 //      the whole warp stepping through the expensive path whenever any one lane has a survivor.
-// Partners land in a per-lane shared list; each sphere's list then goes to the temporary partner list at a
-// warp-aggregated offset, and spheres with more than kSlots partners are queued for a re-scan.
+// Found pairs go to the temporary list (any order) and raise A's count, which was preset to A's number of
+// analytical contacts; a lane with more survivors than it can pool is queued for k_pair_overflow.
 constexpr uint32_t kSurv = 16;
 constexpr uint32_t kFindWarps = 4;
 
-struct SphereCtx {
-    double x, y, z;
-    uint4 rng;
-    uint32_t owner, fam, A;
-    float rf;
-};
-
 __global__ void __launch_bounds__(kFindWarps * 32, 8) k_pair_find(SimConsts k, StateView s, CDView cd,
                                                                   uint32_t tempCap) {
-    __shared__ uint32_t s_pre[kFindWarps][33];             // survivor prefix over lanes
-    __shared__ uint32_t s_j[kFindWarps][32 * kSurv];       // pooled survivors (cell-order index)
-    __shared__ SphereCtx s_ctx[kFindWarps][32];
-    __shared__ uint32_t s_res[kFindWarps][32][kSlots];
-    __shared__ uint32_t s_resCnt[kFindWarps][32];
+    __shared__ uint32_t s_pre[kFindWarps][33];          // survivor prefix over lanes
+    __shared__ uint32_t s_surv[kFindWarps][kSurv][32];  // survivors, [slot][lane]
+    __shared__ SphRec s_ctx[kFindWarps][32];
     const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     bool valid = i < k.n_spheres;
-    s_resCnt[w][lane] = 0;
-    uint32_t surv[kSurv];
     uint32_t nSurv = 0;
-    uint32_t A = 0xFFFFFFFFu;
     if (valid) {
-        const float4 fA = cd.posFSorted[i];
-        A = __float_as_uint(fA.w);
-        if (!index_ok(k.err, 12, A, k.n_spheres)) {
+        const float4 fA = __ldg(cd.posFSorted + i);
+        const SphRec me = load_rec(k, cd, i);
+        if (!index_ok(k.err, 12, me.id, k.n_spheres)) {
             valid = false;
         } else {
-            SphereCtx c;
-            c.A = A;
-            c.x = cd.pXs[i];
-            c.y = cd.pYs[i];
-            c.z = cd.pZs[i];
-            const uint4 mA = cd.metaS[i];
-            c.owner = mA.x;
-            c.fam = mA.z;
-            float rf = __uint_as_float(mA.y);
-            rf += k.beta;
-            c.rf = rf;
-            c.rng = cd.rngS[i];
-            s_ctx[w][lane] = c;
-            const double reach = (double)rf + (double)k.r_max_cd + (double)k.prefilter_abs;
-            const uint32_t x0 = min(sat_u32((c.x - reach) / k.cell_size), k.gx - 1);
-            const uint32_t x1 = min(sat_u32((c.x + reach) / k.cell_size), k.gx - 1);
-            const uint32_t y0 = min(sat_u32((c.y - reach) / k.cell_size), k.gy - 1);
-            const uint32_t y1 = min(sat_u32((c.y + reach) / k.cell_size), k.gy - 1);
-            const uint32_t z0 = min(sat_u32((c.z - reach) / k.cell_size), k.gz - 1);
-            const uint32_t z1 = min(sat_u32((c.z + reach) / k.cell_size), k.gz - 1);
-            const float lim = (rf + k.r_max_cd) * 1.00001f + k.prefilter_abs;
-            const float lim2 = lim * lim;
-            for (uint32_t cz = z0; cz <= z1; cz++) {
-                for (uint32_t cy = y0; cy <= y1; cy++) {
-                    const uint32_t rowBase = k.gx * (cy + k.gy * cz);
-                    const uint32_t j0 = __ldg(cd.cellStart + rowBase + x0);
-                    uint32_t j1 = __ldg(cd.cellStart + rowBase + x1 + 1);
-                    if (!index_ok(k.err, 2, j1, (uint64_t)k.n_spheres + 1)) j1 = j0;
-                    for (uint32_t j = j0; j < j1; j++) {
-                        const float4 fB = __ldg(cd.posFSorted + j);
-                        const float dx = fA.x - fB.x, dy = fA.y - fB.y, dz = fA.z - fB.z;
-                        const bool keep = (dx * dx + dy * dy + dz * dz <= lim2) & (__float_as_uint(fB.w) > A);
-                        if (keep) {
-                            if (nSurv < kSurv) surv[nSurv] = j;
-                            nSurv++;
-                        }
-                    }
-                }
-            }
+            s_ctx[w][lane] = me;
+            const SearchBox b = search_box(k, me.x, me.y, me.z, me.rf);
+            for_each_forward_candidate(k, cd, i, fA, b, prefilter_lim2(k, me.rf), [&](uint32_t j) {
+                if (nSurv < kSurv) s_surv[w][nSurv][lane] = j;
+                nSurv++;
+            });
         }
     }
-    // a lane with more survivors than it can pool is re-scanned by k_pair_overflow
     const bool ovf = valid && nSurv > kSurv;
     const uint32_t pool = (valid && !ovf) ? nSurv : 0u;
     uint32_t incl = pool;
@@ -351,49 +347,39 @@ __global__ void __launch_bounds__(kFindWarps * 32, 8) k_pair_find(SimConsts k, S
         if (lane >= (uint32_t)off) incl += y;
     }
     const uint32_t totalSurv = __shfl_sync(0xffffffffu, incl, 31);
-    const uint32_t sbase = incl - pool;
     s_pre[w][lane + 1] = incl;
     if (lane == 0) s_pre[w][0] = 0;
-    for (uint32_t q = 0; q < pool; q++) s_j[w][sbase + q] = surv[q];
     __syncwarp();
     // exact reference predicate on pooled pairs, all lanes busy
-    for (uint32_t p = lane; p < totalSurv; p += 32) {
-        uint32_t L = 0;  // owning lane: last lane whose prefix is <= p
+    for (uint32_t base = 0; base < totalSurv; base += 32) {
+        const uint32_t p = base + lane;
+        bool hit = false;
+        uint32_t A = 0, B = 0;
+        if (p < totalSurv) {
+            uint32_t L = 0;  // owning lane: last lane whose prefix is <= p
 #pragma unroll
-        for (uint32_t step = 16; step > 0; step >>= 1)
-            if (s_pre[w][L + step] <= p) L += step;
-        const uint32_t j = s_j[w][p];
-        const SphereCtx& a = s_ctx[w][L];
-        if (pair_is_contact(k, s, cd, j, a.owner, a.fam, a.rf, a.x, a.y, a.z, a.rng)) {
-            const uint32_t r = atomicAdd(&s_resCnt[w][L], 1u);
-            if (r < kSlots) s_res[w][L][r] = __float_as_uint(__ldg(cd.posFSorted + j).w);
+            for (uint32_t step = 16; step > 0; step >>= 1)
+                if (s_pre[w][L + step] <= p) L += step;
+            const uint32_t j = s_surv[w][p - s_pre[w][L]][L];
+            const SphRec me = s_ctx[w][L];
+            const SphRec ot = load_rec(k, cd, j);
+            if (me.id < ot.id) {
+                hit = pair_exact(k, s, me, ot);
+                A = me.id;
+                B = ot.id;
+            } else {
+                hit = pair_exact(k, s, ot, me);
+                A = ot.id;
+                B = me.id;
+            }
+            if (hit && !index_ok(k.err, 14, A, k.n_spheres)) hit = false;
         }
+        append_pairs(cd, hit, A, B, tempCap);
     }
-    __syncwarp();
-    const bool ovf2 = ovf || (valid && s_resCnt[w][lane] > kSlots);
-    const uint32_t n = (valid && !ovf2) ? s_resCnt[w][lane] : 0u;
-    // warp-aggregated allocation in the temporary partner list
-    uint32_t inc2 = n;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, inc2, off);
-        if (lane >= (uint32_t)off) inc2 += y;
-    }
-    const uint32_t total = __shfl_sync(0xffffffffu, inc2, 31);
-    uint32_t base = 0;
-    if (lane == 31 && total) base = atomicAdd(&cd.counters[0], total);
-    base = __shfl_sync(0xffffffffu, base, 31);
-    if (!valid) return;
-    if (ovf2) {
+    if (ovf) {
         const uint32_t o = atomicAdd(&cd.counters[1], 1u);
-        cd.ovf[o] = i;  // cell-order index; k_pair_overflow writes cnt and the list
-        return;
+        cd.ovf[o] = i;  // cell-order index; k_pair_overflow searches it again
     }
-    const uint32_t start = base + inc2 - n;
-    cd.cnt[A] = n + cd.nAnal[A];
-    cd.candStart[A] = start;
-    if (start + n <= tempCap)
-        for (uint32_t t = 0; t < n; t++) cd.candTemp[start + t] = s_res[w][lane][t];
 }
 
 void launch_pair_find(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st) {
@@ -402,22 +388,26 @@ void launch_pair_find(const SimConsts& k, const StateView& s, const CDView& cd, 
     k_pair_find<<<blocks_for(k.n_spheres, kFindWarps * 32), kFindWarps * 32, 0, st>>>(k, s, cd, tempCap);
 }
 
-// Spheres the pooled search could not hold: full per-thread search, counted first, then written to a freshly
-// allocated run of the temporary list.  Grid-stride over the device-side overflow count (no host round trip).
+// Spheres the pooled search could not hold: the same forward-half search, one thread per sphere, exact test
+// inline.  Grid-stride over the device-side overflow count (no host round trip).
 __global__ void __launch_bounds__(128) k_pair_overflow(SimConsts k, StateView s, CDView cd, uint32_t tempCap) {
     const uint32_t nOvf = *((volatile uint32_t*)&cd.counters[1]);
     for (uint32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < nOvf; o += gridDim.x * blockDim.x) {
-        const uint32_t iA = cd.ovf[o];
-        if (!index_ok(k.err, 13, iA, k.n_spheres)) continue;
-        const uint32_t A = __float_as_uint(cd.posFSorted[iA].w);
-        const uint32_t n = scan_neighbours(k, s, cd, iA, nullptr, 0);
-        const uint32_t start = atomicAdd(&cd.counters[0], n);
-        cd.cnt[A] = n + cd.nAnal[A];
-        cd.candStart[A] = start;
-        if ((uint64_t)start + n <= tempCap) {
-            const uint32_t got = scan_neighbours(k, s, cd, iA, cd.candTemp + start, n);
-            if (got != n) atomicOr(k.err, ERR_SEGMENT_TOO_LONG);
-        }
+        const uint32_t i = cd.ovf[o];
+        if (!index_ok(k.err, 13, i, k.n_spheres)) continue;
+        const float4 fA = __ldg(cd.posFSorted + i);
+        const SphRec me = load_rec(k, cd, i);
+        const SearchBox b = search_box(k, me.x, me.y, me.z, me.rf);
+        for_each_forward_candidate(k, cd, i, fA, b, prefilter_lim2(k, me.rf), [&](uint32_t j) {
+            const SphRec ot = load_rec(k, cd, j);
+            const bool lower = me.id < ot.id;
+            if (!(lower ? pair_exact(k, s, me, ot) : pair_exact(k, s, ot, me))) return;
+            const uint32_t A = lower ? me.id : ot.id, B = lower ? ot.id : me.id;
+            if (!index_ok(k.err, 14, A, k.n_spheres)) return;
+            const uint32_t pos = atomicAdd(&cd.counters[0], 1u);
+            if (pos < tempCap) cd.candTemp[pos] = make_uint2(A, B);
+            atomicAdd(&cd.cnt[A], 1u);
+        });
     }
 }
 
@@ -427,26 +417,62 @@ void launch_pair_overflow(const SimConsts& k, const StateView& s, const CDView& 
     k_pair_overflow<<<148, 128, 0, st>>>(k, s, cd, tempCap);
 }
 
-// Writes the canonical list: per sphere A (ID order), its sphere--analytical contacts by component id
-// (populateBinSphereTouchingPairs, DEMBinSphereKernels.cu:186-228), then its sphere partners by ascending id.
+// Presets every sphere's contact count to its number of analytical contacts (k_sphere_prep does the same; this is
+// for a repeated search after the temporary list grew).
+__global__ void k_cnt_init(uint32_t n, const uint8_t* __restrict__ nAnal, uint32_t* cnt) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) cnt[i] = nAnal[i];
+}
+
+void launch_cnt_init(const SimConsts& k, const CDView& cd, cudaStream_t st) {
+    if (!(k.n_spheres)) return;
+    ProfScope prof_(KID_OTHER, st);
+    k_cnt_init<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k.n_spheres, cd.nAnal, cd.cnt);
+}
+
+// Places every found pair in A's segment of the new list.  After the scan A's count is no longer needed, so the
+// slots after A's analytical contacts are handed out from the top by decrementing it.
+__global__ void __launch_bounds__(256) k_pair_scatter(SimConsts k, CDView cd, ContactView c, uint32_t nPairs,
+                                                      uint32_t cap) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nPairs) return;
+    const uint2 ab = cd.candTemp[p];
+    if (!index_ok(k.err, 15, ab.x, k.n_spheres)) return;
+    const uint32_t slot = atomicSub(&cd.cnt[ab.x], 1u) - 1u;
+    const uint32_t pos = c.off[ab.x] + slot;
+    if (!index_ok(k.err, 16, pos, cap)) return;
+    c.idB[pos] = ab.y;
+}
+
+void launch_pair_scatter(const SimConsts& k, const CDView& cd, const ContactView& c, uint32_t nPairs, uint32_t cap,
+                         cudaStream_t st) {
+    if (!(nPairs)) return;
+    ProfScope prof_(KID_PAIR_EMIT, st);
+    k_pair_scatter<<<blocks_for(nPairs, 256), 256, 0, st>>>(k, cd, c, nPairs, cap);
+}
+
+// Completes the canonical list: per sphere A (ID order), its sphere--analytical contacts by component id
+// (populateBinSphereTouchingPairs, DEMBinSphereKernels.cu:186-228) in the first slots of its segment, then its
+// sphere partners (placed by k_pair_scatter) sorted by ascending id.
 __global__ void __launch_bounds__(256) k_pair_assemble(SimConsts k, StateView s, CDView cd, ContactView c,
                                                        uint32_t cap) {
     const uint32_t A = blockIdx.x * blockDim.x + threadIdx.x;
     if (A >= k.n_spheres) return;
     const uint32_t begin = c.off[A], end = c.off[A + 1];
-    if (end > cap) {
+    if (end > cap || begin > end) {
         atomicOr(k.err, ERR_CONTACT_CAPACITY);
         return;
     }
-    uint32_t w = begin;
     const uint32_t nAn = cd.nAnal[A];
+    const uint32_t anEnd = min(begin + nAn, end);
+    uint32_t w = begin;
     if (nAn) {
         const double X = cd.pX[A], Y = cd.pY[A], Z = cd.pZ[A];
         const float4 sp = s.sph[A];
         double rD = (double)sp.w;
         rD += (double)k.beta;
         const uint32_t fam = s.loc[s.sOwner[A]].w;
-        for (uint32_t a = 0; a < s.nA && w < end; a++) {
+        for (uint32_t a = 0; a < s.nA && w < anEnd; a++) {
             const AnalPlaced ap = s.anal[a];
             if (s.masks[mask_index(fam, s.loc[ap.owner].w)] != 0) continue;
             const int t = anal_overlap_cd(ap, X, Y, Z, rD, k.beta);
@@ -457,12 +483,12 @@ __global__ void __launch_bounds__(256) k_pair_assemble(SimConsts k, StateView s,
                 w++;
             }
         }
+        if (w != anEnd) atomicOr(k.err, ERR_SEGMENT_TOO_LONG);
     }
-    const uint32_t n = end - w;
-    const uint32_t* src = cd.candTemp + cd.candStart[A];
-    uint32_t* seg = c.idB + w;
-    for (uint32_t i = 0; i < n; i++) {
-        const uint32_t v = src[i];
+    uint32_t* seg = c.idB + anEnd;
+    const uint32_t n = end - anEnd;
+    for (uint32_t i = 1; i < n; i++) {
+        const uint32_t v = seg[i];
         uint32_t j = i;
         while (j > 0 && seg[j - 1] > v) {
             seg[j] = seg[j - 1];
@@ -471,8 +497,8 @@ __global__ void __launch_bounds__(256) k_pair_assemble(SimConsts k, StateView s,
         seg[j] = v;
     }
     for (uint32_t i = 0; i < n; i++) {
-        c.idA[w + i] = A;
-        c.type[w + i] = DEME_SPHERE_SPHERE_CONTACT;
+        c.idA[anEnd + i] = A;
+        c.type[anEnd + i] = DEME_SPHERE_SPHERE_CONTACT;
     }
 }
 

@@ -56,10 +56,9 @@ struct CDView {
     uint32_t* cellStart;  // nCells + 1
     uint8_t* nAnal;
     uint32_t* cnt;
-    uint32_t* candStart;  // per sphere: first partner in candTemp
-    uint32_t* candTemp;   // partners of all spheres, one run per sphere
-    uint32_t* ovf;        // spheres with more partners than the search keeps in registers
-    uint32_t* counters;   // [0] partners appended, [1] overflow spheres
+    uint2* candTemp;      // found sphere pairs (A, B), A < B, in no particular order
+    uint32_t* ovf;        // spheres with more pre-filter survivors than the pooled search holds
+    uint32_t* counters;   // [0] pairs appended, [1] overflow spheres
 };
 
 // One contact list (kT product) with its history wildcards.
@@ -93,6 +92,9 @@ void launch_cell_scatter(const SimConsts& k, const CDView& cd, cudaStream_t st);
 void launch_gather_sorted(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
 void launch_pair_find(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st);
 void launch_pair_overflow(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st);
+void launch_cnt_init(const SimConsts& k, const CDView& cd, cudaStream_t st);
+void launch_pair_scatter(const SimConsts& k, const CDView& cd, const ContactView& c, uint32_t nPairs, uint32_t cap,
+                         cudaStream_t st);
 void launch_pair_assemble(const SimConsts& k, const StateView& s, const CDView& cd, const ContactView& c, uint32_t cap,
                           cudaStream_t st);
 void launch_history(const SimConsts& k, const ContactView& cur, const ContactView& prev, uint32_t n, uint32_t prevN,
