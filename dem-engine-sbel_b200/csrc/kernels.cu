@@ -214,15 +214,22 @@ __device__ __forceinline__ SphRec load_rec(const SimConsts& k, const CDView& cd,
     return r;
 }
 
-// The reference's pair predicate (see the file comment) with a.id < b.id: the roles matter, because the contact
-// point is formed from B's side exactly as the reference forms it.
-__device__ __forceinline__ bool pair_exact(const SimConsts& k, const StateView& s, const SphRec& a, const SphRec& b) {
+// The reference's pair predicate (see the file comment) with a.id < b.id, in two parts: pair_near (owners,
+// family mask, double-precision overlap of the expanded radii) and pair_bins (the contact point's bin inside both
+// spheres' bin ranges).  The roles matter, because the contact point is formed from B's side exactly as the
+// reference forms it.
+__device__ __forceinline__ bool pair_near(const StateView& s, const SphRec& a, const SphRec& b) {
     if (a.owner == b.owner) return false;
     if (s.masks[mask_index(a.fam, b.fam)] != 0) return false;
     // checkSpheresOverlap<double>, DEMHelperKernels.cu:195-222
     const double radA = (double)a.rf, radB = (double)b.rf;
     const double d2 = (a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y) + (a.z - b.z) * (a.z - b.z);
-    if (d2 > (radA + radB) * (radA + radB)) return false;
+    return d2 <= (radA + radB) * (radA + radB);
+}
+
+__device__ __forceinline__ bool pair_bins(const SimConsts& k, const SphRec& a, const SphRec& b) {
+    const double radA = (double)a.rf, radB = (double)b.rf;
+    const double d2 = (a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y) + (a.z - b.z) * (a.z - b.z);
     float nx = (float)(a.x - b.x), ny = (float)(a.y - b.y), nz = (float)(a.z - b.z);
     normalize_f(nx, ny, nz);
     const double half = (radA + radB - sqrt(d2)) / 2.0;
@@ -233,6 +240,17 @@ __device__ __forceinline__ bool pair_exact(const SimConsts& k, const StateView& 
     const uint32_t bx = sat_u32(cpx / k.bin_size), by = sat_u32(cpy / k.bin_size), bz = sat_u32(cpz / k.bin_size);
     return in_range(bx, a.rng.x) && in_range(by, a.rng.y) && in_range(bz, a.rng.z) && in_range(bx, b.rng.x) &&
            in_range(by, b.rng.y) && in_range(bz, b.rng.z);
+}
+
+__device__ __forceinline__ bool pair_exact(const SimConsts& k, const StateView& s, const SphRec& a, const SphRec& b) {
+    return pair_near(s, a, b) && pair_bins(k, a, b);
+}
+
+// Orders two records by sphere id (selects instead of branching, so a warp runs the test once).
+__device__ __forceinline__ void order_pair(const SphRec& me, const SphRec& ot, SphRec& a, SphRec& b) {
+    const bool lower = me.id < ot.id;
+    a = lower ? me : ot;
+    b = lower ? ot : me;
 }
 
 // Cells the neighbours of a sphere can live in.  Cell coordinates come from cell_of (a multiply by the
@@ -260,25 +278,52 @@ __device__ __forceinline__ SearchBox search_box(const SimConsts& k, double x, do
 // after i's own row in cell order (all of their cells in the box), and in i's own row the spheres after i.  Every
 // unordered pair of spheres within reach is visited exactly once, by the sphere that comes first in cell order.
 // `visit(j)` receives the cell-order index of each candidate that passes the float pre-filter.
+#ifndef DEME_FIND_UNROLL
+#define DEME_FIND_UNROLL 4
+#endif
 template <typename Visit>
 __device__ __forceinline__ void for_each_forward_candidate(const SimConsts& k, const CDView& cd, uint32_t i,
                                                            const float4 fA, const SearchBox& b, float lim2,
                                                            Visit visit) {
-    for (uint32_t cz = max(b.z0, b.cz); cz <= b.z1; cz++) {
-        for (uint32_t cy = (cz == b.cz) ? max(b.y0, b.cy) : b.y0; cy <= b.y1; cy++) {
-            const uint32_t rowBase = k.gx * (cy + k.gy * cz);
-            const bool own = (cz == b.cz) && (cy == b.cy);
-            const uint32_t j0 = own ? i + 1u : __ldg(cd.cellStart + rowBase + b.x0);
-            uint32_t j1 = __ldg(cd.cellStart + rowBase + b.x1 + 1);
-            if (!index_ok(k.err, 2, j1, (uint64_t)k.n_spheres + 1)) j1 = j0;
-            for (uint32_t j = j0; j < j1; j++) {
-                const float4 fB = __ldg(cd.posFSorted + j);
-                const float dx = fA.x - fB.x, dy = fA.y - fB.y, dz = fA.z - fB.z;
+    constexpr uint32_t U = DEME_FIND_UNROLL;
+    // Rows in order: i's own row (from i + 1), the rest of its z layer, then the later layers.  The next row's
+    // bounds are fetched before the current row is tested, and each row's candidates are loaded U at a time, so
+    // several loads are in flight per lane.
+    uint32_t cy = b.cy, cz = b.cz;
+    uint32_t j0 = i + 1u;
+    uint32_t j1 = __ldg(cd.cellStart + k.gx * (cy + k.gy * cz) + b.x1 + 1);
+    while (true) {
+        uint32_t ny = cy + 1u, nz = cz;
+        if (ny > b.y1) {
+            ny = b.y0;
+            nz++;
+        }
+        const bool more = nz <= b.z1;
+        uint32_t nj0 = 0, nj1 = 0;
+        if (more) {
+            const uint32_t rowBase = k.gx * (ny + k.gy * nz);
+            nj0 = __ldg(cd.cellStart + rowBase + b.x0);
+            nj1 = __ldg(cd.cellStart + rowBase + b.x1 + 1);
+        }
+        if (!index_ok(k.err, 2, j1, (uint64_t)k.n_spheres + 1)) j1 = j0;
+        for (uint32_t j = j0; j < j1; j += U) {
+            float4 f[U];
+#pragma unroll
+            for (uint32_t u = 0; u < U; u++)
+                f[u] = (j + u < j1) ? __ldg(cd.posFSorted + j + u) : make_float4(1e30f, 1e30f, 1e30f, 0.f);
+#pragma unroll
+            for (uint32_t u = 0; u < U; u++) {
+                const float dx = fA.x - f[u].x, dy = fA.y - f[u].y, dz = fA.z - f[u].z;
                 // explicit fused multiply-adds: the pre-filter only has to be conservative, its margin covers them
                 const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
-                if (d2 <= lim2) visit(j);
+                if (d2 <= lim2) visit(j + u);  // padding lanes sit 1e30 away and never pass
             }
         }
+        if (!more) break;
+        cy = ny;
+        cz = nz;
+        j0 = nj0;
+        j1 = nj1;
     }
 }
 
@@ -315,11 +360,24 @@ __device__ __forceinline__ void append_pairs(const CDView& cd, bool hit, uint32_
 constexpr uint32_t kSurv = 16;
 constexpr uint32_t kFindWarps = 4;
 
-__global__ void __launch_bounds__(kFindWarps * 32, 8) k_pair_find(SimConsts k, StateView s, CDView cd,
+// Lane that owns pooled pair p: the last lane whose survivor prefix is <= p.
+__device__ __forceinline__ uint32_t pool_owner(const uint32_t* pre, uint32_t p) {
+    uint32_t L = 0;
+#pragma unroll
+    for (uint32_t step = 16; step > 0; step >>= 1)
+        if (pre[L + step] <= p) L += step;
+    return L;
+}
+
+#ifndef DEME_FIND_MIN_BLOCKS
+#define DEME_FIND_MIN_BLOCKS 8
+#endif
+__global__ void __launch_bounds__(kFindWarps * 32, DEME_FIND_MIN_BLOCKS) k_pair_find(SimConsts k, StateView s, CDView cd,
                                                                   uint32_t tempCap) {
     __shared__ uint32_t s_pre[kFindWarps][33];          // survivor prefix over lanes
     __shared__ uint32_t s_surv[kFindWarps][kSurv][32];  // survivors, [slot][lane]
     __shared__ SphRec s_ctx[kFindWarps][32];
+    __shared__ uint16_t s_pass[kFindWarps][32 * kSurv];  // pooled pairs that passed pair_near
     const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     bool valid = i < k.n_spheres;
@@ -350,28 +408,37 @@ __global__ void __launch_bounds__(kFindWarps * 32, 8) k_pair_find(SimConsts k, S
     s_pre[w][lane + 1] = incl;
     if (lane == 0) s_pre[w][0] = 0;
     __syncwarp();
-    // exact reference predicate on pooled pairs, all lanes busy
+    // exact reference predicate on pooled pairs, all lanes busy; first the cheap part, whose survivors (about a
+    // third) are pooled again for the contact-point bin test
+    uint32_t nPass = 0;
     for (uint32_t base = 0; base < totalSurv; base += 32) {
         const uint32_t p = base + lane;
+        bool pass = false;
+        if (p < totalSurv) {
+            const uint32_t L = pool_owner(s_pre[w], p);
+            const SphRec ot = load_rec(k, cd, s_surv[w][p - s_pre[w][L]][L]);
+            SphRec a, b;
+            order_pair(s_ctx[w][L], ot, a, b);
+            pass = pair_near(s, a, b);
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, pass);
+        if (pass) s_pass[w][nPass + __popc(m & ((1u << lane) - 1u))] = (uint16_t)p;
+        nPass += __popc(m);
+    }
+    __syncwarp();
+    for (uint32_t base = 0; base < nPass; base += 32) {
+        const uint32_t q = base + lane;
         bool hit = false;
         uint32_t A = 0, B = 0;
-        if (p < totalSurv) {
-            uint32_t L = 0;  // owning lane: last lane whose prefix is <= p
-#pragma unroll
-            for (uint32_t step = 16; step > 0; step >>= 1)
-                if (s_pre[w][L + step] <= p) L += step;
-            const uint32_t j = s_surv[w][p - s_pre[w][L]][L];
-            const SphRec me = s_ctx[w][L];
-            const SphRec ot = load_rec(k, cd, j);
-            if (me.id < ot.id) {
-                hit = pair_exact(k, s, me, ot);
-                A = me.id;
-                B = ot.id;
-            } else {
-                hit = pair_exact(k, s, ot, me);
-                A = ot.id;
-                B = me.id;
-            }
+        if (q < nPass) {
+            const uint32_t p = s_pass[w][q];
+            const uint32_t L = pool_owner(s_pre[w], p);
+            const SphRec ot = load_rec(k, cd, s_surv[w][p - s_pre[w][L]][L]);
+            SphRec a, b;
+            order_pair(s_ctx[w][L], ot, a, b);
+            hit = pair_bins(k, a, b);
+            A = a.id;
+            B = b.id;
             if (hit && !index_ok(k.err, 14, A, k.n_spheres)) hit = false;
         }
         append_pairs(cd, hit, A, B, tempCap);
@@ -399,10 +466,10 @@ __global__ void __launch_bounds__(128) k_pair_overflow(SimConsts k, StateView s,
         const SphRec me = load_rec(k, cd, i);
         const SearchBox b = search_box(k, me.x, me.y, me.z, me.rf);
         for_each_forward_candidate(k, cd, i, fA, b, prefilter_lim2(k, me.rf), [&](uint32_t j) {
-            const SphRec ot = load_rec(k, cd, j);
-            const bool lower = me.id < ot.id;
-            if (!(lower ? pair_exact(k, s, me, ot) : pair_exact(k, s, ot, me))) return;
-            const uint32_t A = lower ? me.id : ot.id, B = lower ? ot.id : me.id;
+            SphRec a, b;
+            order_pair(me, load_rec(k, cd, j), a, b);
+            if (!pair_exact(k, s, a, b)) return;
+            const uint32_t A = a.id, B = b.id;
             if (!index_ok(k.err, 14, A, k.n_spheres)) return;
             const uint32_t pos = atomicAdd(&cd.counters[0], 1u);
             if (pos < tempCap) cd.candTemp[pos] = make_uint2(A, B);
