@@ -468,11 +468,22 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
     TRY(dalloc_n(h, &cd.pZ, nS));
     TRY(dalloc_n(h, &cd.posF, nS));
     TRY(dalloc_n(h, &cd.posFSorted, nS));
-    TRY(dalloc_n(h, &cd.pXs, nS));
-    TRY(dalloc_n(h, &cd.pYs, nS));
-    TRY(dalloc_n(h, &cd.pZs, nS));
-    TRY(dalloc_n(h, &cd.metaS, nS));
+    TRY(dalloc_n(h, &cd.recS, nS));
     TRY(dalloc_n(h, &cd.rngS, nS));
+    {
+        // runs of consecutive spheres sharing an owner: the search skips them by id
+        uint2* dClump = nullptr;
+        TRY(dalloc_n(h, &dClump, std::max(nS, 1u)));
+        std::vector<uint2> runs(nS);
+        for (uint32_t i = 0; i < nS;) {
+            uint32_t e = i + 1;
+            while (e < nS && s->sphere_owner[e] == s->sphere_owner[i]) e++;
+            for (uint32_t q = i; q < e; q++) runs[q] = make_uint2(i, e - i);
+            i = e;
+        }
+        if (nS) CUDA_TRY(h, cudaMemcpy(dClump, runs.data(), nS * sizeof(uint2), cudaMemcpyHostToDevice));
+        cd.sClump = dClump;
+    }
     TRY(dalloc_n(h, &cd.cellKey, nS));
     TRY(dalloc_n(h, &cd.idSeq, nS));
     TRY(dalloc_n(h, &cd.keySorted, nS));

@@ -140,7 +140,8 @@ __device__ __forceinline__ bool in_range(uint32_t b, uint32_t packed) {
 }
 
 // Cell-order copies of everything the contact search reads, so that a warp (neighbouring cells) reads contiguous
-// memory: position + id for the pre-filter, exact position and (owner, radius, family) for the exact test.
+// memory: position + id for the pre-filter, one 32-byte record (exact position, owner, expanded radius) for the
+// overlap test, bin ranges + family for the contact-point test.
 __global__ void k_gather_sorted(SimConsts k, StateView s, CDView cd) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= k.n_spheres) return;
@@ -148,20 +149,28 @@ __global__ void k_gather_sorted(SimConsts k, StateView s, CDView cd) {
     if (!index_ok(k.err, 1, j, k.n_spheres)) return;
     const float4 p = cd.posF[j];
     cd.posFSorted[i] = make_float4(p.x, p.y, p.z, __uint_as_float(j));
-    cd.pXs[i] = cd.pX[j];
-    cd.pYs[i] = cd.pY[j];
-    cd.pZs[i] = cd.pZ[j];
+    const double X = cd.pX[j], Y = cd.pY[j], Z = cd.pZ[j];
     const uint32_t o = s.sOwner[j];
     const float r = s.sph[j].w;
-    cd.metaS[i] = make_uint4(o, __float_as_uint(r), s.loc[o].w, 0u);
+    float rf = r;
+    rf += k.beta;
+    SphCD rec;
+    rec.x = X;
+    rec.y = Y;
+    rec.z = Z;
+    rec.owner = o;
+    rec.rf = rf;
+    cd.recS[i] = rec;
     // bin ranges of the expanded sphere (reference arithmetic), packed 16 bits per bound
     double rD = (double)r;
     rD += (double)k.beta;
     uint32_t lo[3], hi[3];
-    bin_range(cd.pX[j], rD, k.bin_size, lo[0], hi[0]);
-    bin_range(cd.pY[j], rD, k.bin_size, lo[1], hi[1]);
-    bin_range(cd.pZ[j], rD, k.bin_size, lo[2], hi[2]);
-    cd.rngS[i] = pack_ranges(lo, hi);
+    bin_range(X, rD, k.bin_size, lo[0], hi[0]);
+    bin_range(Y, rD, k.bin_size, lo[1], hi[1]);
+    bin_range(Z, rD, k.bin_size, lo[2], hi[2]);
+    uint4 g = pack_ranges(lo, hi);
+    g.w = s.loc[o].w;
+    cd.rngS[i] = g;
 }
 
 // Counting sort of the spheres by home cell (a radix sort whose single digit spans the cell range): the histogram
@@ -198,36 +207,40 @@ struct SphRec {
     float rf;  // expanded radius (radius + beta) in float, as the reference forms it
 };
 
-__device__ __forceinline__ SphRec load_rec(const SimConsts& k, const CDView& cd, uint32_t j) {
+// Exact position, owner and expanded radius of cell-order sphere j (what the overlap test needs).
+__device__ __forceinline__ void load_near(const CDView& cd, uint32_t j, SphRec& r) {
+    const double2 xy = __ldg(reinterpret_cast<const double2*>(cd.recS) + 2 * (size_t)j);
+    const uint4 zr = __ldg(reinterpret_cast<const uint4*>(cd.recS) + 2 * (size_t)j + 1);
+    r.x = xy.x;
+    r.y = xy.y;
+    r.z = __hiloint2double((int)zr.y, (int)zr.x);
+    r.owner = zr.z;
+    r.rf = __uint_as_float(zr.w);
+}
+
+__device__ __forceinline__ SphRec load_rec(const CDView& cd, uint32_t j) {
     SphRec r;
-    r.x = cd.pXs[j];
-    r.y = cd.pYs[j];
-    r.z = cd.pZs[j];
-    const uint4 m = cd.metaS[j];
-    r.owner = m.x;
-    r.fam = m.z;
-    float rf = __uint_as_float(m.y);
-    rf += k.beta;
-    r.rf = rf;
-    r.rng = cd.rngS[j];
+    load_near(cd, j, r);
+    r.rng = __ldg(cd.rngS + j);
+    r.fam = r.rng.w;
     r.id = __float_as_uint(__ldg(&cd.posFSorted[j].w));
     return r;
 }
 
 // The reference's pair predicate (see the file comment) with a.id < b.id, in two parts: pair_near (owners,
-// family mask, double-precision overlap of the expanded radii) and pair_bins (the contact point's bin inside both
+// double-precision overlap of the expanded radii) and pair_bins (family mask, the contact point's bin inside both
 // spheres' bin ranges).  The roles matter, because the contact point is formed from B's side exactly as the
 // reference forms it.
-__device__ __forceinline__ bool pair_near(const StateView& s, const SphRec& a, const SphRec& b) {
+__device__ __forceinline__ bool pair_near(const SphRec& a, const SphRec& b) {
     if (a.owner == b.owner) return false;
-    if (s.masks[mask_index(a.fam, b.fam)] != 0) return false;
-    // checkSpheresOverlap<double>, DEMHelperKernels.cu:195-222
+    // checkSpheresOverlap<double>, DEMHelperKernels.cu:195-222 (symmetric in a and b to the last bit)
     const double radA = (double)a.rf, radB = (double)b.rf;
     const double d2 = (a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y) + (a.z - b.z) * (a.z - b.z);
     return d2 <= (radA + radB) * (radA + radB);
 }
 
-__device__ __forceinline__ bool pair_bins(const SimConsts& k, const SphRec& a, const SphRec& b) {
+__device__ __forceinline__ bool pair_bins(const SimConsts& k, const StateView& s, const SphRec& a, const SphRec& b) {
+    if (s.masks[mask_index(a.fam, b.fam)] != 0) return false;
     const double radA = (double)a.rf, radB = (double)b.rf;
     const double d2 = (a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y) + (a.z - b.z) * (a.z - b.z);
     float nx = (float)(a.x - b.x), ny = (float)(a.y - b.y), nz = (float)(a.z - b.z);
@@ -243,7 +256,7 @@ __device__ __forceinline__ bool pair_bins(const SimConsts& k, const SphRec& a, c
 }
 
 __device__ __forceinline__ bool pair_exact(const SimConsts& k, const StateView& s, const SphRec& a, const SphRec& b) {
-    return pair_near(s, a, b) && pair_bins(k, a, b);
+    return pair_near(a, b) && pair_bins(k, s, a, b);
 }
 
 // Orders two records by sphere id (selects instead of branching, so a warp runs the test once).
@@ -277,14 +290,15 @@ __device__ __forceinline__ SearchBox search_box(const SimConsts& k, double x, do
 // Visits every candidate j of sphere i (cell-order index) in the FORWARD half of its neighbourhood: rows of cells
 // after i's own row in cell order (all of their cells in the box), and in i's own row the spheres after i.  Every
 // unordered pair of spheres within reach is visited exactly once, by the sphere that comes first in cell order.
-// `visit(j)` receives the cell-order index of each candidate that passes the float pre-filter.
+// `visit(j)` receives the cell-order index of each candidate that passes the float pre-filter and lies outside
+// the run of sphere ids `clump` (first, count) that shares i's owner (such pairs are never contacts).
 #ifndef DEME_FIND_UNROLL
 #define DEME_FIND_UNROLL 4
 #endif
 template <typename Visit>
 __device__ __forceinline__ void for_each_forward_candidate(const SimConsts& k, const CDView& cd, uint32_t i,
                                                            const float4 fA, const SearchBox& b, float lim2,
-                                                           Visit visit) {
+                                                           uint2 clump, Visit visit) {
     constexpr uint32_t U = DEME_FIND_UNROLL;
     // Rows in order: i's own row (from i + 1), the rest of its z layer, then the later layers.  The next row's
     // bounds are fetched before the current row is tested, and each row's candidates are loaded U at a time, so
@@ -316,7 +330,8 @@ __device__ __forceinline__ void for_each_forward_candidate(const SimConsts& k, c
                 const float dx = fA.x - f[u].x, dy = fA.y - f[u].y, dz = fA.z - f[u].z;
                 // explicit fused multiply-adds: the pre-filter only has to be conservative, its margin covers them
                 const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
-                if (d2 <= lim2) visit(j + u);  // padding lanes sit 1e30 away and never pass
+                // padding lanes sit 1e30 away and never pass; spheres of i's own clump are skipped by id
+                if (d2 <= lim2 && __float_as_uint(f[u].w) - clump.x >= clump.y) visit(j + u);
             }
         }
         if (!more) break;
@@ -384,13 +399,13 @@ __global__ void __launch_bounds__(kFindWarps * 32, DEME_FIND_MIN_BLOCKS) k_pair_
     uint32_t nSurv = 0;
     if (valid) {
         const float4 fA = __ldg(cd.posFSorted + i);
-        const SphRec me = load_rec(k, cd, i);
+        const SphRec me = load_rec(cd, i);
         if (!index_ok(k.err, 12, me.id, k.n_spheres)) {
             valid = false;
         } else {
             s_ctx[w][lane] = me;
             const SearchBox b = search_box(k, me.x, me.y, me.z, me.rf);
-            for_each_forward_candidate(k, cd, i, fA, b, prefilter_lim2(k, me.rf), [&](uint32_t j) {
+            for_each_forward_candidate(k, cd, i, fA, b, prefilter_lim2(k, me.rf), __ldg(cd.sClump + me.id), [&](uint32_t j) {
                 if (nSurv < kSurv) s_surv[w][nSurv][lane] = j;
                 nSurv++;
             });
@@ -416,10 +431,9 @@ __global__ void __launch_bounds__(kFindWarps * 32, DEME_FIND_MIN_BLOCKS) k_pair_
         bool pass = false;
         if (p < totalSurv) {
             const uint32_t L = pool_owner(s_pre[w], p);
-            const SphRec ot = load_rec(k, cd, s_surv[w][p - s_pre[w][L]][L]);
-            SphRec a, b;
-            order_pair(s_ctx[w][L], ot, a, b);
-            pass = pair_near(s, a, b);
+            SphRec ot;
+            load_near(cd, s_surv[w][p - s_pre[w][L]][L], ot);
+            pass = pair_near(s_ctx[w][L], ot);
         }
         const uint32_t m = __ballot_sync(0xffffffffu, pass);
         if (pass) s_pass[w][nPass + __popc(m & ((1u << lane) - 1u))] = (uint16_t)p;
@@ -433,10 +447,10 @@ __global__ void __launch_bounds__(kFindWarps * 32, DEME_FIND_MIN_BLOCKS) k_pair_
         if (q < nPass) {
             const uint32_t p = s_pass[w][q];
             const uint32_t L = pool_owner(s_pre[w], p);
-            const SphRec ot = load_rec(k, cd, s_surv[w][p - s_pre[w][L]][L]);
+            const SphRec ot = load_rec(cd, s_surv[w][p - s_pre[w][L]][L]);
             SphRec a, b;
             order_pair(s_ctx[w][L], ot, a, b);
-            hit = pair_bins(k, a, b);
+            hit = pair_bins(k, s, a, b);
             A = a.id;
             B = b.id;
             if (hit && !index_ok(k.err, 14, A, k.n_spheres)) hit = false;
@@ -463,11 +477,11 @@ __global__ void __launch_bounds__(128) k_pair_overflow(SimConsts k, StateView s,
         const uint32_t i = cd.ovf[o];
         if (!index_ok(k.err, 13, i, k.n_spheres)) continue;
         const float4 fA = __ldg(cd.posFSorted + i);
-        const SphRec me = load_rec(k, cd, i);
+        const SphRec me = load_rec(cd, i);
         const SearchBox b = search_box(k, me.x, me.y, me.z, me.rf);
-        for_each_forward_candidate(k, cd, i, fA, b, prefilter_lim2(k, me.rf), [&](uint32_t j) {
+        for_each_forward_candidate(k, cd, i, fA, b, prefilter_lim2(k, me.rf), __ldg(cd.sClump + me.id), [&](uint32_t j) {
             SphRec a, b;
-            order_pair(me, load_rec(k, cd, j), a, b);
+            order_pair(me, load_rec(cd, j), a, b);
             if (!pair_exact(k, s, a, b)) return;
             const uint32_t A = a.id, B = b.id;
             if (!index_ok(k.err, 14, A, k.n_spheres)) return;

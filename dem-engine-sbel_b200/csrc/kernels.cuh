@@ -36,6 +36,13 @@ struct AnalRaw {
     double c1, c2;
 };
 
+// Cell-order record of one sphere for the exact pair test: 32 bytes, read as two 16-byte loads.
+struct __align__(16) SphCD {
+    double x, y, z;
+    uint32_t owner;
+    float rf;  // radius + beta, added in float as the reference does
+};
+
 // Contact-detection work arrays.
 struct CDView {
     double* pX;
@@ -43,11 +50,9 @@ struct CDView {
     double* pZ;
     float4* posF;        // ID order: (x, y, z, CD radius)
     float4* posFSorted;  // cell order: (x, y, z, sphere id bits)
-    double* pXs;         // cell order: exact position
-    double* pYs;
-    double* pZs;
-    uint4* metaS;        // cell order: (owner, radius bits, family, 0)
-    uint4* rngS;         // cell order: bin ranges of the expanded sphere, (lo | hi << 16) per axis
+    SphCD* recS;         // cell order: exact position, owner, expanded radius
+    uint4* rngS;         // cell order: bin ranges of the expanded sphere, (lo | hi << 16) per axis; family in .w
+    const uint2* sClump; // ID order: (first sphere, count) of the run of consecutive spheres sharing the owner
     uint32_t* cellKey;
     uint32_t* idSeq;
     uint32_t* keySorted;
