@@ -645,8 +645,15 @@ void launch_count_by_sphere(const uint32_t* idA, uint32_t n, uint32_t* cnt, cuda
 
 // ------------------------------------------------------------------------------------------------------------
 // Fused force + collection kernel.
+#ifndef DEME_FORCE_THREADS
+#define DEME_FORCE_THREADS 256
+#endif
+#ifndef DEME_FORCE_MIN_BLOCKS
+#define DEME_FORCE_MIN_BLOCKS 4
+#endif
+constexpr uint32_t kForceThreads = DEME_FORCE_THREADS;
 template <bool kStore>
-__global__ void __launch_bounds__(256, 3) k_force(SimConsts k, StateView s, ContactView c, uint32_t n, bool has_hist,
+__global__ void __launch_bounds__(kForceThreads, DEME_FORCE_MIN_BLOCKS) k_force(SimConsts k, StateView s, ContactView c, uint32_t n, bool has_hist,
                                                ContactOutputs out, AnalAccum aa) {
     // analytical owners (walls) collect their reactions block-locally, then one fixed-order reduction
     extern __shared__ float s_anal[];  // 6 floats per analytical owner
@@ -857,14 +864,14 @@ __global__ void k_anal_reduce(AnalAccum aa, uint32_t nBlocks, float4* acc, float
 void launch_force(const SimConsts& k, const StateView& s, const ContactView& c, uint32_t n, bool has_hist,
                   const ContactOutputs* out, const AnalAccum& aa, cudaStream_t st) {
     if (!(n)) return;
-    const uint32_t nb = blocks_for(n, 256);
+    const uint32_t nb = blocks_for(n, kForceThreads);
     const size_t smem = 6u * aa.nAO * sizeof(float);
     {
         ProfScope prof_(KID_FORCE, st);
         if (out)
-            k_force<true><<<nb, 256, smem, st>>>(k, s, c, n, has_hist, *out, aa);
+            k_force<true><<<nb, kForceThreads, smem, st>>>(k, s, c, n, has_hist, *out, aa);
         else
-            k_force<false><<<nb, 256, smem, st>>>(k, s, c, n, has_hist, ContactOutputs{}, aa);
+            k_force<false><<<nb, kForceThreads, smem, st>>>(k, s, c, n, has_hist, ContactOutputs{}, aa);
     }
     if (aa.nAO) {
         ProfScope prof_(KID_OTHER, st);
@@ -872,7 +879,7 @@ void launch_force(const SimConsts& k, const StateView& s, const ContactView& c, 
     }
 }
 
-uint32_t force_blocks(uint32_t n) { return blocks_for(n, 256); }
+uint32_t force_blocks(uint32_t n) { return blocks_for(n, kForceThreads); }
 
 // ------------------------------------------------------------------------------------------------------------
 // integrateOwners (src/kernel/DEMIntegrationKernels.cu:46-179) with the constant prescription table.
