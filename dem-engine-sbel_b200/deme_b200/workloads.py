@@ -97,14 +97,15 @@ def triangle_template(rng, r_nom: float, rho: float, n_mc: int = 20000):
 
 def drum(n_clumps: int = 1_000_000, r_nom: float = 2e-3, rho: float = 2500.0, n_templates: int = 64,
          fill: float = 0.30, packing: float = 0.6, rpm: float = 20.0, dt: float = 5e-6, seed: int = 2,
-         shell: bool = False, spacing: float = 1.02):
+         shell: bool = False, spacing: float = 1.02, wall_clearance: float = 1.05):
     """Rotating drum of three-sphere clumps (analytical cylinder + two end planes, prescribed rotation).
 
     One million clumps of about 8e-8 m^3 do not fit a 30 % fill of an R = 0.25 m, L = 0.3 m drum, so the drum is
     scaled (same L / R ratio) until the clumps at ``packing`` bulk density fill ``fill`` of its volume.
     Clumps start on a loose lattice in the lower part of the drum with random orientations.  ``spacing`` is the
     lattice pitch over the clump's bounding diameter: above 1 no two clumps touch; below 1 neighbouring clumps
-    interpenetrate, which gives a dense bed without settling (used to size CPU samples).
+    interpenetrate, which gives a dense bed without settling (used to size CPU samples).  Lattice sites stay
+    ``wall_clearance`` clump reaches inside the walls; below 1 the outer clumps start in contact with them.
     """
     rng = np.random.default_rng(seed)
     tmpl = [triangle_template(rng, r_nom, rho) for _ in range(n_templates)]
@@ -135,7 +136,8 @@ def drum(n_clumps: int = 1_000_000, r_nom: float = 2e-3, rho: float = 2500.0, n_
     py = -L / 2 + J * dy + np.where(K % 2 == 0, 0.0, dy / 3)
     pz = -R + K * dz
     P = np.stack([px.ravel(), py.ravel(), pz.ravel()], axis=1)
-    inside = (P[:, 0] ** 2 + P[:, 2] ** 2 <= (R - reach * 1.05) ** 2) & (np.abs(P[:, 1]) <= L / 2 - reach * 1.05)
+    c = reach * wall_clearance
+    inside = (P[:, 0] ** 2 + P[:, 2] ** 2 <= (R - c) ** 2) & (np.abs(P[:, 1]) <= L / 2 - c)
     P = P[inside]
     P = P[np.argsort(P[:, 2], kind="stable")]
     if len(P) < n_clumps:
@@ -208,4 +210,87 @@ def packed_clumps(n_clumps: int = 600, r: float = 4e-3, spacing: float = 1.55, s
         s.SetExpandFactor(beta)
     built = s.Initialize()
     built.info.update(workload="packed_clumps", seed=seed)
+    return built
+
+
+def hopper(n: int = 4_000_000, r_median: float = 1.5e-3, sigma: float = 0.25, r_clip=(0.75e-3, 3e-3),
+           rho: float = 2500.0, half_angle_deg: float = 30.0, outlet: float = 0.04, n_classes: int = 64,
+           seed: int = 4, dt: float = 2e-6, cd_freq: int = 5, margin: float | None = None, closed: bool = True,
+           wall_clearance: float = 1.02, packing_seed_jitter: float = 0.9):
+    """Conical hopper of log-normal polydisperse spheres (analytical cone + outlet gate + catch floor).
+
+    Radii are log-normal (median ``r_median``, ``sigma``) clipped to ``r_clip`` and grouped into ``n_classes``
+    sphere types (one template per class, as a reference scene would load them).  Spheres start on a
+    hexagonal lattice of pitch 2 r_max filling the cone from the outlet up, each displaced randomly inside its own
+    lattice cell (no overlaps): a seeded random packing that needs no insertion loop.  The hopper height follows
+    from n.  The gate (family 2) closes the outlet while ``closed``; the floor 0.1 m below catches discharge.
+    Contact detection runs every ``cd_freq`` steps with the contact margin ``margin`` (default 0.1 r_median).
+    ``wall_clearance`` below 1 starts the outer spheres pressed into the walls (used by parity tests).
+    """
+    rng = np.random.default_rng(seed)
+    th = math.radians(half_angle_deg)
+    tan_t, cos_t = math.tan(th), math.cos(th)
+    r = np.clip(rng.lognormal(math.log(r_median), sigma, n), r_clip[0], r_clip[1])
+    edges = np.quantile(r, np.linspace(0, 1, n_classes + 1))
+    cls = np.clip(np.searchsorted(edges, r, side="right") - 1, 0, n_classes - 1)
+    r_cls = np.array([r[cls == c].mean() if np.any(cls == c) else edges[c] for c in range(n_classes)])
+    r = r_cls[cls]
+    r_max = float(r.max())
+    a = 2.0 * r_max * 1.01
+    u_out = (outlet / 2) / tan_t  # axial distance from the apex to the outlet
+    dy, dz = a * math.sqrt(3.0) / 2.0, a * math.sqrt(2.0 / 3.0)
+    u_top = u_out + 10 * a
+    while True:
+        R_top = u_top * tan_t
+        nx, ny, nz = int(2 * R_top / a) + 2, int(2 * R_top / dy) + 2, int((u_top - u_out) / dz) + 2
+        K, J, I = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+        px = -R_top + I * a + np.where((J + K) % 2 == 0, 0.0, a / 2)
+        py = -R_top + J * dy + np.where(K % 2 == 0, 0.0, dy / 3)
+        pz = u_out + r_max + K * dz
+        P = np.stack([px.ravel(), py.ravel(), pz.ravel()], axis=1)
+        rho_ = np.hypot(P[:, 0], P[:, 1])
+        clear = wall_clearance * r_max / cos_t
+        ok = (rho_ <= P[:, 2] * tan_t - clear) & (P[:, 2] <= u_top - r_max)
+        if ok.sum() >= n:
+            break
+        u_top *= 1.15
+    P = P[ok]
+    P = P[np.argsort(P[:, 2], kind="stable")][:n]
+    # random displacement inside each lattice cell, bounded so that no two spheres overlap
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    d *= (rng.random(n) * packing_seed_jitter * np.maximum(a / 2 - r, 0.0))[:, None]
+    P = P + d
+    z_floor = -0.1
+    s = SceneBuilder()
+    side = 2 * (u_top * tan_t) + 8 * r_max
+    height = u_top - z_floor + 8 * r_max
+    box = max(side, height)
+    s.InstructBoxDomainDimension(box, box, box)
+    # place the apex so that the floor sits 4 r_max above the domain's bottom face
+    s.SetCoordSysOrigin("center")
+    shift = -box / 2 + 4 * r_max - z_floor
+    mat = s.LoadMaterial({"E": 1e8, "nu": 0.3, "CoR": 0.4, "mu": 0.5, "Crr": 0.0})
+    types = [s.LoadSphereType(sphere_mass(float(rc), rho), float(rc), mat) for rc in r_cls]
+    pos = P + np.array([0.0, 0.0, shift])
+    b = s.AddClumps([types[c] for c in cls], pos.astype(f32))
+    b.SetFamily(0)
+    wall = s.AddExternalObject()
+    wall.AddCone((0.0, 0.0, shift), (0.0, 0.0, 1.0), th, u_out, u_top, mat)
+    wall.SetFamily(1)
+    floor = s.AddBCPlane((0.0, 0.0, shift + z_floor), (0.0, 0.0, 1.0), mat)
+    floor.SetFamily(1)
+    if closed:
+        gate = s.AddBCPlane((0.0, 0.0, shift + u_out), (0.0, 0.0, 1.0), mat)
+        gate.SetFamily(2)
+        s.SetFamilyFixed(2)
+    s.SetFamilyFixed(1)
+    s.SetInitTimeStep(dt)
+    s.SetGravitationalAcceleration((0, 0, -9.81))
+    s.SetCDUpdateFreq(cd_freq)
+    s.SetExpandFactor(0.1 * r_median if margin is None else margin)
+    s.SetInitBinSize(2.0 * float(r.min()))
+    built = s.Initialize()
+    built.info.update(workload="hopper", n=n, u_out=u_out, u_top=u_top, R_top=u_top * tan_t, r_max=r_max,
+                      lattice_spacing=a, seed=seed, n_classes=n_classes, apex_z=shift)
     return built
