@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/deme_b200.h"
+#include "force_jit.cuh"
 #include "kernels.cuh"
 #include "primitives.cuh"
 
@@ -90,6 +91,7 @@ struct deme_handle {
     double t = 0.0;
     int64_t steps = 0;
     std::vector<void*> allocs;
+    UserForceKernel userForce;  // a compiled force-model string, when one is set
 
     StateView state_view() const {
         StateView s;
@@ -542,14 +544,28 @@ void deme_destroy(deme_handle* h) {
     if (h->hPresc) cudaFreeHost(h->hPresc);
     if (h->own_dt) cudaStreamDestroy(h->own_dt);
     if (h->own_kt) cudaStreamDestroy(h->own_kt);
+    release_user_force_model(h->userForce);
     delete h;
 }
 
 int32_t deme_set_force_model(deme_handle* h, const char* src, const char* const* names, int32_t n) {
     if (!h) return DEME_ERR_INVALID;
-    if (src == nullptr) return DEME_OK;
-    h->err = "custom force models need the NVRTC front end, which this build does not include yet";
-    return DEME_ERR_NVRTC;
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    if (src == nullptr) {
+        // back to the built-in frictional Hertz-Mindlin model and its four history wildcards
+        release_user_force_model(h->userForce);
+        h->nW = h->params.n_contact_wildcards;
+        return DEME_OK;
+    }
+    std::string err;
+    const int32_t rc = compile_user_force_model(src, names, n, h->userForce, err);
+    if (rc != DEME_OK) {
+        h->err = err;
+        return rc;
+    }
+    h->nW = h->userForce.n_wildcards;
+    h->outsValid = false;
+    return DEME_OK;
 }
 
 int32_t deme_set_streams(deme_handle* h, void* kT_stream, void* dT_stream) {
@@ -649,7 +665,7 @@ int32_t deme_compute_forces(deme_handle* h) {
         }
         aa.partial = h->analPartial;
     }
-    launch_force(k, s, c.view(), h->nContacts, h->nW > 0, out, aa, st);
+    launch_force(k, s, c.view(), h->nContacts, h->nW > 0, out, aa, h->userForce.lib ? &h->userForce : nullptr, st);
     TRY(check_launch(h, "force"));
     h->outsValid = out != nullptr;
     return DEME_OK;

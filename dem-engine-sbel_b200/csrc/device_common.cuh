@@ -6,8 +6,10 @@
 // The library is compiled with --fmad=false so every multiply and add rounds on its own, like the CPU oracle,
 // and float-to-integer conversions are written as explicit saturating helpers (PTX cvt semantics).
 #pragma once
+#ifndef __CUDACC_RTC__
 #include <cstdint>
 #include <cuda_runtime.h>
+#endif
 
 #include "../../include/deme_b200.h"
 

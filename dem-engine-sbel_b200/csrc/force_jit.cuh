@@ -1,0 +1,26 @@
+// force_jit.cuh -- run-time compilation of a user force-model string into the force kernel (host side).
+#pragma once
+#include <cstdint>
+#include <string>
+
+#include <cuda_runtime.h>
+
+namespace deme_b200 {
+
+// Maximum number of per-contact wildcards a force model can declare: they live in the contact's float4 history.
+constexpr int kMaxContactWildcards = 4;
+
+struct UserForceKernel {
+    cudaLibrary_t lib = nullptr;
+    cudaKernel_t kern[2] = {nullptr, nullptr};  // [0]: no per-contact outputs, [1]: stores force / contact points
+    int n_wildcards = 0;
+};
+
+// Compiles `model` (the body of a DEM-Engine force-model string) for this device with NVRTC into the force-kernel
+// template.  `names` are the per-contact wildcards; like the reference, they are assigned storage slots in sorted
+// order.  On failure returns a DEME_ERR_* code and fills `err` (the compiler log for a model that does not compile).
+int32_t compile_user_force_model(const char* model, const char* const* names, int32_t n, UserForceKernel& out,
+                                 std::string& err);
+void release_user_force_model(UserForceKernel& k);
+
+}  // namespace deme_b200

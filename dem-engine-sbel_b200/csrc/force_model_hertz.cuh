@@ -28,26 +28,29 @@ struct MaterialTable {
     const float* Crr;
 };
 
+// Contact-pair material parameters from the two materials (matProxy2ContactParam, DEMHelperKernels.cu:316-339):
+// effective Young's and shear moduli, the smaller restitution and the larger friction coefficients, with the
+// reference's double-precision intermediates.
+template <typename T>
+__device__ __forceinline__ void mat_proxy(T& E_cnt, T& G_cnt, T& CoR_cnt, T& mu_cnt, T& Crr_cnt, T E_A, T nu_A, T CoR_A,
+                                          T mu_A, T Crr_A, T E_B, T nu_B, T CoR_B, T mu_B, T Crr_B) {
+    const T invE = (T)((1. - (double)(nu_A * nu_A)) / (double)E_A + (1. - (double)(nu_B * nu_B)) / (double)E_B);
+    E_cnt = (T)(1. / (double)invE);
+    const T invG = (T)(2. * (2. - (double)nu_A) * (1. + (double)nu_A) / (double)E_A +
+                       2. * (2. - (double)nu_B) * (1. + (double)nu_B) / (double)E_B);
+    G_cnt = (T)(1. / (double)invG);
+    CoR_cnt = CoR_A < CoR_B ? CoR_A : CoR_B;
+    mu_cnt = mu_A > mu_B ? mu_A : mu_B;
+    Crr_cnt = Crr_A > Crr_B ? Crr_A : Crr_B;
+}
+
 __device__ __forceinline__ void hertz_mindlin(const ContactGeom& g, const MaterialTable& m, float ts, float3& force,
                                               float3& torque_only_force, float& delta_tan_x, float& delta_tan_y,
                                               float& delta_tan_z, float& delta_time) {
     // material proxies
     float E_cnt, G_cnt, CoR_cnt, mu_cnt, Crr_cnt;
-    {
-        const float E_A = m.E[g.matA], nu_A = m.nu[g.matA], CoR_A = m.CoR[g.matA], mu_A = m.mu[g.matA],
-                    Crr_A = m.Crr[g.matA];
-        const float E_B = m.E[g.matB], nu_B = m.nu[g.matB], CoR_B = m.CoR[g.matB], mu_B = m.mu[g.matB],
-                    Crr_B = m.Crr[g.matB];
-        const float invE =
-            (float)((1. - (double)(nu_A * nu_A)) / (double)E_A + (1. - (double)(nu_B * nu_B)) / (double)E_B);
-        E_cnt = (float)(1. / (double)invE);
-        const float invG = (float)(2. * (2. - (double)nu_A) * (1. + (double)nu_A) / (double)E_A +
-                                   2. * (2. - (double)nu_B) * (1. + (double)nu_B) / (double)E_B);
-        G_cnt = (float)(1. / (double)invG);
-        CoR_cnt = CoR_A < CoR_B ? CoR_A : CoR_B;
-        mu_cnt = mu_A > mu_B ? mu_A : mu_B;
-        Crr_cnt = Crr_A > Crr_B ? Crr_A : Crr_B;
-    }
+    mat_proxy<float>(E_cnt, G_cnt, CoR_cnt, mu_cnt, Crr_cnt, m.E[g.matA], m.nu[g.matA], m.CoR[g.matA], m.mu[g.matA],
+                     m.Crr[g.matA], m.E[g.matB], m.nu[g.matB], m.CoR[g.matB], m.mu[g.matB], m.Crr[g.matB]);
     // rotational velocity of the contact point, mapped to the global frame
     float rAx = g.ARotVel.y * g.locCPA.z - g.ARotVel.z * g.locCPA.y;
     float rAy = g.ARotVel.z * g.locCPA.x - g.ARotVel.x * g.locCPA.z;

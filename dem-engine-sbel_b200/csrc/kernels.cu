@@ -23,6 +23,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "force_jit.cuh"
+#include "force_kernel.cuh"
 #include "kernels.cuh"
 #include "profiler.cuh"
 
@@ -645,203 +647,6 @@ void launch_count_by_sphere(const uint32_t* idA, uint32_t n, uint32_t* cnt, cuda
 
 // ------------------------------------------------------------------------------------------------------------
 // Fused force + collection kernel.
-#ifndef DEME_FORCE_THREADS
-#define DEME_FORCE_THREADS 256
-#endif
-#ifndef DEME_FORCE_MIN_BLOCKS
-#define DEME_FORCE_MIN_BLOCKS 4
-#endif
-constexpr uint32_t kForceThreads = DEME_FORCE_THREADS;
-template <bool kStore>
-__global__ void __launch_bounds__(kForceThreads, DEME_FORCE_MIN_BLOCKS) k_force(SimConsts k, StateView s, ContactView c, uint32_t n, bool has_hist,
-                                               ContactOutputs out, AnalAccum aa) {
-    // analytical owners (walls) collect their reactions block-locally, then one fixed-order reduction
-    extern __shared__ float s_anal[];  // 6 floats per analytical owner
-    for (uint32_t t = threadIdx.x; t < 6u * aa.nAO; t += blockDim.x) s_anal[t] = 0.f;
-    if (aa.nAO) __syncthreads();
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = i < n;
-    uint32_t oA = 0xFFFFFFFFu, oB = 0xFFFFFFFFu;
-    bool bSphere = false;
-    float3 F = make_float3(0.f, 0.f, 0.f), T = make_float3(0.f, 0.f, 0.f);
-    float3 cpA = make_float3(0.f, 0.f, 0.f), cpB = make_float3(0.f, 0.f, 0.f);
-    float4 qA = make_float4(1.f, 0.f, 0.f, 0.f), qB = qA;
-    float mA = 1.f, mB = 1.f;
-    bool active = false;
-    bool ids_ok = valid;
-    if (valid) {
-        const int ct0 = c.type[i];
-        ids_ok = index_ok(k.err, 8, c.idA[i], k.n_spheres) &&
-                 index_ok(k.err, 9, c.idB[i], ct0 == DEME_SPHERE_SPHERE_CONTACT ? k.n_spheres : k.n_anal) &&
-                 index_ok(k.err, 10, ct0 == DEME_SPHERE_SPHERE_CONTACT || ct0 >= 3 ? 0 : 1, 1);
-    }
-    if (ids_ok) {
-        const uint32_t sA = c.idA[i];
-        const uint32_t bId = c.idB[i];
-        int ct = c.type[i];
-        float4 hw = has_hist ? c.hist[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-        ContactGeom g;
-        // body A (always a sphere)
-        oA = s.sOwner[sA];
-        const float4 spA = s.sph[sA];
-        const ushort4 lA = s.loc[oA];
-        qA = s.quat[oA];
-        const float4 vA = s.vel[oA];
-        const float4 wA = s.omg[oA];
-        double AOx, AOy, AOz;
-        voxel_to_pos(k, s.voxel[oA], lA.x, lA.y, lA.z, AOx, AOy, AOz);
-        float rx = spA.x, ry = spA.y, rz = spA.z;
-        rot_f(rx, ry, rz, qA.x, qA.y, qA.z, qA.w);
-        const double Ax = AOx + (double)rx, Ay = AOy + (double)ry, Az = AOz + (double)rz;
-        g.ARadius = spA.w;
-        g.AOwnerMass = vA.w;
-        g.matA = s.sMat[sA];
-        g.ALinVel = make_float3(vA.x, vA.y, vA.z);
-        g.ARotVel = make_float3(wA.x, wA.y, wA.z);
-        mA = vA.w;
-        double BOx, BOy, BOz, CPx = 0, CPy = 0, CPz = 0, depth = 0;
-        float nX = 0, nY = 0, nZ = 0;
-        if (ct == DEME_SPHERE_SPHERE_CONTACT) {
-            bSphere = true;
-            oB = s.sOwner[bId];
-            const float4 spB = s.sph[bId];
-            const ushort4 lB = s.loc[oB];
-            qB = s.quat[oB];
-            const float4 vB = s.vel[oB];
-            const float4 wB = s.omg[oB];
-            voxel_to_pos(k, s.voxel[oB], lB.x, lB.y, lB.z, BOx, BOy, BOz);
-            float bx = spB.x, by = spB.y, bz = spB.z;
-            rot_f(bx, by, bz, qB.x, qB.y, qB.z, qB.w);
-            const double Bx = BOx + (double)bx, By = BOy + (double)by, Bz = BOz + (double)bz;
-            g.BRadius = spB.w;
-            g.BOwnerMass = vB.w;
-            g.matB = s.sMat[bId];
-            g.BLinVel = make_float3(vB.x, vB.y, vB.z);
-            g.BRotVel = make_float3(wB.x, wB.y, wB.z);
-            mB = vB.w;
-            // checkSpheresOverlap<double, float>, DEMHelperKernels.cu:233-264
-            const double radA = (double)g.ARadius, radB = (double)g.BRadius;
-            const double d2 = (Ax - Bx) * (Ax - Bx) + (Ay - By) * (Ay - By) + (Az - Bz) * (Az - Bz);
-            if (d2 > (radA + radB) * (radA + radB)) {
-                ct = DEME_NOT_A_CONTACT;
-            } else {
-                nX = (float)(Ax - Bx);
-                nY = (float)(Ay - By);
-                nZ = (float)(Az - Bz);
-                normalize_f(nX, nY, nZ);
-                depth = radA + radB - sqrt(d2);
-                CPx = Bx + (radB - depth / 2.0) * (double)nX;
-                CPy = By + (radB - depth / 2.0) * (double)nY;
-                CPz = Bz + (radB - depth / 2.0) * (double)nZ;
-            }
-        } else {
-            const AnalPlaced a = s.anal[bId];
-            oB = a.owner;
-            const ushort4 lB = s.loc[oB];
-            qB = s.quat[oB];
-            const float4 vB = s.vel[oB];
-            const float4 wB = s.omg[oB];
-            voxel_to_pos(k, s.voxel[oB], lB.x, lB.y, lB.z, BOx, BOy, BOz);
-            g.BRadius = (float)kHugeFloat;
-            g.BOwnerMass = a.mass;
-            g.matB = a.material;
-            g.BLinVel = make_float3(vB.x, vB.y, vB.z);
-            g.BRotVel = make_float3(wB.x, wB.y, wB.z);
-            ct = anal_overlap_dt(a, Ax, Ay, Az, (double)g.ARadius, CPx, CPy, CPz, nX, nY, nZ, depth);
-        }
-        if (ct != DEME_NOT_A_CONTACT) {
-            active = true;
-            float cax = (float)(CPx - AOx), cay = (float)(CPy - AOy), caz = (float)(CPz - AOz);
-            float cbx = (float)(CPx - BOx), cby = (float)(CPy - BOy), cbz = (float)(CPz - BOz);
-            rot_f(cax, cay, caz, qA.x, -qA.y, -qA.z, -qA.w);
-            rot_f(cbx, cby, cbz, qB.x, -qB.y, -qB.z, -qB.w);
-            cpA = make_float3(cax, cay, caz);
-            cpB = make_float3(cbx, cby, cbz);
-            g.B2A = make_float3(nX, nY, nZ);
-            g.overlapDepth = depth;
-            g.locCPA = cpA;
-            g.locCPB = cpB;
-            g.AoriQ = qA;
-            g.BoriQ = qB;
-            hertz_mindlin(g, s.mat, k.h, F, T, hw.x, hw.y, hw.z, hw.w);
-        } else {
-            hw = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        if (has_hist) c.hist[i] = hw;
-        if (kStore) {
-            out.F[i] = make_float4(F.x, F.y, F.z, 0.f);
-            out.TOF[i] = make_float4(T.x, T.y, T.z, 0.f);
-            out.CPA[i] = make_float4(cpA.x, cpA.y, cpA.z, 0.f);
-            out.CPB[i] = make_float4(cpB.x, cpB.y, cpB.z, 0.f);
-        }
-    }
-    // owner contributions (forceToAcc / forceToAngAcc, src/kernel/DEMCollectForceKernels.cu:68-120)
-    float4 aA = make_float4(0.f, 0.f, 0.f, 0.f), alA = aA, aB = aA, alB = aA;
-    if (active) {
-        const float4 mi = s.moi[oA];
-        const bool bOwnerCounts = bSphere || aa.nAO;
-        aA = make_float4((F.x * 1.f) / mA, (F.y * 1.f) / mA, (F.z * 1.f) / mA, 0.f);
-        float gx = (F.x + T.x) * 1.f, gy = (F.y + T.y) * 1.f, gz = (F.z + T.z) * 1.f;
-        rot_f(gx, gy, gz, qA.x, -qA.y, -qA.z, -qA.w);
-        alA = make_float4((cpA.y * gz - cpA.z * gy) / mi.x, (cpA.z * gx - cpA.x * gz) / mi.y,
-                          (cpA.x * gy - cpA.y * gx) / mi.z, 0.f);
-        if (bOwnerCounts) {
-            const float4 mj = s.moi[oB];
-            if (!bSphere) mB = s.vel[oB].w;  // owner mass of the analytical object (massOwnerBody)
-            aB = make_float4((F.x * -1.f) / mB, (F.y * -1.f) / mB, (F.z * -1.f) / mB, 0.f);
-            float hx = (F.x + T.x) * -1.f, hy = (F.y + T.y) * -1.f, hz = (F.z + T.z) * -1.f;
-            rot_f(hx, hy, hz, qB.x, -qB.y, -qB.z, -qB.w);
-            alB = make_float4((cpB.y * hz - cpB.z * hy) / mj.x, (cpB.z * hx - cpB.x * hz) / mj.y,
-                              (cpB.x * hy - cpB.y * hx) / mj.z, 0.f);
-        }
-    }
-    // A side: contacts of one owner are adjacent (sorted by sphere id; a clump's spheres have consecutive ids).
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t key = ids_ok ? oA : 0xFFFFFFFFu;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        const uint32_t k2 = __shfl_down_sync(0xffffffffu, key, off);
-        const float x0 = __shfl_down_sync(0xffffffffu, aA.x, off);
-        const float x1 = __shfl_down_sync(0xffffffffu, aA.y, off);
-        const float x2 = __shfl_down_sync(0xffffffffu, aA.z, off);
-        const float y0 = __shfl_down_sync(0xffffffffu, alA.x, off);
-        const float y1 = __shfl_down_sync(0xffffffffu, alA.y, off);
-        const float y2 = __shfl_down_sync(0xffffffffu, alA.z, off);
-        if (lane + off < 32 && k2 == key) {
-            aA.x += x0;
-            aA.y += x1;
-            aA.z += x2;
-            alA.x += y0;
-            alA.y += y1;
-            alA.z += y2;
-        }
-    }
-    const uint32_t prevKey = __shfl_up_sync(0xffffffffu, key, 1);
-    const bool head = (lane == 0) || (prevKey != key);
-    if (head && key != 0xFFFFFFFFu) {
-        atomicAdd(&s.acc[key], aA);
-        atomicAdd(&s.alpha[key], alA);
-    }
-    if (active && bSphere) {
-        atomicAdd(&s.acc[oB], aB);
-        atomicAdd(&s.alpha[oB], alB);
-    }
-    if (aa.nAO) {
-        if (active && !bSphere && index_ok(k.err, 11, oB - aa.nClumps, aa.nAO)) {
-            float* slot = s_anal + 6u * (oB - aa.nClumps);
-            atomicAdd(slot + 0, aB.x);
-            atomicAdd(slot + 1, aB.y);
-            atomicAdd(slot + 2, aB.z);
-            atomicAdd(slot + 3, alB.x);
-            atomicAdd(slot + 4, alB.y);
-            atomicAdd(slot + 5, alB.z);
-        }
-        __syncthreads();
-        for (uint32_t t = threadIdx.x; t < 6u * aa.nAO; t += blockDim.x)
-            aa.partial[(size_t)blockIdx.x * 6u * aa.nAO + t] = s_anal[t];
-    }
-}
-
 // Sum the per-block partials of each analytical owner in block order (deterministic) into its accumulators.
 __global__ void k_anal_reduce(AnalAccum aa, uint32_t nBlocks, float4* acc, float4* alpha) {
     __shared__ float sh[256];
@@ -862,16 +667,28 @@ __global__ void k_anal_reduce(AnalAccum aa, uint32_t nBlocks, float4* acc, float
 }
 
 void launch_force(const SimConsts& k, const StateView& s, const ContactView& c, uint32_t n, bool has_hist,
-                  const ContactOutputs* out, const AnalAccum& aa, cudaStream_t st) {
+                  const ContactOutputs* out, const AnalAccum& aa, const UserForceKernel* user, cudaStream_t st) {
     if (!(n)) return;
     const uint32_t nb = blocks_for(n, kForceThreads);
     const size_t smem = 6u * aa.nAO * sizeof(float);
     {
         ProfScope prof_(KID_FORCE, st);
-        if (out)
+        if (user) {
+            // the same kernel template compiled at run time around a user force model
+            SimConsts ka = k;
+            StateView sa = s;
+            ContactView ca = c;
+            uint32_t na = n;
+            bool ha = has_hist;
+            ContactOutputs oa = out ? *out : ContactOutputs{};
+            AnalAccum aaa = aa;
+            void* args[] = {&ka, &sa, &ca, &na, &ha, &oa, &aaa};
+            cudaLaunchKernel((const void*)user->kern[out ? 1 : 0], dim3(nb), dim3(kForceThreads), args, smem, st);
+        } else if (out) {
             k_force<true><<<nb, kForceThreads, smem, st>>>(k, s, c, n, has_hist, *out, aa);
-        else
+        } else {
             k_force<false><<<nb, kForceThreads, smem, st>>>(k, s, c, n, has_hist, ContactOutputs{}, aa);
+        }
     }
     if (aa.nAO) {
         ProfScope prof_(KID_OTHER, st);

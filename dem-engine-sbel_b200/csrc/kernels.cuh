@@ -1,7 +1,9 @@
 // kernels.cuh -- device data views and host launchers of the per-step kernels.
 #pragma once
+#ifndef __CUDACC_RTC__
 #include <cstdint>
 #include <cuda_runtime.h>
+#endif
 
 #include "device_common.cuh"
 #include "force_model_hertz.cuh"
@@ -90,6 +92,7 @@ struct ContactOutputs {
     float4* CPB;
 };
 
+#ifndef __CUDACC_RTC__
 void launch_place_anal(const SimConsts& k, const StateView& s, const AnalRaw* raw, AnalPlaced* placed, uint32_t nA,
                        cudaStream_t st);
 void launch_sphere_prep(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
@@ -105,8 +108,9 @@ void launch_pair_assemble(const SimConsts& k, const StateView& s, const CDView& 
 void launch_history(const SimConsts& k, const ContactView& cur, const ContactView& prev, uint32_t n, uint32_t prevN,
                     bool has_hist, cudaStream_t st);
 void launch_count_by_sphere(const uint32_t* idA, uint32_t n, uint32_t* cnt, cudaStream_t st);
+struct UserForceKernel;
 void launch_force(const SimConsts& k, const StateView& s, const ContactView& c, uint32_t n, bool has_hist,
-                  const ContactOutputs* out, const AnalAccum& aa, cudaStream_t st);
+                  const ContactOutputs* out, const AnalAccum& aa, const UserForceKernel* user, cudaStream_t st);
 uint32_t force_blocks(uint32_t n);
 void launch_integrate(const SimConsts& k, const StateView& s, cudaStream_t st);
 void launch_kinetic_energy(const SimConsts& k, const StateView& s, uint32_t n_clumps, double* out, cudaStream_t st);
@@ -115,5 +119,6 @@ void launch_kinetic_energy(const SimConsts& k, const StateView& s, uint32_t n_cl
 void launch_bin_count(const SimConsts& k, const StateView& s, uint16_t* nBins, uint8_t* nAnal, cudaStream_t st);
 void launch_bin_emit(const SimConsts& k, const StateView& s, const uint32_t* off, uint32_t* bins, uint32_t* sph,
                      cudaStream_t st);
+#endif
 
 }  // namespace deme_b200

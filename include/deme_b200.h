@@ -220,6 +220,9 @@ typedef struct {
 
 typedef struct deme_handle deme_handle;
 
+/* The entry points (the run-time compiler of force models reads this header for its types only). */
+#ifndef __CUDACC_RTC__
+
 /* Version and error text. */
 int32_t deme_abi_version(void);
 const char* deme_status_string(int32_t status);
@@ -235,7 +238,14 @@ const char* deme_get_error(deme_handle* h);
 /* Force model.  src == NULL selects the built-in frictional Hertz-Mindlin model (FullHertzianForceModel.cu);
  * otherwise `src` is a user force-model snippet compiled with NVRTC into the force-kernel template, with the
  * given per-contact wildcard names (DefineContactForceModel, src/DEM/APIPublic.cpp:116-121;
- * DEMForceModel::SetPerContactWildcards, src/DEM/AuxClasses.cpp:256-266). */
+ * DEMForceModel::SetPerContactWildcards, src/DEM/AuxClasses.cpp:256-266).
+ * In scope, with the reference's names: force, torque_only_force (outputs), B2A, overlapDepth, contactPnt,
+ * AOwnerPos, BOwnerPos, bodyAPos, ARadius, BRadius, AOwnerMass, BOwnerMass, AoriQw..AoriQz, BoriQw..BoriQz,
+ * locCPA, locCPB, bodyAMatType, bodyBMatType, the material arrays E, nu, CoR, mu, Crr, ts, ALinVel, BLinVel,
+ * ARotVel, BRotVel, AOwnerFamily, BOwnerFamily, myContactType, myContactID, and each wildcard as a float; helpers
+ * float3 arithmetic, dot, cross, length, normalize, applyOriQToVector3, matProxy2ContactParam, deme:: constants.
+ * At most 4 wildcards (DEME_ERR_INVALID beyond).  A string that does not compile returns DEME_ERR_NVRTC and
+ * deme_get_error holds the compiler log (lines of the string are reported as "force_model_string"). */
 int32_t deme_set_force_model(deme_handle* h, const char* src, const char* const* wildcard_names, int32_t n_wildcards);
 
 /* Contact detection on the current state (kT: contactDetection, src/algorithms/DEMCubContactDetection.cu:39-397),
@@ -326,6 +336,8 @@ size_t deme_radix_sort_scratch_bytes(uint32_t n);
  *   corrupt each other's results.  Serialise them, e.g. one stream per device. */
 int32_t deme_radix_sort_pairs_static(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                                      uint32_t* vals_out, uint32_t n, int32_t key_bits, void* stream);
+
+#endif /* __CUDACC_RTC__ */
 
 #ifdef __cplusplus
 }
