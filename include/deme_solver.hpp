@@ -1,0 +1,805 @@
+/* deme_solver.hpp -- C++ DEMSolver facade over the C ABI of deme_b200.h (header-only, C++17).
+ *
+ * Keeps the scene-building and stepping API of deme::DEMSolver (src/DEM/API.h:44-887): LoadMaterial,
+ * LoadClumpType / LoadSphereType, AddClumps (DEMClumpBatch setters), AddExternalObject / AddBCPlane
+ * (DEMExternObj::AddPlane, plus AddCylinder / AddCone), the family controls, DefineContactForceModel with
+ * SetPerContactWildcards, the world and time-stepping setters, Initialize, DoDynamics / DoDynamicsThenSync /
+ * DoStepDynamics and owner-state queries.  Initialize flattens the scene exactly as the reference's host code does
+ * before its JIT step (src/DEM/APIPrivate.cpp:222-369, 574-687, 903-1048; src/DEM/dT.cpp:480-640;
+ * src/DEM/HostSideHelpers.hpp:328-350) and hands the flat arrays to deme_create.  The Python SceneBuilder
+ * (deme_b200/scene.py) implements the same flattening; tests check that the two agree array by array.
+ *
+ * Prescribed motions are constants (the reference also accepts time-dependent C expressions; a non-constant
+ * expression throws here).  Errors throw std::runtime_error with the library's message, as DEME_ERROR does.
+ */
+#ifndef DEME_SOLVER_HPP
+#define DEME_SOLVER_HPP
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <set>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include <vector_functions.h>
+#include <vector_types.h>
+
+#include "deme_b200.h"
+
+namespace deme {
+
+enum class TIME_INTEGRATOR { FORWARD_EULER = 0, CENTERED_DIFFERENCE = 1, EXTENDED_TAYLOR = 2 };
+
+class DEMMaterial {
+  public:
+    explicit DEMMaterial(const std::unordered_map<std::string, float>& props, unsigned order)
+        : mat_prop(props), load_order(order) {}
+    std::unordered_map<std::string, float> mat_prop;
+    unsigned load_order;
+};
+
+class DEMClumpTemplate {
+  public:
+    float mass = 0.f;
+    float3 MOI{0.f, 0.f, 0.f};
+    std::vector<float> radii;
+    std::vector<float3> relPos;
+    std::vector<std::shared_ptr<DEMMaterial>> materials;
+    unsigned mark = 0;
+    unsigned nComp() const { return (unsigned)radii.size(); }
+};
+
+class DEMClumpBatch {
+  public:
+    explicit DEMClumpBatch(size_t n) : nClumps(n), vel(n, float3{0, 0, 0}), angVel(n, float3{0, 0, 0}),
+                                       oriQ(n, float4{0, 0, 0, 1}), families(n, 0) {}
+    size_t GetNumClumps() const { return nClumps; }
+    void SetTypes(const std::vector<std::shared_ptr<DEMClumpTemplate>>& t) { check(t.size(), "SetTypes"); types = t; }
+    void SetType(const std::shared_ptr<DEMClumpTemplate>& t) { SetTypes({nClumps, t}); }
+    void SetPos(const std::vector<float3>& p) { check(p.size(), "SetPos"); xyz = p; }
+    void SetVel(const std::vector<float3>& v) { check(v.size(), "SetVel"); vel = v; }
+    void SetVel(float3 v) { SetVel(std::vector<float3>(nClumps, v)); }
+    void SetAngVel(const std::vector<float3>& w) { check(w.size(), "SetAngVel"); angVel = w; }
+    void SetAngVel(float3 w) { SetAngVel(std::vector<float3>(nClumps, w)); }
+    /* quaternions as float4 with .w the scalar part (the reference's convention) */
+    void SetOriQ(const std::vector<float4>& q) { check(q.size(), "SetOriQ"); oriQ = q; }
+    void SetOriQ(float4 q) { SetOriQ(std::vector<float4>(nClumps, q)); }
+    void SetFamilies(const std::vector<unsigned>& f) {
+        check(f.size(), "SetFamilies");
+        for (unsigned v : f)
+            if (v > 255) throw std::runtime_error("Some clumps are instructed to have a family number larger than 255");
+        families = f;
+    }
+    void SetFamilies(unsigned f) { SetFamilies(std::vector<unsigned>(nClumps, f)); }
+    void SetFamily(unsigned f) { SetFamilies(f); }
+
+    size_t nClumps;
+    std::vector<std::shared_ptr<DEMClumpTemplate>> types;
+    std::vector<float3> xyz, vel, angVel;
+    std::vector<float4> oriQ;
+    std::vector<unsigned> families;
+
+  private:
+    void check(size_t n, const char* what) const {
+        if (n != nClumps) throw std::runtime_error(std::string(what) + ": input length does not match the batch");
+    }
+};
+
+struct DEMAnalEntity {
+    int type;  // DEME_ANAL_*
+    std::shared_ptr<DEMMaterial> material;
+    float3 pos, rot;
+    float size1, size2, size3;
+    int normal;  // 0 inward (default), 1 outward
+};
+
+class DEMExternObj {
+  public:
+    explicit DEMExternObj(unsigned order) : load_order(order) {}
+    void SetFamily(unsigned code) {
+        if (code > 255) throw std::runtime_error("family number is larger than the max allowance 255");
+        family_code = code;
+    }
+    void SetMass(float m) { mass = m; }
+    void SetMOI(float3 moi) { MOI = moi; }
+    void SetInitPos(float3 p) { init_pos = p; }
+    void AddPlane(float3 pos, float3 normal, const std::shared_ptr<DEMMaterial>& mat) {
+        entities.push_back({DEME_ANAL_PLANE, mat, pos, normalize_host(normal), 0.f, 0.f, 0.f, 0});
+    }
+    /* infinite cylinder through `point` along `axis`; spheres live inside unless normal_outward */
+    void AddCylinder(float3 point, float3 axis, float radius, const std::shared_ptr<DEMMaterial>& mat,
+                     bool normal_outward = false) {
+        entities.push_back({DEME_ANAL_CYLINDER, mat, point, normalize_host(axis), radius, 0.f, 0.f, normal_outward});
+    }
+    /* cone with apex `apex` opening along `axis`; the wall exists for axial distances [u_min, u_max] */
+    void AddCone(float3 apex, float3 axis, float half_angle, float u_min, float u_max,
+                 const std::shared_ptr<DEMMaterial>& mat, bool normal_outward = false) {
+        entities.push_back({DEME_ANAL_CONE, mat, apex, normalize_host(axis), half_angle, u_min, u_max, normal_outward});
+    }
+    /* helper_math normalize on the host: v * (1 / sqrtf(dot(v, v))) in float */
+    static float3 normalize_host(float3 v) {
+        const float d = v.x * v.x + v.y * v.y + v.z * v.z;
+        const float inv = 1.0f / std::sqrt(d);
+        return float3{v.x * inv, v.y * inv, v.z * inv};
+    }
+
+    unsigned load_order;
+    unsigned family_code = DEME_RESERVED_FAMILY;
+    float3 init_pos{0.f, 0.f, 0.f};
+    float mass = 1e15f;
+    float3 MOI{1e15f, 1e15f, 1e15f};
+    std::vector<DEMAnalEntity> entities;
+};
+
+class DEMForceModel {
+  public:
+    void DefineCustomModel(const std::string& model) { m_force_model = model; custom = true; }
+    int ReadCustomModelFile(const std::string& path) {
+        std::ifstream f(path);
+        if (!f) return 1;
+        std::stringstream ss;
+        ss << f.rdbuf();
+        DefineCustomModel(ss.str());
+        return 0;
+    }
+    void SetPerContactWildcards(const std::set<std::string>& names) { m_contact_wildcards = names; }
+
+    bool custom = false;
+    std::string m_force_model;
+    std::set<std::string> m_contact_wildcards{"delta_tan_x", "delta_tan_y", "delta_tan_z", "delta_time"};
+};
+
+/* The flattened scene Initialize hands to deme_create (owned arrays; `scene` points into them). */
+struct FlatScene {
+    deme_sim_params params{};
+    deme_scene scene{};
+    std::vector<uint64_t> voxel;
+    std::vector<uint16_t> locX, locY, locZ;
+    std::vector<float> oriQw, oriQx, oriQy, oriQz, vX, vY, vZ, omgX, omgY, omgZ, mass, mmiXX, mmiYY, mmiZZ;
+    std::vector<uint8_t> family;
+    std::vector<uint32_t> sphere_owner;
+    std::vector<float> relX, relY, relZ, radius;
+    std::vector<uint8_t> sphere_material;
+    std::vector<uint8_t> anal_type, anal_normal, anal_material;
+    std::vector<uint32_t> anal_owner;
+    std::vector<float> anal_relX, anal_relY, anal_relZ, anal_rotX, anal_rotY, anal_rotZ, anal_size1, anal_size2,
+        anal_size3, anal_mass;
+    std::vector<float> mat_E, mat_nu, mat_CoR, mat_mu, mat_Crr;
+    std::vector<uint8_t> family_masks;
+    std::vector<deme_family_prescription> prescriptions;
+
+    void point() {
+        deme_scene& s = scene;
+        s.n_owners = (uint32_t)voxel.size();
+        s.n_spheres = (uint32_t)radius.size();
+        s.n_anal = (uint32_t)anal_type.size();
+        s.n_materials = (uint32_t)mat_E.size();
+        s.voxel = voxel.data();
+        s.locX = locX.data();
+        s.locY = locY.data();
+        s.locZ = locZ.data();
+        s.oriQw = oriQw.data();
+        s.oriQx = oriQx.data();
+        s.oriQy = oriQy.data();
+        s.oriQz = oriQz.data();
+        s.vX = vX.data();
+        s.vY = vY.data();
+        s.vZ = vZ.data();
+        s.omgX = omgX.data();
+        s.omgY = omgY.data();
+        s.omgZ = omgZ.data();
+        s.family = family.data();
+        s.mass = mass.data();
+        s.mmiXX = mmiXX.data();
+        s.mmiYY = mmiYY.data();
+        s.mmiZZ = mmiZZ.data();
+        s.sphere_owner = sphere_owner.data();
+        s.relX = relX.data();
+        s.relY = relY.data();
+        s.relZ = relZ.data();
+        s.radius = radius.data();
+        s.sphere_material = sphere_material.data();
+        s.anal_type = anal_type.data();
+        s.anal_owner = anal_owner.data();
+        s.anal_normal = anal_normal.data();
+        s.anal_material = anal_material.data();
+        s.anal_relX = anal_relX.data();
+        s.anal_relY = anal_relY.data();
+        s.anal_relZ = anal_relZ.data();
+        s.anal_rotX = anal_rotX.data();
+        s.anal_rotY = anal_rotY.data();
+        s.anal_rotZ = anal_rotZ.data();
+        s.anal_size1 = anal_size1.data();
+        s.anal_size2 = anal_size2.data();
+        s.anal_size3 = anal_size3.data();
+        s.anal_mass = anal_mass.data();
+        s.mat_E = mat_E.data();
+        s.mat_nu = mat_nu.data();
+        s.mat_CoR = mat_CoR.data();
+        s.mat_mu = mat_mu.data();
+        s.mat_Crr = mat_Crr.data();
+        s.family_masks = family_masks.data();
+        s.prescriptions = prescriptions.data();
+    }
+};
+
+class DEMSolver {
+  public:
+    DEMSolver() = default;
+    ~DEMSolver() {
+        if (h) deme_destroy(h);
+    }
+    DEMSolver(const DEMSolver&) = delete;
+    DEMSolver& operator=(const DEMSolver&) = delete;
+
+    // ---- world ----
+    void InstructBoxDomainDimension(float x, float y, float z) { box = float3{x, y, z}; has_box = true; }
+    void SetCoordSysOrigin(const std::string& where) { origin = where; }
+    void SetCoordSysOrigin(float3 lbf) { LBF = lbf; origin = "explicit"; }
+    void InstructBoxDomainBoundingBC(const std::string& inst, const std::shared_ptr<DEMMaterial>& mat) {
+        bounding_bc = inst;
+        bounding_mat = mat;
+    }
+    void SetGravitationalAcceleration(float3 g) { G = g; }
+    void SetInitTimeStep(double ts) { h_step = ts; }
+    void UpdateStepSize(double ts) {
+        h_step = ts;
+        if (h) check(deme_set_time_step(h, (float)ts));
+    }
+    void SetInitBinSize(double b) { bin_size = b; }
+    void SetCDUpdateFreq(int f) { update_freq = f; }
+    void SetExpandFactor(float beta, bool fix = true) { expand_factor = beta; expand_fixed = fix; }
+    void SetMaxVelocity(float v) { max_vel = v; }
+    void SetExpandSafetyParam(float s) { safety = s; }
+    void SetIntegrator(TIME_INTEGRATOR t) { integrator = (int)t; }
+
+    // ---- materials, templates, clumps, objects ----
+    std::shared_ptr<DEMMaterial> LoadMaterial(const std::unordered_map<std::string, float>& props) {
+        materials.push_back(std::make_shared<DEMMaterial>(props, (unsigned)materials.size()));
+        return materials.back();
+    }
+    std::shared_ptr<DEMClumpTemplate> LoadClumpType(float mass, float3 moi, const std::vector<float>& radii,
+                                                    const std::vector<float3>& relPos,
+                                                    const std::vector<std::shared_ptr<DEMMaterial>>& mats) {
+        if (radii.size() != relPos.size() || radii.size() != mats.size())
+            throw std::runtime_error("LoadClumpType: radii, positions and materials differ in length");
+        auto t = std::make_shared<DEMClumpTemplate>();
+        t->mass = mass;
+        t->MOI = moi;
+        t->radii = radii;
+        t->relPos = relPos;
+        t->materials = mats;
+        t->mark = (unsigned)templates.size();
+        templates.push_back(t);
+        return t;
+    }
+    std::shared_ptr<DEMClumpTemplate> LoadClumpType(float mass, float3 moi, const std::vector<float>& radii,
+                                                    const std::vector<float3>& relPos,
+                                                    const std::shared_ptr<DEMMaterial>& mat) {
+        return LoadClumpType(mass, moi, radii, relPos, std::vector<std::shared_ptr<DEMMaterial>>(radii.size(), mat));
+    }
+    /* APIPublic.cpp:402-409: MOI 2/5 m r^2 */
+    std::shared_ptr<DEMClumpTemplate> LoadSphereType(float mass, float radius,
+                                                     const std::shared_ptr<DEMMaterial>& mat) {
+        const float I = (float)(2.0 / 5.0 * mass * radius * radius);
+        return LoadClumpType(mass, float3{I, I, I}, {radius}, {float3{0.f, 0.f, 0.f}}, mat);
+    }
+    std::shared_ptr<DEMClumpBatch> AddClumps(const std::vector<std::shared_ptr<DEMClumpTemplate>>& types,
+                                             const std::vector<float3>& xyz) {
+        auto b = std::make_shared<DEMClumpBatch>(xyz.size());
+        b->SetTypes(types);
+        b->SetPos(xyz);
+        batches.push_back(b);
+        return b;
+    }
+    std::shared_ptr<DEMClumpBatch> AddClumps(const std::shared_ptr<DEMClumpTemplate>& type,
+                                             const std::vector<float3>& xyz) {
+        return AddClumps(std::vector<std::shared_ptr<DEMClumpTemplate>>(xyz.size(), type), xyz);
+    }
+    std::shared_ptr<DEMExternObj> AddExternalObject() {
+        ext.push_back(std::make_shared<DEMExternObj>((unsigned)ext.size()));
+        return ext.back();
+    }
+    std::shared_ptr<DEMExternObj> AddBCPlane(float3 pos, float3 normal, const std::shared_ptr<DEMMaterial>& mat) {
+        auto o = AddExternalObject();
+        o->AddPlane(pos, normal, mat);
+        return o;
+    }
+
+    // ---- families ----
+    void DisableContactBetweenFamilies(unsigned a, unsigned b) {
+        const unsigned lo = std::min(a, b), hi = std::max(a, b);
+        if ((1u + hi) * hi / 2u + lo >= 255u * 256u / 2u)
+            throw std::runtime_error("family mask entry out of range (the mask table holds 32640 entries)");
+        no_contact.emplace_back(a, b);
+    }
+    void SetFamilyFixed(unsigned fam) {
+        Presc p(fam);
+        p.linVel = {"0", "0", "0"};
+        p.rotVel = {"0", "0", "0"};
+        p.linVelP = p.rotVelP = p.linPosP = p.rotPosP = true;
+        presc.push_back(p);
+    }
+    void SetFamilyPrescribedLinVel(unsigned fam, const std::string& vx, const std::string& vy, const std::string& vz,
+                                   bool dictate = true) {
+        Presc p(fam);
+        p.linVel = {vx, vy, vz};
+        p.linVelP = p.rotVelP = dictate;
+        presc.push_back(p);
+    }
+    void SetFamilyPrescribedAngVel(unsigned fam, const std::string& wx, const std::string& wy, const std::string& wz,
+                                   bool dictate = true) {
+        Presc p(fam);
+        p.rotVel = {wx, wy, wz};
+        p.linVelP = p.rotVelP = dictate;
+        presc.push_back(p);
+    }
+    void SetFamilyPrescribedPosition(unsigned fam, const std::string& x, const std::string& y, const std::string& z) {
+        Presc p(fam);
+        p.linPos = {x, y, z};
+        p.linPosP = p.rotPosP = true;
+        presc.push_back(p);
+    }
+
+    // ---- force model ----
+    std::shared_ptr<DEMForceModel> UseFrictionalHertzianModel() {
+        force_model = std::make_shared<DEMForceModel>();
+        return force_model;
+    }
+    std::shared_ptr<DEMForceModel> DefineContactForceModel(const std::string& model) {
+        force_model = std::make_shared<DEMForceModel>();
+        force_model->DefineCustomModel(model);
+        force_model->m_contact_wildcards.clear();
+        return force_model;
+    }
+    std::shared_ptr<DEMForceModel> ReadContactForceModel(const std::string& path) {
+        force_model = std::make_shared<DEMForceModel>();
+        force_model->m_contact_wildcards.clear();
+        if (force_model->ReadCustomModelFile(path)) throw std::runtime_error("cannot read force model file " + path);
+        return force_model;
+    }
+
+    // ---- lifecycle ----
+    /* The scene as last flattened (by Flatten or Initialize). */
+    const FlatScene& GetFlatScene() const { return *flat; }
+    /* Flattens the scene (what Initialize uploads); usable without a GPU.  Initialize flattens again, which
+     * replaces the FlatScene a previous call returned. */
+    const FlatScene& Flatten() {
+        flat = std::make_unique<FlatScene>();
+        build_flat(*flat);
+        return *flat;
+    }
+    void Initialize() {
+        Flatten();
+        if (h) {
+            deme_destroy(h);
+            h = nullptr;
+        }
+        const int32_t st = deme_create(&flat->params, &flat->scene, &h);
+        if (st != DEME_OK) {
+            std::string msg = h ? deme_get_error(h) : "";
+            if (h) deme_destroy(h);
+            h = nullptr;
+            throw std::runtime_error(std::string("Initialize: ") + deme_status_string(st) + ": " + msg);
+        }
+        if (force_model && force_model->custom) {
+            std::vector<const char*> names;
+            for (const auto& n : force_model->m_contact_wildcards) names.push_back(n.c_str());
+            check(deme_set_force_model(h, force_model->m_force_model.c_str(), names.data(), (int32_t)names.size()));
+        }
+    }
+    /* dT's cycle loop (src/DEM/dT.cpp:1527): steps while the accumulated time is below the duration */
+    void DoDynamics(double duration) {
+        const double hs = (double)flat->params.h;
+        int32_t n = 0;
+        for (double t = 0.0; t < duration; t += hs) n++;
+        if (n) check(deme_step(h, n));
+    }
+    void DoDynamicsThenSync(double duration) {
+        DoDynamics(duration);
+        check(deme_sync(h));
+    }
+    void DoStepDynamics() { check(deme_step(h, 1)); }
+
+    // ---- queries (GetOwner*, src/DEM/API.h:196-214) ----
+    float3 GetOwnerPosition(uint32_t owner) {
+        pull();
+        const deme_sim_params& p = flat->params;
+        const uint64_t v = st_voxel[owner];
+        const uint64_t mx = (1ull << p.nvXp2) - 1, my = (1ull << p.nvYp2) - 1;
+        const double X = (double)(v & mx) * p.voxel_size + (double)st_locX[owner] * p.l;
+        const double Y = (double)((v >> p.nvXp2) & my) * p.voxel_size + (double)st_locY[owner] * p.l;
+        const double Z = (double)(v >> (p.nvXp2 + p.nvYp2)) * p.voxel_size + (double)st_locZ[owner] * p.l;
+        return float3{(float)(X + p.lbf[0]), (float)(Y + p.lbf[1]), (float)(Z + p.lbf[2])};
+    }
+    float3 GetOwnerVelocity(uint32_t owner) {
+        pull();
+        return float3{st_f[0][owner], st_f[1][owner], st_f[2][owner]};
+    }
+    float3 GetOwnerAngVel(uint32_t owner) {
+        pull();
+        return float3{st_f[3][owner], st_f[4][owner], st_f[5][owner]};
+    }
+    float4 GetOwnerOriQ(uint32_t owner) {
+        pull();
+        return float4{st_f[7][owner], st_f[8][owner], st_f[9][owner], st_f[6][owner]};
+    }
+    uint32_t GetNumContacts() {
+        uint32_t n = 0;
+        check(deme_get_num_contacts(h, &n));
+        return n;
+    }
+    double GetTotalKineticEnergy() {
+        double ke = 0;
+        check(deme_kinetic_energy(h, &ke));
+        return ke;
+    }
+    double GetSimTime() {
+        double t = 0;
+        int64_t s = 0;
+        check(deme_get_time(h, &t, &s));
+        return t;
+    }
+    deme_handle* GetHandle() const { return h; }
+
+  private:
+    struct Presc {
+        explicit Presc(unsigned f) : family(f) {}
+        unsigned family;
+        std::vector<std::string> linPos{"none", "none", "none"}, linVel{"none", "none", "none"},
+            rotVel{"none", "none", "none"};
+        bool linVelP = false, rotVelP = false, linPosP = false, rotPosP = false;
+    };
+
+    void check(int32_t st) {
+        if (st != DEME_OK) throw std::runtime_error(std::string(deme_status_string(st)) + ": " + deme_get_error(h));
+    }
+
+    void pull() {
+        const uint32_t n = flat->scene.n_owners;
+        st_voxel.resize(n);
+        st_locX.resize(n);
+        st_locY.resize(n);
+        st_locZ.resize(n);
+        for (auto& v : st_f) v.resize(n);
+        deme_state s{};
+        s.voxel = st_voxel.data();
+        s.locX = st_locX.data();
+        s.locY = st_locY.data();
+        s.locZ = st_locZ.data();
+        s.vX = st_f[0].data();
+        s.vY = st_f[1].data();
+        s.vZ = st_f[2].data();
+        s.omgX = st_f[3].data();
+        s.omgY = st_f[4].data();
+        s.omgZ = st_f[5].data();
+        s.oriQw = st_f[6].data();
+        s.oriQx = st_f[7].data();
+        s.oriQy = st_f[8].data();
+        s.oriQz = st_f[9].data();
+        check(deme_download_state(h, &s));
+    }
+
+    static double kernel_literal(double x) {  // std::fixed, 17 decimals, parsed back (APIPrivate.cpp:1358-1359)
+        char buf[128];
+        std::snprintf(buf, sizeof(buf), "%.17f", x);
+        return std::strtod(buf, nullptr);
+    }
+    static double constant_expr(const std::string& e) {
+        char* end = nullptr;
+        const double v = std::strtod(e.c_str(), &end);
+        while (end && *end == ' ') end++;
+        if (!end || end == e.c_str() || *end != '\0')
+            throw std::runtime_error("prescription '" + e + "' is not a constant (only constant prescriptions are "
+                                     "supported)");
+        return v;
+    }
+
+    /* figureOutNV, src/DEM/APIPrivate.cpp:222-333 (no exact direction) */
+    void figure_out_nv(uint8_t nv[3], double& l) const {
+        float XYZ[3] = {box.x, box.y, box.z};
+        int rank[3] = {0, 1, 2};
+        for (int i = 0; i < 2; i++)
+            for (int j = i + 1; j < 3; j++)
+                if (XYZ[i] > XYZ[j]) {
+                    std::swap(XYZ[i], XYZ[j]);
+                    std::swap(rank[i], rank[j]);
+                }
+        const float size321[3] = {XYZ[0], XYZ[1], XYZ[2]};
+        int more[2] = {0, 0};
+        for (int a = 0; a < 2; a++) {
+            while (XYZ[a] < XYZ[a + 1]) {
+                if (std::sqrt(2.0) * (double)XYZ[a] > (double)XYZ[a + 1]) break;
+                more[a]++;
+                XYZ[a] = (float)((double)XYZ[a] * 2.0);
+            }
+        }
+        const int base = (64 - more[0] - more[1]) / 3;
+        int left = (64 - more[0] - more[1]) % 3;
+        int b3 = base, b2 = b3 + more[0], b1 = b2 + more[1];
+        while (left > 0) {
+            if (b3 < b2)
+                b3++;
+            else if (b2 < b1)
+                b2++;
+            else
+                b1++;
+            left--;
+        }
+        const int bits[3] = {b3, b2, b1};
+        if (b1 + b2 + b3 > 64)
+            throw std::runtime_error("domain needs more than 64 voxel bits under the reference's bit split; use a "
+                                     "domain whose two smaller sides are within a factor sqrt(2)");
+        double lmax = 0.0;
+        for (int i = 0; i < 3; i++) lmax = std::max(lmax, (double)size321[i] / 65536.0 / std::ldexp(1.0, bits[i]));
+        l = (double)(float)lmax;
+        for (int i = 0; i < 3; i++) nv[rank[i]] = (uint8_t)bits[i];
+    }
+
+    void build_flat(FlatScene& f) {
+        if (!has_box) throw std::runtime_error("InstructBoxDomainDimension must be called before Initialize");
+        uint8_t nv[3];
+        double l = 0.0;
+        figure_out_nv(nv, l);
+        const double voxel_size = 65536.0 * l;
+        float3 lbf = LBF;
+        if (origin == "center")
+            lbf = float3{-(box.x / 2.0f), -(box.y / 2.0f), -(box.z / 2.0f)};
+        else if (origin != "explicit")
+            throw std::runtime_error("Unrecognized location of system origin.");
+        if (bounding_bc != "none" && !bounding_added) {
+            auto b = AddExternalObject();
+            const float X = lbf.x, Y = lbf.y, Z = lbf.z, bx = box.x, by = box.y, bz = box.z;
+            const auto& m = bounding_mat;
+            b->AddPlane(float3{X + bx / 2.0f, Y + by / 2.0f, Z}, float3{0, 0, 1}, m);
+            if (bounding_bc != "only_bottom") {
+                b->AddPlane(float3{X, Y + by / 2.0f, Z + bz / 2.0f}, float3{1, 0, 0}, m);
+                b->AddPlane(float3{X + bx, Y + by / 2.0f, Z + bz / 2.0f}, float3{-1, 0, 0}, m);
+                b->AddPlane(float3{X + bx / 2.0f, Y, Z + bz / 2.0f}, float3{0, 1, 0}, m);
+                b->AddPlane(float3{X + bx / 2.0f, Y + by, Z + bz / 2.0f}, float3{0, -1, 0}, m);
+                if (bounding_bc != "top_open") b->AddPlane(float3{X + bx / 2.0f, Y + by / 2.0f, Z + bz}, float3{0, 0, -1}, m);
+            }
+            bounding_added = true;
+        }
+        std::vector<Presc> all_presc = presc;
+        {  // validateUserInputs: the reserved family is fixed
+            Presc p(DEME_RESERVED_FAMILY);
+            p.linVel = {"0", "0", "0"};
+            p.rotVel = {"0", "0", "0"};
+            p.linVelP = p.rotVelP = p.linPosP = p.rotPosP = true;
+            all_presc.push_back(p);
+        }
+        // ---- owners: clumps in batch order, then external objects (dT.cpp:522-640) ----
+        std::vector<const DEMClumpBatch*> bs;
+        size_t nClumps = 0;
+        for (const auto& b : batches) {
+            bs.push_back(b.get());
+            nClumps += b->nClumps;
+        }
+        const size_t nExt = ext.size(), nO = nClumps + nExt;
+        auto resize = [nO](auto&... v) { (v.resize(nO), ...); };
+        resize(f.voxel, f.locX, f.locY, f.locZ, f.oriQw, f.oriQx, f.oriQy, f.oriQz, f.vX, f.vY, f.vZ, f.omgX, f.omgY,
+               f.omgZ, f.family, f.mass, f.mmiXX, f.mmiYY, f.mmiZZ);
+        std::vector<float3> pos(nO);
+        size_t o = 0;
+        for (const DEMClumpBatch* b : bs) {
+            for (size_t i = 0; i < b->nClumps; i++, o++) {
+                const DEMClumpTemplate& t = *b->types[i];
+                pos[o] = b->xyz[i];
+                f.oriQw[o] = b->oriQ[i].w;
+                f.oriQx[o] = b->oriQ[i].x;
+                f.oriQy[o] = b->oriQ[i].y;
+                f.oriQz[o] = b->oriQ[i].z;
+                f.vX[o] = b->vel[i].x;
+                f.vY[o] = b->vel[i].y;
+                f.vZ[o] = b->vel[i].z;
+                f.omgX[o] = b->angVel[i].x;
+                f.omgY[o] = b->angVel[i].y;
+                f.omgZ[o] = b->angVel[i].z;
+                f.family[o] = (uint8_t)b->families[i];
+                f.mass[o] = t.mass;
+                f.mmiXX[o] = t.MOI.x;
+                f.mmiYY[o] = t.MOI.y;
+                f.mmiZZ[o] = t.MOI.z;
+                for (unsigned k = 0; k < t.nComp(); k++) {
+                    f.sphere_owner.push_back((uint32_t)o);
+                    f.radius.push_back(t.radii[k]);
+                    f.relX.push_back(t.relPos[k].x);
+                    f.relY.push_back(t.relPos[k].y);
+                    f.relZ.push_back(t.relPos[k].z);
+                    f.sphere_material.push_back((uint8_t)t.materials[k]->load_order);
+                }
+            }
+        }
+        for (size_t e = 0; e < nExt; e++, o++) {
+            const DEMExternObj& x = *ext[e];
+            pos[o] = x.init_pos;
+            f.oriQw[o] = 1.f;
+            f.oriQx[o] = f.oriQy[o] = f.oriQz[o] = 0.f;
+            f.vX[o] = f.vY[o] = f.vZ[o] = f.omgX[o] = f.omgY[o] = f.omgZ[o] = 0.f;
+            f.family[o] = (uint8_t)x.family_code;
+            f.mass[o] = x.mass;
+            f.mmiXX[o] = x.MOI.x;
+            f.mmiYY[o] = x.MOI.y;
+            f.mmiZZ[o] = x.MOI.z;
+            for (const DEMAnalEntity& a : x.entities) {
+                f.anal_type.push_back((uint8_t)a.type);
+                f.anal_owner.push_back((uint32_t)o);
+                f.anal_normal.push_back((uint8_t)a.normal);
+                f.anal_material.push_back((uint8_t)a.material->load_order);
+                f.anal_relX.push_back(a.pos.x);
+                f.anal_relY.push_back(a.pos.y);
+                f.anal_relZ.push_back(a.pos.z);
+                f.anal_rotX.push_back(a.rot.x);
+                f.anal_rotY.push_back(a.rot.y);
+                f.anal_rotZ.push_back(a.rot.z);
+                f.anal_size1.push_back(a.size1);
+                f.anal_size2.push_back(a.size2);
+                f.anal_size3.push_back(a.size3);
+                f.anal_mass.push_back(x.mass);
+            }
+        }
+        if (f.anal_type.size() > 255) throw std::runtime_error("at most 255 analytical components");
+        // ---- initial encoding of xyz - LBF (hostPositionToVoxelID, HostSideHelpers.hpp:328-350) ----
+        for (size_t i = 0; i < nO; i++) {
+            const double p[3] = {(double)(pos[i].x - lbf.x), (double)(pos[i].y - lbf.y), (double)(pos[i].z - lbf.z)};
+            uint64_t n[3];
+            uint16_t s[3];
+            for (int a = 0; a < 3; a++) {
+                double q = p[a] / voxel_size;
+                if (!(q > 0)) q = 0.0;
+                n[a] = (uint64_t)std::floor(q);
+                double sub = (p[a] - (double)n[a] * voxel_size) / l;
+                if (!(sub > 0)) sub = 0.0;
+                sub = std::min(sub, 65535.0);
+                s[a] = (uint16_t)std::floor(sub);
+            }
+            f.voxel[i] = n[0] + (n[1] << nv[0]) + (n[2] << (nv[0] + nv[1]));
+            f.locX[i] = s[0];
+            f.locY[i] = s[1];
+            f.locZ[i] = s[2];
+        }
+        // ---- materials ----
+        auto prop = [](const DEMMaterial& m, const char* key) {
+            auto it = m.mat_prop.find(key);
+            return it == m.mat_prop.end() ? 0.f : it->second;
+        };
+        for (const auto& m : materials) {
+            f.mat_E.push_back(prop(*m, "E"));
+            f.mat_nu.push_back(prop(*m, "nu"));
+            f.mat_CoR.push_back(prop(*m, "CoR"));
+            f.mat_mu.push_back(prop(*m, "mu"));
+            f.mat_Crr.push_back(prop(*m, "Crr"));
+        }
+        // ---- family masks and merged prescriptions (figureOutFamilyMasks, APIPrivate.cpp:574-645) ----
+        f.family_masks.assign(DEME_NUM_FAMILY_MASK, 0);
+        for (const auto& pr : no_contact) {
+            const unsigned lo = std::min(pr.first, pr.second), hi = std::max(pr.first, pr.second);
+            f.family_masks[(1 + hi) * hi / 2 + lo] = 1;
+        }
+        std::map<unsigned, Presc> merged;
+        for (const Presc& p : all_presc) {
+            auto it = merged.find(p.family);
+            if (it == merged.end()) it = merged.emplace(p.family, Presc(p.family)).first;
+            Presc& m = it->second;
+            for (int k = 0; k < 3; k++) {
+                if (p.linPos[k] != "none") m.linPos[k] = p.linPos[k];
+                if (p.linVel[k] != "none") m.linVel[k] = p.linVel[k];
+                if (p.rotVel[k] != "none") m.rotVel[k] = p.rotVel[k];
+            }
+            m.linVelP |= p.linVelP;
+            m.rotVelP |= p.rotVelP;
+            m.linPosP |= p.linPosP;
+            m.rotPosP |= p.rotPosP;
+        }
+        f.prescriptions.assign(DEME_NUM_FAMILIES, deme_family_prescription{});
+        for (const auto& kv : merged) {
+            deme_family_prescription& e = f.prescriptions[kv.first];
+            const Presc& m = kv.second;
+            e.used = 1;
+            e.lin_vel_prescribed = m.linVelP;
+            e.rot_vel_prescribed = m.rotVelP;
+            e.lin_pos_prescribed = m.linPosP;
+            e.rot_pos_prescribed = m.rotPosP;
+            for (int k = 0; k < 3; k++) {
+                if (m.linVel[k] != "none") {
+                    e.has_vel[k] = 1;
+                    e.vel[k] = (float)constant_expr(m.linVel[k]);
+                }
+                if (m.rotVel[k] != "none") {
+                    e.has_omg[k] = 1;
+                    e.omg[k] = (float)constant_expr(m.rotVel[k]);
+                }
+                if (m.linPos[k] != "none") {
+                    e.has_pos[k] = 1;
+                    e.pos[k] = constant_expr(m.linPos[k]);
+                }
+            }
+        }
+        // ---- bins (decideBinSize, APIPrivate.cpp:335-369) and expand factor (APIPrivate.cpp:730-758) ----
+        double rmin = HUGE_VAL;
+        for (float r : f.radius) rmin = std::min(rmin, (double)r);
+        for (const auto& t : templates)
+            for (float r : t->radii) rmin = std::min(rmin, (double)r);
+        double bs_ = bin_size;
+        if (!(bs_ > 0.0)) {
+            if (!(rmin > 1e-12)) throw std::runtime_error("spheres with zero radius and no bin size given");
+            bs_ = 2.0 * (double)(float)rmin;
+        }
+        uint32_t nb[3];
+        for (int i = 0; i < 3; i++) nb[i] = (uint32_t)(voxel_size * std::ldexp(1.0, nv[i]) / bs_) + 1u;
+        const double beta = expand_fixed ? (double)expand_factor
+                                         : (double)(float)((double)max_vel * h_step * update_freq * (double)safety);
+        deme_sim_params& p = f.params;
+        p = deme_sim_params{};
+        p.nvXp2 = nv[0];
+        p.nvYp2 = nv[1];
+        p.nvZp2 = nv[2];
+        p.nbX = nb[0];
+        p.nbY = nb[1];
+        p.nbZ = nb[2];
+        p.l = l;
+        p.voxel_size = voxel_size;
+        p.l_kernel = kernel_literal(l);
+        p.voxel_size_kernel = kernel_literal(voxel_size);
+        p.bin_size = bs_;
+        p.lbf[0] = lbf.x;
+        p.lbf[1] = lbf.y;
+        p.lbf[2] = lbf.z;
+        p.G[0] = G.x;
+        p.G[1] = G.y;
+        p.G[2] = G.z;
+        p.h = (float)h_step;
+        p.beta = (float)beta;
+        p.integrator = integrator;
+        p.cd_update_freq = update_freq;
+        p.n_contact_wildcards = force_model && force_model->custom ? (int32_t)force_model->m_contact_wildcards.size()
+                                                                   : 4;
+        p.domain[0] = box.x;
+        p.domain[1] = box.y;
+        p.domain[2] = box.z;
+        f.point();
+    }
+
+    std::vector<std::shared_ptr<DEMMaterial>> materials;
+    std::vector<std::shared_ptr<DEMClumpTemplate>> templates;
+    std::vector<std::shared_ptr<DEMClumpBatch>> batches;
+    std::vector<std::shared_ptr<DEMExternObj>> ext;
+    float3 box{0.f, 0.f, 0.f};
+    bool has_box = false;
+    std::string origin = "explicit";
+    float3 LBF{0.f, 0.f, 0.f};
+    std::string bounding_bc = "none";
+    std::shared_ptr<DEMMaterial> bounding_mat;
+    bool bounding_added = false;
+    float3 G{0.f, 0.f, 0.f};
+    double h_step = -1.0;
+    double bin_size = -1.0;
+    float expand_factor = 0.f;
+    bool expand_fixed = false;
+    float max_vel = -1.f;
+    float safety = 1.f;
+    int update_freq = 0;
+    int integrator = DEME_INTEGRATOR_EXTENDED_TAYLOR;
+    std::vector<std::pair<unsigned, unsigned>> no_contact;
+    std::vector<Presc> presc;
+    std::shared_ptr<DEMForceModel> force_model;
+    std::unique_ptr<FlatScene> flat;
+    deme_handle* h = nullptr;
+    std::vector<uint64_t> st_voxel;
+    std::vector<uint16_t> st_locX, st_locY, st_locZ;
+    std::vector<float> st_f[10];
+};
+
+}  // namespace deme
+
+#endif /* DEME_SOLVER_HPP */

@@ -1,0 +1,163 @@
+// Builds one scene through the C++ DEMSolver facade (include/deme_solver.hpp) from per-clump inputs written by
+// tests/test_cpp_facade.py, flattens it (no GPU needed) and writes every flat array for comparison with the Python
+// SceneBuilder.  With a step count it also initializes the solver on the GPU, steps, and writes the owner state.
+// Usage: facade_dump <inputs.bin> <out.bin> [steps]
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+
+#include "deme_solver.hpp"
+
+using namespace deme;
+
+template <typename T>
+static std::vector<T> read_vec(std::ifstream& in) {
+    uint64_t n = 0;
+    in.read(reinterpret_cast<char*>(&n), sizeof(n));
+    std::vector<T> v(n);
+    in.read(reinterpret_cast<char*>(v.data()), (std::streamsize)(n * sizeof(T)));
+    return v;
+}
+
+template <typename T>
+static void put(std::ofstream& out, const char* name, const T* data, size_t n) {
+    const uint32_t len = (uint32_t)std::strlen(name);
+    const uint64_t bytes = n * sizeof(T);
+    out.write(reinterpret_cast<const char*>(&len), sizeof(len));
+    out.write(name, len);
+    out.write(reinterpret_cast<const char*>(&bytes), sizeof(bytes));
+    out.write(reinterpret_cast<const char*>(data), (std::streamsize)bytes);
+}
+template <typename T>
+static void put(std::ofstream& out, const char* name, const std::vector<T>& v) {
+    put(out, name, v.data(), v.size());
+}
+
+int main(int argc, char** argv) {
+    if (argc != 3 && argc != 4) return 2;
+    std::ifstream in(argv[1], std::ios::binary);
+    const auto types = read_vec<int32_t>(in);    // batch 1 template index per clump
+    const auto xyz1 = read_vec<float>(in);       // batch 1 positions (3 per clump)
+    const auto q1 = read_vec<float>(in);         // batch 1 quaternions (w, x, y, z)
+    const auto v1 = read_vec<float>(in);         // batch 1 velocities
+    const auto w1 = read_vec<float>(in);         // batch 1 angular velocities
+    const auto fam1 = read_vec<int32_t>(in);     // batch 1 families
+    const auto xyz2 = read_vec<float>(in);       // batch 2 positions
+
+    DEMSolver s;
+    s.InstructBoxDomainDimension(0.3f, 0.3f, 0.45f);
+    s.SetCoordSysOrigin("center");
+    auto m0 = s.LoadMaterial({{"E", 1e7f}, {"nu", 0.3f}, {"CoR", 0.5f}, {"mu", 0.5f}, {"Crr", 0.0f}});
+    auto m1 = s.LoadMaterial({{"E", 5e7f}, {"nu", 0.25f}, {"CoR", 0.3f}, {"mu", 0.4f}, {"Crr", 0.02f}});
+    s.InstructBoxDomainBoundingBC("top_open", m0);
+    std::vector<std::shared_ptr<DEMClumpTemplate>> T;
+    T.push_back(s.LoadSphereType(1.361e-3f, 5e-3f, m0));
+    T.push_back(s.LoadClumpType(2.5e-3f, float3{1e-7f, 1.2e-7f, 1.5e-7f}, {4e-3f, 5e-3f, 4.5e-3f},
+                                {float3{3e-3f, 0.f, 0.f}, float3{-1.5e-3f, 2.6e-3f, 0.f}, float3{-1.5e-3f, -2.6e-3f, 0.f}},
+                                {m0, m1, m0}));
+    T.push_back(s.LoadClumpType(1.8e-3f, float3{8e-8f, 9e-8f, 9e-8f}, {4e-3f, 4e-3f},
+                                {float3{0.f, 0.f, 2.5e-3f}, float3{0.f, 0.f, -2.5e-3f}}, m1));
+    const size_t n1 = types.size(), n2 = xyz2.size() / 3;
+    std::vector<std::shared_ptr<DEMClumpTemplate>> tv;
+    std::vector<float3> p1, vv, ww, p2;
+    std::vector<float4> qq;
+    std::vector<unsigned> ff;
+    for (size_t i = 0; i < n1; i++) {
+        tv.push_back(T[types[i]]);
+        p1.push_back(float3{xyz1[3 * i], xyz1[3 * i + 1], xyz1[3 * i + 2]});
+        qq.push_back(float4{q1[4 * i + 1], q1[4 * i + 2], q1[4 * i + 3], q1[4 * i]});
+        vv.push_back(float3{v1[3 * i], v1[3 * i + 1], v1[3 * i + 2]});
+        ww.push_back(float3{w1[3 * i], w1[3 * i + 1], w1[3 * i + 2]});
+        ff.push_back((unsigned)fam1[i]);
+    }
+    for (size_t i = 0; i < n2; i++) p2.push_back(float3{xyz2[3 * i], xyz2[3 * i + 1], xyz2[3 * i + 2]});
+    auto b1 = s.AddClumps(tv, p1);
+    b1->SetOriQ(qq);
+    b1->SetVel(vv);
+    b1->SetAngVel(ww);
+    b1->SetFamilies(ff);
+    auto b2 = s.AddClumps(T[2], p2);
+    b2->SetFamily(3);
+    s.AddBCPlane(float3{0.f, 0.f, -0.1f}, float3{0.1f, 0.f, 1.f}, m1);
+    auto wall = s.AddExternalObject();
+    wall->AddCylinder(float3{0.f, 0.f, 0.f}, float3{0.f, 0.f, 1.f}, 0.12f, m0);
+    wall->AddCone(float3{0.f, 0.f, -0.2f}, float3{0.f, 0.f, 1.f}, 0.5235988f, 0.03f, 0.15f, m1);
+    wall->SetFamily(10);
+    s.SetFamilyFixed(3);
+    s.SetFamilyPrescribedAngVel(10, "0", "2.0943951", "0");
+    s.SetFamilyPrescribedLinVel(4, "0.1", "none", "0");
+    s.DisableContactBetweenFamilies(3, 10);
+    s.SetInitTimeStep(1e-5);
+    s.SetGravitationalAcceleration(float3{0.f, 0.f, -9.81f});
+    s.SetCDUpdateFreq(5);
+    s.SetExpandFactor(1e-4f);
+    const FlatScene& f = s.Flatten();
+
+    std::ofstream out(argv[2], std::ios::binary);
+    put(out, "params", &f.params, 1);
+    put(out, "voxel", f.voxel);
+    put(out, "locX", f.locX);
+    put(out, "locY", f.locY);
+    put(out, "locZ", f.locZ);
+    put(out, "oriQw", f.oriQw);
+    put(out, "oriQx", f.oriQx);
+    put(out, "oriQy", f.oriQy);
+    put(out, "oriQz", f.oriQz);
+    put(out, "vX", f.vX);
+    put(out, "vY", f.vY);
+    put(out, "vZ", f.vZ);
+    put(out, "omgX", f.omgX);
+    put(out, "omgY", f.omgY);
+    put(out, "omgZ", f.omgZ);
+    put(out, "family", f.family);
+    put(out, "mass", f.mass);
+    put(out, "mmiXX", f.mmiXX);
+    put(out, "mmiYY", f.mmiYY);
+    put(out, "mmiZZ", f.mmiZZ);
+    put(out, "sphere_owner", f.sphere_owner);
+    put(out, "relX", f.relX);
+    put(out, "relY", f.relY);
+    put(out, "relZ", f.relZ);
+    put(out, "radius", f.radius);
+    put(out, "sphere_material", f.sphere_material);
+    put(out, "anal_type", f.anal_type);
+    put(out, "anal_owner", f.anal_owner);
+    put(out, "anal_normal", f.anal_normal);
+    put(out, "anal_material", f.anal_material);
+    put(out, "anal_relX", f.anal_relX);
+    put(out, "anal_relY", f.anal_relY);
+    put(out, "anal_relZ", f.anal_relZ);
+    put(out, "anal_rotX", f.anal_rotX);
+    put(out, "anal_rotY", f.anal_rotY);
+    put(out, "anal_rotZ", f.anal_rotZ);
+    put(out, "anal_size1", f.anal_size1);
+    put(out, "anal_size2", f.anal_size2);
+    put(out, "anal_size3", f.anal_size3);
+    put(out, "anal_mass", f.anal_mass);
+    put(out, "mat_E", f.mat_E);
+    put(out, "mat_nu", f.mat_nu);
+    put(out, "mat_CoR", f.mat_CoR);
+    put(out, "mat_mu", f.mat_mu);
+    put(out, "mat_Crr", f.mat_Crr);
+    put(out, "family_masks", f.family_masks);
+    put(out, "prescriptions", f.prescriptions);
+    if (argc == 4) {
+        const int steps = std::atoi(argv[3]);
+        s.Initialize();  // flattens again: use the new FlatScene from here on
+        for (int i = 0; i < steps; i++) s.DoStepDynamics();
+        const size_t nO = s.GetFlatScene().voxel.size();
+        std::vector<float3> pos(nO), vel(nO);
+        for (size_t o = 0; o < nO; o++) {
+            pos[o] = s.GetOwnerPosition((uint32_t)o);
+            vel[o] = s.GetOwnerVelocity((uint32_t)o);
+        }
+        const double ke = s.GetTotalKineticEnergy();
+        const uint32_t nc = s.GetNumContacts();
+        put(out, "run_pos", pos);
+        put(out, "run_vel", vel);
+        put(out, "run_ke", &ke, 1);
+        put(out, "run_ncontacts", &nc, 1);
+    }
+    return 0;
+}

@@ -1,0 +1,161 @@
+"""The C++ DEMSolver facade (include/deme_solver.hpp) flattens a scene exactly as the Python SceneBuilder does.
+
+tests/cpp/facade_dump.cpp builds a scene with every kind of input (sphere and clump templates with mixed
+materials, two clump batches with orientations, velocities and families, bounding planes, an extra plane, a
+cylinder and a cone on one family-10 object, fixed and prescribed families, a family mask, contact margin and CD
+frequency) through the C++ API, and writes the flat arrays Initialize would upload.  The same scene is built here
+with SceneBuilder; every array and the parameter and prescription structs must agree bit for bit.  Compiling and
+running the C++ side needs no GPU.
+"""
+import ctypes as C
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from _util import ROOT, capi
+from deme_b200 import solver
+from deme_b200.scene import SceneBuilder
+
+f32 = np.float32
+CUDA_INC = "/usr/local/cuda/include"
+
+
+def scene_inputs(seed=5):
+    rng = np.random.default_rng(seed)
+    n1, n2 = 57, 23
+    types = rng.integers(0, 3, n1).astype(np.int32)
+    xyz1 = rng.uniform(-0.1, 0.1, (n1, 3)).astype(f32)
+    q = rng.normal(size=(n1, 4))
+    q1 = (q / np.linalg.norm(q, axis=1)[:, None]).astype(f32)
+    v1 = rng.normal(0, 0.3, (n1, 3)).astype(f32)
+    w1 = rng.normal(0, 3.0, (n1, 3)).astype(f32)
+    fam1 = rng.integers(0, 6, n1).astype(np.int32)
+    xyz2 = rng.uniform(-0.1, 0.1, (n2, 3)).astype(f32)
+    return types, xyz1, q1, v1, w1, fam1, xyz2
+
+
+def python_scene(types, xyz1, q1, v1, w1, fam1, xyz2):
+    s = SceneBuilder()
+    s.InstructBoxDomainDimension(0.3, 0.3, 0.45)
+    s.SetCoordSysOrigin("center")
+    m0 = s.LoadMaterial({"E": 1e7, "nu": 0.3, "CoR": 0.5, "mu": 0.5, "Crr": 0.0})
+    m1 = s.LoadMaterial({"E": 5e7, "nu": 0.25, "CoR": 0.3, "mu": 0.4, "Crr": 0.02})
+    s.InstructBoxDomainBoundingBC("top_open", m0)
+    mass_s, r_s = float(f32(1.361e-3)), float(f32(5e-3))
+    T = [s.LoadSphereType(mass_s, r_s, m0),
+         s.LoadClumpType(2.5e-3, (1e-7, 1.2e-7, 1.5e-7), [4e-3, 5e-3, 4.5e-3],
+                         [[3e-3, 0, 0], [-1.5e-3, 2.6e-3, 0], [-1.5e-3, -2.6e-3, 0]], [m0, m1, m0]),
+         s.LoadClumpType(1.8e-3, (8e-8, 9e-8, 9e-8), [4e-3, 4e-3], [[0, 0, 2.5e-3], [0, 0, -2.5e-3]], m1)]
+    b1 = s.AddClumps([T[t] for t in types], xyz1)
+    b1.SetOriQ(q1)
+    b1.SetVel(v1)
+    b1.SetAngVel(w1)
+    b1.SetFamilies(fam1)
+    b2 = s.AddClumps(T[2], xyz2)
+    b2.SetFamily(3)
+    s.AddBCPlane((0, 0, -0.1), (0.1, 0, 1), m1)
+    wall = s.AddExternalObject()
+    wall.AddCylinder((0, 0, 0), (0, 0, 1), 0.12, m0)
+    wall.AddCone((0, 0, -0.2), (0, 0, 1), float(f32(0.5235988)), 0.03, 0.15, m1)
+    wall.SetFamily(10)
+    s.SetFamilyFixed(3)
+    s.SetFamilyPrescribedAngVel(10, "0", "2.0943951", "0")
+    s.SetFamilyPrescribedLinVel(4, "0.1", "none", "0")
+    s.DisableContactBetweenFamilies(3, 10)
+    s.SetInitTimeStep(1e-5)
+    s.SetGravitationalAcceleration((0, 0, -9.81))
+    s.SetCDUpdateFreq(5)
+    s.SetExpandFactor(1e-4)
+    return s.Initialize()
+
+
+def read_dump(path):
+    out = {}
+    with open(path, "rb") as f:
+        data = f.read()
+    i = 0
+    while i < len(data):
+        n = int(np.frombuffer(data, np.uint32, 1, i)[0])
+        i += 4
+        name = data[i:i + n].decode()
+        i += n
+        nb = int(np.frombuffer(data, np.uint64, 1, i)[0])
+        i += 8
+        out[name] = data[i:i + nb]
+        i += nb
+    return out
+
+
+@pytest.fixture(scope="module")
+def dump(tmp_path_factory):
+    if shutil.which("g++") is None or not os.path.exists(os.path.join(CUDA_INC, "vector_types.h")):
+        pytest.skip("g++ or the CUDA headers are missing")
+    solver.load_product_library()  # the facade links the product library
+    d = tmp_path_factory.mktemp("facade")
+    exe = build_exe(d)
+    inputs = scene_inputs()
+    inp = write_inputs(d, inputs)
+    subprocess.check_call([exe, str(inp), str(d / "out.bin")])
+    return read_dump(d / "out.bin"), python_scene(*inputs)
+
+
+def write_inputs(d, inputs):
+    inp = d / "inputs.bin"
+    with open(inp, "wb") as f:
+        for a in inputs:
+            a = np.ascontiguousarray(a)
+            f.write(np.uint64(a.size).tobytes())
+            f.write(a.tobytes())
+    return inp
+
+
+def test_flat_arrays_agree_bit_for_bit(dump):
+    cpp, built = dump
+    names = [k for k in cpp if k not in ("params", "prescriptions")]
+    assert len(names) == 45
+    for k in names:
+        py = np.ascontiguousarray(built.arrays[k])
+        assert cpp[k] == py.tobytes(), f"array {k} differs"
+
+
+def build_exe(d):
+    exe = str(d / "facade_dump")
+    libdir = os.path.dirname(solver.LIB_PATH)
+    subprocess.check_call(["g++", "-std=c++17", "-O1", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), "-I",
+                           CUDA_INC, os.path.join(ROOT, "tests", "cpp", "facade_dump.cpp"), "-o", exe, "-L", libdir,
+                           "-ldeme_b200", f"-Wl,-rpath,{libdir}"])
+    return exe
+
+
+def test_params_and_prescriptions_agree(dump):
+    cpp, built = dump
+    assert cpp["params"] == bytes(built.params)
+    assert cpp["prescriptions"] == bytes(built.prescriptions)
+    p = capi.SimParams.from_buffer_copy(cpp["params"])
+    assert p.cd_update_freq == 5 and abs(p.beta - 1e-4) < 1e-9 and (p.nvXp2, p.nvYp2, p.nvZp2) == (21, 21, 22)
+
+
+@pytest.mark.gpu
+def test_cpp_facade_steps_like_the_python_solver(tmp_path):
+    """Initialize + DoStepDynamics through the C++ facade and through the Python Solver on the same scene: the same
+    contact count, kinetic energy within 1e-5, owner positions within 1e-7 m after 3 steps (owner accumulators sum
+    with float atomics, so the last bits may differ between runs)."""
+    solver.load_product_library()
+    exe = build_exe(tmp_path)
+    inputs = scene_inputs()
+    inp = write_inputs(tmp_path, inputs)
+    subprocess.check_call([exe, str(inp), str(tmp_path / "out.bin"), "3"])
+    cpp = read_dump(tmp_path / "out.bin")
+    built = python_scene(*inputs)
+    g = solver.Solver(built)
+    g.step(3)
+    st = g.state()
+    pos = built.decode_positions(st, kernel_literals=False) + np.asarray(built.params.lbf, np.float64)
+    cpos = np.frombuffer(cpp["run_pos"], f32).reshape(-1, 3).astype(np.float64)
+    assert np.abs(cpos - pos).max() <= 1e-7, np.abs(cpos - pos).max()
+    assert int(np.frombuffer(cpp["run_ncontacts"], np.uint32)[0]) == g.num_contacts()
+    ke = float(np.frombuffer(cpp["run_ke"], np.float64)[0])
+    assert abs(ke - g.kinetic_energy()) <= 1e-5 * abs(g.kinetic_energy())
