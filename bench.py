@@ -49,7 +49,7 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms while the timed region runs."""
 
     def __init__(self, index: int):
         self.index = index
@@ -62,12 +62,18 @@ class ClockSampler:
              "clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms",
-                                          "200", "-i", str(self.index)], stdout=subprocess.PIPE,
+                                          "50", "-i", str(self.index)], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except Exception:
             self.proc = None
+
+    def wait_first(self, timeout: float = 5.0):
+        """Block until nvidia-smi has reported once, so that a short timed region is still sampled."""
+        t0 = time.perf_counter()
+        while self.proc and not self.rows and time.perf_counter() - t0 < timeout:
+            time.sleep(0.01)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -104,12 +110,14 @@ def algorithmic_bytes(kernel: str, nS: int, nO: int, nC: int, n_cells: int) -> f
         # material (21 B); per owner: voxel, loc, quat, vel+mass, omega, MOI (80 B) + accumulators (32 B)
         return 41.0 * nC + 21.0 * nS + 112.0 * nO
     if kernel == "pair_find":
-        # per sphere: cell-order position+radius and id (20 B), exact position, owner, radius (44 B), count and
-        # list start (8 B); the cell table once; partner ids written once (4 B per sphere-sphere contact)
-        return 72.0 * nS + 4.0 * n_cells + 4.0 * nC
+        # per sphere: cell-order float position + id (16 B), exact record (position, owner, radius: 32 B), bin
+        # ranges + family (16 B), clump run (8 B); the cell table once; per found pair its (A, B) entry (8 B) and
+        # the count update (4 B)
+        return 72.0 * nS + 4.0 * n_cells + 12.0 * nC
     if kernel == "pair_assemble":
-        # per sphere: offsets, counts, list start (16 B); partner ids read (4 B) and idA, idB, type written (9 B)
-        return 16.0 * nS + 13.0 * nC
+        # scatter: per pair its (A, B) entry (8 B), the count (4 B) and idB written (4 B); assemble: per sphere
+        # offsets and analytical count (9 B), per contact idB read and idA, idB, type written (13 B)
+        return 9.0 * nS + 29.0 * nC
     if kernel == "integrate":
         return 160.0 * nO
     if kernel == "sort_onesweep":
@@ -184,7 +192,7 @@ def cpu_baseline_sample(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--clumps", type=int, default=1_000_000)
@@ -268,6 +276,7 @@ def main():
     # ---- warm-up (the clock sampler starts here so it has samples when the timed region is short) ----
     sampler = ClockSampler(local_rank)
     sampler.start()
+    sampler.wait_first()
     s.step(args.warmup)
     s.sync()
     torch.cuda.synchronize()
