@@ -1,0 +1,635 @@
+// adjoint.cu -- adjoint of the DEM step for scenes of single spheres with plane walls (no reference counterpart).
+//
+// deme_adjoint_record runs the forward steps and keeps a checkpoint (owner state and the current contact list with
+// its history) every K steps.  deme_adjoint_backward walks the checkpoints from the last: it restores one,
+// recomputes its K steps with the production kernels while recording each step's state and contact list, then
+// runs the reverse pass over those steps.  Per step the contact set is the one the forward pass found, held fixed.
+// The reverse pass is
+//   * k_adj_integrate: the Extended Taylor update x' = x + h v + h^2/2 a, v' = v + h a, w' = w + h alpha
+//     (src/kernel/DEMIntegrationKernels.cu:46-179) reversed per owner, which turns the state gradients into the
+//     gradients of the owner's summed force and torque;
+//   * k_adj_contact: per contact, the derivative of the built-in frictional Hertz-Mindlin law (adjoint_law.cuh)
+//     and of its geometry, scattered onto both owners' position, velocity and angular-velocity gradients, the
+//     gradient of the incoming history, and the material-parameter gradients (FP64 accumulators);
+//   * k_adj_hist_scatter: the history map (src/kernel/DEMHistoryMappingKernels.cu) reversed, so the incoming-history
+//     gradient reaches the previous step's updated history.
+// Angular velocities are differentiated in the world frame, where an isotropic sphere's orientation does not enter
+// the contact law.  The model is evaluated from the recorded FP32 state; the state gradients are carried and
+// accumulated in FP64 (they sum many contributions of both signs), as are the material-parameter gradients.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "adjoint_law.cuh"
+#include "handle.cuh"
+#include "profiler.cuh"
+
+using namespace deme_b200;
+
+struct Checkpoint {
+    uint64_t* voxel = nullptr;
+    ushort4* loc = nullptr;
+    float4* quat = nullptr;
+    float4* vel = nullptr;
+    float4* omg = nullptr;
+    uint32_t n = 0, cap = 0;
+    uint32_t* idA = nullptr;
+    uint32_t* idB = nullptr;
+    uint8_t* type = nullptr;
+    float4* hist = nullptr;
+    uint32_t* off = nullptr;
+    int64_t steps = 0;
+    double t = 0.0;
+};
+
+struct AdjointTape {
+    int K = 0;
+    int nSteps = 0;
+    std::vector<Checkpoint> cps;  // cps[j]: state before step j*K
+    Checkpoint fin;               // state after the last step
+    // one segment of recorded steps
+    double* X = nullptr;  // K x nO x 3 positions (world, relative to the domain corner)
+    float4* V = nullptr;  // K x nO velocities
+    float4* W = nullptr;  // K x nO angular velocities (world frame)
+    uint32_t poolCap = 0;
+    uint32_t* cA = nullptr;
+    uint32_t* cB = nullptr;
+    uint8_t* cT = nullptr;
+    float4* cH = nullptr;
+    uint32_t* cM = nullptr;
+    std::vector<uint32_t> stepN, stepBase;
+    // reverse-pass buffers
+    double *lx = nullptr, *lv = nullptr, *lw = nullptr, *nlx = nullptr, *nlv = nullptr, *nlw = nullptr;  // 3 per owner
+    double *lF = nullptr, *lT = nullptr;
+    uint32_t gCap = 0;
+    float4 *gA = nullptr, *gB = nullptr, *gC = nullptr;  // history gradients (current, previous, carried)
+    double* gmat = nullptr;                             // nM x 4
+};
+
+namespace {
+
+inline unsigned nblk(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+// State of every owner at a step start: position (double, kernel literals), velocity, world-frame angular velocity.
+__global__ void k_adj_record_state(SimConsts k, StateView s, uint32_t nO, double* X, float4* V, float4* W) {
+    const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= nO) return;
+    const ushort4 l = s.loc[o];
+    double x, y, z;
+    voxel_to_pos(k, s.voxel[o], l.x, l.y, l.z, x, y, z);
+    X[3 * (size_t)o] = x;
+    X[3 * (size_t)o + 1] = y;
+    X[3 * (size_t)o + 2] = z;
+    V[o] = s.vel[o];
+    const float4 q = s.quat[o];
+    float4 w = s.omg[o];
+    rot_f(w.x, w.y, w.z, q.x, q.y, q.z, q.w);
+    W[o] = w;
+}
+
+__device__ __forceinline__ bool owner_free(const StateView& s, uint32_t o, uint32_t nClumps) {
+    return o < nClumps && !s.presc[s.loc[o].w].used;
+}
+
+// Reverse of x' = x + h v + h^2/2 a, v' = v + h a, w' = w + h alpha (a = F/m + g, alpha = T/I): the gradients of
+// the owner's summed force and torque, and the direct part of the step-start state gradients.
+__global__ void k_adj_integrate(StateView s, uint32_t nO, uint32_t nClumps, double h, const double* lx,
+                                const double* lv, const double* lw, double* lF, double* lT, double* nlx, double* nlv,
+                                double* nlw) {
+    const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= nO) return;
+    const bool f = owner_free(s, o, nClumps);
+    const double m = s.vel[o].w, I = s.moi[o].x;
+    const double c = 0.5 * h * h;
+    for (int a = 0; a < 3; a++) {
+        const size_t q = 3 * (size_t)o + a;
+        const double x = lx[q], v = lv[q], w = lw[q];
+        lF[q] = f ? (c * x + h * v) / m : 0.0;
+        lT[q] = f ? h * w / I : 0.0;
+        nlx[q] = f ? x : 0.0;
+        nlv[q] = f ? v + h * x : 0.0;
+        nlw[q] = f ? w : 0.0;
+    }
+}
+
+__device__ __forceinline__ void add3(double* a, uint32_t o, dv3 g) {
+    atomicAdd(a + 3 * (size_t)o, g.x);
+    atomicAdd(a + 3 * (size_t)o + 1, g.y);
+    atomicAdd(a + 3 * (size_t)o + 2, g.z);
+}
+__device__ __forceinline__ dv3 ld3(const double* a, uint32_t o) {
+    return mk(a[3 * (size_t)o], a[3 * (size_t)o + 1], a[3 * (size_t)o + 2]);
+}
+
+__device__ __forceinline__ double dbeta_de(double e) {
+    e = e > kTiny ? e : kTiny;
+    const double le = log(e);
+    const double d = le * le + kPi2;
+    return (1.0 / e) * kPi2 / (d * sqrt(d));
+}
+
+// Per contact of one recorded step: the law's derivative, scattered to both owners and to the material gradients.
+__global__ void __launch_bounds__(256) k_adj_contact(SimConsts k, StateView s, uint32_t n, uint32_t nClumps,
+                                                     uint32_t nM, const uint32_t* cA, const uint32_t* cB,
+                                                     const uint8_t* cT, const float4* cH, const double* X,
+                                                     const float4* V, const float4* W, const double* lF,
+                                                     const double* lT, const float4* gHout, float4* gHin,
+                                                     double* nlx, double* nlv, double* nlw, double* gmat) {
+    extern __shared__ double s_g[];  // nM x (E, CoR, mu, Crr)
+    for (uint32_t t = threadIdx.x; t < 4u * nM; t += blockDim.x) s_g[t] = 0.0;
+    __syncthreads();
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const uint32_t sA = cA[i], bId = cB[i];
+        const bool ss = cT[i] == DEME_SPHERE_SPHERE_CONTACT;
+        bool ok = index_ok(k.err, 20, sA, k.n_spheres) && index_ok(k.err, 21, bId, ss ? k.n_spheres : k.n_anal);
+        float4 gin = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (ok) {
+            const uint32_t oA = s.sOwner[sA];
+            const dv3 xA = mk(X[3 * (size_t)oA], X[3 * (size_t)oA + 1], X[3 * (size_t)oA + 2]);
+            const double rA = (double)s.sph[sA].w;
+            const double mA = (double)s.vel[oA].w;
+            const uint32_t matA = s.sMat[sA];
+            LawIn in;
+            uint32_t oB = 0, matB = 0;
+            double rB, mB, D = 1.0, a_ = 0.0, b_ = 0.0;
+            dv3 nrm;
+            bool active = false;
+            if (ss) {
+                oB = s.sOwner[bId];
+                const dv3 xB = mk(X[3 * (size_t)oB], X[3 * (size_t)oB + 1], X[3 * (size_t)oB + 2]);
+                rB = (double)s.sph[bId].w;
+                mB = (double)s.vel[oB].w;
+                matB = s.sMat[bId];
+                const dv3 d = xA - xB;
+                D = norm(d);
+                active = D <= rA + rB && D > 0.0;
+                if (active) {
+                    nrm = (1.0 / D) * d;
+                    in.delta = rA + rB - D;
+                    a_ = rA - in.delta / 2.0;
+                    b_ = rB - in.delta / 2.0;
+                    in.rAv = (-a_) * nrm;
+                    in.rBv = b_ * nrm;
+                    in.vB = to_dv3(V[oB]);
+                    in.wB = to_dv3(W[oB]);
+                }
+            } else {
+                const AnalPlaced ap = s.anal[bId];
+                oB = ap.owner;
+                nrm = mk(ap.dx, ap.dy, ap.dz);
+                const double dist = dot(xA - mk(ap.x, ap.y, ap.z), nrm);
+                in.delta = (rA - dist) / 2.0;
+                active = ap.type == DEME_ANAL_PLANE && in.delta >= 0.0;
+                rB = (double)1e15f;
+                mB = (double)ap.mass;
+                matB = ap.material;
+                in.rAv = (-(dist + in.delta)) * nrm;
+                in.rBv = mk(0, 0, 0);
+                in.vB = in.wB = mk(0, 0, 0);
+            }
+            if (active) {
+                in.n = nrm;
+                in.vA = to_dv3(V[oA]);
+                in.wA = to_dv3(W[oA]);
+                const float4 hi = cH[i];
+                in.dtan = mk(hi.x, hi.y, hi.z);
+                in.tau = hi.w;
+                in.meff = mA * mB / (mA + mB);
+                in.Rs = rA * rB / (rA + rB);
+                in.h = (double)k.h;
+                const double EA = s.mat.E[matA], EB = s.mat.E[matB], nuA = s.mat.nu[matA], nuB = s.mat.nu[matB];
+                const double invE = (1.0 - nuA * nuA) / EA + (1.0 - nuB * nuB) / EB;
+                in.Es = 1.0 / invE;
+                const double invG = 2.0 * (2.0 - nuA) * (1.0 + nuA) / EA + 2.0 * (2.0 - nuB) * (1.0 + nuB) / EB;
+                in.Gs = 1.0 / invG;
+                const double corA = s.mat.CoR[matA], corB = s.mat.CoR[matB];
+                const double cor = corA < corB ? corA : corB;
+                const uint32_t corSrc = corA < corB ? matA : matB;
+                const double muA = s.mat.mu[matA], muB = s.mat.mu[matB];
+                in.mu = muA > muB ? muA : muB;
+                const uint32_t muSrc = muA > muB ? matA : matB;
+                const double crA = s.mat.Crr[matA], crB = s.mat.Crr[matB];
+                in.crr = crA > crB ? crA : crB;
+                const uint32_t crSrc = crA > crB ? matA : matB;
+                const double le = log(cor > kTiny ? cor : kTiny);
+                in.be = le / sqrt(le * le + kPi2);
+                // upstream gradients: forces and torques of both owners (B only when it is a sphere)
+                const dv3 gFA = ld3(lF, oA), gTA = ld3(lT, oA);
+                const dv3 gFB = ss ? ld3(lF, oB) : mk(0, 0, 0), gTB = ss ? ld3(lT, oB) : mk(0, 0, 0);
+                const dv3 g_u = cross(gTA, in.rAv) - cross(gTB, in.rBv);
+                const float4 gho = gHout ? gHout[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+                dv3 f, t;
+                LawGrad G;
+                law_vjp(in, gFA - gFB + g_u, g_u, mk(gho.x, gho.y, gho.z), gho.w, f, t, G);
+                const dv3 u = f + t;
+                G.rAv += cross(u, gTA);
+                if (ss) G.rBv -= cross(u, gTB);
+                if (ss) {
+                    const double g_a = -dot(G.rAv, nrm), g_b = dot(G.rBv, nrm);
+                    const dv3 g_n = G.n - a_ * G.rAv + b_ * G.rBv;
+                    const double g_delta = G.delta - g_a / 2.0 - g_b / 2.0;
+                    const dv3 g_d = (1.0 / D) * (g_n - dot(g_n, nrm) * nrm) + (-g_delta) * nrm;
+                    add3(nlx, oA, g_d);
+                    add3(nlx, oB, -g_d);
+                    add3(nlv, oB, G.vB);
+                    add3(nlw, oB, G.wB);
+                } else {
+                    const double g_dist = -G.delta / 2.0 - dot(G.rAv, nrm) / 2.0;
+                    add3(nlx, oA, g_dist * nrm);
+                }
+                add3(nlv, oA, G.vA);
+                add3(nlw, oA, G.wA);
+                gin = make_float4((float)G.dtan.x, (float)G.dtan.y, (float)G.dtan.z, (float)G.tau);
+                // material parameters (matProxy2ContactParam's derivatives)
+                const double Es2 = in.Es * in.Es, Gs2 = in.Gs * in.Gs;
+                atomicAdd(&s_g[4 * matA], G.Es * Es2 * (1.0 - nuA * nuA) / (EA * EA) +
+                                              G.Gs * Gs2 * 2.0 * (2.0 - nuA) * (1.0 + nuA) / (EA * EA));
+                atomicAdd(&s_g[4 * matB], G.Es * Es2 * (1.0 - nuB * nuB) / (EB * EB) +
+                                              G.Gs * Gs2 * 2.0 * (2.0 - nuB) * (1.0 + nuB) / (EB * EB));
+                atomicAdd(&s_g[4 * corSrc + 1], G.be * dbeta_de(cor));
+                atomicAdd(&s_g[4 * muSrc + 2], G.mu);
+                atomicAdd(&s_g[4 * crSrc + 3], G.crr);
+            }
+        }
+        gHin[i] = gin;
+    }
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < 4u * nM; t += blockDim.x)
+        if (s_g[t] != 0.0) atomicAdd(&gmat[t], s_g[t]);
+}
+
+// The history map reversed: the incoming-history gradient of a contact goes to its partner in the previous list.
+__global__ void k_adj_hist_scatter(uint32_t n, const uint32_t* map, const float4* gHin, float4* gPrev, uint32_t nPrev,
+                                   uint32_t* err) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t m = map[i];
+    if (m != DEME_NULL_MAPPING_PARTNER && index_ok(err, 22, m, nPrev)) gPrev[m] = gHin[i];
+}
+
+// Re-indexes history gradients from one list (CSR offsets `off` by sphere) to another holding the same contacts
+// (the list a checkpoint stored and the one recomputed from it can differ in order or, rarely, in members).
+__global__ void k_adj_rekey(uint32_t n, const uint32_t* A, const uint32_t* B, const uint8_t* T, const uint32_t* off,
+                            const uint32_t* oB, const uint8_t* oT, uint32_t nOld, const float4* gOld, float4* gNew,
+                            uint32_t nS, uint32_t* err) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 g = make_float4(0.f, 0.f, 0.f, 0.f);
+    const uint32_t a = A[i];
+    if (index_ok(err, 23, a, nS)) {
+        uint32_t lo = off[a], hi = off[a + 1];
+        if (hi > nOld) hi = nOld;
+        const uint64_t key = ((uint64_t)(T[i] == DEME_SPHERE_SPHERE_CONTACT ? 1u : 0u) << 32) | B[i];
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            const uint64_t km = ((uint64_t)(oT[mid] == DEME_SPHERE_SPHERE_CONTACT ? 1u : 0u) << 32) | oB[mid];
+            if (km < key)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        if (lo < min(off[a + 1], nOld) && oB[lo] == B[i] && oT[lo] == T[i]) g = gOld[lo];
+    }
+    gNew[i] = g;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------------ host ----
+namespace {
+
+int32_t alloc_checkpoint(deme_handle* h, Checkpoint& c, uint32_t nContacts) {
+    if (!c.voxel) {
+        TRY(dalloc_n(h, &c.voxel, h->nO));
+        TRY(dalloc_n(h, &c.loc, h->nO));
+        TRY(dalloc_n(h, &c.quat, h->nO));
+        TRY(dalloc_n(h, &c.vel, h->nO));
+        TRY(dalloc_n(h, &c.omg, h->nO));
+        TRY(dalloc_n(h, &c.off, (size_t)h->nS + 1));
+    }
+    if (nContacts > c.cap || !c.idA) {
+        dfree(h, c.idA);
+        dfree(h, c.idB);
+        dfree(h, c.type);
+        dfree(h, c.hist);
+        c.idA = c.idB = nullptr;
+        c.type = nullptr;
+        c.hist = nullptr;
+        const uint32_t cap = std::max<uint32_t>(nContacts + nContacts / 8 + 64, 64u);
+        TRY(dalloc_n(h, &c.idA, cap));
+        TRY(dalloc_n(h, &c.idB, cap));
+        TRY(dalloc_n(h, &c.type, cap));
+        TRY(dalloc_n(h, &c.hist, cap));
+        c.cap = cap;
+    }
+    return DEME_OK;
+}
+
+void free_checkpoint(deme_handle* h, Checkpoint& c) {
+    for (void* p : {(void*)c.voxel, (void*)c.loc, (void*)c.quat, (void*)c.vel, (void*)c.omg, (void*)c.off,
+                    (void*)c.idA, (void*)c.idB, (void*)c.type, (void*)c.hist})
+        dfree(h, p);
+    c = Checkpoint{};
+}
+
+int32_t save_checkpoint(deme_handle* h, Checkpoint& c) {
+    const uint32_t n = h->nContacts;
+    TRY(alloc_checkpoint(h, c, n));
+    cudaStream_t st = h->st_dt;
+    const ContactBuf& L = h->lists[h->cur];
+    CUDA_TRY(h, cudaMemcpyAsync(c.voxel, h->voxel, h->nO * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(h, cudaMemcpyAsync(c.loc, h->loc, h->nO * sizeof(ushort4), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(h, cudaMemcpyAsync(c.quat, h->quat, h->nO * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(h, cudaMemcpyAsync(c.vel, h->vel, h->nO * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(h, cudaMemcpyAsync(c.omg, h->omg, h->nO * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    if (n) {
+        CUDA_TRY(h, cudaMemcpyAsync(c.idA, L.idA, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+        CUDA_TRY(h, cudaMemcpyAsync(c.idB, L.idB, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+        CUDA_TRY(h, cudaMemcpyAsync(c.type, L.type, n * sizeof(uint8_t), cudaMemcpyDeviceToDevice, st));
+        CUDA_TRY(h, cudaMemcpyAsync(c.hist, L.hist, n * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    }
+    CUDA_TRY(h, cudaMemcpyAsync(c.off, L.off, ((size_t)h->nS + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    c.n = n;
+    c.steps = h->steps;
+    c.t = h->t;
+    return DEME_OK;
+}
+
+int32_t restore_checkpoint(deme_handle* h, const Checkpoint& c) {
+    cudaStream_t st = h->st_dt;
+    ContactBuf& L = h->lists[h->cur];
+    TRY(ensure_list(h, L, c.n));
+    CUDA_TRY(h, cudaMemcpyAsync(h->voxel, c.voxel, h->nO * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(h, cudaMemcpyAsync(h->loc, c.loc, h->nO * sizeof(ushort4), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(h, cudaMemcpyAsync(h->quat, c.quat, h->nO * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(h, cudaMemcpyAsync(h->vel, c.vel, h->nO * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(h, cudaMemcpyAsync(h->omg, c.omg, h->nO * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    if (c.n) {
+        CUDA_TRY(h, cudaMemcpyAsync(L.idA, c.idA, c.n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+        CUDA_TRY(h, cudaMemcpyAsync(L.idB, c.idB, c.n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+        CUDA_TRY(h, cudaMemcpyAsync(L.type, c.type, c.n * sizeof(uint8_t), cudaMemcpyDeviceToDevice, st));
+        CUDA_TRY(h, cudaMemcpyAsync(L.hist, c.hist, c.n * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    }
+    CUDA_TRY(h, cudaMemcpyAsync(L.off, c.off, ((size_t)h->nS + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    h->nContacts = c.n;
+    h->steps = c.steps;
+    h->t = c.t;
+    h->outsValid = false;
+    return DEME_OK;
+}
+
+// The scenes the adjoint covers: single spheres (relative position 0, isotropic inertia) with plane walls, the
+// built-in model, Extended Taylor integration, contact detection every step, no prescribed sphere families.
+int32_t check_adjoint_scene(deme_handle* h) {
+    if (h->userForce.lib) {
+        h->err = "adjoint: only the built-in Hertz-Mindlin model is differentiated";
+        return DEME_ERR_INVALID;
+    }
+    if (h->params.integrator != DEME_INTEGRATOR_EXTENDED_TAYLOR || h->params.cd_update_freq > 1) {
+        h->err = "adjoint: needs Extended Taylor integration and contact detection every step";
+        return DEME_ERR_INVALID;
+    }
+    std::vector<float4> sph(h->nS), moi(h->nO);
+    std::vector<uint32_t> owner(h->nS);
+    std::vector<ushort4> loc(h->nO);
+    std::vector<AnalRaw> anal(std::max(h->nA, 1u));
+    std::vector<Prescription> presc(DEME_NUM_FAMILIES);
+    CUDA_TRY(h, cudaMemcpy(sph.data(), h->sph, h->nS * sizeof(float4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(owner.data(), h->sOwner, h->nS * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(moi.data(), h->moi, h->nO * sizeof(float4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(loc.data(), h->loc, h->nO * sizeof(ushort4), cudaMemcpyDeviceToHost));
+    if (h->nA) CUDA_TRY(h, cudaMemcpy(anal.data(), h->analRaw, h->nA * sizeof(AnalRaw), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(presc.data(), h->presc, DEME_NUM_FAMILIES * sizeof(Prescription), cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < h->nS; i++) {
+        if (owner[i] != i || sph[i].x != 0.f || sph[i].y != 0.f || sph[i].z != 0.f) {
+            h->err = "adjoint: every owner must be one sphere centred on it";
+            return DEME_ERR_INVALID;
+        }
+        if (moi[i].x != moi[i].y || moi[i].x != moi[i].z) {
+            h->err = "adjoint: sphere moments of inertia must be isotropic";
+            return DEME_ERR_INVALID;
+        }
+        if (presc[loc[i].w].used) {
+            h->err = "adjoint: sphere families must not be prescribed";
+            return DEME_ERR_INVALID;
+        }
+    }
+    for (uint32_t a = 0; a < h->nA; a++)
+        if (anal[a].type != DEME_ANAL_PLANE) {
+            h->err = "adjoint: walls must be planes";
+            return DEME_ERR_INVALID;
+        }
+    return DEME_OK;
+}
+
+}  // namespace
+
+void adjoint_release(deme_handle* h) {
+    if (!h->adj) return;
+    AdjointTape* t = h->adj;
+    for (Checkpoint& c : t->cps) free_checkpoint(h, c);
+    free_checkpoint(h, t->fin);
+    for (void* p : {(void*)t->X, (void*)t->V, (void*)t->W, (void*)t->cA, (void*)t->cB, (void*)t->cT, (void*)t->cH,
+                    (void*)t->cM, (void*)t->lx, (void*)t->lv, (void*)t->lw, (void*)t->nlx, (void*)t->nlv,
+                    (void*)t->nlw, (void*)t->lF, (void*)t->lT, (void*)t->gA, (void*)t->gB, (void*)t->gC,
+                    (void*)t->gmat})
+        dfree(h, p);
+    delete t;
+    h->adj = nullptr;
+}
+
+extern "C" {
+
+int32_t deme_set_material(deme_handle* h, uint32_t m, float E, float nu, float CoR, float mu, float Crr) {
+    if (!h || m >= h->nM) return DEME_ERR_INVALID;
+    const float v[5] = {E, nu, CoR, mu, Crr};
+    for (int k = 0; k < 5; k++)
+        CUDA_TRY(h, cudaMemcpy(h->mat + (size_t)k * h->nM + m, &v[k], sizeof(float), cudaMemcpyHostToDevice));
+    return DEME_OK;
+}
+
+int32_t deme_adjoint_record(deme_handle* h, int32_t n_steps, int32_t checkpoint_every) {
+    if (!h || n_steps <= 0 || checkpoint_every <= 0) return DEME_ERR_INVALID;
+    TRY(check_adjoint_scene(h));
+    adjoint_release(h);
+    h->adj = new AdjointTape();
+    AdjointTape* t = h->adj;
+    t->K = checkpoint_every;
+    t->nSteps = n_steps;
+    t->cps.resize((size_t)((n_steps + checkpoint_every - 1) / checkpoint_every));
+    for (int32_t s = 0; s < n_steps; s++) {
+        if (s % checkpoint_every == 0) TRY(save_checkpoint(h, t->cps[(size_t)(s / checkpoint_every)]));
+        TRY(deme_step(h, 1));
+    }
+    TRY(save_checkpoint(h, t->fin));
+    CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
+    return read_device_errors(h);
+}
+
+int32_t deme_adjoint_backward(deme_handle* h, const deme_adjoint_seed* seed, deme_adjoint_grads* out) {
+    if (!h || !out) return DEME_ERR_INVALID;
+    AdjointTape* t = h->adj;
+    if (!t) {
+        h->err = "deme_adjoint_backward: no recorded window (call deme_adjoint_record first)";
+        return DEME_ERR_STATE;
+    }
+    const uint32_t nO = h->nO, nM = std::max(h->nM, 1u);
+    const int K = t->K, nSeg = (int)t->cps.size();
+    cudaStream_t st = h->st_dt;
+    const SimConsts& k = h->k;
+    // buffers
+    if (!t->lx) {
+        for (double** p : {&t->lx, &t->lv, &t->lw, &t->nlx, &t->nlv, &t->nlw, &t->lF, &t->lT})
+            TRY(dalloc_n(h, p, 3 * (size_t)nO));
+        TRY(dalloc_n(h, &t->gmat, 4 * (size_t)nM));
+        TRY(dalloc_n(h, &t->X, (size_t)K * nO * 3));
+        TRY(dalloc_n(h, &t->V, (size_t)K * nO));
+        TRY(dalloc_n(h, &t->W, (size_t)K * nO));
+    }
+    CUDA_TRY(h, cudaMemsetAsync(t->gmat, 0, 4 * (size_t)nM * sizeof(double), st));
+    {
+        const double* src[3] = {seed ? seed->d_pos : nullptr, seed ? seed->d_vel : nullptr,
+                                seed ? seed->d_angvel : nullptr};
+        double* dst[3] = {t->lx, t->lv, t->lw};
+        for (int a = 0; a < 3; a++) {
+            if (src[a])
+                CUDA_TRY(h, cudaMemcpy(dst[a], src[a], 3 * (size_t)nO * sizeof(double), cudaMemcpyHostToDevice));
+            else
+                CUDA_TRY(h, cudaMemset(dst[a], 0, 3 * (size_t)nO * sizeof(double)));
+        }
+    }
+    uint32_t gCap = t->gCap;
+    auto ensure_g = [&](uint32_t n) -> int32_t {
+        if (n <= gCap && t->gA) return DEME_OK;
+        // the carried buffer keeps its content across a resize
+        const uint32_t cap = n + n / 4 + 1024;
+        float4* nc = nullptr;
+        TRY(dalloc_n(h, &nc, cap));
+        if (t->gC && gCap) CUDA_TRY(h, cudaMemcpyAsync(nc, t->gC, gCap * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+        CUDA_TRY(h, cudaStreamSynchronize(st));
+        dfree(h, t->gA);
+        dfree(h, t->gB);
+        dfree(h, t->gC);
+        t->gA = t->gB = nullptr;
+        TRY(dalloc_n(h, &t->gA, cap));
+        TRY(dalloc_n(h, &t->gB, cap));
+        t->gC = nc;
+        gCap = t->gCap = cap;
+        return DEME_OK;
+    };
+    for (int j = nSeg - 1; j >= 0; j--) {
+        const Checkpoint& cp = t->cps[(size_t)j];
+        const int len = std::min(K, t->nSteps - j * K);
+        // ---- recompute the segment, recording every step's state and contacts ----
+        TRY(restore_checkpoint(h, cp));
+        t->stepN.assign((size_t)len, 0);
+        t->stepBase.assign((size_t)len, 0);
+        uint32_t base = 0;
+        for (int s = 0; s < len; s++) {
+            StateView sv = h->state_view();
+            k_adj_record_state<<<nblk(nO, 256), 256, 0, st>>>(k, sv, nO, t->X + (size_t)s * nO * 3,
+                                                               t->V + (size_t)s * nO, t->W + (size_t)s * nO);
+            TRY(deme_detect_contacts(h));
+            const uint32_t n = h->nContacts;
+            if (base + n > t->poolCap) {  // grow the pool, keeping the steps recorded so far
+                const uint32_t cap = std::max<uint32_t>((uint32_t)std::min<uint64_t>(0xFFFFFFF0ull,
+                                                        (uint64_t)(base + n) * 3 / 2 + (uint64_t)len * 1024), 4096u);
+                uint32_t *nA = nullptr, *nB = nullptr, *nM2 = nullptr;
+                uint8_t* nT = nullptr;
+                float4* nH = nullptr;
+                TRY(dalloc_n(h, &nA, cap));
+                TRY(dalloc_n(h, &nB, cap));
+                TRY(dalloc_n(h, &nT, cap));
+                TRY(dalloc_n(h, &nH, cap));
+                TRY(dalloc_n(h, &nM2, cap));
+                if (base) {
+                    CUDA_TRY(h, cudaMemcpyAsync(nA, t->cA, base * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+                    CUDA_TRY(h, cudaMemcpyAsync(nB, t->cB, base * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+                    CUDA_TRY(h, cudaMemcpyAsync(nT, t->cT, base * sizeof(uint8_t), cudaMemcpyDeviceToDevice, st));
+                    CUDA_TRY(h, cudaMemcpyAsync(nH, t->cH, base * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+                    CUDA_TRY(h, cudaMemcpyAsync(nM2, t->cM, base * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+                }
+                CUDA_TRY(h, cudaStreamSynchronize(st));
+                dfree(h, t->cA);
+                dfree(h, t->cB);
+                dfree(h, t->cT);
+                dfree(h, t->cH);
+                dfree(h, t->cM);
+                t->cA = nA;
+                t->cB = nB;
+                t->cT = nT;
+                t->cH = nH;
+                t->cM = nM2;
+                t->poolCap = cap;
+            }
+            const ContactBuf& L = h->lists[h->cur];
+            if (n) {
+                CUDA_TRY(h, cudaMemcpyAsync(t->cA + base, L.idA, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+                CUDA_TRY(h, cudaMemcpyAsync(t->cB + base, L.idB, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+                CUDA_TRY(h, cudaMemcpyAsync(t->cT + base, L.type, n * sizeof(uint8_t), cudaMemcpyDeviceToDevice, st));
+                CUDA_TRY(h, cudaMemcpyAsync(t->cH + base, L.hist, n * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+                CUDA_TRY(h, cudaMemcpyAsync(t->cM + base, L.mapping, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                                            st));
+            }
+            t->stepN[(size_t)s] = n;
+            t->stepBase[(size_t)s] = base;
+            base += n;
+            TRY(deme_compute_forces(h));
+            TRY(deme_integrate(h));
+        }
+        uint32_t need = cp.n;
+        for (uint32_t n : t->stepN) need = std::max(need, n);
+        if (j < nSeg - 1) need = std::max(need, t->cps[(size_t)j + 1].n);
+        TRY(ensure_g(need));
+        // ---- the history gradient entering the segment's last step ----
+        const float4* gOut = nullptr;
+        if (j < nSeg - 1) {
+            const Checkpoint& nx = t->cps[(size_t)j + 1];
+            const uint32_t n = t->stepN[(size_t)len - 1], b = t->stepBase[(size_t)len - 1];
+            if (n) {
+                k_adj_rekey<<<nblk(n, 256), 256, 0, st>>>(n, t->cA + b, t->cB + b, t->cT + b, nx.off, nx.idB, nx.type,
+                                                          nx.n, t->gC, t->gA, h->nS, h->dErr);
+                gOut = t->gA;
+            }
+        }
+        // ---- reverse over the segment ----
+        for (int s = len - 1; s >= 0; s--) {
+            const uint32_t n = t->stepN[(size_t)s], b = t->stepBase[(size_t)s];
+            StateView sv = h->state_view();
+            k_adj_integrate<<<nblk(nO, 256), 256, 0, st>>>(sv, nO, h->nClumps, (double)k.h, t->lx, t->lv, t->lw, t->lF, t->lT,
+                                                            t->nlx, t->nlv, t->nlw);
+            if (n)
+                k_adj_contact<<<nblk(n, 256), 256, 4 * nM * sizeof(double), st>>>(
+                    k, sv, n, h->nClumps, nM, t->cA + b, t->cB + b, t->cT + b, t->cH + b, t->X + (size_t)s * nO * 3,
+                    t->V + (size_t)s * nO, t->W + (size_t)s * nO, t->lF, t->lT, gOut, t->gB, t->nlx, t->nlv, t->nlw,
+                    t->gmat);
+            std::swap(t->lx, t->nlx);
+            std::swap(t->lv, t->nlv);
+            std::swap(t->lw, t->nlw);
+            // incoming-history gradients go to the previous list (the previous step's, or the checkpoint's)
+            const uint32_t nPrev = s > 0 ? t->stepN[(size_t)s - 1] : cp.n;
+            float4* dst = s > 0 ? t->gA : t->gC;
+            if (nPrev) CUDA_TRY(h, cudaMemsetAsync(dst, 0, nPrev * sizeof(float4), st));
+            if (n && nPrev)
+                k_adj_hist_scatter<<<nblk(n, 256), 256, 0, st>>>(n, t->cM + b, t->gB, dst, nPrev, h->dErr);
+            gOut = t->gA;
+        }
+        TRY(check_launch(h, "adjoint"));
+    }
+    // ---- results ----
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    double* dsts[3] = {out->d_pos0, out->d_vel0, out->d_angvel0};
+    const double* srcs[3] = {t->lx, t->lv, t->lw};
+    for (int a = 0; a < 3; a++)
+        if (dsts[a])
+            CUDA_TRY(h, cudaMemcpy(dsts[a], srcs[a], 3 * (size_t)nO * sizeof(double), cudaMemcpyDeviceToHost));
+    if (out->d_material)
+        CUDA_TRY(h, cudaMemcpy(out->d_material, t->gmat, 4 * (size_t)h->nM * sizeof(double), cudaMemcpyDeviceToHost));
+    TRY(restore_checkpoint(h, t->fin));
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    return read_device_errors(h);
+}
+
+}  // extern "C"

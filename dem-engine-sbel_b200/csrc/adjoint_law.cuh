@@ -1,0 +1,174 @@
+// adjoint_law.cuh -- reverse-mode derivative of one contact of the built-in frictional Hertz-Mindlin model, for the
+// adjoint of a sphere step (adjoint.cu).  The forward part restates force_model_hertz.cuh for single-sphere owners
+// with their angular velocity in the world frame, in double precision; the reverse part propagates the gradients
+// of the contact's force, torque-only force and updated history back to its inputs (relative position, both
+// velocities and angular velocities, the incoming history) and to the pair's material parameters
+// (E*, G*, beta, mu, Crr).  Each reverse step is the derivative of the forward line it follows.
+#pragma once
+#include "device_common.cuh"
+
+namespace deme_b200 {
+
+struct dv3 {
+    double x, y, z;
+};
+__device__ __forceinline__ dv3 mk(double x, double y, double z) { return dv3{x, y, z}; }
+__device__ __forceinline__ dv3 operator+(dv3 a, dv3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ dv3 operator-(dv3 a, dv3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ dv3 operator-(dv3 a) { return mk(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ dv3 operator*(double s, dv3 a) { return mk(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ void operator+=(dv3& a, dv3 b) { a = a + b; }
+__device__ __forceinline__ void operator-=(dv3& a, dv3 b) { a = a - b; }
+__device__ __forceinline__ double dot(dv3 a, dv3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ dv3 cross(dv3 a, dv3 b) {
+    return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ double norm(dv3 a) { return sqrt(dot(a, a)); }
+__device__ __forceinline__ dv3 to_dv3(float4 v) { return mk(v.x, v.y, v.z); }
+
+constexpr double kC5 = 1.825741858350554;  // 2 sqrt(5/6)
+constexpr double kPi2 = 9.869604401089358;
+constexpr double kTiny = 1e-12;
+
+struct LawIn {
+    dv3 n, rAv, rBv;  // unit normal B -> A and lever arms from the owners to the contact point
+    double delta;     // overlap depth
+    dv3 vA, vB, wA, wB;
+    dv3 dtan;         // incoming tangential displacement history
+    double tau;       // incoming contact duration
+    double Es, Gs, be, mu, crr, meff, Rs, h;
+};
+
+struct LawGrad {
+    dv3 n, rAv, rBv;
+    double delta;
+    dv3 vA, vB, wA, wB, dtan;
+    double tau, Es, Gs, be, mu, crr;
+};
+
+// Forward: contact force f, torque-only force t, updated history (dt3, tau2).  Reverse: given g_f, g_t and the
+// gradients of the updated history, fills G.
+__device__ __forceinline__ void law_vjp(const LawIn& in, dv3 g_f, dv3 g_t, dv3 g_dt3, double g_tau2, dv3& f_out,
+                                        dv3& t_out, LawGrad& G) {
+    const dv3 n = in.n;
+    // ---- forward, keeping what the reverse pass needs ----
+    const dv3 WA = cross(in.wA, in.rAv), WB = cross(in.wB, in.rBv);
+    const dv3 vr = in.vA + WA - in.vB - WB;
+    const double p = dot(vr, n);
+    const dv3 vt = vr - p * n;
+    const dv3 dt1 = in.dtan + in.h * vt;
+    const double q = dot(dt1, n);
+    const dv3 dt2 = dt1 - q * n;
+    const double tau2 = in.tau + in.h;
+    const double s = sqrt(in.delta * in.Rs);
+    const double Sn = 2.0 * in.Es * s;
+    const double kn = (2.0 / 3.0) * Sn;
+    const double ssm = sqrt(Sn * in.meff);
+    const double gn = kC5 * in.be * ssm;
+    const double fnm = kn * in.delta + gn * p;
+    const dv3 fn = fnm * n;
+    const double A = fabs(fnm);
+    // rolling resistance once the contact is older than the collision time
+    const double Reff = sqrt(in.Rs);
+    const double kns = (4.0 / 3.0) * in.Es * sqrt(Reff);
+    const double gns = -2.0 * sqrt((5.0 / 3.0) * in.meff * in.Es) * in.be * pow(Reff, 0.25);
+    const double dc = gns / (2.0 * sqrt(kns * in.meff));
+    bool roll = in.crr > 0.0;
+    if (roll && dc < 1.0) {
+        const double tcoll = 3.1415926535897932385 * sqrt(in.meff / (kns * (1.0 - dc * dc)));
+        if (tau2 <= tcoll) roll = false;
+    }
+    const dv3 vroll = WB - WA;
+    const double L = norm(vroll);
+    roll = roll && L > kTiny;
+    const dv3 e = roll ? (1.0 / L) * vroll : mk(0, 0, 0);
+    t_out = roll ? (in.crr * A) * e : mk(0, 0, 0);
+    // tangential with Coulomb cap
+    const double kt = 8.0 * in.Gs * s;
+    const double smk = sqrt(in.meff * kt);
+    const double gt = -kC5 * in.be * smk;
+    const dv3 Ft = (-kt) * dt2 - gt * vt;
+    const double ft = norm(Ft);
+    const bool big = in.mu > 0.0 && ft > kTiny;
+    const bool cap = big && ft > A * in.mu;
+    const double rr = cap ? A * in.mu / ft : 1.0;
+    const dv3 Ftp = big ? rr * Ft : mk(0, 0, 0);
+    f_out = fn + Ftp;
+
+    // ---- reverse ----
+    dv3 g_fn = g_f, g_Ftp = g_f;
+    dv3 g_dt2 = mk(0, 0, 0), g_vt = mk(0, 0, 0), g_n = mk(0, 0, 0), g_WA = mk(0, 0, 0), g_WB = mk(0, 0, 0);
+    double g_kt = 0.0, g_gt = 0.0, g_A = 0.0;
+    G.mu = 0.0;
+    if (cap) {  // dt3 = (Ftp + gt vt) / (-kt)
+        const dv3 X = Ftp + gt * vt;
+        g_Ftp -= (1.0 / kt) * g_dt3;
+        g_gt += -dot(g_dt3, vt) / kt;
+        g_vt += (-gt / kt) * g_dt3;
+        g_kt += dot(g_dt3, X) / (kt * kt);
+    } else {
+        g_dt2 += g_dt3;
+    }
+    dv3 g_Ft = big ? rr * g_Ftp : mk(0, 0, 0);
+    if (cap) {
+        const double g_rr = dot(g_Ftp, Ft);
+        g_A += g_rr * in.mu / ft;
+        G.mu += g_rr * A / ft;
+        const double g_ft = -g_rr * A * in.mu / (ft * ft);
+        g_Ft += (g_ft / ft) * Ft;
+    }
+    g_kt += -dot(g_Ft, dt2);
+    g_dt2 += (-kt) * g_Ft;
+    g_gt += -dot(g_Ft, vt);
+    g_vt += (-gt) * g_Ft;
+    G.be = g_gt * (-kC5 * smk);
+    g_kt += g_gt * (-kC5 * in.be * in.meff / (2.0 * (smk > 0.0 ? smk : 1.0)));
+    G.Gs = 8.0 * s * g_kt;
+    double g_s = 8.0 * in.Gs * g_kt;
+    G.crr = 0.0;
+    if (roll) {  // t = crr A e, e = vroll / |vroll|
+        const double ge = dot(g_t, e);
+        G.crr = A * ge;
+        g_A += in.crr * ge;
+        const dv3 g_e = (in.crr * A) * g_t;
+        const dv3 g_vroll = (1.0 / L) * (g_e - dot(g_e, e) * e);
+        g_WB += g_vroll;
+        g_WA -= g_vroll;
+    }
+    const double g_fnm = g_A * (fnm > 0.0 ? 1.0 : (fnm < 0.0 ? -1.0 : 0.0)) + dot(g_fn, n);
+    g_n += fnm * g_fn;
+    const double g_kn = g_fnm * in.delta;
+    double g_delta = g_fnm * kn;
+    const double g_gn = g_fnm * p;
+    double g_p = g_fnm * gn;
+    G.be += g_gn * kC5 * ssm;
+    const double g_Sn = g_gn * kC5 * in.be * in.meff / (2.0 * (ssm > 0.0 ? ssm : 1.0)) + (2.0 / 3.0) * g_kn;
+    G.Es = 2.0 * s * g_Sn;
+    g_s += 2.0 * in.Es * g_Sn;
+    g_delta += g_s * in.Rs / (2.0 * (s > 0.0 ? s : 1.0));
+    G.tau = g_tau2;
+    dv3 g_dt1 = g_dt2;
+    const double g_q = -dot(g_dt2, n);
+    g_n += (-q) * g_dt2;
+    g_dt1 += g_q * n;
+    g_n += g_q * dt1;
+    G.dtan = g_dt1;
+    g_vt += in.h * g_dt1;
+    dv3 g_vr = g_vt;
+    g_p += -dot(g_vt, n);
+    g_n += (-p) * g_vt;
+    g_vr += g_p * n;
+    g_n += g_p * vr;
+    g_WA += g_vr;
+    g_WB -= g_vr;
+    G.vA = g_vr;
+    G.vB = -g_vr;
+    G.wA = cross(in.rAv, g_WA);
+    G.rAv = cross(g_WA, in.wA);
+    G.wB = cross(in.rBv, g_WB);
+    G.rBv = cross(g_WB, in.wB);
+    G.n = g_n;
+    G.delta = g_delta;
+}
+
+}  // namespace deme_b200

@@ -16,115 +16,11 @@
 
 #include "../../include/deme_b200.h"
 #include "force_jit.cuh"
+#include "handle.cuh"
 #include "kernels.cuh"
 #include "primitives.cuh"
 
-using namespace deme_b200;
-
-namespace {
-
-struct ContactBuf {
-    uint32_t cap = 0;
-    uint32_t* idA = nullptr;
-    uint32_t* idB = nullptr;
-    uint8_t* type = nullptr;
-    float4* hist = nullptr;
-    uint32_t* mapping = nullptr;
-    uint32_t* off = nullptr;  // nS + 1, allocated once
-    ContactView view() const { return ContactView{idA, idB, type, hist, mapping, off}; }
-};
-
-}  // namespace
-
-struct deme_handle {
-    std::string err;
-    int device = 0;
-    cudaStream_t st_dt = nullptr, st_kt = nullptr;
-    cudaStream_t own_dt = nullptr, own_kt = nullptr;
-    deme_sim_params params{};
-    SimConsts k{};
-    uint32_t nO = 0, nS = 0, nA = 0, nM = 0, nClumps = 0;
-    int nW = 0;
-    // scene and state
-    uint64_t* voxel = nullptr;
-    ushort4* loc = nullptr;
-    float4* quat = nullptr;
-    float4* vel = nullptr;
-    float4* omg = nullptr;
-    float4* moi = nullptr;
-    float4* acc = nullptr;
-    float4* alpha = nullptr;
-    float4* sph = nullptr;
-    uint32_t* sOwner = nullptr;
-    uint8_t* sMat = nullptr;
-    uint8_t* masks = nullptr;
-    float* mat = nullptr;  // 5 x nM
-    AnalRaw* analRaw = nullptr;
-    AnalPlaced* analPlaced = nullptr;
-    Prescription* presc = nullptr;
-    // contact detection
-    CDView cd{};
-    uint32_t nCells = 0;
-    int cellBits = 0;
-    uint32_t candCap = 0;
-    ContactBuf lists[2];
-    int cur = 0;
-    uint32_t nContacts = 0;
-    // per-contact outputs
-    bool keepOutputs = false;
-    bool useOnesweep = false;  // sort spheres by cell with the multi-pass onesweep instead of the counting sort
-    uint32_t outCap = 0;
-    ContactOutputs outs{nullptr, nullptr, nullptr, nullptr};
-    bool outsValid = false;
-    // scratch
-    void* scratch = nullptr;
-    size_t scratchBytes = 0;
-    uint32_t* dTotal = nullptr;
-    uint32_t* hTotal = nullptr;
-    uint32_t* dErr = nullptr;
-    uint32_t* hErr = nullptr;
-    double* dKE = nullptr;
-    double* hKE = nullptr;
-    Prescription* hPresc = nullptr;
-    float* analPartial = nullptr;
-    size_t analPartialCap = 0;
-    double t = 0.0;
-    int64_t steps = 0;
-    std::vector<void*> allocs;
-    UserForceKernel userForce;  // a compiled force-model string, when one is set
-
-    StateView state_view() const {
-        StateView s;
-        s.voxel = voxel;
-        s.loc = loc;
-        s.quat = quat;
-        s.vel = vel;
-        s.omg = omg;
-        s.moi = moi;
-        s.acc = acc;
-        s.alpha = alpha;
-        s.sph = sph;
-        s.sOwner = sOwner;
-        s.sMat = sMat;
-        s.masks = masks;
-        s.mat = MaterialTable{mat, mat + nM, mat + 2 * nM, mat + 3 * nM, mat + 4 * nM};
-        s.anal = analPlaced;
-        s.nA = nA;
-        s.presc = presc;
-        return s;
-    }
-};
-
-#define CUDA_TRY(h, expr)                                                                        \
-    do {                                                                                         \
-        cudaError_t e_ = (expr);                                                                 \
-        if (e_ != cudaSuccess) {                                                                 \
-            (h)->err = std::string(#expr) + ": " + cudaGetErrorString(e_);                       \
-            return e_ == cudaErrorMemoryAllocation ? DEME_ERR_OOM : DEME_ERR_CUDA;               \
-        }                                                                                        \
-    } while (0)
-
-static int32_t dalloc(deme_handle* h, void** p, size_t bytes) {
+int32_t dalloc(deme_handle* h, void** p, size_t bytes) {
     if (bytes == 0) bytes = 16;
     cudaError_t e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) {
@@ -134,24 +30,14 @@ static int32_t dalloc(deme_handle* h, void** p, size_t bytes) {
     h->allocs.push_back(*p);
     return DEME_OK;
 }
-template <typename T>
-static int32_t dalloc_n(deme_handle* h, T** p, size_t n) {
-    return dalloc(h, reinterpret_cast<void**>(p), n * sizeof(T));
-}
-static void dfree(deme_handle* h, void* p) {
+void dfree(deme_handle* h, void* p) {
     if (!p) return;
     auto it = std::find(h->allocs.begin(), h->allocs.end(), p);
     if (it != h->allocs.end()) h->allocs.erase(it);
     cudaFree(p);
 }
 
-#define TRY(expr)                      \
-    do {                               \
-        int32_t s_ = (expr);           \
-        if (s_ != DEME_OK) return s_;  \
-    } while (0)
-
-static int32_t check_launch(deme_handle* h, const char* what) {
+int32_t check_launch(deme_handle* h, const char* what) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         h->err = std::string(what) + ": " + cudaGetErrorString(e);
@@ -160,7 +46,7 @@ static int32_t check_launch(deme_handle* h, const char* what) {
     return DEME_OK;
 }
 
-static int32_t read_device_errors(deme_handle* h) {
+int32_t read_device_errors(deme_handle* h) {
     CUDA_TRY(h, cudaMemcpyAsync(h->hErr, h->dErr, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->st_dt));
     CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
     if (*h->hErr) {
@@ -191,7 +77,7 @@ static int32_t ensure_scratch(deme_handle* h, size_t bytes) {
     return DEME_OK;
 }
 
-static int32_t ensure_list(deme_handle* h, ContactBuf& b, uint32_t n) {
+int32_t ensure_list(deme_handle* h, ContactBuf& b, uint32_t n) {
     if (n <= b.cap) return DEME_OK;
     uint32_t cap = std::max<uint32_t>(1024u, (uint32_t)std::min<uint64_t>(0xFFFFFFF0ull, (uint64_t)n * 5 / 4 + 64));
     dfree(h, b.idA);
@@ -536,6 +422,7 @@ void deme_destroy(deme_handle* h) {
     if (!h) return;
     if (h->own_dt) cudaStreamSynchronize(h->own_dt);
     if (h->own_kt) cudaStreamSynchronize(h->own_kt);
+    adjoint_release(h);  // frees its arrays through dfree, so before the bulk free below
     for (void* p : h->allocs) cudaFree(p);
     h->allocs.clear();
     if (h->hTotal) cudaFreeHost(h->hTotal);

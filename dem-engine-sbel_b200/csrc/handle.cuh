@@ -1,0 +1,132 @@
+// handle.cuh -- the solver handle behind the C ABI and the host helpers shared by capi.cu and adjoint.cu.
+#pragma once
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/deme_b200.h"
+#include "force_jit.cuh"
+#include "kernels.cuh"
+
+using namespace deme_b200;
+
+struct AdjointTape;  // adjoint.cu
+
+struct ContactBuf {
+    uint32_t cap = 0;
+    uint32_t* idA = nullptr;
+    uint32_t* idB = nullptr;
+    uint8_t* type = nullptr;
+    float4* hist = nullptr;
+    uint32_t* mapping = nullptr;
+    uint32_t* off = nullptr;  // nS + 1, allocated once
+    ContactView view() const { return ContactView{idA, idB, type, hist, mapping, off}; }
+};
+
+struct deme_handle {
+    std::string err;
+    int device = 0;
+    cudaStream_t st_dt = nullptr, st_kt = nullptr;
+    cudaStream_t own_dt = nullptr, own_kt = nullptr;
+    deme_sim_params params{};
+    SimConsts k{};
+    uint32_t nO = 0, nS = 0, nA = 0, nM = 0, nClumps = 0;
+    int nW = 0;
+    // scene and state
+    uint64_t* voxel = nullptr;
+    ushort4* loc = nullptr;
+    float4* quat = nullptr;
+    float4* vel = nullptr;
+    float4* omg = nullptr;
+    float4* moi = nullptr;
+    float4* acc = nullptr;
+    float4* alpha = nullptr;
+    float4* sph = nullptr;
+    uint32_t* sOwner = nullptr;
+    uint8_t* sMat = nullptr;
+    uint8_t* masks = nullptr;
+    float* mat = nullptr;  // 5 x nM
+    AnalRaw* analRaw = nullptr;
+    AnalPlaced* analPlaced = nullptr;
+    Prescription* presc = nullptr;
+    // contact detection
+    CDView cd{};
+    uint32_t nCells = 0;
+    int cellBits = 0;
+    uint32_t candCap = 0;
+    ContactBuf lists[2];
+    int cur = 0;
+    uint32_t nContacts = 0;
+    // per-contact outputs
+    bool keepOutputs = false;
+    bool useOnesweep = false;  // sort spheres by cell with the multi-pass onesweep instead of the counting sort
+    uint32_t outCap = 0;
+    ContactOutputs outs{nullptr, nullptr, nullptr, nullptr};
+    bool outsValid = false;
+    // scratch
+    void* scratch = nullptr;
+    size_t scratchBytes = 0;
+    uint32_t* dTotal = nullptr;
+    uint32_t* hTotal = nullptr;
+    uint32_t* dErr = nullptr;
+    uint32_t* hErr = nullptr;
+    double* dKE = nullptr;
+    double* hKE = nullptr;
+    Prescription* hPresc = nullptr;
+    float* analPartial = nullptr;
+    size_t analPartialCap = 0;
+    double t = 0.0;
+    int64_t steps = 0;
+    std::vector<void*> allocs;
+    UserForceKernel userForce;  // a compiled force-model string, when one is set
+    AdjointTape* adj = nullptr;  // checkpoints of deme_adjoint_record
+
+    StateView state_view() const {
+        StateView s;
+        s.voxel = voxel;
+        s.loc = loc;
+        s.quat = quat;
+        s.vel = vel;
+        s.omg = omg;
+        s.moi = moi;
+        s.acc = acc;
+        s.alpha = alpha;
+        s.sph = sph;
+        s.sOwner = sOwner;
+        s.sMat = sMat;
+        s.masks = masks;
+        s.mat = MaterialTable{mat, mat + nM, mat + 2 * nM, mat + 3 * nM, mat + 4 * nM};
+        s.anal = analPlaced;
+        s.nA = nA;
+        s.presc = presc;
+        return s;
+    }
+};
+
+#define CUDA_TRY(h, expr)                                                                        \
+    do {                                                                                         \
+        cudaError_t e_ = (expr);                                                                 \
+        if (e_ != cudaSuccess) {                                                                 \
+            (h)->err = std::string(#expr) + ": " + cudaGetErrorString(e_);                       \
+            return e_ == cudaErrorMemoryAllocation ? DEME_ERR_OOM : DEME_ERR_CUDA;               \
+        }                                                                                        \
+    } while (0)
+
+#define TRY(expr)                      \
+    do {                               \
+        int32_t s_ = (expr);           \
+        if (s_ != DEME_OK) return s_;  \
+    } while (0)
+
+int32_t dalloc(deme_handle* h, void** p, size_t bytes);
+void dfree(deme_handle* h, void* p);
+int32_t check_launch(deme_handle* h, const char* what);
+int32_t read_device_errors(deme_handle* h);
+int32_t ensure_list(deme_handle* h, ContactBuf& b, uint32_t n);
+void adjoint_release(deme_handle* h);  // adjoint.cu
+
+template <typename T>
+inline int32_t dalloc_n(deme_handle* h, T** p, size_t n) {
+    return dalloc(h, reinterpret_cast<void**>(p), n * sizeof(T));
+}

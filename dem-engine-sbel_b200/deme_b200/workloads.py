@@ -294,3 +294,37 @@ def hopper(n: int = 4_000_000, r_median: float = 1.5e-3, sigma: float = 0.25, r_
     built.info.update(workload="hopper", n=n, u_out=u_out, u_top=u_top, R_top=u_top * tan_t, r_max=r_max,
                       lattice_spacing=a, seed=seed, n_classes=n_classes, apex_z=shift)
     return built
+
+
+def sphere_pile(n: int = 60, seed: int = 3, h: float = 2e-5, spread: float = 5.2e-3, noise: float = 4e-4,
+                vel_scale: float = 0.05, spin_scale: float = 20.0, lift: float = 2.2e-3):
+    """Loose pile of single spheres (radii U[2, 3] mm, two materials) pressed onto a floor plane with random
+    velocities and spins: every contact branch of the Hertz-Mindlin model is active within a few dozen steps.
+    Used by the adjoint tests."""
+    rng = np.random.default_rng(seed)
+    r = rng.uniform(2e-3, 3e-3, n).astype(f32)
+    rho = 2500.0
+    s = SceneBuilder()
+    s.InstructBoxDomainDimension(0.2, 0.2, 0.2)
+    s.SetCoordSysOrigin("center")
+    m0 = s.LoadMaterial({"E": 1e7, "nu": 0.3, "CoR": 0.5, "mu": 0.3, "Crr": 0.01})
+    m1 = s.LoadMaterial({"E": 5e7, "nu": 0.25, "CoR": 0.4, "mu": 0.5, "Crr": 0.03})
+    side = int(np.ceil(n ** (1 / 3)))
+    idx = np.arange(n)
+    z0 = -0.05
+    x = np.stack([(idx % side) * spread, ((idx // side) % side) * spread, z0 + (idx // side // side) * spread + lift],
+                 1)
+    x += rng.normal(0, noise, x.shape)
+    types = [s.LoadSphereType(float(f32(sphere_mass(float(ri), rho))), float(ri), m0 if i % 2 == 0 else m1)
+             for i, ri in enumerate(r)]
+    b = s.AddClumps(types, x.astype(f32))
+    b.SetVel(rng.normal(0, vel_scale, (n, 3)).astype(f32))
+    b.SetAngVel(rng.normal(0, spin_scale, (n, 3)).astype(f32))
+    s.AddBCPlane((0, 0, z0), (0, 0, 1), m1)
+    s.SetInitTimeStep(h)
+    s.SetGravitationalAcceleration((0, 0, -9.81))
+    s.SetCDUpdateFreq(1)
+    s.SetExpandFactor(0.0)  # contacts are exactly the overlapping pairs (the unset default would shrink them)
+    built = s.Initialize()
+    built.info.update(workload="sphere_pile", n=n, seed=seed)
+    return built

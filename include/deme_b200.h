@@ -318,6 +318,32 @@ int32_t deme_radix_sort_pairs_device(const uint32_t* keys_in, const uint32_t* va
                                      size_t scratch_bytes, void* stream);
 size_t deme_radix_sort_scratch_bytes(uint32_t n);
 
+/* ---- Adjoint of the step (no reference counterpart) ----------------------------------------------------------
+ * For scenes of single spheres (centred, isotropic inertia) with plane walls, the built-in Hertz-Mindlin model,
+ * Extended Taylor integration and contact detection every step.  deme_adjoint_record runs n_steps forward from the
+ * current state, keeping a checkpoint every `checkpoint_every` steps; deme_adjoint_backward takes the gradient of
+ * a loss with respect to the final state and returns it with respect to the state before the window and to the
+ * material parameters, recomputing each window segment from its checkpoint.  The contact set of each step is the
+ * one the forward pass found.  Angular velocities are in the world frame.  The model runs on the recorded FP32
+ * state; gradients are accumulated in FP64.  The handle ends at the recorded final state. */
+typedef struct {
+    const double* d_pos;     /* n_owners x 3, dL/d(final position); NULL = 0 */
+    const double* d_vel;     /* n_owners x 3, dL/d(final velocity); NULL = 0 */
+    const double* d_angvel;  /* n_owners x 3, dL/d(final angular velocity, world frame); NULL = 0 */
+} deme_adjoint_seed;
+
+typedef struct {
+    double* d_pos0;      /* n_owners x 3 (may be NULL) */
+    double* d_vel0;      /* n_owners x 3 (may be NULL) */
+    double* d_angvel0;   /* n_owners x 3 (may be NULL) */
+    double* d_material;  /* n_materials x 4: dL/dE, dL/dCoR, dL/dmu, dL/dCrr (may be NULL) */
+} deme_adjoint_grads;
+
+int32_t deme_adjoint_record(deme_handle* h, int32_t n_steps, int32_t checkpoint_every);
+int32_t deme_adjoint_backward(deme_handle* h, const deme_adjoint_seed* seed, deme_adjoint_grads* out);
+/* Replaces material m's properties (LoadMaterial keys E, nu, CoR, mu, Crr) for the following steps. */
+int32_t deme_set_material(deme_handle* h, uint32_t m, float E, float nu, float CoR, float mu, float Crr);
+
 /* Largest n deme_radix_sort_pairs_static accepts. */
 #define DEME_SORT_STATIC_MAX_N 1048576u
 
