@@ -199,6 +199,9 @@ def main():
     ap.add_argument("--ref-clumps", type=int, default=200_000)
     ap.add_argument("--ref-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint timing on the column collapse")
+    ap.add_argument("--adjoint-steps", type=int, default=2000)
+    ap.add_argument("--adjoint-checkpoint", type=int, default=100)
     ap.add_argument("--settle-steps", type=int, default=15000,
                     help="untimed preparation: steps at --settle-dt that let the loose lattice fall into a bed")
     ap.add_argument("--settle-dt", type=float, default=2e-5)
@@ -352,6 +355,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(args)
+    adj = None if args.no_adjoint else adjoint_measure(args, stream)
 
     if rank == 0:
         line = {
@@ -371,13 +375,61 @@ def main():
             "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": C.sizeof(capi.FamilyPrescription),
                     "d2h_bytes_per_step": 8},
-            "gpu_launches": int(launches), "clocks": clocks,
+            "gpu_launches": int(launches), "clocks": clocks, "adjoint": adj,
         }
         print(json.dumps(line), flush=True)
     s.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def adjoint_measure(args, stream):
+    """Adjoint timing on the column collapse: plain forward steps, the checkpointed forward (record) and the
+    backward pass (segment recomputation + reverse), each timed with CUDA events on the solver's stream."""
+    import numpy as np
+    import torch
+    from deme_b200 import Solver, adjoint, workloads
+    built = workloads.column_collapse()
+    T, K = args.adjoint_steps, args.adjoint_checkpoint
+    n = built.counts["s"]
+
+    def solver():
+        s = Solver(built)
+        s.lib.deme_set_streams(s.h, C.c_void_p(stream.cuda_stream), C.c_void_p(stream.cuda_stream))
+        return s
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), r
+
+    w = solver()  # warm-up: allocations and first launches of every kernel involved
+    adjoint.record(w, min(T, 2 * K), K)
+    adjoint.backward(w, d_pos=np.zeros((built.counts["o"], 3)))
+    w.close()
+    sf = solver()
+    t_fwd, _ = timed(lambda: sf.step(T))
+    sf.close()
+    sa = solver()
+    t_rec, _ = timed(lambda: adjoint.record(sa, T, K))
+    pos, _, _ = adjoint.final_state(sa)
+    init = built.decode_positions(built.initial_state(), kernel_literals=False)[:n]
+    loss, g = workloads.collapse_loss(pos[:n], init[:, :2].mean(0), float(init[:, 2].min()))
+    seed = np.zeros((built.counts["o"], 3))
+    seed[:n] = g
+    t_bwd, out = timed(lambda: adjoint.backward(sa, d_pos=seed))
+    nC = sa.num_contacts()
+    sa.close()
+    return {"workload": "column collapse: 20,000 spheres r U[2,3] mm released over a floor plane, dt 1e-5, CD every "
+                        "step, contact margin 0", "steps": T, "checkpoint_every": K, "fwd_ms_per_step": t_fwd / T,
+            "record_ms_per_step": t_rec / T, "adjoint_ms_per_step": t_bwd / T, "adjoint_over_forward": t_bwd / t_fwd,
+            "loss": loss, "dL_dE_CoR_mu_Crr": [float(v) for v in out["d_material"][0]], "n_contacts_final": nC,
+            "gradient_precision": "FP64 accumulators, FP32 state"}
 
 
 def s_grid_cells(built):

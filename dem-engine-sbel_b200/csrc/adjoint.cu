@@ -65,6 +65,7 @@ struct AdjointTape {
     uint32_t gCap = 0;
     float4 *gA = nullptr, *gB = nullptr, *gC = nullptr;  // history gradients (current, previous, carried)
     double* gmat = nullptr;                             // nM x 4
+    double floors[3] = {1e-4, 1e-4, 1e-6};              // see deme_adjoint_set_floors
 };
 
 namespace {
@@ -135,7 +136,8 @@ __global__ void __launch_bounds__(256) k_adj_contact(SimConsts k, StateView s, u
                                                      const uint8_t* cT, const float4* cH, const double* X,
                                                      const float4* V, const float4* W, const double* lF,
                                                      const double* lT, const float4* gHout, float4* gHin,
-                                                     double* nlx, double* nlv, double* nlw, double* gmat) {
+                                                     double* nlx, double* nlv, double* nlw, double* gmat,
+                                                     double3 floors) {
     extern __shared__ double s_g[];  // nM x (E, CoR, mu, Crr)
     for (uint32_t t = threadIdx.x; t < 4u * nM; t += blockDim.x) s_g[t] = 0.0;
     __syncthreads();
@@ -199,6 +201,9 @@ __global__ void __launch_bounds__(256) k_adj_contact(SimConsts k, StateView s, u
                 in.meff = mA * mB / (mA + mB);
                 in.Rs = rA * rB / (rA + rB);
                 in.h = (double)k.h;
+                in.floor_delta_rel = floors.x;
+                in.floor_roll_speed = floors.y;
+                in.floor_ft = floors.z;
                 const double EA = s.mat.E[matA], EB = s.mat.E[matB], nuA = s.mat.nu[matA], nuB = s.mat.nu[matB];
                 const double invE = (1.0 - nuA * nuA) / EA + (1.0 - nuB * nuB) / EB;
                 in.Es = 1.0 / invE;
@@ -450,12 +455,24 @@ int32_t deme_set_material(deme_handle* h, uint32_t m, float E, float nu, float C
     return DEME_OK;
 }
 
+int32_t deme_adjoint_set_floors(deme_handle* h, double overlap_rel, double roll_speed, double tangential_force) {
+    if (!h || !(overlap_rel >= 0.0) || !(roll_speed >= 0.0) || !(tangential_force >= 0.0)) return DEME_ERR_INVALID;
+    if (!h->adj) h->adj = new AdjointTape();
+    h->adj->floors[0] = overlap_rel;
+    h->adj->floors[1] = roll_speed;
+    h->adj->floors[2] = tangential_force;
+    return DEME_OK;
+}
+
 int32_t deme_adjoint_record(deme_handle* h, int32_t n_steps, int32_t checkpoint_every) {
     if (!h || n_steps <= 0 || checkpoint_every <= 0) return DEME_ERR_INVALID;
     TRY(check_adjoint_scene(h));
+    double floors[3] = {1e-4, 1e-4, 1e-6};
+    if (h->adj) std::copy(h->adj->floors, h->adj->floors + 3, floors);
     adjoint_release(h);
     h->adj = new AdjointTape();
     AdjointTape* t = h->adj;
+    std::copy(floors, floors + 3, t->floors);
     t->K = checkpoint_every;
     t->nSteps = n_steps;
     t->cps.resize((size_t)((n_steps + checkpoint_every - 1) / checkpoint_every));
@@ -471,7 +488,7 @@ int32_t deme_adjoint_record(deme_handle* h, int32_t n_steps, int32_t checkpoint_
 int32_t deme_adjoint_backward(deme_handle* h, const deme_adjoint_seed* seed, deme_adjoint_grads* out) {
     if (!h || !out) return DEME_ERR_INVALID;
     AdjointTape* t = h->adj;
-    if (!t) {
+    if (!t || t->cps.empty()) {
         h->err = "deme_adjoint_backward: no recorded window (call deme_adjoint_record first)";
         return DEME_ERR_STATE;
     }
@@ -604,7 +621,7 @@ int32_t deme_adjoint_backward(deme_handle* h, const deme_adjoint_seed* seed, dem
                 k_adj_contact<<<nblk(n, 256), 256, 4 * nM * sizeof(double), st>>>(
                     k, sv, n, h->nClumps, nM, t->cA + b, t->cB + b, t->cT + b, t->cH + b, t->X + (size_t)s * nO * 3,
                     t->V + (size_t)s * nO, t->W + (size_t)s * nO, t->lF, t->lT, gOut, t->gB, t->nlx, t->nlv, t->nlw,
-                    t->gmat);
+                    t->gmat, make_double3(t->floors[0], t->floors[1], t->floors[2]));
             std::swap(t->lx, t->nlx);
             std::swap(t->lv, t->nlv);
             std::swap(t->lw, t->nlw);

@@ -37,6 +37,9 @@ struct LawIn {
     dv3 dtan;         // incoming tangential displacement history
     double tau;       // incoming contact duration
     double Es, Gs, be, mu, crr, meff, Rs, h;
+    // floors in the derivatives at the law's non-smooth points (0 = exact): overlap relative to R* (the damping's
+    // overlap^(1/4)), relative rolling speed (the rolling torque's direction), tangential force (the Coulomb cap)
+    double floor_delta_rel, floor_roll_speed, floor_ft;
 };
 
 struct LawGrad {
@@ -111,18 +114,21 @@ __device__ __forceinline__ void law_vjp(const LawIn& in, dv3 g_f, dv3 g_t, dv3 g
     }
     dv3 g_Ft = big ? rr * g_Ftp : mk(0, 0, 0);
     if (cap) {
+        const double ftd = fmax(ft, in.floor_ft);
         const double g_rr = dot(g_Ftp, Ft);
-        g_A += g_rr * in.mu / ft;
-        G.mu += g_rr * A / ft;
-        const double g_ft = -g_rr * A * in.mu / (ft * ft);
-        g_Ft += (g_ft / ft) * Ft;
+        g_A += g_rr * in.mu / ftd;
+        G.mu += g_rr * A / ftd;
+        const double g_ft = -g_rr * A * in.mu / (ftd * ftd);
+        g_Ft += (g_ft / ftd) * Ft;
     }
     g_kt += -dot(g_Ft, dt2);
     g_dt2 += (-kt) * g_Ft;
     g_gt += -dot(g_Ft, vt);
     g_vt += (-gt) * g_Ft;
+    const double s_d = fmax(s, in.Rs * sqrt(in.floor_delta_rel));  // s = sqrt(delta R*), floored in derivatives
+    const double smk_d = sqrt(in.meff * 8.0 * in.Gs * s_d);
     G.be = g_gt * (-kC5 * smk);
-    g_kt += g_gt * (-kC5 * in.be * in.meff / (2.0 * (smk > 0.0 ? smk : 1.0)));
+    g_kt += g_gt * (-kC5 * in.be * in.meff / (2.0 * (smk_d > 0.0 ? smk_d : 1.0)));
     G.Gs = 8.0 * s * g_kt;
     double g_s = 8.0 * in.Gs * g_kt;
     G.crr = 0.0;
@@ -131,7 +137,7 @@ __device__ __forceinline__ void law_vjp(const LawIn& in, dv3 g_f, dv3 g_t, dv3 g
         G.crr = A * ge;
         g_A += in.crr * ge;
         const dv3 g_e = (in.crr * A) * g_t;
-        const dv3 g_vroll = (1.0 / L) * (g_e - dot(g_e, e) * e);
+        const dv3 g_vroll = (1.0 / fmax(L, in.floor_roll_speed)) * (g_e - dot(g_e, e) * e);
         g_WB += g_vroll;
         g_WA -= g_vroll;
     }
@@ -141,11 +147,12 @@ __device__ __forceinline__ void law_vjp(const LawIn& in, dv3 g_f, dv3 g_t, dv3 g
     double g_delta = g_fnm * kn;
     const double g_gn = g_fnm * p;
     double g_p = g_fnm * gn;
+    const double ssm_d = sqrt(2.0 * in.Es * s_d * in.meff);
     G.be += g_gn * kC5 * ssm;
-    const double g_Sn = g_gn * kC5 * in.be * in.meff / (2.0 * (ssm > 0.0 ? ssm : 1.0)) + (2.0 / 3.0) * g_kn;
+    const double g_Sn = g_gn * kC5 * in.be * in.meff / (2.0 * (ssm_d > 0.0 ? ssm_d : 1.0)) + (2.0 / 3.0) * g_kn;
     G.Es = 2.0 * s * g_Sn;
     g_s += 2.0 * in.Es * g_Sn;
-    g_delta += g_s * in.Rs / (2.0 * (s > 0.0 ? s : 1.0));
+    g_delta += g_s * in.Rs / (2.0 * (s_d > 0.0 ? s_d : 1.0));
     G.tau = g_tau2;
     dv3 g_dt1 = g_dt2;
     const double g_q = -dot(g_dt2, n);

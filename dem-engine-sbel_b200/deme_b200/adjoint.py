@@ -108,3 +108,11 @@ def make_rollout_function():
             return g, None, None, None, None, None
 
     return DEMRollout
+
+
+def set_floors(solver, overlap_rel: float, roll_speed: float, tangential_force: float):
+    """Floors in the derivatives at the contact law's non-smooth points (zeros: exact derivative)."""
+    solver.lib.deme_adjoint_set_floors.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
+    solver.lib.deme_adjoint_set_floors.restype = C.c_int32
+    solver._check(solver.lib.deme_adjoint_set_floors(solver.h, overlap_rel, roll_speed, tangential_force),
+                  "adjoint_set_floors")

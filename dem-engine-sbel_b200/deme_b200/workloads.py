@@ -328,3 +328,65 @@ def sphere_pile(n: int = 60, seed: int = 3, h: float = 2e-5, spread: float = 5.2
     built = s.Initialize()
     built.info.update(workload="sphere_pile", n=n, seed=seed)
     return built
+
+
+def column_collapse(n: int = 20000, r_range=(2e-3, 3e-3), rho: float = 2500.0, n_classes: int = 32, seed: int = 6,
+                    dt: float = 1e-5, aspect: float = 3.0):
+    """Column collapse for the adjoint: n single spheres (radii uniform in r_range, grouped into n_classes sphere
+    types) on a jittered square lattice of pitch 2 r_max (no overlaps) forming a column height:width = aspect over
+    a floor plane, released from rest.  20,000 spheres of 2-3 mm do not fit the stated 0.05 x 0.05 x 0.15 m column,
+    so the cross-section is widened (recorded in ``info``).  Contact margin 0, contact detection every step."""
+    rng = np.random.default_rng(seed)
+    r = rng.uniform(r_range[0], r_range[1], n)
+    edges = np.linspace(r_range[0], r_range[1], n_classes + 1)
+    cls = np.clip(np.searchsorted(edges, r, side="right") - 1, 0, n_classes - 1)
+    r_cls = 0.5 * (edges[:-1] + edges[1:])
+    r_max = float(r_cls.max())
+    a = 2.0 * r_max * 1.01
+    per_side = int(math.ceil((n / aspect) ** (1.0 / 3.0)))
+    layers = int(math.ceil(n / (per_side * per_side)))
+    idx = np.arange(n)
+    w = per_side * a
+    P = np.stack([(idx % per_side) * a - w / 2 + a / 2, ((idx // per_side) % per_side) * a - w / 2 + a / 2,
+                  (idx // (per_side * per_side)) * a + r_max * 1.01], 1)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    d *= (rng.random(n) * 0.9 * np.maximum(a / 2 - r_cls[cls], 0.0))[:, None]
+    P += d
+    height = layers * a
+    s = SceneBuilder()
+    box = max(4 * w, 1.3 * height) + 0.05
+    s.InstructBoxDomainDimension(box, box, box)
+    s.SetCoordSysOrigin("center")
+    z_floor = -box / 2 + 0.02
+    mat = s.LoadMaterial({"E": 1e7, "nu": 0.3, "CoR": 0.5, "mu": 0.5, "Crr": 0.02})
+    types = [s.LoadSphereType(float(f32(sphere_mass(float(rc), rho))), float(rc), mat) for rc in r_cls]
+    s.AddClumps([types[c] for c in cls], (P + np.array([0.0, 0.0, z_floor])).astype(f32))
+    s.AddBCPlane((0, 0, z_floor), (0, 0, 1), mat)
+    s.SetInitTimeStep(dt)
+    s.SetGravitationalAcceleration((0, 0, -9.81))
+    s.SetCDUpdateFreq(1)
+    s.SetExpandFactor(0.0)
+    built = s.Initialize()
+    built.info.update(workload="column_collapse", n=n, width=w, height=height, layers=layers, per_side=per_side,
+                      lattice_spacing=a, z_floor=z_floor, seed=seed)
+    return built
+
+
+def collapse_loss(pos: np.ndarray, axis_xy, z0: float):
+    """Column-collapse loss on final positions (n x 3): mean squared horizontal runout from the column axis
+    (axis_xy) plus a heap-angle proxy, the mean height above the floor z0 over the RMS runout.  Returns the loss and
+    its gradient with respect to pos."""
+    dx = pos[:, 0] - axis_xy[0]
+    dy = pos[:, 1] - axis_xy[1]
+    dz = pos[:, 2] - z0
+    n = len(pos)
+    R2 = np.mean(dx * dx + dy * dy)
+    Rrms = math.sqrt(R2)
+    H = np.mean(dz)
+    loss = R2 + H / Rrms
+    g = np.zeros_like(pos)
+    dR2 = np.stack([2 * dx / n, 2 * dy / n, np.zeros(n)], 1)
+    g += dR2 * (1.0 - 0.5 * H / (Rrms ** 3))
+    g[:, 2] += 1.0 / (n * Rrms)
+    return float(loss), g

@@ -341,6 +341,12 @@ typedef struct {
 
 int32_t deme_adjoint_record(deme_handle* h, int32_t n_steps, int32_t checkpoint_every);
 int32_t deme_adjoint_backward(deme_handle* h, const deme_adjoint_seed* seed, deme_adjoint_grads* out);
+/* Floors in the adjoint's derivatives at the contact law's non-smooth points: overlap relative to R* (the damping's
+ * overlap^(1/4) is unbounded in slope at contact onset), relative rolling speed in m/s (the rolling torque's
+ * direction flips through zero speed) and tangential force in N (the Coulomb cap's 1/|Ft|).  Where a floor binds,
+ * the gradient is that of the smoothed law; the exact derivative there only describes a neighbourhood far smaller
+ * than any useful parameter change.  Defaults 1e-4, 1e-4, 1e-6; zeros give the exact derivative. */
+int32_t deme_adjoint_set_floors(deme_handle* h, double overlap_rel, double roll_speed, double tangential_force);
 /* Replaces material m's properties (LoadMaterial keys E, nu, CoR, mu, Crr) for the following steps. */
 int32_t deme_set_material(deme_handle* h, uint32_t m, float E, float nu, float CoR, float mu, float Crr);
 

@@ -26,6 +26,12 @@ C5 = 1.825741858350554   # 2 sqrt(5/6), src/DEM/Defines.h
 PI2 = 9.869604401089358
 TINY = 1e-12
 HUGE_R = 1e15
+# Floors in the derivatives at the model's non-smooth points (the same values as the CUDA adjoint): the rolling
+# torque's direction (relative rolling speed, m/s), the damping's overlap^(1/4) (overlap relative to R*) and the
+# Coulomb cap's 1/|Ft| (N).  The forward model is unchanged; where a floor binds, the derivative is that of the
+# smoothed law, because the exact one (unbounded at zero rolling speed or zero overlap) measures sensitivity only
+# in a neighbourhood far smaller than any parameter change of interest.
+REG = {"delta_rel": 1e-4, "roll_speed": 1e-4, "ft": 1e-6}
 
 
 @dataclass
@@ -284,7 +290,7 @@ def contact_law_vjp(geo, I, vA, vB, wA, wB, hist, Es, Gs, be, mu, crr, meff, Rs,
     g_vt += np.where(cap[:, None], -gt[:, None] * g_dt3 / kt_safe[:, None], 0.0)
     g_kt += np.where(cap, _dot(g_dt3, X) / kt_safe ** 2, 0.0)
     g_dt2 += np.where(cap[:, None], 0.0, g_dt3)
-    ft_safe = np.where(ft > 0, ft, 1.0)
+    ft_safe = np.where(ft > 0, np.maximum(ft, REG["ft"]), 1.0)
     rr = I["rr"]
     g_Ft = np.where(big[:, None], rr[:, None] * g_Ftp_c, 0.0)
     g_rr = np.where(cap, _dot(g_Ftp_c, Ft), 0.0)
@@ -299,8 +305,10 @@ def contact_law_vjp(geo, I, vA, vB, wA, wB, hist, Es, Gs, be, mu, crr, meff, Rs,
     g_vt += -gt[:, None] * g_Ft
     # gt = -C5 be sqrt(meff kt); kt = 8 Gs s
     smk = np.sqrt(meff * kt)
+    s_d = np.maximum(I["s"], Rs * np.sqrt(REG["delta_rel"]))  # s = sqrt(delta Rs) floored in derivatives
+    smk_d = np.sqrt(meff * 8 * Gs * s_d)
     g_be = g_gt * (-C5 * smk)
-    g_kt += g_gt * (-C5 * be * meff / (2 * np.where(smk > 0, smk, 1.0)))
+    g_kt += g_gt * (-C5 * be * meff / (2 * np.where(smk_d > 0, smk_d, 1.0)))
     g_Gs = 8 * I["s"] * g_kt
     g_s = 8 * Gs * g_kt
     # rolling: t = crr A e
@@ -309,7 +317,7 @@ def contact_law_vjp(geo, I, vA, vB, wA, wB, hist, Es, Gs, be, mu, crr, meff, Rs,
     g_crr = np.where(roll, A * ge, 0.0)
     g_A += np.where(roll, crr * ge, 0.0)
     g_e = (crr * A)[:, None] * g_t
-    L_safe = np.where(L > 0, L, 1.0)
+    L_safe = np.where(L > 0, np.maximum(L, REG["roll_speed"]), 1.0)
     g_vroll = np.where(roll[:, None], (g_e - _dot(g_e, e)[:, None] * e) / L_safe[:, None], 0.0)
     g_WB += g_vroll
     g_WA -= g_vroll
@@ -325,12 +333,13 @@ def contact_law_vjp(geo, I, vA, vB, wA, wB, hist, Es, Gs, be, mu, crr, meff, Rs,
     g_p = g_fnm * gn
     Sn = I["Sn"]
     ssm = np.sqrt(Sn * meff)
+    ssm_d = np.sqrt(2 * Es * s_d * meff)
     g_be += g_gn * C5 * ssm
-    g_Sn = g_gn * C5 * be * meff / (2 * np.where(ssm > 0, ssm, 1.0)) + (2.0 / 3.0) * g_kn
+    g_Sn = g_gn * C5 * be * meff / (2 * np.where(ssm_d > 0, ssm_d, 1.0)) + (2.0 / 3.0) * g_kn
     g_Es = 2 * I["s"] * g_Sn
     g_s += 2 * Es * g_Sn
     s = I["s"]
-    g_delta += g_s * Rs / (2 * np.where(s > 0, s, 1.0))
+    g_delta += g_s * Rs / (2 * np.where(s_d > 0, s_d, 1.0))
     # history
     g_tau = g_tau2
     q, dt1 = I["q"], I["dt1"]

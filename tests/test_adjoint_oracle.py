@@ -1,11 +1,21 @@
 """The FP64 host adjoint (oracle/adjoint_fp64.py) against central finite differences of the FP64 forward model:
 gradients of a linear loss of the final state with respect to the material parameters (E, CoR, mu, Crr) and to
 initial positions, velocities and angular velocities, on a small pile of spheres on a floor plane (sphere-sphere
-and sphere-plane contacts, Coulomb cap and rolling resistance active).  Bar: 1e-5 relative."""
+and sphere-plane contacts, Coulomb cap and rolling resistance active).  Bar: 1e-5 relative.  The derivative floors
+are set to zero here (exact derivative of the discrete model)."""
 import numpy as np
 import pytest
 
 from oracle import adjoint_fp64 as A
+
+
+@pytest.fixture(autouse=True)
+def exact_derivatives():
+    """These tests check the exact derivative of the discrete model: no floors at the non-smooth points."""
+    saved = dict(A.REG)
+    A.REG.update(delta_rel=0.0, roll_speed=0.0, ft=0.0)
+    yield
+    A.REG.update(saved)
 
 
 def pile(seed=1, n=40):
