@@ -173,7 +173,14 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
         h->err = "voxel bits nvXp2 + nvYp2 + nvZp2 exceed 64: voxel ids would wrap";
         return DEME_ERR_INVALID;
     }
-    if (h->nA > 255) {
+    if (s->owner_anal_first && s->owner_anal_count) {
+        // packed scenes: each owner meets only its own range of components (at most 255 of them)
+        for (uint32_t o = 0; o < h->nO; o++)
+            if (s->owner_anal_count[o] > 255 || (uint64_t)s->owner_anal_first[o] + s->owner_anal_count[o] > h->nA) {
+                h->err = "owner analytical range out of bounds or wider than 255 components";
+                return DEME_ERR_INVALID;
+            }
+    } else if (h->nA > 255) {
         h->err = "at most 255 analytical components";
         return DEME_ERR_INVALID;
     }
@@ -187,7 +194,8 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
             return DEME_ERR_INVALID;
         }
     for (uint32_t i = 0; i < nS; i++)
-        if (s->sphere_owner[i] >= nO || s->sphere_material[i] >= std::max(nM, 1u)) {
+        if (s->sphere_owner[i] >= nO ||
+            (s->sphere_material_wide ? s->sphere_material_wide[i] : s->sphere_material[i]) >= std::max(nM, 1u)) {
             h->err = "sphere owner or material out of range";
             return DEME_ERR_INVALID;
         }
@@ -286,7 +294,18 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
         for (uint32_t i = 0; i < nS; i++) sph[i] = make_float4(s->relX[i], s->relY[i], s->relZ[i], s->radius[i]);
         CUDA_TRY(h, cudaMemcpy(h->sph, sph.data(), nS * sizeof(float4), cudaMemcpyHostToDevice));
         CUDA_TRY(h, cudaMemcpy(h->sOwner, s->sphere_owner, nS * sizeof(uint32_t), cudaMemcpyHostToDevice));
-        CUDA_TRY(h, cudaMemcpy(h->sMat, s->sphere_material, nS, cudaMemcpyHostToDevice));
+        {
+            std::vector<uint16_t> mat16(std::max(nS, 1u));
+            for (uint32_t i = 0; i < nS; i++)
+                mat16[i] = s->sphere_material_wide ? s->sphere_material_wide[i] : (uint16_t)s->sphere_material[i];
+            CUDA_TRY(h, cudaMemcpy(h->sMat, mat16.data(), nS * sizeof(uint16_t), cudaMemcpyHostToDevice));
+        }
+        if (s->owner_anal_first && s->owner_anal_count) {
+            std::vector<uint2> rg(nO);
+            for (uint32_t o = 0; o < nO; o++) rg[o] = make_uint2(s->owner_anal_first[o], s->owner_anal_count[o]);
+            TRY(dalloc_n(h, &h->ownerAnal, nO));
+            CUDA_TRY(h, cudaMemcpy(h->ownerAnal, rg.data(), nO * sizeof(uint2), cudaMemcpyHostToDevice));
+        }
         std::vector<uint8_t> masks(DEME_NUM_FAMILY_MASK, 0);
         if (s->family_masks) std::memcpy(masks.data(), s->family_masks, DEME_NUM_FAMILY_MASK);
         CUDA_TRY(h, cudaMemcpy(h->masks, masks.data(), DEME_NUM_FAMILY_MASK, cudaMemcpyHostToDevice));
@@ -315,7 +334,7 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
             r.owner = s->anal_owner[a];
             r.type = s->anal_type[a];
             r.normal = s->anal_normal[a];
-            r.material = s->anal_material[a];
+            r.material = s->anal_material_wide ? s->anal_material_wide[a] : (uint16_t)s->anal_material[a];
             // cone wall: sin and cos of the half angle, computed once on the host
             r.c1 = std::sin((double)r.size1);
             r.c2 = std::cos((double)r.size1);
@@ -540,8 +559,8 @@ int32_t deme_compute_forces(deme_handle* h) {
         TRY(ensure_outputs(h, h->nContacts));
         out = &h->outs;
     }
-    AnalAccum aa{nullptr, h->nClumps, h->nO - h->nClumps};
-    if (aa.nAO) {
+    AnalAccum aa{nullptr, h->nClumps, h->nO - h->nClumps, h->nO - h->nClumps > 64};
+    if (aa.nAO && !aa.direct) {
         const size_t need = (size_t)force_blocks(std::max(h->nContacts, 1u)) * 6u * aa.nAO;
         if (need > h->analPartialCap) {
             dfree(h, h->analPartial);

@@ -65,7 +65,8 @@ struct AnalPlaced {
     double x, y, z;        // component reference point (double)
     float dx, dy, dz;      // rotated direction (plane normal / axis)
     uint32_t owner;
-    uint8_t type, normal, material, pad;
+    uint8_t type, normal;
+    uint16_t material;
     float mass;
     double size1, c1, c2, umin, umax;  // cylinder radius / cone (sin, cos, axial range)
 };

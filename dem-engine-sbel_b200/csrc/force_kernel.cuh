@@ -23,8 +23,11 @@ __global__ void __launch_bounds__(kForceThreads, DEME_FORCE_MIN_BLOCKS) k_force(
                                                ContactOutputs out, AnalAccum aa) {
     // analytical owners (walls) collect their reactions block-locally, then one fixed-order reduction
     extern __shared__ float s_anal[];  // 6 floats per analytical owner
-    for (uint32_t t = threadIdx.x; t < 6u * aa.nAO; t += blockDim.x) s_anal[t] = 0.f;
-    if (aa.nAO) __syncthreads();
+    const bool partials = aa.nAO && !aa.direct;
+    if (partials) {
+        for (uint32_t t = threadIdx.x; t < 6u * aa.nAO; t += blockDim.x) s_anal[t] = 0.f;
+        __syncthreads();
+    }
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = i < n;
     uint32_t oA = 0xFFFFFFFFu, oB = 0xFFFFFFFFu;
@@ -226,7 +229,11 @@ __global__ void __launch_bounds__(kForceThreads, DEME_FORCE_MIN_BLOCKS) k_force(
         atomicAdd(&s.acc[oB], aB);
         atomicAdd(&s.alpha[oB], alB);
     }
-    if (aa.nAO) {
+    if (aa.nAO && aa.direct && active && !bSphere) {
+        atomicAdd(&s.acc[oB], aB);
+        atomicAdd(&s.alpha[oB], alB);
+    }
+    if (partials) {
         if (active && !bSphere && index_ok(k.err, 11, oB - aa.nClumps, aa.nAO)) {
             float* slot = s_anal + 6u * (oB - aa.nClumps);
             atomicAdd(slot + 0, aB.x);

@@ -44,12 +44,13 @@ struct deme_handle {
     float4* alpha = nullptr;
     float4* sph = nullptr;
     uint32_t* sOwner = nullptr;
-    uint8_t* sMat = nullptr;
+    uint16_t* sMat = nullptr;
     uint8_t* masks = nullptr;
     float* mat = nullptr;  // 5 x nM
     AnalRaw* analRaw = nullptr;
     AnalPlaced* analPlaced = nullptr;
     Prescription* presc = nullptr;
+    uint2* ownerAnal = nullptr;  // packed scenes: per owner (first, count) of its analytical components
     // contact detection
     CDView cd{};
     uint32_t nCells = 0;
@@ -100,6 +101,7 @@ struct deme_handle {
         s.anal = analPlaced;
         s.nA = nA;
         s.presc = presc;
+        s.ownerAnal = ownerAnal;
         return s;
     }
 };

@@ -32,6 +32,12 @@ namespace deme_b200 {
 
 static inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
 
+// The analytical components the spheres of `owner` may meet: all of them, or the owner's range when the scene
+// packs several independent scenes (their walls must not reach each other's spheres).
+__device__ __forceinline__ uint2 anal_range(const StateView& s, uint32_t owner) {
+    return s.ownerAnal ? s.ownerAnal[owner] : make_uint2(0u, s.nA);
+}
+
 // Sphere centre in double (owner position + rotated relative position), DEMBinSphereKernels.cu:39-51.
 __device__ __forceinline__ void sphere_center(const SimConsts& k, const StateView& s, uint32_t sid, uint32_t& owner,
                                               float4& sp, double& X, double& Y, double& Z) {
@@ -73,7 +79,6 @@ __global__ void k_place_anal(SimConsts k, StateView s, const AnalRaw* raw, AnalP
     a.type = r.type;
     a.normal = r.normal;
     a.material = r.material;
-    a.pad = 0;
     a.mass = r.mass;
     a.size1 = (double)r.size1;
     a.c1 = r.c1;
@@ -118,7 +123,8 @@ __global__ void __launch_bounds__(256) k_sphere_prep(SimConsts k, StateView s, C
     rD += (double)k.beta;
     const uint32_t fam = s.loc[owner].w;
     uint32_t c = 0;
-    for (uint32_t a = 0; a < s.nA; a++) {
+    const uint2 ar = anal_range(s, owner);
+    for (uint32_t a = ar.x; a < ar.x + ar.y; a++) {
         const AnalPlaced ap = s.anal[a];
         if (s.masks[mask_index(fam, s.loc[ap.owner].w)] != 0) continue;
         if (anal_overlap_cd(ap, X, Y, Z, rD, k.beta) != DEME_NOT_A_CONTACT) c++;
@@ -555,7 +561,8 @@ __global__ void __launch_bounds__(256) k_pair_assemble(SimConsts k, StateView s,
         double rD = (double)sp.w;
         rD += (double)k.beta;
         const uint32_t fam = s.loc[s.sOwner[A]].w;
-        for (uint32_t a = 0; a < s.nA && w < anEnd; a++) {
+        const uint2 ar = anal_range(s, s.sOwner[A]);
+        for (uint32_t a = ar.x; a < ar.x + ar.y && w < anEnd; a++) {
             const AnalPlaced ap = s.anal[a];
             if (s.masks[mask_index(fam, s.loc[ap.owner].w)] != 0) continue;
             const int t = anal_overlap_cd(ap, X, Y, Z, rD, k.beta);
@@ -670,7 +677,8 @@ void launch_force(const SimConsts& k, const StateView& s, const ContactView& c, 
                   const ContactOutputs* out, const AnalAccum& aa, const UserForceKernel* user, cudaStream_t st) {
     if (!(n)) return;
     const uint32_t nb = blocks_for(n, kForceThreads);
-    const size_t smem = 6u * aa.nAO * sizeof(float);
+    const bool partials = aa.nAO && !aa.direct;
+    const size_t smem = partials ? 6u * aa.nAO * sizeof(float) : 0;
     {
         ProfScope prof_(KID_FORCE, st);
         if (user) {
@@ -690,7 +698,7 @@ void launch_force(const SimConsts& k, const StateView& s, const ContactView& c, 
             k_force<false><<<nb, kForceThreads, smem, st>>>(k, s, c, n, has_hist, ContactOutputs{}, aa);
         }
     }
-    if (aa.nAO) {
+    if (partials) {
         ProfScope prof_(KID_OTHER, st);
         k_anal_reduce<<<6u * aa.nAO, 256, 0, st>>>(aa, nb, s.acc, s.alpha);
     }
@@ -850,7 +858,8 @@ __global__ void k_bin_count(SimConsts k, StateView s, uint16_t* nBins, uint8_t* 
     nBins[sid] = (uint16_t)((int)nx * (int)ny * (int)nz);
     const uint32_t fam = s.loc[owner].w;
     uint32_t c = 0;
-    for (uint32_t a = 0; a < s.nA; a++) {
+    const uint2 ar = anal_range(s, owner);
+    for (uint32_t a = ar.x; a < ar.x + ar.y; a++) {
         const AnalPlaced ap = s.anal[a];
         if (s.masks[mask_index(fam, s.loc[ap.owner].w)] != 0) continue;
         if (anal_overlap_cd(ap, X, Y, Z, rD, k.beta) != DEME_NOT_A_CONTACT) c++;

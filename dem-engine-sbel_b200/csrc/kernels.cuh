@@ -22,19 +22,21 @@ struct StateView {
     float4* alpha;  // torque accumulators (alpha)
     const float4* sph;  // (relX, relY, relZ, radius)
     const uint32_t* sOwner;
-    const uint8_t* sMat;
+    const uint16_t* sMat;
     const uint8_t* masks;
     MaterialTable mat;
     const AnalPlaced* anal;
     uint32_t nA;
     const Prescription* presc;  // DEME_NUM_FAMILIES entries
+    const uint2* ownerAnal;     // per owner (first, count) of the analytical components it meets; null = all
 };
 
 // Raw analytical component description (scene constants).
 struct AnalRaw {
     float relX, relY, relZ, rotX, rotY, rotZ, size1, size2, size3, mass;
     uint32_t owner;
-    uint8_t type, normal, material, pad;
+    uint8_t type, normal;
+    uint16_t material;
     double c1, c2;
 };
 
@@ -83,6 +85,7 @@ struct AnalAccum {
     float* partial;     // blocks x nAO x 6
     uint32_t nClumps;   // analytical owners are [nClumps, nClumps + nAO)
     uint32_t nAO;
+    bool direct;        // many analytical owners: float atomics onto their accumulators instead of partials
 };
 
 struct ContactOutputs {

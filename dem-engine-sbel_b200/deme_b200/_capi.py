@@ -135,10 +135,19 @@ SCENE_ARRAYS = [
 ]
 
 
+# optional arrays (packed multi-scene runs); absent keys leave the pointer NULL
+SCENE_EXTENSIONS = [
+    ("sphere_material_wide", np.uint16, "s"),
+    ("anal_material_wide", np.uint16, "a"),
+    ("owner_anal_first", np.uint32, "o"),
+    ("owner_anal_count", np.uint32, "o"),
+]
+
+
 class Scene(C.Structure):
     _fields_ = [("n_owners", C.c_uint32), ("n_spheres", C.c_uint32), ("n_anal", C.c_uint32),
                 ("n_materials", C.c_uint32)] + [(name, _P) for name, _, _ in SCENE_ARRAYS] + [
-                    ("prescriptions", _P)]
+                    ("prescriptions", _P)] + [(name, _P) for name, _, _ in SCENE_EXTENSIONS]
 
 
 STATE_FIELDS = [
@@ -217,6 +226,14 @@ def make_scene_struct(arrays: dict, counts: dict, prescriptions) -> tuple[Scene,
         setattr(s, name, ptr(a) if n > 0 else None)
     keep.append(prescriptions)
     s.prescriptions = C.addressof(prescriptions)
+    for name, dt, key in SCENE_EXTENSIONS:
+        if arrays.get(name) is None:
+            continue
+        a = np.ascontiguousarray(arrays[name], dtype=dt)
+        if a.shape[0] != counts[key]:
+            raise ValueError(f"scene array {name} has {a.shape[0]} entries, expected {counts[key]}")
+        keep.append(a)
+        setattr(s, name, ptr(a) if counts[key] > 0 else None)
     return s, keep
 
 

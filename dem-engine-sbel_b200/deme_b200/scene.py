@@ -71,6 +71,16 @@ class ClumpBatch:
         self.oriQ[:, 0] = 1
         self.families = np.zeros(n, np.uint32)
         self.family_is_specified = False
+        self.analytical_objects = None  # packed scenes: the external objects these clumps may touch
+
+    def SetAnalyticalObjects(self, objs):
+        """Packed independent scenes (no reference counterpart): the spheres of this batch meet only the analytical
+        components of ``objs`` (consecutively loaded external objects), not the walls of other scenes."""
+        objs = list(objs)
+        orders = [o.load_order for o in objs]
+        if orders != list(range(orders[0], orders[0] + len(orders))):
+            raise ValueError("the external objects of one batch must have been added consecutively")
+        self.analytical_objects = objs
 
     def GetNumClumps(self) -> int:
         return len(self.types)
@@ -430,8 +440,8 @@ class SceneBuilder:
         tmpl_off[1:] = np.cumsum(tmpl_nc)
         all_r = np.concatenate([t.radii for t in self.templates]) if nT else np.zeros(0, f32)
         all_p = np.concatenate([t.rel_pos for t in self.templates]) if nT else np.zeros((0, 3), f32)
-        all_m = np.concatenate([[m.load_order for m in t.materials] for t in self.templates]).astype(np.uint8) \
-            if nT else np.zeros(0, np.uint8)
+        all_m = np.concatenate([[m.load_order for m in t.materials] for t in self.templates]).astype(np.uint16) \
+            if nT else np.zeros(0, np.uint16)
         t_mass = np.array([t.mass for t in self.templates], f32)
         t_moi = np.array([t.moi for t in self.templates], f32).reshape(-1, 3)
         if self.batches:
@@ -459,7 +469,7 @@ class SceneBuilder:
         gidx = np.repeat(tmpl_off[types], ncomp) + local
         radius = all_r[gidx].astype(f32)
         rel = all_p[gidx].astype(f32)
-        smat = all_m[gidx].astype(np.uint8)
+        smat_w = all_m[gidx].astype(np.uint16)
         # owner positions relative to LBF in float (input_xyz - LBF, src/DEM/dT.cpp:539)
         ext_xyz = np.array([o.init_pos for o in self.extern], f32).reshape(-1, 3)
         pos_f = np.concatenate([xyz, ext_xyz]).astype(f32) - lbf.astype(f32)
@@ -487,13 +497,35 @@ class SceneBuilder:
             for (tp, mat, pos, rot, s1, s2, s3, nrm) in o.components:
                 comps.append((tp, nClumps + oi, nrm, mat.load_order, pos, rot, s1, s2, s3, o.mass))
         nA = len(comps)
-        if nA > 255:
+        restricted = any(b.analytical_objects is not None for b in self.batches)
+        if nA > 255 and not restricted:
             raise ValueError("at most 255 analytical components (objID_t is uint8)")
+        owner_anal = None
+        if restricted:
+            comp_start = np.zeros(nExt + 1, np.int64)
+            comp_start[1:] = np.cumsum([len(o.components) for o in self.extern])
+            first = np.zeros(nO, np.uint32)
+            count = np.zeros(nO, np.uint32)
+            o0 = 0
+            for b in self.batches:
+                nb_ = b.GetNumClumps()
+                if b.analytical_objects is None:
+                    f_, c_ = 0, nA
+                else:
+                    lo = b.analytical_objects[0].load_order
+                    hi = b.analytical_objects[-1].load_order + 1
+                    f_, c_ = int(comp_start[lo]), int(comp_start[hi] - comp_start[lo])
+                if c_ > 255:
+                    raise ValueError("a batch may meet at most 255 analytical components")
+                first[o0:o0 + nb_] = f_
+                count[o0:o0 + nb_] = c_
+                o0 += nb_
+            owner_anal = (first, count)
         anal = {
             "anal_type": np.array([c[0] for c in comps], np.uint8),
             "anal_owner": np.array([c[1] for c in comps], np.uint32),
             "anal_normal": np.array([c[2] for c in comps], np.uint8),
-            "anal_material": np.array([c[3] for c in comps], np.uint8),
+            "anal_material": np.array([c[3] for c in comps], np.uint16),
             "anal_relX": np.array([c[4][0] for c in comps], f32),
             "anal_relY": np.array([c[4][1] for c in comps], f32),
             "anal_relZ": np.array([c[4][2] for c in comps], f32),
@@ -553,13 +585,21 @@ class SceneBuilder:
         p.n_contact_wildcards = self.n_wildcards
         p.domain[:] = [float(v) for v in self.box]
 
+        wide = len(self.materials) > 256
+        ext_arrays = {}
+        if wide:
+            ext_arrays["sphere_material_wide"] = smat_w
+            ext_arrays["anal_material_wide"] = anal["anal_material"].astype(np.uint16)
+        anal["anal_material"] = (anal["anal_material"] & 0xFF).astype(np.uint8)
+        if owner_anal is not None:
+            ext_arrays["owner_anal_first"], ext_arrays["owner_anal_count"] = owner_anal
         arrays = dict(voxel=vox, locX=lx, locY=ly, locZ=lz, oriQw=oriQw, oriQx=oriQx, oriQy=oriQy, oriQz=oriQz,
                       vX=vX, vY=vY, vZ=vZ, omgX=wX, omgY=wY, omgZ=wZ, family=family, mass=mass,
                       mmiXX=np.ascontiguousarray(moi[:, 0]), mmiYY=np.ascontiguousarray(moi[:, 1]),
                       mmiZZ=np.ascontiguousarray(moi[:, 2]), sphere_owner=sph_owner, relX=np.ascontiguousarray(rel[:, 0]),
                       relY=np.ascontiguousarray(rel[:, 1]), relZ=np.ascontiguousarray(rel[:, 2]), radius=radius,
-                      sphere_material=smat, mat_E=matarr("E"), mat_nu=matarr("nu"), mat_CoR=matarr("CoR"),
-                      mat_mu=matarr("mu"), mat_Crr=matarr("Crr"), family_masks=masks, **anal)
+                      sphere_material=(smat_w & 0xFF).astype(np.uint8), mat_E=matarr("E"), mat_nu=matarr("nu"), mat_CoR=matarr("CoR"),
+                      mat_mu=matarr("mu"), mat_Crr=matarr("Crr"), family_masks=masks, **anal, **ext_arrays)
         counts = dict(o=nO, s=nS, a=nA, m=nM)
         info = dict(n_clumps=nClumps, n_ext=nExt, n_templates=nT, rmin=rmin, bin_size=bin_size, nb=nb, nv=nv, l=l,
                     beta=beta, lbf=lbf.copy(), box=self.box.copy(), merged_prescriptions=self.merged_prescriptions)

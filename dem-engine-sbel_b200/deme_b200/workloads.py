@@ -390,3 +390,97 @@ def collapse_loss(pos: np.ndarray, axis_xy, z0: float):
     g += dR2 * (1.0 - 0.5 * H / (Rrms ** 3))
     g[:, 2] += 1.0 / (n * Rrms)
     return float(loss), g
+
+
+def batch_scene_specs(n_scenes: int = 512, seed: int = 5, n_range=(500, 20000), r_range=(2e-3, 5e-3),
+                      side_range=(0.05, 0.2), mu_range=(0.2, 0.8), cor_range=(0.2, 0.8), packing: float = 0.5):
+    """Per-scene parameters of the batched calibration sweep: sphere count log-uniform in n_range, radius uniform
+    in r_range, box side uniform in side_range (enlarged where the spheres would exceed packing), friction and
+    restitution uniform in their ranges."""
+    rng = np.random.default_rng(seed)
+    N = np.exp(rng.uniform(np.log(n_range[0]), np.log(n_range[1]), n_scenes)).astype(np.int64)
+    r = rng.uniform(*r_range, n_scenes)
+    side = rng.uniform(*side_range, n_scenes)
+    need = (N * (4.0 / 3.0) * np.pi * r ** 3 / packing) ** (1.0 / 3.0)
+    side = np.maximum(side, need)
+    return [dict(n=int(N[i]), r=float(r[i]), side=float(side[i]), mu=float(rng.uniform(*mu_range)),
+                 CoR=float(rng.uniform(*cor_range)), seed=int(seed * 100003 + i)) for i in range(n_scenes)]
+
+
+def _settling_positions(spec, lbf):
+    """Jittered cubic lattice (pitch 2.2 r, jitter 0.1 r) filling the scene's square box from the floor up."""
+    rng = np.random.default_rng(spec["seed"])
+    r, n, side = spec["r"], spec["n"], spec["side"]
+    a = spec.get("pitch", 2.2) * r
+    per = max(int(side // a), 1)
+    idx = np.arange(n)
+    pos = np.stack([lbf[0] + (side - per * a) / 2 + a / 2 + (idx % per) * a,
+                    lbf[1] + (side - per * a) / 2 + a / 2 + ((idx // per) % per) * a,
+                    lbf[2] + spec.get("lift", 1.1) * r + (idx // (per * per)) * a], 1)
+    pos += rng.uniform(-0.1 * r, 0.1 * r, pos.shape)
+    height = (int(np.ceil(n / (per * per))) + 1) * a
+    return pos, height
+
+
+def _add_settling_scene(s, spec, lbf, rho=2500.0):
+    mat = s.LoadMaterial({"E": 1e7, "nu": 0.3, "CoR": spec["CoR"], "mu": spec["mu"], "Crr": 0.0})
+    t = s.LoadSphereType(float(f32(sphere_mass(spec["r"], rho))), spec["r"], mat)
+    pos, height = _settling_positions(spec, lbf)
+    b = s.AddClumps(t, pos.astype(f32))
+    box = s.AddExternalObject()
+    side = spec["side"]
+    X, Y, Z = lbf
+    H = max(height, side)
+    box.AddPlane((X + side / 2, Y + side / 2, Z), (0, 0, 1), mat)
+    box.AddPlane((X, Y + side / 2, Z + H / 2), (1, 0, 0), mat)
+    box.AddPlane((X + side, Y + side / 2, Z + H / 2), (-1, 0, 0), mat)
+    box.AddPlane((X + side / 2, Y, Z + H / 2), (0, 1, 0), mat)
+    box.AddPlane((X + side / 2, Y + side, Z + H / 2), (0, -1, 0), mat)
+    box.AddPlane((X + side / 2, Y + side / 2, Z + H), (0, 0, -1), mat)
+    return b, box, H
+
+
+def batched_settling(specs, dt: float = 1e-5):
+    """The scenes of ``specs`` packed into one: each in its own slot of a cubic grid of slots, with its own walls
+    (six planes) and material; each scene's spheres meet only its own walls.  Scenes never interact (slots are
+    separated by more than a contact reach).  ``info['scenes']`` maps each scene to its sphere range."""
+    heights = [max(_settling_positions(sp, (0.0, 0.0, 0.0))[1], sp["side"]) for sp in specs]
+    slot = max(max(sp["side"] for sp in specs), max(heights)) + 4 * max(sp["r"] for sp in specs) + 0.01
+    per = int(np.ceil(len(specs) ** (1.0 / 3.0)))
+    s = SceneBuilder()
+    world = per * slot + 0.02
+    s.InstructBoxDomainDimension(world, world, world)
+    s.SetCoordSysOrigin("explicit")  # lower corner at the origin
+    ranges = []
+    first = 0
+    for i, sp in enumerate(specs):
+        lbf = (0.01 + (i % per) * slot, 0.01 + ((i // per) % per) * slot, 0.01 + (i // (per * per)) * slot)
+        b, box, _ = _add_settling_scene(s, sp, lbf)
+        b.SetAnalyticalObjects([box])
+        ranges.append((first, sp["n"]))
+        first += sp["n"]
+    s.SetInitTimeStep(dt)
+    s.SetGravitationalAcceleration((0, 0, -9.81))
+    s.SetInitBinSize(2.0 * max(sp["r"] for sp in specs))
+    s.SetCDUpdateFreq(1)
+    s.SetExpandFactor(0.0)
+    built = s.Initialize()
+    built.info.update(workload="batched_settling", n_scenes=len(specs), scenes=ranges, slot=slot, slots_per_axis=per)
+    return built
+
+
+def single_settling(spec, dt: float = 1e-5):
+    """One scene of ``specs`` alone (for the sequential baseline and parity against the packed run)."""
+    s = SceneBuilder()
+    pos, height = _settling_positions(spec, (0.0, 0.0, 0.0))
+    H = max(height, spec["side"])
+    dom = max(spec["side"], H) + 0.02
+    s.InstructBoxDomainDimension(dom, dom, dom)
+    s.SetCoordSysOrigin("explicit")
+    _add_settling_scene(s, spec, (0.01, 0.01, 0.01))
+    s.SetInitTimeStep(dt)
+    s.SetGravitationalAcceleration((0, 0, -9.81))
+    s.SetInitBinSize(2.0 * spec["r"])
+    s.SetCDUpdateFreq(1)
+    s.SetExpandFactor(0.0)
+    return s.Initialize()

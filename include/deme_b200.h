@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define DEME_B200_ABI_VERSION 1
+#define DEME_B200_ABI_VERSION 2
 
 /* Status codes (the reference throws std::runtime_error instead: src/DEM/Structs.h:129-141, src/core/utils/GpuError.h:13-27). */
 typedef enum {
@@ -168,6 +168,11 @@ typedef struct {
     /* families */
     const uint8_t* family_masks;                        /* DEME_NUM_FAMILY_MASK entries, 1 = prevent contact */
     const deme_family_prescription* prescriptions;      /* DEME_NUM_FAMILIES entries */
+    /* Extensions for many independent scenes packed into one (no reference counterpart); NULL = unused. */
+    const uint16_t* sphere_material_wide;  /* per sphere, replaces sphere_material (up to 65536 materials) */
+    const uint16_t* anal_material_wide;    /* per component, replaces anal_material */
+    const uint32_t* owner_anal_first;      /* per owner: its spheres meet only the analytical components */
+    const uint32_t* owner_anal_count;      /*   [first, first + count) (then n_anal may exceed 255) */
 } deme_scene;
 
 /* Mutable owner state (download/upload).  Any pointer may be NULL to skip that array. */

@@ -44,8 +44,10 @@ struct oracle_ctx {
     float *mass, *mXX, *mYY, *mZZ;
     uint32_t* sOwner;
     float *rX, *rY, *rZ, *rad;
-    uint8_t* sMat;
-    uint8_t *aType, *aNormal, *aMat;
+    uint16_t* sMat;
+    uint8_t *aType, *aNormal;
+    uint16_t* aMat;
+    uint32_t *oAFirst, *oACount; /* per owner analytical range (packed scenes), NULL = all */
     uint32_t* aOwner;
     float *aRX, *aRY, *aRZ, *aDX, *aDY, *aDZ, *aS1, *aS2, *aS3, *aMass;
     double *aC1, *aC2; /* cone: sin, cos of the half angle */
@@ -160,6 +162,18 @@ static inline void sphere_pos(const oracle_ctx* c, uint32_t s, double* X, double
     *Z = oz + (double)rz;
 }
 /* Analytical component placement (DEMBinSphereKernels.cu:84-104, DEMCalcForceKernels.cu:123-142). */
+/* Analytical components the spheres of `owner` may meet: all, or the owner's range when independent scenes are packed
+ * into one (their walls must not reach each other's spheres; no reference counterpart). */
+static inline void anal_range(const oracle_ctx* c, uint32_t owner, uint32_t* k0, uint32_t* k1) {
+    if (c->oAFirst && c->oACount) {
+        *k0 = c->oAFirst[owner];
+        *k1 = c->oAFirst[owner] + c->oACount[owner];
+    } else {
+        *k0 = 0;
+        *k1 = c->nA;
+    }
+}
+
 static inline void anal_place(const oracle_ctx* c, uint32_t k, double* X, double* Y, double* Z, float* dx, float* dy,
                               float* dz) {
     uint32_t o = c->aOwner[k];
@@ -352,11 +366,20 @@ oracle_ctx* orc_create(const deme_sim_params* p, const deme_scene* s) {
     XDUP(c->rY, s->relY, nS);
     XDUP(c->rZ, s->relZ, nS);
     XDUP(c->rad, s->radius, nS);
-    XDUP(c->sMat, s->sphere_material, nS);
+    XALLOC(c->sMat, nS);
+    for (uint32_t i = 0; i < nS; i++)
+        c->sMat[i] = s->sphere_material_wide ? s->sphere_material_wide[i] : (uint16_t)s->sphere_material[i];
     XDUP(c->aType, s->anal_type, nA);
     XDUP(c->aOwner, s->anal_owner, nA);
     XDUP(c->aNormal, s->anal_normal, nA);
-    XDUP(c->aMat, s->anal_material, nA);
+    XALLOC(c->aMat, nA);
+    for (uint32_t i = 0; i < nA; i++)
+        c->aMat[i] = s->anal_material_wide ? s->anal_material_wide[i] : (uint16_t)s->anal_material[i];
+    c->oAFirst = c->oACount = NULL;
+    if (s->owner_anal_first && s->owner_anal_count) {
+        XDUP(c->oAFirst, s->owner_anal_first, nO);
+        XDUP(c->oACount, s->owner_anal_count, nO);
+    }
     XDUP(c->aRX, s->anal_relX, nA);
     XDUP(c->aRY, s->anal_relY, nA);
     XDUP(c->aRZ, s->anal_relZ, nA);
@@ -396,7 +419,7 @@ void orc_destroy(oracle_ctx* c) {
                     c->aRY,   c->aRZ,    c->aDX,    c->aDY,    c->aDZ,    c->aS1,    c->aS2,    c->aS3,   c->aMass,
                     c->aC1,   c->aC2,    c->E,      c->nu,     c->CoR,    c->mu,     c->Crr,    c->masks, c->idA,
                     c->idB,   c->map,    c->type,   c->wc,     c->F,      c->TOF,    c->CPA,    c->CPB,   c->pA,
-                    c->pB,    c->pT,     c->nBins,  c->nAnal,  c->pairBin, c->pairSph};
+                    c->pB,    c->pT,     c->nBins,  c->nAnal,  c->pairBin, c->pairSph, c->oAFirst, c->oACount};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     free(c);
 }
@@ -450,7 +473,9 @@ int32_t orc_detect_contacts(oracle_ctx* c) {
         c->nBins[s] = (uint16_t)((int)nx * (int)ny * (int)nz);
         uint8_t cnt = 0;
         uint32_t sf = c->fam[c->sOwner[s]];
-        for (uint32_t k = 0; k < c->nA; k++) {
+        uint32_t k0, k1;
+        anal_range(c, c->sOwner[s], &k0, &k1);
+        for (uint32_t k = k0; k < k1; k++) {
             uint32_t of = c->fam[c->aOwner[k]];
             if (c->masks[mask_index(sf, of)] != 0) continue;
             double ax, ay, az;
@@ -492,7 +517,9 @@ int32_t orc_detect_contacts(oracle_ctx* c) {
                 }
         uint32_t goff = analOff[s];
         uint32_t sf = c->fam[c->sOwner[s]];
-        for (uint32_t k = 0; k < c->nA; k++) {
+        uint32_t k0, k1;
+        anal_range(c, c->sOwner[s], &k0, &k1);
+        for (uint32_t k = k0; k < k1; k++) {
             uint32_t of = c->fam[c->aOwner[k]];
             if (c->masks[mask_index(sf, of)] != 0) continue;
             double ax, ay, az;
