@@ -202,6 +202,11 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint timing on the column collapse")
     ap.add_argument("--adjoint-steps", type=int, default=2000)
     ap.add_argument("--adjoint-checkpoint", type=int, default=100)
+    ap.add_argument("--no-batched", action="store_true", help="skip the packed multi-scene measurement")
+    ap.add_argument("--batch-scenes", type=int, default=512)
+    ap.add_argument("--batch-steps", type=int, default=1000)
+    ap.add_argument("--batch-checkpoint", type=int, default=100)
+    ap.add_argument("--batch-sample", type=int, default=12)
     ap.add_argument("--settle-steps", type=int, default=15000,
                     help="untimed preparation: steps at --settle-dt that let the loose lattice fall into a bed")
     ap.add_argument("--settle-dt", type=float, default=2e-5)
@@ -356,6 +361,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(args)
     adj = None if args.no_adjoint else adjoint_measure(args, stream)
+    batched = None if args.no_batched else batched_measure(args, stream)
 
     if rank == 0:
         line = {
@@ -375,7 +381,7 @@ def main():
             "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": C.sizeof(capi.FamilyPrescription),
                     "d2h_bytes_per_step": 8},
-            "gpu_launches": int(launches), "clocks": clocks, "adjoint": adj,
+            "gpu_launches": int(launches), "clocks": clocks, "adjoint": adj, "batched": batched,
         }
         print(json.dumps(line), flush=True)
     s.close()
@@ -430,6 +436,85 @@ def adjoint_measure(args, stream):
             "record_ms_per_step": t_rec / T, "adjoint_ms_per_step": t_bwd / T, "adjoint_over_forward": t_bwd / t_fwd,
             "loss": loss, "dL_dE_CoR_mu_Crr": [float(v) for v in out["d_material"][0]], "n_contacts_final": nC,
             "gradient_precision": "FP64 accumulators, FP32 state"}
+
+
+def batched_measure(args, stream):
+    """The batched calibration sweep: all scenes packed into one run, a forward window and a forward + adjoint
+    window (per-scene loss: the mean final height of its spheres; gradients for every scene's material), against
+    the same windows run scene by scene (timed on a sample of scenes spanning the sizes, fitted linearly in the
+    sphere count and summed over all scenes)."""
+    import numpy as np
+    import torch
+    from deme_b200 import Solver, adjoint, workloads
+    specs = workloads.batch_scene_specs(args.batch_scenes)
+    T, K = args.batch_steps, args.batch_checkpoint
+
+    def solver(built):
+        s = Solver(built)
+        s.lib.deme_set_streams(s.h, C.c_void_p(stream.cuda_stream), C.c_void_p(stream.cuda_stream))
+        return s
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3, r
+
+    def height_seed(built, ranges):
+        seed = np.zeros((built.counts["o"], 3))
+        for first, n in ranges:
+            seed[first:first + n, 2] = 1.0 / n
+        return seed
+
+    built = workloads.batched_settling(specs)
+    ranges = built.info["scenes"]
+    w = solver(built)
+    w.step(3)
+    w.close()
+    sf = solver(built)
+    t_fwd, _ = timed(lambda: sf.step(T))
+    nC = sf.num_contacts()
+    sf.close()
+    sa = solver(built)
+    t_rec, _ = timed(lambda: adjoint.record(sa, T, K))
+    t_bwd, out = timed(lambda: adjoint.backward(sa, d_pos=height_seed(built, ranges)))
+    sa.close()
+    # scene by scene, on a sample spanning the sizes
+    sizes = np.array([sp["n"] for sp in specs])
+    pick = np.unique(np.argsort(sizes)[np.linspace(0, len(specs) - 1, args.batch_sample).astype(int)])
+    rows = []
+    for i in pick:
+        b1 = workloads.single_settling(specs[i])
+        s1 = solver(b1)
+        s1.step(3)
+        s1.close()
+        s1 = solver(b1)
+        tf, _ = timed(lambda: s1.step(T))
+        s1.close()
+        s1 = solver(b1)
+        tr, _ = timed(lambda: adjoint.record(s1, T, K))
+        tb, _ = timed(lambda: adjoint.backward(s1, d_pos=height_seed(b1, [(0, specs[i]["n"])])))
+        s1.close()
+        rows.append((sizes[i], tf, tr + tb))
+    rows = np.array(rows, dtype=np.float64)
+    fit_f = np.polyfit(rows[:, 0], rows[:, 1], 1)
+    fit_a = np.polyfit(rows[:, 0], rows[:, 2], 1)
+    seq_f = float(np.sum(np.polyval(fit_f, sizes)))
+    seq_a = float(np.sum(np.polyval(fit_a, sizes)))
+    n = len(specs)
+    return {"workload": f"{n} settling scenes packed in one run: 500-20,000 spheres (log-uniform), r 2-5 mm, box "
+                        "0.05-0.2 m, friction and restitution U[0.2, 0.8] per scene, dt 1e-5, CD every step",
+            "n_scenes": n, "n_spheres": int(sizes.sum()), "steps": T, "checkpoint_every": K,
+            "n_contacts_final": nC,
+            "forward_s": t_fwd, "forward_adjoint_s": t_rec + t_bwd,
+            "scenes_per_s": n / t_fwd, "scenes_per_s_with_adjoint": n / (t_rec + t_bwd),
+            "sequential_scenes_per_s": n / seq_f, "sequential_scenes_per_s_with_adjoint": n / seq_a,
+            "speedup_forward": seq_f / t_fwd, "speedup_with_adjoint": seq_a / (t_rec + t_bwd),
+            "sequential_sample": f"{len(rows)} scenes timed alone, time fitted linearly in sphere count",
+            "material_gradients_finite": bool(np.all(np.isfinite(out["d_material"])))}
 
 
 def s_grid_cells(built):
