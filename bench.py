@@ -15,9 +15,11 @@ per-kernel durations that give the roofline of the dominant kernel; an e2e pass 
 pinned host-to-device update of the drum's prescribed rotation and a device-to-host read of the kinetic energy
 every step.
 
---impl reference times the CPU implementation of the same method (the C oracle with OpenMP on all host cores;
-the reference itself has no CPU solver and cannot express the analytical cylinder) on a bounded sample of the
-drum workload.
+--impl reference times the reference's CPU path on a bounded sample: its own kernel code compiled for the CPU
+(OpenMP on all host cores) on the shell variant of the drum, since the reference has no analytical cylinder (the C
+oracle on the analytical drum where that build is absent).  The same line carries `reference_kernels_gpu`: the
+reference's own kernels, NVRTC-compiled for sm_100a, on the full-size shell drum, which the main arm also runs
+(`shell_drum`) for the comparison against the reference's GPU kernels.
 """
 from __future__ import annotations
 
@@ -139,34 +141,127 @@ def build_drum(n_clumps: int, seed: int, spacing: float = 1.02):
 SAMPLE_SPACING = 0.745
 
 
+def shell_drum(n_clumps: int):
+    """The drum as the reference can express it (cylinder replaced by a fixed shell of spheres), on the dense
+    lattice that has the settled bed's contact density; both arms run this scene for the reference-kernel
+    comparison."""
+    from deme_b200 import workloads
+    return workloads.drum(n_clumps=n_clumps, shell=True, spacing=SAMPLE_SPACING)
+
+
+SHELL_WARMUP = 3
+SHELL_STEPS = 40
+
+
+def reference_kernels_gpu(args):
+    """The reference's own kernels (substituted and NVRTC-compiled from its sources, prebuilt under oracle/_ref) on
+    the GPU, on the full-size shell drum.  Device time with CUDA events: first with only the count read-backs the
+    next launch needs, then synchronising after every launch as the reference's host code does."""
+    try:
+        from oracle import ref_gpu
+        built = shell_drum(args.clumps)
+        if not ref_gpu.prebuilt(built) and not ref_gpu.ref_gpu_build.available():
+            return {"unavailable": "reference kernels for this drum size were not prebuilt (needs the reference's "
+                                   "sources at build time)"}
+        ref = ref_gpu.RefGPU(built, fmad=True)
+    except Exception as e:  # the arm must still print its CPU line
+        return {"unavailable": f"{type(e).__name__}: {e}"}
+    ref.step(SHELL_WARMUP)
+    ms = ref.time_steps(SHELL_STEPS)
+    nC = ref.num_contacts()
+    ref.set_sync_each(True)
+    ms_sync = ref.time_steps(SHELL_STEPS // 4)
+    ref.set_sync_each(False)
+    phases = ref.profile_steps(5)
+    # the reference's other contact-kernel variant (SetOneBinPerThread): the better of the two is the baseline
+    ref.set_one_bin_per_thread(True)
+    ref.step(1)
+    ms_thread = ref.time_steps(SHELL_STEPS // 4) / (SHELL_STEPS // 4)
+    phases_thread = ref.profile_steps(2)
+    ref.close()
+    best = min(ms / SHELL_STEPS, ms_thread)
+    v = built.n_spheres / (best / 1e3) / 1e6
+    return {"value": v, "unit": UNIT, "ms_per_step": best,
+            "block_per_bin": {"ms_per_step": ms / SHELL_STEPS, "ms_per_step_sync_each": ms_sync / (SHELL_STEPS // 4),
+                              "phase_ms_per_step": phases},
+            "thread_per_bin": {"ms_per_step": ms_thread, "phase_ms_per_step": phases_thread},
+            "workload": f"drum shell variant: {built.info['n_clumps']} three-sphere clumps + {built.info['n_shell']} "
+                        f"fixed shell spheres + 2 end planes, dense lattice (pitch {SAMPLE_SPACING}), dt 5e-6, CD "
+                        f"every step",
+            "n_spheres": built.n_spheres, "n_contacts": nC, "steps": SHELL_STEPS, "warmup": SHELL_WARMUP,
+            "kernels": "reference src/kernel/*.cu substituted per scene, NVRTC sm_100a (FMA default), CUB "
+                       "sorts/scans/reduce-by-key; value = the faster of its two contact-kernel variants"}
+
+
 def run_reference(args):
-    """CPU implementation of the same method (the C oracle, OpenMP on all host cores) on a bounded sample."""
+    """The reference's CPU path on a bounded sample: its own kernel code compiled for the CPU (oracle/_ref, OpenMP
+    over the emulated blocks) on the shell variant of the drum, or, where that build is absent, the C oracle on the
+    analytical drum.  Also times the reference's kernels on the GPU on the full-size shell drum."""
     from deme_b200 import HandleSolver, capi
-    lib_path = os.path.join(ROOT, "oracle", "_build", "libdeme_oracle.so")
-    if not os.path.exists(lib_path):
-        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
     cores = os.cpu_count() or 1
     n_clumps = min(args.clumps, args.ref_clumps)
-    built = build_drum(n_clumps, seed=1, spacing=SAMPLE_SPACING)
-    orc = HandleSolver(capi.load_library(lib_path), "orc_", built, threads=cores)
+    built = shell_drum(n_clumps)
+    try:
+        from oracle import ref_build
+        lib_path = ref_build.lookup(built)
+    except Exception:
+        lib_path = None
+    if lib_path:
+        kind, prefix, who = "reference", "ref_", "the reference's kernel code compiled for the CPU (oracle/_ref)"
+        wl = f"drum shell variant ({n_clumps} clumps + {built.info['n_shell']} shell spheres)"
+    else:
+        lib_path = os.path.join(ROOT, "oracle", "_build", "libdeme_oracle.so")
+        if not os.path.exists(lib_path):
+            subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+        built = build_drum(n_clumps, seed=1, spacing=SAMPLE_SPACING)
+        kind, prefix, who = "port", "orc_", "the C oracle"
+        wl = f"rotating drum ({n_clumps} clumps)"
+    cpu = HandleSolver(capi.load_library(lib_path), prefix, built, threads=cores)
     w = max(1, min(args.warmup, 2))
     k = max(1, min(args.steps, args.ref_steps))
-    orc.step(w)
+    cpu.step(w)
     t0 = time.perf_counter()
-    orc.step(k)
+    cpu.step(k)
     dt = time.perf_counter() - t0
     v = built.n_spheres * k / dt / 1e6
-    sample = (f"dense drum lattice (pitch {SAMPLE_SPACING} x clump diameter, settled-bed contact density) with "
-              f"{n_clumps} clumps ({built.n_spheres} spheres, {orc.num_contacts()} contacts), {k} timed steps after "
-              f"{w} warm-up steps, C oracle (OpenMP, {cores} threads)")
+    sample = (f"{wl} on the dense lattice (pitch {SAMPLE_SPACING} x clump diameter, settled-bed contact density): "
+              f"{built.n_spheres} spheres, {cpu.num_contacts()} contacts, {k} timed steps after {w} warm-up steps, "
+              f"{who}, OpenMP {cores} threads")
+    cpu.close()
+    gpu = reference_kernels_gpu(args) if not args.no_reference_gpu else None
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": k,
             "warmup": w, "ms_per_step": dt / k * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 forces, f64 positions, integer voxels", "data": "synthetic (seeded)",
-            "config": {"workload": "rotating drum, three-sphere clumps (sample)", "n_clumps": n_clumps,
-                       "n_spheres": built.n_spheres},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": {"workload": wl + " (CPU sample)", "n_clumps": n_clumps, "n_spheres": built.n_spheres},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_kernels_gpu": gpu}
     print(json.dumps(line), flush=True)
+
+
+def shell_drum_measure(args, stream):
+    """This build on the same shell drum the reference's GPU kernels are timed on (device time, CUDA events)."""
+    import torch
+    from deme_b200 import Solver
+    built = shell_drum(args.clumps)
+    s = Solver(built)
+    s.lib.deme_set_streams(s.h, C.c_void_p(stream.cuda_stream), C.c_void_p(stream.cuda_stream))
+    s.step(SHELL_WARMUP)
+    s.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    s.step(SHELL_STEPS)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    nC = s.num_contacts()
+    s.close()
+    return {"value": built.n_spheres * SHELL_STEPS / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": ms / SHELL_STEPS,
+            "workload": f"drum shell variant: {built.info['n_clumps']} three-sphere clumps + {built.info['n_shell']} "
+                        f"fixed shell spheres + 2 end planes, dense lattice (pitch {SAMPLE_SPACING}), dt 5e-6, CD "
+                        f"every step",
+            "n_spheres": built.n_spheres, "n_contacts": nC, "steps": SHELL_STEPS, "warmup": SHELL_WARMUP}
 
 
 def cpu_baseline_sample(args):
@@ -199,6 +294,9 @@ def main():
     ap.add_argument("--ref-clumps", type=int, default=200_000)
     ap.add_argument("--ref-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-shell", action="store_true", help="skip the shell-drum run (the reference-kernel comparison)")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="reference arm: skip timing the reference's kernels on the GPU")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint timing on the column collapse")
     ap.add_argument("--adjoint-steps", type=int, default=2000)
     ap.add_argument("--adjoint-checkpoint", type=int, default=100)
@@ -360,6 +458,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(args)
+    shell = shell_drum_measure(args, stream) if (rank == 0 and not args.no_shell) else None
     adj = None if args.no_adjoint else adjoint_measure(args, stream)
     batched = None if args.no_batched else batched_measure(args, stream)
 
@@ -381,7 +480,7 @@ def main():
             "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": C.sizeof(capi.FamilyPrescription),
                     "d2h_bytes_per_step": 8},
-            "gpu_launches": int(launches), "clocks": clocks, "adjoint": adj, "batched": batched,
+            "gpu_launches": int(launches), "clocks": clocks, "shell_drum": shell, "adjoint": adj, "batched": batched,
         }
         print(json.dumps(line), flush=True)
     s.close()

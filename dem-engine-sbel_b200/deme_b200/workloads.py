@@ -106,6 +106,11 @@ def drum(n_clumps: int = 1_000_000, r_nom: float = 2e-3, rho: float = 2500.0, n_
     lattice pitch over the clump's bounding diameter: above 1 no two clumps touch; below 1 neighbouring clumps
     interpenetrate, which gives a dense bed without settling (used to size CPU samples).  Lattice sites stay
     ``wall_clearance`` clump reaches inside the walls; below 1 the outer clumps start in contact with them.
+
+    ``shell=True`` builds the variant the reference can express, which has only planes and plates as analytical
+    components. The cylinder becomes a shell of fixed spheres of radius ``r_nom``, centred one radius outside R on
+    a square lattice of pitch 1.9 ``r_nom``, so that no bed sphere fits through. The shell does not rotate. The two
+    end planes and the shell form one fixed family with contacts inside it disabled.
     """
     rng = np.random.default_rng(seed)
     tmpl = [triangle_template(rng, r_nom, rho) for _ in range(n_templates)]
@@ -147,6 +152,30 @@ def drum(n_clumps: int = 1_000_000, r_nom: float = 2e-3, rho: float = 2500.0, n_
     b = s.AddClumps(types, P.astype(f32))
     b.SetOriQ(random_quaternions(rng, n_clumps))
     drum_fam = 10
+    if shell:
+        pitch = 1.9 * r_nom
+        Rc = R + r_nom
+        n_ring = int(2 * math.pi * Rc / pitch)
+        n_axial = int(L / pitch) + 1
+        th = 2 * math.pi * np.arange(n_ring) / n_ring
+        ys = -L / 2 + (np.arange(n_axial) + 0.5) * (L / n_axial)
+        TH, Y = np.meshgrid(th, ys, indexing="ij")
+        S = np.stack([Rc * np.cos(TH).ravel(), Y.ravel(), Rc * np.sin(TH).ravel()], 1)
+        shell_t = s.LoadSphereType(sphere_mass(r_nom, rho), r_nom, mat)
+        sb = s.AddClumps([shell_t] * len(S), S.astype(f32))
+        sb.SetFamily(drum_fam)
+        d = s.AddExternalObject()
+        d.AddPlane((0, -L / 2, 0), (0, 1, 0), mat)
+        d.AddPlane((0, L / 2, 0), (0, -1, 0), mat)
+        d.SetFamily(drum_fam)
+        s.SetFamilyFixed(drum_fam)
+        s.DisableContactBetweenFamilies(drum_fam, drum_fam)
+        s.SetInitTimeStep(dt)
+        s.SetGravitationalAcceleration((0, 0, -9.81))
+        built = s.Initialize()
+        built.info.update(workload="drum_shell", R=R, L=L, n_templates=n_templates, seed=seed, vol_clump=vol_clump,
+                          n_clumps=n_clumps, n_shell=len(S), lattice_spacing=a, clump_reach=reach)
+        return built
     d = s.AddExternalObject()
     d.AddCylinder((0, 0, 0), (0, 1, 0), R, mat)
     d.AddPlane((0, -L / 2, 0), (0, 1, 0), mat)

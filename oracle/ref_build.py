@@ -221,10 +221,48 @@ def generate(built, out_root: str = OUT_ROOT) -> tuple[str, list]:
     return d, paths
 
 
+INDEX = os.path.join(OUT_ROOT, "cpu-index.txt")
+
+
+def _index_key(built) -> str:
+    if HERE not in sys.path:
+        sys.path.insert(0, HERE)
+    import ref_gpu_build  # noqa: E402
+    return ref_gpu_build.scene_key(built, fmad=False)
+
+
+def _index_put(built, lib: str):
+    rows = {}
+    if os.path.exists(INDEX):
+        with open(INDEX) as f:
+            rows = dict(line.split() for line in f if line.strip())
+    rows[_index_key(built)] = os.path.relpath(lib, OUT_ROOT)
+    with open(INDEX + ".tmp", "w") as f:
+        f.write("".join(f"{k} {v}\n" for k, v in sorted(rows.items())))
+    os.replace(INDEX + ".tmp", INDEX)
+
+
+def lookup(built) -> str | None:
+    """The CPU build for this scene: built now where the reference's sources exist, else a prebuilt one found
+    through the index (keyed by the scene values the substitution reads), else None."""
+    if available():
+        return build(built)
+    if os.path.exists(INDEX):
+        key = _index_key(built)
+        with open(INDEX) as f:
+            for line in f:
+                k, v = line.split()
+                if k == key and os.path.exists(os.path.join(OUT_ROOT, v)):
+                    return os.path.join(OUT_ROOT, v)
+    return None
+
+
 def build(built, out_root: str = OUT_ROOT, verbose: bool = False) -> str:
     d, paths = generate(built, out_root)
     lib = os.path.join(d, "libdeme_ref.so")
     if os.path.exists(lib):
+        if out_root == OUT_ROOT:
+            _index_put(built, lib)
         return lib
     objs = []
     flags = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-w",
@@ -245,4 +283,6 @@ def build(built, out_root: str = OUT_ROOT, verbose: bool = False) -> str:
     tmp = lib + ".tmp"
     subprocess.check_call(["g++", "-shared", "-fopenmp", "-o", tmp] + objs)
     os.replace(tmp, lib)
+    if out_root == OUT_ROOT:
+        _index_put(built, lib)
     return lib
