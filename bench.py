@@ -239,6 +239,55 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def hopper_measure(args, stream):
+    """Hopper, 4M log-normal spheres in an analytical cone, contact detection every 5 steps with a margin of 0.1
+    median radius.  The seeded packing settles first (untimed, --hopper-settle steps at dt 6e-6, gate closed), then
+    the same bed runs twice at dt 2e-6: with synchronous detection, and with kT and dT on two streams (a detection
+    adopted 5 steps after the poses it was made from).  Device time with CUDA events."""
+    import torch
+    from deme_b200 import Solver, workloads
+    built = workloads.hopper(n=args.hopper_spheres)
+    f = int(built.params.cd_update_freq)
+    dt_run = float(built.params.h)
+    kt = torch.cuda.Stream()
+    s = Solver(built)
+    s.lib.deme_set_streams(s.h, C.c_void_p(kt.cuda_stream), C.c_void_p(stream.cuda_stream))
+    t0 = time.perf_counter()
+    if args.hopper_settle > 0:
+        s.set_time_step(6e-6)
+        s.step(args.hopper_settle)
+        s.set_time_step(dt_run)
+    s.sync()
+    prep_s = time.perf_counter() - t0
+    bed_state, bed_contacts = s.state(), s.contacts()
+    out = {"workload": f"hopper: {built.n_spheres} spheres, log-normal radii (median 1.5 mm, sigma 0.25), 30 deg cone, "
+                       f"40 mm outlet (gate closed), dt {dt_run:g}, CD every {f} steps, margin 0.1 median radius",
+           "initial_state": f"seeded lattice packing settled {args.hopper_settle} steps at dt 6e-6 (untimed, "
+                            f"{prep_s:.1f} s)",
+           "n_spheres": built.n_spheres, "steps": args.hopper_steps, "warmup": 2 * f}
+    for lag in (0, f):
+        s.set_state({k: v for k, v in bed_state.items() if not k.startswith("a")})
+        s.set_contacts({k: bed_contacts[k] for k in ("idA", "idB", "type", "wildcards")})
+        s.set_async_cd(lag)
+        s.step(2 * f)
+        s.sync()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.step(args.hopper_steps)
+        s.sync()  # adopts a pending detection: its kT work is inside the timed region
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        key = "sync" if lag == 0 else "two_streams"
+        out[key] = {"lag": lag, "ms_per_step": ms / args.hopper_steps,
+                    "value": built.n_spheres * args.hopper_steps / (ms / 1e3) / 1e6, "unit": UNIT,
+                    "n_contacts": s.num_contacts()}
+        s.set_async_cd(0)
+    s.close()
+    return out
+
+
 def shell_drum_measure(args, stream):
     """This build on the same shell drum the reference's GPU kernels are timed on (device time, CUDA events)."""
     import torch
@@ -295,6 +344,10 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-shell", action="store_true", help="skip the shell-drum run (the reference-kernel comparison)")
+    ap.add_argument("--no-hopper", action="store_true", help="skip the hopper run (detection every 5 steps, two streams)")
+    ap.add_argument("--hopper-spheres", type=int, default=4_000_000)
+    ap.add_argument("--hopper-steps", type=int, default=500)
+    ap.add_argument("--hopper-settle", type=int, default=40000, help="untimed settling steps of the hopper bed")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="reference arm: skip timing the reference's kernels on the GPU")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint timing on the column collapse")
@@ -459,6 +512,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(args)
     shell = shell_drum_measure(args, stream) if (rank == 0 and not args.no_shell) else None
+    hopper = hopper_measure(args, stream) if (rank == 0 and not args.no_hopper) else None
     adj = None if args.no_adjoint else adjoint_measure(args, stream)
     batched = None if args.no_batched else batched_measure(args, stream)
 
@@ -480,7 +534,7 @@ def main():
             "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": C.sizeof(capi.FamilyPrescription),
                     "d2h_bytes_per_step": 8},
-            "gpu_launches": int(launches), "clocks": clocks, "shell_drum": shell, "adjoint": adj, "batched": batched,
+            "gpu_launches": int(launches), "clocks": clocks, "shell_drum": shell, "hopper": hopper, "adjoint": adj, "batched": batched,
         }
         print(json.dumps(line), flush=True)
     s.close()

@@ -392,8 +392,8 @@ int32_t check_adjoint_scene(deme_handle* h) {
         h->err = "adjoint: only the built-in Hertz-Mindlin model is differentiated";
         return DEME_ERR_INVALID;
     }
-    if (h->params.integrator != DEME_INTEGRATOR_EXTENDED_TAYLOR || h->params.cd_update_freq > 1) {
-        h->err = "adjoint: needs Extended Taylor integration and contact detection every step";
+    if (h->params.integrator != DEME_INTEGRATOR_EXTENDED_TAYLOR || h->params.cd_update_freq > 1 || h->cdLag > 0) {
+        h->err = "adjoint: needs Extended Taylor integration and synchronous contact detection every step";
         return DEME_ERR_INVALID;
     }
     std::vector<float4> sph(h->nS), moi(h->nO);

@@ -439,6 +439,7 @@ int32_t deme_create(const deme_sim_params* params, const deme_scene* scene, deme
 
 void deme_destroy(deme_handle* h) {
     if (!h) return;
+    if (h->cdPending && h->st_kt) cudaStreamSynchronize(h->st_kt);
     if (h->own_dt) cudaStreamSynchronize(h->own_dt);
     if (h->own_kt) cudaStreamSynchronize(h->own_kt);
     adjoint_release(h);  // frees its arrays through dfree, so before the bulk free below
@@ -448,6 +449,9 @@ void deme_destroy(deme_handle* h) {
     if (h->hErr) cudaFreeHost(h->hErr);
     if (h->hKE) cudaFreeHost(h->hKE);
     if (h->hPresc) cudaFreeHost(h->hPresc);
+    if (h->hCounts) cudaFreeHost(h->hCounts);
+    for (cudaEvent_t e : {h->evPose, h->evCounts, h->evListReady, h->evListReleased})
+        if (e) cudaEventDestroy(e);
     if (h->own_dt) cudaStreamDestroy(h->own_dt);
     if (h->own_kt) cudaStreamDestroy(h->own_kt);
     release_user_force_model(h->userForce);
@@ -474,8 +478,11 @@ int32_t deme_set_force_model(deme_handle* h, const char* src, const char* const*
     return DEME_OK;
 }
 
+static int32_t cd_finish(deme_handle* h);
+
 int32_t deme_set_streams(deme_handle* h, void* kT_stream, void* dT_stream) {
     if (!h) return DEME_ERR_INVALID;
+    TRY(cd_finish(h));
     h->st_kt = kT_stream ? (cudaStream_t)kT_stream : h->own_kt;
     h->st_dt = dT_stream ? (cudaStream_t)dT_stream : h->own_dt;
     return DEME_OK;
@@ -494,13 +501,14 @@ int32_t deme_keep_contact_forces(deme_handle* h, int32_t enable) {
 }
 
 // ---------------------------------------------------------------------------------------------------- kT ----
-int32_t deme_detect_contacts(deme_handle* h) {
-    if (!h) return DEME_ERR_INVALID;
-    cudaStream_t st = h->st_dt;
+// Contact search up to the per-sphere offsets of the new list (into lists[cur ^ 1].off), for the poses in `s`, with
+// the analytical components placed into `anal`.  The pair total, the pool count and its overflow counter are copied
+// to `hCnt` (pinned) at the end, on `st`; nothing here waits for the device.
+static int32_t cd_search(deme_handle* h, const StateView& s, AnalPlaced* anal, cudaStream_t st, bool retry,
+                         uint32_t* hCnt) {
     const SimConsts& k = h->k;
-    StateView s = h->state_view();
     CDView& cd = h->cd;
-    launch_place_anal(k, s, h->analRaw, h->analPlaced, h->nA, st);
+    launch_place_anal(k, s, h->analRaw, anal, h->nA, st);
     CUDA_TRY(h, cudaMemsetAsync(cd.cellCount, 0, ((size_t)h->nCells + 1) * sizeof(uint32_t), st));
     launch_sphere_prep(k, s, cd, st);
     exclusive_scan_u32(cd.cellCount, h->nCells + 1, cd.cellStart, nullptr, h->scratch, st);
@@ -509,19 +517,46 @@ int32_t deme_detect_contacts(deme_handle* h) {
     else
         launch_cell_scatter(k, cd, st);
     launch_gather_sorted(k, s, cd, st);
-    const int nxt = h->cur ^ 1;
-    ContactBuf& nb = h->lists[nxt];
+    ContactBuf& nb = h->lists[h->cur ^ 1];
+    CUDA_TRY(h, cudaMemsetAsync(cd.counters, 0, 2 * sizeof(uint32_t), st));
+    if (retry) launch_cnt_init(k, cd, st);
+    launch_pair_find(k, s, cd, h->candCap, st);
+    launch_pair_overflow(k, s, cd, h->candCap, st);
+    TRY(check_launch(h, "contact search"));
+    exclusive_scan_u32(cd.cnt, h->nS + 1, nb.off, h->dTotal, h->scratch, st);
+    CUDA_TRY(h, cudaMemcpyAsync(hCnt + 1, cd.counters, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(h, cudaMemcpyAsync(hCnt, h->dTotal, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    return DEME_OK;
+}
+
+// Writes the new list (n contacts, pool of `pool` pairs) in canonical order into lists[cur ^ 1], on `st`.
+static int32_t cd_assemble(deme_handle* h, const StateView& s, uint32_t n, uint32_t pool, cudaStream_t st) {
+    ContactBuf& nb = h->lists[h->cur ^ 1];
+    TRY(ensure_list(h, nb, n));
+    launch_pair_scatter(h->k, h->cd, nb.view(), pool, nb.cap, st);
+    launch_pair_assemble(h->k, s, h->cd, nb.view(), nb.cap, st);
+    return check_launch(h, "contact assembly");
+}
+
+// History map of the new list against the list in use, remapped history, and the switch to the new list (on dT).
+static int32_t cd_adopt(deme_handle* h, uint32_t n) {
+    ContactBuf& nb = h->lists[h->cur ^ 1];
     ContactBuf& pb = h->lists[h->cur];
+    launch_history(h->k, nb.view(), pb.view(), n, h->nContacts, h->nW > 0, h->st_dt);
+    TRY(check_launch(h, "contact history"));
+    h->cur ^= 1;
+    h->nContacts = n;
+    h->outsValid = false;
+    return DEME_OK;
+}
+
+// Synchronous detection on dT's stream from the current poses (DoStepDynamics with CD due this step).
+static int32_t cd_sync(deme_handle* h) {
+    cudaStream_t st = h->st_dt;
+    StateView s = h->state_view();
     uint32_t n = 0;
     for (int attempt = 0; attempt < 2; attempt++) {
-        CUDA_TRY(h, cudaMemsetAsync(cd.counters, 0, 2 * sizeof(uint32_t), st));
-        if (attempt) launch_cnt_init(k, cd, st);
-        launch_pair_find(k, s, cd, h->candCap, st);
-        launch_pair_overflow(k, s, cd, h->candCap, st);
-        TRY(check_launch(h, "contact search"));
-        exclusive_scan_u32(cd.cnt, h->nS + 1, nb.off, h->dTotal, h->scratch, st);
-        CUDA_TRY(h, cudaMemcpyAsync(h->hTotal + 1, cd.counters, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        CUDA_TRY(h, cudaMemcpyAsync(h->hTotal, h->dTotal, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        TRY(cd_search(h, s, h->analPlaced, st, attempt > 0, h->hTotal));
         CUDA_TRY(h, cudaStreamSynchronize(st));
         n = h->hTotal[0];
         if (h->hTotal[1] <= h->candCap) break;
@@ -532,15 +567,96 @@ int32_t deme_detect_contacts(deme_handle* h) {
         h->err = "contact search: pair list still over capacity after growing";
         return DEME_ERR_OVERFLOW;
     }
-    TRY(ensure_list(h, nb, n));
-    launch_pair_scatter(k, cd, nb.view(), h->hTotal[1], nb.cap, st);
-    launch_pair_assemble(k, s, cd, nb.view(), nb.cap, st);
-    launch_history(k, nb.view(), pb.view(), n, h->nContacts, h->nW > 0, st);
-    TRY(check_launch(h, "contact assembly"));
-    h->cur = nxt;
-    h->nContacts = n;
-    h->outsValid = false;
+    TRY(cd_assemble(h, s, n, h->hTotal[1], st));
+    TRY(cd_adopt(h, n));
     return read_device_errors(h);
+}
+
+static int32_t ensure_async(deme_handle* h) {
+    if (h->kVoxel) return DEME_OK;
+    TRY(dalloc_n(h, &h->kVoxel, std::max(h->nO, 1u)));
+    TRY(dalloc_n(h, &h->kLoc, std::max(h->nO, 1u)));
+    TRY(dalloc_n(h, &h->kQuat, std::max(h->nO, 1u)));
+    TRY(dalloc_n(h, &h->kAnalPlaced, std::max(h->nA, 1u)));
+    CUDA_TRY(h, cudaMallocHost(&h->hCounts, 4 * sizeof(uint32_t)));
+    CUDA_TRY(h, cudaEventCreateWithFlags(&h->evPose, cudaEventDisableTiming));
+    CUDA_TRY(h, cudaEventCreateWithFlags(&h->evCounts, cudaEventDisableTiming));
+    CUDA_TRY(h, cudaEventCreateWithFlags(&h->evListReady, cudaEventDisableTiming));
+    CUDA_TRY(h, cudaEventCreateWithFlags(&h->evListReleased, cudaEventDisableTiming));
+    // nothing has read a list yet: the first search may write lists[cur ^ 1] at once
+    CUDA_TRY(h, cudaEventRecord(h->evListReleased, h->st_dt));
+    return DEME_OK;
+}
+
+// kT's part of an asynchronous detection: snapshot of the poses dT has reached, then the search on st_kt.
+static int32_t cd_start(deme_handle* h) {
+    TRY(ensure_async(h));
+    cudaStream_t kt = h->st_kt;
+    CUDA_TRY(h, cudaEventRecord(h->evPose, h->st_dt));
+    CUDA_TRY(h, cudaStreamWaitEvent(kt, h->evPose, 0));
+    // lists[cur ^ 1] was last read by dT's history map at the previous adoption
+    CUDA_TRY(h, cudaStreamWaitEvent(kt, h->evListReleased, 0));
+    const size_t nO = h->nO;
+    CUDA_TRY(h, cudaMemcpyAsync(h->kVoxel, h->voxel, nO * sizeof(uint64_t), cudaMemcpyDeviceToDevice, kt));
+    CUDA_TRY(h, cudaMemcpyAsync(h->kLoc, h->loc, nO * sizeof(ushort4), cudaMemcpyDeviceToDevice, kt));
+    CUDA_TRY(h, cudaMemcpyAsync(h->kQuat, h->quat, nO * sizeof(float4), cudaMemcpyDeviceToDevice, kt));
+    TRY(cd_search(h, h->kt_view(), h->kAnalPlaced, kt, false, h->hCounts));
+    CUDA_TRY(h, cudaEventRecord(h->evCounts, kt));
+    h->cdPending = true;
+    h->cdAdoptStep = h->steps + h->cdLag;
+    return DEME_OK;
+}
+
+// dT adopts the list kT found: wait for kT's counts, assemble on kT, history map and switch on dT.
+static int32_t cd_finish(deme_handle* h) {
+    if (!h->cdPending) return DEME_OK;
+    h->cdPending = false;
+    cudaStream_t kt = h->st_kt;
+    CUDA_TRY(h, cudaEventSynchronize(h->evCounts));
+    const StateView ks = h->kt_view();
+    if (h->hCounts[1] > h->candCap) {
+        // pool overflow: grow and search the same snapshot again (it is untouched until the next detection)
+        TRY(ensure_cand(h, h->hCounts[1]));
+        TRY(cd_search(h, ks, h->kAnalPlaced, kt, true, h->hCounts));
+        CUDA_TRY(h, cudaStreamSynchronize(kt));
+        if (h->hCounts[1] > h->candCap) {
+            h->err = "contact search: pair list still over capacity after growing";
+            return DEME_ERR_OVERFLOW;
+        }
+    }
+    const uint32_t n = h->hCounts[0];
+    TRY(cd_assemble(h, ks, n, h->hCounts[1], kt));
+    CUDA_TRY(h, cudaEventRecord(h->evListReady, kt));
+    CUDA_TRY(h, cudaStreamWaitEvent(h->st_dt, h->evListReady, 0));
+    TRY(cd_adopt(h, n));
+    CUDA_TRY(h, cudaEventRecord(h->evListReleased, h->st_dt));
+    return DEME_OK;
+}
+
+// A pending asynchronous detection is dropped (its snapshot no longer describes the state).
+static int32_t cd_cancel(deme_handle* h) {
+    if (!h->cdPending) return DEME_OK;
+    h->cdPending = false;
+    CUDA_TRY(h, cudaStreamSynchronize(h->st_kt));
+    return DEME_OK;
+}
+
+int32_t deme_set_async_cd(deme_handle* h, int32_t lag) {
+    if (!h) return DEME_ERR_INVALID;
+    const int32_t f = h->params.cd_update_freq;
+    if (lag < 0 || (lag > 0 && f > 0 && lag > f) || (lag > 1 && f <= 0)) {
+        h->err = "asynchronous detection lag must lie in [0, cd_update_freq] (0 or 1 with detection every step)";
+        return DEME_ERR_INVALID;
+    }
+    TRY(cd_finish(h));
+    h->cdLag = lag;
+    return DEME_OK;
+}
+
+int32_t deme_detect_contacts(deme_handle* h) {
+    if (!h) return DEME_ERR_INVALID;
+    TRY(cd_finish(h));
+    return cd_sync(h);
 }
 
 // ---------------------------------------------------------------------------------------------------- dT ----
@@ -591,7 +707,21 @@ int32_t deme_step(deme_handle* h, int32_t n_steps) {
     if (!h) return DEME_ERR_INVALID;
     for (int32_t i = 0; i < n_steps; i++) {
         const int f = h->params.cd_update_freq;
-        if (f <= 0 || (h->steps % f) == 0) TRY(deme_detect_contacts(h));
+        const bool due = f <= 0 || (h->steps % f) == 0;
+        if (h->cdLag > 0) {
+            // kT/dT on two streams: adopt what kT found cdLag steps ago, then hand kT the poses of this step.  The
+            // first detection of a run is adopted at once, so no step runs without a contact list.
+            if (h->cdPending && h->steps >= h->cdAdoptStep) TRY(cd_finish(h));
+            if (due) {
+                TRY(cd_finish(h));
+                TRY(cd_start(h));
+                if (h->steps == 0 || !h->everDetected) TRY(cd_finish(h));
+                h->everDetected = true;
+            }
+        } else if (due) {
+            TRY(cd_sync(h));
+            h->everDetected = true;
+        }
         TRY(deme_compute_forces(h));
         TRY(deme_integrate(h));
     }
@@ -600,6 +730,7 @@ int32_t deme_step(deme_handle* h, int32_t n_steps) {
 
 int32_t deme_sync(deme_handle* h) {
     if (!h) return DEME_ERR_INVALID;
+    TRY(cd_finish(h));
     CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
     CUDA_TRY(h, cudaStreamSynchronize(h->st_kt));
     return read_device_errors(h);
@@ -646,6 +777,7 @@ int32_t deme_download_state(deme_handle* h, deme_state* o) {
 
 int32_t deme_upload_state(deme_handle* h, const deme_state* s) {
     if (!h || !s) return DEME_ERR_INVALID;
+    TRY(cd_cancel(h));
     const uint32_t n = h->nO;
     CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
     std::vector<ushort4> loc(n);
@@ -721,6 +853,7 @@ int32_t deme_download_contacts(deme_handle* h, deme_contacts* o) {
 
 int32_t deme_upload_contacts(deme_handle* h, const deme_contacts* in) {
     if (!h || !in) return DEME_ERR_INVALID;
+    TRY(cd_cancel(h));
     const uint32_t n = in->n_contacts;
     for (uint32_t i = 0; i < n; i++) {
         const bool ss = in->type[i] == DEME_SPHERE_SPHERE_CONTACT;

@@ -82,6 +82,27 @@ struct deme_handle {
     std::vector<void*> allocs;
     UserForceKernel userForce;  // a compiled force-model string, when one is set
     AdjointTape* adj = nullptr;  // checkpoints of deme_adjoint_record
+    // Asynchronous contact detection (kT on st_kt, dT on st_dt).  With cdLag > 0 a detection due at step k runs on
+    // kT from a snapshot of the owner poses of step k while dT keeps stepping with the current list, and dT adopts
+    // the new list at step k + cdLag.
+    int32_t cdLag = 0;
+    bool cdPending = false;
+    bool everDetected = false;
+    int64_t cdAdoptStep = 0;
+    uint64_t* kVoxel = nullptr;  // kT's snapshot of the owner poses (and families) of the detection step
+    ushort4* kLoc = nullptr;
+    float4* kQuat = nullptr;
+    AnalPlaced* kAnalPlaced = nullptr;  // analytical components placed from that snapshot
+    uint32_t* hCounts = nullptr;        // pinned: total, pool count, device error word, copied at the end of kT's part
+    cudaEvent_t evPose = nullptr, evCounts = nullptr, evListReady = nullptr, evListReleased = nullptr;
+    StateView kt_view() const {
+        StateView s = state_view();
+        s.voxel = kVoxel;
+        s.loc = kLoc;
+        s.quat = kQuat;
+        s.anal = kAnalPlaced;
+        return s;
+    }
 
     StateView state_view() const {
         StateView s;

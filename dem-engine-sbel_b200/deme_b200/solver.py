@@ -229,6 +229,11 @@ class Solver(HandleSolver):
         self.lib.deme_set_streams.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         self._check(self.lib.deme_set_streams(self.h, kt_stream, dt_stream), "set_streams")
 
+    def set_async_cd(self, lag: int):
+        """kT/dT on two streams: detections adopted ``lag`` steps after the poses they were made from (0: in step)."""
+        self.lib.deme_set_async_cd.argtypes = [C.c_void_p, C.c_int32]
+        self._check(self.lib.deme_set_async_cd(self.h, int(lag)), "set_async_cd")
+
     def keep_contact_forces(self, enable: bool = True):
         self.lib.deme_keep_contact_forces.argtypes = [C.c_void_p, C.c_int32]
         self._check(self.lib.deme_keep_contact_forces(self.h, int(enable)), "keep_contact_forces")

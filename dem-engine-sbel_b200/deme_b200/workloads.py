@@ -494,22 +494,36 @@ def batched_settling(specs, dt: float = 1e-5):
     s.SetCDUpdateFreq(1)
     s.SetExpandFactor(0.0)
     built = s.Initialize()
-    built.info.update(workload="batched_settling", n_scenes=len(specs), scenes=ranges, slot=slot, slots_per_axis=per)
+    built.info.update(workload="batched_settling", n_scenes=len(specs), scenes=ranges, slot=slot, slots_per_axis=per,
+                      world=world, bin_size=2.0 * max(sp["r"] for sp in specs))
     return built
 
 
-def single_settling(spec, dt: float = 1e-5):
-    """One scene of ``specs`` alone (for the sequential baseline and parity against the packed run)."""
+def single_settling(spec, dt: float = 1e-5, packed=None, index: int = 0):
+    """One scene of ``specs`` alone (for the sequential baseline and parity against the packed run).
+
+    With ``packed`` (a ``batched_settling`` scene) and the scene's ``index`` in it, the scene is built alone in the
+    packed run's domain, slot and bin size, so that its positions encode on the same voxel grid and its search uses
+    the same cells: the two runs then differ only in the order of float sums."""
     s = SceneBuilder()
-    pos, height = _settling_positions(spec, (0.0, 0.0, 0.0))
-    H = max(height, spec["side"])
-    dom = max(spec["side"], H) + 0.02
-    s.InstructBoxDomainDimension(dom, dom, dom)
+    if packed is None:
+        pos, height = _settling_positions(spec, (0.0, 0.0, 0.0))
+        H = max(height, spec["side"])
+        dom = max(spec["side"], H) + 0.02
+        s.InstructBoxDomainDimension(dom, dom, dom)
+        lbf = (0.01, 0.01, 0.01)
+        bin_size = 2.0 * spec["r"]
+    else:
+        info = packed.info
+        per, slot = info["slots_per_axis"], info["slot"]
+        s.InstructBoxDomainDimension(info["world"], info["world"], info["world"])
+        lbf = (0.01 + (index % per) * slot, 0.01 + ((index // per) % per) * slot, 0.01 + (index // (per * per)) * slot)
+        bin_size = info["bin_size"]
     s.SetCoordSysOrigin("explicit")
-    _add_settling_scene(s, spec, (0.01, 0.01, 0.01))
+    _add_settling_scene(s, spec, lbf)
     s.SetInitTimeStep(dt)
     s.SetGravitationalAcceleration((0, 0, -9.81))
-    s.SetInitBinSize(2.0 * spec["r"])
+    s.SetInitBinSize(bin_size)
     s.SetCDUpdateFreq(1)
     s.SetExpandFactor(0.0)
     return s.Initialize()

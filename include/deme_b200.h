@@ -288,6 +288,16 @@ int32_t deme_set_cell_sort(deme_handle* h, int32_t onesweep);
  * The two workers of the reference are host threads with one stream each (src/core/utils/GpuManager.cpp:8-32). */
 int32_t deme_set_streams(deme_handle* h, void* kT_stream, void* dT_stream);
 
+/* kT and dT as concurrent producer and consumer (the reference's asynchronous kT/dT threads with drift limit
+ * cd_update_freq, src/DEM/dT.cpp:1446-1586, src/DEM/kT.cpp:101-188, src/core/utils/ThreadManager.h:37-94), made
+ * deterministic.  With lag > 0, a detection due at step k runs on the kT stream from a snapshot of the owner poses of
+ * step k while dT keeps stepping with the current list; dT adopts the new list at step k + lag (history remapped from
+ * the list it replaces).  dT therefore uses lists up to lag + cd_update_freq - 1 steps old, which the expand factor
+ * (SetExpandFactor / SetMaxVelocity) must cover, as in the reference.  lag lies in [0, cd_update_freq] (0 or 1 when
+ * detection runs every step); 0 (the default) detects synchronously.  The first detection of a run is adopted at
+ * once.  Uploading state or contacts drops a pending detection; deme_detect_contacts and deme_sync adopt it first. */
+int32_t deme_set_async_cd(deme_handle* h, int32_t lag);
+
 /* Change one family's prescription between steps (the constant-valued form of SetFamilyPrescribedLinVel /
  * SetFamilyPrescribedAngVel / SetFamilyFixed, src/DEM/APIPublic.cpp:145-252, which the reference can only change by
  * re-jitifying).  The value is staged through pinned memory and applied in stream order. */
