@@ -1,0 +1,103 @@
+"""Bulk statistics of a granular state, for comparing long runs whose individual trajectories diverge (contact
+chaos makes two correct solvers part ways after a few hundred steps while the bulk behaviour agrees).
+
+* kinetic energy: translational plus rotational (principal moments in the owner frame, the frame the angular
+  velocity is stored in, as the reference's integrator uses it: src/kernel/DEMIntegrationKernels.cu);
+* packing fraction: sphere volume inside a horizontal slab of a box, counting the part of each sphere that lies in
+  the slab (spherical caps);
+* heap angle: slope of the free surface of a heap, from the highest sphere tops in rings around its axis.
+
+All take a state dict as the solvers' ``state()`` returns it and the built scene it belongs to; coordinates are the
+world frame of the scene builder.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+
+def world_positions(built, state) -> np.ndarray:
+    """Owner positions in the world frame (decoded from voxel and sub-voxel position, plus the domain's lower
+    corner)."""
+    return built.decode_positions(state, kernel_literals=False) + np.asarray(list(built.params.lbf), np.float64)
+
+
+def _owner_sphere_radius(built) -> np.ndarray:
+    """Radius of each single-sphere owner (owners with one sphere centred on them)."""
+    a = built.arrays
+    owner = np.asarray(a["sphere_owner"], np.int64)
+    r = np.zeros(built.counts["o"])
+    r[owner] = np.asarray(a["radius"], np.float64)
+    return r
+
+
+def kinetic_energy(built, state) -> float:
+    """Translational plus rotational kinetic energy of the clump owners (analytical owners carry no mass here)."""
+    a = built.arrays
+    n = int(built.info.get("n_clumps", built.counts["o"]))
+    m = np.asarray(a["mass"], np.float64)[:n]
+    v = np.stack([state["vX"], state["vY"], state["vZ"]], 1).astype(np.float64)[:n]
+    w = np.stack([state["omgX"], state["omgY"], state["omgZ"]], 1).astype(np.float64)[:n]
+    moi = np.stack([a["mmiXX"], a["mmiYY"], a["mmiZZ"]], 1).astype(np.float64)[:n]
+    return float(0.5 * np.sum(m * np.sum(v * v, 1)) + 0.5 * np.sum(moi * w * w))
+
+
+def _cap_volume(r: np.ndarray, h: np.ndarray) -> np.ndarray:
+    """Volume of the part of a sphere of radius r below a plane at height h above its lowest point (0 <= h <= 2r)."""
+    h = np.clip(h, 0.0, 2.0 * r)
+    return math.pi * h * h * (3.0 * r - h) / 3.0
+
+
+def packing_fraction(built, state, xy_lo, xy_hi, z_lo: float, z_hi: float) -> float:
+    """Solid fraction of the box [xy_lo, xy_hi] x [z_lo, z_hi] (spheres cut by the horizontal faces count in part;
+    the vertical faces are taken to be walls that no sphere crosses)."""
+    pos = world_positions(built, state)
+    r = _owner_sphere_radius(built)[:len(pos)]
+    inside = ((pos[:, 0] >= xy_lo[0]) & (pos[:, 0] <= xy_hi[0]) & (pos[:, 1] >= xy_lo[1]) & (pos[:, 1] <= xy_hi[1])
+              & (r > 0))
+    z, rr = pos[inside, 2], r[inside]
+    below_hi = _cap_volume(rr, z_hi - (z - rr))
+    below_lo = _cap_volume(rr, z_lo - (z - rr))
+    vol = np.sum(below_hi - below_lo)
+    return float(vol / ((xy_hi[0] - xy_lo[0]) * (xy_hi[1] - xy_lo[1]) * (z_hi - z_lo)))
+
+
+def bed_height(built, state, z_floor: float, quantile: float = 0.95) -> float:
+    """Height above the floor below which ``quantile`` of the sphere tops lie."""
+    pos = world_positions(built, state)
+    r = _owner_sphere_radius(built)[:len(pos)]
+    ok = r > 0
+    return float(np.quantile(pos[ok, 2] + r[ok] - z_floor, quantile))
+
+
+def heap_profile(built, state, axis_xy, z_floor: float, ring: float, n_rings: int = 40):
+    """Free-surface height of a heap: for rings of width ``ring`` around the axis, the 90th percentile of the sphere
+    tops in the ring (rings holding fewer than 8 spheres are left out).  Returns (ring centres, heights)."""
+    pos = world_positions(built, state)
+    r = _owner_sphere_radius(built)[:len(pos)]
+    ok = r > 0
+    rho = np.hypot(pos[ok, 0] - axis_xy[0], pos[ok, 1] - axis_xy[1])
+    top = pos[ok, 2] + r[ok] - z_floor
+    k = np.floor(rho / ring).astype(np.int64)
+    xs, hs = [], []
+    for i in range(n_rings):
+        sel = k == i
+        if sel.sum() >= 8:
+            xs.append((i + 0.5) * ring)
+            hs.append(float(np.quantile(top[sel], 0.9)))
+    return np.asarray(xs), np.asarray(hs)
+
+
+def heap_angle(built, state, axis_xy, z_floor: float, ring: float) -> float:
+    """Angle of repose in degrees: least-squares slope of the free surface between 20 % and 80 % of the heap's
+    height (the flat summit and the thin toe excluded)."""
+    xs, hs = heap_profile(built, state, axis_xy, z_floor, ring)
+    if len(xs) < 3:
+        return float("nan")
+    top = hs.max()
+    sel = (hs <= 0.8 * top) & (hs >= 0.2 * top)
+    if sel.sum() < 3:
+        sel = np.ones_like(hs, bool)
+    slope = np.polyfit(xs[sel], hs[sel], 1)[0]
+    return float(math.degrees(math.atan(-slope)))

@@ -360,11 +360,14 @@ def sphere_pile(n: int = 60, seed: int = 3, h: float = 2e-5, spread: float = 5.2
 
 
 def column_collapse(n: int = 20000, r_range=(2e-3, 3e-3), rho: float = 2500.0, n_classes: int = 32, seed: int = 6,
-                    dt: float = 1e-5, aspect: float = 3.0):
+                    dt: float = 1e-5, aspect: float = 3.0, domain_widths: float = 4.0, mu: float = 0.5,
+                    Crr: float = 0.02):
     """Column collapse for the adjoint: n single spheres (radii uniform in r_range, grouped into n_classes sphere
     types) on a jittered square lattice of pitch 2 r_max (no overlaps) forming a column height:width = aspect over
     a floor plane, released from rest.  20,000 spheres of 2-3 mm do not fit the stated 0.05 x 0.05 x 0.15 m column,
-    so the cross-section is widened (recorded in ``info``).  Contact margin 0, contact detection every step."""
+    so the cross-section is widened (recorded in ``info``).  Contact margin 0, contact detection every step.  The
+    cubic domain spans ``domain_widths`` column widths (or 1.3 column heights); a run long enough for the heap to
+    spread needs more than the default 4, since spheres that leave the domain are lost."""
     rng = np.random.default_rng(seed)
     r = rng.uniform(r_range[0], r_range[1], n)
     edges = np.linspace(r_range[0], r_range[1], n_classes + 1)
@@ -384,11 +387,11 @@ def column_collapse(n: int = 20000, r_range=(2e-3, 3e-3), rho: float = 2500.0, n
     P += d
     height = layers * a
     s = SceneBuilder()
-    box = max(4 * w, 1.3 * height) + 0.05
+    box = max(domain_widths * w, 1.3 * height) + 0.05
     s.InstructBoxDomainDimension(box, box, box)
     s.SetCoordSysOrigin("center")
     z_floor = -box / 2 + 0.02
-    mat = s.LoadMaterial({"E": 1e7, "nu": 0.3, "CoR": 0.5, "mu": 0.5, "Crr": 0.02})
+    mat = s.LoadMaterial({"E": 1e7, "nu": 0.3, "CoR": 0.5, "mu": mu, "Crr": Crr})
     types = [s.LoadSphereType(float(f32(sphere_mass(float(rc), rho))), float(rc), mat) for rc in r_cls]
     s.AddClumps([types[c] for c in cls], (P + np.array([0.0, 0.0, z_floor])).astype(f32))
     s.AddBCPlane((0, 0, z_floor), (0, 0, 1), mat)
