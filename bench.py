@@ -288,6 +288,37 @@ def hopper_measure(args, stream):
     return out
 
 
+def small_scene_measure(args, stream):
+    """The small settling box (10,000 spheres of 5 mm in a 0.2 x 0.2 x 0.4 m box of six planes, dt 1e-5, CD every
+    step): steps launched one by one, and whole steps replayed from CUDA graphs.  Device time with CUDA events after
+    1,000 untimed steps."""
+    import torch
+    from deme_b200 import Solver, workloads
+    built = workloads.settling_box(n=10000)
+    out = {"workload": "settling box: 10,000 spheres r 5 mm, 0.2 x 0.2 x 0.4 m box of 6 planes, dt 1e-5, CD every step",
+           "n_spheres": built.n_spheres, "steps": args.small_steps, "warmup": 1000}
+    for graph in (False, True):
+        s = Solver(built)
+        s.lib.deme_set_streams(s.h, C.c_void_p(stream.cuda_stream), C.c_void_p(stream.cuda_stream))
+        if graph:
+            s.set_graph(True)
+        s.step(1000)
+        s.sync()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.step(args.small_steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out["graph" if graph else "step_by_step"] = {
+            "us_per_step": ms * 1e3 / args.small_steps,
+            "value": built.n_spheres * args.small_steps / (ms / 1e3) / 1e6, "unit": UNIT,
+            "n_contacts": s.num_contacts(), "graph_windows_replayed": s.graph_stats()[0]}
+        s.close()
+    return out
+
+
 def shell_drum_measure(args, stream):
     """This build on the same shell drum the reference's GPU kernels are timed on (device time, CUDA events)."""
     import torch
@@ -345,6 +376,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-shell", action="store_true", help="skip the shell-drum run (the reference-kernel comparison)")
     ap.add_argument("--no-hopper", action="store_true", help="skip the hopper run (detection every 5 steps, two streams)")
+    ap.add_argument("--no-small", action="store_true", help="skip the small-scene run (step by step against graphs)")
+    ap.add_argument("--autotune", type=int, default=1, help="1: pick the search shape with deme_autotune (untimed)")
+    ap.add_argument("--small-steps", type=int, default=5000)
     ap.add_argument("--hopper-spheres", type=int, default=4_000_000)
     ap.add_argument("--hopper-steps", type=int, default=500)
     ap.add_argument("--hopper-settle", type=int, default=40000, help="untimed settling steps of the hopper bed")
@@ -432,6 +466,11 @@ def main():
         np.savez(args.save_state, **{"st_" + k: v for k, v in st.items() if not k.startswith("a")},
                  **{"c_" + k: c[k] for k in ("idA", "idB", "type", "wildcards")})
 
+    tuning = None
+    if args.autotune:
+        # untimed: time every search shape on a few steps from the prepared state, keep the fastest, restore the state
+        tuning = s.autotune(steps_per_trial=5)
+
     # ---- warm-up (the clock sampler starts here so it has samples when the timed region is short) ----
     sampler = ClockSampler(local_rank)
     sampler.start()
@@ -513,6 +552,7 @@ def main():
         cpu = cpu_baseline_sample(args)
     shell = shell_drum_measure(args, stream) if (rank == 0 and not args.no_shell) else None
     hopper = hopper_measure(args, stream) if (rank == 0 and not args.no_hopper) else None
+    small = small_scene_measure(args, stream) if (rank == 0 and not args.no_small) else None
     adj = None if args.no_adjoint else adjoint_measure(args, stream)
     batched = None if args.no_batched else batched_measure(args, stream)
 
@@ -530,11 +570,12 @@ def main():
                        "initial_state": f"HCP lattice of non-overlapping clumps, settled {args.settle_steps} steps at "
                                         f"dt {args.settle_dt:g} + {args.calm_steps} steps at dt {dt_work:g} "
                                         f"(untimed, {prep_s:.1f} s)",
-                       "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+                       "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}",
+                       "search_shape": tuning},
             "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": C.sizeof(capi.FamilyPrescription),
                     "d2h_bytes_per_step": 8},
-            "gpu_launches": int(launches), "clocks": clocks, "shell_drum": shell, "hopper": hopper, "adjoint": adj, "batched": batched,
+            "gpu_launches": int(launches), "clocks": clocks, "shell_drum": shell, "hopper": hopper, "small_scene": small, "adjoint": adj, "batched": batched,
         }
         print(json.dumps(line), flush=True)
     s.close()

@@ -27,21 +27,7 @@
 
 using namespace deme_b200;
 
-struct Checkpoint {
-    uint64_t* voxel = nullptr;
-    ushort4* loc = nullptr;
-    float4* quat = nullptr;
-    float4* vel = nullptr;
-    float4* omg = nullptr;
-    uint32_t n = 0, cap = 0;
-    uint32_t* idA = nullptr;
-    uint32_t* idB = nullptr;
-    uint8_t* type = nullptr;
-    float4* hist = nullptr;
-    uint32_t* off = nullptr;
-    int64_t steps = 0;
-    double t = 0.0;
-};
+// struct Checkpoint: handle.cuh
 
 struct AdjointTape {
     int K = 0;
@@ -303,7 +289,6 @@ __global__ void k_adj_rekey(uint32_t n, const uint32_t* A, const uint32_t* B, co
 }  // namespace
 
 // ------------------------------------------------------------------------------------------------------ host ----
-namespace {
 
 int32_t alloc_checkpoint(deme_handle* h, Checkpoint& c, uint32_t nContacts) {
     if (!c.voxel) {
@@ -340,6 +325,7 @@ void free_checkpoint(deme_handle* h, Checkpoint& c) {
 }
 
 int32_t save_checkpoint(deme_handle* h, Checkpoint& c) {
+    TRY(refresh_count(h));
     const uint32_t n = h->nContacts;
     TRY(alloc_checkpoint(h, c, n));
     cudaStream_t st = h->st_dt;
@@ -378,12 +364,17 @@ int32_t restore_checkpoint(deme_handle* h, const Checkpoint& c) {
         CUDA_TRY(h, cudaMemcpyAsync(L.hist, c.hist, c.n * sizeof(float4), cudaMemcpyDeviceToDevice, st));
     }
     CUDA_TRY(h, cudaMemcpyAsync(L.off, c.off, ((size_t)h->nS + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(h, cudaMemcpyAsync(L.dN, &c.n, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(h, cudaStreamSynchronize(st));
     h->nContacts = c.n;
+    h->countStale = false;
     h->steps = c.steps;
     h->t = c.t;
     h->outsValid = false;
     return DEME_OK;
 }
+
+namespace {
 
 // The scenes the adjoint covers: single spheres (relative position 0, isotropic inertia) with plane walls, the
 // built-in model, Extended Taylor integration, contact detection every step, no prescribed sphere families.

@@ -19,6 +19,7 @@
 #include "handle.cuh"
 #include "kernels.cuh"
 #include "primitives.cuh"
+#include "profiler.cuh"
 
 int32_t dalloc(deme_handle* h, void** p, size_t bytes) {
     if (bytes == 0) bytes = 16;
@@ -98,6 +99,45 @@ int32_t ensure_list(deme_handle* h, ContactBuf& b, uint32_t n) {
     return DEME_OK;
 }
 
+// Grows a list that is in use, keeping its contents (ids, history, mapping).
+static int32_t ensure_list_keep(deme_handle* h, ContactBuf& b, uint32_t n, uint32_t used, cudaStream_t st) {
+    if (n <= b.cap) return DEME_OK;
+    ContactBuf old = b;
+    ContactBuf grown = b;
+    const uint32_t cap = std::max<uint32_t>(1024u, (uint32_t)std::min<uint64_t>(0xFFFFFFF0ull, (uint64_t)n * 5 / 4 + 64));
+    TRY(dalloc_n(h, &grown.idA, cap));
+    TRY(dalloc_n(h, &grown.idB, cap));
+    TRY(dalloc_n(h, &grown.type, cap));
+    TRY(dalloc_n(h, &grown.hist, cap));
+    TRY(dalloc_n(h, &grown.mapping, cap));
+    grown.cap = cap;
+    if (used) {
+        CUDA_TRY(h, cudaMemcpyAsync(grown.idA, old.idA, used * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+        CUDA_TRY(h, cudaMemcpyAsync(grown.idB, old.idB, used * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+        CUDA_TRY(h, cudaMemcpyAsync(grown.type, old.type, used * sizeof(uint8_t), cudaMemcpyDeviceToDevice, st));
+        CUDA_TRY(h, cudaMemcpyAsync(grown.hist, old.hist, used * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+        CUDA_TRY(h, cudaMemcpyAsync(grown.mapping, old.mapping, used * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    }
+    CUDA_TRY(h, cudaStreamSynchronize(st));
+    dfree(h, old.idA);
+    dfree(h, old.idB);
+    dfree(h, old.type);
+    dfree(h, old.hist);
+    dfree(h, old.mapping);
+    b = grown;
+    return DEME_OK;
+}
+
+// The count of the list in use, read back after a graph replay produced it on the device.
+int32_t refresh_count(deme_handle* h) {
+    if (!h->countStale) return DEME_OK;
+    CUDA_TRY(h, cudaMemcpyAsync(h->hTotal + 3, h->lists[h->cur].dN, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->st_dt));
+    CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
+    h->nContacts = h->hTotal[3];
+    h->countStale = false;
+    return DEME_OK;
+}
+
 static int32_t ensure_cand(deme_handle* h, uint32_t n) {
     if (n <= h->candCap) return DEME_OK;
     const uint32_t cap = std::max<uint32_t>(1024u, (uint32_t)std::min<uint64_t>(0xFFFFFFF0ull, (uint64_t)n * 5 / 4 + 64));
@@ -147,6 +187,31 @@ const char* deme_status_string(int32_t s) {
 }
 
 const char* deme_get_error(deme_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+// Search cells: cubes of edge cell_factor x max(bin size, largest expanded diameter), over the user's domain (or
+// the voxel world), coarsened while there would be more than 2^26 of them.  Factor 1 gives the most cells, which
+// the cell arrays are sized for; any factor >= 1 finds the same pairs.
+static void set_cell_grid(deme_handle* h, double cell_factor) {
+    const deme_sim_params* p = &h->params;
+    SimConsts& k = h->k;
+    const double world[3] = {p->voxel_size * std::ldexp(1.0, p->nvXp2), p->voxel_size * std::ldexp(1.0, p->nvYp2),
+                             p->voxel_size * std::ldexp(1.0, p->nvZp2)};
+    double dom[3];
+    for (int a = 0; a < 3; a++) dom[a] = p->domain[a] > 0.f ? (double)p->domain[a] : world[a];
+    double cs = std::max(p->bin_size, 2.0 * (double)k.r_max_cd) * (1.0 + 1e-6) * std::max(cell_factor, 1.0);
+    if (!(cs > 0.0)) cs = 1.0;
+    auto ncell = [&](double c, double d) { return (uint64_t)std::ceil(d / c) + 1; };
+    while (ncell(cs, dom[0]) * ncell(cs, dom[1]) * ncell(cs, dom[2]) > (1ull << 26)) cs *= 1.25;
+    k.cell_size = cs;
+    k.inv_cell = 1.0 / cs;
+    k.gx = (uint32_t)ncell(cs, dom[0]);
+    k.gy = (uint32_t)ncell(cs, dom[1]);
+    k.gz = (uint32_t)ncell(cs, dom[2]);
+    h->nCells = k.gx * k.gy * k.gz;
+    h->cellBits = 1;
+    while ((1ull << h->cellBits) < h->nCells) h->cellBits++;
+    h->cellFactor = (float)std::max(cell_factor, 1.0);
+}
 
 static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_scene* s) {
     int ndev = 0;
@@ -240,20 +305,7 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
                              p->voxel_size * std::ldexp(1.0, p->nvZp2)};
     const double wmax = std::max(world[0], std::max(world[1], world[2]));
     k.prefilter_abs = (float)(4e-7 * wmax + 1e-9);
-    double dom[3];
-    for (int a = 0; a < 3; a++) dom[a] = p->domain[a] > 0.f ? (double)p->domain[a] : world[a];
-    double cs = std::max(p->bin_size, 2.0 * (double)rmax) * (1.0 + 1e-6);
-    if (!(cs > 0.0)) cs = 1.0;
-    auto ncell = [&](double c, double d) { return (uint64_t)std::ceil(d / c) + 1; };
-    while (ncell(cs, dom[0]) * ncell(cs, dom[1]) * ncell(cs, dom[2]) > (1ull << 26)) cs *= 1.25;
-    k.cell_size = cs;
-    k.inv_cell = 1.0 / cs;
-    k.gx = (uint32_t)ncell(cs, dom[0]);
-    k.gy = (uint32_t)ncell(cs, dom[1]);
-    k.gz = (uint32_t)ncell(cs, dom[2]);
-    h->nCells = k.gx * k.gy * k.gz;
-    h->cellBits = 1;
-    while ((1ull << h->cellBits) < h->nCells) h->cellBits++;
+    set_cell_grid(h, 1.0);
 
     // ---- device arrays ----
     TRY(dalloc_n(h, &h->voxel, nO));
@@ -407,6 +459,8 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
     for (int b = 0; b < 2; b++) {
         TRY(dalloc_n(h, &h->lists[b].off, (size_t)nS + 1));
         CUDA_TRY(h, cudaMemset(h->lists[b].off, 0, ((size_t)nS + 1) * sizeof(uint32_t)));
+        TRY(dalloc_n(h, &h->lists[b].dN, 1));
+        CUDA_TRY(h, cudaMemset(h->lists[b].dN, 0, sizeof(uint32_t)));
         TRY(ensure_list(h, h->lists[b], std::max<uint32_t>(1024u, 4u * nS)));
     }
     TRY(ensure_scratch(h, std::max(radix_sort_scratch_bytes(nS), scan_scratch_bytes(std::max(h->nCells + 1, nS + 1)))));
@@ -452,6 +506,8 @@ void deme_destroy(deme_handle* h) {
     if (h->hCounts) cudaFreeHost(h->hCounts);
     for (cudaEvent_t e : {h->evPose, h->evCounts, h->evListReady, h->evListReleased})
         if (e) cudaEventDestroy(e);
+    for (cudaGraphExec_t g : h->graphExec)
+        if (g) cudaGraphExecDestroy(g);
     if (h->own_dt) cudaStreamDestroy(h->own_dt);
     if (h->own_kt) cudaStreamDestroy(h->own_kt);
     release_user_force_model(h->userForce);
@@ -501,9 +557,9 @@ int32_t deme_keep_contact_forces(deme_handle* h, int32_t enable) {
 }
 
 // ---------------------------------------------------------------------------------------------------- kT ----
-// Contact search up to the per-sphere offsets of the new list (into lists[cur ^ 1].off), for the poses in `s`, with
-// the analytical components placed into `anal`.  The pair total, the pool count and its overflow counter are copied
-// to `hCnt` (pinned) at the end, on `st`; nothing here waits for the device.
+// Contact search up to the per-sphere offsets of the new list (into lists[cur ^ 1].off, its count into .dN), for the
+// poses in `s`, with the analytical components placed into `anal`.  The pair total, the pool count and its overflow
+// counter are copied to `hCnt` (pinned, unless null) at the end, on `st`; nothing here waits for the device.
 static int32_t cd_search(deme_handle* h, const StateView& s, AnalPlaced* anal, cudaStream_t st, bool retry,
                          uint32_t* hCnt) {
     const SimConsts& k = h->k;
@@ -520,20 +576,24 @@ static int32_t cd_search(deme_handle* h, const StateView& s, AnalPlaced* anal, c
     ContactBuf& nb = h->lists[h->cur ^ 1];
     CUDA_TRY(h, cudaMemsetAsync(cd.counters, 0, 2 * sizeof(uint32_t), st));
     if (retry) launch_cnt_init(k, cd, st);
-    launch_pair_find(k, s, cd, h->candCap, st);
+    launch_pair_find(k, s, cd, h->candCap, h->findShape, st);
     launch_pair_overflow(k, s, cd, h->candCap, st);
     TRY(check_launch(h, "contact search"));
-    exclusive_scan_u32(cd.cnt, h->nS + 1, nb.off, h->dTotal, h->scratch, st);
-    CUDA_TRY(h, cudaMemcpyAsync(hCnt + 1, cd.counters, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(h, cudaMemcpyAsync(hCnt, h->dTotal, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    exclusive_scan_u32(cd.cnt, h->nS + 1, nb.off, nb.dN, h->scratch, st);
+    if (hCnt) {
+        CUDA_TRY(h, cudaMemcpyAsync(hCnt + 1, cd.counters, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(h, cudaMemcpyAsync(hCnt, nb.dN, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    }
     return DEME_OK;
 }
 
-// Writes the new list (n contacts, pool of `pool` pairs) in canonical order into lists[cur ^ 1], on `st`.
+// Writes the new list (n contacts, pool of `pool` pairs) in canonical order into lists[cur ^ 1], on `st`.  While a
+// graph is recorded the counts are unknown: n and pool are the capacities, and the kernels read the counts on the
+// device.
 static int32_t cd_assemble(deme_handle* h, const StateView& s, uint32_t n, uint32_t pool, cudaStream_t st) {
     ContactBuf& nb = h->lists[h->cur ^ 1];
-    TRY(ensure_list(h, nb, n));
-    launch_pair_scatter(h->k, h->cd, nb.view(), pool, nb.cap, st);
+    if (!h->capturing) TRY(ensure_list(h, nb, n));
+    launch_pair_scatter(h->k, h->cd, nb.view(), pool, nb.cap, h->candCap, st);
     launch_pair_assemble(h->k, s, h->cd, nb.view(), nb.cap, st);
     return check_launch(h, "contact assembly");
 }
@@ -542,7 +602,8 @@ static int32_t cd_assemble(deme_handle* h, const StateView& s, uint32_t n, uint3
 static int32_t cd_adopt(deme_handle* h, uint32_t n) {
     ContactBuf& nb = h->lists[h->cur ^ 1];
     ContactBuf& pb = h->lists[h->cur];
-    launch_history(h->k, nb.view(), pb.view(), n, h->nContacts, h->nW > 0, h->st_dt);
+    launch_history(h->k, nb.view(), pb.view(), h->capturing ? nb.cap : n, h->capturing ? pb.cap : h->nContacts,
+                   h->nW > 0, h->st_dt);
     TRY(check_launch(h, "contact history"));
     h->cur ^= 1;
     h->nContacts = n;
@@ -554,6 +615,13 @@ static int32_t cd_adopt(deme_handle* h, uint32_t n) {
 static int32_t cd_sync(deme_handle* h) {
     cudaStream_t st = h->st_dt;
     StateView s = h->state_view();
+    if (h->capturing) {
+        // recorded into a graph: no host read; launches cover the capacities, kernels read the counts
+        TRY(cd_search(h, s, h->analPlaced, st, false, nullptr));
+        TRY(cd_assemble(h, s, h->lists[h->cur ^ 1].cap, h->candCap, st));
+        return cd_adopt(h, h->lists[h->cur ^ 1].cap);
+    }
+    TRY(refresh_count(h));
     uint32_t n = 0;
     for (int attempt = 0; attempt < 2; attempt++) {
         TRY(cd_search(h, s, h->analPlaced, st, attempt > 0, h->hTotal));
@@ -670,14 +738,21 @@ int32_t deme_compute_forces(deme_handle* h) {
     CUDA_TRY(h, cudaMemsetAsync(h->acc, 0, h->nO * sizeof(float4), st));
     CUDA_TRY(h, cudaMemsetAsync(h->alpha, 0, h->nO * sizeof(float4), st));
     const ContactBuf& c = h->lists[h->cur];
+    // while a graph is recorded the count is unknown: the launch covers the list's capacity
+    if (!h->capturing) TRY(refresh_count(h));
+    const uint32_t nL = h->capturing ? c.cap : h->nContacts;
     const ContactOutputs* out = nullptr;
     if (h->keepOutputs) {
-        TRY(ensure_outputs(h, h->nContacts));
+        if (!h->capturing) TRY(ensure_outputs(h, nL));
         out = &h->outs;
     }
     AnalAccum aa{nullptr, h->nClumps, h->nO - h->nClumps, h->nO - h->nClumps > 64};
     if (aa.nAO && !aa.direct) {
-        const size_t need = (size_t)force_blocks(std::max(h->nContacts, 1u)) * 6u * aa.nAO;
+        const size_t need = (size_t)force_blocks(std::max(nL, 1u)) * 6u * aa.nAO;
+        if (need > h->analPartialCap && h->capturing) {
+            h->err = "graph recording: wall partials not sized for the list capacity";
+            return DEME_ERR_STATE;
+        }
         if (need > h->analPartialCap) {
             dfree(h, h->analPartial);
             h->analPartial = nullptr;
@@ -687,7 +762,7 @@ int32_t deme_compute_forces(deme_handle* h) {
         }
         aa.partial = h->analPartial;
     }
-    launch_force(k, s, c.view(), h->nContacts, h->nW > 0, out, aa, h->userForce.lib ? &h->userForce : nullptr, st);
+    launch_force(k, s, c.view(), nL, h->nW > 0, out, aa, h->userForce.lib ? &h->userForce : nullptr, st);
     TRY(check_launch(h, "force"));
     h->outsValid = out != nullptr;
     return DEME_OK;
@@ -703,27 +778,280 @@ int32_t deme_integrate(deme_handle* h) {
     return DEME_OK;
 }
 
-int32_t deme_step(deme_handle* h, int32_t n_steps) {
-    if (!h) return DEME_ERR_INVALID;
-    for (int32_t i = 0; i < n_steps; i++) {
-        const int f = h->params.cd_update_freq;
-        const bool due = f <= 0 || (h->steps % f) == 0;
-        if (h->cdLag > 0) {
-            // kT/dT on two streams: adopt what kT found cdLag steps ago, then hand kT the poses of this step.  The
-            // first detection of a run is adopted at once, so no step runs without a contact list.
-            if (h->cdPending && h->steps >= h->cdAdoptStep) TRY(cd_finish(h));
-            if (due) {
-                TRY(cd_finish(h));
-                TRY(cd_start(h));
-                if (h->steps == 0 || !h->everDetected) TRY(cd_finish(h));
-                h->everDetected = true;
-            }
-        } else if (due) {
-            TRY(cd_sync(h));
+// One step launched function by function (DoStepDynamics).
+static int32_t step_plain(deme_handle* h) {
+    const int f = h->params.cd_update_freq;
+    const bool due = f <= 0 || (h->steps % f) == 0;
+    if (h->cdLag > 0) {
+        // kT/dT on two streams: adopt what kT found cdLag steps ago, then hand kT the poses of this step.  The
+        // first detection of a run is adopted at once, so no step runs without a contact list.
+        if (h->cdPending && h->steps >= h->cdAdoptStep) TRY(cd_finish(h));
+        if (due) {
+            TRY(cd_finish(h));
+            TRY(cd_start(h));
+            if (h->steps == 0 || !h->everDetected) TRY(cd_finish(h));
             h->everDetected = true;
         }
-        TRY(deme_compute_forces(h));
-        TRY(deme_integrate(h));
+    } else if (due) {
+        TRY(cd_sync(h));
+        h->everDetected = true;
+    }
+    TRY(deme_compute_forces(h));
+    return deme_integrate(h);
+}
+
+// ------------------------------------------------------------------------------------------ graph replay ----
+// With deme_set_graph, a window of cd_update_freq steps (a detection, then forces and integration each step) is
+// recorded once into a CUDA graph and replayed.  Nothing in a window reads the device from the host: the launches
+// cover the lists' capacities and the kernels read the counts the scans left on the device.  The capacities are
+// fixed before recording with headroom; a window whose lists or pair pool outgrow them sets the device error word,
+// and the batch of windows is then rolled back to a checkpoint and redone step by step (which grows the buffers).
+
+static std::vector<uint8_t> graph_key(const deme_handle* h) {
+    std::vector<uint8_t> key;
+    auto put = [&](const void* p, size_t n) {
+        const uint8_t* b = static_cast<const uint8_t*>(p);
+        key.insert(key.end(), b, b + n);
+    };
+    put(&h->k, sizeof(h->k));
+    for (int b = 0; b < 2; b++) {
+        const ContactView v = h->lists[b].view();
+        put(&v, sizeof(v));
+        put(&h->lists[b].cap, sizeof(uint32_t));
+    }
+    put(&h->cd, sizeof(h->cd));
+    put(&h->candCap, sizeof(h->candCap));
+    put(&h->st_dt, sizeof(h->st_dt));
+    put(&h->keepOutputs, sizeof(h->keepOutputs));
+    put(&h->outs, sizeof(h->outs));
+    put(&h->analPartial, sizeof(h->analPartial));
+    put(&h->analPartialCap, sizeof(h->analPartialCap));
+    put(&h->analPlaced, sizeof(h->analPlaced));
+    put(&h->scratch, sizeof(h->scratch));
+    put(&h->useOnesweep, sizeof(h->useOnesweep));
+    put(&h->nW, sizeof(h->nW));
+    const void* lib = h->userForce.lib;
+    put(&lib, sizeof(lib));
+    put(&h->params.cd_update_freq, sizeof(h->params.cd_update_freq));
+    put(&h->findShape, sizeof(h->findShape));
+    return key;
+}
+
+// Capacities a window needs, fixed before recording: both lists and the pair pool at 1.5 times the current count
+// (at least twice the sphere count), per-contact outputs and wall partials for the list capacity.
+static int32_t graph_prepare(deme_handle* h) {
+    TRY(refresh_count(h));
+    const uint32_t n = h->nContacts;
+    const uint64_t want64 = std::max<uint64_t>((uint64_t)n + n / 2 + 4096u, 2ull * h->nS);
+    const uint32_t want = (uint32_t)std::min<uint64_t>(want64, 0xF0000000ull);
+    TRY(ensure_list_keep(h, h->lists[h->cur], want, n, h->st_dt));
+    TRY(ensure_list(h, h->lists[h->cur ^ 1], want));
+    TRY(ensure_cand(h, std::max<uint32_t>(want, h->hTotal[1] + h->hTotal[1] / 2)));
+    const uint32_t cap = std::max(h->lists[0].cap, h->lists[1].cap);
+    if (h->keepOutputs) TRY(ensure_outputs(h, cap));
+    const uint32_t nAO = h->nO - h->nClumps;
+    if (nAO && nAO <= 64) {
+        const size_t need = (size_t)force_blocks(cap) * 6u * nAO;
+        if (need > h->analPartialCap) {
+            dfree(h, h->analPartial);
+            h->analPartial = nullptr;
+            h->analPartialCap = 0;
+            TRY(dalloc_n(h, &h->analPartial, need + need / 4 + 64));
+            h->analPartialCap = need + need / 4 + 64;
+        }
+    }
+    return DEME_OK;
+}
+
+static int32_t graph_capture(deme_handle* h, int p) {
+    const int f = std::max(1, h->params.cd_update_freq);
+    // the host's bookkeeping is put back after recording: the replays do the work
+    const int cur0 = h->cur;
+    const uint32_t n0 = h->nContacts;
+    const int64_t steps0 = h->steps;
+    const double t0 = h->t;
+    const bool outs0 = h->outsValid, stale0 = h->countStale;
+    CUDA_TRY(h, cudaStreamBeginCapture(h->st_dt, cudaStreamCaptureModeThreadLocal));
+    h->capturing = true;
+    int32_t st = DEME_OK;
+    for (int i = 0; i < f && st == DEME_OK; i++) {
+        if (i == 0) st = cd_sync(h);
+        if (st == DEME_OK) st = deme_compute_forces(h);
+        if (st == DEME_OK) st = deme_integrate(h);
+    }
+    h->capturing = false;
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(h->st_dt, &g);
+    h->cur = cur0;
+    h->nContacts = n0;
+    h->steps = steps0;
+    h->t = t0;
+    h->outsValid = outs0;
+    h->countStale = stale0;
+    if (st != DEME_OK || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        if (st == DEME_OK) h->err = std::string("graph recording: ") + cudaGetErrorString(e);
+        return st != DEME_OK ? st : DEME_ERR_CUDA;
+    }
+    if (h->graphExec[p]) {
+        cudaGraphExecDestroy(h->graphExec[p]);
+        h->graphExec[p] = nullptr;
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&h->graphExec[p], g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+        h->graphExec[p] = nullptr;
+        h->err = std::string("graph instantiation: ") + cudaGetErrorString(ei);
+        return DEME_ERR_CUDA;
+    }
+    h->graphKey[p] = graph_key(h);
+    return DEME_OK;
+}
+
+static int32_t step_graph(deme_handle* h, int32_t n_steps) {
+    const int f = std::max(1, h->params.cd_update_freq);
+    while (n_steps > 0 && h->steps % f != 0) {
+        TRY(step_plain(h));
+        n_steps--;
+    }
+    const int32_t windows = n_steps / f;
+    if (windows > 0) {
+        TRY(graph_prepare(h));
+        TRY(save_checkpoint(h, h->graphCkpt));
+        const int cur0 = h->cur;
+        for (int32_t w = 0; w < windows; w++) {
+            const int p = h->cur;
+            if (!h->graphExec[p] || h->graphKey[p] != graph_key(h)) TRY(graph_capture(h, p));
+            CUDA_TRY(h, cudaGraphLaunch(h->graphExec[p], h->st_dt));
+            h->cur ^= 1;
+            h->steps += f;
+            h->t += (double)h->k.h * f;
+            h->countStale = true;
+            h->outsValid = h->keepOutputs;
+            h->everDetected = true;
+            h->graphReplays++;
+        }
+        // a device error inside the replays (a list or the pair pool outgrew its capacity) voids them
+        CUDA_TRY(h, cudaMemcpyAsync(h->hErr, h->dErr, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->st_dt));
+        CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
+        if (*h->hErr) {
+            *h->hErr = 0;
+            CUDA_TRY(h, cudaMemset(h->dErr, 0, 4 * sizeof(uint32_t)));
+            h->cur = cur0;
+            TRY(restore_checkpoint(h, h->graphCkpt));
+            h->graphRollbacks++;
+            for (int32_t i = 0; i < windows * f; i++) TRY(step_plain(h));
+        }
+        n_steps -= windows * f;
+    }
+    while (n_steps-- > 0) TRY(step_plain(h));
+    return DEME_OK;
+}
+
+int32_t deme_set_graph(deme_handle* h, int32_t enable) {
+    if (!h) return DEME_ERR_INVALID;
+    TRY(cd_finish(h));
+    h->useGraph = enable != 0;
+    return DEME_OK;
+}
+
+int32_t deme_graph_stats(deme_handle* h, int64_t* replays, int64_t* rollbacks) {
+    if (!h) return DEME_ERR_INVALID;
+    if (replays) *replays = h->graphReplays;
+    if (rollbacks) *rollbacks = h->graphRollbacks;
+    return DEME_OK;
+}
+
+// ------------------------------------------------------------------------------------------- search shape ----
+int32_t deme_set_search_shape(deme_handle* h, int32_t shape, float cell_factor) {
+    if (!h) return DEME_ERR_INVALID;
+    if (shape < 0 || shape >= find_shape_count() || !(cell_factor >= 1.f) || cell_factor > 4.f) {
+        h->err = "search shape out of range (shape index in [0, deme_search_shape_count), cell factor in [1, 4])";
+        return DEME_ERR_INVALID;
+    }
+    TRY(cd_finish(h));
+    CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
+    h->findShape = shape;
+    set_cell_grid(h, cell_factor);
+    return DEME_OK;
+}
+
+int32_t deme_search_shape_count(void) { return find_shape_count(); }
+
+// Times every (pooled-search shape, cell factor) pair on a few steps from the same state, keeps the fastest and
+// puts the state back.  Every pair gives the same contact lists, so only the time differs.
+int32_t deme_autotune(deme_handle* h, int32_t steps_per_trial, deme_tuning* out) {
+    if (!h) return DEME_ERR_INVALID;
+    const int32_t steps = steps_per_trial > 0 ? steps_per_trial : 5;
+    const float factors[] = {1.f, 1.25f, 1.5f};
+    TRY(cd_finish(h));
+    Checkpoint ck;
+    TRY(save_checkpoint(h, ck));
+    const int cur0 = h->cur;
+    const bool graph0 = h->useGraph;
+    h->useGraph = false;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CUDA_TRY(h, cudaEventCreate(&e0));
+    CUDA_TRY(h, cudaEventCreate(&e1));
+    float best = 3.4e38f, dflt = 0.f;
+    int bestShape = 0;
+    float bestFactor = 1.f;
+    int trials = 0;
+    int32_t st = DEME_OK;
+    for (int v = 0; v < find_shape_count() && st == DEME_OK; v++) {
+        for (float f : factors) {
+            h->findShape = v;
+            set_cell_grid(h, f);
+            h->cur = cur0;
+            if ((st = restore_checkpoint(h, ck)) != DEME_OK) break;
+            if ((st = step_plain(h)) != DEME_OK) break;  // settles buffer sizes for this shape
+            cudaEventRecord(e0, h->st_dt);
+            for (int32_t i = 0; i < steps && st == DEME_OK; i++) st = step_plain(h);
+            cudaEventRecord(e1, h->st_dt);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms /= (float)steps;
+            if (v == 0 && f == 1.f) dflt = ms;
+            if (ms < best) {
+                best = ms;
+                bestShape = v;
+                bestFactor = f;
+            }
+            trials++;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    h->findShape = bestShape;
+    set_cell_grid(h, bestFactor);
+    h->cur = cur0;
+    const int32_t rs = restore_checkpoint(h, ck);
+    free_checkpoint(h, ck);
+    h->useGraph = graph0;
+    if (st != DEME_OK) return st;
+    TRY(rs);
+    if (out) {
+        uint32_t w = 0, slots = 0;
+        find_shape(bestShape, &w, &slots);
+        out->shape = bestShape;
+        out->find_warps = (int32_t)w;
+        out->find_slots = (int32_t)slots;
+        out->cell_factor = bestFactor;
+        out->ms_per_step = best;
+        out->ms_per_step_default = dflt;
+        out->trials = trials;
+    }
+    return DEME_OK;
+}
+
+int32_t deme_step(deme_handle* h, int32_t n_steps) {
+    if (!h) return DEME_ERR_INVALID;
+    if (h->useGraph && h->cdLag == 0 && !prof_timing()) {
+        TRY(step_graph(h, n_steps));
+    } else {
+        for (int32_t i = 0; i < n_steps; i++) TRY(step_plain(h));
     }
     return check_launch(h, "step");
 }
@@ -822,12 +1150,14 @@ int32_t deme_upload_state(deme_handle* h, const deme_state* s) {
 
 int32_t deme_get_num_contacts(deme_handle* h, uint32_t* n) {
     if (!h || !n) return DEME_ERR_INVALID;
+    TRY(refresh_count(h));
     *n = h->nContacts;
     return DEME_OK;
 }
 
 int32_t deme_download_contacts(deme_handle* h, deme_contacts* o) {
     if (!h || !o) return DEME_ERR_INVALID;
+    TRY(refresh_count(h));
     const uint32_t n = h->nContacts;
     o->n_contacts = n;
     if (o->capacity < n) return DEME_ERR_OVERFLOW;
@@ -897,13 +1227,16 @@ int32_t deme_upload_contacts(deme_handle* h, const deme_contacts* in) {
         CUDA_TRY(h, cudaMemcpy(c.mapping, nul.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice));
     }
     CUDA_TRY(h, cudaMemcpy(c.off, off.data(), off.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(c.dN, &n, sizeof(uint32_t), cudaMemcpyHostToDevice));
     h->nContacts = n;
+    h->countStale = false;
     h->outsValid = false;
     return DEME_OK;
 }
 
 int32_t deme_download_contact_forces(deme_handle* h, deme_contact_forces* o) {
     if (!h || !o) return DEME_ERR_INVALID;
+    TRY(refresh_count(h));
     const uint32_t n = h->nContacts;
     o->n_contacts = n;
     if (o->capacity < n) return DEME_ERR_OVERFLOW;

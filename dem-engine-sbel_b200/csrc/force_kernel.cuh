@@ -29,7 +29,8 @@ __global__ void __launch_bounds__(kForceThreads, DEME_FORCE_MIN_BLOCKS) k_force(
         __syncthreads();
     }
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = i < n;
+    // the count on the device bounds the launch (which may cover the list's capacity)
+    const bool valid = i < (c.dN ? min(n, *c.dN) : n);
     uint32_t oA = 0xFFFFFFFFu, oB = 0xFFFFFFFFu;
     bool bSphere = false;
     float3 F = make_float3(0.f, 0.f, 0.f), T = make_float3(0.f, 0.f, 0.f);

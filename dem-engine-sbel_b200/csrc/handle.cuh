@@ -21,7 +21,25 @@ struct ContactBuf {
     float4* hist = nullptr;
     uint32_t* mapping = nullptr;
     uint32_t* off = nullptr;  // nS + 1, allocated once
-    ContactView view() const { return ContactView{idA, idB, type, hist, mapping, off}; }
+    uint32_t* dN = nullptr;   // the list's contact count on the device, allocated once
+    ContactView view() const { return ContactView{idA, idB, type, hist, mapping, off, dN}; }
+};
+
+// Owner state and contact list at one step (adjoint checkpoints, graph-replay rollback).
+struct Checkpoint {
+    uint64_t* voxel = nullptr;
+    ushort4* loc = nullptr;
+    float4* quat = nullptr;
+    float4* vel = nullptr;
+    float4* omg = nullptr;
+    uint32_t n = 0, cap = 0;
+    uint32_t* idA = nullptr;
+    uint32_t* idB = nullptr;
+    uint8_t* type = nullptr;
+    float4* hist = nullptr;
+    uint32_t* off = nullptr;
+    int64_t steps = 0;
+    double t = 0.0;
 };
 
 struct deme_handle {
@@ -85,6 +103,18 @@ struct deme_handle {
     // Asynchronous contact detection (kT on st_kt, dT on st_dt).  With cdLag > 0 a detection due at step k runs on
     // kT from a snapshot of the owner poses of step k while dT keeps stepping with the current list, and dT adopts
     // the new list at step k + cdLag.
+    // search shape (deme_set_search_shape / deme_autotune): pooled-search block shape and search-cell factor
+    int32_t findShape = 0;
+    float cellFactor = 1.f;
+    // CUDA-graph replay of whole steps (deme_set_graph): one executable graph per parity of `cur` at the start of
+    // a detection window, keyed by everything its launches captured.
+    bool useGraph = false;
+    bool capturing = false;   // the step functions are being recorded: no host reads, launches cover capacities
+    bool countStale = false;  // the list in use came out of a graph replay: its count is on the device only
+    cudaGraphExec_t graphExec[2] = {nullptr, nullptr};
+    std::vector<uint8_t> graphKey[2];
+    Checkpoint graphCkpt;     // state and list at the start of a replayed batch, for rollback
+    int64_t graphReplays = 0, graphRollbacks = 0;
     int32_t cdLag = 0;
     bool cdPending = false;
     bool everDetected = false;
@@ -126,6 +156,12 @@ struct deme_handle {
         return s;
     }
 };
+
+int32_t alloc_checkpoint(deme_handle* h, Checkpoint& c, uint32_t nContacts);
+void free_checkpoint(deme_handle* h, Checkpoint& c);
+int32_t save_checkpoint(deme_handle* h, Checkpoint& c);
+int32_t restore_checkpoint(deme_handle* h, const Checkpoint& c);
+int32_t refresh_count(deme_handle* h);
 
 #define CUDA_TRY(h, expr)                                                                        \
     do {                                                                                         \

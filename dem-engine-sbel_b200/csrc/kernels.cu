@@ -380,8 +380,6 @@ __device__ __forceinline__ void append_pairs(const CDView& cd, bool hit, uint32_
 //      the whole warp stepping through the expensive path whenever any one lane has a survivor.
 // Found pairs go to the temporary list (any order) and raise A's count, which was preset to A's number of
 // analytical contacts; a lane with more survivors than it can pool is queued for k_pair_overflow.
-constexpr uint32_t kSurv = 16;
-constexpr uint32_t kFindWarps = 4;
 
 // Lane that owns pooled pair p: the last lane whose survivor prefix is <= p.
 __device__ __forceinline__ uint32_t pool_owner(const uint32_t* pre, uint32_t p) {
@@ -392,15 +390,16 @@ __device__ __forceinline__ uint32_t pool_owner(const uint32_t* pre, uint32_t p) 
     return L;
 }
 
-#ifndef DEME_FIND_MIN_BLOCKS
-#define DEME_FIND_MIN_BLOCKS 8
-#endif
-__global__ void __launch_bounds__(kFindWarps * 32, DEME_FIND_MIN_BLOCKS) k_pair_find(SimConsts k, StateView s, CDView cd,
-                                                                  uint32_t tempCap) {
-    __shared__ uint32_t s_pre[kFindWarps][33];          // survivor prefix over lanes
-    __shared__ uint32_t s_surv[kFindWarps][kSurv][32];  // survivors, [slot][lane]
-    __shared__ SphRec s_ctx[kFindWarps][32];
-    __shared__ uint16_t s_pass[kFindWarps][32 * kSurv];  // pooled pairs that passed pair_near
+// The pooled search comes in a few block shapes (warps per block, survivor slots per lane), chosen per scene by
+// deme_autotune; every shape finds the same pairs.  Each keeps threads x resident blocks at 1,024 per SM, so the
+// register budget (64 per thread) is the same.
+template <uint32_t kWarps, uint32_t kSlots>
+__global__ void __launch_bounds__(kWarps * 32, 32 / kWarps) k_pair_find(SimConsts k, StateView s, CDView cd,
+                                                                         uint32_t tempCap) {
+    __shared__ uint32_t s_pre[kWarps][33];           // survivor prefix over lanes
+    __shared__ uint32_t s_surv[kWarps][kSlots][32];  // survivors, [slot][lane]
+    __shared__ SphRec s_ctx[kWarps][32];
+    __shared__ uint16_t s_pass[kWarps][32 * kSlots];  // pooled pairs that passed pair_near
     const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     bool valid = i < k.n_spheres;
@@ -414,12 +413,12 @@ __global__ void __launch_bounds__(kFindWarps * 32, DEME_FIND_MIN_BLOCKS) k_pair_
             s_ctx[w][lane] = me;
             const SearchBox b = search_box(k, me.x, me.y, me.z, me.rf);
             for_each_forward_candidate(k, cd, i, fA, b, prefilter_lim2(k, me.rf), __ldg(cd.sClump + me.id), [&](uint32_t j) {
-                if (nSurv < kSurv) s_surv[w][nSurv][lane] = j;
+                if (nSurv < kSlots) s_surv[w][nSurv][lane] = j;
                 nSurv++;
             });
         }
     }
-    const bool ovf = valid && nSurv > kSurv;
+    const bool ovf = valid && nSurv > kSlots;
     const uint32_t pool = (valid && !ovf) ? nSurv : 0u;
     uint32_t incl = pool;
 #pragma unroll
@@ -471,10 +470,42 @@ __global__ void __launch_bounds__(kFindWarps * 32, DEME_FIND_MIN_BLOCKS) k_pair_
     }
 }
 
-void launch_pair_find(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st) {
+namespace {
+struct FindShape {
+    uint32_t warps, slots;
+};
+constexpr FindShape kFindShapes[] = {{4, 16}, {2, 16}, {8, 16}, {4, 8}, {4, 24}};
+constexpr int kNumFindShapes = sizeof(kFindShapes) / sizeof(kFindShapes[0]);
+}  // namespace
+
+int find_shape_count() { return kNumFindShapes; }
+void find_shape(int v, uint32_t* warps, uint32_t* slots) {
+    const FindShape f = kFindShapes[(v >= 0 && v < kNumFindShapes) ? v : 0];
+    *warps = f.warps;
+    *slots = f.slots;
+}
+
+void launch_pair_find(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, int shape,
+                      cudaStream_t st) {
     if (!(k.n_spheres)) return;
     ProfScope prof_(KID_PAIR_COUNT, st);
-    k_pair_find<<<blocks_for(k.n_spheres, kFindWarps * 32), kFindWarps * 32, 0, st>>>(k, s, cd, tempCap);
+    const uint32_t n = k.n_spheres;
+    switch (shape) {
+        case 1:
+            k_pair_find<2, 16><<<blocks_for(n, 64), 64, 0, st>>>(k, s, cd, tempCap);
+            break;
+        case 2:
+            k_pair_find<8, 16><<<blocks_for(n, 256), 256, 0, st>>>(k, s, cd, tempCap);
+            break;
+        case 3:
+            k_pair_find<4, 8><<<blocks_for(n, 128), 128, 0, st>>>(k, s, cd, tempCap);
+            break;
+        case 4:
+            k_pair_find<4, 24><<<blocks_for(n, 128), 128, 0, st>>>(k, s, cd, tempCap);
+            break;
+        default:
+            k_pair_find<4, 16><<<blocks_for(n, 128), 128, 0, st>>>(k, s, cd, tempCap);
+    }
 }
 
 // Spheres the pooled search could not hold: the same forward-half search, one thread per sphere, exact test
@@ -521,10 +552,14 @@ void launch_cnt_init(const SimConsts& k, const CDView& cd, cudaStream_t st) {
 
 // Places every found pair in A's segment of the new list.  After the scan A's count is no longer needed, so the
 // slots after A's analytical contacts are handed out from the top by decrementing it.
+// The pool count is read on the device (counters[0]), so the launch may cover more threads than pairs; a pool that
+// outgrew its buffer (only possible when the host did not see the count first) is flagged.
 __global__ void __launch_bounds__(256) k_pair_scatter(SimConsts k, CDView cd, ContactView c, uint32_t nPairs,
-                                                      uint32_t cap) {
+                                                      uint32_t cap, uint32_t poolCap) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= nPairs) return;
+    const uint32_t pool = cd.counters[0];
+    if (p == 0 && pool > poolCap) atomicOr(k.err, ERR_CONTACT_CAPACITY);
+    if (p >= min(nPairs, min(pool, poolCap))) return;
     const uint2 ab = cd.candTemp[p];
     if (!index_ok(k.err, 15, ab.x, k.n_spheres)) return;
     const uint32_t slot = atomicSub(&cd.cnt[ab.x], 1u) - 1u;
@@ -534,10 +569,10 @@ __global__ void __launch_bounds__(256) k_pair_scatter(SimConsts k, CDView cd, Co
 }
 
 void launch_pair_scatter(const SimConsts& k, const CDView& cd, const ContactView& c, uint32_t nPairs, uint32_t cap,
-                         cudaStream_t st) {
+                         uint32_t poolCap, cudaStream_t st) {
     if (!(nPairs)) return;
     ProfScope prof_(KID_PAIR_EMIT, st);
-    k_pair_scatter<<<blocks_for(nPairs, 256), 256, 0, st>>>(k, cd, c, nPairs, cap);
+    k_pair_scatter<<<blocks_for(nPairs, 256), 256, 0, st>>>(k, cd, c, nPairs, cap, poolCap);
 }
 
 // Completes the canonical list: per sphere A (ID order), its sphere--analytical contacts by component id
@@ -607,6 +642,9 @@ void launch_pair_assemble(const SimConsts& k, const StateView& s, const CDView& 
 __global__ void __launch_bounds__(256) k_history(uint32_t n, ContactView cur, ContactView prev, bool has_hist,
                                                  uint32_t nS, uint32_t prevN, uint32_t* err) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    // the counts on the device bound the launch (it may cover a list's capacity)
+    if (cur.dN) n = min(n, *cur.dN);
+    if (prev.dN) prevN = *prev.dN;
     if (i >= n) return;
     const uint32_t A = cur.idA[i], B = cur.idB[i];
     const uint8_t t = cur.type[i];

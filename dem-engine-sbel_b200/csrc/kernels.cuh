@@ -78,6 +78,7 @@ struct ContactView {
     float4* hist;       // (delta_tan_x, delta_tan_y, delta_tan_z, delta_time)
     uint32_t* mapping;
     uint32_t* off;      // CSR offsets by sphere (nS + 1)
+    uint32_t* dN;       // number of contacts, on the device (written by the scan that makes the offsets)
 };
 
 // Reactions on analytical owners (walls): block partials, reduced in fixed order.
@@ -101,11 +102,14 @@ void launch_place_anal(const SimConsts& k, const StateView& s, const AnalRaw* ra
 void launch_sphere_prep(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
 void launch_cell_scatter(const SimConsts& k, const CDView& cd, cudaStream_t st);
 void launch_gather_sorted(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
-void launch_pair_find(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st);
+void launch_pair_find(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, int shape,
+                      cudaStream_t st);
+int find_shape_count();                                     // block shapes of the pooled search
+void find_shape(int v, uint32_t* warps, uint32_t* slots);  // warps per block and survivor slots per lane of shape v
 void launch_pair_overflow(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st);
 void launch_cnt_init(const SimConsts& k, const CDView& cd, cudaStream_t st);
 void launch_pair_scatter(const SimConsts& k, const CDView& cd, const ContactView& c, uint32_t nPairs, uint32_t cap,
-                         cudaStream_t st);
+                         uint32_t poolCap, cudaStream_t st);
 void launch_pair_assemble(const SimConsts& k, const StateView& s, const CDView& cd, const ContactView& c, uint32_t cap,
                           cudaStream_t st);
 void launch_history(const SimConsts& k, const ContactView& cur, const ContactView& prev, uint32_t n, uint32_t prevN,

@@ -30,6 +30,7 @@ const char* kernel_name(int id);
 void prof_begin(int id, cudaStream_t st);
 void prof_end(int id, cudaStream_t st);
 int64_t launch_count();
+bool prof_timing();  // per-kernel timing is on (its events are recorded at launch time, so graphs are not used)
 
 struct ProfScope {
     int id;

@@ -249,6 +249,13 @@ def state_struct(arrays: dict) -> tuple[State, list]:
     return st, keep
 
 
+class Tuning(C.Structure):
+    """deme_tuning: the search shape deme_autotune chose."""
+    _fields_ = [("shape", C.c_int32), ("find_warps", C.c_int32), ("find_slots", C.c_int32),
+                ("cell_factor", C.c_float), ("ms_per_step", C.c_float), ("ms_per_step_default", C.c_float),
+                ("trials", C.c_int32)]
+
+
 def bind(lib: C.CDLL, prefix: str):
     """Declare the argument/return types of the shared entry points under ``prefix``."""
     VP = C.c_void_p

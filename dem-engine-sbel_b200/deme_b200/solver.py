@@ -234,6 +234,30 @@ class Solver(HandleSolver):
         self.lib.deme_set_async_cd.argtypes = [C.c_void_p, C.c_int32]
         self._check(self.lib.deme_set_async_cd(self.h, int(lag)), "set_async_cd")
 
+    def set_graph(self, enable: bool = True):
+        """Replay whole steps from CUDA graphs (see deme_set_graph)."""
+        self.lib.deme_set_graph.argtypes = [C.c_void_p, C.c_int32]
+        self._check(self.lib.deme_set_graph(self.h, int(enable)), "set_graph")
+
+    def graph_stats(self) -> tuple[int, int]:
+        """(windows replayed from graphs, batches rolled back)."""
+        r, b = C.c_int64(0), C.c_int64(0)
+        self.lib.deme_graph_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        self._check(self.lib.deme_graph_stats(self.h, C.byref(r), C.byref(b)), "graph_stats")
+        return int(r.value), int(b.value)
+
+    def set_search_shape(self, shape: int, cell_factor: float = 1.0):
+        """Block shape of the pooled pair search and search-cell scale (see deme_set_search_shape)."""
+        self.lib.deme_set_search_shape.argtypes = [C.c_void_p, C.c_int32, C.c_float]
+        self._check(self.lib.deme_set_search_shape(self.h, int(shape), float(cell_factor)), "set_search_shape")
+
+    def autotune(self, steps_per_trial: int = 5) -> dict:
+        """Times every search shape and keeps the fastest; the state is left as it was (see deme_autotune)."""
+        t = capi.Tuning()
+        self.lib.deme_autotune.argtypes = [C.c_void_p, C.c_int32, C.POINTER(capi.Tuning)]
+        self._check(self.lib.deme_autotune(self.h, int(steps_per_trial), C.byref(t)), "autotune")
+        return {name: getattr(t, name) for name, _ in capi.Tuning._fields_}
+
     def keep_contact_forces(self, enable: bool = True):
         self.lib.deme_keep_contact_forces.argtypes = [C.c_void_p, C.c_int32]
         self._check(self.lib.deme_keep_contact_forces(self.h, int(enable)), "keep_contact_forces")

@@ -298,6 +298,42 @@ int32_t deme_set_streams(deme_handle* h, void* kT_stream, void* dT_stream);
  * once.  Uploading state or contacts drops a pending detection; deme_detect_contacts and deme_sync adopt it first. */
 int32_t deme_set_async_cd(deme_handle* h, int32_t lag);
 
+/* Whole steps as CUDA graphs (no reference counterpart: its host code launches and synchronises kernel by kernel,
+ * src/DEM/dT.cpp:1446-1586).  With enable != 0, deme_step records a window of cd_update_freq steps (one detection,
+ * then forces and integration each step) into a CUDA graph once and replays it; nothing in a window waits for the
+ * host.  Launches cover the contact lists' capacities, sized before recording at 1.5 times the current count (at
+ * least twice the sphere count), and the kernels read the counts on the device.  A replayed batch in which a list
+ * or the pair pool outgrew its capacity is rolled back to the checkpoint taken at its start and redone step by step,
+ * so results do not depend on the mode.  Steps before the next detection step, and those left after the last whole
+ * window, run step by step.  A graph is recorded again whenever anything it captured changes (buffers, streams,
+ * time step, force model, stored outputs).  Not used with deme_set_async_cd lag > 0 or while per-kernel timing
+ * (deme_kernel_timing) is on.  Helps small scenes, whose steps are bound by launch latency. */
+int32_t deme_set_graph(deme_handle* h, int32_t enable);
+/* Windows replayed from graphs and batches rolled back, since the handle was created. */
+int32_t deme_graph_stats(deme_handle* h, int64_t* replays, int64_t* rollbacks);
+
+/* Search shape (no reference counterpart: the reference's bin size, SetInitBinSize, sets both its bins and its
+ * work per thread).  `shape` picks a block shape of the pooled pair search (index < deme_search_shape_count();
+ * 0, the default, is 4 warps with 16 survivor slots per lane) and `cell_factor` in [1, 4] scales the search cells
+ * (edge cell_factor x max(bin size, largest expanded diameter)).  Every shape finds the same contacts. */
+int32_t deme_set_search_shape(deme_handle* h, int32_t shape, float cell_factor);
+int32_t deme_search_shape_count(void);
+
+typedef struct {
+    int32_t shape;         /* index passed to deme_set_search_shape */
+    int32_t find_warps;    /* warps per block of the pooled search */
+    int32_t find_slots;    /* survivor slots per lane */
+    float cell_factor;
+    float ms_per_step;     /* the chosen shape's time per step in the trials */
+    float ms_per_step_default;
+    int32_t trials;
+} deme_tuning;
+
+/* Autotuner: times every search shape with cell factors 1, 1.25 and 1.5 on `steps_per_trial` steps (5 when <= 0)
+ * from the current state, keeps the fastest, and restores the state and contact history, so the run continues as
+ * if it had not been called.  `out` may be NULL. */
+int32_t deme_autotune(deme_handle* h, int32_t steps_per_trial, deme_tuning* out);
+
 /* Change one family's prescription between steps (the constant-valued form of SetFamilyPrescribedLinVel /
  * SetFamilyPrescribedAngVel / SetFamilyFixed, src/DEM/APIPublic.cpp:145-252, which the reference can only change by
  * re-jitifying).  The value is staged through pinned memory and applied in stream order. */
