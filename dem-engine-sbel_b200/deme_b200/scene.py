@@ -56,6 +56,10 @@ class ClumpTemplate:
     radii: np.ndarray
     rel_pos: np.ndarray
     materials: list
+    name: str = ""  # DEMClumpTemplate::m_name; "%04d" of the load count unless assigned (APIPublic.cpp:337-341)
+
+    def AssignName(self, some_name: str):
+        self.name = some_name
 
 
 class ClumpBatch:
@@ -300,7 +304,7 @@ class SceneBuilder:
         if not isinstance(materials, (list, tuple)):
             materials = [materials] * len(radii)
         t = ClumpTemplate(len(self.templates), float(np.float32(mass)), tuple(np.asarray(moi, f32)), radii, rel_pos,
-                          list(materials))
+                          list(materials), "%04d" % len(self.templates))
         self.templates.append(t)
         return t
 
@@ -602,7 +606,9 @@ class SceneBuilder:
                       mat_mu=matarr("mu"), mat_Crr=matarr("Crr"), family_masks=masks, **anal, **ext_arrays)
         counts = dict(o=nO, s=nS, a=nA, m=nM)
         info = dict(n_clumps=nClumps, n_ext=nExt, n_templates=nT, rmin=rmin, bin_size=bin_size, nb=nb, nv=nv, l=l,
-                    beta=beta, lbf=lbf.copy(), box=self.box.copy(), merged_prescriptions=self.merged_prescriptions)
+                    beta=beta, lbf=lbf.copy(), box=self.box.copy(), merged_prescriptions=self.merged_prescriptions,
+                    owner_template=np.asarray(types, np.int64) if nClumps else np.zeros(0, np.int64),
+                    template_names=[t.name for t in self.templates])
         return BuiltScene(p, arrays, counts, presc, info)
 
     @staticmethod

@@ -159,6 +159,34 @@ class HandleSolver:
         self._check(self._fn("download_contact_forces")(self.h, C.byref(c)), "download_contact_forces")
         return {k: v[:c.n_contacts] for k, v in d.items()}
 
+    # ---- output in DEM-Engine's CSV formats (deme_b200.io; WriteSphereFile etc., src/DEM/API.h:319-324) ----
+    def SetOutputContent(self, content: int):
+        self._out_content = int(content)
+
+    def SetContactOutputContent(self, content: int):
+        self._cnt_out_content = int(content)
+
+    def DisableFamilyOutput(self, fam: int):
+        self._no_output = tuple(sorted(set(getattr(self, "_no_output", ())) | {int(fam)}))
+
+    def WriteSphereFile(self, path: str):
+        from . import io
+        io.write_sphere_file(path, self.built, self.state(), getattr(self, "_out_content", io.DEFAULT_CONTENT),
+                             getattr(self, "_no_output", ()))
+
+    def WriteClumpFile(self, path: str):
+        from . import io
+        io.write_clump_file(path, self.built, self.state(), getattr(self, "_out_content", io.DEFAULT_CONTENT),
+                            getattr(self, "_no_output", ()))
+
+    def WriteContactFile(self, path: str):
+        """Forces, points and normals need the per-contact forces of the last step (the CUDA solver keeps them after
+        keep_contact_forces(True))."""
+        from . import io
+        content = getattr(self, "_cnt_out_content", io.DEFAULT_CONTACT_CONTENT)
+        forces = self.contact_forces() if content != io.OWNERS else None
+        io.write_contact_file(path, self.built, self.state(), self.contacts(), forces, content)
+
     def bin_assignment(self, with_pairs: bool = True) -> dict:
         nb = np.zeros(max(self.nS, 1), np.uint16)
         na = np.zeros(max(self.nS, 1), np.uint8)

@@ -49,6 +49,8 @@ class DEMMaterial {
 
 class DEMClumpTemplate {
   public:
+    std::string m_name = "NULL";  // "%04d" of the load count unless assigned (src/DEM/APIPublic.cpp:337-341)
+    void AssignName(const std::string& some_name) { m_name = some_name; }
     float mass = 0.f;
     float3 MOI{0.f, 0.f, 0.f};
     std::vector<float> radii;
@@ -176,6 +178,9 @@ struct FlatScene {
     std::vector<float> mat_E, mat_nu, mat_CoR, mat_mu, mat_Crr;
     std::vector<uint8_t> family_masks;
     std::vector<deme_family_prescription> prescriptions;
+    // clump owners' template marks and the templates' names (the clump file's clump_type column)
+    std::vector<uint32_t> owner_template;
+    std::vector<std::string> template_names;
 
     void point() {
         deme_scene& s = scene;
@@ -232,6 +237,139 @@ struct FlatScene {
     }
 };
 
+// ---- CSV output in DEM-Engine's formats (writeSpheresAsCsv / writeClumpsAsCsv / writeContactsAsCsv,
+// src/DEM/dT.cpp:896-1180).  Values are formed in float as the reference's host code forms them and printed as a
+// default std::ostream prints a float.  Contact points are rotated with owner A's quaternion (the reference uses
+// the quaternion of the owner whose index equals the contact's index).
+// OUTPUT_CONTENT / CNT_OUTPUT_CONTENT bits (src/DEM/Defines.h:118-143)
+namespace OUTPUT_CONTENT {
+constexpr unsigned XYZ = 0, QUAT = 1, ABSV = 2, VEL = 4, ANG_VEL = 8, ACC = 16, ANG_ACC = 32, FAMILY = 64, MAT = 128;
+}
+namespace CNT_OUTPUT_CONTENT {
+constexpr unsigned OWNERS = 0, FORCE = 1, POINT = 2, COMPONENT = 4, NORMAL = 8, TORQUE_ONLY_FORCE = 16;
+}
+
+// Owner state as deme_download_state fills it.
+struct OwnerState {
+    std::vector<uint64_t> voxel;
+    std::vector<uint16_t> locX, locY, locZ;
+    std::vector<float> oriQw, oriQx, oriQy, oriQz, vX, vY, vZ;
+    std::vector<uint8_t> family;
+    void resize(size_t n) {
+        voxel.resize(n);
+        locX.resize(n);
+        locY.resize(n);
+        locZ.resize(n);
+        for (auto* v : {&oriQw, &oriQx, &oriQy, &oriQz, &vX, &vY, &vZ}) v->resize(n);
+        family.resize(n);
+    }
+};
+
+namespace csv_detail {
+// hostVoxelIDToPosition<float> plus the domain's lower corner (src/DEM/HostSideHelpers.hpp:308-324)
+inline float3 owner_com(const FlatScene& f, const OwnerState& st, size_t o) {
+    const deme_sim_params& p = f.params;
+    const uint64_t v = st.voxel[o];
+    const uint64_t mx = (1ull << p.nvXp2) - 1, my = (1ull << p.nvYp2) - 1;
+    const float vs = (float)p.voxel_size, l = (float)p.l;
+    const float X = (float)(v & mx) * vs + (float)st.locX[o] * l;
+    const float Y = (float)((v >> p.nvXp2) & my) * vs + (float)st.locY[o] * l;
+    const float Z = (float)(v >> (p.nvXp2 + p.nvYp2)) * vs + (float)st.locZ[o] * l;
+    return float3{X + p.lbf[0], Y + p.lbf[1], Z + p.lbf[2]};
+}
+// hostApplyOriQToVector3<float, float> (src/DEM/HostSideHelpers.hpp:384-394)
+inline float3 rotate(float3 r, float Qw, float Qx, float Qy, float Qz) {
+    const float X = (2.f * (Qw * Qw + Qx * Qx) - 1.f) * r.x + (2.f * (Qx * Qy - Qw * Qz)) * r.y +
+                    (2.f * (Qx * Qz + Qw * Qy)) * r.z;
+    const float Y = (2.f * (Qx * Qy + Qw * Qz)) * r.x + (2.f * (Qw * Qw + Qy * Qy) - 1.f) * r.y +
+                    (2.f * (Qy * Qz - Qw * Qx)) * r.z;
+    const float Z = (2.f * (Qx * Qz - Qw * Qy)) * r.x + (2.f * (Qy * Qz + Qw * Qx)) * r.y +
+                    (2.f * (Qw * Qw + Qz * Qz) - 1.f) * r.z;
+    return float3{X, Y, Z};
+}
+inline float speed(float x, float y, float z) { return std::sqrt(x * x + y * y + z * z); }
+}  // namespace csv_detail
+
+inline void write_sphere_csv(std::ostream& os, const FlatScene& f, const OwnerState& st, unsigned content,
+                             const std::set<unsigned>& no_output = {}) {
+    using namespace csv_detail;
+    os << "X,Y,Z,r";
+    if (content & OUTPUT_CONTENT::ABSV) os << ",absv";
+    if (content & OUTPUT_CONTENT::VEL) os << ",v_x,v_y,v_z";
+    if (content & OUTPUT_CONTENT::FAMILY) os << ",family";
+    os << "\n";
+    for (size_t i = 0; i < f.radius.size(); i++) {
+        const size_t o = f.sphere_owner[i];
+        if (no_output.count(st.family[o])) continue;
+        const float3 c = owner_com(f, st, o);
+        const float3 d = rotate(float3{f.relX[i], f.relY[i], f.relZ[i]}, st.oriQw[o], st.oriQx[o], st.oriQy[o],
+                                st.oriQz[o]);
+        os << c.x + d.x << "," << c.y + d.y << "," << c.z + d.z << "," << f.radius[i];
+        if (content & OUTPUT_CONTENT::ABSV) os << "," << speed(st.vX[o], st.vY[o], st.vZ[o]);
+        if (content & OUTPUT_CONTENT::VEL) os << "," << st.vX[o] << "," << st.vY[o] << "," << st.vZ[o];
+        if (content & OUTPUT_CONTENT::FAMILY) os << "," << +st.family[o];
+        os << "\n";
+    }
+}
+
+inline void write_clump_csv(std::ostream& os, const FlatScene& f, const OwnerState& st, unsigned content,
+                            const std::set<unsigned>& no_output = {}) {
+    using namespace csv_detail;
+    os << "X,Y,Z,Qw,Qx,Qy,Qz,clump_type";
+    if (content & OUTPUT_CONTENT::ABSV) os << ",absv";
+    if (content & OUTPUT_CONTENT::VEL) os << ",v_x,v_y,v_z";
+    if (content & OUTPUT_CONTENT::FAMILY) os << ",family";
+    os << "\n";
+    for (size_t o = 0; o < f.owner_template.size(); o++) {
+        if (no_output.count(st.family[o])) continue;
+        const float3 c = owner_com(f, st, o);
+        os << c.x << "," << c.y << "," << c.z << "," << st.oriQw[o] << "," << st.oriQx[o] << "," << st.oriQy[o]
+           << "," << st.oriQz[o] << "," << f.template_names.at(f.owner_template[o]);
+        if (content & OUTPUT_CONTENT::ABSV) os << "," << speed(st.vX[o], st.vY[o], st.vZ[o]);
+        if (content & OUTPUT_CONTENT::VEL) os << "," << st.vX[o] << "," << st.vY[o] << "," << st.vZ[o];
+        if (content & OUTPUT_CONTENT::FAMILY) os << "," << +st.family[o];
+        os << "\n";
+    }
+}
+
+// Contacts as deme_download_contacts gives them; force, torque-only force and A's local contact point (n x 3 each)
+// as deme_download_contact_forces gives them.
+inline void write_contact_csv(std::ostream& os, const FlatScene& f, const OwnerState& st,
+                              const std::vector<uint32_t>& idA, const std::vector<uint32_t>& idB,
+                              const std::vector<uint8_t>& type, const std::vector<float>& force,
+                              const std::vector<float>& tof, const std::vector<float>& cpA, unsigned content) {
+    using namespace csv_detail;
+    os << "A,B,contact_type";
+    if (content & CNT_OUTPUT_CONTENT::FORCE) os << ",f_x,f_y,f_z";
+    if (content & CNT_OUTPUT_CONTENT::POINT) os << ",X,Y,Z";
+    if (content & CNT_OUTPUT_CONTENT::NORMAL) os << ",n_x,n_y,n_z";
+    if (content & CNT_OUTPUT_CONTENT::TORQUE_ONLY_FORCE) os << ",tof_x,tof_y,tof_z";
+    os << "\n";
+    for (size_t i = 0; i < idA.size(); i++) {
+        if (type[i] == DEME_NOT_A_CONTACT) continue;
+        const uint32_t oA = f.sphere_owner[idA[i]];
+        const uint32_t oB = type[i] == DEME_SPHERE_SPHERE_CONTACT ? f.sphere_owner[idB[i]] : f.anal_owner[idB[i]];
+        os << oA << "," << oB << "," << (type[i] == DEME_SPHERE_SPHERE_CONTACT ? "SS" : (type[i] == 2 ? "SM" : "SA"));
+        if (content & CNT_OUTPUT_CONTENT::FORCE)
+            os << "," << force[3 * i] << "," << force[3 * i + 1] << "," << force[3 * i + 2];
+        const float3 c = owner_com(f, st, oA);
+        float3 p = rotate(float3{cpA[3 * i], cpA[3 * i + 1], cpA[3 * i + 2]}, st.oriQw[oA], st.oriQx[oA],
+                          st.oriQy[oA], st.oriQz[oA]);
+        p = float3{c.x + p.x, c.y + p.y, c.z + p.z};
+        if (content & CNT_OUTPUT_CONTENT::POINT) os << "," << p.x << "," << p.y << "," << p.z;
+        if (content & CNT_OUTPUT_CONTENT::NORMAL) {
+            const float3 d = rotate(float3{f.relX[idA[i]], f.relY[idA[i]], f.relZ[idA[i]]}, st.oriQw[oA],
+                                    st.oriQx[oA], st.oriQy[oA], st.oriQz[oA]);
+            float nx = p.x - (c.x + d.x), ny = p.y - (c.y + d.y), nz = p.z - (c.z + d.z);
+            const float inv = 1.f / std::sqrt(nx * nx + ny * ny + nz * nz);
+            os << "," << nx * inv << "," << ny * inv << "," << nz * inv;
+        }
+        if (content & CNT_OUTPUT_CONTENT::TORQUE_ONLY_FORCE)
+            os << "," << tof[3 * i] << "," << tof[3 * i + 1] << "," << tof[3 * i + 2];
+        os << "\n";
+    }
+}
+
 class DEMSolver {
   public:
     DEMSolver() = default;
@@ -279,6 +417,9 @@ class DEMSolver {
         t->relPos = relPos;
         t->materials = mats;
         t->mark = (unsigned)templates.size();
+        char name[16];
+        std::snprintf(name, sizeof(name), "%04d", (int)templates.size());
+        t->AssignName(name);
         templates.push_back(t);
         return t;
     }
@@ -391,6 +532,7 @@ class DEMSolver {
             h = nullptr;
             throw std::runtime_error(std::string("Initialize: ") + deme_status_string(st) + ": " + msg);
         }
+        if (cnt_out_content != CNT_OUTPUT_CONTENT::OWNERS) check(deme_keep_contact_forces(h, 1));
         if (force_model && force_model->custom) {
             std::vector<const char*> names;
             for (const auto& n : force_model->m_contact_wildcards) names.push_back(n.c_str());
@@ -409,6 +551,74 @@ class DEMSolver {
         check(deme_sync(h));
     }
     void DoStepDynamics() { check(deme_step(h, 1)); }
+
+    // ---- output (WriteSphereFile / WriteClumpFile / WriteContactFile, src/DEM/API.h:319-324, 430-436) ----
+    void SetOutputContent(unsigned content) { out_content = content; }
+    void SetContactOutputContent(unsigned content) { cnt_out_content = content; }
+    void DisableFamilyOutput(unsigned fam) { no_output.insert(fam); }
+    void WriteSphereFile(const std::string& path) {
+        std::ofstream os(path);
+        write_sphere_csv(os, *flat, pull_owner_state(), out_content, no_output);
+    }
+    void WriteClumpFile(const std::string& path) {
+        std::ofstream os(path);
+        write_clump_csv(os, *flat, pull_owner_state(), out_content, no_output);
+    }
+    /* Needs the per-contact forces of the last step: kept from Initialize on unless the contact output content was
+     * set to owners only before it. */
+    void WriteContactFile(const std::string& path) {
+        uint32_t n = 0;
+        check(deme_get_num_contacts(h, &n));
+        const size_t cap = std::max<size_t>(n, 1);
+        std::vector<uint32_t> idA(cap), idB(cap), map(cap);
+        std::vector<uint8_t> type(cap);
+        deme_contacts c{};
+        c.capacity = (uint32_t)cap;
+        c.idA = idA.data();
+        c.idB = idB.data();
+        c.type = type.data();
+        c.mapping = map.data();
+        check(deme_download_contacts(h, &c));
+        idA.resize(n);
+        idB.resize(n);
+        type.resize(n);
+        std::vector<float> F(3 * cap, 0.f), T(3 * cap, 0.f), P(3 * cap, 0.f);
+        if (cnt_out_content != CNT_OUTPUT_CONTENT::OWNERS) {
+            deme_contact_forces cf{};
+            cf.capacity = (uint32_t)cap;
+            cf.force = F.data();
+            cf.torque_only_force = T.data();
+            cf.cpA = P.data();
+            check(deme_download_contact_forces(h, &cf));
+        }
+        std::ofstream os(path);
+        write_contact_csv(os, *flat, pull_owner_state(), idA, idB, type, F, T, P, cnt_out_content);
+    }
+
+    /* ReadClumpXyzFromCsv / ReadClumpQuatFromCsv (src/DEM/API.h:326-371): clump type name -> coordinates or
+     * quaternions (w, x, y, z) from a clump file, in file order. */
+    static std::unordered_map<std::string, std::vector<float3>> ReadClumpXyzFromCsv(
+        const std::string& path, const std::string& clump_header = "clump_type", const std::string& x_header = "X",
+        const std::string& y_header = "Y", const std::string& z_header = "Z") {
+        std::unordered_map<std::string, std::vector<float3>> out;
+        for (const auto& r : read_csv_columns(path, {clump_header, x_header, y_header, z_header}))
+            out[r[0]].push_back(float3{std::stof(r[1]), std::stof(r[2]), std::stof(r[3])});
+        return out;
+    }
+    static std::unordered_map<std::string, std::vector<float4>> ReadClumpQuatFromCsv(
+        const std::string& path, const std::string& clump_header = "clump_type", const std::string& qw_header = "Qw",
+        const std::string& qx_header = "Qx", const std::string& qy_header = "Qy", const std::string& qz_header = "Qz") {
+        std::unordered_map<std::string, std::vector<float4>> out;
+        for (const auto& r : read_csv_columns(path, {clump_header, qw_header, qx_header, qy_header, qz_header})) {
+            float4 q;
+            q.w = std::stof(r[1]);
+            q.x = std::stof(r[2]);
+            q.y = std::stof(r[3]);
+            q.z = std::stof(r[4]);
+            out[r[0]].push_back(q);
+        }
+        return out;
+    }
 
     // ---- queries (GetOwner*, src/DEM/API.h:196-214) ----
     float3 GetOwnerPosition(uint32_t owner) {
@@ -462,6 +672,61 @@ class DEMSolver {
 
     void check(int32_t st) {
         if (st != DEME_OK) throw std::runtime_error(std::string(deme_status_string(st)) + ": " + deme_get_error(h));
+    }
+
+    OwnerState pull_owner_state() {
+        OwnerState st;
+        const uint32_t n = flat->scene.n_owners;
+        st.resize(n);
+        deme_state s{};
+        s.voxel = st.voxel.data();
+        s.locX = st.locX.data();
+        s.locY = st.locY.data();
+        s.locZ = st.locZ.data();
+        s.oriQw = st.oriQw.data();
+        s.oriQx = st.oriQx.data();
+        s.oriQy = st.oriQy.data();
+        s.oriQz = st.oriQz.data();
+        s.vX = st.vX.data();
+        s.vY = st.vY.data();
+        s.vZ = st.vZ.data();
+        s.family = st.family.data();
+        check(deme_download_state(h, &s));
+        return st;
+    }
+    static std::vector<std::vector<std::string>> read_csv_columns(const std::string& path,
+                                                                  const std::vector<std::string>& headers) {
+        std::ifstream in(path);
+        if (!in) throw std::runtime_error("cannot open " + path);
+        auto split = [](const std::string& line) {
+            std::vector<std::string> cells;
+            std::stringstream ss(line);
+            std::string c;
+            while (std::getline(ss, c, ',')) {
+                const size_t a = c.find_first_not_of(" \t\r"), b = c.find_last_not_of(" \t\r");
+                cells.push_back(a == std::string::npos ? std::string() : c.substr(a, b - a + 1));
+            }
+            return cells;
+        };
+        std::string line;
+        std::vector<std::string> head;
+        while (head.empty() && std::getline(in, line))
+            if (line.find_first_not_of(" \t\r") != std::string::npos) head = split(line);
+        std::vector<size_t> idx;
+        for (const auto& hname : headers) {
+            const auto it = std::find(head.begin(), head.end(), hname);
+            if (it == head.end()) throw std::runtime_error("column " + hname + " missing from " + path);
+            idx.push_back((size_t)(it - head.begin()));
+        }
+        std::vector<std::vector<std::string>> rows;
+        while (std::getline(in, line)) {
+            if (line.find_first_not_of(" \t\r") == std::string::npos) continue;
+            const auto cells = split(line);
+            std::vector<std::string> r;
+            for (size_t k : idx) r.push_back(k < cells.size() ? cells[k] : std::string());
+            rows.push_back(r);
+        }
+        return rows;
     }
 
     void pull() {
@@ -591,6 +856,8 @@ class DEMSolver {
                f.omgZ, f.family, f.mass, f.mmiXX, f.mmiYY, f.mmiZZ);
         std::vector<float3> pos(nO);
         size_t o = 0;
+        f.template_names.clear();
+        for (const auto& t : templates) f.template_names.push_back(t->m_name);
         for (const DEMClumpBatch* b : bs) {
             for (size_t i = 0; i < b->nClumps; i++, o++) {
                 const DEMClumpTemplate& t = *b->types[i];
@@ -610,6 +877,7 @@ class DEMSolver {
                 f.mmiXX[o] = t.MOI.x;
                 f.mmiYY[o] = t.MOI.y;
                 f.mmiZZ[o] = t.MOI.z;
+                f.owner_template.push_back(t.mark);
                 for (unsigned k = 0; k < t.nComp(); k++) {
                     f.sphere_owner.push_back((uint32_t)o);
                     f.radius.push_back(t.radii[k]);
@@ -795,6 +1063,9 @@ class DEMSolver {
     std::shared_ptr<DEMForceModel> force_model;
     std::unique_ptr<FlatScene> flat;
     deme_handle* h = nullptr;
+    unsigned out_content = OUTPUT_CONTENT::QUAT | OUTPUT_CONTENT::ABSV;
+    unsigned cnt_out_content = CNT_OUTPUT_CONTENT::FORCE | CNT_OUTPUT_CONTENT::POINT;
+    std::set<unsigned> no_output;
     std::vector<uint64_t> st_voxel;
     std::vector<uint16_t> st_locX, st_locY, st_locZ;
     std::vector<float> st_f[10];

@@ -6,6 +6,7 @@
 #include <cstring>
 #include <fstream>
 #include <iostream>
+#include <sstream>
 
 #include "deme_solver.hpp"
 
@@ -142,6 +143,45 @@ int main(int argc, char** argv) {
     put(out, "mat_Crr", f.mat_Crr);
     put(out, "family_masks", f.family_masks);
     put(out, "prescriptions", f.prescriptions);
+    {
+        // CSV output of the initial state (every column), for comparison with the Python writers
+        OwnerState st;
+        st.voxel = f.voxel;
+        st.locX = f.locX;
+        st.locY = f.locY;
+        st.locZ = f.locZ;
+        st.oriQw = f.oriQw;
+        st.oriQx = f.oriQx;
+        st.oriQy = f.oriQy;
+        st.oriQz = f.oriQz;
+        st.vX = f.vX;
+        st.vY = f.vY;
+        st.vZ = f.vZ;
+        st.family = f.family;
+        const unsigned all = OUTPUT_CONTENT::ABSV | OUTPUT_CONTENT::VEL | OUTPUT_CONTENT::FAMILY;
+        std::ostringstream sph, clu;
+        write_sphere_csv(sph, f, st, all, {3});
+        write_clump_csv(clu, f, st, all);
+        const std::string a = sph.str(), b = clu.str();
+        put(out, "csv_spheres", a.data(), a.size());
+        put(out, "csv_clumps", b.data(), b.size());
+        // a contact file from a synthetic list: two sphere pairs and one sphere--plane contact
+        const std::vector<uint32_t> idA{0, 1, 2}, idB{1, 3, 0};
+        const std::vector<uint8_t> type{DEME_SPHERE_SPHERE_CONTACT, DEME_SPHERE_SPHERE_CONTACT,
+                                        DEME_SPHERE_PLANE_CONTACT};
+        std::vector<float> F(9), T(9), P(9);
+        for (int i = 0; i < 9; i++) {
+            F[i] = 0.5f * (float)(i + 1) - 1.25f;
+            T[i] = 0.01f * (float)(i * i);
+            P[i] = 1e-3f * (float)(i % 3 + 1) * (i % 2 ? -1.f : 1.f);
+        }
+        std::ostringstream cnt;
+        write_contact_csv(cnt, f, st, idA, idB, type, F, T, P,
+                          CNT_OUTPUT_CONTENT::FORCE | CNT_OUTPUT_CONTENT::POINT | CNT_OUTPUT_CONTENT::NORMAL |
+                              CNT_OUTPUT_CONTENT::TORQUE_ONLY_FORCE);
+        const std::string c = cnt.str();
+        put(out, "csv_contacts", c.data(), c.size());
+    }
     if (argc == 4) {
         const int steps = std::atoi(argv[3]);
         s.Initialize();  // flattens again: use the new FlatScene from here on
