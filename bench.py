@@ -550,11 +550,23 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(args)
-    shell = shell_drum_measure(args, stream) if (rank == 0 and not args.no_shell) else None
-    hopper = hopper_measure(args, stream) if (rank == 0 and not args.no_hopper) else None
-    small = small_scene_measure(args, stream) if (rank == 0 and not args.no_small) else None
-    adj = None if args.no_adjoint else adjoint_measure(args, stream)
-    batched = None if args.no_batched else batched_measure(args, stream, rank, world, dist)
+    def clocked(fn):
+        """Runs a section with the SM clocks and throttle reasons sampled during it."""
+        sampler = ClockSampler(local_rank)
+        sampler.start()
+        sampler.wait_first()
+        out = fn()
+        c = sampler.stop()
+        if isinstance(out, dict):
+            out["clocks"] = c
+        return out
+
+    # the adjoint and batched targets first, before the long hopper run heats the GPU
+    adj = None if args.no_adjoint else clocked(lambda: adjoint_measure(args, stream))
+    batched = None if args.no_batched else clocked(lambda: batched_measure(args, stream, rank, world, dist))
+    shell = clocked(lambda: shell_drum_measure(args, stream)) if (rank == 0 and not args.no_shell) else None
+    hopper = clocked(lambda: hopper_measure(args, stream)) if (rank == 0 and not args.no_hopper) else None
+    small = clocked(lambda: small_scene_measure(args, stream)) if (rank == 0 and not args.no_small) else None
 
     if rank == 0:
         line = {
