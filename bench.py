@@ -378,6 +378,7 @@ def main():
     ap.add_argument("--no-hopper", action="store_true", help="skip the hopper run (detection every 5 steps, two streams)")
     ap.add_argument("--no-small", action="store_true", help="skip the small-scene run (step by step against graphs)")
     ap.add_argument("--autotune", type=int, default=1, help="1: pick the search shape with deme_autotune (untimed)")
+    ap.add_argument("--graph", type=int, default=1, help="1: replay whole steps from CUDA graphs (deme_set_graph)")
     ap.add_argument("--small-steps", type=int, default=5000)
     ap.add_argument("--hopper-spheres", type=int, default=4_000_000)
     ap.add_argument("--hopper-steps", type=int, default=500)
@@ -466,6 +467,8 @@ def main():
         np.savez(args.save_state, **{"st_" + k: v for k, v in st.items() if not k.startswith("a")},
                  **{"c_" + k: c[k] for k in ("idA", "idB", "type", "wildcards")})
 
+    if args.graph:
+        s.set_graph(True)  # whole steps replayed from CUDA graphs (no host synchronisation inside a step)
     tuning = None
     if args.autotune:
         # untimed: time every search shape on a few steps from the prepared state, keep the fastest, restore the state
@@ -583,7 +586,7 @@ def main():
                                         f"dt {args.settle_dt:g} + {args.calm_steps} steps at dt {dt_work:g} "
                                         f"(untimed, {prep_s:.1f} s)",
                        "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}",
-                       "search_shape": tuning},
+                       "search_shape": tuning, "cuda_graphs": bool(args.graph)},
             "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": C.sizeof(capi.FamilyPrescription),
                     "d2h_bytes_per_step": 8},

@@ -56,6 +56,7 @@ int32_t read_device_errors(deme_handle* h) {
         cudaMemcpy(w, h->dErr, sizeof(w), cudaMemcpyDeviceToHost);
         h->err = "device error word " + std::to_string(e) +
                  ((e & ERR_SORT_LOOKBACK_TIMEOUT) ? " (radix sort look-back timed out)" : "") +
+                ((e & ERR_SCAN_LOOKBACK_TIMEOUT) ? " (scan look-back timed out)" : "") +
                  ((e & ERR_CONTACT_CAPACITY) ? " (contact capacity exceeded)" : "") +
                  ((e & ERR_SEGMENT_TOO_LONG) ? " (contact segment mismatch)" : "") +
                  ((e & ERR_INDEX) ? " (index out of range at site " + std::to_string(w[1]) + ": " +
@@ -63,7 +64,7 @@ int32_t read_device_errors(deme_handle* h) {
                                   : "");
         *h->hErr = 0;
         cudaMemsetAsync(h->dErr, 0, 4 * sizeof(uint32_t), h->st_dt);
-        return (e & ERR_SORT_LOOKBACK_TIMEOUT) ? DEME_ERR_TIMEOUT : DEME_ERR_OVERFLOW;
+        return (e & (ERR_SORT_LOOKBACK_TIMEOUT | ERR_SCAN_LOOKBACK_TIMEOUT)) ? DEME_ERR_TIMEOUT : DEME_ERR_OVERFLOW;
     }
     return DEME_OK;
 }
@@ -463,7 +464,8 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
         CUDA_TRY(h, cudaMemset(h->lists[b].dN, 0, sizeof(uint32_t)));
         TRY(ensure_list(h, h->lists[b], std::max<uint32_t>(1024u, 4u * nS)));
     }
-    TRY(ensure_scratch(h, std::max(radix_sort_scratch_bytes(nS), scan_scratch_bytes(std::max(h->nCells + 1, nS + 1)))));
+    TRY(ensure_scratch(h, std::max({radix_sort_scratch_bytes(nS), scan_scratch_bytes(std::max(h->nCells + 1, nS + 1)),
+                                    scan_onepass_scratch_bytes(std::max(h->nCells + 1, nS + 1))})));
     TRY(dalloc_n(h, &h->dTotal, 4));
     TRY(dalloc_n(h, &h->dErr, 4));
     h->k.err = h->dErr;
@@ -508,6 +510,7 @@ void deme_destroy(deme_handle* h) {
         if (e) cudaEventDestroy(e);
     for (cudaGraphExec_t g : h->graphExec)
         if (g) cudaGraphExecDestroy(g);
+    if (h->hWindows) cudaFreeHost(h->hWindows);
     if (h->own_dt) cudaStreamDestroy(h->own_dt);
     if (h->own_kt) cudaStreamDestroy(h->own_kt);
     release_user_force_model(h->userForce);
@@ -567,7 +570,7 @@ static int32_t cd_search(deme_handle* h, const StateView& s, AnalPlaced* anal, c
     launch_place_anal(k, s, h->analRaw, anal, h->nA, st);
     CUDA_TRY(h, cudaMemsetAsync(cd.cellCount, 0, ((size_t)h->nCells + 1) * sizeof(uint32_t), st));
     launch_sphere_prep(k, s, cd, st);
-    exclusive_scan_u32(cd.cellCount, h->nCells + 1, cd.cellStart, nullptr, h->scratch, st);
+    exclusive_scan_u32_onepass(cd.cellCount, h->nCells + 1, cd.cellStart, nullptr, h->scratch, h->dErr, st);
     if (h->useOnesweep)
         radix_sort_pairs(cd.cellKey, cd.idSeq, cd.keySorted, cd.idSorted, h->nS, h->cellBits, h->scratch, h->dErr, st);
     else
@@ -579,7 +582,7 @@ static int32_t cd_search(deme_handle* h, const StateView& s, AnalPlaced* anal, c
     launch_pair_find(k, s, cd, h->candCap, h->findShape, st);
     launch_pair_overflow(k, s, cd, h->candCap, st);
     TRY(check_launch(h, "contact search"));
-    exclusive_scan_u32(cd.cnt, h->nS + 1, nb.off, nb.dN, h->scratch, st);
+    exclusive_scan_u32_onepass(cd.cnt, h->nS + 1, nb.off, nb.dN, h->scratch, h->dErr, st);
     if (hCnt) {
         CUDA_TRY(h, cudaMemcpyAsync(hCnt + 1, cd.counters, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         CUDA_TRY(h, cudaMemcpyAsync(hCnt, nb.dN, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
@@ -804,8 +807,10 @@ static int32_t step_plain(deme_handle* h) {
 // With deme_set_graph, a window of cd_update_freq steps (a detection, then forces and integration each step) is
 // recorded once into a CUDA graph and replayed.  Nothing in a window reads the device from the host: the launches
 // cover the lists' capacities and the kernels read the counts the scans left on the device.  The capacities are
-// fixed before recording with headroom; a window whose lists or pair pool outgrow them sets the device error word,
-// and the batch of windows is then rolled back to a checkpoint and redone step by step (which grows the buffers).
+// fixed before recording with headroom; a window whose lists or pair pool outgrow them sets the device error word.
+// From then on every force, history and integration kernel of the batch returns at once, so the state stays that
+// of the last completed window (each window ends by counting itself done when the error word is clear), and the
+// host redoes the remaining steps one by one, which grows the buffers.
 
 static std::vector<uint8_t> graph_key(const deme_handle* h) {
     std::vector<uint8_t> key;
@@ -837,16 +842,21 @@ static std::vector<uint8_t> graph_key(const deme_handle* h) {
     return key;
 }
 
-// Capacities a window needs, fixed before recording: both lists and the pair pool at 1.5 times the current count
-// (at least twice the sphere count), per-contact outputs and wall partials for the list capacity.
+// Capacities a window needs, fixed before recording: both lists and the pair pool at 1.25 times the current count
+// plus 4,096 (twice the sphere count before the first detection), per-contact outputs and wall partials for the
+// list capacity.  A window that outgrows them is redone step by step, which grows them.
 static int32_t graph_prepare(deme_handle* h) {
     TRY(refresh_count(h));
     const uint32_t n = h->nContacts;
-    const uint64_t want64 = std::max<uint64_t>((uint64_t)n + n / 2 + 4096u, 2ull * h->nS);
+    const uint64_t want64 = std::max<uint64_t>((uint64_t)n + n / 4 + 4096u, h->everDetected ? 0ull : 2ull * h->nS);
     const uint32_t want = (uint32_t)std::min<uint64_t>(want64, 0xF0000000ull);
     TRY(ensure_list_keep(h, h->lists[h->cur], want, n, h->st_dt));
     TRY(ensure_list(h, h->lists[h->cur ^ 1], want));
-    TRY(ensure_cand(h, std::max<uint32_t>(want, h->hTotal[1] + h->hTotal[1] / 2)));
+    TRY(ensure_cand(h, std::max<uint32_t>(want, h->hTotal[1] + h->hTotal[1] / 4 + 4096u)));
+    if (!h->dWindows) {
+        TRY(dalloc_n(h, &h->dWindows, 1));
+        CUDA_TRY(h, cudaMallocHost(&h->hWindows, 2 * sizeof(uint32_t)));
+    }
     const uint32_t cap = std::max(h->lists[0].cap, h->lists[1].cap);
     if (h->keepOutputs) TRY(ensure_outputs(h, cap));
     const uint32_t nAO = h->nO - h->nClumps;
@@ -879,6 +889,7 @@ static int32_t graph_capture(deme_handle* h, int p) {
         if (st == DEME_OK) st = deme_compute_forces(h);
         if (st == DEME_OK) st = deme_integrate(h);
     }
+    if (st == DEME_OK) launch_window_done(h->dErr, h->dWindows, h->st_dt);
     h->capturing = false;
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(h->st_dt, &g);
@@ -918,30 +929,37 @@ static int32_t step_graph(deme_handle* h, int32_t n_steps) {
     const int32_t windows = n_steps / f;
     if (windows > 0) {
         TRY(graph_prepare(h));
-        TRY(save_checkpoint(h, h->graphCkpt));
         const int cur0 = h->cur;
+        const int64_t steps0 = h->steps;
+        const double t0 = h->t;
+        CUDA_TRY(h, cudaMemsetAsync(h->dWindows, 0, sizeof(uint32_t), h->st_dt));
         for (int32_t w = 0; w < windows; w++) {
             const int p = h->cur;
             if (!h->graphExec[p] || h->graphKey[p] != graph_key(h)) TRY(graph_capture(h, p));
             CUDA_TRY(h, cudaGraphLaunch(h->graphExec[p], h->st_dt));
             h->cur ^= 1;
             h->steps += f;
-            h->t += (double)h->k.h * f;
+            for (int i = 0; i < f; i++) h->t += (double)h->k.h;  // as deme_integrate adds it, step by step
             h->countStale = true;
             h->outsValid = h->keepOutputs;
             h->everDetected = true;
             h->graphReplays++;
         }
-        // a device error inside the replays (a list or the pair pool outgrew its capacity) voids them
-        CUDA_TRY(h, cudaMemcpyAsync(h->hErr, h->dErr, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->st_dt));
+        CUDA_TRY(h, cudaMemcpyAsync(h->hWindows, h->dWindows, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->st_dt));
+        CUDA_TRY(h, cudaMemcpyAsync(h->hWindows + 1, h->dErr, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->st_dt));
         CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
-        if (*h->hErr) {
-            *h->hErr = 0;
+        if (h->hWindows[1]) {
+            // a list or the pair pool outgrew its capacity in window `done`: the state and the list in use are those
+            // its detection started from; redo the rest step by step
+            const int32_t done = (int32_t)h->hWindows[0];
             CUDA_TRY(h, cudaMemset(h->dErr, 0, 4 * sizeof(uint32_t)));
-            h->cur = cur0;
-            TRY(restore_checkpoint(h, h->graphCkpt));
+            h->cur = cur0 ^ (done & 1);
+            h->steps = steps0 + (int64_t)done * f;
+            h->t = t0;
+            for (int32_t i = 0; i < done * f; i++) h->t += (double)h->k.h;
+            h->outsValid = false;
             h->graphRollbacks++;
-            for (int32_t i = 0; i < windows * f; i++) TRY(step_plain(h));
+            for (int32_t i = 0; i < (windows - done) * f; i++) TRY(step_plain(h));
         }
         n_steps -= windows * f;
     }

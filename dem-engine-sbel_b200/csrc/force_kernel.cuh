@@ -21,6 +21,12 @@ constexpr uint32_t kForceThreads = DEME_FORCE_THREADS;
 template <bool kStore>
 __global__ void __launch_bounds__(kForceThreads, DEME_FORCE_MIN_BLOCKS) k_force(SimConsts k, StateView s, ContactView c, uint32_t n, bool has_hist,
                                                ContactOutputs out, AnalAccum aa) {
+    // a device error earlier in the step (a list or pool outgrew its capacity inside a replayed graph) voids the
+    // step: nothing is written, and the host redoes it from the untouched state
+    if (__syncthreads_or(threadIdx.x == 0 && *k.err != 0u)) return;
+    // blocks past the count (a launch that covers the list's capacity) have nothing to do; k_anal_reduce reads the
+    // same count and skips their partials
+    if (c.dN && blockIdx.x * blockDim.x >= min(n, *c.dN)) return;
     // analytical owners (walls) collect their reactions block-locally, then one fixed-order reduction
     extern __shared__ float s_anal[];  // 6 floats per analytical owner
     const bool partials = aa.nAO && !aa.direct;

@@ -113,7 +113,8 @@ struct deme_handle {
     bool countStale = false;  // the list in use came out of a graph replay: its count is on the device only
     cudaGraphExec_t graphExec[2] = {nullptr, nullptr};
     std::vector<uint8_t> graphKey[2];
-    Checkpoint graphCkpt;     // state and list at the start of a replayed batch, for rollback
+    uint32_t* dWindows = nullptr;  // windows of a replayed batch that completed without a device error
+    uint32_t* hWindows = nullptr;  // pinned: that count, then the error word
     int64_t graphReplays = 0, graphRollbacks = 0;
     int32_t cdLag = 0;
     bool cdPending = false;

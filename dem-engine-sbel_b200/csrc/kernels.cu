@@ -642,6 +642,7 @@ void launch_pair_assemble(const SimConsts& k, const StateView& s, const CDView& 
 __global__ void __launch_bounds__(256) k_history(uint32_t n, ContactView cur, ContactView prev, bool has_hist,
                                                  uint32_t nS, uint32_t prevN, uint32_t* err) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (*err != 0u) return;  // a voided step (see k_force)
     // the counts on the device bound the launch (it may cover a list's capacity)
     if (cur.dN) n = min(n, *cur.dN);
     if (prev.dN) prevN = *prev.dN;
@@ -693,8 +694,12 @@ void launch_count_by_sphere(const uint32_t* idA, uint32_t n, uint32_t* cnt, cuda
 // ------------------------------------------------------------------------------------------------------------
 // Fused force + collection kernel.
 // Sum the per-block partials of each analytical owner in block order (deterministic) into its accumulators.
-__global__ void k_anal_reduce(AnalAccum aa, uint32_t nBlocks, float4* acc, float4* alpha) {
+__global__ void k_anal_reduce(AnalAccum aa, uint32_t nBlocks, float4* acc, float4* alpha, const uint32_t* err,
+                              const uint32_t* dN) {
     __shared__ float sh[256];
+    if (__syncthreads_or(threadIdx.x == 0 && *err != 0u)) return;  // a voided step (see k_force)
+    // only the force blocks that held contacts wrote partials
+    if (dN) nBlocks = min(nBlocks, (*dN + kForceThreads - 1) / kForceThreads);
     const uint32_t slot = blockIdx.x / 6u, comp = blockIdx.x % 6u;
     float v = 0.f;
     for (uint32_t b = threadIdx.x; b < nBlocks; b += blockDim.x) v += aa.partial[(size_t)b * 6u * aa.nAO + 6u * slot + comp];
@@ -738,17 +743,27 @@ void launch_force(const SimConsts& k, const StateView& s, const ContactView& c, 
     }
     if (partials) {
         ProfScope prof_(KID_OTHER, st);
-        k_anal_reduce<<<6u * aa.nAO, 256, 0, st>>>(aa, nb, s.acc, s.alpha);
+        k_anal_reduce<<<6u * aa.nAO, 256, 0, st>>>(aa, nb, s.acc, s.alpha, k.err, c.dN);
     }
 }
 
 uint32_t force_blocks(uint32_t n) { return blocks_for(n, kForceThreads); }
+
+// End of a replayed window: counts the windows that completed without a device error.
+__global__ void k_window_done(const uint32_t* err, uint32_t* done) {
+    if (*err == 0u) atomicAdd(done, 1u);
+}
+void launch_window_done(const uint32_t* err, uint32_t* done, cudaStream_t st) {
+    ProfScope prof_(KID_OTHER, st);
+    k_window_done<<<1, 1, 0, st>>>(err, done);
+}
 
 // ------------------------------------------------------------------------------------------------------------
 // integrateOwners (src/kernel/DEMIntegrationKernels.cu:46-179) with the constant prescription table.
 __global__ void __launch_bounds__(256) k_integrate(SimConsts k, StateView s) {
     const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= k.n_owners) return;
+    if (*k.err != 0u) return;  // a voided step (see k_force) leaves the state as it was
     ushort4 l = s.loc[o];
     const Prescription pr = s.presc[l.w];
     float4 v = s.vel[o];

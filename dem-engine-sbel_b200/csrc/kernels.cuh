@@ -119,6 +119,7 @@ struct UserForceKernel;
 void launch_force(const SimConsts& k, const StateView& s, const ContactView& c, uint32_t n, bool has_hist,
                   const ContactOutputs* out, const AnalAccum& aa, const UserForceKernel* user, cudaStream_t st);
 uint32_t force_blocks(uint32_t n);
+void launch_window_done(const uint32_t* err, uint32_t* done, cudaStream_t st);
 void launch_integrate(const SimConsts& k, const StateView& s, cudaStream_t st);
 void launch_kinetic_energy(const SimConsts& k, const StateView& s, uint32_t n_clumps, double* out, cudaStream_t st);
 

@@ -174,6 +174,117 @@ static void exclusive_scan_impl(const T* in, uint32_t n, uint32_t* out, uint32_t
 void exclusive_scan_u32(const uint32_t* in, uint32_t n, uint32_t* out, uint32_t* total, void* scratch, cudaStream_t st) {
     exclusive_scan_impl<uint32_t>(in, n, out, total, static_cast<uint8_t*>(scratch), st);
 }
+// ---------------------------------------------------------- single-pass scan ----
+// Exclusive scan of uint32 in one pass over the data: tiles take ids in launch order from a ticket, publish their
+// sum, and look back at their predecessors' published sums (a warp reads 32 at a time) until one carries its
+// inclusive prefix, then publish their own inclusive prefix and write their outputs.  Reads the input once and
+// writes the output once.  Each status word is (flag << 32) | value, flag 1 = tile sum, 2 = inclusive prefix; a
+// wait that outlasts kScanSpinLimit polls sets ERR_SCAN_LOOKBACK_TIMEOUT and ends (the results are then void).
+constexpr uint32_t kScanSpinLimit = 1u << 24;
+
+__device__ __forceinline__ void scan_publish(unsigned long long* w, uint32_t flag, uint32_t v) {
+    atomicExch(w, ((unsigned long long)flag << 32) | v);
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_onepass_kernel(const uint32_t* in, uint32_t n, uint32_t* out,
+                                                                    uint32_t* total_out, unsigned long long* status,
+                                                                    uint32_t* ticket, uint32_t nTiles, uint32_t* err) {
+    __shared__ uint32_t sh[kScanThreads / 32];
+    __shared__ uint32_t s_tile, s_prefix;
+    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const size_t base = (size_t)tile * kScanTile + (size_t)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    load_items<uint32_t>(in, n, base, v);
+    uint32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) s += v[i];
+    uint32_t total;
+    const uint32_t excl = block_exclusive_scan<uint32_t>(s, sh, total);
+    if (threadIdx.x < 32) {
+        const uint32_t lane = threadIdx.x;
+        uint32_t prefix = 0;
+        if (tile > 0) {
+            if (lane == 0) scan_publish(status + tile, 1u, total);
+            int64_t pos = (int64_t)tile - 1;  // lane l reads tile pos - l
+            uint32_t spins = 0;
+            while (true) {
+                const int64_t j = pos - (int64_t)lane;
+                const unsigned long long w =
+                    j >= 0 ? *reinterpret_cast<volatile unsigned long long*>(status + j) : (2ull << 32);
+                const uint32_t flag = (uint32_t)(w >> 32);
+                const uint32_t incl = __ballot_sync(0xffffffffu, flag == 2u);
+                const uint32_t zero = __ballot_sync(0xffffffffu, flag == 0u);
+                const int first = incl ? __ffs(incl) - 1 : 32;  // nearest predecessor with its inclusive prefix
+                const uint32_t need = first == 32 ? 0xffffffffu : (first == 31 ? 0xffffffffu : ((2u << first) - 1u));
+                if (zero & need) {
+                    if (++spins > kScanSpinLimit) {
+                        if (lane == 0) atomicOr(err, ERR_SCAN_LOOKBACK_TIMEOUT);
+                        break;
+                    }
+                    continue;
+                }
+                uint32_t c = (int)lane <= first ? (uint32_t)w : 0u;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+                prefix += c;
+                if (first < 32) break;
+                pos -= 32;
+            }
+        }
+        if (lane == 0) {
+            scan_publish(status + tile, 2u, prefix + total);
+            s_prefix = prefix;
+        }
+    }
+    __syncthreads();
+    uint32_t run = s_prefix + excl;
+    if (base + kScanItems <= n && ((reinterpret_cast<uintptr_t>(out + base) & 15u) == 0)) {
+        uint4* p = reinterpret_cast<uint4*>(out + base);
+#pragma unroll
+        for (int q = 0; q < kScanItems / 4; q++) {
+            uint4 t;
+            t.x = run;
+            run += v[4 * q];
+            t.y = run;
+            run += v[4 * q + 1];
+            t.z = run;
+            run += v[4 * q + 2];
+            t.w = run;
+            run += v[4 * q + 3];
+            p[q] = t;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < kScanItems; i++) {
+            const size_t idx = base + i;
+            if (idx < n) out[idx] = run;
+            run += v[i];
+        }
+    }
+    if (total_out && tile == nTiles - 1 && threadIdx.x == kScanThreads - 1) *total_out = run;
+}
+
+size_t scan_onepass_scratch_bytes(uint32_t n) {
+    const size_t tiles = ((size_t)n + kScanTile - 1) / kScanTile;
+    return (tiles + 2) * sizeof(unsigned long long) + 256;
+}
+
+void exclusive_scan_u32_onepass(const uint32_t* in, uint32_t n, uint32_t* out, uint32_t* total, void* scratch,
+                                uint32_t* err, cudaStream_t st) {
+    if (n == 0) {
+        if (total) cudaMemsetAsync(total, 0, sizeof(uint32_t), st);
+        return;
+    }
+    const uint32_t nTiles = (n + kScanTile - 1) / kScanTile;
+    unsigned long long* status = static_cast<unsigned long long*>(scratch);
+    uint32_t* ticket = reinterpret_cast<uint32_t*>(status + nTiles);
+    cudaMemsetAsync(status, 0, ((size_t)nTiles + 1) * sizeof(unsigned long long), st);
+    ProfScope prof_(KID_SCAN, st);
+    scan_onepass_kernel<<<nTiles, kScanThreads, 0, st>>>(in, n, out, total, status, ticket, nTiles, err);
+}
+
 void exclusive_scan_u16(const uint16_t* in, uint32_t n, uint32_t* out, uint32_t* total, void* scratch, cudaStream_t st) {
     exclusive_scan_impl<uint16_t>(in, n, out, total, static_cast<uint8_t*>(scratch), st);
 }

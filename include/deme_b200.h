@@ -301,10 +301,11 @@ int32_t deme_set_async_cd(deme_handle* h, int32_t lag);
 /* Whole steps as CUDA graphs (no reference counterpart: its host code launches and synchronises kernel by kernel,
  * src/DEM/dT.cpp:1446-1586).  With enable != 0, deme_step records a window of cd_update_freq steps (one detection,
  * then forces and integration each step) into a CUDA graph once and replays it; nothing in a window waits for the
- * host.  Launches cover the contact lists' capacities, sized before recording at 1.5 times the current count (at
- * least twice the sphere count), and the kernels read the counts on the device.  A replayed batch in which a list
- * or the pair pool outgrew its capacity is rolled back to the checkpoint taken at its start and redone step by step,
- * so results do not depend on the mode.  Steps before the next detection step, and those left after the last whole
+ * host.  Launches cover the contact lists' capacities, sized before recording at 1.25 times the current count
+ * plus 4,096 (twice the sphere count before the first detection), and the kernels read the counts on the device.  A window in which a list or the
+ * pair pool outgrows its capacity sets the device error word, after which every force, history and integration
+ * kernel of the batch returns at once; the host then redoes the remaining steps one by one from the state of the
+ * last completed window, so results do not depend on the mode.  Steps before the next detection step, and those left after the last whole
  * window, run step by step.  A graph is recorded again whenever anything it captured changes (buffers, streams,
  * time step, force model, stored outputs).  Not used with deme_set_async_cd lag > 0 or while per-kernel timing
  * (deme_kernel_timing) is on.  Helps small scenes, whose steps are bound by launch latency. */
