@@ -883,6 +883,7 @@ static int32_t graph_capture(deme_handle* h, int p) {
     const bool outs0 = h->outsValid, stale0 = h->countStale;
     CUDA_TRY(h, cudaStreamBeginCapture(h->st_dt, cudaStreamCaptureModeThreadLocal));
     h->capturing = true;
+    const int64_t launches0 = launch_count();
     int32_t st = DEME_OK;
     for (int i = 0; i < f && st == DEME_OK; i++) {
         if (i == 0) st = cd_sync(h);
@@ -891,6 +892,9 @@ static int32_t graph_capture(deme_handle* h, int p) {
     }
     if (st == DEME_OK) launch_window_done(h->dErr, h->dWindows, h->st_dt);
     h->capturing = false;
+    // recording counted its launches once; the replays add them back each time they run
+    const int64_t recorded = launch_count() - launches0;
+    add_launches(-recorded);
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(h->st_dt, &g);
     h->cur = cur0;
@@ -917,6 +921,7 @@ static int32_t graph_capture(deme_handle* h, int p) {
         return DEME_ERR_CUDA;
     }
     h->graphKey[p] = graph_key(h);
+    h->graphKernels[p] = recorded;
     return DEME_OK;
 }
 
@@ -937,6 +942,7 @@ static int32_t step_graph(deme_handle* h, int32_t n_steps) {
             const int p = h->cur;
             if (!h->graphExec[p] || h->graphKey[p] != graph_key(h)) TRY(graph_capture(h, p));
             CUDA_TRY(h, cudaGraphLaunch(h->graphExec[p], h->st_dt));
+            add_launches(h->graphKernels[p]);
             h->cur ^= 1;
             h->steps += f;
             for (int i = 0; i < f; i++) h->t += (double)h->k.h;  // as deme_integrate adds it, step by step

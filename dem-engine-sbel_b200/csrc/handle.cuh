@@ -112,6 +112,7 @@ struct deme_handle {
     bool capturing = false;   // the step functions are being recorded: no host reads, launches cover capacities
     bool countStale = false;  // the list in use came out of a graph replay: its count is on the device only
     cudaGraphExec_t graphExec[2] = {nullptr, nullptr};
+    int64_t graphKernels[2] = {0, 0};  // kernel launches recorded in each graph
     std::vector<uint8_t> graphKey[2];
     uint32_t* dWindows = nullptr;  // windows of a replayed batch that completed without a device error
     uint32_t* hWindows = nullptr;  // pinned: that count, then the error word

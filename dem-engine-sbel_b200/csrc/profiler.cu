@@ -45,6 +45,8 @@ void prof_end(int id, cudaStream_t st) {
 
 int64_t launch_count() { return g_launches.load(); }
 
+void add_launches(int64_t n) { g_launches += n; }
+
 bool prof_timing() { return g_timing; }
 
 }  // namespace deme_b200

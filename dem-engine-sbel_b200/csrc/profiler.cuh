@@ -30,6 +30,7 @@ const char* kernel_name(int id);
 void prof_begin(int id, cudaStream_t st);
 void prof_end(int id, cudaStream_t st);
 int64_t launch_count();
+void add_launches(int64_t n);  // kernels a replayed CUDA graph ran (recorded once, counted at every replay)
 bool prof_timing();  // per-kernel timing is on (its events are recorded at launch time, so graphs are not used)
 
 struct ProfScope {

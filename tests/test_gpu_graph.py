@@ -52,6 +52,26 @@ def test_graph_replay_equals_step_by_step():
     assert len(g[1]["idA"]) > 0
 
 
+def test_replayed_kernels_are_counted():
+    import ctypes as C
+    from deme_b200 import Solver
+    built = workloads.packed_clumps(n_clumps=300, seed=7, spacing=1.35)  # contacts from the first step on
+    counts = {}
+    for graph in (False, True):
+        s = Solver(built)
+        s.lib.deme_launch_count.restype = C.c_int64
+        if graph:
+            s.set_graph(True)
+        s.step(2)
+        n0 = s.lib.deme_launch_count()
+        s.step(10)
+        s.sync()
+        counts[graph] = s.lib.deme_launch_count() - n0
+        s.close()
+    # a replayed window runs the kernels the step-by-step path launches, plus the one that counts the window
+    assert counts[True] == counts[False] + 10, counts
+
+
 def test_graph_windows_with_detection_every_four_steps():
     built = workloads.hopper(n=20000, seed=5, cd_freq=4, wall_clearance=0.95)
     g = run(built, 42, True, chunks=2)  # 21 steps per call: windows of 4 plus steps outside them
