@@ -514,6 +514,8 @@ void deme_destroy(deme_handle* h) {
     if (h->own_dt) cudaStreamDestroy(h->own_dt);
     if (h->own_kt) cudaStreamDestroy(h->own_kt);
     release_user_force_model(h->userForce);
+    release_family_change_rules(h->famRules);
+    if (h->hTime) cudaFreeHost(h->hTime);
     delete h;
 }
 
@@ -781,6 +783,20 @@ int32_t deme_integrate(deme_handle* h) {
     return DEME_OK;
 }
 
+// ChangeFamilyWhen rules between the forces and the integration of a step (routineChecks, src/DEM/dT.cpp:1434-1444),
+// then the device time advances with the step.
+static int32_t apply_family_rules(deme_handle* h) {
+    if (!h->famRules.kern) return DEME_OK;
+    SimConsts k = h->k;
+    StateView s = h->state_view();
+    const double* t = h->dTime;
+    void* args[] = {&k, &s, &t};
+    CUDA_TRY(h, cudaLaunchKernel((const void*)h->famRules.kern, dim3((h->nO + 255) / 256), dim3(256), args, 0,
+                                 h->st_dt));
+    add_launches(1);
+    return DEME_OK;
+}
+
 // One step launched function by function (DoStepDynamics).
 static int32_t step_plain(deme_handle* h) {
     const int f = h->params.cd_update_freq;
@@ -800,7 +816,10 @@ static int32_t step_plain(deme_handle* h) {
         h->everDetected = true;
     }
     TRY(deme_compute_forces(h));
-    return deme_integrate(h);
+    TRY(apply_family_rules(h));
+    TRY(deme_integrate(h));
+    if (h->famRules.kern) launch_advance_time(h->dTime, h->k.h, h->st_dt);
+    return DEME_OK;
 }
 
 // ------------------------------------------------------------------------------------------ graph replay ----
@@ -837,6 +856,8 @@ static std::vector<uint8_t> graph_key(const deme_handle* h) {
     put(&h->nW, sizeof(h->nW));
     const void* lib = h->userForce.lib;
     put(&lib, sizeof(lib));
+    const void* rules = h->famRules.lib;
+    put(&rules, sizeof(rules));
     put(&h->params.cd_update_freq, sizeof(h->params.cd_update_freq));
     put(&h->findShape, sizeof(h->findShape));
     return key;
@@ -888,7 +909,9 @@ static int32_t graph_capture(deme_handle* h, int p) {
     for (int i = 0; i < f && st == DEME_OK; i++) {
         if (i == 0) st = cd_sync(h);
         if (st == DEME_OK) st = deme_compute_forces(h);
+        if (st == DEME_OK) st = apply_family_rules(h);
         if (st == DEME_OK) st = deme_integrate(h);
+        if (st == DEME_OK && h->famRules.kern) launch_advance_time(h->dTime, h->k.h, h->st_dt);
     }
     if (st == DEME_OK) launch_window_done(h->dErr, h->dWindows, h->st_dt);
     h->capturing = false;
@@ -987,6 +1010,33 @@ int32_t deme_graph_stats(deme_handle* h, int64_t* replays, int64_t* rollbacks) {
     return DEME_OK;
 }
 
+// ------------------------------------------------------------------------------------------ family changes ----
+int32_t deme_set_family_change_rules(deme_handle* h, int32_t n, const uint32_t* from, const uint32_t* to,
+                                     const char* const* conditions) {
+    if (!h || n < 0) return DEME_ERR_INVALID;
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    TRY(cd_finish(h));
+    if (n > 0 && !h->dTime) {
+        TRY(dalloc_n(h, &h->dTime, 1));
+        CUDA_TRY(h, cudaMallocHost(&h->hTime, sizeof(double)));
+    }
+    std::string err;
+    const int32_t rc = compile_family_change_rules(n, from, to, conditions, h->famRules, err);
+    if (rc != DEME_OK) h->err = err;
+    return rc;
+}
+
+int32_t deme_change_family(deme_handle* h, uint32_t from, uint32_t to) {
+    if (!h) return DEME_ERR_INVALID;
+    if (from > 255u || to > 255u) {
+        h->err = "family numbers lie in [0, 255]";
+        return DEME_ERR_INVALID;
+    }
+    TRY(cd_finish(h));
+    launch_change_family(h->loc, h->nO, from, to, h->st_dt);
+    return check_launch(h, "change_family");
+}
+
 // ------------------------------------------------------------------------------------------- search shape ----
 int32_t deme_set_search_shape(deme_handle* h, int32_t shape, float cell_factor) {
     if (!h) return DEME_ERR_INVALID;
@@ -1072,6 +1122,10 @@ int32_t deme_autotune(deme_handle* h, int32_t steps_per_trial, deme_tuning* out)
 
 int32_t deme_step(deme_handle* h, int32_t n_steps) {
     if (!h) return DEME_ERR_INVALID;
+    if (h->famRules.kern) {  // the rules read the time on the device: start it from the host's
+        *h->hTime = h->t;
+        CUDA_TRY(h, cudaMemcpyAsync(h->dTime, h->hTime, sizeof(double), cudaMemcpyHostToDevice, h->st_dt));
+    }
     if (h->useGraph && h->cdLag == 0 && !prof_timing()) {
         TRY(step_graph(h, n_steps));
     } else {

@@ -191,4 +191,114 @@ void release_user_force_model(UserForceKernel& k) {
     k = UserForceKernel{};
 }
 
+namespace {
+// Every whole-word `return` of a condition becomes `shouldMakeChange =` (the reference's replace_pattern).
+std::string returns_to_decision(const std::string& c) {
+    std::string out;
+    size_t i = 0;
+    auto word = [](char ch) { return std::isalnum((unsigned char)ch) || ch == '_'; };
+    while (i < c.size()) {
+        if (c.compare(i, 6, "return") == 0 && (i == 0 || !word(c[i - 1])) && (i + 6 >= c.size() || !word(c[i + 6]))) {
+            out += "shouldMakeChange =";
+            i += 6;
+        } else {
+            out += c[i++];
+        }
+    }
+    return out;
+}
+
+const char* kFamilySource =
+    "#include <stdint.h>\n"
+    "#include \"force_model_api.cuh\"\n"
+    "#include \"family_change_kernel.cuh\"\n";
+}  // namespace
+
+int32_t compile_family_change_rules(int32_t n, const uint32_t* from, const uint32_t* to,
+                                    const char* const* conditions, FamilyChangeKernel& out, std::string& err) {
+    if (n <= 0) {
+        release_family_change_rules(out);
+        return DEME_OK;
+    }
+    std::string inc;
+    for (int32_t i = 0; i < n; i++) {
+        if (!from || !to || !conditions || !conditions[i] || from[i] > 255u || to[i] > 255u) {
+            err = "family change rule " + std::to_string(i) + ": families must lie in [0, 255] and the condition exist";
+            return DEME_ERR_INVALID;
+        }
+        inc += "if (family_code == " + std::to_string(from[i]) + "u) {\nbool shouldMakeChange = false;\n{\n#line 1 \"" +
+               "family_change_rule_" + std::to_string(i) + "\"\n" + returns_to_decision(conditions[i]) +
+               "\n}\nif (shouldMakeChange) newFamily = " + std::to_string(to[i]) + "u;\n}\n";
+    }
+    int dev = 0;
+    cudaDeviceProp prop{};
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+        err = "no current CUDA device";
+        return DEME_ERR_NO_DEVICE;
+    }
+    const std::string arch = "--gpu-architecture=sm_" + std::to_string(prop.major * 10 + prop.minor) +
+                             (prop.major >= 9 ? "a" : "");
+    std::vector<const char*> hnames, htexts;
+    for (const JitHeader& hdr : kJitHeaders) {
+        hnames.push_back(hdr.name);
+        htexts.push_back(hdr.text);
+    }
+    hnames.push_back("stdint.h");
+    htexts.push_back(kStdintStub);
+    hnames.push_back("stddef.h");
+    htexts.push_back(kStddefStub);
+    hnames.push_back("deme_family_change_rules.inc");
+    htexts.push_back(inc.c_str());
+    nvrtcProgram prog = nullptr;
+    if (nvrtcCreateProgram(&prog, kFamilySource, "deme_family_change.cu", (int)hnames.size(), htexts.data(),
+                           hnames.data()) != NVRTC_SUCCESS) {
+        err = "nvrtcCreateProgram failed";
+        return DEME_ERR_NVRTC;
+    }
+    const char* expr = "deme_b200::k_family_change";
+    nvrtcAddNameExpression(prog, expr);
+    const char* opts[] = {arch.c_str(), "--fmad=false", "-std=c++17", "-lineinfo"};
+    const nvrtcResult rc = nvrtcCompileProgram(prog, 4, opts);
+    if (rc != NVRTC_SUCCESS) {
+        size_t logSize = 0;
+        nvrtcGetProgramLogSize(prog, &logSize);
+        std::string log(logSize, '\0');
+        if (logSize) nvrtcGetProgramLog(prog, &log[0]);
+        err = std::string("family change rules did not compile: ") + nvrtcGetErrorString(rc) + "\n" + log;
+        nvrtcDestroyProgram(&prog);
+        return DEME_ERR_NVRTC;
+    }
+    size_t sz = 0;
+    std::vector<char> cubin;
+    std::string lowered;
+    bool ok = nvrtcGetCUBINSize(prog, &sz) == NVRTC_SUCCESS && sz > 0;
+    if (ok) {
+        cubin.resize(sz);
+        ok = nvrtcGetCUBIN(prog, cubin.data()) == NVRTC_SUCCESS;
+    }
+    const char* name = nullptr;
+    ok = ok && nvrtcGetLoweredName(prog, expr, &name) == NVRTC_SUCCESS && name;
+    if (ok) lowered = name;
+    nvrtcDestroyProgram(&prog);
+    if (!ok) {
+        err = "NVRTC produced no loadable image for the family change rules";
+        return DEME_ERR_NVRTC;
+    }
+    FamilyChangeKernel k;
+    if (cudaLibraryLoadData(&k.lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0) != cudaSuccess ||
+        cudaLibraryGetKernel(&k.kern, k.lib, lowered.c_str()) != cudaSuccess) {
+        err = std::string("loading the family change rules failed: ") + cudaGetErrorString(cudaGetLastError());
+        if (k.lib) cudaLibraryUnload(k.lib);
+        return DEME_ERR_CUDA;
+    }
+    release_family_change_rules(out);
+    out = k;
+    return DEME_OK;
+}
+
+void release_family_change_rules(FamilyChangeKernel& k) {
+    if (k.lib) cudaLibraryUnload(k.lib);
+    k = FamilyChangeKernel{};
+}
+
 }  // namespace deme_b200

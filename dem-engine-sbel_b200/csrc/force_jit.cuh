@@ -23,4 +23,15 @@ int32_t compile_user_force_model(const char* model, const char* const* names, in
                                  std::string& err);
 void release_user_force_model(UserForceKernel& k);
 
+// Family-change rules (ChangeFamilyWhen) compiled into k_family_change (family_change_kernel.cuh).
+struct FamilyChangeKernel {
+    cudaLibrary_t lib = nullptr;
+    cudaKernel_t kern = nullptr;
+};
+// n rules: owners of family from[i] move to family to[i] when conditions[i] (a code block whose `return` gives the
+// decision) holds.  On failure returns a DEME_ERR_* code and fills `err` (the compiler log).
+int32_t compile_family_change_rules(int32_t n, const uint32_t* from, const uint32_t* to,
+                                    const char* const* conditions, FamilyChangeKernel& out, std::string& err);
+void release_family_change_rules(FamilyChangeKernel& k);
+
 }  // namespace deme_b200

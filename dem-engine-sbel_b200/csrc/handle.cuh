@@ -99,6 +99,9 @@ struct deme_handle {
     int64_t steps = 0;
     std::vector<void*> allocs;
     UserForceKernel userForce;  // a compiled force-model string, when one is set
+    FamilyChangeKernel famRules;  // compiled ChangeFamilyWhen rules, when some are set
+    double* dTime = nullptr;      // the time on the device (the rules read it), advanced once per step
+    double* hTime = nullptr;      // pinned copy the host writes before each deme_step
     AdjointTape* adj = nullptr;  // checkpoints of deme_adjoint_record
     // Asynchronous contact detection (kT on st_kt, dT on st_dt).  With cdLag > 0 a detection due at step k runs on
     // kT from a snapshot of the owner poses of step k while dT keeps stepping with the current list, and dT adopts

@@ -749,6 +749,29 @@ void launch_force(const SimConsts& k, const StateView& s, const ContactView& c, 
 
 uint32_t force_blocks(uint32_t n) { return blocks_for(n, kForceThreads); }
 
+// ChangeFamily (src/DEM/APIPublic.cpp:184-208): every owner of family `from` moves to family `to`.
+__global__ void k_change_family(ushort4* loc, uint32_t n, uint32_t from, uint32_t to) {
+    const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    ushort4 l = loc[o];
+    if (l.w == from) {
+        l.w = (unsigned short)to;
+        loc[o] = l;
+    }
+}
+void launch_change_family(ushort4* loc, uint32_t n, uint32_t from, uint32_t to, cudaStream_t st) {
+    if (!n) return;
+    ProfScope prof_(KID_OTHER, st);
+    k_change_family<<<blocks_for(n, 256), 256, 0, st>>>(loc, n, from, to);
+}
+
+// The simulation time on the device (read by the family-change rules), advanced once per step.
+__global__ void k_advance_time(double* time, float h) { *time += (double)h; }
+void launch_advance_time(double* time, float h, cudaStream_t st) {
+    ProfScope prof_(KID_OTHER, st);
+    k_advance_time<<<1, 1, 0, st>>>(time, h);
+}
+
 // End of a replayed window: counts the windows that completed without a device error.
 __global__ void k_window_done(const uint32_t* err, uint32_t* done) {
     if (*err == 0u) atomicAdd(done, 1u);

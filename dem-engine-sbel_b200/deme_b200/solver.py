@@ -274,6 +274,21 @@ class Solver(HandleSolver):
         self._check(self.lib.deme_graph_stats(self.h, C.byref(r), C.byref(b)), "graph_stats")
         return int(r.value), int(b.value)
 
+    def change_family(self, family_from: int, family_to: int):
+        """ChangeFamily: every owner of one family moves to another now."""
+        self.lib.deme_change_family.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
+        self._check(self.lib.deme_change_family(self.h, int(family_from), int(family_to)), "change_family")
+
+    def set_family_change_rules(self, rules):
+        """ChangeFamilyWhen rules, a list of (from, to, condition) applied every step (see
+        deme_set_family_change_rules); an empty list removes them."""
+        n = len(rules)
+        fr = (C.c_uint32 * max(n, 1))(*[int(r[0]) for r in rules])
+        to = (C.c_uint32 * max(n, 1))(*[int(r[1]) for r in rules])
+        cond = (C.c_char_p * max(n, 1))(*[r[2].encode() for r in rules])
+        self.lib.deme_set_family_change_rules.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
+        self._check(self.lib.deme_set_family_change_rules(self.h, n, fr, to, cond), "set_family_change_rules")
+
     def set_search_shape(self, shape: int, cell_factor: float = 1.0):
         """Block shape of the pooled pair search and search-cell scale (see deme_set_search_shape)."""
         self.lib.deme_set_search_shape.argtypes = [C.c_void_p, C.c_int32, C.c_float]

@@ -298,6 +298,19 @@ int32_t deme_set_streams(deme_handle* h, void* kT_stream, void* dT_stream);
  * once.  Uploading state or contacts drops a pending detection; deme_detect_contacts and deme_sync adopt it first. */
 int32_t deme_set_async_cd(deme_handle* h, int32_t lag);
 
+/* Family changes.  deme_change_family moves every owner of family `from` to family `to` now (ChangeFamily,
+ * src/DEM/APIPublic.cpp:184-208).  deme_set_family_change_rules compiles n rules with NVRTC (ChangeFamilyWhen,
+ * src/DEM/APIPublic.cpp:167-182, applied by applyFamilyChanges, src/kernel/DEMModeratorKernels.cu:9-38): at every
+ * step, after the forces and before the integration, an owner of family from[i] moves to to[i] when conditions[i]
+ * returns true.  A condition is a code block that ends with `return <bool>;` and may use pos (double3, the owner's
+ * position from the domain's lower corner), vel, acc (float3), mass, family_code, t (time) and h (step), with the
+ * float3 helpers force models have.  Rules test the family the owner had at the start of the step; when several
+ * apply, the last one wins.  n = 0 removes the rules.  A rule that does not compile returns DEME_ERR_NVRTC with the
+ * log. */
+int32_t deme_change_family(deme_handle* h, uint32_t from, uint32_t to);
+int32_t deme_set_family_change_rules(deme_handle* h, int32_t n, const uint32_t* from, const uint32_t* to,
+                                     const char* const* conditions);
+
 /* Whole steps as CUDA graphs (no reference counterpart: its host code launches and synchronises kernel by kernel,
  * src/DEM/dT.cpp:1446-1586).  With enable != 0, deme_step records a window of cd_update_freq steps (one detection,
  * then forces and integration each step) into a CUDA graph once and replays it; nothing in a window waits for the

@@ -491,6 +491,13 @@ class DEMSolver {
         presc.push_back(p);
     }
 
+    // ---- family changes (ChangeFamilyWhen / ChangeFamily, src/DEM/API.h:282-286) ----
+    /* Rules are compiled at Initialize and applied every step after the forces. */
+    void ChangeFamilyWhen(unsigned from, unsigned to, const std::string& condition) {
+        fam_rules.push_back({from, to, condition});
+    }
+    void ChangeFamily(unsigned from, unsigned to) { check(deme_change_family(h, from, to)); }
+
     // ---- force model ----
     std::shared_ptr<DEMForceModel> UseFrictionalHertzianModel() {
         force_model = std::make_shared<DEMForceModel>();
@@ -533,6 +540,16 @@ class DEMSolver {
             throw std::runtime_error(std::string("Initialize: ") + deme_status_string(st) + ": " + msg);
         }
         if (cnt_out_content != CNT_OUTPUT_CONTENT::OWNERS) check(deme_keep_contact_forces(h, 1));
+        if (!fam_rules.empty()) {
+            std::vector<uint32_t> from, to;
+            std::vector<const char*> cond;
+            for (const auto& r : fam_rules) {
+                from.push_back(r.from);
+                to.push_back(r.to);
+                cond.push_back(r.condition.c_str());
+            }
+            check(deme_set_family_change_rules(h, (int32_t)fam_rules.size(), from.data(), to.data(), cond.data()));
+        }
         if (force_model && force_model->custom) {
             std::vector<const char*> names;
             for (const auto& n : force_model->m_contact_wildcards) names.push_back(n.c_str());
@@ -1063,6 +1080,11 @@ class DEMSolver {
     std::shared_ptr<DEMForceModel> force_model;
     std::unique_ptr<FlatScene> flat;
     deme_handle* h = nullptr;
+    struct FamilyRule {
+        unsigned from, to;
+        std::string condition;
+    };
+    std::vector<FamilyRule> fam_rules;
     unsigned out_content = OUTPUT_CONTENT::QUAT | OUTPUT_CONTENT::ABSV;
     unsigned cnt_out_content = CNT_OUTPUT_CONTENT::FORCE | CNT_OUTPUT_CONTENT::POINT;
     std::set<unsigned> no_output;
