@@ -612,14 +612,34 @@ __global__ void __launch_bounds__(256) k_pair_assemble(SimConsts k, StateView s,
     }
     uint32_t* seg = c.idB + anEnd;
     const uint32_t n = end - anEnd;
-    for (uint32_t i = 1; i < n; i++) {
-        const uint32_t v = seg[i];
-        uint32_t j = i;
-        while (j > 0 && seg[j - 1] > v) {
-            seg[j] = seg[j - 1];
-            j--;
+    constexpr uint32_t kReg = 8;
+    if (n <= kReg) {
+        // short segments (nearly all): loaded at once, sorted in registers, stored at once
+        uint32_t v[kReg];
+#pragma unroll
+        for (uint32_t i = 0; i < kReg; i++) v[i] = i < n ? seg[i] : 0xFFFFFFFFu;
+#pragma unroll
+        for (uint32_t i = 1; i < kReg; i++) {
+#pragma unroll
+            for (uint32_t j = i; j > 0; j--) {
+                const uint32_t a = v[j - 1], b = v[j];
+                v[j - 1] = min(a, b);
+                v[j] = max(a, b);
+            }
         }
-        seg[j] = v;
+#pragma unroll
+        for (uint32_t i = 0; i < kReg; i++)
+            if (i < n) seg[i] = v[i];
+    } else {
+        for (uint32_t i = 1; i < n; i++) {
+            const uint32_t v = seg[i];
+            uint32_t j = i;
+            while (j > 0 && seg[j - 1] > v) {
+                seg[j] = seg[j - 1];
+                j--;
+            }
+            seg[j] = v;
+        }
     }
     for (uint32_t i = 0; i < n; i++) {
         c.idA[anEnd + i] = A;
