@@ -57,9 +57,13 @@ __global__ void __launch_bounds__(kForceThreads, DEME_FORCE_MIN_BLOCKS) k_force(
         int ct = c.type[i];
         float4 hw = has_hist ? c.hist[i] : make_float4(0.f, 0.f, 0.f, 0.f);
         ContactGeom g;
-        // body A (always a sphere)
-        oA = s.sOwner[sA];
-        const float4 spA = s.sph[sA];
+        // body A (always a sphere); body B's sphere record and owner id are fetched alongside, so that its owner
+        // loads do not wait behind A's arithmetic
+        const bool ssEarly = ct == DEME_SPHERE_SPHERE_CONTACT;
+        oA = __ldg(s.sOwner + sA);
+        const uint32_t oBEarly = ssEarly ? __ldg(s.sOwner + bId) : 0u;
+        const float4 spA = __ldg(s.sph + sA);
+        const float4 spBEarly = ssEarly ? __ldg(s.sph + bId) : make_float4(0.f, 0.f, 0.f, 0.f);
         const ushort4 lA = s.loc[oA];
         qA = s.quat[oA];
         const float4 vA = s.vel[oA];
@@ -79,8 +83,8 @@ __global__ void __launch_bounds__(kForceThreads, DEME_FORCE_MIN_BLOCKS) k_force(
         float nX = 0, nY = 0, nZ = 0;
         if (ct == DEME_SPHERE_SPHERE_CONTACT) {
             bSphere = true;
-            oB = s.sOwner[bId];
-            const float4 spB = s.sph[bId];
+            oB = oBEarly;
+            const float4 spB = spBEarly;
             const ushort4 lB = s.loc[oB];
             qB = s.quat[oB];
             const float4 vB = s.vel[oB];
