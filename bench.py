@@ -550,9 +550,6 @@ def main():
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = world * built.n_spheres * args.steps / float(te.item()) / 1e6
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(args)
     def clocked(fn):
         """Runs a section with the SM clocks and throttle reasons sampled during it."""
         sampler = ClockSampler(local_rank)
@@ -570,6 +567,10 @@ def main():
     shell = clocked(lambda: shell_drum_measure(args, stream)) if (rank == 0 and not args.no_shell) else None
     hopper = clocked(lambda: hopper_measure(args, stream)) if (rank == 0 and not args.no_hopper) else None
     small = clocked(lambda: small_scene_measure(args, stream)) if (rank == 0 and not args.no_small) else None
+    # the CPU sample last: its OpenMP threads would otherwise share the host with the GPU sections' host code
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(args)
 
     if rank == 0:
         line = {
