@@ -345,6 +345,7 @@ int32_t save_checkpoint(deme_handle* h, Checkpoint& c) {
     c.n = n;
     c.steps = h->steps;
     c.t = h->t;
+    c.tf = h->tf;
     return DEME_OK;
 }
 
@@ -370,6 +371,7 @@ int32_t restore_checkpoint(deme_handle* h, const Checkpoint& c) {
     h->countStale = false;
     h->steps = c.steps;
     h->t = c.t;
+    h->tf = c.tf;
     h->outsValid = false;
     return DEME_OK;
 }
@@ -381,6 +383,10 @@ namespace {
 int32_t check_adjoint_scene(deme_handle* h) {
     if (h->userForce.lib) {
         h->err = "adjoint: only the built-in Hertz-Mindlin model is differentiated";
+        return DEME_ERR_INVALID;
+    }
+    if (h->motion.lib || h->famRules.lib) {
+        h->err = "adjoint: prescribed-motion expressions and family-change rules are not differentiated";
         return DEME_ERR_INVALID;
     }
     if (h->params.integrator != DEME_INTEGRATOR_EXTENDED_TAYLOR || h->params.cd_update_freq > 1 || h->cdLag > 0) {

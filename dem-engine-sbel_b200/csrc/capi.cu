@@ -515,7 +515,7 @@ void deme_destroy(deme_handle* h) {
     if (h->own_kt) cudaStreamDestroy(h->own_kt);
     release_user_force_model(h->userForce);
     release_family_change_rules(h->famRules);
-    if (h->hTime) cudaFreeHost(h->hTime);
+    release_prescribed_motion(h->motion);
     delete h;
 }
 
@@ -525,6 +525,7 @@ int32_t deme_set_force_model(deme_handle* h, const char* src, const char* const*
     if (src == nullptr) {
         // back to the built-in frictional Hertz-Mindlin model and its four history wildcards
         release_user_force_model(h->userForce);
+        h->jitGeneration++;
         h->nW = h->params.n_contact_wildcards;
         return DEME_OK;
     }
@@ -534,6 +535,7 @@ int32_t deme_set_force_model(deme_handle* h, const char* src, const char* const*
         h->err = err;
         return rc;
     }
+    h->jitGeneration++;
     h->nW = h->userForce.n_wildcards;
     h->outsValid = false;
     return DEME_OK;
@@ -773,12 +775,34 @@ int32_t deme_compute_forces(deme_handle* h) {
     return DEME_OK;
 }
 
+// The time as the reference's dT advances it: a float plus the step, once per step.
+static void advance_host_time(deme_handle* h) {
+    h->t += (double)h->k.h;
+    h->tf = h->tf + h->k.h;
+}
+
+// Family-change rules and prescribed-motion expressions read the time from the device.
+static bool needs_device_time(const deme_handle* h) { return h->famRules.kern || h->motion.kern; }
+
 int32_t deme_integrate(deme_handle* h) {
     if (!h) return DEME_ERR_INVALID;
     cudaStream_t st = h->st_dt;
-    launch_integrate(h->k, h->state_view(), st);
+    if (h->motion.kern) {
+        SimConsts k = h->k;
+        StateView s = h->state_view();
+        const float* t = h->dTime;
+        void* args[] = {&k, &s, &t};
+        if (h->nO) {
+            ProfScope prof_(KID_INTEGRATE, st);
+            CUDA_TRY(h, cudaLaunchKernel((const void*)h->motion.kern, dim3((h->nO + 255) / 256), dim3(256), args, 0,
+                                         st));  // ProfScope counts the launch
+        }
+    } else {
+        launch_integrate(h->k, h->state_view(), st);
+    }
+    if (needs_device_time(h)) launch_advance_time(h->dTime, h->k.h, h->dErr, st);
     TRY(check_launch(h, "integrate"));
-    h->t += (double)h->k.h;
+    advance_host_time(h);
     h->steps++;
     return DEME_OK;
 }
@@ -789,7 +813,7 @@ static int32_t apply_family_rules(deme_handle* h) {
     if (!h->famRules.kern) return DEME_OK;
     SimConsts k = h->k;
     StateView s = h->state_view();
-    const double* t = h->dTime;
+    const float* t = h->dTime;
     void* args[] = {&k, &s, &t};
     CUDA_TRY(h, cudaLaunchKernel((const void*)h->famRules.kern, dim3((h->nO + 255) / 256), dim3(256), args, 0,
                                  h->st_dt));
@@ -818,7 +842,6 @@ static int32_t step_plain(deme_handle* h) {
     TRY(deme_compute_forces(h));
     TRY(apply_family_rules(h));
     TRY(deme_integrate(h));
-    if (h->famRules.kern) launch_advance_time(h->dTime, h->k.h, h->st_dt);
     return DEME_OK;
 }
 
@@ -858,6 +881,9 @@ static std::vector<uint8_t> graph_key(const deme_handle* h) {
     put(&lib, sizeof(lib));
     const void* rules = h->famRules.lib;
     put(&rules, sizeof(rules));
+    const void* motion = h->motion.lib;
+    put(&motion, sizeof(motion));
+    put(&h->jitGeneration, sizeof(h->jitGeneration));  // a new image may load where a released one was
     put(&h->params.cd_update_freq, sizeof(h->params.cd_update_freq));
     put(&h->findShape, sizeof(h->findShape));
     return key;
@@ -901,6 +927,7 @@ static int32_t graph_capture(deme_handle* h, int p) {
     const uint32_t n0 = h->nContacts;
     const int64_t steps0 = h->steps;
     const double t0 = h->t;
+    const float tf0 = h->tf;
     const bool outs0 = h->outsValid, stale0 = h->countStale;
     CUDA_TRY(h, cudaStreamBeginCapture(h->st_dt, cudaStreamCaptureModeThreadLocal));
     h->capturing = true;
@@ -911,7 +938,6 @@ static int32_t graph_capture(deme_handle* h, int p) {
         if (st == DEME_OK) st = deme_compute_forces(h);
         if (st == DEME_OK) st = apply_family_rules(h);
         if (st == DEME_OK) st = deme_integrate(h);
-        if (st == DEME_OK && h->famRules.kern) launch_advance_time(h->dTime, h->k.h, h->st_dt);
     }
     if (st == DEME_OK) launch_window_done(h->dErr, h->dWindows, h->st_dt);
     h->capturing = false;
@@ -924,6 +950,7 @@ static int32_t graph_capture(deme_handle* h, int p) {
     h->nContacts = n0;
     h->steps = steps0;
     h->t = t0;
+    h->tf = tf0;
     h->outsValid = outs0;
     h->countStale = stale0;
     if (st != DEME_OK || e != cudaSuccess) {
@@ -960,6 +987,7 @@ static int32_t step_graph(deme_handle* h, int32_t n_steps) {
         const int cur0 = h->cur;
         const int64_t steps0 = h->steps;
         const double t0 = h->t;
+        const float tf0 = h->tf;
         CUDA_TRY(h, cudaMemsetAsync(h->dWindows, 0, sizeof(uint32_t), h->st_dt));
         for (int32_t w = 0; w < windows; w++) {
             const int p = h->cur;
@@ -968,7 +996,7 @@ static int32_t step_graph(deme_handle* h, int32_t n_steps) {
             add_launches(h->graphKernels[p]);
             h->cur ^= 1;
             h->steps += f;
-            for (int i = 0; i < f; i++) h->t += (double)h->k.h;  // as deme_integrate adds it, step by step
+            for (int i = 0; i < f; i++) advance_host_time(h);  // as deme_integrate adds it, step by step
             h->countStale = true;
             h->outsValid = h->keepOutputs;
             h->everDetected = true;
@@ -985,7 +1013,9 @@ static int32_t step_graph(deme_handle* h, int32_t n_steps) {
             h->cur = cur0 ^ (done & 1);
             h->steps = steps0 + (int64_t)done * f;
             h->t = t0;
-            for (int32_t i = 0; i < done * f; i++) h->t += (double)h->k.h;
+            h->tf = tf0;
+            for (int32_t i = 0; i < done * f; i++) advance_host_time(h);
+            if (needs_device_time(h)) launch_set_time(h->dTime, h->tf, h->st_dt);
             h->outsValid = false;
             h->graphRollbacks++;
             for (int32_t i = 0; i < (windows - done) * f; i++) TRY(step_plain(h));
@@ -1011,18 +1041,36 @@ int32_t deme_graph_stats(deme_handle* h, int64_t* replays, int64_t* rollbacks) {
 }
 
 // ------------------------------------------------------------------------------------------ family changes ----
+// The device copy of the time, allocated with the first rule or expression and started from the host's.
+static int32_t ensure_device_time(deme_handle* h, bool needed) {
+    if (!needed || h->dTime) return DEME_OK;
+    TRY(dalloc_n(h, &h->dTime, 1));
+    launch_set_time(h->dTime, h->tf, h->st_dt);
+    return check_launch(h, "set_time");
+}
+
 int32_t deme_set_family_change_rules(deme_handle* h, int32_t n, const uint32_t* from, const uint32_t* to,
                                      const char* const* conditions) {
     if (!h || n < 0) return DEME_ERR_INVALID;
     CUDA_TRY(h, cudaSetDevice(h->device));
     TRY(cd_finish(h));
-    if (n > 0 && !h->dTime) {
-        TRY(dalloc_n(h, &h->dTime, 1));
-        CUDA_TRY(h, cudaMallocHost(&h->hTime, sizeof(double)));
-    }
+    TRY(ensure_device_time(h, n > 0));
     std::string err;
     const int32_t rc = compile_family_change_rules(n, from, to, conditions, h->famRules, err);
     if (rc != DEME_OK) h->err = err;
+    else h->jitGeneration++;
+    return rc;
+}
+
+int32_t deme_set_prescribed_motion(deme_handle* h, int32_t n, const deme_motion_expressions* m) {
+    if (!h || n < 0 || (n > 0 && !m)) return DEME_ERR_INVALID;
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    TRY(cd_finish(h));
+    TRY(ensure_device_time(h, n > 0));
+    std::string err;
+    const int32_t rc = compile_prescribed_motion(n, m, h->motion, err);
+    if (rc != DEME_OK) h->err = err;
+    else h->jitGeneration++;
     return rc;
 }
 
@@ -1122,10 +1170,9 @@ int32_t deme_autotune(deme_handle* h, int32_t steps_per_trial, deme_tuning* out)
 
 int32_t deme_step(deme_handle* h, int32_t n_steps) {
     if (!h) return DEME_ERR_INVALID;
-    if (h->famRules.kern) {  // the rules read the time on the device: start it from the host's
-        *h->hTime = h->t;
-        CUDA_TRY(h, cudaMemcpyAsync(h->dTime, h->hTime, sizeof(double), cudaMemcpyHostToDevice, h->st_dt));
-    }
+    // rules and expressions read the time on the device: start it from the host's (a kernel argument, so no
+    // staging buffer is read after this call returns)
+    if (needs_device_time(h)) launch_set_time(h->dTime, h->tf, h->st_dt);
     if (h->useGraph && h->cdLag == 0 && !prof_timing()) {
         TRY(step_graph(h, n_steps));
     } else {

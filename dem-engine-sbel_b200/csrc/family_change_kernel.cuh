@@ -6,7 +6,8 @@
 //   if (family_code == FROM) { bool shouldMakeChange = false; { <condition, its `return` turned into
 //   `shouldMakeChange =`> } if (shouldMakeChange) newFamily = TO; }
 // A condition sees the names the reference gives it: pos (double3, the owner's position from the domain's lower
-// corner, as voxelIDToPosition returns it), vel and acc (float3), mass, family_code, t (the time) and h (the step).
+// corner, as voxelIDToPosition returns it), vel and acc (float3), mass, family_code, t (the time: a float advanced
+// by h each step, as the reference's dT advances it) and h (the step).
 // Rules test the family the owner had when the kernel started; when several apply, the last one wins.  The kernel
 // runs after the forces and before the integration of a step, as the reference's routineChecks does.
 #pragma once
@@ -14,7 +15,7 @@
 
 namespace deme_b200 {
 
-__global__ void __launch_bounds__(256) k_family_change(SimConsts k, StateView s, const double* time) {
+__global__ void __launch_bounds__(256) k_family_change(SimConsts k, StateView s, const float* time) {
     const uint32_t myOwner = blockIdx.x * blockDim.x + threadIdx.x;
     if (myOwner >= k.n_owners) return;
     if (*k.err != 0u) return;  // a voided step leaves the state as it was
@@ -27,7 +28,7 @@ __global__ void __launch_bounds__(256) k_family_change(SimConsts k, StateView s,
     const float3 vel = make_float3(v4.x, v4.y, v4.z);
     const float3 acc = make_float3(a4.x, a4.y, a4.z);
     const float mass = v4.w;
-    const float t = (float)*time;
+    const float t = *time;
     const float h = k.h;
     unsigned int newFamily = family_code;
     (void)pos;

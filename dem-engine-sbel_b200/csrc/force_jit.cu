@@ -11,6 +11,7 @@
 #include <mutex>
 #include <string>
 #include <unordered_map>
+#include <utility>
 #include <vector>
 
 #include <nvrtc.h>
@@ -214,22 +215,13 @@ const char* kFamilySource =
     "#include \"family_change_kernel.cuh\"\n";
 }  // namespace
 
-int32_t compile_family_change_rules(int32_t n, const uint32_t* from, const uint32_t* to,
-                                    const char* const* conditions, FamilyChangeKernel& out, std::string& err) {
-    if (n <= 0) {
-        release_family_change_rules(out);
-        return DEME_OK;
-    }
-    std::string inc;
-    for (int32_t i = 0; i < n; i++) {
-        if (!from || !to || !conditions || !conditions[i] || from[i] > 255u || to[i] > 255u) {
-            err = "family change rule " + std::to_string(i) + ": families must lie in [0, 255] and the condition exist";
-            return DEME_ERR_INVALID;
-        }
-        inc += "if (family_code == " + std::to_string(from[i]) + "u) {\nbool shouldMakeChange = false;\n{\n#line 1 \"" +
-               "family_change_rule_" + std::to_string(i) + "\"\n" + returns_to_decision(conditions[i]) +
-               "\n}\nif (shouldMakeChange) newFamily = " + std::to_string(to[i]) + "u;\n}\n";
-    }
+namespace {
+
+// Compiles `source` for the current device with the embedded header set plus the generated files `extra`
+// (name, text), and loads the kernel named by `expr`.  `what` names the user input in error messages.
+int32_t build_one_kernel(const char* source, const char* prog_name,
+                         const std::vector<std::pair<std::string, std::string>>& extra, const char* expr,
+                         const char* what, cudaLibrary_t& lib, cudaKernel_t& kern, std::string& err) {
     int dev = 0;
     cudaDeviceProp prop{};
     if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
@@ -247,15 +239,16 @@ int32_t compile_family_change_rules(int32_t n, const uint32_t* from, const uint3
     htexts.push_back(kStdintStub);
     hnames.push_back("stddef.h");
     htexts.push_back(kStddefStub);
-    hnames.push_back("deme_family_change_rules.inc");
-    htexts.push_back(inc.c_str());
+    for (const auto& e : extra) {
+        hnames.push_back(e.first.c_str());
+        htexts.push_back(e.second.c_str());
+    }
     nvrtcProgram prog = nullptr;
-    if (nvrtcCreateProgram(&prog, kFamilySource, "deme_family_change.cu", (int)hnames.size(), htexts.data(),
-                           hnames.data()) != NVRTC_SUCCESS) {
+    if (nvrtcCreateProgram(&prog, source, prog_name, (int)hnames.size(), htexts.data(), hnames.data()) !=
+        NVRTC_SUCCESS) {
         err = "nvrtcCreateProgram failed";
         return DEME_ERR_NVRTC;
     }
-    const char* expr = "deme_b200::k_family_change";
     nvrtcAddNameExpression(prog, expr);
     const char* opts[] = {arch.c_str(), "--fmad=false", "-std=c++17", "-lineinfo"};
     const nvrtcResult rc = nvrtcCompileProgram(prog, 4, opts);
@@ -264,7 +257,7 @@ int32_t compile_family_change_rules(int32_t n, const uint32_t* from, const uint3
         nvrtcGetProgramLogSize(prog, &logSize);
         std::string log(logSize, '\0');
         if (logSize) nvrtcGetProgramLog(prog, &log[0]);
-        err = std::string("family change rules did not compile: ") + nvrtcGetErrorString(rc) + "\n" + log;
+        err = std::string(what) + " did not compile: " + nvrtcGetErrorString(rc) + "\n" + log;
         nvrtcDestroyProgram(&prog);
         return DEME_ERR_NVRTC;
     }
@@ -281,16 +274,44 @@ int32_t compile_family_change_rules(int32_t n, const uint32_t* from, const uint3
     if (ok) lowered = name;
     nvrtcDestroyProgram(&prog);
     if (!ok) {
-        err = "NVRTC produced no loadable image for the family change rules";
+        err = std::string("NVRTC produced no loadable image for the ") + what;
         return DEME_ERR_NVRTC;
     }
-    FamilyChangeKernel k;
-    if (cudaLibraryLoadData(&k.lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0) != cudaSuccess ||
-        cudaLibraryGetKernel(&k.kern, k.lib, lowered.c_str()) != cudaSuccess) {
-        err = std::string("loading the family change rules failed: ") + cudaGetErrorString(cudaGetLastError());
-        if (k.lib) cudaLibraryUnload(k.lib);
+    lib = nullptr;
+    kern = nullptr;
+    if (cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0) != cudaSuccess ||
+        cudaLibraryGetKernel(&kern, lib, lowered.c_str()) != cudaSuccess) {
+        err = std::string("loading the ") + what + " failed: " + cudaGetErrorString(cudaGetLastError());
+        if (lib) cudaLibraryUnload(lib);
+        lib = nullptr;
+        kern = nullptr;
         return DEME_ERR_CUDA;
     }
+    return DEME_OK;
+}
+
+}  // namespace
+
+int32_t compile_family_change_rules(int32_t n, const uint32_t* from, const uint32_t* to,
+                                    const char* const* conditions, FamilyChangeKernel& out, std::string& err) {
+    if (n <= 0) {
+        release_family_change_rules(out);
+        return DEME_OK;
+    }
+    std::string inc;
+    for (int32_t i = 0; i < n; i++) {
+        if (!from || !to || !conditions || !conditions[i] || from[i] > 255u || to[i] > 255u) {
+            err = "family change rule " + std::to_string(i) + ": families must lie in [0, 255] and the condition exist";
+            return DEME_ERR_INVALID;
+        }
+        inc += "if (family_code == " + std::to_string(from[i]) + "u) {\nbool shouldMakeChange = false;\n{\n#line 1 \"" +
+               "family_change_rule_" + std::to_string(i) + "\"\n" + returns_to_decision(conditions[i]) +
+               "\n}\nif (shouldMakeChange) newFamily = " + std::to_string(to[i]) + "u;\n}\n";
+    }
+    FamilyChangeKernel k;
+    const int32_t rc = build_one_kernel(kFamilySource, "deme_family_change.cu", {{"deme_family_change_rules.inc", inc}},
+                                        "deme_b200::k_family_change", "family change rules", k.lib, k.kern, err);
+    if (rc != DEME_OK) return rc;
     release_family_change_rules(out);
     out = k;
     return DEME_OK;
@@ -299,6 +320,70 @@ int32_t compile_family_change_rules(int32_t n, const uint32_t* from, const uint3
 void release_family_change_rules(FamilyChangeKernel& k) {
     if (k.lib) cudaLibraryUnload(k.lib);
     k = FamilyChangeKernel{};
+}
+
+namespace {
+const char* kMotionSource =
+    "#include <stdint.h>\n"
+    "#include \"force_model_api.cuh\"\n"
+    "#include \"prescribed_motion_kernel.cuh\"\n";
+
+// `<name> = <expression>;` under a #line naming the family and component, so the compiler log points at it.
+void assign(std::string& out, int32_t family, const char* what, const char* name, const char* expr) {
+    if (!expr) return;
+    out += "\n#line 1 \"family_" + std::to_string(family) + "_" + what + "\"\n";
+    out += std::string(name) + " = " + expr + ";\n";
+}
+}  // namespace
+
+int32_t compile_prescribed_motion(int32_t n, const deme_motion_expressions* m, MotionKernel& out, std::string& err) {
+    if (n <= 0) {
+        release_prescribed_motion(out);
+        return DEME_OK;
+    }
+    if (!m) {
+        err = "prescribed motions: null array";
+        return DEME_ERR_INVALID;
+    }
+    std::string vel, pos;
+    std::vector<bool> seen(DEME_NUM_FAMILIES, false);
+    for (int32_t i = 0; i < n; i++) {
+        const deme_motion_expressions& e = m[i];
+        if (e.family < 0 || e.family >= DEME_NUM_FAMILIES || seen[e.family]) {
+            err = "prescribed motion " + std::to_string(i) + ": family must lie in [0, 255] and appear once";
+            return DEME_ERR_INVALID;
+        }
+        seen[e.family] = true;
+        static const char* kVel[3] = {"vX", "vY", "vZ"};
+        static const char* kOmg[3] = {"omgBarX", "omgBarY", "omgBarZ"};
+        static const char* kPos[3] = {"X", "Y", "Z"};
+        static const char* kVelWhat[3] = {"lin_vel_x", "lin_vel_y", "lin_vel_z"};
+        static const char* kOmgWhat[3] = {"ang_vel_x", "ang_vel_y", "ang_vel_z"};
+        static const char* kPosWhat[3] = {"lin_pos_x", "lin_pos_y", "lin_pos_z"};
+        const std::string head = "case " + std::to_string(e.family) + "u: {";
+        vel += head;
+        for (int c = 0; c < 3; c++) assign(vel, e.family, kVelWhat[c], kVel[c], e.lin_vel[c]);
+        for (int c = 0; c < 3; c++) assign(vel, e.family, kOmgWhat[c], kOmg[c], e.ang_vel[c]);
+        vel += "LinPrescribed = " + std::to_string(e.lin_vel_prescribed ? 1 : 0) + "; RotPrescribed = " +
+               std::to_string(e.rot_vel_prescribed ? 1 : 0) + "; break; }\n";
+        pos += head;
+        for (int c = 0; c < 3; c++) assign(pos, e.family, kPosWhat[c], kPos[c], e.lin_pos[c]);
+        pos += "LinPrescribed = " + std::to_string(e.lin_pos_prescribed ? 1 : 0) + "; RotPrescribed = " +
+               std::to_string(e.rot_pos_prescribed ? 1 : 0) + "; break; }\n";
+    }
+    MotionKernel k;
+    const int32_t rc = build_one_kernel(kMotionSource, "deme_prescribed_motion.cu",
+                                        {{"deme_motion_vel.inc", vel}, {"deme_motion_pos.inc", pos}},
+                                        "deme_b200::k_integrate_motion", "prescribed motion", k.lib, k.kern, err);
+    if (rc != DEME_OK) return rc;
+    release_prescribed_motion(out);
+    out = k;
+    return DEME_OK;
+}
+
+void release_prescribed_motion(MotionKernel& k) {
+    if (k.lib) cudaLibraryUnload(k.lib);
+    k = MotionKernel{};
 }
 
 }  // namespace deme_b200

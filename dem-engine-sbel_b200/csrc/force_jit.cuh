@@ -5,6 +5,8 @@
 
 #include <cuda_runtime.h>
 
+#include "../../include/deme_b200.h"
+
 namespace deme_b200 {
 
 // Maximum number of per-contact wildcards a force model can declare: they live in the contact's float4 history.
@@ -33,5 +35,16 @@ struct FamilyChangeKernel {
 int32_t compile_family_change_rules(int32_t n, const uint32_t* from, const uint32_t* to,
                                     const char* const* conditions, FamilyChangeKernel& out, std::string& err);
 void release_family_change_rules(FamilyChangeKernel& k);
+
+// Prescribed motions written as expressions (SetFamilyPrescribedLinVel / AngVel / Position with strings that are not
+// constants) compiled into k_integrate_motion (prescribed_motion_kernel.cuh).
+struct MotionKernel {
+    cudaLibrary_t lib = nullptr;
+    cudaKernel_t kern = nullptr;
+};
+// n families' expressions; n <= 0 releases the kernel.  On failure returns a DEME_ERR_* code and fills `err` (the
+// compiler log for an expression that does not compile); `out` is then unchanged.
+int32_t compile_prescribed_motion(int32_t n, const deme_motion_expressions* m, MotionKernel& out, std::string& err);
+void release_prescribed_motion(MotionKernel& k);
 
 }  // namespace deme_b200

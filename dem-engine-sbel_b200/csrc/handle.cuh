@@ -40,6 +40,7 @@ struct Checkpoint {
     uint32_t* off = nullptr;
     int64_t steps = 0;
     double t = 0.0;
+    float tf = 0.f;
 };
 
 struct deme_handle {
@@ -96,12 +97,15 @@ struct deme_handle {
     float* analPartial = nullptr;
     size_t analPartialCap = 0;
     double t = 0.0;
+    float tf = 0.f;  // the time as the reference's dT keeps it (a float, advanced by h each step): rules and
+                     // prescribed-motion expressions see this one
     int64_t steps = 0;
     std::vector<void*> allocs;
     UserForceKernel userForce;  // a compiled force-model string, when one is set
     FamilyChangeKernel famRules;  // compiled ChangeFamilyWhen rules, when some are set
-    double* dTime = nullptr;      // the time on the device (the rules read it), advanced once per step
-    double* hTime = nullptr;      // pinned copy the host writes before each deme_step
+    MotionKernel motion;          // compiled prescribed-motion expressions, when some are set
+    uint64_t jitGeneration = 0;   // counts changes of the run-time compiled kernels (recorded graphs hold them)
+    float* dTime = nullptr;       // tf on the device (rules and expressions read it), advanced once per step
     AdjointTape* adj = nullptr;  // checkpoints of deme_adjoint_record
     // Asynchronous contact detection (kT on st_kt, dT on st_dt).  With cdLag > 0 a detection due at step k runs on
     // kT from a snapshot of the owner poses of step k while dT keeps stepping with the current list, and dT adopts

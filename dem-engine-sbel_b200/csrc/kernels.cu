@@ -26,6 +26,7 @@
 #include "force_jit.cuh"
 #include "force_kernel.cuh"
 #include "kernels.cuh"
+#include "integrate_kernel.cuh"
 #include "profiler.cuh"
 
 namespace deme_b200 {
@@ -785,11 +786,20 @@ void launch_change_family(ushort4* loc, uint32_t n, uint32_t from, uint32_t to, 
     k_change_family<<<blocks_for(n, 256), 256, 0, st>>>(loc, n, from, to);
 }
 
-// The simulation time on the device (read by the family-change rules), advanced once per step.
-__global__ void k_advance_time(double* time, float h) { *time += (double)h; }
-void launch_advance_time(double* time, float h, cudaStream_t st) {
+// The simulation time on the device (read by the family-change rules and prescribed-motion expressions): a float
+// advanced by h once per step, as the reference's dT advances timeElapsed (src/DEM/dT.cpp:1585).  A voided step
+// does not advance it.
+__global__ void k_advance_time(float* time, float h, const uint32_t* err) {
+    if (*err == 0u) *time = *time + h;
+}
+void launch_advance_time(float* time, float h, const uint32_t* err, cudaStream_t st) {
     ProfScope prof_(KID_OTHER, st);
-    k_advance_time<<<1, 1, 0, st>>>(time, h);
+    k_advance_time<<<1, 1, 0, st>>>(time, h, err);
+}
+__global__ void k_set_time(float* time, float t) { *time = t; }
+void launch_set_time(float* time, float t, cudaStream_t st) {
+    ProfScope prof_(KID_OTHER, st);
+    k_set_time<<<1, 1, 0, st>>>(time, t);
 }
 
 // End of a replayed window: counts the windows that completed without a device error.
@@ -807,97 +817,7 @@ __global__ void __launch_bounds__(256) k_integrate(SimConsts k, StateView s) {
     const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= k.n_owners) return;
     if (*k.err != 0u) return;  // a voided step (see k_force) leaves the state as it was
-    ushort4 l = s.loc[o];
-    const Prescription pr = s.presc[l.w];
-    float4 v = s.vel[o];
-    float4 w = s.omg[o];
-    const float4 a = s.acc[o];
-    const float4 al = s.alpha[o];
-    const float ovx = v.x, ovy = v.y, ovz = v.z, owx = w.x, owy = w.y, owz = w.z;
-    bool linV = false, rotV = false, linP = false, rotP = false;
-    if (pr.used) {
-        if (pr.has_vel[0]) v.x = pr.vel[0];
-        if (pr.has_vel[1]) v.y = pr.vel[1];
-        if (pr.has_vel[2]) v.z = pr.vel[2];
-        if (pr.has_omg[0]) w.x = pr.omg[0];
-        if (pr.has_omg[1]) w.y = pr.omg[1];
-        if (pr.has_omg[2]) w.z = pr.omg[2];
-        linV = pr.lin_vel;
-        rotV = pr.rot_vel;
-    }
-    const float h = k.h;
-    float ux = 0.f, uy = 0.f, uz = 0.f, qx = 0.f, qy = 0.f, qz = 0.f;
-    if (!linV) {
-        ux = (a.x + k.G[0]) * h;
-        uy = (a.y + k.G[1]) * h;
-        uz = (a.z + k.G[2]) * h;
-        v.x += ux;
-        v.y += uy;
-        v.z += uz;
-    }
-    if (!rotV) {
-        qx = al.x * h;
-        qy = al.y * h;
-        qz = al.z * h;
-        w.x += qx;
-        w.y += qy;
-        w.z += qz;
-    }
-    float px, py, pz, rx, ry, rz;
-    if (k.integrator == DEME_INTEGRATOR_FORWARD_EULER) {
-        px = ovx; py = ovy; pz = ovz;
-        rx = owx; ry = owy; rz = owz;
-    } else if (k.integrator == DEME_INTEGRATOR_CENTERED_DIFFERENCE) {
-        px = ovx + ux; py = ovy + uy; pz = ovz + uz;
-        rx = owx + qx; ry = owy + qy; rz = owz + qz;
-    } else {
-        px = ovx + ux * 0.5f; py = ovy + uy * 0.5f; pz = ovz + uz * 0.5f;
-        rx = owx + qx * 0.5f; ry = owy + qy * 0.5f; rz = owz + qz * 0.5f;
-    }
-    double X, Y, Z;
-    uint64_t vox = s.voxel[o];
-    voxel_to_pos(k, vox, l.x, l.y, l.z, X, Y, Z);
-    if (pr.used) {
-        if (pr.has_pos[0]) X = pr.pos[0];
-        if (pr.has_pos[1]) Y = pr.pos[1];
-        if (pr.has_pos[2]) Z = pr.pos[2];
-        linP = pr.lin_pos;
-        rotP = pr.rot_pos;
-    }
-    if (!linP) {
-        X += (double)px * (double)h;
-        Y += (double)py * (double)h;
-        Z += (double)pz * (double)h;
-    }
-    uint16_t sx, sy, sz;
-    pos_to_voxel(k, X, Y, Z, vox, sx, sy, sz);
-    l.x = sx;
-    l.y = sy;
-    l.z = sz;
-    float4 q = s.quat[o];
-    if (!rotP) {
-        double q0 = 1.0, q1 = rx, q2 = ry, q3 = rz;
-        const double len = sqrt(q1 * q1 + q2 * q2 + q3 * q3);
-        const double theta = 0.5 * (double)h * len;
-        if (len > 0) {
-            q0 = cos(theta);
-            const double sn = sin(theta) / len;
-            q1 *= sn;
-            q2 *= sn;
-            q3 *= sn;
-        }
-        const float a1 = q.x, b1 = q.y, c1 = q.z, d1 = q.w;
-        const float a2 = (float)q0, b2 = (float)q1, c2 = (float)q2, d2 = (float)q3;
-        q.x = a1 * a2 - b1 * b2 - c1 * c2 - d1 * d2;
-        q.y = a1 * b2 + b1 * a2 + c1 * d2 - d1 * c2;
-        q.z = a1 * c2 - b1 * d2 + c1 * a2 + d1 * b2;
-        q.w = a1 * d2 + b1 * c2 - c1 * b2 + d1 * a2;
-    }
-    s.vel[o] = v;
-    s.omg[o] = w;
-    s.voxel[o] = vox;
-    s.loc[o] = l;
-    s.quat[o] = q;
+    integrate_owner(k, s, o, 0.f, TableMotion{s.presc});
 }
 
 void launch_integrate(const SimConsts& k, const StateView& s, cudaStream_t st) {

@@ -121,7 +121,8 @@ void launch_force(const SimConsts& k, const StateView& s, const ContactView& c, 
 uint32_t force_blocks(uint32_t n);
 void launch_window_done(const uint32_t* err, uint32_t* done, cudaStream_t st);
 void launch_change_family(ushort4* loc, uint32_t n, uint32_t from, uint32_t to, cudaStream_t st);
-void launch_advance_time(double* time, float h, cudaStream_t st);
+void launch_advance_time(float* time, float h, const uint32_t* err, cudaStream_t st);
+void launch_set_time(float* time, float t, cudaStream_t st);
 void launch_integrate(const SimConsts& k, const StateView& s, cudaStream_t st);
 void launch_kinetic_energy(const SimConsts& k, const StateView& s, uint32_t n_clumps, double* out, cudaStream_t st);
 

@@ -85,6 +85,20 @@ class FamilyPrescription(C.Structure):
     ]
 
 
+class MotionExpressions(C.Structure):
+    """deme_motion_expressions: one family's prescribed motion as C expression strings (NULL = free)."""
+    _fields_ = [
+        ("family", C.c_int32),
+        ("lin_vel_prescribed", C.c_uint8),
+        ("rot_vel_prescribed", C.c_uint8),
+        ("lin_pos_prescribed", C.c_uint8),
+        ("rot_pos_prescribed", C.c_uint8),
+        ("lin_vel", C.c_char_p * 3),
+        ("ang_vel", C.c_char_p * 3),
+        ("lin_pos", C.c_char_p * 3),
+    ]
+
+
 SCENE_ARRAYS = [
     # (field, dtype, count key)
     ("voxel", np.uint64, "o"),

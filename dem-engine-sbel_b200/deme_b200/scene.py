@@ -160,13 +160,13 @@ class _Prescription:
     rotPosPrescribed: bool = False
 
 
-def _const(expr: str) -> float:
+def _const(expr: str):
+    """The value of a prescription string that is a plain number, else None: an expression (of the time t, as the
+    reference accepts), compiled at run time into the integration kernel by deme_set_prescribed_motion."""
     try:
         return float(expr)
-    except ValueError as e:
-        raise NotImplementedError(
-            f"prescription '{expr}' is not a constant; time-dependent expressions go through the C++ DEMSolver "
-            "facade") from e
+    except ValueError:
+        return None
 
 
 class BuiltScene:
@@ -607,6 +607,7 @@ class SceneBuilder:
         counts = dict(o=nO, s=nS, a=nA, m=nM)
         info = dict(n_clumps=nClumps, n_ext=nExt, n_templates=nT, rmin=rmin, bin_size=bin_size, nb=nb, nv=nv, l=l,
                     beta=beta, lbf=lbf.copy(), box=self.box.copy(), merged_prescriptions=self.merged_prescriptions,
+                    motion_expressions=self.motion_expressions,
                     owner_template=np.asarray(types, np.int64) if nClumps else np.zeros(0, np.int64),
                     template_names=[t.name for t in self.templates])
         return BuiltScene(p, arrays, counts, presc, info)
@@ -641,7 +642,16 @@ class SceneBuilder:
             m.linPosPrescribed |= pr.linPosPrescribed
             m.rotPosPrescribed |= pr.rotPosPrescribed
         self.merged_prescriptions = merged
+        self.motion_expressions = []
         for fam, m in merged.items():
+            strings = [x for x in m.linVel + m.rotVel + m.linPos if x != "none"]
+            if any(_const(x) is None for x in strings):
+                # the whole family goes to the compiled kernel; its table entry stays unused
+                self.motion_expressions.append(dict(
+                    family=fam, lin_vel=list(m.linVel), ang_vel=list(m.rotVel), lin_pos=list(m.linPos),
+                    lin_vel_prescribed=m.linVelPrescribed, rot_vel_prescribed=m.rotVelPrescribed,
+                    lin_pos_prescribed=m.linPosPrescribed, rot_pos_prescribed=m.rotPosPrescribed))
+                continue
             e = arr[fam]
             e.used = 1
             e.lin_vel_prescribed = int(m.linVelPrescribed)

@@ -230,6 +230,13 @@ class Solver(HandleSolver):
         self.nO = built.counts["o"]
         self.nS = built.counts["s"]
         self.nW = built.params.n_contact_wildcards
+        motion = built.info.get("motion_expressions") if isinstance(built.info, dict) else None
+        if motion:
+            try:
+                self.set_prescribed_motion(motion)
+            except DemeError:
+                self.close()
+                raise
 
     def _check(self, st, what):
         if st != capi.DEME_OK:
@@ -288,6 +295,32 @@ class Solver(HandleSolver):
         cond = (C.c_char_p * max(n, 1))(*[r[2].encode() for r in rules])
         self.lib.deme_set_family_change_rules.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
         self._check(self.lib.deme_set_family_change_rules(self.h, n, fr, to, cond), "set_family_change_rules")
+
+    def set_prescribed_motion(self, families):
+        """Prescribed motions written as expressions, one dict per family with keys family, lin_vel, ang_vel,
+        lin_pos (three strings each, "none" = free) and the four *_prescribed flags (see
+        deme_set_prescribed_motion); an empty list returns every family to its constant table entry."""
+        n = len(families)
+        arr = (capi.MotionExpressions * max(n, 1))()
+        keep = []
+
+        def enc(x):
+            if x is None or x == "none":
+                return None
+            b = str(x).encode()
+            keep.append(b)
+            return b
+        for i, f in enumerate(families):
+            e = arr[i]
+            e.family = int(f["family"])
+            for k in ("lin_vel_prescribed", "rot_vel_prescribed", "lin_pos_prescribed", "rot_pos_prescribed"):
+                setattr(e, k, int(bool(f.get(k, False))))
+            for k in ("lin_vel", "ang_vel", "lin_pos"):
+                xs = list(f.get(k, ["none"] * 3))
+                for c in range(3):
+                    getattr(e, k)[c] = enc(xs[c])
+        self.lib.deme_set_prescribed_motion.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+        self._check(self.lib.deme_set_prescribed_motion(self.h, n, arr), "set_prescribed_motion")
 
     def set_search_shape(self, shape: int, cell_factor: float = 1.0):
         """Block shape of the pooled pair search and search-cell scale (see deme_set_search_shape)."""

@@ -69,6 +69,58 @@ def settling_box(n: int = 10000, r: float = 5e-3, rho: float = 2600.0, box=(0.2,
     return built
 
 
+PISTON_VZ = "(t > 1e-4) ? 0.5 * sin(2000.0 * deme::PI * (t - 1e-4)) : 0.0"
+SLIDER_X = "0.03 + 2.0 * t"
+SPINNER_WZ = "(t < 2e-4) ? 4000.0 * t : 0.8 - 1000.0 * (t - 2e-4)"
+
+
+def shaker_box(n: int = 500, r: float = 5e-3, rho: float = 2600.0, box=(0.08, 0.08, 0.12), spacing: float = 2.05,
+               jitter: float = 0.05, seed: int = 24, dt: float = 1e-5, piston_vz: str = PISTON_VZ,
+               slider_x: str = SLIDER_X, spinner_wz: str = SPINNER_WZ):
+    """Spheres on a jittered lattice in a box of 6 planes, with three families moved by time expressions (the
+    reference's prescribed-motion strings, compiled into the integration kernel at run time):
+
+    * family 1, the lattice's bottom layer: vertical velocity ``piston_vz`` (dictated; the rotation is held);
+    * family 2, one sphere of the second layer: X (from the domain's lower corner) follows ``slider_x``, Y and Z
+      stay free of prescription but are not integrated (a prescribed position holds the whole pose);
+    * family 3, the third layer: angular velocity about z follows ``spinner_wz`` (not dictated: it is added to
+      the integrated motion, as the reference does for dictate = false).
+    """
+    rng = np.random.default_rng(seed)
+    s = SceneBuilder()
+    s.InstructBoxDomainDimension(*box)
+    s.SetCoordSysOrigin("center")
+    mat = s.LoadMaterial({"E": 1e7, "nu": 0.3, "CoR": 0.5, "mu": 0.5, "Crr": 0.01})
+    s.InstructBoxDomainBoundingBC("all", mat)
+    t = s.LoadSphereType(sphere_mass(r, rho), r, mat)
+    a = spacing * r
+    nx, ny = int(box[0] // a), int(box[1] // a)
+    lbf = -np.asarray(box) / 2
+    x0 = lbf[0] + (box[0] - nx * a) / 2 + a / 2
+    y0 = lbf[1] + (box[1] - ny * a) / 2 + a / 2
+    z0 = lbf[2] + a / 2 + 0.2 * r
+    idx = np.arange(n)
+    layer = idx // (nx * ny)
+    pos = np.stack([x0 + (idx % nx) * a, y0 + ((idx // nx) % ny) * a, z0 + layer * a], axis=1)
+    pos += rng.uniform(-jitter * r, jitter * r, size=pos.shape)
+    fam = np.zeros(n, np.int64)
+    fam[layer == 0] = 1
+    fam[(layer == 1) & (idx == nx * ny + (nx * ny) // 2)] = 2
+    fam[layer == 2] = 3
+    b = s.AddClumps(t, pos.astype(f32))
+    b.SetVel(rng.normal(0, 0.05, size=(n, 3)).astype(f32))
+    b.SetFamilies(fam)
+    s.SetFamilyPrescribedLinVel(1, "0", "0", piston_vz)
+    s.SetFamilyPrescribedPosition(2, slider_x, "none", "none")
+    s.SetFamilyPrescribedAngVel(3, "0", "0", spinner_wz, dictate=False)
+    s.SetInitTimeStep(dt)
+    s.SetGravitationalAcceleration((0, 0, -9.81))
+    s.SetInitBinSize(2.0 * r)
+    built = s.Initialize()
+    built.info.update(workload="shaker_box", seed=seed)
+    return built
+
+
 def triangle_template(rng, r_nom: float, rho: float, n_mc: int = 20000):
     """Three-sphere triangular clump: radii U[0.8, 1.2] r_nom, centres 0.6 r from the clump centroid.
 

@@ -353,6 +353,30 @@ int32_t deme_autotune(deme_handle* h, int32_t steps_per_trial, deme_tuning* out)
  * re-jitifying).  The value is staged through pinned memory and applied in stream order. */
 int32_t deme_set_family_prescription(deme_handle* h, int32_t family, const deme_family_prescription* p);
 
+/* A family's prescribed motion written as C expressions: SetFamilyPrescribedLinVel / SetFamilyPrescribedAngVel /
+ * SetFamilyPrescribedPosition with strings that are not constants (src/DEM/APIPublic.cpp:210-273).  Each non-NULL
+ * string is pasted into the integration kernel as `vX = <string>;` (lin_vel), `omgBarX = <string>;` (ang_vel) or
+ * `X = <string>;` (lin_pos, measured from the domain's lower corner), the way equipFamilyPrescribedMotions pastes
+ * them (src/DEM/APIPrivate.cpp:1005-1048).  An expression sees t (float: the time at the start of the step,
+ * accumulated in float as the reference's dT accumulates it), family, the components it prescribes and deme::PI.
+ * NULL leaves a component free (the reference's "none"). */
+typedef struct {
+    int32_t family;
+    uint8_t lin_vel_prescribed; /* the family's linear velocity is dictated, not integrated */
+    uint8_t rot_vel_prescribed;
+    uint8_t lin_pos_prescribed;
+    uint8_t rot_pos_prescribed;
+    const char* lin_vel[3];
+    const char* ang_vel[3];
+    const char* lin_pos[3];
+} deme_motion_expressions;
+
+/* Compiles the prescribed motions of n families (each at most once) with NVRTC into the integration kernel; from
+ * the next step those families follow their expressions instead of their constant table entries.  n = 0 returns
+ * every family to its table entry.  A set that does not compile returns DEME_ERR_NVRTC with the compiler's log in
+ * deme_get_error and leaves the previous set in place. */
+int32_t deme_set_prescribed_motion(deme_handle* h, int32_t n, const deme_motion_expressions* m);
+
 /* Instrumentation.  deme_launch_count: kernels launched by this library in this process.  deme_kernel_timing(1)
  * brackets every launch with CUDA events on its stream; deme_kernel_times sums them per kernel name.  (The reference
  * keeps host wall-clock timers per phase instead: src/DEM/kT.h:179-181, src/DEM/dT.h:253-255.) */

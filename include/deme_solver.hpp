@@ -9,8 +9,9 @@
  * src/DEM/HostSideHelpers.hpp:328-350) and hands the flat arrays to deme_create.  The Python SceneBuilder
  * (deme_b200/scene.py) implements the same flattening; tests check that the two agree array by array.
  *
- * Prescribed motions are constants (the reference also accepts time-dependent C expressions; a non-constant
- * expression throws here).  Errors throw std::runtime_error with the library's message, as DEME_ERROR does.
+ * Prescribed motions that are plain numbers go into the per-family constant table; a family with any other string
+ * (a C expression of the time t, as the reference accepts) is compiled at Initialize into the integration kernel
+ * by deme_set_prescribed_motion.  Errors throw std::runtime_error with the library's message, as DEME_ERROR does.
  */
 #ifndef DEME_SOLVER_HPP
 #define DEME_SOLVER_HPP
@@ -178,6 +179,9 @@ struct FlatScene {
     std::vector<float> mat_E, mat_nu, mat_CoR, mat_mu, mat_Crr;
     std::vector<uint8_t> family_masks;
     std::vector<deme_family_prescription> prescriptions;
+    // families whose prescription holds an expression: strings kept here, pointed to by `motion`
+    std::vector<std::vector<std::string>> motion_strings;  // per entry: vX vY vZ wX wY wZ X Y Z ("none" = free)
+    std::vector<deme_motion_expressions> motion;
     // clump owners' template marks and the templates' names (the clump file's clump_type column)
     std::vector<uint32_t> owner_template;
     std::vector<std::string> template_names;
@@ -550,6 +554,19 @@ class DEMSolver {
             }
             check(deme_set_family_change_rules(h, (int32_t)fam_rules.size(), from.data(), to.data(), cond.data()));
         }
+        if (!flat->motion.empty()) {
+            for (size_t i = 0; i < flat->motion.size(); i++) {
+                const std::vector<std::string>& x = flat->motion_strings[i];
+                deme_motion_expressions& me = flat->motion[i];
+                auto str = [&](int j) { return x[j] == "none" ? nullptr : x[j].c_str(); };
+                for (int k = 0; k < 3; k++) {
+                    me.lin_vel[k] = str(k);
+                    me.ang_vel[k] = str(3 + k);
+                    me.lin_pos[k] = str(6 + k);
+                }
+            }
+            check(deme_set_prescribed_motion(h, (int32_t)flat->motion.size(), flat->motion.data()));
+        }
         if (force_model && force_model->custom) {
             std::vector<const char*> names;
             for (const auto& n : force_model->m_contact_wildcards) names.push_back(n.c_str());
@@ -776,14 +793,12 @@ class DEMSolver {
         std::snprintf(buf, sizeof(buf), "%.17f", x);
         return std::strtod(buf, nullptr);
     }
-    static double constant_expr(const std::string& e) {
+    /* a prescription string that is a plain number; anything else is an expression compiled at Initialize */
+    static bool constant_expr(const std::string& e, double& v) {
         char* end = nullptr;
-        const double v = std::strtod(e.c_str(), &end);
+        v = std::strtod(e.c_str(), &end);
         while (end && *end == ' ') end++;
-        if (!end || end == e.c_str() || *end != '\0')
-            throw std::runtime_error("prescription '" + e + "' is not a constant (only constant prescriptions are "
-                                     "supported)");
-        return v;
+        return end && end != e.c_str() && *end == '\0';
     }
 
     /* figureOutNV, src/DEM/APIPrivate.cpp:222-333 (no exact direction) */
@@ -987,26 +1002,45 @@ class DEMSolver {
             m.rotPosP |= p.rotPosP;
         }
         f.prescriptions.assign(DEME_NUM_FAMILIES, deme_family_prescription{});
+        f.motion_strings.clear();
+        f.motion.clear();
         for (const auto& kv : merged) {
             deme_family_prescription& e = f.prescriptions[kv.first];
             const Presc& m = kv.second;
+            bool expression = false;
+            double v = 0.0;
+            for (int k = 0; k < 3; k++)
+                for (const std::string* x : {&m.linVel[k], &m.rotVel[k], &m.linPos[k]})
+                    if (*x != "none" && !constant_expr(*x, v)) expression = true;
+            if (expression) {  // the whole family goes to the compiled kernel; its table entry stays unused
+                f.motion_strings.push_back({m.linVel[0], m.linVel[1], m.linVel[2], m.rotVel[0], m.rotVel[1],
+                                            m.rotVel[2], m.linPos[0], m.linPos[1], m.linPos[2]});
+                deme_motion_expressions me{};
+                me.family = (int32_t)kv.first;
+                me.lin_vel_prescribed = m.linVelP;
+                me.rot_vel_prescribed = m.rotVelP;
+                me.lin_pos_prescribed = m.linPosP;
+                me.rot_pos_prescribed = m.rotPosP;
+                f.motion.push_back(me);
+                continue;
+            }
             e.used = 1;
             e.lin_vel_prescribed = m.linVelP;
             e.rot_vel_prescribed = m.rotVelP;
             e.lin_pos_prescribed = m.linPosP;
             e.rot_pos_prescribed = m.rotPosP;
             for (int k = 0; k < 3; k++) {
-                if (m.linVel[k] != "none") {
+                if (m.linVel[k] != "none" && constant_expr(m.linVel[k], v)) {
                     e.has_vel[k] = 1;
-                    e.vel[k] = (float)constant_expr(m.linVel[k]);
+                    e.vel[k] = (float)v;
                 }
-                if (m.rotVel[k] != "none") {
+                if (m.rotVel[k] != "none" && constant_expr(m.rotVel[k], v)) {
                     e.has_omg[k] = 1;
-                    e.omg[k] = (float)constant_expr(m.rotVel[k]);
+                    e.omg[k] = (float)v;
                 }
-                if (m.linPos[k] != "none") {
+                if (m.linPos[k] != "none" && constant_expr(m.linPos[k], v)) {
                     e.has_pos[k] = 1;
-                    e.pos[k] = constant_expr(m.linPos[k]);
+                    e.pos[k] = v;
                 }
             }
         }

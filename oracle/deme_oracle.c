@@ -1187,3 +1187,9 @@ double orc_kinetic_energy(oracle_ctx* c) {
 }
 int32_t orc_max_spheres_in_bin(oracle_ctx* c) { return c->maxInBin; }
 double orc_time(oracle_ctx* c) { return c->t; }
+
+int32_t orc_set_family_prescription(oracle_ctx* c, int32_t family, const deme_family_prescription* p) {
+    if (!c || !p || family < 0 || family >= DEME_NUM_FAMILIES) return DEME_ERR_INVALID;
+    c->presc[family] = *p;
+    return DEME_OK;
+}

@@ -39,6 +39,9 @@ int32_t orc_bin_assignment(oracle_ctx* c, uint16_t* n_bins, uint8_t* n_anal, uin
 double orc_kinetic_energy(oracle_ctx* c);
 int32_t orc_max_spheres_in_bin(oracle_ctx* c);
 double orc_time(oracle_ctx* c);
+/* Replaces one family's constant prescription (deme_set_family_prescription's counterpart); a test that checks
+ * prescribed-motion expressions sets, before each step, the values the expressions take at that step's time. */
+int32_t orc_set_family_prescription(oracle_ctx* c, int32_t family, const deme_family_prescription* p);
 
 #ifdef __cplusplus
 }

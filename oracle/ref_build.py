@@ -260,7 +260,8 @@ def lookup(built) -> str | None:
 def build(built, out_root: str = OUT_ROOT, verbose: bool = False) -> str:
     d, paths = generate(built, out_root)
     lib = os.path.join(d, "libdeme_ref.so")
-    if os.path.exists(lib):
+    harness = os.path.join(HERE, "ref_harness.cpp")
+    if os.path.exists(lib) and os.path.getmtime(lib) >= os.path.getmtime(harness):
         if out_root == OUT_ROOT:
             _index_put(built, lib)
         return lib

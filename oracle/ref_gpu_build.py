@@ -213,6 +213,7 @@ PARITY_SCENES = {
     "settle": lambda w: w.settling_box(n=600, r=5e-3, box=(0.08, 0.08, 0.12), spacing=1.99, jitter=0.03, seed=23,
                                        vel_scale=0.3, ang_scale=30.0),
     "drum_shell": lambda w: w.drum(20000, shell=True, spacing=0.745),
+    "shaker": lambda w: w.shaker_box(),
 }
 
 

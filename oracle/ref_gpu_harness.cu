@@ -121,6 +121,7 @@ struct refg_ctx {
     int nW = 0;
     int cd_freq = 0;
     double t = 0;
+    float tf = 0.f;  // the time as the reference's dT keeps it (float timeElapsed, src/DEM/dT.h:216)
     int64_t steps = 0;
     size_t nC = 0, nPrev = 0;
 
@@ -688,11 +689,12 @@ bool do_forces(refg_ctx* c) {
 }
 
 bool do_integrate(refg_ctx* c) {
-    float t = (float)c->t;
+    float t = c->tf;
     void* args[] = {&c->d_sp, &c->d_dt, &t};
     if (!launch(c, K_INTEGRATE, blocks_for(c->nO, DEME_NUM_BODIES_PER_BLOCK), DEME_NUM_BODIES_PER_BLOCK, args))
         return false;
     c->t += (double)c->sp.h;
+    c->tf += c->sp.h;  // timeElapsed += simParams->h (src/DEM/dT.cpp:1585)
     c->steps++;
     return true;
 }

@@ -111,6 +111,7 @@ struct ref_ctx {
     uint32_t nO, nS, nA;
     int nW;
     double t;
+    float tf;  // the time as the reference's dT keeps it (float timeElapsed, src/DEM/dT.h:216)
     int64_t steps;
     int cd_freq;
     std::vector<uint64_t> voxel;
@@ -246,6 +247,7 @@ ref_ctx* ref_create(const deme_sim_params* p, const deme_scene* s) {
     c->nW = p->n_contact_wildcards;
     c->cd_freq = p->cd_update_freq;
     c->t = 0;
+    c->tf = 0.f;
     c->steps = 0;
     uint32_t nO = c->nO, nS = c->nS;
     auto cp = [](auto& v, const auto* src, size_t n) {
@@ -475,8 +477,9 @@ int32_t ref_compute_forces(ref_ctx* c) {
 int32_t ref_integrate(ref_ctx* c) {
     c->pack();
     launch(blocks_for(c->nO, DEME_NUM_BODIES_PER_BLOCK), DEME_NUM_BODIES_PER_BLOCK,
-           [&] { integrateOwners(&c->sp, &c->dt, (float)c->t); });
+           [&] { integrateOwners(&c->sp, &c->dt, c->tf); });
     c->t += (double)c->sp.h;
+    c->tf += c->sp.h;  // timeElapsed += simParams->h (src/DEM/dT.cpp:1585)
     c->steps++;
     return DEME_OK;
 }

@@ -114,3 +114,39 @@ class _Built:
 def load_golden(name):
     rec = np.load(os.path.join(GOLDEN_DIR, name + ".npz"))
     return _Built(rec).inner, rec
+
+
+def shaker_motion(t32) -> dict:
+    """The shaker box's prescribed motions (workloads.shaker_box) evaluated at the float time ``t32`` the way the
+    compiled expressions evaluate them (t promoted to double, the result stored in the component's type), as
+    constant prescriptions per family, for the oracle, which integrates from a constant table."""
+    import math
+    t = float(np.float32(t32))
+    out = {}
+    p = capi.FamilyPrescription()
+    p.used, p.lin_vel_prescribed, p.rot_vel_prescribed = 1, 1, 1
+    p.has_vel[:] = [1, 1, 1]
+    vz = 0.5 * math.sin(2000.0 * math.pi * (t - 1e-4)) if t > 1e-4 else 0.0
+    p.vel[:] = [0.0, 0.0, float(np.float32(vz))]
+    out[1] = p
+    p = capi.FamilyPrescription()
+    p.used, p.lin_pos_prescribed, p.rot_pos_prescribed = 1, 1, 1
+    p.has_pos[:] = [1, 0, 0]
+    p.pos[:] = [0.03 + 2.0 * t, 0.0, 0.0]
+    out[2] = p
+    p = capi.FamilyPrescription()
+    p.used = 1
+    p.has_omg[:] = [1, 1, 1]
+    wz = 4000.0 * t if t < 2e-4 else 0.8 - 1000.0 * (t - 2e-4)
+    p.omg[:] = [0.0, 0.0, float(np.float32(wz))]
+    out[3] = p
+    return out
+
+
+def set_oracle_motion(orc, table: dict):
+    """Loads constant prescriptions into an oracle (orc_set_family_prescription)."""
+    import ctypes as C
+    fn = orc.lib.orc_set_family_prescription
+    fn.argtypes = [C.c_void_p, C.c_int32, C.POINTER(capi.FamilyPrescription)]
+    for fam, p in table.items():
+        assert fn(orc.h, int(fam), C.byref(p)) == capi.DEME_OK

@@ -88,6 +88,7 @@ int main(int argc, char** argv) {
     s.SetFamilyFixed(3);
     s.SetFamilyPrescribedAngVel(10, "0", "2.0943951", "0");
     s.SetFamilyPrescribedLinVel(4, "0.1", "none", "0");
+    s.SetFamilyPrescribedLinVel(5, "0", "0", "0.2 * sin(3000.0 * t)");
     s.DisableContactBetweenFamilies(3, 10);
     s.SetInitTimeStep(1e-5);
     s.SetGravitationalAcceleration(float3{0.f, 0.f, -9.81f});
@@ -143,6 +144,19 @@ int main(int argc, char** argv) {
     put(out, "mat_Crr", f.mat_Crr);
     put(out, "family_masks", f.family_masks);
     put(out, "prescriptions", f.prescriptions);
+    {
+        // families handed to deme_set_prescribed_motion: family, four flags, nine strings, '|'-separated lines
+        std::string m;
+        for (size_t i = 0; i < f.motion.size(); i++) {
+            const deme_motion_expressions& e = f.motion[i];
+            m += std::to_string(e.family) + "|" + std::to_string(e.lin_vel_prescribed) + "|" +
+                 std::to_string(e.rot_vel_prescribed) + "|" + std::to_string(e.lin_pos_prescribed) + "|" +
+                 std::to_string(e.rot_pos_prescribed);
+            for (const std::string& x : f.motion_strings[i]) m += "|" + x;
+            m += "\n";
+        }
+        put(out, "motion", m.data(), m.size());
+    }
     {
         // CSV output of the initial state (every column), for comparison with the Python writers
         OwnerState st;

@@ -64,6 +64,7 @@ def python_scene(types, xyz1, q1, v1, w1, fam1, xyz2):
     s.SetFamilyFixed(3)
     s.SetFamilyPrescribedAngVel(10, "0", "2.0943951", "0")
     s.SetFamilyPrescribedLinVel(4, "0.1", "none", "0")
+    s.SetFamilyPrescribedLinVel(5, "0", "0", "0.2 * sin(3000.0 * t)")
     s.DisableContactBetweenFamilies(3, 10)
     s.SetInitTimeStep(1e-5)
     s.SetGravitationalAcceleration((0, 0, -9.81))
@@ -138,7 +139,7 @@ def test_csv_output_agrees_byte_for_byte(dump, tmp_path):
 
 def test_flat_arrays_agree_bit_for_bit(dump):
     cpp, built = dump
-    names = [k for k in cpp if k not in ("params", "prescriptions") and not k.startswith("csv_")]
+    names = [k for k in cpp if k not in ("params", "prescriptions", "motion") and not k.startswith("csv_")]
     assert len(names) == 45
     for k in names:
         py = np.ascontiguousarray(built.arrays[k])
@@ -160,6 +161,20 @@ def test_params_and_prescriptions_agree(dump):
     assert cpp["prescriptions"] == bytes(built.prescriptions)
     p = capi.SimParams.from_buffer_copy(cpp["params"])
     assert p.cd_update_freq == 5 and abs(p.beta - 1e-4) < 1e-9 and (p.nvXp2, p.nvYp2, p.nvZp2) == (21, 21, 22)
+
+
+def test_expression_families_agree(dump):
+    """A family whose prescription is an expression goes to deme_set_prescribed_motion from both front ends."""
+    cpp, built = dump
+    lines = [ln.split("|") for ln in cpp["motion"].decode().splitlines()]
+    py = []
+    for m in built.info["motion_expressions"]:
+        py.append([str(m["family"])] + [str(int(bool(m[k]))) for k in ("lin_vel_prescribed", "rot_vel_prescribed",
+                                                                        "lin_pos_prescribed", "rot_pos_prescribed")]
+                  + list(m["lin_vel"]) + list(m["ang_vel"]) + list(m["lin_pos"]))
+    assert lines == py
+    assert lines and lines[0][0] == "5" and lines[0][7] == "0.2 * sin(3000.0 * t)"
+    assert built.prescriptions[5].used == 0
 
 
 @pytest.mark.gpu

@@ -72,8 +72,8 @@ def test_rules_match_the_oracle(graph):
     if graph:
         g.set_graph(True)
     o = oracle(built)
-    steps, t = 40, 0.0
-    h = float(built.params.h)
+    steps, t = 40, np.float32(0.0)
+    h = np.float32(built.params.h)
     for chunk in range(4):
         g.step(steps // 4)
         for _ in range(steps // 4):
@@ -83,7 +83,7 @@ def test_rules_match_the_oracle(graph):
             st["family"] = oracle_rules(built, st, t)
             o.set_state(st)
             o.integrate()
-            t += h
+            t = np.float32(t + h)  # the reference's dT keeps the time as a float
         sg, so = g.state(), o.state()
         np.testing.assert_array_equal(sg["family"], so["family"], err_msg=f"chunk {chunk} families")
         cg, co = g.contacts(), canonical(o.contacts())
