@@ -449,7 +449,7 @@ int32_t deme_set_material(deme_handle* h, uint32_t m, float E, float nu, float C
     const float v[5] = {E, nu, CoR, mu, Crr};
     for (int k = 0; k < 5; k++)
         CUDA_TRY(h, cudaMemcpy(h->mat + (size_t)k * h->nM + m, &v[k], sizeof(float), cudaMemcpyHostToDevice));
-    return DEME_OK;
+    return refresh_material_pairs(h);
 }
 
 int32_t deme_adjoint_set_floors(deme_handle* h, double overlap_rel, double roll_speed, double tangential_force) {

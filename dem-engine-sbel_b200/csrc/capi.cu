@@ -129,6 +129,13 @@ static int32_t ensure_list_keep(deme_handle* h, ContactBuf& b, uint32_t n, uint3
     return DEME_OK;
 }
 
+// The built-in model's contact-pair parameters, recomputed whenever a material changes.
+int32_t refresh_material_pairs(deme_handle* h) {
+    if (!h->matPair) return DEME_OK;
+    launch_material_pairs(h->state_view().mat, h->nM, h->matPair, h->st_dt);
+    return check_launch(h, "material_pairs");
+}
+
 // The count of the list in use, read back after a graph replay produced it on the device.
 int32_t refresh_count(deme_handle* h) {
     if (!h->countStale) return DEME_OK;
@@ -322,6 +329,7 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
     TRY(dalloc_n(h, &h->sMat, nS));
     TRY(dalloc_n(h, &h->masks, DEME_NUM_FAMILY_MASK));
     TRY(dalloc_n(h, &h->mat, 5 * std::max(nM, 1u)));
+    if (nM && nM <= kMaxPairTableMaterials) TRY(dalloc_n(h, &h->matPair, 2 * (size_t)nM * nM));
     TRY(dalloc_n(h, &h->analRaw, std::max(nA, 1u)));
     TRY(dalloc_n(h, &h->analPlaced, std::max(nA, 1u)));
     TRY(dalloc_n(h, &h->presc, DEME_NUM_FAMILIES));
@@ -371,6 +379,7 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
             mat[4 * nM + m] = s->mat_Crr[m];
         }
         CUDA_TRY(h, cudaMemcpy(h->mat, mat.data(), mat.size() * sizeof(float), cudaMemcpyHostToDevice));
+        TRY(refresh_material_pairs(h));
         std::vector<AnalRaw> raw(std::max(nA, 1u));
         for (uint32_t a = 0; a < nA; a++) {
             AnalRaw r{};

@@ -26,6 +26,10 @@ struct MaterialTable {
     const float* CoR;
     const float* mu;
     const float* Crr;
+    // contact-pair parameters precomputed by contact_params for every (a, b) (two float4 per pair: E_cnt, G_cnt,
+    // CoR_cnt, mu_cnt / Crr_cnt, beta), or null: then they are computed per contact
+    const float4* pair = nullptr;
+    uint32_t nM = 0;
 };
 
 // Contact-pair material parameters from the two materials (matProxy2ContactParam, DEMHelperKernels.cu:316-339):
@@ -44,13 +48,36 @@ __device__ __forceinline__ void mat_proxy(T& E_cnt, T& G_cnt, T& CoR_cnt, T& mu_
     Crr_cnt = Crr_A > Crr_B ? Crr_A : Crr_B;
 }
 
+// The parameters of a contact between materials a and b that depend on nothing else: matProxy2ContactParam and
+// the damping ratio beta = ln e / sqrt(ln^2 e + pi^2) of the pair's restitution coefficient, in the reference's
+// precision (FullHertzianForceModel.cu).  The pair table is filled by this same function, so a table entry and an
+// inline evaluation are bit-identical.
+__device__ __forceinline__ void contact_params(const MaterialTable& m, uint32_t a, uint32_t b, float& E_cnt,
+                                               float& G_cnt, float& CoR_cnt, float& mu_cnt, float& Crr_cnt,
+                                               float& beta) {
+    mat_proxy<float>(E_cnt, G_cnt, CoR_cnt, mu_cnt, Crr_cnt, m.E[a], m.nu[a], m.CoR[a], m.mu[a], m.Crr[a], m.E[b],
+                     m.nu[b], m.CoR[b], m.mu[b], m.Crr[b]);
+    const float loge = (float)(((double)CoR_cnt < kTinyFloat) ? log(kTinyFloat) : (double)logf(CoR_cnt));
+    beta = (float)((double)loge / sqrt((double)(loge * loge) + kPiSquared));
+}
+
 __device__ __forceinline__ void hertz_mindlin(const ContactGeom& g, const MaterialTable& m, float ts, float3& force,
                                               float3& torque_only_force, float& delta_tan_x, float& delta_tan_y,
                                               float& delta_tan_z, float& delta_time) {
     // material proxies
-    float E_cnt, G_cnt, CoR_cnt, mu_cnt, Crr_cnt;
-    mat_proxy<float>(E_cnt, G_cnt, CoR_cnt, mu_cnt, Crr_cnt, m.E[g.matA], m.nu[g.matA], m.CoR[g.matA], m.mu[g.matA],
-                     m.Crr[g.matA], m.E[g.matB], m.nu[g.matB], m.CoR[g.matB], m.mu[g.matB], m.Crr[g.matB]);
+    float E_cnt, G_cnt, CoR_cnt, mu_cnt, Crr_cnt, beta;
+    if (m.pair) {
+        const float4* e = m.pair + 2u * ((size_t)g.matA * m.nM + g.matB);
+        const float4 p0 = __ldg(e), p1 = __ldg(e + 1);
+        E_cnt = p0.x;
+        G_cnt = p0.y;
+        CoR_cnt = p0.z;
+        mu_cnt = p0.w;
+        Crr_cnt = p1.x;
+        beta = p1.y;
+    } else {
+        contact_params(m, g.matA, g.matB, E_cnt, G_cnt, CoR_cnt, mu_cnt, Crr_cnt, beta);
+    }
     // rotational velocity of the contact point, mapped to the global frame
     float rAx = g.ARotVel.y * g.locCPA.z - g.ARotVel.z * g.locCPA.y;
     float rAy = g.ARotVel.z * g.locCPA.x - g.ARotVel.x * g.locCPA.z;
@@ -77,8 +104,6 @@ __device__ __forceinline__ void hertz_mindlin(const ContactGeom& g, const Materi
     const float sqrt_Rd = (float)sqrt(g.overlapDepth * (double)(g.ARadius * g.BRadius) /
                                       (double)(g.ARadius + g.BRadius));
     const float Sn = (float)(2. * (double)E_cnt * (double)sqrt_Rd);
-    const float loge = (float)(((double)CoR_cnt < kTinyFloat) ? log(kTinyFloat) : (double)logf(CoR_cnt));
-    const float beta = (float)((double)loge / sqrt((double)(loge * loge) + kPiSquared));
     const float k_n = (float)(kTwoOverThree * (double)Sn);
     const float gamma_n = (float)(kTwoTimesSqrtFiveOverSix * (double)beta * (double)sqrtf(Sn * mass_eff));
     const float scal = (float)((double)k_n * g.overlapDepth + (double)(gamma_n * proj));

@@ -66,6 +66,7 @@ struct deme_handle {
     uint16_t* sMat = nullptr;
     uint8_t* masks = nullptr;
     float* mat = nullptr;  // 5 x nM
+    float4* matPair = nullptr;  // contact-pair parameters, 2 x nM x nM (kMaxPairTableMaterials materials at most)
     AnalRaw* analRaw = nullptr;
     AnalPlaced* analPlaced = nullptr;
     Prescription* presc = nullptr;
@@ -157,7 +158,7 @@ struct deme_handle {
         s.sOwner = sOwner;
         s.sMat = sMat;
         s.masks = masks;
-        s.mat = MaterialTable{mat, mat + nM, mat + 2 * nM, mat + 3 * nM, mat + 4 * nM};
+        s.mat = MaterialTable{mat, mat + nM, mat + 2 * nM, mat + 3 * nM, mat + 4 * nM, matPair, nM};
         s.anal = analPlaced;
         s.nA = nA;
         s.presc = presc;
@@ -171,6 +172,7 @@ void free_checkpoint(deme_handle* h, Checkpoint& c);
 int32_t save_checkpoint(deme_handle* h, Checkpoint& c);
 int32_t restore_checkpoint(deme_handle* h, const Checkpoint& c);
 int32_t refresh_count(deme_handle* h);
+int32_t refresh_material_pairs(deme_handle* h);
 
 #define CUDA_TRY(h, expr)                                                                        \
     do {                                                                                         \

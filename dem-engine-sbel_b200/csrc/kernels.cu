@@ -797,6 +797,21 @@ void launch_advance_time(float* time, float h, const uint32_t* err, cudaStream_t
     k_advance_time<<<1, 1, 0, st>>>(time, h, err);
 }
 __global__ void k_set_time(float* time, float t) { *time = t; }
+
+// The contact-pair parameter table of the built-in model (contact_params for every ordered material pair).
+__global__ void k_material_pairs(MaterialTable m, uint32_t nM, float4* out) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nM * nM) return;
+    float E, G, CoR, mu, Crr, beta;
+    contact_params(m, p / nM, p % nM, E, G, CoR, mu, Crr, beta);
+    out[2u * p] = make_float4(E, G, CoR, mu);
+    out[2u * p + 1u] = make_float4(Crr, beta, 0.f, 0.f);
+}
+void launch_material_pairs(const MaterialTable& m, uint32_t nM, float4* out, cudaStream_t st) {
+    if (!nM || !out) return;
+    ProfScope prof_(KID_OTHER, st);
+    k_material_pairs<<<blocks_for(nM * nM, 256), 256, 0, st>>>(m, nM, out);
+}
 void launch_set_time(float* time, float t, cudaStream_t st) {
     ProfScope prof_(KID_OTHER, st);
     k_set_time<<<1, 1, 0, st>>>(time, t);

@@ -123,6 +123,9 @@ void launch_window_done(const uint32_t* err, uint32_t* done, cudaStream_t st);
 void launch_change_family(ushort4* loc, uint32_t n, uint32_t from, uint32_t to, cudaStream_t st);
 void launch_advance_time(float* time, float h, const uint32_t* err, cudaStream_t st);
 void launch_set_time(float* time, float t, cudaStream_t st);
+// Scenes with at most this many materials keep a table of contact-pair parameters (2 float4 per ordered pair).
+constexpr uint32_t kMaxPairTableMaterials = 256;
+void launch_material_pairs(const MaterialTable& m, uint32_t nM, float4* out, cudaStream_t st);
 void launch_integrate(const SimConsts& k, const StateView& s, cudaStream_t st);
 void launch_kinetic_energy(const SimConsts& k, const StateView& s, uint32_t n_clumps, double* out, cudaStream_t st);
 
