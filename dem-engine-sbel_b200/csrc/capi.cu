@@ -313,6 +313,20 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
                              p->voxel_size * std::ldexp(1.0, p->nvZp2)};
     const double wmax = std::max(world[0], std::max(world[1], world[2]));
     k.prefilter_abs = (float)(4e-7 * wmax + 1e-9);
+    {
+        // sphere id in the low bits of the record's last word, a CD radius bound in the bits above (at least 4 of
+        // them; with fewer the bound is r_max_cd for every sphere)
+        uint32_t idBits = 1;
+        while (idBits < 31 && (1ull << idBits) < (uint64_t)nS) idBits++;
+        if (32 - idBits >= 4) {
+            k.q_shift = idBits;
+            k.q_scale = rmax / (float)((1u << (32 - idBits)) - 1u);
+        } else {
+            k.q_shift = 31;
+            k.q_scale = rmax;
+        }
+        k.id_mask = (1u << k.q_shift) - 1u;
+    }
     set_cell_grid(h, 1.0);
 
     // ---- device arrays ----
@@ -594,6 +608,7 @@ static int32_t cd_search(deme_handle* h, const StateView& s, AnalPlaced* anal, c
     if (retry) launch_cnt_init(k, cd, st);
     launch_pair_find(k, s, cd, h->candCap, h->findShape, st);
     launch_pair_overflow(k, s, cd, h->candCap, st);
+    launch_pair_exact(k, s, cd, h->candCap, st);
     TRY(check_launch(h, "contact search"));
     exclusive_scan_u32_onepass(cd.cnt, h->nS + 1, nb.off, nb.dN, h->scratch, h->dErr, st);
     if (hCnt) {

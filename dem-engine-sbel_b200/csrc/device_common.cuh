@@ -48,6 +48,10 @@ struct SimConsts {
     uint32_t gx, gy, gz;
     float r_max_cd;      // largest CD radius (radius + beta)
     float prefilter_abs; // absolute slack of the float pre-filter
+    // the cell-order float4 records carry the sphere id in their low q_shift bits and, above them, an upper bound
+    // of the CD radius in units of q_scale (see k_gather_sorted)
+    uint32_t q_shift, id_mask;
+    float q_scale;
     uint32_t* err;       // device error block (4 words), see index_ok
 };
 

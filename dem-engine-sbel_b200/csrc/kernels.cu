@@ -149,20 +149,23 @@ __device__ __forceinline__ bool in_range(uint32_t b, uint32_t packed) {
 }
 
 // Cell-order copies of everything the contact search reads, so that a warp (neighbouring cells) reads contiguous
-// memory: position + id for the pre-filter, one 32-byte record (exact position, owner, expanded radius) for the
-// overlap test, bin ranges + family for the contact-point test.
+// memory: position + id + radius bound for the pre-filter, one 32-byte record (exact position, owner, expanded
+// radius) for the overlap test, bin ranges + family for the contact-point test.
 __global__ void k_gather_sorted(SimConsts k, StateView s, CDView cd) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= k.n_spheres) return;
     const uint32_t j = cd.idSorted[i];
     if (!index_ok(k.err, 1, j, k.n_spheres)) return;
     const float4 p = cd.posF[j];
-    cd.posFSorted[i] = make_float4(p.x, p.y, p.z, __uint_as_float(j));
     const double X = cd.pX[j], Y = cd.pY[j], Z = cd.pZ[j];
     const uint32_t o = s.sOwner[j];
     const float r = s.sph[j].w;
     float rf = r;
     rf += k.beta;
+    // CD radius bound: q units of q_scale, rounded up and one unit over, so q * q_scale >= rf despite float rounding
+    const uint32_t qMax = 0xFFFFFFFFu >> k.q_shift;
+    const uint32_t q = k.q_scale > 0.f ? min(qMax, (uint32_t)ceilf(rf / k.q_scale) + 1u) : qMax;
+    cd.posFSorted[i] = make_float4(p.x, p.y, p.z, __uint_as_float(j | (q << k.q_shift)));
     SphCD rec;
     rec.x = X;
     rec.y = Y;
@@ -227,12 +230,12 @@ __device__ __forceinline__ void load_near(const CDView& cd, uint32_t j, SphRec& 
     r.rf = __uint_as_float(zr.w);
 }
 
-__device__ __forceinline__ SphRec load_rec(const CDView& cd, uint32_t j) {
+__device__ __forceinline__ SphRec load_rec(const SimConsts& k, const CDView& cd, uint32_t j) {
     SphRec r;
     load_near(cd, j, r);
     r.rng = __ldg(cd.rngS + j);
     r.fam = r.rng.w;
-    r.id = __float_as_uint(__ldg(&cd.posFSorted[j].w));
+    r.id = __float_as_uint(__ldg(&cd.posFSorted[j].w)) & k.id_mask;
     return r;
 }
 
@@ -262,10 +265,6 @@ __device__ __forceinline__ bool pair_bins(const SimConsts& k, const StateView& s
     const uint32_t bx = sat_u32(cpx / k.bin_size), by = sat_u32(cpy / k.bin_size), bz = sat_u32(cpz / k.bin_size);
     return in_range(bx, a.rng.x) && in_range(by, a.rng.y) && in_range(bz, a.rng.z) && in_range(bx, b.rng.x) &&
            in_range(by, b.rng.y) && in_range(bz, b.rng.z);
-}
-
-__device__ __forceinline__ bool pair_exact(const SimConsts& k, const StateView& s, const SphRec& a, const SphRec& b) {
-    return pair_near(a, b) && pair_bins(k, s, a, b);
 }
 
 // Orders two records by sphere id (selects instead of branching, so a warp runs the test once).
@@ -300,13 +299,15 @@ __device__ __forceinline__ SearchBox search_box(const SimConsts& k, double x, do
 // after i's own row in cell order (all of their cells in the box), and in i's own row the spheres after i.  Every
 // unordered pair of spheres within reach is visited exactly once, by the sphere that comes first in cell order.
 // `visit(j)` receives the cell-order index of each candidate that passes the float pre-filter and lies outside
-// the run of sphere ids `clump` (first, count) that shares i's owner (such pairs are never contacts).
+// the run of sphere ids `clump` (first, count) that shares i's owner (such pairs are never contacts).  The
+// pre-filter has two levels: the distance against `lim2` (i's radius plus the largest radius), then, for the few
+// candidates within it, against i's radius `rfA` plus the candidate's own radius bound from its record.
 #ifndef DEME_FIND_UNROLL
 #define DEME_FIND_UNROLL 4
 #endif
 template <typename Visit>
 __device__ __forceinline__ void for_each_forward_candidate(const SimConsts& k, const CDView& cd, uint32_t i,
-                                                           const float4 fA, const SearchBox& b, float lim2,
+                                                           const float4 fA, const SearchBox& b, float lim2, float rfA,
                                                            uint2 clump, Visit visit) {
     constexpr uint32_t U = DEME_FIND_UNROLL;
     // Rows in order: i's own row (from i + 1), the rest of its z layer, then the later layers.  The next row's
@@ -340,7 +341,12 @@ __device__ __forceinline__ void for_each_forward_candidate(const SimConsts& k, c
                 // explicit fused multiply-adds: the pre-filter only has to be conservative, its margin covers them
                 const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
                 // padding lanes sit 1e30 away and never pass; spheres of i's own clump are skipped by id
-                if (d2 <= lim2 && __float_as_uint(f[u].w) - clump.x >= clump.y) visit(j + u);
+                if (d2 <= lim2) {
+                    const uint32_t wv = __float_as_uint(f[u].w);
+                    const float rb = (float)(wv >> k.q_shift) * k.q_scale;
+                    const float lim = (rfA + rb) * 1.00001f + k.prefilter_abs;
+                    if ((wv & k.id_mask) - clump.x >= clump.y && d2 <= lim * lim) visit(j + u);
+                }
             }
         }
         if (!more) break;
@@ -356,31 +362,17 @@ __device__ __forceinline__ float prefilter_lim2(const SimConsts& k, float rf) {
     return lim * lim;
 }
 
-// Appends found pairs (A, B) to the temporary list with one atomic per warp and counts them on A.  All 32 lanes
-// of the warp call it together.
-__device__ __forceinline__ void append_pairs(const CDView& cd, bool hit, uint32_t A, uint32_t B, uint32_t tempCap) {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t m = __ballot_sync(0xffffffffu, hit);
-    if (!m) return;
-    const uint32_t leader = __ffs(m) - 1u;
-    uint32_t start = 0;
-    if (lane == leader) start = atomicAdd(&cd.counters[0], (uint32_t)__popc(m));
-    start = __shfl_sync(0xffffffffu, start, leader);
-    if (hit) {
-        const uint32_t pos = start + __popc(m & ((1u << lane) - 1u));
-        if (pos < tempCap) cd.candTemp[pos] = make_uint2(A, B);
-        atomicAdd(&cd.cnt[A], 1u);
-    }
-}
-
-// One search pass, threads in cell order (a warp shares neighbour cells), in three phases per warp:
-//   1. each lane runs the cheap float pre-filter over the forward half of its neighbourhood and keeps the
-//      survivors' cell-order indices in shared memory;
-//   2. the warp pools all survivors (prefix sum over lanes), so that
-//   3. all 32 lanes run the double-precision reference predicate on pooled (sphere, candidate) pairs, instead of
-//      the whole warp stepping through the expensive path whenever any one lane has a survivor.
-// Found pairs go to the temporary list (any order) and raise A's count, which was preset to A's number of
-// analytical contacts; a lane with more survivors than it can pool is queued for k_pair_overflow.
+// One search pass in two kernels.
+//   k_pair_find, threads in cell order (a warp shares neighbour cells): each lane runs the float pre-filter over
+//   the forward half of its neighbourhood and keeps the survivors' cell-order indices in shared memory; with both
+//   radii in the pre-filter nearly all survivors are contacts.  The warp then writes all its (sphere, candidate)
+//   survivors to the pair pool with one atomic, coalesced; a lane with more survivors than it can hold is queued
+//   for k_pair_overflow.
+//   k_pair_exact, one thread per pool entry: the double-precision reference predicate, which rewrites the entry as
+//   the pair (A, B) with A < B by sphere id, or as kNoPair, and counts a found pair on A (whose count was preset to
+//   A's number of analytical contacts).
+// Splitting keeps the scan kernel small (more warps resident to hide its loads) and gives the exact test one
+// independent thread per pair.
 
 // Lane that owns pooled pair p: the last lane whose survivor prefix is <= p.
 __device__ __forceinline__ uint32_t pool_owner(const uint32_t* pre, uint32_t p) {
@@ -391,29 +383,31 @@ __device__ __forceinline__ uint32_t pool_owner(const uint32_t* pre, uint32_t p) 
     return L;
 }
 
-// The pooled search comes in a few block shapes (warps per block, survivor slots per lane), chosen per scene by
-// deme_autotune; every shape finds the same pairs.  Each keeps threads x resident blocks at 1,024 per SM, so the
-// register budget (64 per thread) is the same.
+// The search comes in a few block shapes (warps per block, survivor slots per lane), chosen per scene by
+// deme_autotune; every shape finds the same pairs.
+#ifndef DEME_FIND_RESIDENT_WARPS
+#define DEME_FIND_RESIDENT_WARPS 48
+#endif
 template <uint32_t kWarps, uint32_t kSlots>
-__global__ void __launch_bounds__(kWarps * 32, 32 / kWarps) k_pair_find(SimConsts k, StateView s, CDView cd,
-                                                                         uint32_t tempCap) {
+__global__ void __launch_bounds__(kWarps * 32, DEME_FIND_RESIDENT_WARPS / kWarps)
+    k_pair_find(SimConsts k, StateView s, CDView cd, uint32_t tempCap) {
     __shared__ uint32_t s_pre[kWarps][33];           // survivor prefix over lanes
     __shared__ uint32_t s_surv[kWarps][kSlots][32];  // survivors, [slot][lane]
-    __shared__ SphRec s_ctx[kWarps][32];
-    __shared__ uint16_t s_pass[kWarps][32 * kSlots];  // pooled pairs that passed pair_near
     const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     bool valid = i < k.n_spheres;
     uint32_t nSurv = 0;
     if (valid) {
         const float4 fA = __ldg(cd.posFSorted + i);
-        const SphRec me = load_rec(cd, i);
+        SphRec me;
+        load_near(cd, i, me);
+        me.id = __float_as_uint(fA.w) & k.id_mask;
         if (!index_ok(k.err, 12, me.id, k.n_spheres)) {
             valid = false;
         } else {
-            s_ctx[w][lane] = me;
             const SearchBox b = search_box(k, me.x, me.y, me.z, me.rf);
-            for_each_forward_candidate(k, cd, i, fA, b, prefilter_lim2(k, me.rf), __ldg(cd.sClump + me.id), [&](uint32_t j) {
+            for_each_forward_candidate(k, cd, i, fA, b, prefilter_lim2(k, me.rf), me.rf, __ldg(cd.sClump + me.id),
+                                       [&](uint32_t j) {
                 if (nSurv < kSlots) s_surv[w][nSurv][lane] = j;
                 nSurv++;
             });
@@ -431,39 +425,13 @@ __global__ void __launch_bounds__(kWarps * 32, 32 / kWarps) k_pair_find(SimConst
     s_pre[w][lane + 1] = incl;
     if (lane == 0) s_pre[w][0] = 0;
     __syncwarp();
-    // exact reference predicate on pooled pairs, all lanes busy; first the cheap part, whose survivors (about a
-    // third) are pooled again for the contact-point bin test
-    uint32_t nPass = 0;
-    for (uint32_t base = 0; base < totalSurv; base += 32) {
-        const uint32_t p = base + lane;
-        bool pass = false;
-        if (p < totalSurv) {
-            const uint32_t L = pool_owner(s_pre[w], p);
-            SphRec ot;
-            load_near(cd, s_surv[w][p - s_pre[w][L]][L], ot);
-            pass = pair_near(s_ctx[w][L], ot);
-        }
-        const uint32_t m = __ballot_sync(0xffffffffu, pass);
-        if (pass) s_pass[w][nPass + __popc(m & ((1u << lane) - 1u))] = (uint16_t)p;
-        nPass += __popc(m);
-    }
-    __syncwarp();
-    for (uint32_t base = 0; base < nPass; base += 32) {
-        const uint32_t q = base + lane;
-        bool hit = false;
-        uint32_t A = 0, B = 0;
-        if (q < nPass) {
-            const uint32_t p = s_pass[w][q];
-            const uint32_t L = pool_owner(s_pre[w], p);
-            const SphRec ot = load_rec(cd, s_surv[w][p - s_pre[w][L]][L]);
-            SphRec a, b;
-            order_pair(s_ctx[w][L], ot, a, b);
-            hit = pair_bins(k, s, a, b);
-            A = a.id;
-            B = b.id;
-            if (hit && !index_ok(k.err, 14, A, k.n_spheres)) hit = false;
-        }
-        append_pairs(cd, hit, A, B, tempCap);
+    uint32_t base = 0;
+    if (lane == 0 && totalSurv) base = atomicAdd(&cd.counters[0], totalSurv);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    const uint32_t iWarp = i - lane;
+    for (uint32_t p = lane; p < totalSurv; p += 32) {
+        const uint32_t L = pool_owner(s_pre[w], p);
+        if (base + p < tempCap) cd.candTemp[base + p] = make_uint2(iWarp + L, s_surv[w][p - s_pre[w][L]][L]);
     }
     if (ovf) {
         const uint32_t o = atomicAdd(&cd.counters[1], 1u);
@@ -509,27 +477,56 @@ void launch_pair_find(const SimConsts& k, const StateView& s, const CDView& cd, 
     }
 }
 
-// Spheres the pooled search could not hold: the same forward-half search, one thread per sphere, exact test
-// inline.  Grid-stride over the device-side overflow count (no host round trip).
+// Spheres whose survivors k_pair_find could not hold: the same forward-half search, one thread per sphere, each
+// survivor appended to the pair pool for k_pair_exact.  Grid-stride over the device-side overflow count (no host
+// round trip).
 __global__ void __launch_bounds__(128) k_pair_overflow(SimConsts k, StateView s, CDView cd, uint32_t tempCap) {
     const uint32_t nOvf = *((volatile uint32_t*)&cd.counters[1]);
     for (uint32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < nOvf; o += gridDim.x * blockDim.x) {
         const uint32_t i = cd.ovf[o];
         if (!index_ok(k.err, 13, i, k.n_spheres)) continue;
         const float4 fA = __ldg(cd.posFSorted + i);
-        const SphRec me = load_rec(cd, i);
+        SphRec me;
+        load_near(cd, i, me);
+        me.id = __float_as_uint(fA.w) & k.id_mask;
+        if (!index_ok(k.err, 12, me.id, k.n_spheres)) continue;
         const SearchBox b = search_box(k, me.x, me.y, me.z, me.rf);
-        for_each_forward_candidate(k, cd, i, fA, b, prefilter_lim2(k, me.rf), __ldg(cd.sClump + me.id), [&](uint32_t j) {
-            SphRec a, b;
-            order_pair(me, load_rec(cd, j), a, b);
-            if (!pair_exact(k, s, a, b)) return;
-            const uint32_t A = a.id, B = b.id;
-            if (!index_ok(k.err, 14, A, k.n_spheres)) return;
+        for_each_forward_candidate(k, cd, i, fA, b, prefilter_lim2(k, me.rf), me.rf, __ldg(cd.sClump + me.id),
+                                   [&](uint32_t j) {
             const uint32_t pos = atomicAdd(&cd.counters[0], 1u);
-            if (pos < tempCap) cd.candTemp[pos] = make_uint2(A, B);
-            atomicAdd(&cd.cnt[A], 1u);
+            if (pos < tempCap) cd.candTemp[pos] = make_uint2(i, j);
         });
     }
+}
+
+// The reference's pair predicate on every pool entry (cell-order indices of a sphere and its candidate), rewritten
+// in place as the pair (A, B) or kNoPair.  The launch may cover the pool's capacity: it reads the count on the
+// device.  All lanes of a warp reach the end together (no early return), so the count updates stay simple.
+__global__ void __launch_bounds__(256) k_pair_exact(SimConsts k, StateView s, CDView cd, uint32_t tempCap) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n = min(*((volatile uint32_t*)&cd.counters[0]), tempCap);
+    if (p >= n) return;
+    const uint2 ij = cd.candTemp[p];
+    uint2 out = make_uint2(kNoPair, kNoPair);
+    if (index_ok(k.err, 17, ij.x, k.n_spheres) && index_ok(k.err, 18, ij.y, k.n_spheres)) {
+        const SphRec me = load_rec(k, cd, ij.x);
+        const SphRec ot = load_rec(k, cd, ij.y);
+        if (pair_near(me, ot)) {
+            SphRec a, b;
+            order_pair(me, ot, a, b);
+            if (pair_bins(k, s, a, b) && index_ok(k.err, 14, a.id, k.n_spheres)) {
+                out = make_uint2(a.id, b.id);
+                atomicAdd(&cd.cnt[a.id], 1u);
+            }
+        }
+    }
+    cd.candTemp[p] = out;
+}
+
+void launch_pair_exact(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st) {
+    if (!(k.n_spheres) || !tempCap) return;
+    ProfScope prof_(KID_PAIR_EXACT, st);
+    k_pair_exact<<<blocks_for(tempCap, 256), 256, 0, st>>>(k, s, cd, tempCap);
 }
 
 void launch_pair_overflow(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st) {
@@ -562,6 +559,7 @@ __global__ void __launch_bounds__(256) k_pair_scatter(SimConsts k, CDView cd, Co
     if (p == 0 && pool > poolCap) atomicOr(k.err, ERR_CONTACT_CAPACITY);
     if (p >= min(nPairs, min(pool, poolCap))) return;
     const uint2 ab = cd.candTemp[p];
+    if (ab.x == kNoPair) return;  // a pool entry k_pair_exact rejected
     if (!index_ok(k.err, 15, ab.x, k.n_spheres)) return;
     const uint32_t slot = atomicSub(&cd.cnt[ab.x], 1u) - 1u;
     const uint32_t pos = c.off[ab.x] + slot;

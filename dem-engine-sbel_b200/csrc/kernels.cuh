@@ -65,7 +65,8 @@ struct CDView {
     uint32_t* cellStart;  // nCells + 1
     uint8_t* nAnal;
     uint32_t* cnt;
-    uint2* candTemp;      // found sphere pairs (A, B), A < B, in no particular order
+    uint2* candTemp;      // pair pool: survivors (cell-order sphere, candidate), then after k_pair_exact the found
+                          // pairs (A, B), A < B by id, or kNoPair; in no particular order
     uint32_t* ovf;        // spheres with more pre-filter survivors than the pooled search holds
     uint32_t* counters;   // [0] pairs appended, [1] overflow spheres
 };
@@ -107,6 +108,9 @@ void launch_pair_find(const SimConsts& k, const StateView& s, const CDView& cd, 
 int find_shape_count();                                     // block shapes of the pooled search
 void find_shape(int v, uint32_t* warps, uint32_t* slots);  // warps per block and survivor slots per lane of shape v
 void launch_pair_overflow(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st);
+void launch_pair_exact(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st);
+// a pair-pool entry that k_pair_exact rejected
+constexpr uint32_t kNoPair = 0xFFFFFFFFu;
 void launch_cnt_init(const SimConsts& k, const CDView& cd, cudaStream_t st);
 void launch_pair_scatter(const SimConsts& k, const CDView& cd, const ContactView& c, uint32_t nPairs, uint32_t cap,
                          uint32_t poolCap, cudaStream_t st);

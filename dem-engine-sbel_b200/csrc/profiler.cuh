@@ -22,6 +22,7 @@ enum KernelId : int {
     KID_HISTORY,
     KID_FORCE,
     KID_INTEGRATE,
+    KID_PAIR_EXACT,
     KID_OTHER,
     KID_COUNT
 };
