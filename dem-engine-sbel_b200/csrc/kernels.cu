@@ -303,7 +303,7 @@ __device__ __forceinline__ SearchBox search_box(const SimConsts& k, double x, do
 // pre-filter has two levels: the distance against `lim2` (i's radius plus the largest radius), then, for the few
 // candidates within it, against i's radius `rfA` plus the candidate's own radius bound from its record.
 #ifndef DEME_FIND_UNROLL
-#define DEME_FIND_UNROLL 4
+#define DEME_FIND_UNROLL 2
 #endif
 template <typename Visit>
 __device__ __forceinline__ void for_each_forward_candidate(const SimConsts& k, const CDView& cd, uint32_t i,
