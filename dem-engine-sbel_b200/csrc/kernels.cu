@@ -443,7 +443,9 @@ namespace {
 struct FindShape {
     uint32_t warps, slots;
 };
-constexpr FindShape kFindShapes[] = {{4, 16}, {2, 16}, {8, 16}, {4, 8}, {4, 24}};
+// the last shape holds only two survivors per lane, so most spheres go through k_pair_overflow (it keeps that path
+// covered by the shape-equivalence tests; the autotuner rarely keeps it)
+constexpr FindShape kFindShapes[] = {{4, 16}, {2, 16}, {8, 16}, {4, 8}, {4, 24}, {4, 2}};
 constexpr int kNumFindShapes = sizeof(kFindShapes) / sizeof(kFindShapes[0]);
 }  // namespace
 
@@ -471,6 +473,9 @@ void launch_pair_find(const SimConsts& k, const StateView& s, const CDView& cd, 
             break;
         case 4:
             k_pair_find<4, 24><<<blocks_for(n, 128), 128, 0, st>>>(k, s, cd, tempCap);
+            break;
+        case 5:
+            k_pair_find<4, 2><<<blocks_for(n, 128), 128, 0, st>>>(k, s, cd, tempCap);
             break;
         default:
             k_pair_find<4, 16><<<blocks_for(n, 128), 128, 0, st>>>(k, s, cd, tempCap);
