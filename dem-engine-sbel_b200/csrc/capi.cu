@@ -598,11 +598,12 @@ static int32_t cd_search(deme_handle* h, const StateView& s, AnalPlaced* anal, c
     CUDA_TRY(h, cudaMemsetAsync(cd.cellCount, 0, ((size_t)h->nCells + 1) * sizeof(uint32_t), st));
     launch_sphere_prep(k, s, cd, st);
     exclusive_scan_u32_onepass(cd.cellCount, h->nCells + 1, cd.cellStart, nullptr, h->scratch, h->dErr, st);
-    if (h->useOnesweep)
+    if (h->useOnesweep) {
         radix_sort_pairs(cd.cellKey, cd.idSeq, cd.keySorted, cd.idSorted, h->nS, h->cellBits, h->scratch, h->dErr, st);
-    else
-        launch_cell_scatter(k, cd, st);
-    launch_gather_sorted(k, s, cd, st);
+        launch_gather_sorted(k, s, cd, st);
+    } else {
+        launch_cell_scatter(k, s, cd, st);  // counting sort and record writes in one pass
+    }
     ContactBuf& nb = h->lists[h->cur ^ 1];
     CUDA_TRY(h, cudaMemsetAsync(cd.counters, 0, 2 * sizeof(uint32_t), st));
     if (retry) launch_cnt_init(k, cd, st);

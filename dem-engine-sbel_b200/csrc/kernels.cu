@@ -150,12 +150,10 @@ __device__ __forceinline__ bool in_range(uint32_t b, uint32_t packed) {
 
 // Cell-order copies of everything the contact search reads, so that a warp (neighbouring cells) reads contiguous
 // memory: position + id + radius bound for the pre-filter, one 32-byte record (exact position, owner, expanded
-// radius) for the overlap test, bin ranges + family for the contact-point test.
-__global__ void k_gather_sorted(SimConsts k, StateView s, CDView cd) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= k.n_spheres) return;
-    const uint32_t j = cd.idSorted[i];
-    if (!index_ok(k.err, 1, j, k.n_spheres)) return;
+// radius) for the overlap test, bin ranges + family for the contact-point test.  This writes those of sphere j
+// (ID order) into slot i.
+__device__ __forceinline__ void write_cell_records(const SimConsts& k, const StateView& s, const CDView& cd,
+                                                   uint32_t i, uint32_t j) {
     const float4 p = cd.posF[j];
     const double X = cd.pX[j], Y = cd.pY[j], Z = cd.pZ[j];
     const uint32_t o = s.sOwner[j];
@@ -185,24 +183,34 @@ __global__ void k_gather_sorted(SimConsts k, StateView s, CDView cd) {
     cd.rngS[i] = g;
 }
 
+// After a radix sort by cell: slot i gathers sphere idSorted[i].
+__global__ void k_gather_sorted(SimConsts k, StateView s, CDView cd) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= k.n_spheres) return;
+    const uint32_t j = cd.idSorted[i];
+    if (!index_ok(k.err, 1, j, k.n_spheres)) return;
+    write_cell_records(k, s, cd, i, j);
+}
+
 // Counting sort of the spheres by home cell (a radix sort whose single digit spans the cell range): the histogram
 // was taken in k_sphere_prep and scanned into cellStart; each sphere takes a slot of its cell by decrementing the
 // cell's count.  The order inside a cell is not defined, which the search does not depend on (partner lists are
 // sorted when the contact list is assembled).
-__global__ void k_cell_scatter(uint32_t n, const uint32_t* __restrict__ cellKey, const uint32_t* __restrict__ cellStart,
-                               uint32_t* cellCount, uint32_t* idSorted) {
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    const uint32_t key = cellKey[s];
-    const uint32_t slot = cellStart[key] + atomicSub(&cellCount[key], 1u) - 1u;
-    idSorted[slot] = s;
+// Sphere j takes its slot and writes its cell-order records there at once (coalesced reads of j's data, scattered
+// record writes), so no index array is written and gathered again.
+__global__ void k_cell_scatter(SimConsts k, StateView s, CDView cd) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= k.n_spheres) return;
+    const uint32_t key = cd.cellKey[j];
+    const uint32_t slot = cd.cellStart[key] + atomicSub(&cd.cellCount[key], 1u) - 1u;
+    if (!index_ok(k.err, 1, slot, k.n_spheres)) return;
+    write_cell_records(k, s, cd, slot, j);
 }
 
-void launch_cell_scatter(const SimConsts& k, const CDView& cd, cudaStream_t st) {
+void launch_cell_scatter(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st) {
     if (!(k.n_spheres)) return;
     ProfScope prof_(KID_CELL_SCATTER, st);
-    k_cell_scatter<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k.n_spheres, cd.cellKey, cd.cellStart, cd.cellCount,
-                                                                  cd.idSorted);
+    k_cell_scatter<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
 }
 
 void launch_gather_sorted(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st) {

@@ -101,7 +101,7 @@ struct ContactOutputs {
 void launch_place_anal(const SimConsts& k, const StateView& s, const AnalRaw* raw, AnalPlaced* placed, uint32_t nA,
                        cudaStream_t st);
 void launch_sphere_prep(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
-void launch_cell_scatter(const SimConsts& k, const CDView& cd, cudaStream_t st);
+void launch_cell_scatter(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
 void launch_gather_sorted(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
 void launch_pair_find(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, int shape,
                       cudaStream_t st);
