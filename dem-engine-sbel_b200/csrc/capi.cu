@@ -1126,7 +1126,7 @@ int32_t deme_set_search_shape(deme_handle* h, int32_t shape, float cell_factor) 
 
 int32_t deme_search_shape_count(void) { return find_shape_count(); }
 
-// Times every (pooled-search shape, cell factor) pair on a few steps from the same state, keeps the fastest and
+// Times every (candidate-scan shape, cell factor) pair on a few steps from the same state, keeps the fastest and
 // puts the state back.  Every pair gives the same contact lists, so only the time differs.
 int32_t deme_autotune(deme_handle* h, int32_t steps_per_trial, deme_tuning* out) {
     if (!h) return DEME_ERR_INVALID;

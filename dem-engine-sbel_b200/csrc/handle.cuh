@@ -111,7 +111,7 @@ struct deme_handle {
     // Asynchronous contact detection (kT on st_kt, dT on st_dt).  With cdLag > 0 a detection due at step k runs on
     // kT from a snapshot of the owner poses of step k while dT keeps stepping with the current list, and dT adopts
     // the new list at step k + cdLag.
-    // search shape (deme_set_search_shape / deme_autotune): pooled-search block shape and search-cell factor
+    // search shape (deme_set_search_shape / deme_autotune): candidate-scan block shape and search-cell factor
     int32_t findShape = 0;
     float cellFactor = 1.f;
     // CUDA-graph replay of whole steps (deme_set_graph): one executable graph per parity of `cur` at the start of

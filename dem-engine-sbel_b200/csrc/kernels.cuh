@@ -67,8 +67,8 @@ struct CDView {
     uint32_t* cnt;
     uint2* candTemp;      // pair pool: survivors (cell-order sphere, candidate), then after k_pair_exact the found
                           // pairs (A, B), A < B by id, or kNoPair; in no particular order
-    uint32_t* ovf;        // spheres with more pre-filter survivors than the pooled search holds
-    uint32_t* counters;   // [0] pairs appended, [1] overflow spheres
+    uint32_t* ovf;        // spheres with more pre-filter survivors than the candidate scan's slots hold
+    uint32_t* counters;   // [0] pair-pool entries (survivors) appended, [1] overflow spheres
 };
 
 // One contact list (kT product) with its history wildcards.
@@ -105,7 +105,7 @@ void launch_cell_scatter(const SimConsts& k, const StateView& s, const CDView& c
 void launch_gather_sorted(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
 void launch_pair_find(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, int shape,
                       cudaStream_t st);
-int find_shape_count();                                     // block shapes of the pooled search
+int find_shape_count();                                     // block shapes of the candidate scan
 void find_shape(int v, uint32_t* warps, uint32_t* slots);  // warps per block and survivor slots per lane of shape v
 void launch_pair_overflow(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st);
 void launch_pair_exact(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st);

@@ -327,7 +327,7 @@ int32_t deme_set_graph(deme_handle* h, int32_t enable);
 int32_t deme_graph_stats(deme_handle* h, int64_t* replays, int64_t* rollbacks);
 
 /* Search shape (no reference counterpart: the reference's bin size, SetInitBinSize, sets both its bins and its
- * work per thread).  `shape` picks a block shape of the pooled pair search (index < deme_search_shape_count();
+ * work per thread).  `shape` picks a block shape of the candidate scan (index < deme_search_shape_count();
  * 0, the default, is 4 warps with 16 survivor slots per lane) and `cell_factor` in [1, 4] scales the search cells
  * (edge cell_factor x max(bin size, largest expanded diameter)).  Every shape finds the same contacts. */
 int32_t deme_set_search_shape(deme_handle* h, int32_t shape, float cell_factor);
@@ -335,7 +335,7 @@ int32_t deme_search_shape_count(void);
 
 typedef struct {
     int32_t shape;         /* index passed to deme_set_search_shape */
-    int32_t find_warps;    /* warps per block of the pooled search */
+    int32_t find_warps;    /* warps per block of the candidate scan */
     int32_t find_slots;    /* survivor slots per lane */
     float cell_factor;
     float ms_per_step;     /* the chosen shape's time per step in the trials */
