@@ -778,8 +778,16 @@ int32_t deme_compute_forces(deme_handle* h) {
         if (!h->capturing) TRY(ensure_outputs(h, nL));
         out = &h->outs;
     }
-    AnalAccum aa{nullptr, h->nClumps, h->nO - h->nClumps, h->nO - h->nClumps > 64};
+    AnalAccum aa{nullptr, nullptr, h->nClumps, h->nO - h->nClumps, h->nO - h->nClumps > 64};
     if (aa.nAO && !aa.direct) {
+        if (!h->analChunks) {
+            if (h->capturing) {
+                h->err = "graph recording: wall partial sums not allocated";
+                return DEME_ERR_STATE;
+            }
+            TRY(dalloc_n(h, &h->analChunks, (size_t)6u * aa.nAO * kAnalChunks));
+        }
+        aa.chunks = h->analChunks;
         const size_t need = (size_t)force_blocks(std::max(nL, 1u)) * 6u * aa.nAO;
         if (need > h->analPartialCap && h->capturing) {
             h->err = "graph recording: wall partials not sized for the list capacity";
@@ -941,6 +949,7 @@ static int32_t graph_prepare(deme_handle* h) {
             TRY(dalloc_n(h, &h->analPartial, need + need / 4 + 64));
             h->analPartialCap = need + need / 4 + 64;
         }
+        if (!h->analChunks) TRY(dalloc_n(h, &h->analChunks, (size_t)6u * nAO * kAnalChunks));
     }
     return DEME_OK;
 }

@@ -11,11 +11,13 @@
 
 namespace deme_b200 {
 
+// 128-thread blocks, 8 resident per SM (64 registers a thread): smaller blocks wait less at the block-wide
+// barriers (the voided-step check and the wall partials) than 256 x 4 or 512 x 2.
 #ifndef DEME_FORCE_THREADS
-#define DEME_FORCE_THREADS 256
+#define DEME_FORCE_THREADS 128
 #endif
 #ifndef DEME_FORCE_MIN_BLOCKS
-#define DEME_FORCE_MIN_BLOCKS 4
+#define DEME_FORCE_MIN_BLOCKS 8
 #endif
 constexpr uint32_t kForceThreads = DEME_FORCE_THREADS;
 template <bool kStore>

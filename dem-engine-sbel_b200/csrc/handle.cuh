@@ -96,6 +96,7 @@ struct deme_handle {
     double* hKE = nullptr;
     Prescription* hPresc = nullptr;
     float* analPartial = nullptr;
+    float* analChunks = nullptr;  // range sums of the wall partials (6 x analytical owners x kAnalChunks)
     size_t analPartialCap = 0;
     double t = 0.0;
     float tf = 0.f;  // the time as the reference's dT keeps it (a float, advanced by h each step): rules and

@@ -725,27 +725,36 @@ void launch_count_by_sphere(const uint32_t* idA, uint32_t n, uint32_t* cnt, cuda
 
 // ------------------------------------------------------------------------------------------------------------
 // Fused force + collection kernel.
-// Sum the per-block partials of each analytical owner in block order (deterministic) into its accumulators.
-__global__ void k_anal_reduce(AnalAccum aa, uint32_t nBlocks, float4* acc, float4* alpha, const uint32_t* err,
-                              const uint32_t* dN) {
+// The per-block partials of each analytical owner summed in a fixed order (deterministic) into its accumulators,
+// in two kernels so that the whole GPU takes part: block (owner component, chunk) sums the partials of a contiguous
+// range of force blocks with a fixed tree, then one thread per owner component adds its chunk sums in order.
+__global__ void k_anal_reduce(AnalAccum aa, uint32_t nBlocks, const uint32_t* err, const uint32_t* dN) {
     __shared__ float sh[256];
     if (__syncthreads_or(threadIdx.x == 0 && *err != 0u)) return;  // a voided step (see k_force)
     // only the force blocks that held contacts wrote partials
     if (dN) nBlocks = min(nBlocks, (*dN + kForceThreads - 1) / kForceThreads);
-    const uint32_t slot = blockIdx.x / 6u, comp = blockIdx.x % 6u;
+    const uint32_t sc = blockIdx.x, chunk = blockIdx.y;
+    const uint32_t slot = sc / 6u, comp = sc % 6u;
+    const uint32_t len = (nBlocks + kAnalChunks - 1u) / kAnalChunks;
+    const uint32_t b0 = chunk * len, b1 = min(nBlocks, b0 + len);
     float v = 0.f;
-    for (uint32_t b = threadIdx.x; b < nBlocks; b += blockDim.x) v += aa.partial[(size_t)b * 6u * aa.nAO + 6u * slot + comp];
+    for (uint32_t b = b0 + threadIdx.x; b < b1; b += blockDim.x) v += aa.partial[(size_t)b * 6u * aa.nAO + 6u * slot + comp];
     sh[threadIdx.x] = v;
     __syncthreads();
     for (uint32_t w = blockDim.x / 2; w > 0; w >>= 1) {
         if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        const uint32_t o = aa.nClumps + slot;
-        float* dst = comp < 3 ? &acc[o].x : &alpha[o].x;
-        dst[comp % 3] = sh[0];
-    }
+    if (threadIdx.x == 0) aa.chunks[sc * kAnalChunks + chunk] = sh[0];
+}
+__global__ void k_anal_reduce_final(AnalAccum aa, float4* acc, float4* alpha, const uint32_t* err) {
+    const uint32_t sc = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sc >= 6u * aa.nAO || *err != 0u) return;
+    float v = 0.f;
+    for (uint32_t c = 0; c < kAnalChunks; c++) v += aa.chunks[sc * kAnalChunks + c];
+    const uint32_t o = aa.nClumps + sc / 6u, comp = sc % 6u;
+    float* dst = comp < 3 ? &acc[o].x : &alpha[o].x;
+    dst[comp % 3] = v;
 }
 
 void launch_force(const SimConsts& k, const StateView& s, const ContactView& c, uint32_t n, bool has_hist,
@@ -775,7 +784,11 @@ void launch_force(const SimConsts& k, const StateView& s, const ContactView& c, 
     }
     if (partials) {
         ProfScope prof_(KID_OTHER, st);
-        k_anal_reduce<<<6u * aa.nAO, 256, 0, st>>>(aa, nb, s.acc, s.alpha, k.err, c.dN);
+        k_anal_reduce<<<dim3(6u * aa.nAO, kAnalChunks), 256, 0, st>>>(aa, nb, k.err, c.dN);
+    }
+    if (partials) {
+        ProfScope prof_(KID_OTHER, st);
+        k_anal_reduce_final<<<blocks_for(6u * aa.nAO, 128), 128, 0, st>>>(aa, s.acc, s.alpha, k.err);
     }
 }
 

@@ -85,6 +85,7 @@ struct ContactView {
 // Reactions on analytical owners (walls): block partials, reduced in fixed order.
 struct AnalAccum {
     float* partial;     // blocks x nAO x 6
+    float* chunks;      // (nAO x 6) x kAnalChunks sums of contiguous ranges of block partials
     uint32_t nClumps;   // analytical owners are [nClumps, nClumps + nAO)
     uint32_t nAO;
     bool direct;        // many analytical owners: float atomics onto their accumulators instead of partials
@@ -109,6 +110,8 @@ int find_shape_count();                                     // block shapes of t
 void find_shape(int v, uint32_t* warps, uint32_t* slots);  // warps per block and survivor slots per lane of shape v
 void launch_pair_overflow(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st);
 void launch_pair_exact(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st);
+// ranges the wall partials of the force blocks are first summed over (then the range sums, in order)
+constexpr uint32_t kAnalChunks = 32;
 // a pair-pool entry that k_pair_exact rejected
 constexpr uint32_t kNoPair = 0xFFFFFFFFu;
 void launch_cnt_init(const SimConsts& k, const CDView& cd, cudaStream_t st);
