@@ -528,6 +528,8 @@ void deme_destroy(deme_handle* h) {
     if (h->hErr) cudaFreeHost(h->hErr);
     if (h->hKE) cudaFreeHost(h->hKE);
     if (h->hPresc) cudaFreeHost(h->hPresc);
+    for (cudaEvent_t e : h->prescDone)
+        if (e) cudaEventDestroy(e);
     if (h->hCounts) cudaFreeHost(h->hCounts);
     for (cudaEvent_t e : {h->evPose, h->evCounts, h->evListReady, h->evListReleased})
         if (e) cudaEventDestroy(e);
@@ -1421,9 +1423,15 @@ int32_t deme_download_contact_forces(deme_handle* h, deme_contact_forces* o) {
 
 int32_t deme_set_family_prescription(deme_handle* h, int32_t family, const deme_family_prescription* src) {
     if (!h || !src || family < 0 || family >= DEME_NUM_FAMILIES) return DEME_ERR_INVALID;
-    if (!h->hPresc) CUDA_TRY(h, cudaMallocHost(&h->hPresc, sizeof(Prescription)));
-    CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));  // the staging buffer may still feed an earlier copy
-    Prescription& q = *h->hPresc;
+    if (!h->hPresc) {
+        CUDA_TRY(h, cudaMallocHost(&h->hPresc, deme_handle::kPrescSlots * sizeof(Prescription)));
+        for (cudaEvent_t& e : h->prescDone) CUDA_TRY(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    // a ring of staging slots: only a slot whose earlier copy has not run yet is waited for
+    const int slot = h->prescNext;
+    h->prescNext = (slot + 1) % deme_handle::kPrescSlots;
+    CUDA_TRY(h, cudaEventSynchronize(h->prescDone[slot]));
+    Prescription& q = h->hPresc[slot];
     q = Prescription{};
     q.used = src->used;
     q.lin_vel = src->lin_vel_prescribed;
@@ -1438,7 +1446,8 @@ int32_t deme_set_family_prescription(deme_handle* h, int32_t family, const deme_
         q.omg[c] = src->omg[c];
         q.pos[c] = src->pos[c];
     }
-    CUDA_TRY(h, cudaMemcpyAsync(h->presc + family, h->hPresc, sizeof(Prescription), cudaMemcpyHostToDevice, h->st_dt));
+    CUDA_TRY(h, cudaMemcpyAsync(h->presc + family, &q, sizeof(Prescription), cudaMemcpyHostToDevice, h->st_dt));
+    CUDA_TRY(h, cudaEventRecord(h->prescDone[slot], h->st_dt));
     return DEME_OK;
 }
 

@@ -94,7 +94,11 @@ struct deme_handle {
     uint32_t* hErr = nullptr;
     double* dKE = nullptr;
     double* hKE = nullptr;
+    // pinned staging ring for deme_set_family_prescription: slot i may be rewritten once its copy has run
+    static constexpr int kPrescSlots = 8;
     Prescription* hPresc = nullptr;
+    cudaEvent_t prescDone[kPrescSlots] = {};
+    int prescNext = 0;
     float* analPartial = nullptr;
     float* analChunks = nullptr;  // range sums of the wall partials (6 x analytical owners x kAnalChunks)
     size_t analPartialCap = 0;
