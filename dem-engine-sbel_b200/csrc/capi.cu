@@ -1040,7 +1040,14 @@ static int32_t step_graph(deme_handle* h, int32_t n_steps) {
         }
         CUDA_TRY(h, cudaMemcpyAsync(h->hWindows, h->dWindows, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->st_dt));
         CUDA_TRY(h, cudaMemcpyAsync(h->hWindows + 1, h->dErr, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->st_dt));
+        // the count of the list in use comes back with them, so the next call needs no read of its own
+        CUDA_TRY(h, cudaMemcpyAsync(h->hTotal + 3, h->lists[h->cur].dN, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                    h->st_dt));
         CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
+        if (!h->hWindows[1]) {
+            h->nContacts = h->hTotal[3];
+            h->countStale = false;
+        }
         if (h->hWindows[1]) {
             // a list or the pair pool outgrew its capacity in window `done`: the state and the list in use are those
             // its detection started from; redo the rest step by step
