@@ -1233,57 +1233,55 @@ int32_t deme_sync(deme_handle* h) {
 }
 
 // ---------------------------------------------------------------------------------------------- transfer ----
-int32_t deme_download_state(deme_handle* h, deme_state* o) {
-    if (!h || !o) return DEME_ERR_INVALID;
-    const uint32_t n = h->nO;
-    CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
-    std::vector<ushort4> loc(n);
-    std::vector<float4> q(n), v(n), w(n), a(n), al(n);
-    CUDA_TRY(h, cudaMemcpy(loc.data(), h->loc, n * sizeof(ushort4), cudaMemcpyDeviceToHost));
-    CUDA_TRY(h, cudaMemcpy(q.data(), h->quat, n * sizeof(float4), cudaMemcpyDeviceToHost));
-    CUDA_TRY(h, cudaMemcpy(v.data(), h->vel, n * sizeof(float4), cudaMemcpyDeviceToHost));
-    CUDA_TRY(h, cudaMemcpy(w.data(), h->omg, n * sizeof(float4), cudaMemcpyDeviceToHost));
-    CUDA_TRY(h, cudaMemcpy(a.data(), h->acc, n * sizeof(float4), cudaMemcpyDeviceToHost));
-    CUDA_TRY(h, cudaMemcpy(al.data(), h->alpha, n * sizeof(float4), cudaMemcpyDeviceToHost));
-    if (o->voxel) CUDA_TRY(h, cudaMemcpy(o->voxel, h->voxel, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
-    for (uint32_t i = 0; i < n; i++) {
-        if (o->locX) o->locX[i] = loc[i].x;
-        if (o->locY) o->locY[i] = loc[i].y;
-        if (o->locZ) o->locZ[i] = loc[i].z;
-        if (o->family) o->family[i] = (uint8_t)loc[i].w;
-        if (o->oriQw) o->oriQw[i] = q[i].x;
-        if (o->oriQx) o->oriQx[i] = q[i].y;
-        if (o->oriQy) o->oriQy[i] = q[i].z;
-        if (o->oriQz) o->oriQz[i] = q[i].w;
-        if (o->vX) o->vX[i] = v[i].x;
-        if (o->vY) o->vY[i] = v[i].y;
-        if (o->vZ) o->vZ[i] = v[i].z;
-        if (o->omgX) o->omgX[i] = w[i].x;
-        if (o->omgY) o->omgY[i] = w[i].y;
-        if (o->omgZ) o->omgZ[i] = w[i].z;
-        if (o->aX) o->aX[i] = a[i].x;
-        if (o->aY) o->aY[i] = a[i].y;
-        if (o->aZ) o->aZ[i] = a[i].z;
-        if (o->alphaX) o->alphaX[i] = al[i].x;
-        if (o->alphaY) o->alphaY[i] = al[i].y;
-        if (o->alphaZ) o->alphaZ[i] = al[i].z;
+// Owners [first, first + count) between the device arrays and a deme_state whose arrays hold `count` entries (any
+// array may be NULL).  An upload reads the packed records back first, so fields the caller leaves NULL keep their
+// device values.
+static int32_t transfer_state(deme_handle* h, uint32_t first, uint32_t count, deme_state* o, const deme_state* in) {
+    if ((uint64_t)first + count > h->nO) {
+        h->err = "owner range [" + std::to_string(first) + ", " + std::to_string((uint64_t)first + count) +
+                 ") beyond the " + std::to_string(h->nO) + " owners";
+        return DEME_ERR_INVALID;
     }
-    return DEME_OK;
-}
-
-int32_t deme_upload_state(deme_handle* h, const deme_state* s) {
-    if (!h || !s) return DEME_ERR_INVALID;
-    TRY(cd_cancel(h));
-    const uint32_t n = h->nO;
+    if (in) TRY(cd_cancel(h));
     CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
+    const uint32_t n = count;
+    if (n == 0) return DEME_OK;
     std::vector<ushort4> loc(n);
     std::vector<float4> q(n), v(n), w(n), a(n), al(n);
-    CUDA_TRY(h, cudaMemcpy(loc.data(), h->loc, n * sizeof(ushort4), cudaMemcpyDeviceToHost));
-    CUDA_TRY(h, cudaMemcpy(q.data(), h->quat, n * sizeof(float4), cudaMemcpyDeviceToHost));
-    CUDA_TRY(h, cudaMemcpy(v.data(), h->vel, n * sizeof(float4), cudaMemcpyDeviceToHost));
-    CUDA_TRY(h, cudaMemcpy(w.data(), h->omg, n * sizeof(float4), cudaMemcpyDeviceToHost));
-    CUDA_TRY(h, cudaMemcpy(a.data(), h->acc, n * sizeof(float4), cudaMemcpyDeviceToHost));
-    CUDA_TRY(h, cudaMemcpy(al.data(), h->alpha, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(loc.data(), h->loc + first, n * sizeof(ushort4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(q.data(), h->quat + first, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(v.data(), h->vel + first, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(w.data(), h->omg + first, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(a.data(), h->acc + first, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(al.data(), h->alpha + first, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    if (o) {
+        if (o->voxel)
+            CUDA_TRY(h, cudaMemcpy(o->voxel, h->voxel + first, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+        for (uint32_t i = 0; i < n; i++) {
+            if (o->locX) o->locX[i] = loc[i].x;
+            if (o->locY) o->locY[i] = loc[i].y;
+            if (o->locZ) o->locZ[i] = loc[i].z;
+            if (o->family) o->family[i] = (uint8_t)loc[i].w;
+            if (o->oriQw) o->oriQw[i] = q[i].x;
+            if (o->oriQx) o->oriQx[i] = q[i].y;
+            if (o->oriQy) o->oriQy[i] = q[i].z;
+            if (o->oriQz) o->oriQz[i] = q[i].w;
+            if (o->vX) o->vX[i] = v[i].x;
+            if (o->vY) o->vY[i] = v[i].y;
+            if (o->vZ) o->vZ[i] = v[i].z;
+            if (o->omgX) o->omgX[i] = w[i].x;
+            if (o->omgY) o->omgY[i] = w[i].y;
+            if (o->omgZ) o->omgZ[i] = w[i].z;
+            if (o->aX) o->aX[i] = a[i].x;
+            if (o->aY) o->aY[i] = a[i].y;
+            if (o->aZ) o->aZ[i] = a[i].z;
+            if (o->alphaX) o->alphaX[i] = al[i].x;
+            if (o->alphaY) o->alphaY[i] = al[i].y;
+            if (o->alphaZ) o->alphaZ[i] = al[i].z;
+        }
+        return DEME_OK;
+    }
+    const deme_state* s = in;
     for (uint32_t i = 0; i < n; i++) {
         if (s->locX) loc[i].x = s->locX[i];
         if (s->locY) loc[i].y = s->locY[i];
@@ -1306,14 +1304,34 @@ int32_t deme_upload_state(deme_handle* h, const deme_state* s) {
         if (s->alphaY) al[i].y = s->alphaY[i];
         if (s->alphaZ) al[i].z = s->alphaZ[i];
     }
-    if (s->voxel) CUDA_TRY(h, cudaMemcpy(h->voxel, s->voxel, n * sizeof(uint64_t), cudaMemcpyHostToDevice));
-    CUDA_TRY(h, cudaMemcpy(h->loc, loc.data(), n * sizeof(ushort4), cudaMemcpyHostToDevice));
-    CUDA_TRY(h, cudaMemcpy(h->quat, q.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
-    CUDA_TRY(h, cudaMemcpy(h->vel, v.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
-    CUDA_TRY(h, cudaMemcpy(h->omg, w.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
-    CUDA_TRY(h, cudaMemcpy(h->acc, a.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
-    CUDA_TRY(h, cudaMemcpy(h->alpha, al.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    if (s->voxel) CUDA_TRY(h, cudaMemcpy(h->voxel + first, s->voxel, n * sizeof(uint64_t), cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(h->loc + first, loc.data(), n * sizeof(ushort4), cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(h->quat + first, q.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(h->vel + first, v.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(h->omg + first, w.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(h->acc + first, a.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(h->alpha + first, al.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
     return DEME_OK;
+}
+
+int32_t deme_download_state(deme_handle* h, deme_state* o) {
+    if (!h || !o) return DEME_ERR_INVALID;
+    return transfer_state(h, 0, h->nO, o, nullptr);
+}
+
+int32_t deme_upload_state(deme_handle* h, const deme_state* s) {
+    if (!h || !s) return DEME_ERR_INVALID;
+    return transfer_state(h, 0, h->nO, nullptr, s);
+}
+
+int32_t deme_download_state_range(deme_handle* h, uint32_t first, uint32_t count, deme_state* o) {
+    if (!h || !o) return DEME_ERR_INVALID;
+    return transfer_state(h, first, count, o, nullptr);
+}
+
+int32_t deme_upload_state_range(deme_handle* h, uint32_t first, uint32_t count, const deme_state* s) {
+    if (!h || !s) return DEME_ERR_INVALID;
+    return transfer_state(h, first, count, nullptr, s);
 }
 
 int32_t deme_get_num_contacts(deme_handle* h, uint32_t* n) {
@@ -1431,8 +1449,12 @@ int32_t deme_download_contact_forces(deme_handle* h, deme_contact_forces* o) {
 int32_t deme_set_family_prescription(deme_handle* h, int32_t family, const deme_family_prescription* src) {
     if (!h || !src || family < 0 || family >= DEME_NUM_FAMILIES) return DEME_ERR_INVALID;
     if (!h->hPresc) {
-        CUDA_TRY(h, cudaMallocHost(&h->hPresc, deme_handle::kPrescSlots * sizeof(Prescription)));
-        for (cudaEvent_t& e : h->prescDone) CUDA_TRY(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        // the events first: the ring counts as set up (hPresc non-null) only once every slot has its event
+        for (cudaEvent_t& e : h->prescDone)
+            if (!e) CUDA_TRY(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        Prescription* ring = nullptr;
+        CUDA_TRY(h, cudaMallocHost(&ring, deme_handle::kPrescSlots * sizeof(Prescription)));
+        h->hPresc = ring;
     }
     // a ring of staging slots: only a slot whose earlier copy has not run yet is waited for
     const int slot = h->prescNext;
@@ -1469,6 +1491,22 @@ int32_t deme_get_time(deme_handle* h, double* t, int64_t* steps) {
     if (!h) return DEME_ERR_INVALID;
     if (t) *t = h->t;
     if (steps) *steps = h->steps;
+    return DEME_OK;
+}
+
+int32_t deme_set_time(deme_handle* h, double t, float t_float, int64_t steps) {
+    if (!h || steps < 0) return DEME_ERR_INVALID;
+    TRY(cd_finish(h));
+    h->t = t;
+    h->tf = t_float;
+    h->steps = steps;
+    if (h->dTime) launch_set_time(h->dTime, h->tf, h->st_dt);
+    return check_launch(h, "set_time");
+}
+
+int32_t deme_get_time_float(deme_handle* h, float* t_float) {
+    if (!h || !t_float) return DEME_ERR_INVALID;
+    *t_float = h->tf;
     return DEME_OK;
 }
 

@@ -7,8 +7,13 @@
 // __device__ array, so every device that loads this library holds kStaticSortScratchBytes until the process
 // exits.  Host code cannot use the array's name as a device pointer (on the host it names a stand-in object), so
 // its device address is looked up with cudaGetSymbolAddress once per device, on the first call made with that
-// device current, and passed to the kernels.  Nothing here calls cudaMalloc/cudaFree or any allocating library
-// routine.
+// device current, and passed to the kernels.  That address is kept for the life of the process, so calls after a
+// cudaDeviceReset of that device are not supported.  Nothing here calls cudaMalloc/cudaFree or any allocating
+// library routine.
+//
+// deme_radix_sort_status reads back the error word of a sort (this one's, or the allocating sort's in its caller's
+// scratch): a look-back wait of the sort that ran out of its iteration limit leaves the output unordered, and only
+// the word tells.
 #include <mutex>
 
 #include "../../include/deme_b200.h"
@@ -64,4 +69,24 @@ extern "C" int32_t deme_radix_sort_pairs_static(const uint32_t* keys_in, const u
     if (cudaMemsetAsync(err, 0, sizeof(uint32_t), st) != cudaSuccess) return DEME_ERR_CUDA;
     deme_b200::radix_sort_pairs(keys_in, vals_in, keys_out, vals_out, n, key_bits, scratch, err, st);
     return cudaGetLastError() == cudaSuccess ? DEME_OK : DEME_ERR_CUDA;
+}
+
+extern "C" int32_t deme_radix_sort_status(const void* scratch, uint32_t n, void* stream, uint32_t* word) {
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint32_t* err = nullptr;
+    if (scratch) {
+        // deme_radix_sort_pairs_device: the word follows the sort's own scratch in the caller's buffer
+        err = reinterpret_cast<const uint32_t*>(static_cast<const uint8_t*>(scratch) +
+                                                deme_b200::radix_sort_scratch_bytes(n));
+    } else {
+        uint8_t* base = nullptr;
+        const int32_t rc = static_scratch(st, &base);
+        if (rc != DEME_OK) return rc;
+        err = reinterpret_cast<const uint32_t*>(base + kErrOffset);
+    }
+    uint32_t w = 0;
+    if (cudaMemcpyAsync(&w, err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess) return DEME_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return DEME_ERR_CUDA;
+    if (word) *word = w;
+    return w == 0u ? DEME_OK : DEME_ERR_TIMEOUT;
 }

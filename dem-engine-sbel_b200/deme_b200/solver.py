@@ -260,6 +260,20 @@ class Solver(HandleSolver):
         self.lib.deme_set_time_step.argtypes = [C.c_void_p, C.c_float]
         self._check(self.lib.deme_set_time_step(self.h, h), "set_time_step")
 
+    def time(self) -> tuple[float, float, int]:
+        """(time, the reference's float time, steps taken)."""
+        t, tf, n = C.c_double(0), C.c_float(0), C.c_int64(0)
+        self.lib.deme_get_time.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+        self.lib.deme_get_time_float.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
+        self._check(self.lib.deme_get_time(self.h, C.byref(t), C.byref(n)), "get_time")
+        self._check(self.lib.deme_get_time_float(self.h, C.byref(tf)), "get_time_float")
+        return float(t.value), float(tf.value), int(n.value)
+
+    def set_time(self, t: float, t_float: float, steps: int):
+        """Carries a run's time and step counter over into this handle."""
+        self.lib.deme_set_time.argtypes = [C.c_void_p, C.c_double, C.c_float, C.c_int64]
+        self._check(self.lib.deme_set_time(self.h, t, t_float, int(steps)), "set_time")
+
     def set_streams(self, kt_stream: int | None, dt_stream: int | None):
         self.lib.deme_set_streams.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         self._check(self.lib.deme_set_streams(self.h, kt_stream, dt_stream), "set_streams")

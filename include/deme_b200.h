@@ -271,6 +271,11 @@ int32_t deme_sync(deme_handle* h);
 /* State and contact transfer (GetOwner* / SetOwner*, src/DEM/API.h:196-214; WriteContactFile, API.h:324). */
 int32_t deme_download_state(deme_handle* h, deme_state* out);
 int32_t deme_upload_state(deme_handle* h, const deme_state* in);
+/* The same for owners [first, first + count) only; the arrays of the struct hold `count` entries.  An upload
+ * leaves the fields whose arrays are NULL as they were.  This is what one owner's GetOwner* / SetOwner* costs in
+ * the reference (dT::getOwnerPos / setOwnerPos and their siblings, src/DEM/dT.cpp:1705-1810). */
+int32_t deme_download_state_range(deme_handle* h, uint32_t first, uint32_t count, deme_state* out);
+int32_t deme_upload_state_range(deme_handle* h, uint32_t first, uint32_t count, const deme_state* in);
 int32_t deme_get_num_contacts(deme_handle* h, uint32_t* n);
 int32_t deme_download_contacts(deme_handle* h, deme_contacts* out);
 /* Replace the current contact list and its wildcards (history); mapping is ignored.  Used to inject identical
@@ -389,6 +394,12 @@ int32_t deme_set_time_step(deme_handle* h, float h_step);
 
 /* Simulation time advanced so far and step counter. */
 int32_t deme_get_time(deme_handle* h, double* t, int64_t* steps);
+/* The time as the reference's dT keeps it (timeElapsed, a float advanced by h every step, src/DEM/dT.h:216): what
+ * prescribed-motion expressions and family-change rules see. */
+int32_t deme_get_time_float(deme_handle* h, float* t_float);
+/* Sets the time (double and the reference's float), and the step counter that schedules contact detection.  Used to
+ * carry a run over into a new handle (UpdateClumps, src/DEM/APIPublic.cpp:792-843, keeps the simulation time). */
+int32_t deme_set_time(deme_handle* h, double t, float t_float, int64_t steps);
 /* Sum of 0.5 m v^2 + 0.5 I omega^2 over clump owners (DEMOwnerQueryKernels.cu:10-37 computes the per-owner term;
  * the reference's GetTotalKineticEnergy returns 0, src/DEM/dT.cpp:154-171). */
 int32_t deme_kinetic_energy(deme_handle* h, double* ke);
@@ -401,11 +412,21 @@ int32_t deme_bin_assignment(deme_handle* h, uint16_t* n_bins_per_sphere, uint8_t
                             uint32_t pair_capacity, uint32_t* bin_ids, uint32_t* sphere_ids, uint32_t* n_pairs);
 
 /* Stable radix sort of (key, value) u32 pairs held in device memory (project-written onesweep sort; replaces
- * cub::DeviceRadixSort::SortPairs, src/algorithms/DEMCubWrappers.cu:43-59).  Sorts bits [0, key_bits). */
+ * cub::DeviceRadixSort::SortPairs, src/algorithms/DEMCubWrappers.cu:43-59).  Sorts bits [0, key_bits).
+ * The call returns once the work is queued on `stream`; its error word sits in the last 16 bytes of `scratch`
+ * (offset deme_radix_sort_scratch_bytes(n) - 16) and is read with deme_radix_sort_status. */
 int32_t deme_radix_sort_pairs_device(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                                      uint32_t* vals_out, uint32_t n, int32_t key_bits, void* scratch,
                                      size_t scratch_bytes, void* stream);
 size_t deme_radix_sort_scratch_bytes(uint32_t n);
+
+/* Outcome of the last sort queued on `stream`: scratch = the buffer given to deme_radix_sort_pairs_device for n
+ * pairs, or NULL for deme_radix_sort_pairs_static.  Waits for `stream`, stores the sort's error word in *word (may
+ * be NULL) and returns DEME_OK when it is 0, DEME_ERR_TIMEOUT when a bounded look-back wait of the sort ran out (the
+ * output is then not in order; sorting again is safe, since every sort clears the word first).  No counterpart
+ * in the reference, whose CUB sort reports nothing on the device (src/algorithms/DEMCubWrappers.cu:43-59).
+ * Allocates nothing. */
+int32_t deme_radix_sort_status(const void* scratch, uint32_t n, void* stream, uint32_t* word);
 
 /* ---- Adjoint of the step (no reference counterpart) ----------------------------------------------------------
  * For scenes of single spheres (centred, isotropic inertia) with plane walls, the built-in Hertz-Mindlin model,
@@ -454,7 +475,10 @@ int32_t deme_set_material(deme_handle* h, uint32_t m, float E, float nu, float C
  * - The first call on each device (with that device current) looks up the scratch address; make it before any
  *   stream capture.  A first call on a capturing stream returns DEME_ERR_STATE.
  * - All calls on one device share the scratch: calls that overlap in time (other streams, other threads) race and
- *   corrupt each other's results.  Serialise them, e.g. one stream per device. */
+ *   corrupt each other's results.  Serialise them, e.g. one stream per device.
+ * - The sort's error word stays in the scratch until the next call: deme_radix_sort_status(NULL, n, stream, &w)
+ *   reports whether the last sort completed in order.
+ * - The scratch address is kept for the life of the process: calls after cudaDeviceReset are not supported. */
 int32_t deme_radix_sort_pairs_static(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                                      uint32_t* vals_out, uint32_t n, int32_t key_bits, void* stream);
 

@@ -527,11 +527,40 @@ class DEMSolver {
      * replaces the FlatScene a previous call returned. */
     const FlatScene& Flatten() {
         flat = std::make_unique<FlatScene>();
-        build_flat(*flat);
+        build_flat(*flat, batches);
         return *flat;
     }
     void Initialize() {
-        Flatten();
+        system_batches = batches;
+        create_handle();
+        // after the flattening, which may add the bounding-box object
+        n_clumps_init = n_clumps_system;
+        n_ext_init = ext.size();
+        n_templates_init = templates.size();
+        n_materials_init = materials.size();
+        n_presc_init = presc.size();
+    }
+
+    /* dT's cycle loop (src/DEM/dT.cpp:1527): steps while the accumulated time is below the duration */
+    void DoDynamics(double duration) {
+        const double hs = (double)flat->params.h;
+        int32_t n = 0;
+        for (double t = 0.0; t < duration; t += hs) n++;
+        if (n) check(deme_step(h, n));
+    }
+    void DoDynamicsThenSync(double duration) {
+        DoDynamics(duration);
+        check(deme_sync(h));
+    }
+    void DoStepDynamics() { check(deme_step(h, 1)); }
+
+  private:
+    // Flattens the system (the batches in it, in order) and creates the handle with everything Initialize sets.
+    void create_handle() {
+        flat = std::make_unique<FlatScene>();
+        build_flat(*flat, system_batches);
+        n_clumps_system = 0;
+        for (const auto& b : system_batches) n_clumps_system += b->nClumps;
         if (h) {
             deme_destroy(h);
             h = nullptr;
@@ -573,19 +602,8 @@ class DEMSolver {
             check(deme_set_force_model(h, force_model->m_force_model.c_str(), names.data(), (int32_t)names.size()));
         }
     }
-    /* dT's cycle loop (src/DEM/dT.cpp:1527): steps while the accumulated time is below the duration */
-    void DoDynamics(double duration) {
-        const double hs = (double)flat->params.h;
-        int32_t n = 0;
-        for (double t = 0.0; t < duration; t += hs) n++;
-        if (n) check(deme_step(h, n));
-    }
-    void DoDynamicsThenSync(double duration) {
-        DoDynamics(duration);
-        check(deme_sync(h));
-    }
-    void DoStepDynamics() { check(deme_step(h, 1)); }
 
+  public:
     // ---- output (WriteSphereFile / WriteClumpFile / WriteContactFile, src/DEM/API.h:319-324, 430-436) ----
     void SetOutputContent(unsigned content) { out_content = content; }
     void SetContactOutputContent(unsigned content) { cnt_out_content = content; }
@@ -654,29 +672,185 @@ class DEMSolver {
         return out;
     }
 
-    // ---- queries (GetOwner*, src/DEM/API.h:196-214) ----
+    // ---- owner state (GetOwner* / SetOwner*, src/DEM/API.h:194-214; dT::getOwnerPos and its siblings,
+    // src/DEM/dT.cpp:1705-1810).  Owner ids are the reference's: clumps of the first Initialize, then the external
+    // objects, then the clumps each UpdateClumps added, in order. ----
     float3 GetOwnerPosition(uint32_t owner) {
-        pull();
+        const One o = one(owner);
         const deme_sim_params& p = flat->params;
-        const uint64_t v = st_voxel[owner];
         const uint64_t mx = (1ull << p.nvXp2) - 1, my = (1ull << p.nvYp2) - 1;
-        const double X = (double)(v & mx) * p.voxel_size + (double)st_locX[owner] * p.l;
-        const double Y = (double)((v >> p.nvXp2) & my) * p.voxel_size + (double)st_locY[owner] * p.l;
-        const double Z = (double)(v >> (p.nvXp2 + p.nvYp2)) * p.voxel_size + (double)st_locZ[owner] * p.l;
+        const double X = (double)(o.voxel & mx) * p.voxel_size + (double)o.loc[0] * p.l;
+        const double Y = (double)((o.voxel >> p.nvXp2) & my) * p.voxel_size + (double)o.loc[1] * p.l;
+        const double Z = (double)(o.voxel >> (p.nvXp2 + p.nvYp2)) * p.voxel_size + (double)o.loc[2] * p.l;
         return float3{(float)(X + p.lbf[0]), (float)(Y + p.lbf[1]), (float)(Z + p.lbf[2])};
     }
     float3 GetOwnerVelocity(uint32_t owner) {
-        pull();
-        return float3{st_f[0][owner], st_f[1][owner], st_f[2][owner]};
+        const One o = one(owner);
+        return float3{o.f[0], o.f[1], o.f[2]};
     }
     float3 GetOwnerAngVel(uint32_t owner) {
-        pull();
-        return float3{st_f[3][owner], st_f[4][owner], st_f[5][owner]};
+        const One o = one(owner);
+        return float3{o.f[3], o.f[4], o.f[5]};
     }
     float4 GetOwnerOriQ(uint32_t owner) {
-        pull();
-        return float4{st_f[7][owner], st_f[8][owner], st_f[9][owner], st_f[6][owner]};
+        const One o = one(owner);
+        return float4{o.f[7], o.f[8], o.f[9], o.f[6]};
     }
+    /* Linear and angular acceleration from the contacts of the last step (gravity not included), as the
+     * reference's aX / alphaX hold them after its force collection. */
+    float3 GetOwnerAcc(uint32_t owner) {
+        const One o = one(owner);
+        return float3{o.f[10], o.f[11], o.f[12]};
+    }
+    float3 GetOwnerAngAcc(uint32_t owner) {
+        const One o = one(owner);
+        return float3{o.f[13], o.f[14], o.f[15]};
+    }
+    /* setOwnerPos: the position relative to the domain's lower corner, encoded on the voxel grid
+     * (hostPositionToVoxelID, src/DEM/HostSideHelpers.hpp:328-350). */
+    void SetOwnerPosition(uint32_t owner, float3 pos) {
+        const deme_sim_params& p = flat->params;
+        const double X = (double)(pos.x - p.lbf[0]), Y = (double)(pos.y - p.lbf[1]), Z = (double)(pos.z - p.lbf[2]);
+        uint64_t voxel = 0;
+        uint16_t loc[3];
+        encode_position(p, X, Y, Z, voxel, loc);
+        deme_state s{};
+        s.voxel = &voxel;
+        s.locX = &loc[0];
+        s.locY = &loc[1];
+        s.locZ = &loc[2];
+        check(deme_upload_state_range(h, handle_owner(owner), 1, &s));
+    }
+    void SetOwnerVelocity(uint32_t owner, float3 vel) {
+        deme_state s{};
+        s.vX = &vel.x;
+        s.vY = &vel.y;
+        s.vZ = &vel.z;
+        check(deme_upload_state_range(h, handle_owner(owner), 1, &s));
+    }
+    void SetOwnerAngVel(uint32_t owner, float3 angVel) {
+        deme_state s{};
+        s.omgX = &angVel.x;
+        s.omgY = &angVel.y;
+        s.omgZ = &angVel.z;
+        check(deme_upload_state_range(h, handle_owner(owner), 1, &s));
+    }
+    void SetOwnerOriQ(uint32_t owner, float4 oriQ) {
+        deme_state s{};
+        s.oriQw = &oriQ.w;
+        s.oriQx = &oriQ.x;
+        s.oriQy = &oriQ.y;
+        s.oriQz = &oriQ.z;
+        check(deme_upload_state_range(h, handle_owner(owner), 1, &s));
+    }
+
+    // ---- adding clumps to a running simulation (ClearCache / UpdateClumps, src/DEM/APIPublic.cpp:470-490,
+    // 792-843) ----
+    /* Forgets the cached clump batches, so that a following AddClumps + UpdateClumps adds only the new ones.  The
+     * clumps already in the simulation stay. */
+    void ClearCache() { batches.clear(); }
+    /* Adds every currently cached clump batch to the simulation: the clumps and spheres already there keep their
+     * state, contact history and ids (new spheres follow the old ones), the simulation time carries on, and the
+     * new clumps start from the state their batches give.  As in the reference, new clump templates, external
+     * objects, materials or family prescriptions since Initialize are refused; without a ClearCache the clumps
+     * cached before Initialize are added a second time. */
+    void UpdateClumps() {
+        if (!h) throw std::runtime_error("UpdateClumps: call it only after Initialize");
+        if (ext.size() != n_ext_init)
+            throw std::runtime_error("UpdateClumps cannot be used after loading new analytical objects");
+        if (templates.size() != n_templates_init)
+            throw std::runtime_error("UpdateClumps cannot be used after loading new clump templates");
+        if (materials.size() != n_materials_init || presc.size() != n_presc_init)
+            throw std::runtime_error("UpdateClumps should not be used if you introduce new material types or family "
+                                     "prescriptions");
+        // the run so far: owner state, contact list with its history, time
+        const uint32_t nO_old = flat->scene.n_owners;
+        const size_t nC_old = n_clumps_system;
+        OwnerState st = pull_owner_state();
+        std::vector<float> omg[3];
+        for (auto& v : omg) v.resize(nO_old);
+        {
+            deme_state s{};
+            s.omgX = omg[0].data();
+            s.omgY = omg[1].data();
+            s.omgZ = omg[2].data();
+            check(deme_download_state(h, &s));
+        }
+        uint32_t nc = 0;
+        check(deme_get_num_contacts(h, &nc));
+        const uint32_t cap = std::max<uint32_t>(nc, 1);
+        const int nw = (force_model && force_model->custom) ? (int)force_model->m_contact_wildcards.size()
+                                                             : flat->params.n_contact_wildcards;
+        std::vector<uint32_t> idA(cap), idB(cap), map(cap);
+        std::vector<uint8_t> type(cap);
+        std::vector<float> wc((size_t)std::max(nw, 1) * cap);
+        deme_contacts c{};
+        c.capacity = cap;
+        c.idA = idA.data();
+        c.idB = idB.data();
+        c.type = type.data();
+        c.mapping = map.data();
+        c.wildcards = nw ? wc.data() : nullptr;
+        check(deme_download_contacts(h, &c));
+        double t = 0.0;
+        float tf = 0.f;
+        int64_t steps = 0;
+        check(deme_get_time(h, &t, &steps));
+        check(deme_get_time_float(h, &tf));
+        // the system grows by the cached batches; flatten and create the new handle as Initialize does
+        for (const auto& b : batches) system_batches.push_back(b);
+        create_handle();
+        // carry the run over: old clumps keep their ids, the external objects move behind the new clumps
+        const size_t nC_new = n_clumps_system, nExt = ext.size();
+        FlatScene& f = *flat;
+        std::vector<uint64_t> voxel = f.voxel;
+        std::vector<uint16_t> lx = f.locX, ly = f.locY, lz = f.locZ;
+        std::vector<float> qw = f.oriQw, qx = f.oriQx, qy = f.oriQy, qz = f.oriQz, vx = f.vX, vy = f.vY, vz = f.vZ,
+                           wx = f.omgX, wy = f.omgY, wz = f.omgZ;
+        std::vector<uint8_t> fam = f.family;
+        auto carry = [&](size_t from, size_t to) {
+            voxel[to] = st.voxel[from];
+            lx[to] = st.locX[from];
+            ly[to] = st.locY[from];
+            lz[to] = st.locZ[from];
+            qw[to] = st.oriQw[from];
+            qx[to] = st.oriQx[from];
+            qy[to] = st.oriQy[from];
+            qz[to] = st.oriQz[from];
+            vx[to] = st.vX[from];
+            vy[to] = st.vY[from];
+            vz[to] = st.vZ[from];
+            wx[to] = omg[0][from];
+            wy[to] = omg[1][from];
+            wz[to] = omg[2][from];
+            fam[to] = st.family[from];
+        };
+        for (size_t o = 0; o < nC_old; o++) carry(o, o);
+        for (size_t e = 0; e < nExt; e++) carry(nC_old + e, nC_new + e);
+        deme_state s{};
+        s.voxel = voxel.data();
+        s.locX = lx.data();
+        s.locY = ly.data();
+        s.locZ = lz.data();
+        s.oriQw = qw.data();
+        s.oriQx = qx.data();
+        s.oriQy = qy.data();
+        s.oriQz = qz.data();
+        s.vX = vx.data();
+        s.vY = vy.data();
+        s.vZ = vz.data();
+        s.omgX = wx.data();
+        s.omgY = wy.data();
+        s.omgZ = wz.data();
+        s.family = fam.data();
+        check(deme_upload_state(h, &s));
+        // sphere ids of the old clumps are unchanged (new spheres follow them), as are analytical component ids,
+        // so the contact list and its history carry over as they are
+        c.n_contacts = nc;
+        if (nc) check(deme_upload_contacts(h, &c));
+        check(deme_set_time(h, t, tf, steps));
+    }
+
     uint32_t GetNumContacts() {
         uint32_t n = 0;
         check(deme_get_num_contacts(h, &n));
@@ -763,29 +937,76 @@ class DEMSolver {
         return rows;
     }
 
-    void pull() {
-        const uint32_t n = flat->scene.n_owners;
-        st_voxel.resize(n);
-        st_locX.resize(n);
-        st_locY.resize(n);
-        st_locZ.resize(n);
-        for (auto& v : st_f) v.resize(n);
+    // hostPositionToVoxelID (src/DEM/HostSideHelpers.hpp:328-350) for a position relative to the lower corner;
+    // positions outside the voxel world clamp to its faces instead of wrapping.
+    static void encode_position(const uint8_t nv[3], double voxel_size, double l, double X, double Y, double Z,
+                                uint64_t& voxel, uint16_t sub[3]) {
+        const double p[3] = {X, Y, Z};
+        uint64_t n[3];
+        for (int a = 0; a < 3; a++) {
+            double q = p[a] / voxel_size;
+            if (!(q > 0)) q = 0.0;
+            n[a] = (uint64_t)std::floor(q);
+            double u = (p[a] - (double)n[a] * voxel_size) / l;
+            if (!(u > 0)) u = 0.0;
+            u = std::min(u, 65535.0);
+            sub[a] = (uint16_t)std::floor(u);
+        }
+        voxel = n[0] + (n[1] << nv[0]) + (n[2] << (nv[0] + nv[1]));
+    }
+    static void encode_position(const deme_sim_params& p, double X, double Y, double Z, uint64_t& voxel,
+                                uint16_t sub[3]) {
+        const uint8_t nv[3] = {p.nvXp2, p.nvYp2, p.nvZp2};
+        encode_position(nv, p.voxel_size, p.l, X, Y, Z, voxel, sub);
+    }
+
+    // The handle's index of a reference owner id: the reference numbers the clumps of the first Initialize, then
+    // the external objects, then the clumps of each UpdateClumps; the handle keeps every clump before the
+    // external objects.
+    uint32_t handle_owner(uint32_t owner) const {
+        const size_t nExt = n_ext_init;
+        const uint32_t nO = flat ? flat->scene.n_owners : 0;
+        uint32_t o = owner;
+        if (owner >= n_clumps_init && owner < n_clumps_init + nExt)
+            o = (uint32_t)(n_clumps_system + (owner - n_clumps_init));
+        else if (owner >= n_clumps_init + nExt)
+            o = (uint32_t)(owner - nExt);
+        if (!h || o >= nO) throw std::runtime_error("owner id " + std::to_string(owner) + " out of range");
+        return o;
+    }
+
+    // One owner's state (a ranged download of one entry).
+    struct One {
+        uint64_t voxel = 0;
+        uint16_t loc[3] = {0, 0, 0};
+        float f[16] = {};  // v, omega, q (w, x, y, z), a, alpha
+    };
+    One one(uint32_t owner) {
+        One o;
         deme_state s{};
-        s.voxel = st_voxel.data();
-        s.locX = st_locX.data();
-        s.locY = st_locY.data();
-        s.locZ = st_locZ.data();
-        s.vX = st_f[0].data();
-        s.vY = st_f[1].data();
-        s.vZ = st_f[2].data();
-        s.omgX = st_f[3].data();
-        s.omgY = st_f[4].data();
-        s.omgZ = st_f[5].data();
-        s.oriQw = st_f[6].data();
-        s.oriQx = st_f[7].data();
-        s.oriQy = st_f[8].data();
-        s.oriQz = st_f[9].data();
-        check(deme_download_state(h, &s));
+        s.voxel = &o.voxel;
+        s.locX = &o.loc[0];
+        s.locY = &o.loc[1];
+        s.locZ = &o.loc[2];
+        float* f = o.f;
+        s.vX = f + 0;
+        s.vY = f + 1;
+        s.vZ = f + 2;
+        s.omgX = f + 3;
+        s.omgY = f + 4;
+        s.omgZ = f + 5;
+        s.oriQw = f + 6;
+        s.oriQx = f + 7;
+        s.oriQy = f + 8;
+        s.oriQz = f + 9;
+        s.aX = f + 10;
+        s.aY = f + 11;
+        s.aZ = f + 12;
+        s.alphaX = f + 13;
+        s.alphaY = f + 14;
+        s.alphaZ = f + 15;
+        check(deme_download_state_range(h, handle_owner(owner), 1, &s));
+        return o;
     }
 
     static double kernel_literal(double x) {  // std::fixed, 17 decimals, parsed back (APIPrivate.cpp:1358-1359)
@@ -842,7 +1063,7 @@ class DEMSolver {
         for (int i = 0; i < 3; i++) nv[rank[i]] = (uint8_t)bits[i];
     }
 
-    void build_flat(FlatScene& f) {
+    void build_flat(FlatScene& f, const std::vector<std::shared_ptr<DEMClumpBatch>>& batches) {
         if (!has_box) throw std::runtime_error("InstructBoxDomainDimension must be called before Initialize");
         uint8_t nv[3];
         double l = 0.0;
@@ -951,22 +1172,12 @@ class DEMSolver {
         if (f.anal_type.size() > 255) throw std::runtime_error("at most 255 analytical components");
         // ---- initial encoding of xyz - LBF (hostPositionToVoxelID, HostSideHelpers.hpp:328-350) ----
         for (size_t i = 0; i < nO; i++) {
-            const double p[3] = {(double)(pos[i].x - lbf.x), (double)(pos[i].y - lbf.y), (double)(pos[i].z - lbf.z)};
-            uint64_t n[3];
-            uint16_t s[3];
-            for (int a = 0; a < 3; a++) {
-                double q = p[a] / voxel_size;
-                if (!(q > 0)) q = 0.0;
-                n[a] = (uint64_t)std::floor(q);
-                double sub = (p[a] - (double)n[a] * voxel_size) / l;
-                if (!(sub > 0)) sub = 0.0;
-                sub = std::min(sub, 65535.0);
-                s[a] = (uint16_t)std::floor(sub);
-            }
-            f.voxel[i] = n[0] + (n[1] << nv[0]) + (n[2] << (nv[0] + nv[1]));
-            f.locX[i] = s[0];
-            f.locY[i] = s[1];
-            f.locZ[i] = s[2];
+            uint16_t sub[3];
+            encode_position(nv, voxel_size, l, (double)(pos[i].x - lbf.x), (double)(pos[i].y - lbf.y),
+                            (double)(pos[i].z - lbf.z), f.voxel[i], sub);
+            f.locX[i] = sub[0];
+            f.locY[i] = sub[1];
+            f.locZ[i] = sub[2];
         }
         // ---- materials ----
         auto prop = [](const DEMMaterial& m, const char* key) {
@@ -1122,9 +1333,10 @@ class DEMSolver {
     unsigned out_content = OUTPUT_CONTENT::QUAT | OUTPUT_CONTENT::ABSV;
     unsigned cnt_out_content = CNT_OUTPUT_CONTENT::FORCE | CNT_OUTPUT_CONTENT::POINT;
     std::set<unsigned> no_output;
-    std::vector<uint64_t> st_voxel;
-    std::vector<uint16_t> st_locX, st_locY, st_locZ;
-    std::vector<float> st_f[10];
+    // the system's clump batches (flattened into the handle, in order) and what UpdateClumps checks against
+    std::vector<std::shared_ptr<DEMClumpBatch>> system_batches;
+    size_t n_clumps_init = 0, n_clumps_system = 0, n_ext_init = 0, n_templates_init = 0, n_materials_init = 0,
+           n_presc_init = 0;
 };
 
 }  // namespace deme

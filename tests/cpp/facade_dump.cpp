@@ -1,7 +1,9 @@
 // Builds one scene through the C++ DEMSolver facade (include/deme_solver.hpp) from per-clump inputs written by
 // tests/test_cpp_facade.py, flattens it (no GPU needed) and writes every flat array for comparison with the Python
 // SceneBuilder.  With a step count it also initializes the solver on the GPU, steps, and writes the owner state.
-// Usage: facade_dump <inputs.bin> <out.bin> [steps]
+// With "ops" after the step count it then exercises the per-owner setters and getters (SetOwner* / GetOwnerAcc /
+// GetOwnerAngAcc) and UpdateClumps, writing what it set and what it read back.
+// Usage: facade_dump <inputs.bin> <out.bin> [steps [ops]]
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -36,7 +38,7 @@ static void put(std::ofstream& out, const char* name, const std::vector<T>& v) {
 }
 
 int main(int argc, char** argv) {
-    if (argc != 3 && argc != 4) return 2;
+    if (argc < 3 || argc > 5) return 2;
     std::ifstream in(argv[1], std::ios::binary);
     const auto types = read_vec<int32_t>(in);    // batch 1 template index per clump
     const auto xyz1 = read_vec<float>(in);       // batch 1 positions (3 per clump)
@@ -196,7 +198,7 @@ int main(int argc, char** argv) {
         const std::string c = cnt.str();
         put(out, "csv_contacts", c.data(), c.size());
     }
-    if (argc == 4) {
+    if (argc >= 4) {
         const int steps = std::atoi(argv[3]);
         s.Initialize();  // flattens again: use the new FlatScene from here on
         for (int i = 0; i < steps; i++) s.DoStepDynamics();
@@ -212,6 +214,60 @@ int main(int argc, char** argv) {
         put(out, "run_vel", vel);
         put(out, "run_ke", &ke, 1);
         put(out, "run_ncontacts", &nc, 1);
+        if (argc == 5 && std::string(argv[4]) == "ops") {
+            // accelerations of the last step, owner by owner
+            std::vector<float3> acc(nO), aacc(nO);
+            for (size_t o = 0; o < nO; o++) {
+                acc[o] = s.GetOwnerAcc((uint32_t)o);
+                aacc[o] = s.GetOwnerAngAcc((uint32_t)o);
+            }
+            put(out, "ops_acc", acc);
+            put(out, "ops_angacc", aacc);
+            // one setter per owner 0..3, read back, then one more step
+            const float3 p0{0.01f, -0.02f, 0.05f}, v1{0.3f, -0.1f, 0.2f}, w2{5.f, -3.f, 1.f};
+            const float4 q3{0.f, 0.6f, 0.f, 0.8f};  // (x, y, z, w)
+            s.SetOwnerPosition(0, p0);
+            s.SetOwnerVelocity(1, v1);
+            s.SetOwnerAngVel(2, w2);
+            s.SetOwnerOriQ(3, q3);
+            const float3 rb[3] = {s.GetOwnerPosition(0), s.GetOwnerVelocity(1), s.GetOwnerAngVel(2)};
+            const float4 rq = s.GetOwnerOriQ(3);
+            put(out, "ops_readback", rb, 3);
+            put(out, "ops_readback_q", &rq, 1);
+            s.DoStepDynamics();
+            for (size_t o = 0; o < nO; o++) {
+                pos[o] = s.GetOwnerPosition((uint32_t)o);
+                vel[o] = s.GetOwnerVelocity((uint32_t)o);
+            }
+            put(out, "ops_pos", pos);
+            put(out, "ops_vel", vel);
+            // UpdateClumps: forget the cached batches, add three spheres, carry the run over
+            const uint32_t nc_before = s.GetNumContacts();
+            const double t_before = s.GetSimTime();
+            s.ClearCache();
+            std::vector<float3> p3{float3{-0.05f, 0.05f, 0.15f}, float3{0.05f, 0.05f, 0.15f},
+                                   float3{0.f, -0.05f, 0.15f}};
+            auto b3 = s.AddClumps(T[0], p3);
+            b3->SetVel(std::vector<float3>(3, float3{0.f, 0.f, -0.5f}));
+            s.UpdateClumps();
+            const size_t nO2 = s.GetFlatScene().voxel.size();
+            std::vector<float3> upos(nO2), uvel(nO2);
+            for (size_t o = 0; o < nO2; o++) {
+                upos[o] = s.GetOwnerPosition((uint32_t)o);
+                uvel[o] = s.GetOwnerVelocity((uint32_t)o);
+            }
+            const uint32_t nc_after = s.GetNumContacts();
+            const double t_after = s.GetSimTime();
+            put(out, "upd_pos", upos);
+            put(out, "upd_vel", uvel);
+            const uint32_t ncs[2] = {nc_before, nc_after};
+            const double ts[2] = {t_before, t_after};
+            put(out, "upd_ncontacts", ncs, 2);
+            put(out, "upd_time", ts, 2);
+            for (int i = 0; i < 3; i++) s.DoStepDynamics();
+            for (size_t o = 0; o < nO2; o++) upos[o] = s.GetOwnerPosition((uint32_t)o);
+            put(out, "upd_pos_after", upos);
+        }
     }
     return 0;
 }

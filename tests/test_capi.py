@@ -36,7 +36,7 @@ def test_abi_version_and_status_strings():
     assert lib.deme_status_string(6) == b"DEME_ERR_TIMEOUT"
 
 
-def test_struct_sizes_match_header():
+def test_struct_sizes_match_header(tmp_path):
     # compile a tiny C program against the header and compare sizeof with the ctypes mirror
     src = r"""
     #include <stdio.h>
@@ -47,8 +47,7 @@ def test_struct_sizes_match_header():
         return 0;
     }
     """
-    tmp = os.path.join(ROOT, "_work", "sizes")
-    os.makedirs(os.path.dirname(tmp), exist_ok=True)
+    tmp = str(tmp_path / "sizes")
     with open(tmp + ".c", "w") as f:
         f.write(src)
     subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), tmp + ".c", "-o", tmp])

@@ -37,7 +37,8 @@ def scene_inputs(seed=5):
     return types, xyz1, q1, v1, w1, fam1, xyz2
 
 
-def python_scene(types, xyz1, q1, v1, w1, fam1, xyz2):
+def python_scene(types, xyz1, q1, v1, w1, fam1, xyz2, extra=None):
+    """The scene of tests/cpp/facade_dump.cpp; `extra` = (positions, velocity) of sphere clumps of a third batch."""
     s = SceneBuilder()
     s.InstructBoxDomainDimension(0.3, 0.3, 0.45)
     s.SetCoordSysOrigin("center")
@@ -56,6 +57,9 @@ def python_scene(types, xyz1, q1, v1, w1, fam1, xyz2):
     b1.SetFamilies(fam1)
     b2 = s.AddClumps(T[2], xyz2)
     b2.SetFamily(3)
+    if extra is not None:
+        b3 = s.AddClumps(T[0], np.asarray(extra[0], f32))
+        b3.SetVel(np.tile(np.asarray(extra[1], f32), (len(extra[0]), 1)))
     s.AddBCPlane((0, 0, -0.1), (0.1, 0, 1), m1)
     wall = s.AddExternalObject()
     wall.AddCylinder((0, 0, 0), (0, 0, 1), 0.12, m0)
@@ -198,3 +202,94 @@ def test_cpp_facade_steps_like_the_python_solver(tmp_path):
     assert int(np.frombuffer(cpp["run_ncontacts"], np.uint32)[0]) == g.num_contacts()
     ke = float(np.frombuffer(cpp["run_ke"], np.float64)[0])
     assert abs(ke - g.kinetic_energy()) <= 1e-5 * abs(g.kinetic_energy())
+
+
+@pytest.mark.gpu
+def test_cpp_facade_owner_setters_getters_and_update_clumps(tmp_path):
+    """SetOwnerPosition / SetOwnerVelocity / SetOwnerAngVel / SetOwnerOriQ, GetOwnerAcc / GetOwnerAngAcc and
+    UpdateClumps through the C++ facade (src/DEM/API.h:194-214, 392), against the Python Solver doing the same
+    through deme_upload_state / deme_download_state:
+    * the accelerations read owner by owner equal the whole-state download (float-sum-order bound);
+    * each setter reads back what was set (the position to within the sub-voxel step) and the next step moves the
+      owners as the Python run with the same state edits does;
+    * UpdateClumps keeps every owner's state, the contact count and the time, puts the external objects after the
+      old clumps in the reference's owner numbering and the new clumps after them, and the run continues as a fresh
+      handle with the carried-over state, contacts and time does."""
+    solver.load_product_library()
+    exe = build_exe(tmp_path)
+    inputs = scene_inputs()
+    inp = write_inputs(tmp_path, inputs)
+    subprocess.check_call([exe, str(inp), str(tmp_path / "out.bin"), "3", "ops"])
+    cpp = read_dump(tmp_path / "out.bin")
+    built = python_scene(*inputs)
+    lbf = np.asarray(built.params.lbf, np.float64)
+    nO = built.counts["o"]
+    g = solver.Solver(built)
+    g.step(3)
+    st = g.state()
+    # accelerations of the last step
+    acc = np.stack([st["aX"], st["aY"], st["aZ"]], 1).astype(np.float64)
+    aacc = np.stack([st["alphaX"], st["alphaY"], st["alphaZ"]], 1).astype(np.float64)
+    cacc = np.frombuffer(cpp["ops_acc"], f32).reshape(-1, 3).astype(np.float64)
+    caacc = np.frombuffer(cpp["ops_angacc"], f32).reshape(-1, 3).astype(np.float64)
+    assert cacc.shape == (nO, 3)
+    assert np.abs(cacc - acc).max() <= 1e-4 * max(np.abs(acc).max(), 1e-6)
+    assert np.abs(caacc - aacc).max() <= 1e-4 * max(np.abs(aacc).max(), 1e-6)
+    # setters read back
+    p0, v1, w2 = np.array([0.01, -0.02, 0.05], f32), np.array([0.3, -0.1, 0.2], f32), np.array([5, -3, 1], f32)
+    q3 = np.array([0.8, 0.0, 0.6, 0.0], f32)  # (w, x, y, z)
+    rb = np.frombuffer(cpp["ops_readback"], f32).reshape(3, 3)
+    rq = np.frombuffer(cpp["ops_readback_q"], f32)
+    assert np.abs(rb[0].astype(np.float64) - p0).max() <= 2 * built.params.l + 1e-7
+    np.testing.assert_array_equal(rb[1], v1)
+    np.testing.assert_array_equal(rb[2], w2)
+    np.testing.assert_array_equal(rq, [q3[1], q3[2], q3[3], q3[0]])  # float4 (x, y, z, w)
+    # the same edits through the whole-state upload, then one step
+    p = built.params
+    rel = (p0 - np.asarray(p.lbf, f32)).astype(np.float64)[None, :]
+    vox, sx, sy, sz = SceneBuilder.host_position_to_voxel(rel, (p.nvXp2, p.nvYp2, p.nvZp2), p.voxel_size, p.l)
+    st["voxel"][0], st["locX"][0], st["locY"][0], st["locZ"][0] = vox[0], sx[0], sy[0], sz[0]
+    st["vX"][1], st["vY"][1], st["vZ"][1] = v1
+    st["omgX"][2], st["omgY"][2], st["omgZ"][2] = w2
+    st["oriQw"][3], st["oriQx"][3], st["oriQy"][3], st["oriQz"][3] = q3
+    g.set_state(st)
+    g.step(1)
+    st = g.state()
+    pos = built.decode_positions(st, kernel_literals=False) + lbf
+    cpos = np.frombuffer(cpp["ops_pos"], f32).reshape(-1, 3).astype(np.float64)
+    assert np.abs(cpos - pos).max() <= 1e-7, np.abs(cpos - pos).max()
+    # UpdateClumps: nothing moves, the counts and the time carry over, owners are numbered as the reference does
+    nC = built.info["n_clumps"]
+    nExt = nO - nC
+    upos = np.frombuffer(cpp["upd_pos"], f32).reshape(-1, 3).astype(np.float64)
+    assert upos.shape == (nO + 3, 3)
+    np.testing.assert_array_equal(upos[:nO], cpos)
+    p3 = np.array([[-0.05, 0.05, 0.15], [0.05, 0.05, 0.15], [0.0, -0.05, 0.15]], f32)
+    assert np.abs(upos[nO:] - p3).max() <= 2 * built.params.l + 1e-7
+    uvel = np.frombuffer(cpp["upd_vel"], f32).reshape(-1, 3)
+    np.testing.assert_array_equal(uvel[nO:], np.tile(np.array([0, 0, -0.5], f32), (3, 1)))
+    ncs = np.frombuffer(cpp["upd_ncontacts"], np.uint32)
+    ts = np.frombuffer(cpp["upd_time"], np.float64)
+    assert ncs[0] == ncs[1] == g.num_contacts() and ts[0] == ts[1]
+    # the carried-over run: the same scene with the third batch, the old owners' state (external objects behind the
+    # new clumps in the handle), the old contacts and the time
+    built3 = python_scene(*inputs, extra=(p3, (0.0, 0.0, -0.5)))
+    assert built3.counts["o"] == nO + 3 and built3.info["n_clumps"] == nC + 3
+    g3 = solver.Solver(built3)
+    s3 = g3.state()
+    for k in s3:
+        if k.startswith("a"):
+            continue
+        s3[k][:nC] = st[k][:nC]
+        s3[k][nC + 3:] = st[k][nC:]
+    g3.set_state(s3)
+    c = g.contacts()
+    g3.set_contacts({k: c[k] for k in ("idA", "idB", "type", "wildcards")})
+    g3.set_time(*g.time())
+    g3.step(3)
+    pos3 = built3.decode_positions(g3.state(), kernel_literals=False) + lbf
+    ref_order = np.concatenate([pos3[:nC], pos3[nC + 3:], pos3[nC:nC + 3]])  # the reference's owner numbering
+    after = np.frombuffer(cpp["upd_pos_after"], f32).reshape(-1, 3).astype(np.float64)
+    assert np.abs(after - ref_order).max() <= 1e-7, np.abs(after - ref_order).max()
+    assert (after[nO:, 2] < upos[nO:, 2]).all()  # the new spheres fall
+    assert nExt > 0

@@ -34,7 +34,15 @@ def _lib():
                                                                      C.c_void_p]
     lib.deme_radix_sort_scratch_bytes.restype = C.c_size_t
     lib.deme_radix_sort_scratch_bytes.argtypes = [C.c_uint32]
+    lib.deme_radix_sort_status.restype = C.c_int32
+    lib.deme_radix_sort_status.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(C.c_uint32)]
     return lib
+
+
+def _status(lib, scratch, n, st):
+    word = C.c_uint32(0xDEADBEEF)
+    rc = lib.deme_radix_sort_status(scratch, n, st, C.byref(word))
+    return rc, word.value
 
 
 def _inputs(n, bits, seed):
@@ -53,6 +61,8 @@ def _sort_device(lib, kin, vin, n, bits, st):
     rc = lib.deme_radix_sort_pairs_device(kin.data_ptr(), vin.data_ptr(), kout.data_ptr(), vout.data_ptr(), n, bits,
                                           scratch.data_ptr(), nb, st)
     assert rc == 0
+    # the sort's error word, in the last bytes of the caller's scratch, reports a completed sort
+    assert _status(lib, scratch.data_ptr(), n, st) == (0, 0)
     return kout, vout
 
 
@@ -62,6 +72,7 @@ def _sort_static(lib, kin, vin, n, bits, st):
     rc = lib.deme_radix_sort_pairs_static(kin.data_ptr(), vin.data_ptr(), kout.data_ptr(), vout.data_ptr(), n, bits,
                                           st)
     assert rc == 0, rc
+    assert _status(lib, None, n, st) == (0, 0)
     return kout, vout
 
 
@@ -106,6 +117,8 @@ from deme_b200 import solver
 lib = solver.load_product_library()
 lib.deme_radix_sort_pairs_static.restype = C.c_int32
 lib.deme_radix_sort_pairs_static.argtypes = [C.c_void_p] * 4 + [C.c_uint32, C.c_int32, C.c_void_p]
+lib.deme_radix_sort_status.restype = C.c_int32
+lib.deme_radix_sort_status.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(C.c_uint32)]
 n = 50_000
 rng = np.random.default_rng(5)
 keys = rng.integers(0, 1 << 12, n, dtype=np.uint32)
@@ -113,12 +126,18 @@ vals = np.arange(n, dtype=np.uint32)
 kin = torch.from_numpy(keys.view(np.int32)).cuda(); vin = torch.from_numpy(vals.view(np.int32)).cuda()
 kout = torch.empty_like(kin); vout = torch.empty_like(vin)
 st = torch.cuda.current_stream().cuda_stream
-for _ in range(2):
+free = []
+for _ in range(4):
     rc = lib.deme_radix_sort_pairs_static(kin.data_ptr(), vin.data_ptr(), kout.data_ptr(), vout.data_ptr(), n, 12, st)
     assert rc == 0, rc
+    w = C.c_uint32(1)
+    assert lib.deme_radix_sort_status(None, n, st, C.byref(w)) == 0 and w.value == 0
     torch.cuda.synchronize()
     o = np.argsort(keys, kind="stable")
     assert (kout.cpu().numpy().view(np.uint32) == keys[o]).all() and (vout.cpu().numpy().view(np.uint32) == vals[o]).all()
+    free.append(torch.cuda.mem_get_info()[0])
+# after the first call (which loads the library's device code), further calls take no device memory
+assert len(set(free[1:])) == 1, free
 print("ok")
 """
 
