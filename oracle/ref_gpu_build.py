@@ -228,11 +228,14 @@ def bench_shell_drum(n_clumps: int = 1_000_000, spacing: float = 0.745):
 
 def prebuild(bench_clumps: int = 1_000_000, cpu_sample_clumps: int = 200_000) -> list:
     """For machines without the reference's sources: the driver, the parity scenes' cubins (FMA off), the benchmark
-    drum's cubins (NVRTC default), and the reference's CPU build for the benchmark's bounded CPU sample."""
+    drum's cubins (NVRTC default and FMA off), and the reference's CPU build for the benchmark's bounded CPU
+    sample."""
     out = [build_harness()]
     for name in PARITY_SCENES:
         out.append(build_cubins(parity_scene(name), fmad=False))
     out.append(build_cubins(bench_shell_drum(bench_clumps), fmad=True))
+    # the full-size parity test runs the benchmark drum against both builds
+    out.append(build_cubins(bench_shell_drum(bench_clumps), fmad=False))
     out.append(_ref_build().build(bench_shell_drum(cpu_sample_clumps)))
     return out
 
