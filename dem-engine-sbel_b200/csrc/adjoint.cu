@@ -353,6 +353,7 @@ int32_t restore_checkpoint(deme_handle* h, const Checkpoint& c) {
     cudaStream_t st = h->st_dt;
     ContactBuf& L = h->lists[h->cur];
     TRY(ensure_list(h, L, c.n));
+    h->analFresh = false;
     CUDA_TRY(h, cudaMemcpyAsync(h->voxel, c.voxel, h->nO * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
     CUDA_TRY(h, cudaMemcpyAsync(h->loc, c.loc, h->nO * sizeof(ushort4), cudaMemcpyDeviceToDevice, st));
     CUDA_TRY(h, cudaMemcpyAsync(h->quat, c.quat, h->nO * sizeof(float4), cudaMemcpyDeviceToDevice, st));

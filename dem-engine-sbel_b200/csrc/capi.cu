@@ -336,6 +336,7 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
     TRY(dalloc_n(h, &h->vel, nO));
     TRY(dalloc_n(h, &h->omg, nO));
     TRY(dalloc_n(h, &h->moi, nO));
+    TRY(dalloc_n(h, &h->invMoi, nO));
     TRY(dalloc_n(h, &h->acc, nO));
     TRY(dalloc_n(h, &h->alpha, nO));
     TRY(dalloc_n(h, &h->sph, nS));
@@ -349,13 +350,14 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
     TRY(dalloc_n(h, &h->presc, DEME_NUM_FAMILIES));
     {
         std::vector<ushort4> loc(nO);
-        std::vector<float4> quat(nO), vel(nO), omg(nO), moi(nO);
+        std::vector<float4> quat(nO), vel(nO), omg(nO), moi(nO), invMoi(nO);
         for (uint32_t o = 0; o < nO; o++) {
             loc[o] = make_ushort4(s->locX[o], s->locY[o], s->locZ[o], s->family[o]);
             quat[o] = make_float4(s->oriQw[o], s->oriQx[o], s->oriQy[o], s->oriQz[o]);
             vel[o] = make_float4(s->vX[o], s->vY[o], s->vZ[o], s->mass[o]);
             omg[o] = make_float4(s->omgX[o], s->omgY[o], s->omgZ[o], 0.f);
             moi[o] = make_float4(s->mmiXX[o], s->mmiYY[o], s->mmiZZ[o], 0.f);
+            invMoi[o] = make_float4(1.f / s->mmiXX[o], 1.f / s->mmiYY[o], 1.f / s->mmiZZ[o], 1.f / s->mass[o]);
         }
         CUDA_TRY(h, cudaMemcpy(h->voxel, s->voxel, nO * sizeof(uint64_t), cudaMemcpyHostToDevice));
         CUDA_TRY(h, cudaMemcpy(h->loc, loc.data(), nO * sizeof(ushort4), cudaMemcpyHostToDevice));
@@ -363,6 +365,7 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
         CUDA_TRY(h, cudaMemcpy(h->vel, vel.data(), nO * sizeof(float4), cudaMemcpyHostToDevice));
         CUDA_TRY(h, cudaMemcpy(h->omg, omg.data(), nO * sizeof(float4), cudaMemcpyHostToDevice));
         CUDA_TRY(h, cudaMemcpy(h->moi, moi.data(), nO * sizeof(float4), cudaMemcpyHostToDevice));
+        CUDA_TRY(h, cudaMemcpy(h->invMoi, invMoi.data(), nO * sizeof(float4), cudaMemcpyHostToDevice));
         CUDA_TRY(h, cudaMemset(h->acc, 0, nO * sizeof(float4)));
         CUDA_TRY(h, cudaMemset(h->alpha, 0, nO * sizeof(float4)));
         std::vector<float4> sph(nS);
@@ -446,10 +449,6 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
     }
     // ---- contact-detection work arrays ----
     CDView& cd = h->cd;
-    TRY(dalloc_n(h, &cd.pX, nS));
-    TRY(dalloc_n(h, &cd.pY, nS));
-    TRY(dalloc_n(h, &cd.pZ, nS));
-    TRY(dalloc_n(h, &cd.posF, nS));
     TRY(dalloc_n(h, &cd.posFSorted, nS));
     TRY(dalloc_n(h, &cd.recS, nS));
     TRY(dalloc_n(h, &cd.rngS, nS));
@@ -597,6 +596,8 @@ static int32_t cd_search(deme_handle* h, const StateView& s, AnalPlaced* anal, c
     const SimConsts& k = h->k;
     CDView& cd = h->cd;
     launch_place_anal(k, s, h->analRaw, anal, h->nA, st);
+    // the forces of this step, on the same poses, reuse the placement
+    if (anal == h->analPlaced) h->analFresh = true;
     CUDA_TRY(h, cudaMemsetAsync(cd.cellCount, 0, ((size_t)h->nCells + 1) * sizeof(uint32_t), st));
     launch_sphere_prep(k, s, cd, st);
     exclusive_scan_u32_onepass(cd.cellCount, h->nCells + 1, cd.cellStart, nullptr, h->scratch, h->dErr, st);
@@ -767,7 +768,8 @@ int32_t deme_compute_forces(deme_handle* h) {
     cudaStream_t st = h->st_dt;
     const SimConsts& k = h->k;
     StateView s = h->state_view();
-    launch_place_anal(k, s, h->analRaw, h->analPlaced, h->nA, st);
+    if (!h->analFresh) launch_place_anal(k, s, h->analRaw, h->analPlaced, h->nA, st);
+    h->analFresh = false;
     // prepareForceArrays (src/kernel/DEMPrepForceKernels.cu:23-31): accumulators start from zero every step
     CUDA_TRY(h, cudaMemsetAsync(h->acc, 0, h->nO * sizeof(float4), st));
     CUDA_TRY(h, cudaMemsetAsync(h->alpha, 0, h->nO * sizeof(float4), st));
@@ -821,6 +823,7 @@ static bool needs_device_time(const deme_handle* h) { return h->famRules.kern ||
 
 int32_t deme_integrate(deme_handle* h) {
     if (!h) return DEME_ERR_INVALID;
+    h->analFresh = false;  // the poses move
     cudaStream_t st = h->st_dt;
     if (h->motion.kern) {
         SimConsts k = h->k;
@@ -1242,7 +1245,10 @@ static int32_t transfer_state(deme_handle* h, uint32_t first, uint32_t count, de
                  ") beyond the " + std::to_string(h->nO) + " owners";
         return DEME_ERR_INVALID;
     }
-    if (in) TRY(cd_cancel(h));
+    if (in) {
+        TRY(cd_cancel(h));
+        h->analFresh = false;
+    }
     CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
     const uint32_t n = count;
     if (n == 0) return DEME_OK;

@@ -127,6 +127,49 @@ __device__ __forceinline__ void rot_f(float& X, float& Y, float& Z, float w, flo
     Z = (2.0f * (x * z - w * y)) * ox + (2.0f * (y * z + w * x)) * oy + (2.0f * (w * w + z * z) - 1.0f) * oz;
 }
 
+// The matrix of applyOriQToVector3<float, float> for one quaternion: its nine coefficients formed exactly as rot_f
+// forms them, so rot_apply equals rot_f bit for bit.  Rotating by the conjugate quaternion (the inverse rotation,
+// which the reference writes as applyOriQToVector3 with -x, -y, -z) gives the transposed coefficients exactly --
+// negating a component is exact, and a - (-b) rounds as a + b -- so rot_apply_t equals rot_f of the conjugate bit
+// for bit.  One matrix thus serves every rotation by a body's orientation in a kernel.
+struct RotF {
+    float m00, m01, m02, m10, m11, m12, m20, m21, m22;
+};
+__device__ __forceinline__ RotF rot_matrix(float w, float x, float y, float z) {
+    RotF r;
+    r.m00 = 2.0f * (w * w + x * x) - 1.0f;
+    r.m01 = 2.0f * (x * y - w * z);
+    r.m02 = 2.0f * (x * z + w * y);
+    r.m10 = 2.0f * (x * y + w * z);
+    r.m11 = 2.0f * (w * w + y * y) - 1.0f;
+    r.m12 = 2.0f * (y * z - w * x);
+    r.m20 = 2.0f * (x * z - w * y);
+    r.m21 = 2.0f * (y * z + w * x);
+    r.m22 = 2.0f * (w * w + z * z) - 1.0f;
+    return r;
+}
+__device__ __forceinline__ void rot_apply(const RotF& r, float& X, float& Y, float& Z) {
+    const float ox = X, oy = Y, oz = Z;
+    X = r.m00 * ox + r.m01 * oy + r.m02 * oz;
+    Y = r.m10 * ox + r.m11 * oy + r.m12 * oz;
+    Z = r.m20 * ox + r.m21 * oy + r.m22 * oz;
+}
+__device__ __forceinline__ void rot_apply_t(const RotF& r, float& X, float& Y, float& Z) {
+    const float ox = X, oy = Y, oz = Z;
+    X = r.m00 * ox + r.m10 * oy + r.m20 * oz;
+    Y = r.m01 * ox + r.m11 * oy + r.m21 * oz;
+    Z = r.m02 * ox + r.m12 * oy + r.m22 * oz;
+}
+
+// Rotational velocity of a body's contact point in the global frame, as the reference's force model forms it:
+// cross(omega, local contact point) in the body frame, then the body's orientation applied
+// (FullHertzianForceModel.cu), every operation rounded on its own.
+__device__ __forceinline__ float3 rot_cp_velocity(const RotF& r, float3 w, float3 cp) {
+    float x = w.y * cp.z - w.z * cp.y, y = w.z * cp.x - w.x * cp.z, z = w.x * cp.y - w.y * cp.x;
+    rot_apply(r, x, y, z);
+    return make_float3(x, y, z);
+}
+
 // locateMaskPair (DEMHelperKernels.cu:51-56)
 __device__ __forceinline__ uint32_t mask_index(uint32_t i, uint32_t j) {
     if (i > j) {

@@ -44,7 +44,6 @@ __global__ void __launch_bounds__(kForceThreads, DEME_FORCE_MIN_BLOCKS) k_force(
     float3 F = make_float3(0.f, 0.f, 0.f), T = make_float3(0.f, 0.f, 0.f);
     float3 cpA = make_float3(0.f, 0.f, 0.f), cpB = make_float3(0.f, 0.f, 0.f);
     float4 qA = make_float4(1.f, 0.f, 0.f, 0.f), qB = qA;
-    float mA = 1.f, mB = 1.f;
     bool active = false;
     bool ids_ok = valid;
     if (valid) {
@@ -72,15 +71,17 @@ __global__ void __launch_bounds__(kForceThreads, DEME_FORCE_MIN_BLOCKS) k_force(
         const float4 wA = s.omg[oA];
         double AOx, AOy, AOz;
         voxel_to_pos(k, s.voxel[oA], lA.x, lA.y, lA.z, AOx, AOy, AOz);
+        // one rotation matrix per body serves every rotation by its orientation here (rot_matrix)
+        const RotF RA = rot_matrix(qA.x, qA.y, qA.z, qA.w);
+        RotF RB;
         float rx = spA.x, ry = spA.y, rz = spA.z;
-        rot_f(rx, ry, rz, qA.x, qA.y, qA.z, qA.w);
+        rot_apply(RA, rx, ry, rz);
         const double Ax = AOx + (double)rx, Ay = AOy + (double)ry, Az = AOz + (double)rz;
         g.ARadius = spA.w;
         g.AOwnerMass = vA.w;
         g.matA = s.sMat[sA];
         g.ALinVel = make_float3(vA.x, vA.y, vA.z);
         g.ARotVel = make_float3(wA.x, wA.y, wA.z);
-        mA = vA.w;
         double BOx, BOy, BOz, CPx = 0, CPy = 0, CPz = 0, depth = 0;
         float nX = 0, nY = 0, nZ = 0;
         if (ct == DEME_SPHERE_SPHERE_CONTACT) {
@@ -92,15 +93,15 @@ __global__ void __launch_bounds__(kForceThreads, DEME_FORCE_MIN_BLOCKS) k_force(
             const float4 vB = s.vel[oB];
             const float4 wB = s.omg[oB];
             voxel_to_pos(k, s.voxel[oB], lB.x, lB.y, lB.z, BOx, BOy, BOz);
+            RB = rot_matrix(qB.x, qB.y, qB.z, qB.w);
             float bx = spB.x, by = spB.y, bz = spB.z;
-            rot_f(bx, by, bz, qB.x, qB.y, qB.z, qB.w);
+            rot_apply(RB, bx, by, bz);
             const double Bx = BOx + (double)bx, By = BOy + (double)by, Bz = BOz + (double)bz;
             g.BRadius = spB.w;
             g.BOwnerMass = vB.w;
             g.matB = s.sMat[bId];
             g.BLinVel = make_float3(vB.x, vB.y, vB.z);
             g.BRotVel = make_float3(wB.x, wB.y, wB.z);
-            mB = vB.w;
             // checkSpheresOverlap<double, float>, DEMHelperKernels.cu:233-264
             const double radA = (double)g.ARadius, radB = (double)g.BRadius;
             const double d2 = (Ax - Bx) * (Ax - Bx) + (Ay - By) * (Ay - By) + (Az - Bz) * (Az - Bz);
@@ -124,6 +125,7 @@ __global__ void __launch_bounds__(kForceThreads, DEME_FORCE_MIN_BLOCKS) k_force(
             const float4 vB = s.vel[oB];
             const float4 wB = s.omg[oB];
             voxel_to_pos(k, s.voxel[oB], lB.x, lB.y, lB.z, BOx, BOy, BOz);
+            RB = rot_matrix(qB.x, qB.y, qB.z, qB.w);
             g.BRadius = (float)kHugeFloat;
             g.BOwnerMass = a.mass;
             g.matB = a.material;
@@ -135,16 +137,16 @@ __global__ void __launch_bounds__(kForceThreads, DEME_FORCE_MIN_BLOCKS) k_force(
             active = true;
             float cax = (float)(CPx - AOx), cay = (float)(CPy - AOy), caz = (float)(CPz - AOz);
             float cbx = (float)(CPx - BOx), cby = (float)(CPy - BOy), cbz = (float)(CPz - BOz);
-            rot_f(cax, cay, caz, qA.x, -qA.y, -qA.z, -qA.w);
-            rot_f(cbx, cby, cbz, qB.x, -qB.y, -qB.z, -qB.w);
+            rot_apply_t(RA, cax, cay, caz);
+            rot_apply_t(RB, cbx, cby, cbz);
             cpA = make_float3(cax, cay, caz);
             cpB = make_float3(cbx, cby, cbz);
             g.B2A = make_float3(nX, nY, nZ);
             g.overlapDepth = depth;
             g.locCPA = cpA;
             g.locCPB = cpB;
-            g.AoriQ = qA;
-            g.BoriQ = qB;
+            g.ARotCP = rot_cp_velocity(RA, g.ARotVel, cpA);
+            g.BRotCP = rot_cp_velocity(RB, g.BRotVel, cpB);
 #ifdef DEME_USER_FORCE_MODEL
             {
                 // The names a DEM-Engine force-model string uses (calculateContactForces,
@@ -191,24 +193,26 @@ __global__ void __launch_bounds__(kForceThreads, DEME_FORCE_MIN_BLOCKS) k_force(
             out.CPB[i] = make_float4(cpB.x, cpB.y, cpB.z, 0.f);
         }
     }
-    // owner contributions (forceToAcc / forceToAngAcc, src/kernel/DEMCollectForceKernels.cu:68-120)
+    // owner contributions (forceToAcc / forceToAngAcc, src/kernel/DEMCollectForceKernels.cu:68-120): the
+    // reference divides by the mass and the principal moments; this multiplies by their reciprocals (within one
+    // rounding of the quotient), which saves a division sequence per component
     float4 aA = make_float4(0.f, 0.f, 0.f, 0.f), alA = aA, aB = aA, alB = aA;
     if (active) {
-        const float4 mi = s.moi[oA];
+        const float4 mi = __ldg(s.invMoi + oA);
         const bool bOwnerCounts = bSphere || aa.nAO;
-        aA = make_float4((F.x * 1.f) / mA, (F.y * 1.f) / mA, (F.z * 1.f) / mA, 0.f);
-        float gx = (F.x + T.x) * 1.f, gy = (F.y + T.y) * 1.f, gz = (F.z + T.z) * 1.f;
-        rot_f(gx, gy, gz, qA.x, -qA.y, -qA.z, -qA.w);
-        alA = make_float4((cpA.y * gz - cpA.z * gy) / mi.x, (cpA.z * gx - cpA.x * gz) / mi.y,
-                          (cpA.x * gy - cpA.y * gx) / mi.z, 0.f);
+        aA = make_float4(F.x * mi.w, F.y * mi.w, F.z * mi.w, 0.f);
+        float gx = F.x + T.x, gy = F.y + T.y, gz = F.z + T.z;
+        // the matrices again from the quaternions (cached loads), rather than held through the contact model
+        rot_apply_t(rot_matrix(qA.x, qA.y, qA.z, qA.w), gx, gy, gz);
+        alA = make_float4((cpA.y * gz - cpA.z * gy) * mi.x, (cpA.z * gx - cpA.x * gz) * mi.y,
+                          (cpA.x * gy - cpA.y * gx) * mi.z, 0.f);
         if (bOwnerCounts) {
-            const float4 mj = s.moi[oB];
-            if (!bSphere) mB = s.vel[oB].w;  // owner mass of the analytical object (massOwnerBody)
-            aB = make_float4((F.x * -1.f) / mB, (F.y * -1.f) / mB, (F.z * -1.f) / mB, 0.f);
-            float hx = (F.x + T.x) * -1.f, hy = (F.y + T.y) * -1.f, hz = (F.z + T.z) * -1.f;
-            rot_f(hx, hy, hz, qB.x, -qB.y, -qB.z, -qB.w);
-            alB = make_float4((cpB.y * hz - cpB.z * hy) / mj.x, (cpB.z * hx - cpB.x * hz) / mj.y,
-                              (cpB.x * hy - cpB.y * hx) / mj.z, 0.f);
+            const float4 mj = __ldg(s.invMoi + oB);  // for an analytical owner, its owner mass (massOwnerBody)
+            aB = make_float4(-F.x * mj.w, -F.y * mj.w, -F.z * mj.w, 0.f);
+            float hx = -(F.x + T.x), hy = -(F.y + T.y), hz = -(F.z + T.z);
+            rot_apply_t(rot_matrix(qB.x, qB.y, qB.z, qB.w), hx, hy, hz);
+            alB = make_float4((cpB.y * hz - cpB.z * hy) * mj.x, (cpB.z * hx - cpB.x * hz) * mj.y,
+                              (cpB.x * hy - cpB.y * hx) * mj.z, 0.f);
         }
     }
     // A side: contacts of one owner are adjacent (sorted by sphere id; a clump's spheres have consecutive ids).

@@ -15,7 +15,8 @@ struct ContactGeom {
     double overlapDepth;
     float3 locCPA, locCPB;
     float ARadius, BRadius, AOwnerMass, BOwnerMass;
-    float4 AoriQ, BoriQ;  // (w, x, y, z)
+    float3 ARotCP, BRotCP;  // rotational velocity of the contact point in the global frame: the owner's
+                            // orientation applied to cross(omega, local contact point) (rot_cp_velocity)
     float3 ALinVel, BLinVel, ARotVel, BRotVel;
     uint32_t matA, matB;
 };
@@ -78,15 +79,8 @@ __device__ __forceinline__ void hertz_mindlin(const ContactGeom& g, const Materi
     } else {
         contact_params(m, g.matA, g.matB, E_cnt, G_cnt, CoR_cnt, mu_cnt, Crr_cnt, beta);
     }
-    // rotational velocity of the contact point, mapped to the global frame
-    float rAx = g.ARotVel.y * g.locCPA.z - g.ARotVel.z * g.locCPA.y;
-    float rAy = g.ARotVel.z * g.locCPA.x - g.ARotVel.x * g.locCPA.z;
-    float rAz = g.ARotVel.x * g.locCPA.y - g.ARotVel.y * g.locCPA.x;
-    float rBx = g.BRotVel.y * g.locCPB.z - g.BRotVel.z * g.locCPB.y;
-    float rBy = g.BRotVel.z * g.locCPB.x - g.BRotVel.x * g.locCPB.z;
-    float rBz = g.BRotVel.x * g.locCPB.y - g.BRotVel.y * g.locCPB.x;
-    rot_f(rAx, rAy, rAz, g.AoriQ.x, g.AoriQ.y, g.AoriQ.z, g.AoriQ.w);
-    rot_f(rBx, rBy, rBz, g.BoriQ.x, g.BoriQ.y, g.BoriQ.z, g.BoriQ.w);
+    const float rAx = g.ARotCP.x, rAy = g.ARotCP.y, rAz = g.ARotCP.z;
+    const float rBx = g.BRotCP.x, rBy = g.BRotCP.y, rBz = g.BRotCP.z;
     const float nX = g.B2A.x, nY = g.B2A.y, nZ = g.B2A.z;
     // normal part and history update
     const float vx = (g.ALinVel.x + rAx) - (g.BLinVel.x + rBx);

@@ -59,6 +59,7 @@ struct deme_handle {
     float4* vel = nullptr;
     float4* omg = nullptr;
     float4* moi = nullptr;
+    float4* invMoi = nullptr;
     float4* acc = nullptr;
     float4* alpha = nullptr;
     float4* sph = nullptr;
@@ -69,6 +70,7 @@ struct deme_handle {
     float4* matPair = nullptr;  // contact-pair parameters, 2 x nM x nM (kMaxPairTableMaterials materials at most)
     AnalRaw* analRaw = nullptr;
     AnalPlaced* analPlaced = nullptr;
+    bool analFresh = false;  // analPlaced holds the placement for the current poses (a detection of this step made it)
     Prescription* presc = nullptr;
     uint2* ownerAnal = nullptr;  // packed scenes: per owner (first, count) of its analytical components
     // contact detection
@@ -157,6 +159,7 @@ struct deme_handle {
         s.vel = vel;
         s.omg = omg;
         s.moi = moi;
+        s.invMoi = invMoi;
         s.acc = acc;
         s.alpha = alpha;
         s.sph = sph;

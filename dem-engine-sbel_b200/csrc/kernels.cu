@@ -97,8 +97,9 @@ void launch_place_anal(const SimConsts& k, const StateView& s, const AnalRaw* ra
 }
 
 // ------------------------------------------------------------------------------------------------------------
-// Per sphere: exact position, CD radius, home cell, analytical-contact count
-// (getNumberOfBinsEachSphereTouches's analytical loop, DEMBinSphereKernels.cu:72-113).
+// Per sphere: home cell and analytical-contact count (getNumberOfBinsEachSphereTouches's analytical loop,
+// DEMBinSphereKernels.cu:72-113).  The exact position is not stored: the cell-order record writer forms it again
+// from the owner pose (the same arithmetic, so the same bits), which costs less than writing and re-reading it.
 __global__ void __launch_bounds__(256) k_sphere_prep(SimConsts k, StateView s, CDView cd) {
     const uint32_t sid = blockIdx.x * blockDim.x + threadIdx.x;
     if (sid >= k.n_spheres) return;
@@ -106,12 +107,6 @@ __global__ void __launch_bounds__(256) k_sphere_prep(SimConsts k, StateView s, C
     float4 sp;
     double X, Y, Z;
     sphere_center(k, s, sid, owner, sp, X, Y, Z);
-    cd.pX[sid] = X;
-    cd.pY[sid] = Y;
-    cd.pZ[sid] = Z;
-    float rf = sp.w;
-    rf += k.beta;
-    cd.posF[sid] = make_float4((float)X, (float)Y, (float)Z, rf);
     const uint32_t cx = cell_of(X, k.inv_cell, k.gx);
     const uint32_t cy = cell_of(Y, k.inv_cell, k.gy);
     const uint32_t cz = cell_of(Z, k.inv_cell, k.gz);
@@ -154,10 +149,12 @@ __device__ __forceinline__ bool in_range(uint32_t b, uint32_t packed) {
 // (ID order) into slot i.
 __device__ __forceinline__ void write_cell_records(const SimConsts& k, const StateView& s, const CDView& cd,
                                                    uint32_t i, uint32_t j) {
-    const float4 p = cd.posF[j];
-    const double X = cd.pX[j], Y = cd.pY[j], Z = cd.pZ[j];
-    const uint32_t o = s.sOwner[j];
-    const float r = s.sph[j].w;
+    uint32_t o;
+    float4 sp;
+    double X, Y, Z;
+    sphere_center(k, s, j, o, sp, X, Y, Z);
+    const float4 p = make_float4((float)X, (float)Y, (float)Z, 0.f);
+    const float r = sp.w;
     float rf = r;
     rf += k.beta;
     // CD radius bound: q units of q_scale, rounded up and one unit over, so q * q_scale >= rf despite float rounding
@@ -603,8 +600,10 @@ __global__ void __launch_bounds__(256) k_pair_assemble(SimConsts k, StateView s,
     const uint32_t anEnd = min(begin + nAn, end);
     uint32_t w = begin;
     if (nAn) {
-        const double X = cd.pX[A], Y = cd.pY[A], Z = cd.pZ[A];
-        const float4 sp = s.sph[A];
+        uint32_t owner;
+        float4 sp;
+        double X, Y, Z;
+        sphere_center(k, s, A, owner, sp, X, Y, Z);
         double rD = (double)sp.w;
         rD += (double)k.beta;
         const uint32_t fam = s.loc[s.sOwner[A]].w;

@@ -18,6 +18,7 @@ struct StateView {
     float4* vel;    // (vx, vy, vz, mass)
     float4* omg;    // (wx, wy, wz, 0)
     const float4* moi;
+    const float4* invMoi;  // (1 / Ixx, 1 / Iyy, 1 / Izz, 1 / mass), for the accelerations of the force kernel
     float4* acc;    // force accumulators (a)
     float4* alpha;  // torque accumulators (alpha)
     const float4* sph;  // (relX, relY, relZ, radius)
@@ -49,10 +50,6 @@ struct __align__(16) SphCD {
 
 // Contact-detection work arrays.
 struct CDView {
-    double* pX;
-    double* pY;
-    double* pZ;
-    float4* posF;        // ID order: (x, y, z, CD radius)
     float4* posFSorted;  // cell order: (x, y, z, sphere id bits)
     SphCD* recS;         // cell order: exact position, owner, expanded radius
     uint4* rngS;         // cell order: bin ranges of the expanded sphere, (lo | hi << 16) per axis; family in .w

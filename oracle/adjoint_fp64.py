@@ -230,9 +230,11 @@ def forces(sc: SphereScene, x, v, w, ss, sp, hss, hsp, keep=False):
     return F, T, out
 
 
-def rollout(sc: SphereScene, x0, v0, w0, n_steps: int, free=None):
+def rollout(sc: SphereScene, x0, v0, w0, n_steps: int, free=None, init=None):
     """Forward pass; returns the final (x, v, w) and the list of steps (state, contacts and histories at each
-    step start).  ``free`` masks the spheres that integrate (all by default)."""
+    step start).  ``free`` masks the spheres that integrate (all by default).  ``init`` = (ss, sp, hist_ss,
+    hist_sp) is the contact list of the step before the window with its updated histories, so that a window cut
+    from a longer run keeps the contact histories it starts with."""
     x, v, w = x0.astype(np.float64).copy(), v0.astype(np.float64).copy(), w0.astype(np.float64).copy()
     n = len(sc.r)
     free = np.ones(n, bool) if free is None else free
@@ -241,6 +243,9 @@ def rollout(sc: SphereScene, x0, v0, w0, n_steps: int, free=None):
     prev_sp = np.zeros((0, 2), np.int64)
     hout_ss = np.zeros((0, 4))
     hout_sp = np.zeros((0, 4))
+    if init is not None:
+        prev_ss, prev_sp = np.asarray(init[0], np.int64).reshape(-1, 2), np.asarray(init[1], np.int64).reshape(-1, 2)
+        hout_ss, hout_sp = np.asarray(init[2], np.float64).reshape(-1, 4), np.asarray(init[3], np.float64).reshape(-1, 4)
     for _ in range(n_steps):
         ss, sp = detect(sc, x)
         mss = _match(ss[:, 0] * (n + 1) + ss[:, 1], prev_ss[:, 0] * (n + 1) + prev_ss[:, 1])

@@ -130,32 +130,75 @@ def test_torch_autograd_function_gives_the_adjoint_gradients():
     assert np.all(err <= bar), (params.grad, gm)
 
 
-def test_column_collapse_with_default_floors_matches_host():
-    """A column of 300 spheres released over a floor for 2000 steps (contact onsets at near-zero rolling speed: the
-    exact derivative is unbounded there) with the default derivative floors on both sides: the CUDA and FP64 host
-    adjoints agree on the E, CoR and mu gradients within 5e-2 relative (the trajectories separate chaotically over
-    2000 steps) and on the Crr gradient in sign and within a factor 2: it comes from rolling contacts at near-zero
-    relative spin, where the CUDA forward (orientation integrated in the owner frame) and the FP64 model differ most,
-    and central differences of the FP64 forward themselves spread by 40 % over 0.3-3 % steps."""
+def _host_contacts(c):
+    """A GPU contact list with its updated histories, split as the host model keeps it (sphere pairs, sphere-plane
+    pairs, each with its history)."""
+    from deme_b200 import capi
+    ss = c["type"] == capi.SPHERE_SPHERE_CONTACT
+    pairs = np.stack([c["idA"], c["idB"]], 1).astype(np.int64)
+    h = c["wildcards"].T.astype(np.float64)
+    return pairs[ss], pairs[~ss], h[ss], h[~ss]
+
+
+def test_column_collapse_windows_match_host_adjoint_on_the_gpu_trajectory():
+    """A column of 300 spheres released over a floor, 2000 steps, default derivative floors on both sides.  Over so
+    many steps the FP32 CUDA trajectory and an FP64 rollout of the same start separate chaotically, and so do their
+    gradients (central differences of the FP64 forward themselves spread by 40 % over 0.3-3 % steps), so the run is
+    checked window by window on the CUDA trajectory itself: from the state and contact histories the CUDA run had
+    at the start of each 100-step window, the CUDA adjoint of the window (seeded with the gradient the later windows
+    returned) and the FP64 host adjoint of an FP64 rollout of that window agree on the E, CoR and mu gradients within
+    2 % of the window's largest material gradient and on the gradient with respect to the window's initial positions
+    within 2 % of its largest.  The Crr gradient comes from rolling contacts whose torque direction flips where the
+    relative rolling speed crosses zero, which the FP32 and FP64 rollouts reach at slightly different steps, so
+    single windows can disagree even in sign: summed over the windows, its differences stay within half of the
+    summed host gradients."""
     from deme_b200 import Solver, adjoint
     built = workloads.column_collapse(n=300)
     g = Solver(built)
     n = built.counts["s"]
-    T = 2000
+    T, W = 2000, 100
     init = built.decode_positions(built.initial_state(), kernel_literals=False)[:n]
-    adjoint.record(g, T, 100)
+    starts = []
+    for w in range(T // W):
+        starts.append((g.state(), g.contacts() if w else None))
+        g.step(W)
     pos, _, _ = adjoint.final_state(g)
     axis, z0 = init[:, :2].mean(0), float(init[:, 2].min())
     _, gpos = workloads.collapse_loss(pos[:n], axis, z0)
-    seed = np.zeros((built.counts["o"], 3))
-    seed[:n] = gpos
-    out = adjoint.backward(g, d_pos=seed)
-    sc, x0, v0, w0 = A.from_built(built)
-    (xf, _, _), rec = A.rollout(sc, x0, v0, w0, T)
-    _, gh = workloads.collapse_loss(xf, axis, z0)
-    gm = A.adjoint(sc, rec, gh, np.zeros((n, 3)), np.zeros((n, 3)))[3][0]
-    gg = out["d_material"][0]
-    for j, name in enumerate(("E", "CoR", "mu")):
-        assert abs(gg[j] - gm[j]) <= 5e-2 * abs(gm[j]), (name, gg[j], gm[j])
-    assert gg[3] * gm[3] > 0 and 0.5 <= gg[3] / gm[3] <= 2.0, (gg[3], gm[3])
-    assert np.all(np.isfinite(gg)) and abs(gg[1]) < 1.0 and abs(gg[3]) < 1.0
+    nO = built.counts["o"]
+    seed = [np.zeros((nO, 3)) for _ in range(3)]
+    seed[0][:n] = gpos
+    worst = np.zeros(4)
+    worst_x = 0.0
+    ratio_crr = []
+    crr_diff = crr_host = 0.0
+    for w in range(T // W - 1, -1, -1):
+        st, c = starts[w]
+        g.set_state({k: v for k, v in st.items() if not k.startswith("a")})
+        if c is not None:
+            g.set_contacts({k: c[k] for k in ("idA", "idB", "type", "wildcards")})
+        adjoint.record(g, W, W)
+        out = adjoint.backward(g, d_pos=seed[0], d_vel=seed[1], d_angvel=seed[2])
+        sc, x0, v0, _ = A.from_built(built, state=st)
+        w0 = adjoint.world_angular_velocity(st)[:n]
+        hc = _host_contacts(c) if c is not None else None
+        _, rec = A.rollout(sc, x0, v0, w0, W, init=hc)
+        hx, hv, hw, hm = A.adjoint(sc, rec, seed[0][:n], seed[1][:n], seed[2][:n])
+        gm = out["d_material"][0]
+        scale = np.abs(hm[0]).max()
+        err = np.abs(gm - hm[0]) / max(scale, 1e-300)
+        worst = np.maximum(worst, err)
+        assert np.all(err[:3] <= 2e-2), (w, gm, hm[0])
+        crr_diff += abs(gm[3] - hm[0][3])
+        crr_host += abs(hm[0][3])
+        if abs(hm[0][3]) > 1e-3 * scale:
+            ratio_crr.append(gm[3] / hm[0][3])
+        ex = np.abs(out["d_pos0"][:n] - hx).max() / max(np.abs(hx).max(), 1e-300)
+        worst_x = max(worst_x, ex)
+        assert ex <= 2e-2, (w, ex)
+        seed = [out["d_pos0"], out["d_vel0"], out["d_angvel0"]]
+    r = np.array(ratio_crr)
+    assert crr_diff <= 0.5 * crr_host, (crr_diff, crr_host, r)
+    print(f"column collapse, 20 windows of 100 steps: largest material-gradient difference (E, CoR, mu, Crr) "
+          f"{worst.round(5)} of the window's largest, position gradient {worst_x:.2e}; Crr summed difference "
+          f"{crr_diff / max(crr_host, 1e-300):.3f} of the summed host gradients, ratios {r.round(3)}")
