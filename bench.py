@@ -155,6 +155,8 @@ def shell_drum(n_clumps: int):
 
 SHELL_WARMUP = 3
 SHELL_STEPS = 40
+WEDGE_WARMUP = 5
+WEDGE_STEPS = 50
 
 
 def reference_kernels_gpu(args):
@@ -197,6 +199,63 @@ def reference_kernels_gpu(args):
                        "sorts/scans/reduce-by-key; value = the faster of its two contact-kernel variants"}
 
 
+def reference_kernels_quick(args, which: str):
+    """The reference's kernels (thread per bin) on the shell drum or the wedge hopper, for the main line's ratio."""
+    try:
+        from oracle import ref_gpu
+        from deme_b200 import workloads
+        built = shell_drum(args.clumps) if which == "shell" else workloads.hopper_wedge(n=args.hopper_spheres)
+        if not ref_gpu.prebuilt(built) and not ref_gpu.ref_gpu_build.available():
+            return {"unavailable": "reference kernels for this scene were not prebuilt"}
+        ref = ref_gpu.RefGPU(built, fmad=True)
+    except Exception as e:
+        return {"unavailable": f"{type(e).__name__}: {e}"}
+    try:
+        warm, steps = (SHELL_WARMUP, SHELL_STEPS // 4) if which == "shell" else (WEDGE_WARMUP, WEDGE_STEPS)
+        ref.set_one_bin_per_thread(True)
+        ref.step(warm)
+        ms = ref.time_steps(steps)
+        nC = ref.num_contacts()
+    except Exception as e:
+        ref.close()
+        return {"unavailable": f"{type(e).__name__}: {e}"}
+    ref.close()
+    return {"value": built.n_spheres * steps / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": ms / steps,
+            "n_spheres": built.n_spheres, "n_contacts": nC, "steps": steps, "warmup": warm,
+            "kernels": "reference src/kernel/*.cu substituted per scene, NVRTC sm_100a (FMA default), CUB; thread "
+                       "per bin"}
+
+
+def reference_kernels_wedge(args):
+    """The reference's own kernels on the GPU on the plane-only wedge hopper (4M log-normal spheres, CD every 5
+    steps), its thread-per-bin contact kernels (the faster variant on the drum), from the lattice start."""
+    try:
+        from oracle import ref_gpu
+        from deme_b200 import workloads
+        built = workloads.hopper_wedge(n=args.hopper_spheres)
+        if not ref_gpu.prebuilt(built) and not ref_gpu.ref_gpu_build.available():
+            return {"unavailable": "reference kernels for the wedge hopper were not prebuilt (needs the reference's "
+                                   "sources at build time)"}
+        ref = ref_gpu.RefGPU(built, fmad=True)
+    except Exception as e:
+        return {"unavailable": f"{type(e).__name__}: {e}"}
+    try:
+        ref.set_one_bin_per_thread(True)
+        ref.step(WEDGE_WARMUP)
+        ms = ref.time_steps(WEDGE_STEPS)
+        nC = ref.num_contacts()
+        phases = ref.profile_steps(10)
+    except Exception as e:
+        ref.close()
+        return {"unavailable": f"{type(e).__name__}: {e}"}
+    ref.close()
+    return {"value": built.n_spheres * WEDGE_STEPS / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": ms / WEDGE_STEPS,
+            "workload": wedge_workload(built), "n_spheres": built.n_spheres, "n_contacts": nC, "steps": WEDGE_STEPS,
+            "warmup": WEDGE_WARMUP, "phase_ms_per_step": phases,
+            "kernels": "reference src/kernel/*.cu substituted per scene, NVRTC sm_100a (FMA default), CUB; thread "
+                       "per bin"}
+
+
 def run_reference(args):
     """The reference's CPU path on a bounded sample: its own kernel code compiled for the CPU (oracle/_ref, OpenMP
     over the emulated blocks) on the shell variant of the drum, or, where that build is absent, the C oracle on the
@@ -233,21 +292,26 @@ def run_reference(args):
               f"{who}, OpenMP {cores} threads")
     cpu.close()
     gpu = reference_kernels_gpu(args) if not args.no_reference_gpu else None
+    wedge = reference_kernels_wedge(args) if not args.no_reference_gpu and not args.no_hopper else None
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": k,
             "warmup": w, "ms_per_step": dt / k * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 forces, f64 positions, integer voxels", "data": "synthetic (seeded)",
             "config": {"workload": wl + " (CPU sample)", "n_clumps": n_clumps, "n_spheres": built.n_spheres},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "reference_kernels_gpu": gpu}
+            "reference_kernels_gpu": gpu, "reference_kernels_gpu_hopper_wedge": wedge}
     print(json.dumps(line), flush=True)
 
 
 def hopper_measure(args, stream):
-    """Hopper, 4M log-normal spheres in an analytical cone, contact detection every 5 steps with a margin of 0.1
-    median radius.  The seeded packing settles first (untimed, --hopper-settle steps at dt 6e-6, gate closed), then
-    the same bed runs twice at dt 2e-6: with synchronous detection, and with kT and dT on two streams (a detection
-    adopted 5 steps after the poses it was made from).  Device time with CUDA events."""
+    """Hopper discharge: 4M log-normal spheres in an analytical cone, contact detection every 5 steps with a margin
+    of 0.1 median radius.  The seeded packing settles first with the outlet gate closed (untimed, --hopper-settle
+    steps at dt 6e-6); then the gate opens (its family changes to one that has no contact with the spheres, as the
+    reference's ChangeFamily + DisableContactBetweenFamilies do) and the discharge runs --hopper-steps steps at
+    dt 2e-6 twice from the same opened bed: with synchronous detection, and with kT and dT on two streams (a
+    detection adopted 5 steps after the poses it was made from).  Device time with CUDA events; the per-kernel
+    shares of the synchronous run come from deme_kernel_timing over two detection periods."""
+    import numpy as np
     import torch
     from deme_b200 import Solver, workloads
     built = workloads.hopper(n=args.hopper_spheres)
@@ -263,11 +327,15 @@ def hopper_measure(args, stream):
         s.set_time_step(dt_run)
     s.sync()
     prep_s = time.perf_counter() - t0
+    s.change_family(2, workloads.GATE_OPEN_FAMILY)  # the gate opens
     bed_state, bed_contacts = s.state(), s.contacts()
-    out = {"workload": f"hopper: {built.n_spheres} spheres, log-normal radii (median 1.5 mm, sigma 0.25), 30 deg cone, "
-                       f"40 mm outlet (gate closed), dt {dt_run:g}, CD every {f} steps, margin 0.1 median radius",
-           "initial_state": f"seeded lattice packing settled {args.hopper_settle} steps at dt 6e-6 (untimed, "
-                            f"{prep_s:.1f} s)",
+    apex = float(built.info["apex_z"])
+    u_out = float(built.info["u_out"])
+    out = {"workload": f"hopper discharge: {built.n_spheres} spheres, log-normal radii (median 1.5 mm, sigma 0.25), "
+                       f"30 deg cone, 40 mm outlet opened after settling, dt {dt_run:g}, CD every {f} steps, margin "
+                       f"0.1 median radius",
+           "initial_state": f"seeded lattice packing settled {args.hopper_settle} steps at dt 6e-6 with the gate "
+                            f"closed (untimed, {prep_s:.1f} s), then the gate opened",
            "n_spheres": built.n_spheres, "steps": args.hopper_steps, "warmup": 2 * f}
     for lag in (0, f):
         s.set_state({k: v for k, v in bed_state.items() if not k.startswith("a")})
@@ -284,12 +352,66 @@ def hopper_measure(args, stream):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         key = "sync" if lag == 0 else "two_streams"
+        z = built.decode_positions(s.state(), kernel_literals=False)[:built.n_spheres, 2]
+        lbf_z = float(built.params.lbf[2])
         out[key] = {"lag": lag, "ms_per_step": ms / args.hopper_steps,
                     "value": built.n_spheres * args.hopper_steps / (ms / 1e3) / 1e6, "unit": UNIT,
-                    "n_contacts": s.num_contacts()}
+                    "n_contacts": s.num_contacts(),
+                    "spheres_below_outlet": int(np.sum(z + lbf_z < apex + u_out))}
+        if lag == 0:
+            ks = kernel_breakdown(s, 2 * f)
+            tot = sum(ks.values())
+            out["kernel_ms_per_step"] = ks
+            out["history_share"] = ks.get("history", 0.0) / tot if tot > 0 else None
         s.set_async_cd(0)
     s.close()
     return out
+
+
+def kernel_breakdown(s, steps: int) -> dict:
+    """Per-kernel device milliseconds per step over `steps` steps (deme_kernel_timing brackets every launch)."""
+    lib = s.lib
+    lib.deme_kernel_timing(1)
+    s.step(steps)
+    s.sync()
+    names = (C.c_char_p * 32)()
+    tot = (C.c_double * 32)()
+    cnt = (C.c_int64 * 32)()
+    nk = C.c_int32(0)
+    lib.deme_kernel_times(32, names, tot, cnt, C.byref(nk))
+    lib.deme_kernel_timing(0)
+    return {names[i].decode(): tot[i] / steps for i in range(nk.value) if cnt[i] > 0}
+
+
+def hopper_wedge_measure(args, stream):
+    """This build on the plane-only wedge hopper (the same 4M log-normal spheres, volume equal to the cone's) from its
+    lattice start with the gate closed, CD every 5 steps: the scene the reference's kernels are timed on for the
+    polydisperse hopper workload."""
+    import torch
+    from deme_b200 import Solver, workloads
+    built = workloads.hopper_wedge(n=args.hopper_spheres)
+    s = Solver(built)
+    s.lib.deme_set_streams(s.h, C.c_void_p(stream.cuda_stream), C.c_void_p(stream.cuda_stream))
+    s.step(WEDGE_WARMUP)
+    s.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    s.step(WEDGE_STEPS)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    nC = s.num_contacts()
+    s.close()
+    return {"value": built.n_spheres * WEDGE_STEPS / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": ms / WEDGE_STEPS,
+            "workload": wedge_workload(built), "n_spheres": built.n_spheres, "n_contacts": nC, "steps": WEDGE_STEPS,
+            "warmup": WEDGE_WARMUP}
+
+
+def wedge_workload(built) -> str:
+    return (f"wedge hopper (planes only): {built.n_spheres} log-normal spheres, 30 deg walls, 40 mm outlet slot "
+            f"(gate closed), length {built.info['L']:.3f} m for the cone's volume {built.info['cone_volume']:.4f} "
+            f"m^3, lattice start, dt 2e-6, CD every 5 steps, margin 0.1 median radius")
 
 
 def small_scene_measure(args, stream):
@@ -385,7 +507,7 @@ def main():
     ap.add_argument("--graph", type=int, default=1, help="1: replay whole steps from CUDA graphs (deme_set_graph)")
     ap.add_argument("--small-steps", type=int, default=5000)
     ap.add_argument("--hopper-spheres", type=int, default=4_000_000)
-    ap.add_argument("--hopper-steps", type=int, default=500)
+    ap.add_argument("--hopper-steps", type=int, default=5000)
     ap.add_argument("--hopper-settle", type=int, default=40000, help="untimed settling steps of the hopper bed")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="reference arm: skip timing the reference's kernels on the GPU")
@@ -569,7 +691,11 @@ def main():
     adj = None if args.no_adjoint else clocked(lambda: adjoint_measure(args, stream))
     batched = None if args.no_batched else clocked(lambda: batched_measure(args, stream, rank, world, dist))
     shell = clocked(lambda: shell_drum_measure(args, stream)) if (rank == 0 and not args.no_shell) else None
+    # the reference's kernels on the same shell drum (thread per bin, its faster variant), for the ratio
+    ref_shell = reference_kernels_quick(args, "shell") if (rank == 0 and not args.no_shell) else None
     hopper = clocked(lambda: hopper_measure(args, stream)) if (rank == 0 and not args.no_hopper) else None
+    wedge = clocked(lambda: hopper_wedge_measure(args, stream)) if (rank == 0 and not args.no_hopper) else None
+    ref_wedge = reference_kernels_quick(args, "wedge") if (rank == 0 and not args.no_hopper) else None
     small = clocked(lambda: small_scene_measure(args, stream)) if (rank == 0 and not args.no_small) else None
     # the CPU sample last: its OpenMP threads would otherwise share the host with the GPU sections' host code
     cpu = None
@@ -577,8 +703,17 @@ def main():
         cpu = cpu_baseline_sample(args)
 
     if rank == 0:
+        def versus(ours, ref):
+            if not ours or not ref or "value" not in ours or "value" not in ref:
+                return {"unavailable": (ref or {}).get("unavailable", "not measured")}
+            return {"this_build": ours["value"], "reference_kernels": ref["value"], "ratio": ours["value"] / ref["value"],
+                    "unit": UNIT, "workload": ours["workload"]}
+
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "metric": METRIC, "value": value, "unit": UNIT,
+            # the same scene run by the reference's own kernels on this GPU (printed early, ahead of the details)
+            "vs_reference_kernels": {"shell_drum": versus(shell, ref_shell), "hopper_wedge": versus(wedge, ref_wedge)},
+            "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 forces/velocities, f64 positions on integer voxels",
             "data": "synthetic (seeded drum generator)",
@@ -595,7 +730,9 @@ def main():
             "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": C.sizeof(capi.FamilyPrescription),
                     "d2h_bytes_per_step": 8},
-            "gpu_launches": int(launches), "clocks": clocks, "shell_drum": shell, "hopper": hopper, "small_scene": small, "adjoint": adj, "batched": batched,
+            "gpu_launches": int(launches), "clocks": clocks, "shell_drum": shell, "reference_kernels_shell_drum": ref_shell,
+            "hopper": hopper, "hopper_wedge": wedge, "reference_kernels_hopper_wedge": ref_wedge, "small_scene": small,
+            "adjoint": adj, "batched": batched,
         }
         print(json.dumps(line), flush=True)
     s.close()

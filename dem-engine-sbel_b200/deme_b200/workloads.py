@@ -294,31 +294,21 @@ def packed_clumps(n_clumps: int = 600, r: float = 4e-3, spacing: float = 1.55, s
     return built
 
 
-def hopper(n: int = 4_000_000, r_median: float = 1.5e-3, sigma: float = 0.25, r_clip=(0.75e-3, 3e-3),
-           rho: float = 2500.0, half_angle_deg: float = 30.0, outlet: float = 0.04, n_classes: int = 64,
-           seed: int = 4, dt: float = 2e-6, cd_freq: int = 5, margin: float | None = None, closed: bool = True,
-           wall_clearance: float = 1.02, packing_seed_jitter: float = 0.9):
-    """Conical hopper of log-normal polydisperse spheres (analytical cone + outlet gate + catch floor).
+# Family the hopper's outlet gate (family 2) moves to when it opens: fixed, and with no contact with the spheres
+# (family 0), as the reference's scripts open a gate with ChangeFamily + DisableContactBetweenFamilies.
+GATE_OPEN_FAMILY = 3
 
-    Radii are log-normal (median ``r_median``, ``sigma``) clipped to ``r_clip`` and grouped into ``n_classes``
-    sphere types (one template per class, as a reference scene would load them).  Spheres start on a
-    hexagonal lattice of pitch 2 r_max filling the cone from the outlet up, each displaced randomly inside its own
-    lattice cell (no overlaps): a seeded random packing that needs no insertion loop.  The hopper height follows
-    from n.  The gate (family 2) closes the outlet while ``closed``; the floor 0.1 m below catches discharge.
-    Contact detection runs every ``cd_freq`` steps with the contact margin ``margin`` (default 0.1 r_median).
-    ``wall_clearance`` below 1 starts the outer spheres pressed into the walls (used by parity tests).
-    """
-    rng = np.random.default_rng(seed)
-    th = math.radians(half_angle_deg)
-    tan_t, cos_t = math.tan(th), math.cos(th)
+
+def _hopper_radii(n, r_median, sigma, r_clip, n_classes, rng):
     r = np.clip(rng.lognormal(math.log(r_median), sigma, n), r_clip[0], r_clip[1])
     edges = np.quantile(r, np.linspace(0, 1, n_classes + 1))
     cls = np.clip(np.searchsorted(edges, r, side="right") - 1, 0, n_classes - 1)
     r_cls = np.array([r[cls == c].mean() if np.any(cls == c) else edges[c] for c in range(n_classes)])
-    r = r_cls[cls]
-    r_max = float(r.max())
-    a = 2.0 * r_max * 1.01
-    u_out = (outlet / 2) / tan_t  # axial distance from the apex to the outlet
+    return r_cls[cls], r_cls, cls
+
+
+def _hopper_top(n, a, r_max, tan_t, cos_t, u_out, wall_clearance):
+    """Height of the cone that holds n lattice sites of pitch a above the outlet, and the sites."""
     dy, dz = a * math.sqrt(3.0) / 2.0, a * math.sqrt(2.0 / 3.0)
     u_top = u_out + 10 * a
     while True:
@@ -333,9 +323,33 @@ def hopper(n: int = 4_000_000, r_median: float = 1.5e-3, sigma: float = 0.25, r_
         clear = wall_clearance * r_max / cos_t
         ok = (rho_ <= P[:, 2] * tan_t - clear) & (P[:, 2] <= u_top - r_max)
         if ok.sum() >= n:
-            break
+            return u_top, P[ok]
         u_top *= 1.15
-    P = P[ok]
+
+
+def hopper(n: int = 4_000_000, r_median: float = 1.5e-3, sigma: float = 0.25, r_clip=(0.75e-3, 3e-3),
+           rho: float = 2500.0, half_angle_deg: float = 30.0, outlet: float = 0.04, n_classes: int = 64,
+           seed: int = 4, dt: float = 2e-6, cd_freq: int = 5, margin: float | None = None, closed: bool = True,
+           wall_clearance: float = 1.02, packing_seed_jitter: float = 0.9):
+    """Conical hopper of log-normal polydisperse spheres (analytical cone + outlet gate + catch floor).
+
+    Radii are log-normal (median ``r_median``, ``sigma``) clipped to ``r_clip`` and grouped into ``n_classes``
+    sphere types (one template per class, as a reference scene would load them).  Spheres start on a
+    hexagonal lattice of pitch 2 r_max filling the cone from the outlet up, each displaced randomly inside its own
+    lattice cell (no overlaps): a seeded random packing that needs no insertion loop.  The hopper height follows
+    from n.  The gate (family 2) closes the outlet while ``closed``; changing its family to ``GATE_OPEN_FAMILY``
+    (deme_change_family / ChangeFamily) opens it.  The floor 0.1 m below catches discharge.
+    Contact detection runs every ``cd_freq`` steps with the contact margin ``margin`` (default 0.1 r_median).
+    ``wall_clearance`` below 1 starts the outer spheres pressed into the walls (used by parity tests).
+    """
+    rng = np.random.default_rng(seed)
+    th = math.radians(half_angle_deg)
+    tan_t, cos_t = math.tan(th), math.cos(th)
+    r, r_cls, cls = _hopper_radii(n, r_median, sigma, r_clip, n_classes, rng)
+    r_max = float(r.max())
+    a = 2.0 * r_max * 1.01
+    u_out = (outlet / 2) / tan_t  # axial distance from the apex to the outlet
+    u_top, P = _hopper_top(n, a, r_max, tan_t, cos_t, u_out, wall_clearance)
     P = P[np.argsort(P[:, 2], kind="stable")][:n]
     # random displacement inside each lattice cell, bounded so that no two spheres overlap
     d = rng.normal(size=(n, 3))
@@ -365,6 +379,8 @@ def hopper(n: int = 4_000_000, r_median: float = 1.5e-3, sigma: float = 0.25, r_
         gate = s.AddBCPlane((0.0, 0.0, shift + u_out), (0.0, 0.0, 1.0), mat)
         gate.SetFamily(2)
         s.SetFamilyFixed(2)
+        s.SetFamilyFixed(GATE_OPEN_FAMILY)
+        s.DisableContactBetweenFamilies(0, GATE_OPEN_FAMILY)
     s.SetFamilyFixed(1)
     s.SetInitTimeStep(dt)
     s.SetGravitationalAcceleration((0, 0, -9.81))
@@ -373,7 +389,86 @@ def hopper(n: int = 4_000_000, r_median: float = 1.5e-3, sigma: float = 0.25, r_
     s.SetInitBinSize(2.0 * float(r.min()))
     built = s.Initialize()
     built.info.update(workload="hopper", n=n, u_out=u_out, u_top=u_top, R_top=u_top * tan_t, r_max=r_max,
-                      lattice_spacing=a, seed=seed, n_classes=n_classes, apex_z=shift)
+                      lattice_spacing=a, seed=seed, n_classes=n_classes, apex_z=shift,
+                      volume=math.pi * tan_t ** 2 * (u_top ** 3 - u_out ** 3) / 3.0)
+    return built
+
+
+def hopper_wedge(n: int = 4_000_000, r_median: float = 1.5e-3, sigma: float = 0.25, r_clip=(0.75e-3, 3e-3),
+                 rho: float = 2500.0, half_angle_deg: float = 30.0, outlet: float = 0.04, n_classes: int = 64,
+                 seed: int = 4, dt: float = 2e-6, cd_freq: int = 5, margin: float | None = None,
+                 packing_seed_jitter: float = 0.9):
+    """The hopper as the reference can express it, with planes only: a wedge (V-shaped trough) whose two walls lean
+    ``half_angle_deg`` from the vertical, closed by two end planes, with an outlet slot ``outlet`` wide under a gate
+    plane and a catch floor 0.1 m below.  Its length makes its volume between the outlet and the top equal to the
+    conical hopper's for the same n; the same log-normal spheres start on the same kind of lattice.  Used to time
+    the reference's own kernels on the polydisperse hopper workload, since the cone has no counterpart there."""
+    rng = np.random.default_rng(seed)
+    th = math.radians(half_angle_deg)
+    tan_t, cos_t = math.tan(th), math.cos(th)
+    r, r_cls, cls = _hopper_radii(n, r_median, sigma, r_clip, n_classes, rng)
+    r_max = float(r.max())
+    a = 2.0 * r_max * 1.01
+    u_out = (outlet / 2) / tan_t
+    u_top, _ = _hopper_top(n, a, r_max, tan_t, cos_t, u_out, 1.02)
+    volume = math.pi * tan_t ** 2 * (u_top ** 3 - u_out ** 3) / 3.0
+    L = volume / (tan_t * (u_top ** 2 - u_out ** 2))  # trough cross-section between outlet and top, times L
+    dy, dz = a * math.sqrt(3.0) / 2.0, a * math.sqrt(2.0 / 3.0)
+    while True:
+        X_top = u_top * tan_t
+        nx, ny, nz = int(2 * X_top / a) + 2, int(L / dy) + 2, int((u_top - u_out) / dz) + 2
+        K, J, I = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+        px = -X_top + I * a + np.where((J + K) % 2 == 0, 0.0, a / 2)
+        py = -L / 2 + r_max * 1.02 + J * dy + np.where(K % 2 == 0, 0.0, dy / 3)
+        pz = u_out + r_max + K * dz
+        P = np.stack([px.ravel(), py.ravel(), pz.ravel()], axis=1)
+        clear = 1.02 * r_max / cos_t
+        ok = ((np.abs(P[:, 0]) <= P[:, 2] * tan_t - clear) & (P[:, 2] <= u_top - r_max)
+              & (np.abs(P[:, 1]) <= L / 2 - 1.02 * r_max))
+        if ok.sum() >= n:
+            break
+        L *= 1.05
+    P = P[ok]
+    P = P[np.argsort(P[:, 2], kind="stable")][:n]
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    d *= (rng.random(n) * packing_seed_jitter * np.maximum(a / 2 - r, 0.0))[:, None]
+    P = P + d
+    z_floor = -0.1
+    s = SceneBuilder()
+    side = max(2 * u_top * tan_t, L) + 8 * r_max
+    height = u_top - z_floor + 8 * r_max
+    box = max(side, height)
+    s.InstructBoxDomainDimension(box, box, box)
+    s.SetCoordSysOrigin("center")
+    shift = -box / 2 + 4 * r_max - z_floor
+    mat = s.LoadMaterial({"E": 1e8, "nu": 0.3, "CoR": 0.4, "mu": 0.5, "Crr": 0.0})
+    types = [s.LoadSphereType(sphere_mass(float(rc), rho), float(rc), mat) for rc in r_cls]
+    b = s.AddClumps([types[c] for c in cls], (P + np.array([0.0, 0.0, shift])).astype(f32))
+    b.SetFamily(0)
+    walls = s.AddExternalObject()
+    apex = (0.0, 0.0, shift)
+    walls.AddPlane(apex, (cos_t, 0.0, math.sin(th)), mat)   # x >= -z tan(theta)
+    walls.AddPlane(apex, (-cos_t, 0.0, math.sin(th)), mat)  # x <= z tan(theta)
+    walls.AddPlane((0.0, -L / 2, shift), (0.0, 1.0, 0.0), mat)
+    walls.AddPlane((0.0, L / 2, shift), (0.0, -1.0, 0.0), mat)
+    walls.AddPlane((0.0, 0.0, shift + z_floor), (0.0, 0.0, 1.0), mat)
+    walls.SetFamily(1)
+    gate = s.AddBCPlane((0.0, 0.0, shift + u_out), (0.0, 0.0, 1.0), mat)
+    gate.SetFamily(2)
+    s.SetFamilyFixed(1)
+    s.SetFamilyFixed(2)
+    s.SetFamilyFixed(GATE_OPEN_FAMILY)
+    s.DisableContactBetweenFamilies(0, GATE_OPEN_FAMILY)
+    s.SetInitTimeStep(dt)
+    s.SetGravitationalAcceleration((0, 0, -9.81))
+    s.SetCDUpdateFreq(cd_freq)
+    s.SetExpandFactor(0.1 * r_median if margin is None else margin)
+    s.SetInitBinSize(2.0 * float(r.min()))
+    built = s.Initialize()
+    built.info.update(workload="hopper_wedge", n=n, u_out=u_out, u_top=u_top, L=L, r_max=r_max, lattice_spacing=a,
+                      seed=seed, n_classes=n_classes, apex_z=shift,
+                      volume=L * tan_t * (u_top ** 2 - u_out ** 2), cone_volume=volume)
     return built
 
 

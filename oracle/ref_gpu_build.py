@@ -226,7 +226,7 @@ def bench_shell_drum(n_clumps: int = 1_000_000, spacing: float = 0.745):
     return _workloads().drum(n_clumps, shell=True, spacing=spacing)
 
 
-def prebuild(bench_clumps: int = 1_000_000, cpu_sample_clumps: int = 200_000) -> list:
+def prebuild(bench_clumps: int = 1_000_000, cpu_sample_clumps: int = 200_000, bench_hopper_spheres: int = 4_000_000) -> list:
     """For machines without the reference's sources: the driver, the parity scenes' cubins (FMA off), the benchmark
     drum's cubins (NVRTC default and FMA off), and the reference's CPU build for the benchmark's bounded CPU
     sample."""
@@ -236,6 +236,8 @@ def prebuild(bench_clumps: int = 1_000_000, cpu_sample_clumps: int = 200_000) ->
     out.append(build_cubins(bench_shell_drum(bench_clumps), fmad=True))
     # the full-size parity test runs the benchmark drum against both builds
     out.append(build_cubins(bench_shell_drum(bench_clumps), fmad=False))
+    # the plane-only wedge hopper the benchmark times the reference's kernels on
+    out.append(build_cubins(_workloads().hopper_wedge(n=bench_hopper_spheres), fmad=True))
     out.append(_ref_build().build(bench_shell_drum(cpu_sample_clumps)))
     return out
 
