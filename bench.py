@@ -598,7 +598,7 @@ def main():
     tuning = None
     if args.autotune:
         # untimed: time every search shape on a few steps from the prepared state, keep the fastest, restore the state
-        tuning = s.autotune(steps_per_trial=5)
+        tuning = s.autotune(steps_per_trial=10)
 
     # ---- warm-up (the clock sampler starts here so it has samples when the timed region is short) ----
     sampler = ClockSampler(local_rank)
@@ -790,24 +790,31 @@ def adjoint_measure(args, stream):
 
 
 def batched_measure(args, stream, rank=0, world=1, dist=None):
-    """The batched calibration sweep: all scenes packed into one run, a forward window and a forward + adjoint
-    window (per-scene loss: the mean final height of its spheres; gradients for every scene's material), against
-    the same windows run scene by scene (timed on a sample of scenes spanning the sizes, fitted linearly in the
-    sphere count and summed over all scenes).  With N ranks the scenes are split by sphere count (each rank packs
+    """The batched calibration sweep: all scenes packed into one run (each scene with its own search grid, shapes
+    from the autotuner, whole steps replayed from CUDA graphs), a forward window and a forward + adjoint window
+    (per-scene loss: the mean final height of its spheres; gradients for every scene's material), against the same
+    windows run scene by scene.  The scenes start pressed (lattice pitch 1.98 r) so that contacts carry the load
+    from the first step.  Scene by scene, the forward window is timed for every scene with CUDA graphs and on a
+    sample spanning the sizes without them; the adjoint window on a sample (the sample times are fitted linearly in
+    the sphere count and summed over all scenes).  With N ranks the scenes are split by sphere count (each rank packs
     its share; no exchange while stepping), times are the max over ranks, and the per-scene gradients are gathered
     with one all-reduce at the end; the scene-by-scene baseline is measured on one GPU only."""
     import numpy as np
     import torch
     from deme_b200 import Solver, adjoint, sharding, workloads
     all_specs = workloads.batch_scene_specs(args.batch_scenes)
+    for sp in all_specs:
+        sp.update(pitch=1.98, lift=0.98)
     shard = (sharding.partition_scenes([sp["n"] for sp in all_specs], world)[rank] if world > 1
              else list(range(len(all_specs))))
     specs = [all_specs[i] for i in shard]
     T, K = args.batch_steps, args.batch_checkpoint
 
-    def solver(built):
+    def solver(built, graph=False):
         s = Solver(built)
         s.lib.deme_set_streams(s.h, C.c_void_p(stream.cuda_stream), C.c_void_p(stream.cuda_stream))
+        if graph:
+            s.set_graph(True)
         return s
 
     def timed(fn):
@@ -828,19 +835,27 @@ def batched_measure(args, stream, rank=0, world=1, dist=None):
     built = workloads.batched_settling(specs)
     ranges = built.info["scenes"]
     w = solver(built)
-    w.step(3)
+    tuning = w.autotune(steps_per_trial=3)  # untimed; the shapes apply to every packed run below
     w.close()
-    sf = solver(built)
+
+    def tuned(s):
+        s.set_search_shape(tuning["shape"], tuning["cell_factor"])
+        s.set_kernel_shapes(tuning["force_shape"], tuning["exact_threads"], tuning["integrate_threads"])
+        return s
+
+    sf = tuned(solver(built, graph=True))
+    sf.step(3)
     t_fwd, _ = timed(lambda: sf.step(T))
     nC = sf.num_contacts()
     sf.close()
-    sa = solver(built)
+    sa = tuned(solver(built))
     t_rec, _ = timed(lambda: adjoint.record(sa, T, K))
     t_bwd, out = timed(lambda: adjoint.backward(sa, d_pos=height_seed(built, ranges)))
     sa.close()
     # each scene loads one material, in scene order: material row i is the gradient of local scene i
     grads = sharding.gather_scene_rows({shard[i]: out["d_material"][i] for i in range(len(shard))}, len(all_specs), 4,
                                        dist=dist, device="cuda")
+    n_spheres = int(sum(sp["n"] for sp in specs))
     if world > 1:
         tt = torch.tensor([t_fwd, t_rec + t_bwd], dtype=torch.float64, device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -848,22 +863,29 @@ def batched_measure(args, stream, rank=0, world=1, dist=None):
         n = len(all_specs)
         return {"workload": f"{n} settling scenes split over {world} GPUs by sphere count, each rank's share packed in "
                             "one run: 500-20,000 spheres (log-uniform), r 2-5 mm, box 0.05-0.2 m, dt 1e-5, CD every "
-                            "step",
+                            "step, pressed start",
                 "n_scenes": n, "n_spheres": int(sum(sp["n"] for sp in all_specs)), "steps": T, "checkpoint_every": K,
                 "forward_s": t_fwd, "forward_adjoint_s": t_adj, "scenes_per_s": n / t_fwd,
                 "scenes_per_s_with_adjoint": n / t_adj, "scaling": "strong (fixed scene set)",
                 "material_gradients_finite": bool(np.all(np.isfinite(grads))),
                 "gathered_gradient_rows": int(np.count_nonzero(np.any(grads != 0, axis=1)))}
-    # scene by scene, on a sample spanning the sizes
+    # scene by scene: the forward window of every scene with CUDA graphs
     sizes = np.array([sp["n"] for sp in specs])
+    seq_graph = 0.0
+    for i in range(len(specs)):
+        b1 = workloads.single_settling(specs[i])
+        s1 = solver(b1, graph=True)
+        s1.step(3)
+        tf, _ = timed(lambda: s1.step(T))
+        s1.close()
+        seq_graph += tf
+    # on a sample spanning the sizes: the forward window launched step by step, and the adjoint window
     pick = np.unique(np.argsort(sizes)[np.linspace(0, len(specs) - 1, args.batch_sample).astype(int)])
     rows = []
     for i in pick:
         b1 = workloads.single_settling(specs[i])
         s1 = solver(b1)
         s1.step(3)
-        s1.close()
-        s1 = solver(b1)
         tf, _ = timed(lambda: s1.step(T))
         s1.close()
         s1 = solver(b1)
@@ -878,14 +900,19 @@ def batched_measure(args, stream, rank=0, world=1, dist=None):
     seq_a = float(np.sum(np.polyval(fit_a, sizes)))
     n = len(specs)
     return {"workload": f"{n} settling scenes packed in one run: 500-20,000 spheres (log-uniform), r 2-5 mm, box "
-                        "0.05-0.2 m, friction and restitution U[0.2, 0.8] per scene, dt 1e-5, CD every step",
-            "n_scenes": n, "n_spheres": int(sizes.sum()), "steps": T, "checkpoint_every": K,
-            "n_contacts_final": nC,
+                        "0.05-0.2 m, friction and restitution U[0.2, 0.8] per scene, dt 1e-5, CD every step, pressed "
+                        "start (lattice pitch 1.98 r)",
+            "n_scenes": n, "n_spheres": n_spheres, "steps": T, "checkpoint_every": K,
+            "n_contacts_final": nC, "contacts_per_sphere_final": nC / n_spheres,
+            "packed_tuning": tuning,
             "forward_s": t_fwd, "forward_adjoint_s": t_rec + t_bwd,
             "scenes_per_s": n / t_fwd, "scenes_per_s_with_adjoint": n / (t_rec + t_bwd),
+            "sequential_scenes_per_s_graphs": n / seq_graph,
             "sequential_scenes_per_s": n / seq_f, "sequential_scenes_per_s_with_adjoint": n / seq_a,
+            "speedup_forward_vs_graphs": seq_graph / t_fwd,
             "speedup_forward": seq_f / t_fwd, "speedup_with_adjoint": seq_a / (t_rec + t_bwd),
-            "sequential_sample": f"{len(rows)} scenes timed alone, time fitted linearly in sphere count",
+            "sequential_sample": f"forward with graphs: all {n} scenes timed alone; step by step and with the "
+                                 f"adjoint: {len(rows)} scenes timed alone, time fitted linearly in sphere count",
             "material_gradients_finite": bool(np.all(np.isfinite(out["d_material"])))}
 
 

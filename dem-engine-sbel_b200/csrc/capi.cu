@@ -196,29 +196,108 @@ const char* deme_status_string(int32_t s) {
 
 const char* deme_get_error(deme_handle* h) { return h ? h->err.c_str() : "null handle"; }
 
-// Search cells: cubes of edge cell_factor x max(bin size, largest expanded diameter), over the user's domain (or
-// the voxel world), coarsened while there would be more than 2^26 of them.  Factor 1 gives the most cells, which
-// the cell arrays are sized for; any factor >= 1 finds the same pairs.
-static void set_cell_grid(deme_handle* h, double cell_factor) {
+// Search cells: per scene, cubes of edge cell_factor x max(bin size, the scene's largest expanded diameter) over the
+// scene's box (the user's domain, or the voxel world, when the run holds one scene), coarsened together while there
+// would be more than 2^26 cells in all.  Factor 1 gives the most cells, which the cell arrays are sized for; any
+// factor >= 1 finds the same pairs.  The grid table goes to the device (h->grids).
+static int32_t set_cell_grid(deme_handle* h, double cell_factor) {
     const deme_sim_params* p = &h->params;
-    SimConsts& k = h->k;
-    const double world[3] = {p->voxel_size * std::ldexp(1.0, p->nvXp2), p->voxel_size * std::ldexp(1.0, p->nvYp2),
-                             p->voxel_size * std::ldexp(1.0, p->nvZp2)};
-    double dom[3];
-    for (int a = 0; a < 3; a++) dom[a] = p->domain[a] > 0.f ? (double)p->domain[a] : world[a];
-    double cs = std::max(p->bin_size, 2.0 * (double)k.r_max_cd) * (1.0 + 1e-6) * std::max(cell_factor, 1.0);
-    if (!(cs > 0.0)) cs = 1.0;
-    auto ncell = [&](double c, double d) { return (uint64_t)std::ceil(d / c) + 1; };
-    while (ncell(cs, dom[0]) * ncell(cs, dom[1]) * ncell(cs, dom[2]) > (1ull << 26)) cs *= 1.25;
-    k.cell_size = cs;
-    k.inv_cell = 1.0 / cs;
-    k.gx = (uint32_t)ncell(cs, dom[0]);
-    k.gy = (uint32_t)ncell(cs, dom[1]);
-    k.gz = (uint32_t)ncell(cs, dom[2]);
-    h->nCells = k.gx * k.gy * k.gz;
+    const double factor = std::max(cell_factor, 1.0);
+    const uint32_t nG = (uint32_t)h->sceneRmax.size();
+    std::vector<SearchGrid> g(nG);
+    double grow = 1.0;
+    uint64_t total = 0;
+    while (true) {
+        total = 0;
+        for (uint32_t sc = 0; sc < nG; sc++) {
+            double cs = std::max(p->bin_size, 2.0 * (double)h->sceneRmax[sc]) * (1.0 + 1e-6) * factor * grow;
+            if (!(cs > 0.0)) cs = 1.0;
+            const double* lo = &h->sceneBox[6 * (size_t)sc];
+            uint64_t n[3];
+            for (int a = 0; a < 3; a++) n[a] = (uint64_t)std::ceil(std::max(lo[3 + a] - lo[a], 0.0) / cs) + 1;
+            SearchGrid& q = g[sc];
+            q = SearchGrid{};
+            q.ox = lo[0];
+            q.oy = lo[1];
+            q.oz = lo[2];
+            q.inv_cell = 1.0 / cs;
+            q.gx = (uint32_t)std::min<uint64_t>(n[0], 1u << 26);
+            q.gy = (uint32_t)std::min<uint64_t>(n[1], 1u << 26);
+            q.gz = (uint32_t)std::min<uint64_t>(n[2], 1u << 26);
+            q.base = (uint32_t)std::min<uint64_t>(total, 0xFFFFFFFFull);
+            q.r_max_cd = h->sceneRmax[sc];
+            total += (uint64_t)q.gx * q.gy * q.gz;
+        }
+        if (total <= (1ull << 26)) break;
+        grow *= 1.25;
+    }
+    h->nCells = (uint32_t)total;
     h->cellBits = 1;
     while ((1ull << h->cellBits) < h->nCells) h->cellBits++;
-    h->cellFactor = (float)std::max(cell_factor, 1.0);
+    h->cellFactor = (float)factor;
+    if (!h->grids) TRY(dalloc_n(h, &h->grids, std::max(nG, 1u)));
+    CUDA_TRY(h, cudaMemcpy(h->grids, g.data(), nG * sizeof(SearchGrid), cudaMemcpyHostToDevice));
+    h->k.grids = h->grids;
+    h->k.grid0 = g[0];  // a run of one scene reads its grid from here; its origin is the domain's corner, base 0
+    return DEME_OK;
+}
+
+// The scenes' boxes and largest expanded radii for the search grids: one scene spanning the domain, or, when the
+// scene packs several independent scenes (owner_scene), one box per scene (scene_box, or the bounding box of the
+// scene's initial owner positions widened by its clump reach and half its size).
+static int32_t set_scene_boxes(deme_handle* h, const deme_scene* s) {
+    const deme_sim_params* p = &h->params;
+    const double world[3] = {p->voxel_size * std::ldexp(1.0, p->nvXp2), p->voxel_size * std::ldexp(1.0, p->nvYp2),
+                             p->voxel_size * std::ldexp(1.0, p->nvZp2)};
+    if (!s->owner_scene) {
+        h->sceneRmax.assign(1, h->k.r_max_cd);
+        h->sceneBox.assign(6, 0.0);
+        for (int a = 0; a < 3; a++) h->sceneBox[3 + a] = p->domain[a] > 0.f ? (double)p->domain[a] : world[a];
+        return DEME_OK;
+    }
+    uint32_t nG = 0;
+    for (uint32_t o = 0; o < h->nO; o++) nG = std::max(nG, s->owner_scene[o] + 1);
+    if (nG > (1u << 20)) {
+        h->err = "owner_scene: more than 2^20 scenes";
+        return DEME_ERR_INVALID;
+    }
+    h->sceneRmax.assign(nG, 0.f);
+    std::vector<float> reach(nG, 0.f);
+    for (uint32_t i = 0; i < h->nS; i++) {
+        const uint32_t sc = s->owner_scene[s->sphere_owner[i]];
+        float r = s->radius[i];
+        r += p->beta;
+        h->sceneRmax[sc] = std::max(h->sceneRmax[sc], r);
+        const float rel = std::sqrt(s->relX[i] * s->relX[i] + s->relY[i] * s->relY[i] + s->relZ[i] * s->relZ[i]);
+        reach[sc] = std::max(reach[sc], rel + r);
+    }
+    h->sceneBox.assign(6 * (size_t)nG, 0.0);
+    if (s->scene_box) {
+        for (size_t i = 0; i < 6 * (size_t)nG; i++) h->sceneBox[i] = (double)s->scene_box[i];
+        return DEME_OK;
+    }
+    std::vector<double> lo(3 * (size_t)nG, 1e300), hi(3 * (size_t)nG, -1e300);
+    const uint64_t mx = (1ull << p->nvXp2) - 1, my = (1ull << p->nvYp2) - 1;
+    for (uint32_t o = 0; o < h->nClumps; o++) {
+        const uint32_t sc = s->owner_scene[o];
+        const uint64_t v = s->voxel[o];
+        const double x[3] = {(double)(v & mx) * p->voxel_size + s->locX[o] * p->l,
+                             (double)((v >> p->nvXp2) & my) * p->voxel_size + s->locY[o] * p->l,
+                             (double)(v >> (p->nvXp2 + p->nvYp2)) * p->voxel_size + s->locZ[o] * p->l};
+        for (int a = 0; a < 3; a++) {
+            lo[3 * sc + a] = std::min(lo[3 * sc + a], x[a]);
+            hi[3 * sc + a] = std::max(hi[3 * sc + a], x[a]);
+        }
+    }
+    for (uint32_t sc = 0; sc < nG; sc++)
+        for (int a = 0; a < 3; a++) {
+            double l0 = lo[3 * sc + a], h0 = hi[3 * sc + a];
+            if (l0 > h0) l0 = h0 = 0.0;  // a scene without clumps
+            const double pad = reach[sc] + 0.25 * (h0 - l0);
+            h->sceneBox[6 * sc + a] = l0 - pad;
+            h->sceneBox[6 * sc + 3 + a] = h0 + pad;
+        }
+    return DEME_OK;
 }
 
 static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_scene* s) {
@@ -312,6 +391,12 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
     const double world[3] = {p->voxel_size * std::ldexp(1.0, p->nvXp2), p->voxel_size * std::ldexp(1.0, p->nvYp2),
                              p->voxel_size * std::ldexp(1.0, p->nvZp2)};
     const double wmax = std::max(world[0], std::max(world[1], world[2]));
+    if (s->owner_scene) {
+        TRY(dalloc_n(h, &h->ownerScene, std::max(nO, 1u)));
+        CUDA_TRY(h, cudaMemcpy(h->ownerScene, s->owner_scene, nO * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        k.ownerScene = h->ownerScene;
+    }
+    TRY(set_scene_boxes(h, s));
     k.prefilter_abs = (float)(4e-7 * wmax + 1e-9);
     {
         // sphere id in the low bits of the record's last word, a CD radius bound in the bits above (at least 4 of
@@ -327,7 +412,7 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
         }
         k.id_mask = (1u << k.q_shift) - 1u;
     }
-    set_cell_grid(h, 1.0);
+    TRY(set_cell_grid(h, 1.0));
 
     // ---- device arrays ----
     TRY(dalloc_n(h, &h->voxel, nO));
@@ -608,11 +693,11 @@ static int32_t cd_search(deme_handle* h, const StateView& s, AnalPlaced* anal, c
         launch_cell_scatter(k, s, cd, st);  // counting sort and record writes in one pass
     }
     ContactBuf& nb = h->lists[h->cur ^ 1];
-    CUDA_TRY(h, cudaMemsetAsync(cd.counters, 0, 2 * sizeof(uint32_t), st));
+    CUDA_TRY(h, cudaMemsetAsync(cd.counters, 0, 3 * sizeof(uint32_t), st));  // pool, overflow, tile queue
     if (retry) launch_cnt_init(k, cd, st);
     launch_pair_find(k, s, cd, h->candCap, h->findShape, st);
     launch_pair_overflow(k, s, cd, h->candCap, st);
-    launch_pair_exact(k, s, cd, h->candCap, st);
+    launch_pair_exact(k, s, cd, h->candCap, h->exactThreads, st);
     TRY(check_launch(h, "contact search"));
     exclusive_scan_u32_onepass(cd.cnt, h->nS + 1, nb.off, nb.dN, h->scratch, h->dErr, st);
     if (hCnt) {
@@ -806,7 +891,8 @@ int32_t deme_compute_forces(deme_handle* h) {
         }
         aa.partial = h->analPartial;
     }
-    launch_force(k, s, c.view(), nL, h->nW > 0, out, aa, h->userForce.lib ? &h->userForce : nullptr, st);
+    launch_force(k, s, c.view(), nL, h->nW > 0, out, aa, h->userForce.lib ? &h->userForce : nullptr, h->forceShape,
+                 st);
     TRY(check_launch(h, "force"));
     h->outsValid = out != nullptr;
     return DEME_OK;
@@ -836,7 +922,7 @@ int32_t deme_integrate(deme_handle* h) {
                                          st));  // ProfScope counts the launch
         }
     } else {
-        launch_integrate(h->k, h->state_view(), st);
+        launch_integrate(h->k, h->state_view(), h->integrateThreads, st);
     }
     if (needs_device_time(h)) launch_advance_time(h->dTime, h->k.h, h->dErr, st);
     TRY(check_launch(h, "integrate"));
@@ -924,6 +1010,10 @@ static std::vector<uint8_t> graph_key(const deme_handle* h) {
     put(&h->jitGeneration, sizeof(h->jitGeneration));  // a new image may load where a released one was
     put(&h->params.cd_update_freq, sizeof(h->params.cd_update_freq));
     put(&h->findShape, sizeof(h->findShape));
+    put(&h->cellFactor, sizeof(h->cellFactor));
+    put(&h->forceShape, sizeof(h->forceShape));
+    put(&h->exactThreads, sizeof(h->exactThreads));
+    put(&h->integrateThreads, sizeof(h->integrateThreads));
     return key;
 }
 
@@ -1141,18 +1231,34 @@ int32_t deme_set_search_shape(deme_handle* h, int32_t shape, float cell_factor) 
     TRY(cd_finish(h));
     CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
     h->findShape = shape;
-    set_cell_grid(h, cell_factor);
-    return DEME_OK;
+    return set_cell_grid(h, cell_factor);
 }
 
 int32_t deme_search_shape_count(void) { return find_shape_count(); }
+
+int32_t deme_force_shape_count(void) { return force_shape_count(); }
+
+int32_t deme_set_kernel_shapes(deme_handle* h, int32_t force_shape, int32_t exact_threads, int32_t integrate_threads) {
+    if (!h) return DEME_ERR_INVALID;
+    auto ok_threads = [](int32_t t) { return t >= 32 && t <= 512 && t % 32 == 0; };
+    if (force_shape < 0 || force_shape >= force_shape_count() || !ok_threads(exact_threads) ||
+        !ok_threads(integrate_threads)) {
+        h->err = "kernel shapes out of range (force shape < deme_force_shape_count(), threads 32..512 in steps of 32)";
+        return DEME_ERR_INVALID;
+    }
+    TRY(cd_finish(h));
+    CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
+    h->forceShape = force_shape;
+    h->exactThreads = (uint32_t)exact_threads;
+    h->integrateThreads = (uint32_t)integrate_threads;
+    return DEME_OK;
+}
 
 // Times every (candidate-scan shape, cell factor) pair on a few steps from the same state, keeps the fastest and
 // puts the state back.  Every pair gives the same contact lists, so only the time differs.
 int32_t deme_autotune(deme_handle* h, int32_t steps_per_trial, deme_tuning* out) {
     if (!h) return DEME_ERR_INVALID;
     const int32_t steps = steps_per_trial > 0 ? steps_per_trial : 5;
-    const float factors[] = {1.f, 1.25f, 1.5f};
     TRY(cd_finish(h));
     Checkpoint ck;
     TRY(save_checkpoint(h, ck));
@@ -1162,38 +1268,81 @@ int32_t deme_autotune(deme_handle* h, int32_t steps_per_trial, deme_tuning* out)
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     CUDA_TRY(h, cudaEventCreate(&e0));
     CUDA_TRY(h, cudaEventCreate(&e1));
+    int trials = 0;
+    int32_t st = DEME_OK;
+    // one trial: the current shapes on `steps` steps from the checkpoint (after one untimed step that settles the
+    // buffer sizes for them)
+    auto trial = [&](float& ms) -> int32_t {
+        h->cur = cur0;
+        TRY(restore_checkpoint(h, ck));
+        TRY(step_plain(h));
+        cudaEventRecord(e0, h->st_dt);
+        for (int32_t i = 0; i < steps; i++) TRY(step_plain(h));
+        cudaEventRecord(e1, h->st_dt);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= (float)steps;
+        trials++;
+        return DEME_OK;
+    };
+    // A shape replaces the one kept so far only when it is at least 1 % faster: trials of a few steps spread by
+    // about that much, and the defaults win ties.
+    constexpr float kMargin = 0.99f;
+    // 1. candidate-scan shape x cell factor, with the default shapes of the other kernels
+    const float factors[] = {1.f, 1.25f, 1.5f};
+    h->forceShape = 0;
+    h->exactThreads = h->integrateThreads = 256;
     float best = 3.4e38f, dflt = 0.f;
     int bestShape = 0;
     float bestFactor = 1.f;
-    int trials = 0;
-    int32_t st = DEME_OK;
     for (int v = 0; v < find_shape_count() && st == DEME_OK; v++) {
         for (float f : factors) {
             h->findShape = v;
-            set_cell_grid(h, f);
-            h->cur = cur0;
-            if ((st = restore_checkpoint(h, ck)) != DEME_OK) break;
-            if ((st = step_plain(h)) != DEME_OK) break;  // settles buffer sizes for this shape
-            cudaEventRecord(e0, h->st_dt);
-            for (int32_t i = 0; i < steps && st == DEME_OK; i++) st = step_plain(h);
-            cudaEventRecord(e1, h->st_dt);
-            cudaEventSynchronize(e1);
+            if ((st = set_cell_grid(h, f)) != DEME_OK) break;
             float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            ms /= (float)steps;
+            if ((st = trial(ms)) != DEME_OK) break;
             if (v == 0 && f == 1.f) dflt = ms;
-            if (ms < best) {
+            if (ms < best * kMargin || (v == 0 && f == 1.f)) {
                 best = ms;
                 bestShape = v;
                 bestFactor = f;
             }
-            trials++;
         }
+    }
+    if (st == DEME_OK) {
+        h->findShape = bestShape;
+        st = set_cell_grid(h, bestFactor);
+    }
+    // 2. force shape, 3. threads of the exact test, 4. threads of the integration, one after the other
+    int bestForce = 0;
+    for (int v = 1; v < force_shape_count() && st == DEME_OK; v++) {
+        h->forceShape = v;
+        float ms = 0.f;
+        if ((st = trial(ms)) != DEME_OK) break;
+        if (ms < best * kMargin) {
+            best = ms;
+            bestForce = v;
+        }
+    }
+    h->forceShape = bestForce;
+    const uint32_t threads[] = {128, 512};
+    for (uint32_t* knob : {&h->exactThreads, &h->integrateThreads}) {
+        const uint32_t keep = *knob;
+        uint32_t pick = keep;
+        for (uint32_t t : threads) {
+            if (st != DEME_OK) break;
+            *knob = t;
+            float ms = 0.f;
+            if ((st = trial(ms)) != DEME_OK) break;
+            if (ms < best * kMargin) {
+                best = ms;
+                pick = t;
+            }
+        }
+        *knob = pick;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    h->findShape = bestShape;
-    set_cell_grid(h, bestFactor);
     h->cur = cur0;
     const int32_t rs = restore_checkpoint(h, ck);
     free_checkpoint(h, ck);
@@ -1202,14 +1351,20 @@ int32_t deme_autotune(deme_handle* h, int32_t steps_per_trial, deme_tuning* out)
     TRY(rs);
     if (out) {
         uint32_t w = 0, slots = 0;
-        find_shape(bestShape, &w, &slots);
+        bool persistent = false;
+        find_shape(bestShape, &w, &slots, &persistent);
         out->shape = bestShape;
         out->find_warps = (int32_t)w;
         out->find_slots = (int32_t)slots;
+        out->find_persistent = persistent ? 1 : 0;
         out->cell_factor = bestFactor;
         out->ms_per_step = best;
         out->ms_per_step_default = dflt;
         out->trials = trials;
+        out->force_shape = h->forceShape;
+        out->force_threads = (int32_t)force_shape_threads(h->forceShape);
+        out->exact_threads = (int32_t)h->exactThreads;
+        out->integrate_threads = (int32_t)h->integrateThreads;
     }
     return DEME_OK;
 }

@@ -25,6 +25,17 @@ constexpr double kTwoTimesSqrtFiveOverSix = 1.825741858350554;
 constexpr double kPi = 3.1415926535897932385;
 constexpr double kPiSquared = 9.869604401089358;
 
+// The search grid of one scene: cubic cells of edge 1 / inv_cell from the origin (ox, oy, oz), in positions
+// relative to the domain's lower corner; cells [base, base + gx gy gz) of the cell arrays, row-major in x.  Positions
+// outside the grid fall into its boundary cells (cell_of clamps), which keeps every search complete.
+struct SearchGrid {
+    double ox, oy, oz;
+    double inv_cell;
+    uint32_t gx, gy, gz, base;
+    float r_max_cd;  // largest CD radius (radius + beta) of the scene's spheres
+    uint32_t pad[3];
+};
+
 // Owner state lives in HBM as packed structure-of-arrays so that one owner is read with a few wide loads:
 //   pos   : uint64 voxel id + ushort4 (locX, locY, locZ, family)
 //   quat  : float4 (w, x, y, z)
@@ -42,11 +53,13 @@ struct SimConsts {
     float G[3];
     int integrator;
     uint32_t n_spheres, n_owners, n_anal;
-    // contact-detection search grid (positions relative to the LBF corner)
-    double cell_size;
-    double inv_cell;     // 1 / cell_size
-    uint32_t gx, gy, gz;
-    float r_max_cd;      // largest CD radius (radius + beta)
+    // contact-detection search grids: one per scene (several only when independent scenes are packed into one
+    // run), each a block of cells in the cell arrays; ownerScene maps an owner to its scene (null: one scene, whose
+    // grid is also held here by value, grid0, so that a plain run reads it from the kernel parameters)
+    const SearchGrid* grids;
+    const uint32_t* ownerScene;
+    SearchGrid grid0;
+    float r_max_cd;      // largest CD radius (radius + beta) of all spheres
     float prefilter_abs; // absolute slack of the float pre-filter
     // the cell-order float4 records carry the sphere id in their low q_shift bits and, above them, an upper bound
     // of the CD radius in units of q_scale (see k_gather_sorted)

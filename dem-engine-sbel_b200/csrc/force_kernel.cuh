@@ -11,18 +11,14 @@
 
 namespace deme_b200 {
 
-// 128-thread blocks, 8 resident per SM (64 registers a thread): smaller blocks wait less at the block-wide
-// barriers (the voided-step check and the wall partials) than 256 x 4 or 512 x 2.
-#ifndef DEME_FORCE_THREADS
-#define DEME_FORCE_THREADS 128
-#endif
-#ifndef DEME_FORCE_MIN_BLOCKS
-#define DEME_FORCE_MIN_BLOCKS 8
-#endif
-constexpr uint32_t kForceThreads = DEME_FORCE_THREADS;
-template <bool kStore>
-__global__ void __launch_bounds__(kForceThreads, DEME_FORCE_MIN_BLOCKS) k_force(SimConsts k, StateView s, ContactView c, uint32_t n, bool has_hist,
-                                               ContactOutputs out, AnalAccum aa) {
+// Block shapes (threads, resident blocks per SM; 64 registers a thread in each): 128 x 8 by default, where blocks
+// wait less at the block-wide barriers (the voided-step check and the wall partials) than 256 x 4 or 512 x 2; the
+// autotuner may pick another.  Run-time compiled user models use the default.
+constexpr uint32_t kForceThreads = 128;
+constexpr uint32_t kForceMinBlocks = 8;
+template <bool kStore, uint32_t kThreads = kForceThreads, uint32_t kMinBlocks = kForceMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_force(SimConsts k, StateView s, ContactView c, uint32_t n,
+                                                               bool has_hist, ContactOutputs out, AnalAccum aa) {
     // a device error earlier in the step (a list or pool outgrew its capacity inside a replayed graph) voids the
     // step: nothing is written, and the host redoes it from the untouched state
     if (__syncthreads_or(threadIdx.x == 0 && *k.err != 0u)) return;

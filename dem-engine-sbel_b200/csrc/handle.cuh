@@ -77,6 +77,10 @@ struct deme_handle {
     CDView cd{};
     uint32_t nCells = 0;
     int cellBits = 0;
+    SearchGrid* grids = nullptr;         // per scene (one for a plain run): see set_cell_grid
+    uint32_t* ownerScene = nullptr;      // packed scenes: scene of each owner
+    std::vector<double> sceneBox;        // per scene: lower and upper corner of its search grid (6 doubles)
+    std::vector<float> sceneRmax;        // per scene: largest expanded radius
     uint32_t candCap = 0;
     ContactBuf lists[2];
     int cur = 0;
@@ -121,6 +125,10 @@ struct deme_handle {
     // search shape (deme_set_search_shape / deme_autotune): candidate-scan block shape and search-cell factor
     int32_t findShape = 0;
     float cellFactor = 1.f;
+    // block shapes of the force kernel, the exact pair test and the integration (deme_set_kernel_shapes)
+    int32_t forceShape = 0;
+    uint32_t exactThreads = 256;
+    uint32_t integrateThreads = 256;
     // CUDA-graph replay of whole steps (deme_set_graph): one executable graph per parity of `cur` at the start of
     // a detection window, keyed by everything its launches captured.
     bool useGraph = false;

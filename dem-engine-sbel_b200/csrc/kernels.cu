@@ -20,6 +20,7 @@
 // Contacts sharing owner(A) are adjacent, so the A side is reduced inside the warp before one vector atomic per
 // segment; the B side uses one float4 atomic per contact.  One kernel per owner integrates
 // (src/kernel/DEMIntegrationKernels.cu:46-179) and clears the accumulators for the next step.
+#include <algorithm>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -32,6 +33,15 @@
 namespace deme_b200 {
 
 static inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+// The search grid of the scene that `owner` belongs to.  kPacked: several scenes, looked up through ownerScene (into
+// `tmp`); otherwise the one grid in the kernel parameters, read from there as it is used.
+template <bool kPacked>
+__device__ __forceinline__ const SearchGrid& grid_of(const SimConsts& k, uint32_t owner, SearchGrid& tmp) {
+    if (!kPacked) return k.grid0;
+    tmp = k.grids[__ldg(k.ownerScene + owner)];
+    return tmp;
+}
 
 // The analytical components the spheres of `owner` may meet: all of them, or the owner's range when the scene
 // packs several independent scenes (their walls must not reach each other's spheres).
@@ -100,6 +110,7 @@ void launch_place_anal(const SimConsts& k, const StateView& s, const AnalRaw* ra
 // Per sphere: home cell and analytical-contact count (getNumberOfBinsEachSphereTouches's analytical loop,
 // DEMBinSphereKernels.cu:72-113).  The exact position is not stored: the cell-order record writer forms it again
 // from the owner pose (the same arithmetic, so the same bits), which costs less than writing and re-reading it.
+template <bool kPacked>
 __global__ void __launch_bounds__(256) k_sphere_prep(SimConsts k, StateView s, CDView cd) {
     const uint32_t sid = blockIdx.x * blockDim.x + threadIdx.x;
     if (sid >= k.n_spheres) return;
@@ -107,10 +118,12 @@ __global__ void __launch_bounds__(256) k_sphere_prep(SimConsts k, StateView s, C
     float4 sp;
     double X, Y, Z;
     sphere_center(k, s, sid, owner, sp, X, Y, Z);
-    const uint32_t cx = cell_of(X, k.inv_cell, k.gx);
-    const uint32_t cy = cell_of(Y, k.inv_cell, k.gy);
-    const uint32_t cz = cell_of(Z, k.inv_cell, k.gz);
-    const uint32_t key = cx + k.gx * (cy + k.gy * cz);
+    SearchGrid tmp;
+    const SearchGrid& g = grid_of<kPacked>(k, owner, tmp);
+    const uint32_t cx = cell_of(kPacked ? X - g.ox : X, g.inv_cell, g.gx);
+    const uint32_t cy = cell_of(kPacked ? Y - g.oy : Y, g.inv_cell, g.gy);
+    const uint32_t cz = cell_of(kPacked ? Z - g.oz : Z, g.inv_cell, g.gz);
+    const uint32_t key = (kPacked ? g.base : 0u) + cx + g.gx * (cy + g.gy * cz);
     cd.cellKey[sid] = key;
     cd.idSeq[sid] = sid;
     atomicAdd(&cd.cellCount[key], 1u);
@@ -132,7 +145,10 @@ __global__ void __launch_bounds__(256) k_sphere_prep(SimConsts k, StateView s, C
 void launch_sphere_prep(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st) {
     if (!(k.n_spheres)) return;
     ProfScope prof_(KID_SPHERE_PREP, st);
-    if (k.n_spheres) k_sphere_prep<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
+    if (k.ownerScene)
+        k_sphere_prep<true><<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
+    else
+        k_sphere_prep<false><<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
 }
 
 __device__ __forceinline__ uint4 pack_ranges(const uint32_t lo[3], const uint32_t hi[3]) {
@@ -286,17 +302,24 @@ struct SearchBox {
     uint32_t x0, x1, y0, y1, z0, z1, cy, cz;
 };
 
-__device__ __forceinline__ SearchBox search_box(const SimConsts& k, double x, double y, double z, float rf) {
-    const double reach = (double)rf + (double)k.r_max_cd + (double)k.prefilter_abs;
+template <bool kPacked>
+__device__ __forceinline__ SearchBox search_box(const SimConsts& k, const SearchGrid& g, double x, double y, double z,
+                                                float rf) {
+    const double reach = (double)rf + (double)g.r_max_cd + (double)k.prefilter_abs;
+    if (kPacked) {  // a single scene's grid starts at the domain's lower corner
+        x -= g.ox;
+        y -= g.oy;
+        z -= g.oz;
+    }
     SearchBox b;
-    b.x0 = cell_of(x - reach, k.inv_cell, k.gx);
-    b.x1 = cell_of(x + reach, k.inv_cell, k.gx);
-    b.y0 = cell_of(y - reach, k.inv_cell, k.gy);
-    b.y1 = cell_of(y + reach, k.inv_cell, k.gy);
-    b.z0 = cell_of(z - reach, k.inv_cell, k.gz);
-    b.z1 = cell_of(z + reach, k.inv_cell, k.gz);
-    b.cy = cell_of(y, k.inv_cell, k.gy);
-    b.cz = cell_of(z, k.inv_cell, k.gz);
+    b.x0 = cell_of(x - reach, g.inv_cell, g.gx);
+    b.x1 = cell_of(x + reach, g.inv_cell, g.gx);
+    b.y0 = cell_of(y - reach, g.inv_cell, g.gy);
+    b.y1 = cell_of(y + reach, g.inv_cell, g.gy);
+    b.z0 = cell_of(z - reach, g.inv_cell, g.gz);
+    b.z1 = cell_of(z + reach, g.inv_cell, g.gz);
+    b.cy = cell_of(y, g.inv_cell, g.gy);
+    b.cz = cell_of(z, g.inv_cell, g.gz);
     return b;
 }
 
@@ -310,17 +333,18 @@ __device__ __forceinline__ SearchBox search_box(const SimConsts& k, double x, do
 #ifndef DEME_FIND_UNROLL
 #define DEME_FIND_UNROLL 2
 #endif
-template <typename Visit>
-__device__ __forceinline__ void for_each_forward_candidate(const SimConsts& k, const CDView& cd, uint32_t i,
-                                                           const float4 fA, const SearchBox& b, float lim2, float rfA,
-                                                           uint2 clump, Visit visit) {
+template <bool kPacked, typename Visit>
+__device__ __forceinline__ void for_each_forward_candidate(const SimConsts& k, const SearchGrid& g, const CDView& cd,
+                                                           uint32_t i, const float4 fA, const SearchBox& b, float lim2,
+                                                           float rfA, uint2 clump, Visit visit) {
     constexpr uint32_t U = DEME_FIND_UNROLL;
     // Rows in order: i's own row (from i + 1), the rest of its z layer, then the later layers.  The next row's
     // bounds are fetched before the current row is tested, and each row's candidates are loaded U at a time, so
     // several loads are in flight per lane.
     uint32_t cy = b.cy, cz = b.cz;
     uint32_t j0 = i + 1u;
-    uint32_t j1 = __ldg(cd.cellStart + k.gx * (cy + k.gy * cz) + b.x1 + 1);
+    const uint32_t* cellStart = kPacked ? cd.cellStart + g.base : cd.cellStart;
+    uint32_t j1 = __ldg(cellStart + g.gx * (cy + g.gy * cz) + b.x1 + 1);
     while (true) {
         uint32_t ny = cy + 1u, nz = cz;
         if (ny > b.y1) {
@@ -330,9 +354,9 @@ __device__ __forceinline__ void for_each_forward_candidate(const SimConsts& k, c
         const bool more = nz <= b.z1;
         uint32_t nj0 = 0, nj1 = 0;
         if (more) {
-            const uint32_t rowBase = k.gx * (ny + k.gy * nz);
-            nj0 = __ldg(cd.cellStart + rowBase + b.x0);
-            nj1 = __ldg(cd.cellStart + rowBase + b.x1 + 1);
+            const uint32_t rowBase = g.gx * (ny + g.gy * nz);
+            nj0 = __ldg(cellStart + rowBase + b.x0);
+            nj1 = __ldg(cellStart + rowBase + b.x1 + 1);
         }
         if (!index_ok(k.err, 2, j1, (uint64_t)k.n_spheres + 1)) j1 = j0;
         for (uint32_t j = j0; j < j1; j += U) {
@@ -362,8 +386,8 @@ __device__ __forceinline__ void for_each_forward_candidate(const SimConsts& k, c
     }
 }
 
-__device__ __forceinline__ float prefilter_lim2(const SimConsts& k, float rf) {
-    const float lim = (rf + k.r_max_cd) * 1.00001f + k.prefilter_abs;
+__device__ __forceinline__ float prefilter_lim2(const SimConsts& k, const SearchGrid& g, float rf) {
+    const float lim = (rf + g.r_max_cd) * 1.00001f + k.prefilter_abs;
     return lim * lim;
 }
 
@@ -393,103 +417,139 @@ __device__ __forceinline__ uint32_t pool_owner(const uint32_t* pre, uint32_t p) 
 #ifndef DEME_FIND_RESIDENT_WARPS
 #define DEME_FIND_RESIDENT_WARPS 48
 #endif
-template <uint32_t kWarps, uint32_t kSlots>
+// kPersistent: a grid of a few blocks per SM that take tiles of kWarps * 32 consecutive cell-order spheres from a
+// work counter (counters[2]) until none is left, instead of one block per tile: tiles of dense cells cost more, and
+// the queue spreads them over the SMs as they free up.
+template <uint32_t kWarps, uint32_t kSlots, bool kPersistent, bool kPacked>
 __global__ void __launch_bounds__(kWarps * 32, DEME_FIND_RESIDENT_WARPS / kWarps)
     k_pair_find(SimConsts k, StateView s, CDView cd, uint32_t tempCap) {
     __shared__ uint32_t s_pre[kWarps][33];           // survivor prefix over lanes
     __shared__ uint32_t s_surv[kWarps][kSlots][32];  // survivors, [slot][lane]
+    __shared__ uint32_t s_tile;
     const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    bool valid = i < k.n_spheres;
-    uint32_t nSurv = 0;
-    if (valid) {
-        const float4 fA = __ldg(cd.posFSorted + i);
-        SphRec me;
-        load_near(cd, i, me);
-        me.id = __float_as_uint(fA.w) & k.id_mask;
-        if (!index_ok(k.err, 12, me.id, k.n_spheres)) {
-            valid = false;
-        } else {
-            const SearchBox b = search_box(k, me.x, me.y, me.z, me.rf);
-            for_each_forward_candidate(k, cd, i, fA, b, prefilter_lim2(k, me.rf), me.rf, __ldg(cd.sClump + me.id),
-                                       [&](uint32_t j) {
-                if (nSurv < kSlots) s_surv[w][nSurv][lane] = j;
-                nSurv++;
-            });
+    uint32_t tile = blockIdx.x;
+    while (true) {
+        if (kPersistent) {
+            __syncthreads();  // every warp is done with the previous tile's shared slots
+            if (threadIdx.x == 0) s_tile = atomicAdd(&cd.counters[2], 1u);
+            __syncthreads();
+            tile = s_tile;
+            if ((uint64_t)tile * blockDim.x >= k.n_spheres) return;
         }
-    }
-    const bool ovf = valid && nSurv > kSlots;
-    const uint32_t pool = (valid && !ovf) ? nSurv : 0u;
-    uint32_t incl = pool;
+        const uint32_t i = tile * blockDim.x + threadIdx.x;
+        bool valid = i < k.n_spheres;
+        uint32_t nSurv = 0;
+        if (valid) {
+            const float4 fA = __ldg(cd.posFSorted + i);
+            SphRec me;
+            load_near(cd, i, me);
+            me.id = __float_as_uint(fA.w) & k.id_mask;
+            if (!index_ok(k.err, 12, me.id, k.n_spheres)) {
+                valid = false;
+            } else {
+                SearchGrid tmp;
+                const SearchGrid& g = grid_of<kPacked>(k, me.owner, tmp);
+                const SearchBox b = search_box<kPacked>(k, g, me.x, me.y, me.z, me.rf);
+                for_each_forward_candidate<kPacked>(k, g, cd, i, fA, b, prefilter_lim2(k, g, me.rf), me.rf,
+                                           __ldg(cd.sClump + me.id), [&](uint32_t j) {
+                    if (nSurv < kSlots) s_surv[w][nSurv][lane] = j;
+                    nSurv++;
+                });
+            }
+        }
+        const bool ovf = valid && nSurv > kSlots;
+        const uint32_t pool = (valid && !ovf) ? nSurv : 0u;
+        uint32_t incl = pool;
 #pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
-        if (lane >= (uint32_t)off) incl += y;
-    }
-    const uint32_t totalSurv = __shfl_sync(0xffffffffu, incl, 31);
-    s_pre[w][lane + 1] = incl;
-    if (lane == 0) s_pre[w][0] = 0;
-    __syncwarp();
-    uint32_t base = 0;
-    if (lane == 0 && totalSurv) base = atomicAdd(&cd.counters[0], totalSurv);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    const uint32_t iWarp = i - lane;
-    for (uint32_t p = lane; p < totalSurv; p += 32) {
-        const uint32_t L = pool_owner(s_pre[w], p);
-        if (base + p < tempCap) cd.candTemp[base + p] = make_uint2(iWarp + L, s_surv[w][p - s_pre[w][L]][L]);
-    }
-    if (ovf) {
-        const uint32_t o = atomicAdd(&cd.counters[1], 1u);
-        cd.ovf[o] = i;  // cell-order index; k_pair_overflow searches it again
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= (uint32_t)off) incl += y;
+        }
+        const uint32_t totalSurv = __shfl_sync(0xffffffffu, incl, 31);
+        s_pre[w][lane + 1] = incl;
+        if (lane == 0) s_pre[w][0] = 0;
+        __syncwarp();
+        uint32_t base = 0;
+        if (lane == 0 && totalSurv) base = atomicAdd(&cd.counters[0], totalSurv);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        const uint32_t iWarp = i - lane;
+        for (uint32_t p = lane; p < totalSurv; p += 32) {
+            const uint32_t L = pool_owner(s_pre[w], p);
+            if (base + p < tempCap) cd.candTemp[base + p] = make_uint2(iWarp + L, s_surv[w][p - s_pre[w][L]][L]);
+        }
+        if (ovf) {
+            const uint32_t o = atomicAdd(&cd.counters[1], 1u);
+            cd.ovf[o] = i;  // cell-order index; k_pair_overflow searches it again
+        }
+        if (!kPersistent) return;
     }
 }
 
 namespace {
 struct FindShape {
     uint32_t warps, slots;
+    bool persistent;
 };
-// the last shape holds only two survivors per lane, so most spheres go through k_pair_overflow (it keeps that path
-// covered by the shape-equivalence tests; the autotuner rarely keeps it)
-constexpr FindShape kFindShapes[] = {{4, 16}, {2, 16}, {8, 16}, {4, 8}, {4, 24}, {4, 2}};
+// the sixth shape holds only two survivors per lane, so most spheres go through k_pair_overflow (it keeps that path
+// covered by the shape-equivalence tests; the autotuner rarely keeps it); the last two take their tiles from a work
+// queue (persistent blocks)
+constexpr FindShape kFindShapes[] = {{4, 16, false}, {2, 16, false}, {8, 16, false}, {4, 8, false},
+                                     {4, 24, false}, {4, 2, false},  {4, 16, true},  {8, 16, true}};
 constexpr int kNumFindShapes = sizeof(kFindShapes) / sizeof(kFindShapes[0]);
+
+int sm_count() {
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    }
+    return n;
+}
+
+template <uint32_t kWarps, uint32_t kSlots, bool kPersistent>
+void launch_find(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st) {
+    const uint32_t threads = kWarps * 32;
+    const uint32_t tiles = blocks_for(k.n_spheres, threads);
+    // persistent: as many blocks as stay resident (the kernel's launch bounds), at most one per tile
+    const uint32_t grid = kPersistent ? std::min<uint32_t>(tiles, (uint32_t)sm_count() * (DEME_FIND_RESIDENT_WARPS /
+                                                                                           kWarps))
+                                      : tiles;
+    if (k.ownerScene)
+        k_pair_find<kWarps, kSlots, kPersistent, true><<<grid, threads, 0, st>>>(k, s, cd, tempCap);
+    else
+        k_pair_find<kWarps, kSlots, kPersistent, false><<<grid, threads, 0, st>>>(k, s, cd, tempCap);
+}
 }  // namespace
 
 int find_shape_count() { return kNumFindShapes; }
-void find_shape(int v, uint32_t* warps, uint32_t* slots) {
+void find_shape(int v, uint32_t* warps, uint32_t* slots, bool* persistent) {
     const FindShape f = kFindShapes[(v >= 0 && v < kNumFindShapes) ? v : 0];
     *warps = f.warps;
     *slots = f.slots;
+    if (persistent) *persistent = f.persistent;
 }
 
 void launch_pair_find(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, int shape,
                       cudaStream_t st) {
     if (!(k.n_spheres)) return;
     ProfScope prof_(KID_PAIR_COUNT, st);
-    const uint32_t n = k.n_spheres;
     switch (shape) {
-        case 1:
-            k_pair_find<2, 16><<<blocks_for(n, 64), 64, 0, st>>>(k, s, cd, tempCap);
-            break;
-        case 2:
-            k_pair_find<8, 16><<<blocks_for(n, 256), 256, 0, st>>>(k, s, cd, tempCap);
-            break;
-        case 3:
-            k_pair_find<4, 8><<<blocks_for(n, 128), 128, 0, st>>>(k, s, cd, tempCap);
-            break;
-        case 4:
-            k_pair_find<4, 24><<<blocks_for(n, 128), 128, 0, st>>>(k, s, cd, tempCap);
-            break;
-        case 5:
-            k_pair_find<4, 2><<<blocks_for(n, 128), 128, 0, st>>>(k, s, cd, tempCap);
-            break;
-        default:
-            k_pair_find<4, 16><<<blocks_for(n, 128), 128, 0, st>>>(k, s, cd, tempCap);
+        case 1: launch_find<2, 16, false>(k, s, cd, tempCap, st); break;
+        case 2: launch_find<8, 16, false>(k, s, cd, tempCap, st); break;
+        case 3: launch_find<4, 8, false>(k, s, cd, tempCap, st); break;
+        case 4: launch_find<4, 24, false>(k, s, cd, tempCap, st); break;
+        case 5: launch_find<4, 2, false>(k, s, cd, tempCap, st); break;
+        case 6: launch_find<4, 16, true>(k, s, cd, tempCap, st); break;
+        case 7: launch_find<8, 16, true>(k, s, cd, tempCap, st); break;
+        default: launch_find<4, 16, false>(k, s, cd, tempCap, st);
     }
 }
 
 // Spheres whose survivors k_pair_find could not hold: the same forward-half search, one thread per sphere, each
 // survivor appended to the pair pool for k_pair_exact.  Grid-stride over the device-side overflow count (no host
 // round trip).
+template <bool kPacked>
 __global__ void __launch_bounds__(128) k_pair_overflow(SimConsts k, StateView s, CDView cd, uint32_t tempCap) {
     const uint32_t nOvf = *((volatile uint32_t*)&cd.counters[1]);
     for (uint32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < nOvf; o += gridDim.x * blockDim.x) {
@@ -500,8 +560,11 @@ __global__ void __launch_bounds__(128) k_pair_overflow(SimConsts k, StateView s,
         load_near(cd, i, me);
         me.id = __float_as_uint(fA.w) & k.id_mask;
         if (!index_ok(k.err, 12, me.id, k.n_spheres)) continue;
-        const SearchBox b = search_box(k, me.x, me.y, me.z, me.rf);
-        for_each_forward_candidate(k, cd, i, fA, b, prefilter_lim2(k, me.rf), me.rf, __ldg(cd.sClump + me.id),
+        SearchGrid tmp;
+        const SearchGrid& g = grid_of<kPacked>(k, me.owner, tmp);
+        const SearchBox b = search_box<kPacked>(k, g, me.x, me.y, me.z, me.rf);
+        for_each_forward_candidate<kPacked>(k, g, cd, i, fA, b, prefilter_lim2(k, g, me.rf), me.rf,
+                                            __ldg(cd.sClump + me.id),
                                    [&](uint32_t j) {
             const uint32_t pos = atomicAdd(&cd.counters[0], 1u);
             if (pos < tempCap) cd.candTemp[pos] = make_uint2(i, j);
@@ -512,7 +575,7 @@ __global__ void __launch_bounds__(128) k_pair_overflow(SimConsts k, StateView s,
 // The reference's pair predicate on every pool entry (cell-order indices of a sphere and its candidate), rewritten
 // in place as the pair (A, B) or kNoPair.  The launch may cover the pool's capacity: it reads the count on the
 // device.  All lanes of a warp reach the end together (no early return), so the count updates stay simple.
-__global__ void __launch_bounds__(256) k_pair_exact(SimConsts k, StateView s, CDView cd, uint32_t tempCap) {
+__global__ void __launch_bounds__(512) k_pair_exact(SimConsts k, StateView s, CDView cd, uint32_t tempCap) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = min(*((volatile uint32_t*)&cd.counters[0]), tempCap);
     if (p >= n) return;
@@ -533,16 +596,20 @@ __global__ void __launch_bounds__(256) k_pair_exact(SimConsts k, StateView s, CD
     cd.candTemp[p] = out;
 }
 
-void launch_pair_exact(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st) {
+void launch_pair_exact(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, uint32_t threads,
+                       cudaStream_t st) {
     if (!(k.n_spheres) || !tempCap) return;
     ProfScope prof_(KID_PAIR_EXACT, st);
-    k_pair_exact<<<blocks_for(tempCap, 256), 256, 0, st>>>(k, s, cd, tempCap);
+    k_pair_exact<<<blocks_for(tempCap, threads), threads, 0, st>>>(k, s, cd, tempCap);
 }
 
 void launch_pair_overflow(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st) {
     if (!(k.n_spheres)) return;
     ProfScope prof_(KID_PAIR_OVERFLOW, st);
-    k_pair_overflow<<<148, 128, 0, st>>>(k, s, cd, tempCap);
+    if (k.ownerScene)
+        k_pair_overflow<true><<<148, 128, 0, st>>>(k, s, cd, tempCap);
+    else
+        k_pair_overflow<false><<<148, 128, 0, st>>>(k, s, cd, tempCap);
 }
 
 // Presets every sphere's contact count to its number of analytical contacts (k_sphere_prep does the same; this is
@@ -727,11 +794,12 @@ void launch_count_by_sphere(const uint32_t* idA, uint32_t n, uint32_t* cnt, cuda
 // The per-block partials of each analytical owner summed in a fixed order (deterministic) into its accumulators,
 // in two kernels so that the whole GPU takes part: block (owner component, chunk) sums the partials of a contiguous
 // range of force blocks with a fixed tree, then one thread per owner component adds its chunk sums in order.
-__global__ void k_anal_reduce(AnalAccum aa, uint32_t nBlocks, const uint32_t* err, const uint32_t* dN) {
+__global__ void k_anal_reduce(AnalAccum aa, uint32_t nBlocks, uint32_t forceThreads, const uint32_t* err,
+                              const uint32_t* dN) {
     __shared__ float sh[256];
     if (__syncthreads_or(threadIdx.x == 0 && *err != 0u)) return;  // a voided step (see k_force)
     // only the force blocks that held contacts wrote partials
-    if (dN) nBlocks = min(nBlocks, (*dN + kForceThreads - 1) / kForceThreads);
+    if (dN) nBlocks = min(nBlocks, (*dN + forceThreads - 1) / forceThreads);
     const uint32_t sc = blockIdx.x, chunk = blockIdx.y;
     const uint32_t slot = sc / 6u, comp = sc % 6u;
     const uint32_t len = (nBlocks + kAnalChunks - 1u) / kAnalChunks;
@@ -756,10 +824,34 @@ __global__ void k_anal_reduce_final(AnalAccum aa, float4* acc, float4* alpha, co
     dst[comp % 3] = v;
 }
 
+namespace {
+struct ForceShape {
+    uint32_t threads, minBlocks;
+};
+constexpr ForceShape kForceShapes[] = {{kForceThreads, kForceMinBlocks}, {256, 4}, {64, 16}};
+constexpr int kNumForceShapes = sizeof(kForceShapes) / sizeof(kForceShapes[0]);
+
+template <uint32_t T, uint32_t B>
+void launch_force_shape(const SimConsts& k, const StateView& s, const ContactView& c, uint32_t n, bool has_hist,
+                        const ContactOutputs* out, const AnalAccum& aa, size_t smem, cudaStream_t st) {
+    const uint32_t nb = blocks_for(n, T);
+    if (out)
+        k_force<true, T, B><<<nb, T, smem, st>>>(k, s, c, n, has_hist, *out, aa);
+    else
+        k_force<false, T, B><<<nb, T, smem, st>>>(k, s, c, n, has_hist, ContactOutputs{}, aa);
+}
+}  // namespace
+
+int force_shape_count() { return kNumForceShapes; }
+uint32_t force_shape_threads(int shape) { return kForceShapes[(shape >= 0 && shape < kNumForceShapes) ? shape : 0].threads; }
+
 void launch_force(const SimConsts& k, const StateView& s, const ContactView& c, uint32_t n, bool has_hist,
-                  const ContactOutputs* out, const AnalAccum& aa, const UserForceKernel* user, cudaStream_t st) {
+                  const ContactOutputs* out, const AnalAccum& aa, const UserForceKernel* user, int shape,
+                  cudaStream_t st) {
     if (!(n)) return;
-    const uint32_t nb = blocks_for(n, kForceThreads);
+    if (user) shape = 0;  // run-time compiled models come in the default shape
+    const uint32_t threads = force_shape_threads(shape);
+    const uint32_t nb = blocks_for(n, threads);
     const bool partials = aa.nAO && !aa.direct;
     const size_t smem = partials ? 6u * aa.nAO * sizeof(float) : 0;
     {
@@ -775,15 +867,17 @@ void launch_force(const SimConsts& k, const StateView& s, const ContactView& c, 
             AnalAccum aaa = aa;
             void* args[] = {&ka, &sa, &ca, &na, &ha, &oa, &aaa};
             cudaLaunchKernel((const void*)user->kern[out ? 1 : 0], dim3(nb), dim3(kForceThreads), args, smem, st);
-        } else if (out) {
-            k_force<true><<<nb, kForceThreads, smem, st>>>(k, s, c, n, has_hist, *out, aa);
+        } else if (shape == 1) {
+            launch_force_shape<256, 4>(k, s, c, n, has_hist, out, aa, smem, st);
+        } else if (shape == 2) {
+            launch_force_shape<64, 16>(k, s, c, n, has_hist, out, aa, smem, st);
         } else {
-            k_force<false><<<nb, kForceThreads, smem, st>>>(k, s, c, n, has_hist, ContactOutputs{}, aa);
+            launch_force_shape<kForceThreads, kForceMinBlocks>(k, s, c, n, has_hist, out, aa, smem, st);
         }
     }
     if (partials) {
         ProfScope prof_(KID_OTHER, st);
-        k_anal_reduce<<<dim3(6u * aa.nAO, kAnalChunks), 256, 0, st>>>(aa, nb, k.err, c.dN);
+        k_anal_reduce<<<dim3(6u * aa.nAO, kAnalChunks), 256, 0, st>>>(aa, nb, threads, k.err, c.dN);
     }
     if (partials) {
         ProfScope prof_(KID_OTHER, st);
@@ -791,7 +885,8 @@ void launch_force(const SimConsts& k, const StateView& s, const ContactView& c, 
     }
 }
 
-uint32_t force_blocks(uint32_t n) { return blocks_for(n, kForceThreads); }
+// the most force blocks any shape launches for n contacts (the wall partials are sized for it)
+uint32_t force_blocks(uint32_t n) { return blocks_for(n, 64); }
 
 // ChangeFamily (src/DEM/APIPublic.cpp:184-208): every owner of family `from` moves to family `to`.
 __global__ void k_change_family(ushort4* loc, uint32_t n, uint32_t from, uint32_t to) {
@@ -851,17 +946,17 @@ void launch_window_done(const uint32_t* err, uint32_t* done, cudaStream_t st) {
 
 // ------------------------------------------------------------------------------------------------------------
 // integrateOwners (src/kernel/DEMIntegrationKernels.cu:46-179) with the constant prescription table.
-__global__ void __launch_bounds__(256) k_integrate(SimConsts k, StateView s) {
+__global__ void __launch_bounds__(512) k_integrate(SimConsts k, StateView s) {
     const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= k.n_owners) return;
     if (*k.err != 0u) return;  // a voided step (see k_force) leaves the state as it was
     integrate_owner(k, s, o, 0.f, TableMotion{s.presc});
 }
 
-void launch_integrate(const SimConsts& k, const StateView& s, cudaStream_t st) {
+void launch_integrate(const SimConsts& k, const StateView& s, uint32_t threads, cudaStream_t st) {
     if (!(k.n_owners)) return;
     ProfScope prof_(KID_INTEGRATE, st);
-    if (k.n_owners) k_integrate<<<blocks_for(k.n_owners, 256), 256, 0, st>>>(k, s);
+    if (k.n_owners) k_integrate<<<blocks_for(k.n_owners, threads), threads, 0, st>>>(k, s);
 }
 
 // Kinetic energy of clump owners: per-owner term of DEMOwnerQueryKernels.cu:10-37, summed in double.

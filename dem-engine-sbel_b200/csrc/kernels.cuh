@@ -103,10 +103,12 @@ void launch_cell_scatter(const SimConsts& k, const StateView& s, const CDView& c
 void launch_gather_sorted(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
 void launch_pair_find(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, int shape,
                       cudaStream_t st);
-int find_shape_count();                                     // block shapes of the candidate scan
-void find_shape(int v, uint32_t* warps, uint32_t* slots);  // warps per block and survivor slots per lane of shape v
+int find_shape_count();  // block shapes of the candidate scan
+// warps per block, survivor slots per lane and work-queue (persistent) form of shape v
+void find_shape(int v, uint32_t* warps, uint32_t* slots, bool* persistent);
 void launch_pair_overflow(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st);
-void launch_pair_exact(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st);
+void launch_pair_exact(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, uint32_t threads,
+                       cudaStream_t st);
 // ranges the wall partials of the force blocks are first summed over (then the range sums, in order)
 constexpr uint32_t kAnalChunks = 32;
 // a pair-pool entry that k_pair_exact rejected
@@ -121,8 +123,11 @@ void launch_history(const SimConsts& k, const ContactView& cur, const ContactVie
 void launch_count_by_sphere(const uint32_t* idA, uint32_t n, uint32_t* cnt, cudaStream_t st);
 struct UserForceKernel;
 void launch_force(const SimConsts& k, const StateView& s, const ContactView& c, uint32_t n, bool has_hist,
-                  const ContactOutputs* out, const AnalAccum& aa, const UserForceKernel* user, cudaStream_t st);
+                  const ContactOutputs* out, const AnalAccum& aa, const UserForceKernel* user, int shape,
+                  cudaStream_t st);
 uint32_t force_blocks(uint32_t n);
+int force_shape_count();                 // block shapes of the force kernel
+uint32_t force_shape_threads(int shape);
 void launch_window_done(const uint32_t* err, uint32_t* done, cudaStream_t st);
 void launch_change_family(ushort4* loc, uint32_t n, uint32_t from, uint32_t to, cudaStream_t st);
 void launch_advance_time(float* time, float h, const uint32_t* err, cudaStream_t st);
@@ -130,7 +135,7 @@ void launch_set_time(float* time, float t, cudaStream_t st);
 // Scenes with at most this many materials keep a table of contact-pair parameters (2 float4 per ordered pair).
 constexpr uint32_t kMaxPairTableMaterials = 256;
 void launch_material_pairs(const MaterialTable& m, uint32_t nM, float4* out, cudaStream_t st);
-void launch_integrate(const SimConsts& k, const StateView& s, cudaStream_t st);
+void launch_integrate(const SimConsts& k, const StateView& s, uint32_t threads, cudaStream_t st);
 void launch_kinetic_energy(const SimConsts& k, const StateView& s, uint32_t n_clumps, double* out, cudaStream_t st);
 
 // Reference bin assignment (parity path).

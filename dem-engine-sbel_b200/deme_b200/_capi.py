@@ -155,6 +155,8 @@ SCENE_EXTENSIONS = [
     ("anal_material_wide", np.uint16, "a"),
     ("owner_anal_first", np.uint32, "o"),
     ("owner_anal_count", np.uint32, "o"),
+    ("owner_scene", np.uint32, "o"),
+    ("scene_box", np.float32, None),  # 6 per scene
 ]
 
 
@@ -244,10 +246,10 @@ def make_scene_struct(arrays: dict, counts: dict, prescriptions) -> tuple[Scene,
         if arrays.get(name) is None:
             continue
         a = np.ascontiguousarray(arrays[name], dtype=dt)
-        if a.shape[0] != counts[key]:
+        if key is not None and a.shape[0] != counts[key]:
             raise ValueError(f"scene array {name} has {a.shape[0]} entries, expected {counts[key]}")
         keep.append(a)
-        setattr(s, name, ptr(a) if counts[key] > 0 else None)
+        setattr(s, name, ptr(a) if a.size > 0 else None)
     return s, keep
 
 
@@ -267,7 +269,8 @@ class Tuning(C.Structure):
     """deme_tuning: the search shape deme_autotune chose."""
     _fields_ = [("shape", C.c_int32), ("find_warps", C.c_int32), ("find_slots", C.c_int32),
                 ("cell_factor", C.c_float), ("ms_per_step", C.c_float), ("ms_per_step_default", C.c_float),
-                ("trials", C.c_int32)]
+                ("trials", C.c_int32), ("find_persistent", C.c_int32), ("force_shape", C.c_int32),
+                ("force_threads", C.c_int32), ("exact_threads", C.c_int32), ("integrate_threads", C.c_int32)]
 
 
 def bind(lib: C.CDLL, prefix: str):

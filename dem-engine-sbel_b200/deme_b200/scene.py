@@ -76,6 +76,13 @@ class ClumpBatch:
         self.families = np.zeros(n, np.uint32)
         self.family_is_specified = False
         self.analytical_objects = None  # packed scenes: the external objects these clumps may touch
+        self.scene_box = None  # packed scenes: (lower, upper) corner of this batch's own search grid
+
+    def SetSceneBox(self, lower, upper):
+        """Packed independent scenes (no reference counterpart): this batch is a scene of its own whose spheres stay
+        inside the box [lower, upper] (user coordinates); it gets a contact-search grid of its own, with cells
+        sized by its own spheres.  Either every batch of a scene builder has a box or none has."""
+        self.scene_box = (np.asarray(lower, np.float64), np.asarray(upper, np.float64))
 
     def SetAnalyticalObjects(self, objs):
         """Packed independent scenes (no reference counterpart): the spheres of this batch meet only the analytical
@@ -597,6 +604,20 @@ class SceneBuilder:
         anal["anal_material"] = (anal["anal_material"] & 0xFF).astype(np.uint8)
         if owner_anal is not None:
             ext_arrays["owner_anal_first"], ext_arrays["owner_anal_count"] = owner_anal
+        boxed = [b.scene_box is not None for b in self.batches]
+        if any(boxed):
+            if not all(boxed):
+                raise ValueError("SetSceneBox: either every clump batch has a scene box or none has")
+            owner_scene = np.zeros(nO, np.uint32)
+            boxes = np.zeros((len(self.batches), 6), f32)
+            o0 = 0
+            for i, b in enumerate(self.batches):
+                owner_scene[o0:o0 + b.GetNumClumps()] = i
+                o0 += b.GetNumClumps()
+                boxes[i, :3] = b.scene_box[0] - lbf
+                boxes[i, 3:] = b.scene_box[1] - lbf
+            ext_arrays["owner_scene"] = owner_scene
+            ext_arrays["scene_box"] = boxes.ravel()
         arrays = dict(voxel=vox, locX=lx, locY=ly, locZ=lz, oriQw=oriQw, oriQx=oriQx, oriQy=oriQy, oriQz=oriQz,
                       vX=vX, vY=vY, vZ=vZ, omgX=wX, omgY=wY, omgZ=wZ, family=family, mass=mass,
                       mmiXX=np.ascontiguousarray(moi[:, 0]), mmiYY=np.ascontiguousarray(moi[:, 1]),

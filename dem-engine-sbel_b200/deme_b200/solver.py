@@ -341,6 +341,12 @@ class Solver(HandleSolver):
         self.lib.deme_set_search_shape.argtypes = [C.c_void_p, C.c_int32, C.c_float]
         self._check(self.lib.deme_set_search_shape(self.h, int(shape), float(cell_factor)), "set_search_shape")
 
+    def set_kernel_shapes(self, force_shape: int = 0, exact_threads: int = 256, integrate_threads: int = 256):
+        """Block shapes of the force kernel, the exact pair test and the integration (see deme_set_kernel_shapes)."""
+        self.lib.deme_set_kernel_shapes.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]
+        self._check(self.lib.deme_set_kernel_shapes(self.h, int(force_shape), int(exact_threads),
+                                                    int(integrate_threads)), "set_kernel_shapes")
+
     def autotune(self, steps_per_trial: int = 5) -> dict:
         """Times every search shape and keeps the fastest; the state is left as it was (see deme_autotune)."""
         t = capi.Tuning()

@@ -634,8 +634,9 @@ def batched_settling(specs, dt: float = 1e-5):
     first = 0
     for i, sp in enumerate(specs):
         lbf = (0.01 + (i % per) * slot, 0.01 + ((i // per) % per) * slot, 0.01 + (i // (per * per)) * slot)
-        b, box, _ = _add_settling_scene(s, sp, lbf)
+        b, box, H = _add_settling_scene(s, sp, lbf)
         b.SetAnalyticalObjects([box])
+        b.SetSceneBox(lbf, (lbf[0] + sp["side"], lbf[1] + sp["side"], lbf[2] + H))
         ranges.append((first, sp["n"]))
         first += sp["n"]
     s.SetInitTimeStep(dt)

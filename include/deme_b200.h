@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define DEME_B200_ABI_VERSION 2
+#define DEME_B200_ABI_VERSION 3
 
 /* Status codes (the reference throws std::runtime_error instead: src/DEM/Structs.h:129-141, src/core/utils/GpuError.h:13-27). */
 typedef enum {
@@ -173,6 +173,10 @@ typedef struct {
     const uint16_t* anal_material_wide;    /* per component, replaces anal_material */
     const uint32_t* owner_anal_first;      /* per owner: its spheres meet only the analytical components */
     const uint32_t* owner_anal_count;      /*   [first, first + count) (then n_anal may exceed 255) */
+    const uint32_t* owner_scene;           /* per owner: the scene it belongs to (0 .. n_scenes - 1); each scene gets
+                                              a search grid of its own, sized by its own spheres */
+    const float* scene_box;                /* n_scenes x 6: lower and upper corner of each scene's search grid,
+                                              relative to the domain's lower corner (NULL: from the initial poses) */
 } deme_scene;
 
 /* Mutable owner state (download/upload).  Any pointer may be NULL to skip that array. */
@@ -333,24 +337,36 @@ int32_t deme_graph_stats(deme_handle* h, int64_t* replays, int64_t* rollbacks);
 
 /* Search shape (no reference counterpart: the reference's bin size, SetInitBinSize, sets both its bins and its
  * work per thread).  `shape` picks a block shape of the candidate scan (index < deme_search_shape_count();
- * 0, the default, is 4 warps with 16 survivor slots per lane) and `cell_factor` in [1, 4] scales the search cells
- * (edge cell_factor x max(bin size, largest expanded diameter)).  Every shape finds the same contacts. */
+ * 0, the default, is 4 warps with 16 survivor slots per lane; the last two take their tiles of spheres from a work
+ * queue, with a few persistent blocks per SM) and `cell_factor` in [1, 4] scales the search cells (edge
+ * cell_factor x max(bin size, the scene's largest expanded diameter)).  Every shape finds the same contacts. */
 int32_t deme_set_search_shape(deme_handle* h, int32_t shape, float cell_factor);
 int32_t deme_search_shape_count(void);
+/* Block shapes of the other per-step kernels (no reference counterpart): `force_shape` < deme_force_shape_count()
+ * (0, the default: 128 threads, 8 blocks per SM; 1: 256 x 4; 2: 64 x 16), and the threads per block of the exact
+ * pair test and of the integration (32 to 512, multiples of 32; 256 by default).  They change speed only. */
+int32_t deme_set_kernel_shapes(deme_handle* h, int32_t force_shape, int32_t exact_threads, int32_t integrate_threads);
+int32_t deme_force_shape_count(void);
 
 typedef struct {
     int32_t shape;         /* index passed to deme_set_search_shape */
     int32_t find_warps;    /* warps per block of the candidate scan */
     int32_t find_slots;    /* survivor slots per lane */
     float cell_factor;
-    float ms_per_step;     /* the chosen shape's time per step in the trials */
+    float ms_per_step;     /* the chosen shapes' time per step in the trials */
     float ms_per_step_default;
     int32_t trials;
+    int32_t find_persistent;    /* the candidate scan takes its tiles from a work queue */
+    int32_t force_shape;        /* arguments of deme_set_kernel_shapes */
+    int32_t force_threads;
+    int32_t exact_threads;
+    int32_t integrate_threads;
 } deme_tuning;
 
-/* Autotuner: times every search shape with cell factors 1, 1.25 and 1.5 on `steps_per_trial` steps (5 when <= 0)
- * from the current state, keeps the fastest, and restores the state and contact history, so the run continues as
- * if it had not been called.  `out` may be NULL. */
+/* Autotuner: times every search shape with cell factors 1, 1.25 and 1.5, then (with the best of those) every force
+ * shape, then 128, 256 and 512 threads per block for the exact pair test and for the integration, each trial on
+ * `steps_per_trial` steps (5 when <= 0) from the current state; keeps the fastest, and restores the state and
+ * contact history, so the run continues as if it had not been called.  `out` may be NULL. */
 int32_t deme_autotune(deme_handle* h, int32_t steps_per_trial, deme_tuning* out);
 
 /* Change one family's prescription between steps (the constant-valued form of SetFamilyPrescribedLinVel /
