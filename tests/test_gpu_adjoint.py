@@ -202,3 +202,62 @@ def test_column_collapse_windows_match_host_adjoint_on_the_gpu_trajectory():
     print(f"column collapse, 20 windows of 100 steps: largest material-gradient difference (E, CoR, mu, Crr) "
           f"{worst.round(5)} of the window's largest, position gradient {worst_x:.2e}; Crr summed difference "
           f"{crr_diff / max(crr_host, 1e-300):.3f} of the summed host gradients, ratios {r.round(3)}")
+
+
+def _fd_material(sc, x0, v0, w0, T, loss_of, rel=1e-3):
+    """Central differences of the FP64 forward at relative step `rel` for material 0's E, CoR, mu, Crr."""
+    out = np.zeros(4)
+    for j, field in enumerate(("E", "CoR", "mu", "Crr")):
+        base = float(getattr(sc, field)[0])
+        if base == 0.0:
+            continue
+        vals = []
+        for sgn in (1.0, -1.0):
+            sc2 = A.SphereScene(**{k: getattr(sc, k) for k in sc.__dataclass_fields__})
+            arr = getattr(sc2, field).copy()
+            arr[0] = base * (1.0 + sgn * rel)
+            setattr(sc2, field, arr)
+            (xf, _, _), _ = A.rollout(sc2, x0, v0, w0, T)
+            vals.append(loss_of(xf))
+        out[j] = (vals[0] - vals[1]) / (2.0 * rel * base)
+    return out
+
+
+@pytest.mark.parametrize("T,bars", [(300, {"E": 1e-3, "CoR": 1e-3}), (1000, {"CoR": 2e-3})])
+def test_reduced_column_collapse_against_fd_of_fp64_forward(T, bars):
+    """The column-collapse loss (mean squared runout plus the heap-angle proxy) of a reduced collapse, 60 spheres of
+    2-3 mm released onto the floor, checkpoints every 100 steps, exact derivatives (floors 0) on both sides: the
+    CUDA adjoint's material gradients against central differences of the FP64 forward at relative step 1e-3.
+    Over the first 300 steps (fall and first impact) the E and CoR gradients agree within 1e-3; over 1000 steps
+    (the heap forms) the CoR gradient still does, while E and Crr come from contacts that open and close and from
+    rolling torques that flip direction, where the loss is not smooth at the scale of a 1e-3 parameter step (the
+    differences at 1e-3 and 1e-4 disagree with each other); those are printed.  Friction is not yet loaded over
+    these windows (its gradient is 0 on both sides)."""
+    from deme_b200 import Solver, adjoint
+    built = workloads.column_collapse(n=60)
+    n = built.counts["s"]
+    g = Solver(built)
+    adjoint.set_floors(g, 0.0, 0.0, 0.0)
+    saved = dict(A.REG)
+    A.REG.update(delta_rel=0.0, roll_speed=0.0, ft=0.0)
+    try:
+        sc, x0, v0, w0 = A.from_built(built)
+        axis, z0 = x0[:, :2].mean(0), float(x0[:, 2].min())
+        adjoint.record(g, T, 100)
+        st = g.state()
+        xf = built.decode_positions(st)[:n]
+        _, gpos = workloads.collapse_loss(xf, axis, z0)
+        seed = np.zeros((built.counts["o"], 3))
+        seed[:n] = gpos
+        gg = adjoint.backward(g, d_pos=seed)["d_material"][0]
+        fd = _fd_material(sc, x0, v0, w0, T, lambda x: workloads.collapse_loss(x, axis, z0)[0])
+    finally:
+        A.REG.update(saved)
+    names = ("E", "CoR", "mu", "Crr")
+    err = {nm: abs(gg[j] - fd[j]) / max(abs(fd[j]), 1e-300) for j, nm in enumerate(names)}
+    print(f"reduced collapse, {T} steps: CUDA adjoint {gg}, FD of the FP64 forward {fd}, relative differences "
+          f"{ {k: round(v, 6) for k, v in err.items()} }")
+    for nm, bar in bars.items():
+        assert err[nm] <= bar, (nm, err[nm], gg, fd)
+    if fd[2] == 0.0:  # no contact reached its Coulomb cap
+        assert abs(gg[2]) <= 1e-9 * np.abs(gg).max(), gg
