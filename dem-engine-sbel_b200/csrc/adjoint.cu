@@ -1,27 +1,35 @@
-// adjoint.cu -- adjoint of the DEM step for scenes of single spheres with plane walls (no reference counterpart).
+// adjoint.cu -- adjoint of the DEM step for clumps and spheres with analytical walls (no reference counterpart).
 //
 // deme_adjoint_record runs the forward steps and keeps a checkpoint (owner state and the current contact list with
 // its history) every K steps.  deme_adjoint_backward walks the checkpoints from the last: it restores one,
-// recomputes its K steps with the production kernels while recording each step's state and contact list, then
-// runs the reverse pass over those steps.  Per step the contact set is the one the forward pass found, held fixed.
-// The reverse pass is
-//   * k_adj_integrate: the Extended Taylor update x' = x + h v + h^2/2 a, v' = v + h a, w' = w + h alpha
-//     (src/kernel/DEMIntegrationKernels.cu:46-179) reversed per owner, which turns the state gradients into the
-//     gradients of the owner's summed force and torque;
-//   * k_adj_contact: per contact, the derivative of the built-in frictional Hertz-Mindlin law (adjoint_law.cuh)
-//     and of its geometry, scattered onto both owners' position, velocity and angular-velocity gradients, the
-//     gradient of the incoming history, and the material-parameter gradients (FP64 accumulators);
+// recomputes its K steps with the production kernels while recording each step's state, angular accelerations and
+// contact list, then runs the reverse pass over those steps.  Per step the contact set is the one the forward pass
+// found, held fixed.  The reverse pass is
+//   * k_adj_integrate: the Extended Taylor update (src/kernel/DEMIntegrationKernels.cu:46-179) reversed per owner:
+//     x' = x + h v + h^2/2 a, v' = v + h a with a = F/m + g; w' = w + h alpha and q' = q (x) exp(h (w + h alpha/2))
+//     with alpha = T / I from the owner-frame torque T (forceToAngAcc, src/kernel/DEMCollectForceKernels.cu:68-120).
+//     It turns the state gradients into the gradients of the owner's summed force and owner-frame torque, and
+//     gives the direct part of the step-start state gradients (orientation included);
+//   * k_adj_contact: per contact, the derivative of the built-in frictional Hertz-Mindlin law (adjoint_law.cuh) and
+//     of its geometry -- sphere centres X + R(q) r of clump members, the wall geometry of planes, cylinders and
+//     cones (adjoint_rigid.cuh), lever arms and their owner-frame images, contact-point velocities R(q) (w x s),
+//     owner-frame torques -- scattered onto both owners' position, velocity, quaternion and angular-velocity
+//     gradients, the gradient of the incoming history, and the
+//     material-parameter gradients (FP64 accumulators);
 //   * k_adj_hist_scatter: the history map (src/kernel/DEMHistoryMappingKernels.cu) reversed, so the incoming-history
 //     gradient reaches the previous step's updated history.
-// Angular velocities are differentiated in the world frame, where an isotropic sphere's orientation does not enter
-// the contact law.  The model is evaluated from the recorded FP32 state; the state gradients are carried and
-// accumulated in FP64 (they sum many contributions of both signs), as are the material-parameter gradients.
+// The state carried is the stored one: position, velocity, quaternion and owner-frame angular velocity.  At the
+// interface angular velocities are in the world frame and quaternion gradients hold the world angular velocity
+// fixed (k_adj_seed, k_adj_result).  Owners of prescribed families are driven: their recorded motion enters the
+// contacts, and their gradients are 0.  The model is evaluated from the recorded FP32 state (sphere centres and
+// wall placements formed as the forward step forms them); the state gradients are carried and accumulated in FP64
+// (they sum many contributions of both signs), as are the material-parameter gradients.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
 
-#include "adjoint_law.cuh"
+#include "adjoint_rigid.cuh"
 #include "handle.cuh"
 #include "profiler.cuh"
 
@@ -35,9 +43,11 @@ struct AdjointTape {
     std::vector<Checkpoint> cps;  // cps[j]: state before step j*K
     Checkpoint fin;               // state after the last step
     // one segment of recorded steps
-    double* X = nullptr;  // K x nO x 3 positions (world, relative to the domain corner)
-    float4* V = nullptr;  // K x nO velocities
-    float4* W = nullptr;  // K x nO angular velocities (world frame)
+    double* X = nullptr;   // K x nO x 3 positions (world, relative to the domain corner)
+    float4* V = nullptr;   // K x nO velocities
+    float4* Q = nullptr;   // K x nO quaternions
+    float4* W = nullptr;   // K x nO angular velocities (owner frame)
+    float4* Al = nullptr;  // K x nO angular accelerations (owner frame) of the step's forces
     uint32_t poolCap = 0;
     uint32_t* cA = nullptr;
     uint32_t* cB = nullptr;
@@ -45,8 +55,9 @@ struct AdjointTape {
     float4* cH = nullptr;
     uint32_t* cM = nullptr;
     std::vector<uint32_t> stepN, stepBase;
-    // reverse-pass buffers
-    double *lx = nullptr, *lv = nullptr, *lw = nullptr, *nlx = nullptr, *nlv = nullptr, *nlw = nullptr;  // 3 per owner
+    // reverse-pass buffers: 3 per owner, 4 for the quaternions
+    double *lx = nullptr, *lv = nullptr, *lw = nullptr, *nlx = nullptr, *nlv = nullptr, *nlw = nullptr;
+    double *lq = nullptr, *nlq = nullptr;
     double *lF = nullptr, *lT = nullptr;
     uint32_t gCap = 0;
     float4 *gA = nullptr, *gB = nullptr, *gC = nullptr;  // history gradients (current, previous, carried)
@@ -58,8 +69,10 @@ namespace {
 
 inline unsigned nblk(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
 
-// State of every owner at a step start: position (double, kernel literals), velocity, world-frame angular velocity.
-__global__ void k_adj_record_state(SimConsts k, StateView s, uint32_t nO, double* X, float4* V, float4* W) {
+// State of every owner at a step start: position (double, kernel literals), velocity, quaternion, owner-frame
+// angular velocity.
+__global__ void k_adj_record_state(SimConsts k, StateView s, uint32_t nO, double* X, float4* V, float4* Q,
+                                   float4* W) {
     const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= nO) return;
     const ushort4 l = s.loc[o];
@@ -69,35 +82,13 @@ __global__ void k_adj_record_state(SimConsts k, StateView s, uint32_t nO, double
     X[3 * (size_t)o + 1] = y;
     X[3 * (size_t)o + 2] = z;
     V[o] = s.vel[o];
-    const float4 q = s.quat[o];
-    float4 w = s.omg[o];
-    rot_f(w.x, w.y, w.z, q.x, q.y, q.z, q.w);
-    W[o] = w;
+    Q[o] = s.quat[o];
+    W[o] = s.omg[o];
 }
 
+// Free owners are the clumps of families without a prescription; the scene check admits no partly prescribed one.
 __device__ __forceinline__ bool owner_free(const StateView& s, uint32_t o, uint32_t nClumps) {
     return o < nClumps && !s.presc[s.loc[o].w].used;
-}
-
-// Reverse of x' = x + h v + h^2/2 a, v' = v + h a, w' = w + h alpha (a = F/m + g, alpha = T/I): the gradients of
-// the owner's summed force and torque, and the direct part of the step-start state gradients.
-__global__ void k_adj_integrate(StateView s, uint32_t nO, uint32_t nClumps, double h, const double* lx,
-                                const double* lv, const double* lw, double* lF, double* lT, double* nlx, double* nlv,
-                                double* nlw) {
-    const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= nO) return;
-    const bool f = owner_free(s, o, nClumps);
-    const double m = s.vel[o].w, I = s.moi[o].x;
-    const double c = 0.5 * h * h;
-    for (int a = 0; a < 3; a++) {
-        const size_t q = 3 * (size_t)o + a;
-        const double x = lx[q], v = lv[q], w = lw[q];
-        lF[q] = f ? (c * x + h * v) / m : 0.0;
-        lT[q] = f ? h * w / I : 0.0;
-        nlx[q] = f ? x : 0.0;
-        nlv[q] = f ? v + h * x : 0.0;
-        nlw[q] = f ? w : 0.0;
-    }
 }
 
 __device__ __forceinline__ void add3(double* a, uint32_t o, dv3 g) {
@@ -105,8 +96,112 @@ __device__ __forceinline__ void add3(double* a, uint32_t o, dv3 g) {
     atomicAdd(a + 3 * (size_t)o + 1, g.y);
     atomicAdd(a + 3 * (size_t)o + 2, g.z);
 }
+__device__ __forceinline__ void add4(double* a, uint32_t o, const dq4& g) {
+    atomicAdd(a + 4 * (size_t)o, g.w);
+    atomicAdd(a + 4 * (size_t)o + 1, g.u.x);
+    atomicAdd(a + 4 * (size_t)o + 2, g.u.y);
+    atomicAdd(a + 4 * (size_t)o + 3, g.u.z);
+}
 __device__ __forceinline__ dv3 ld3(const double* a, uint32_t o) {
     return mk(a[3 * (size_t)o], a[3 * (size_t)o + 1], a[3 * (size_t)o + 2]);
+}
+__device__ __forceinline__ dq4 ld4(const double* a, uint32_t o) {
+    return dq4{a[4 * (size_t)o], mk(a[4 * (size_t)o + 1], a[4 * (size_t)o + 2], a[4 * (size_t)o + 3])};
+}
+__device__ __forceinline__ void st3(double* a, uint32_t o, dv3 g) {
+    a[3 * (size_t)o] = g.x;
+    a[3 * (size_t)o + 1] = g.y;
+    a[3 * (size_t)o + 2] = g.z;
+}
+__device__ __forceinline__ void st4(double* a, uint32_t o, const dq4& g) {
+    a[4 * (size_t)o] = g.w;
+    a[4 * (size_t)o + 1] = g.u.x;
+    a[4 * (size_t)o + 2] = g.u.y;
+    a[4 * (size_t)o + 3] = g.u.z;
+}
+
+// Reverse of one owner's step (the forward form is in the file header).  In: the gradients of the step-end state
+// (lx, lv, lq, lw: position, velocity, quaternion, owner-frame angular velocity) and the recorded step-start
+// quaternion, angular velocity and angular acceleration.  Out: the gradients of the owner's summed force (lF,
+// world) and torque (lT, owner frame), and the direct part of the step-start state gradients.
+__global__ void k_adj_integrate(StateView s, uint32_t nO, uint32_t nClumps, double h, const float4* Q,
+                                const float4* W, const float4* Al, const double* lx, const double* lv,
+                                const double* lq, const double* lw, double* lF, double* lT, double* nlx,
+                                double* nlv, double* nlq, double* nlw) {
+    const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= nO) return;
+    const dv3 zero = mk(0, 0, 0);
+    if (!owner_free(s, o, nClumps)) {
+        st3(lF, o, zero);
+        st3(lT, o, zero);
+        st3(nlx, o, zero);
+        st3(nlv, o, zero);
+        st3(nlw, o, zero);
+        st4(nlq, o, dq4{0.0, zero});
+        return;
+    }
+    const double m = s.vel[o].w;
+    const float4 Mi = s.moi[o];
+    const dv3 gx = ld3(lx, o), gv = ld3(lv, o), gw = ld3(lw, o);
+    const dq4 gq = ld4(lq, o);
+    // translation
+    const dv3 ga = (0.5 * h * h) * gx + h * gv;
+    st3(lF, o, (1.0 / m) * ga);
+    st3(nlx, o, gx);
+    st3(nlv, o, gv + h * gx);
+    // rotation: r = w + h alpha / 2, p = exp(h r), q' = q (x) p, w' = w + h alpha
+    const dq4 q = to_dq4(Q[o]);
+    const float4 wf = W[o], af = Al[o];
+    const dv3 w = mk(wf.x, wf.y, wf.z), al = mk(af.x, af.y, af.z);
+    const dv3 r = w + (0.5 * h) * al;
+    const double L = norm(r), th = 0.5 * h * L;
+    dq4 p{1.0, zero};
+    if (L > 0.0) p = dq4{cos(th), (sin(th) / L) * r};
+    dq4 gq0, gp;
+    qmul_vjp(q, p, gq, gq0, gp);
+    const dv3 gr = qexp_vjp(r, h, gp);
+    const dv3 gal = h * gw + (0.5 * h) * gr;
+    st3(lT, o, mk(gal.x / Mi.x, gal.y / Mi.y, gal.z / Mi.z));
+    st3(nlw, o, gw + gr);
+    st4(nlq, o, gq0);
+}
+
+// The seed's angular-velocity gradient from the world frame to the owner frame, at the final state: w_world =
+// R(q) w, so dL/dw = R(q)^T dL/dw_world and dL/dq gains the derivative of R(q) w.
+__global__ void k_adj_seed(uint32_t nO, const float4* Q, const float4* W, double* lq, double* lw) {
+    const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= nO) return;
+    const dq4 q = to_dq4(Q[o]);
+    const float4 wf = W[o];
+    const dv3 gW = ld3(lw, o);
+    st3(lw, o, qrot_t(q, gW));
+    dq4 gq = ld4(lq, o);
+    gq += qrot_vjp(q, mk(wf.x, wf.y, wf.z), gW);
+    st4(lq, o, gq);
+}
+
+// The result at the window start in the interface's variables: w = R(q)^T w_world, so dL/dw_world = R(q) dL/dw
+// and the quaternion gradient at fixed w_world gains the derivative of R(q)^T w_world.  Driven owners get 0.
+__global__ void k_adj_result(StateView s, uint32_t nO, uint32_t nClumps, const float4* Q, const float4* W,
+                             double* lx, double* lv, double* lq, double* lw) {
+    const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= nO) return;
+    const dv3 zero = mk(0, 0, 0);
+    if (!owner_free(s, o, nClumps)) {
+        st3(lx, o, zero);
+        st3(lv, o, zero);
+        st3(lw, o, zero);
+        st4(lq, o, dq4{0.0, zero});
+        return;
+    }
+    const dq4 q = to_dq4(Q[o]);
+    const float4 wf = W[o];
+    const dv3 gw = ld3(lw, o);
+    const dv3 wW = qrot(q, mk(wf.x, wf.y, wf.z));
+    st3(lw, o, qrot(q, gw));
+    dq4 gq = ld4(lq, o);
+    gq += qrot_vjp(q, gw, wW);
+    st4(lq, o, gq);
 }
 
 __device__ __forceinline__ double dbeta_de(double e) {
@@ -116,14 +211,29 @@ __device__ __forceinline__ double dbeta_de(double e) {
     return (1.0 / e) * kPi2 / (d * sqrt(d));
 }
 
+// A sphere's offset from its owner as the forward step forms it: rotated in float (rot_f), then added in double.
+__device__ __forceinline__ dv3 sphere_offset(float4 sp, float4 q) {
+    float rx = sp.x, ry = sp.y, rz = sp.z;
+    rot_f(rx, ry, rz, q.x, q.y, q.z, q.w);
+    return mk(rx, ry, rz);
+}
+
 // Per contact of one recorded step: the law's derivative, scattered to both owners and to the material gradients.
-__global__ void __launch_bounds__(256) k_adj_contact(SimConsts k, StateView s, uint32_t n, uint32_t nClumps,
+// Geometry (checkSpheresOverlap / checkSphereEntityOverlap forms, src/kernel/DEMHelperKernels.cu:233-264, 394-445):
+//   sphere pair:  c = X + R(q) r per side, d = cA - cB, D = |d|, n = d / D, delta = rA + rB - D,
+//                 CP = cB + (rB - delta / 2) n;
+//   wall:         gap, n at cA (wall_geom), delta = (rA - gap) / 2, CP = cA - n (gap + rA) / 2;
+//   lever arms rAv = CP - XA, rBv = CP - XB, taken to the owner frames as s = R(q)^T r.
+// As the forward step forms them (force_kernel.cuh): the rotational velocity at the contact point is R(q) (w x s)
+// per body, and the owner-frame torques are sA x R(qA)^T (f + t) and sB x R(qB)^T -(f + t) (t: the torque-only
+// force); lT carries the gradients of the owners' summed owner-frame torques.
+__global__ void __launch_bounds__(256) k_adj_contact(SimConsts k, StateView s, const AnalRaw* raw, uint32_t n,
                                                      uint32_t nM, const uint32_t* cA, const uint32_t* cB,
                                                      const uint8_t* cT, const float4* cH, const double* X,
-                                                     const float4* V, const float4* W, const double* lF,
-                                                     const double* lT, const float4* gHout, float4* gHin,
-                                                     double* nlx, double* nlv, double* nlw, double* gmat,
-                                                     double3 floors) {
+                                                     const float4* V, const float4* Q, const float4* W,
+                                                     const double* lF, const double* lT, const float4* gHout,
+                                                     float4* gHin, double* nlx, double* nlv, double* nlq, double* nlw,
+                                                     double* gmat, double3 floors) {
     extern __shared__ double s_g[];  // nM x (E, CoR, mu, Crr)
     for (uint32_t t = threadIdx.x; t < 4u * nM; t += blockDim.x) s_g[t] = 0.0;
     __syncthreads();
@@ -135,52 +245,76 @@ __global__ void __launch_bounds__(256) k_adj_contact(SimConsts k, StateView s, u
         float4 gin = make_float4(0.f, 0.f, 0.f, 0.f);
         if (ok) {
             const uint32_t oA = s.sOwner[sA];
-            const dv3 xA = mk(X[3 * (size_t)oA], X[3 * (size_t)oA + 1], X[3 * (size_t)oA + 2]);
-            const double rA = (double)s.sph[sA].w;
+            const float4 spA = s.sph[sA], qfA = Q[oA], wfA = W[oA];
+            const dq4 qA = to_dq4(qfA);
+            const dv3 XA = ld3(X, oA), wbA = mk(wfA.x, wfA.y, wfA.z);
+            const dv3 cAc = XA + sphere_offset(spA, qfA);
+            const double rA = (double)spA.w;
             const double mA = (double)s.vel[oA].w;
             const uint32_t matA = s.sMat[sA];
             LawIn in;
+            dv3 in_rAv = mk(0, 0, 0), in_rBv = mk(0, 0, 0);
             uint32_t oB = 0, matB = 0;
-            double rB, mB, D = 1.0, a_ = 0.0, b_ = 0.0;
-            dv3 nrm;
+            float4 spB = make_float4(0.f, 0.f, 0.f, 0.f), qfB = make_float4(1.f, 0.f, 0.f, 0.f);
+            double rB = 0.0, mB = 1.0, D = 1.0, bb = 0.0, kk = 0.0;
+            dv3 nrm = mk(0, 0, 0), XB = mk(0, 0, 0);
+            WallGeom wg;
             bool active = false;
             if (ss) {
                 oB = s.sOwner[bId];
-                const dv3 xB = mk(X[3 * (size_t)oB], X[3 * (size_t)oB + 1], X[3 * (size_t)oB + 2]);
-                rB = (double)s.sph[bId].w;
+                spB = s.sph[bId];
+                qfB = Q[oB];
+                XB = ld3(X, oB);
+                const dv3 cBc = XB + sphere_offset(spB, qfB);
+                rB = (double)spB.w;
                 mB = (double)s.vel[oB].w;
                 matB = s.sMat[bId];
-                const dv3 d = xA - xB;
+                const dv3 d = cAc - cBc;
                 D = norm(d);
                 active = D <= rA + rB && D > 0.0;
                 if (active) {
                     nrm = (1.0 / D) * d;
                     in.delta = rA + rB - D;
-                    a_ = rA - in.delta / 2.0;
-                    b_ = rB - in.delta / 2.0;
-                    in.rAv = (-a_) * nrm;
-                    in.rBv = b_ * nrm;
-                    in.vB = to_dv3(V[oB]);
-                    in.wB = to_dv3(W[oB]);
+                    bb = rB - in.delta / 2.0;
+                    const dv3 CP = cBc + bb * nrm;
+                    in_rAv = CP - XA;
+                    in_rBv = CP - XB;
                 }
             } else {
-                const AnalPlaced ap = s.anal[bId];
-                oB = ap.owner;
-                nrm = mk(ap.dx, ap.dy, ap.dz);
-                const double dist = dot(xA - mk(ap.x, ap.y, ap.z), nrm);
-                in.delta = (rA - dist) / 2.0;
-                active = ap.type == DEME_ANAL_PLANE && in.delta >= 0.0;
+                const AnalRaw ar = raw[bId];
+                oB = ar.owner;
+                qfB = Q[oB];
+                XB = ld3(X, oB);
+                // the wall placed as k_place_anal places it: reference point and direction rotated in float
+                float px = ar.relX, py = ar.relY, pz = ar.relZ, dx = ar.rotX, dy = ar.rotY, dz = ar.rotZ;
+                rot_f(px, py, pz, qfB.x, qfB.y, qfB.z, qfB.w);
+                rot_f(dx, dy, dz, qfB.x, qfB.y, qfB.z, qfB.w);
+                const dv3 P = XB + mk(px, py, pz), dir = mk(dx, dy, dz);
                 rB = (double)1e15f;
-                mB = (double)ap.mass;
-                matB = ap.material;
-                in.rAv = (-(dist + in.delta)) * nrm;
-                in.rBv = mk(0, 0, 0);
-                in.vB = in.wB = mk(0, 0, 0);
+                mB = (double)ar.mass;
+                matB = ar.material;
+                if (wall_geom(ar.type, ar.normal, (double)ar.size1, ar.c1, ar.c2, (double)ar.size2, (double)ar.size3, P,
+                              dir, cAc, wg)) {
+                    in.delta = (rA - wg.gap) / 2.0;
+                    active = in.delta >= 0.0;
+                    nrm = wg.n;
+                    kk = (wg.gap + rA) / 2.0;
+                    const dv3 CP = cAc - kk * nrm;
+                    in_rAv = CP - XA;
+                    in_rBv = CP - XB;
+                }
             }
             if (active) {
+                const float4 wfB = W[oB];
+                const dv3 wbB = mk(wfB.x, wfB.y, wfB.z);
+                const dq4 qB = to_dq4(qfB);
+                const dv3 rAv = in_rAv, rBv = in_rBv;
+                const dv3 sA = qrot_t(qA, rAv), sB = qrot_t(qB, rBv);
                 in.n = nrm;
                 in.vA = to_dv3(V[oA]);
-                in.wA = to_dv3(W[oA]);
+                in.vB = to_dv3(V[oB]);
+                in.WA = qrot(qA, cross(wbA, sA));
+                in.WB = qrot(qB, cross(wbB, sB));
                 const float4 hi = cH[i];
                 in.dtan = mk(hi.x, hi.y, hi.z);
                 in.tau = hi.w;
@@ -206,32 +340,66 @@ __global__ void __launch_bounds__(256) k_adj_contact(SimConsts k, StateView s, u
                 const uint32_t crSrc = crA > crB ? matA : matB;
                 const double le = log(cor > kTiny ? cor : kTiny);
                 in.be = le / sqrt(le * le + kPi2);
-                // upstream gradients: forces and torques of both owners (B only when it is a sphere)
+                // upstream gradients: forces (world) and owner-frame torques of both owners (driven owners carry 0)
                 const dv3 gFA = ld3(lF, oA), gTA = ld3(lT, oA);
                 const dv3 gFB = ss ? ld3(lF, oB) : mk(0, 0, 0), gTB = ss ? ld3(lT, oB) : mk(0, 0, 0);
-                const dv3 g_u = cross(gTA, in.rAv) - cross(gTB, in.rBv);
+                // torque sA x R^T u: its gradient with respect to u (= f + t) is R (gT x sA)
+                const dv3 g_u = qrot(qA, cross(gTA, sA)) - qrot(qB, cross(gTB, sB));
                 const float4 gho = gHout ? gHout[i] : make_float4(0.f, 0.f, 0.f, 0.f);
                 dv3 f, t;
                 LawGrad G;
                 law_vjp(in, gFA - gFB + g_u, g_u, mk(gho.x, gho.y, gho.z), gho.w, f, t, G);
                 const dv3 u = f + t;
-                G.rAv += cross(u, gTA);
-                if (ss) G.rBv -= cross(u, gTB);
+                // A side: torque sA x bA (bA = R^T u) and contact-point velocity R (wA x sA), back to sA, wA, qA
+                const dv3 bA = qrot_t(qA, u);
+                dv3 g_sA = cross(bA, gTA);
+                const dv3 gbA = cross(gTA, sA);
+                dq4 gqA = qrot_vjp(qA, gbA, u);
+                const dv3 gcA_ = qrot_t(qA, G.WA);
+                gqA += qrot_vjp(qA, cross(wbA, sA), G.WA);
+                const dv3 g_wbA = cross(sA, gcA_);
+                g_sA += cross(gcA_, wbA);
+                const dv3 g_rAv = qrot(qA, g_sA);  // sA = R^T rAv
+                gqA += qrot_vjp(qA, g_sA, rAv);
+                // B side likewise (torque -u); for a wall only the lever arm's path counts (its owner is driven)
+                const dv3 gcB_ = qrot_t(qB, G.WB);
+                dv3 g_sB = cross(gcB_, wbB);
+                dq4 gqB = qrot_vjp(qB, cross(wbB, sB), G.WB);
+                const dv3 g_wbB = cross(sB, gcB_);
                 if (ss) {
-                    const double g_a = -dot(G.rAv, nrm), g_b = dot(G.rBv, nrm);
-                    const dv3 g_n = G.n - a_ * G.rAv + b_ * G.rBv;
-                    const double g_delta = G.delta - g_a / 2.0 - g_b / 2.0;
-                    const dv3 g_d = (1.0 / D) * (g_n - dot(g_n, nrm) * nrm) + (-g_delta) * nrm;
-                    add3(nlx, oA, g_d);
-                    add3(nlx, oB, -g_d);
-                    add3(nlv, oB, G.vB);
-                    add3(nlw, oB, G.wB);
-                } else {
-                    const double g_dist = -G.delta / 2.0 - dot(G.rAv, nrm) / 2.0;
-                    add3(nlx, oA, g_dist * nrm);
+                    const dv3 bB = qrot_t(qB, -u);
+                    g_sB += cross(bB, gTB);
+                    const dv3 gbB = cross(gTB, sB);
+                    gqB += qrot_vjp(qB, gbB, -u);
                 }
+                const dv3 g_rBv = qrot(qB, g_sB);
+                gqB += qrot_vjp(qB, g_sB, rBv);
+                // geometry reversed: contact point, normal and depth back to the sphere centres and the owners
+                const dv3 gCP = g_rAv + g_rBv;
+                dv3 gcA;
+                if (ss) {
+                    const double g_delta = G.delta - 0.5 * dot(gCP, nrm);
+                    const dv3 g_n = G.n + bb * gCP;
+                    const dv3 g_d = (1.0 / D) * (g_n - dot(g_n, nrm) * nrm) + (-g_delta) * nrm;
+                    gcA = g_d;
+                    const dv3 gcB = gCP - g_d;
+                    // owner B: its position directly and through its sphere centre, its offset's rotation
+                    add3(nlx, oB, gcB - g_rBv);
+                    add3(nlv, oB, G.vB);
+                    add3(nlw, oB, g_wbB);
+                    if (spB.x != 0.f || spB.y != 0.f || spB.z != 0.f) gqB += qrot_vjp(qB, mk(spB.x, spB.y, spB.z), gcB);
+                    add4(nlq, oB, gqB);
+                } else {
+                    const double g_kk = -dot(gCP, nrm);
+                    const dv3 g_n = G.n - kk * gCP;
+                    const double g_gap = -0.5 * G.delta + 0.5 * g_kk;
+                    gcA = gCP + wall_geom_vjp(wg, g_gap, g_n);
+                }
+                add3(nlx, oA, gcA - g_rAv);
                 add3(nlv, oA, G.vA);
-                add3(nlw, oA, G.wA);
+                add3(nlw, oA, g_wbA);
+                if (spA.x != 0.f || spA.y != 0.f || spA.z != 0.f) gqA += qrot_vjp(qA, mk(spA.x, spA.y, spA.z), gcA);
+                add4(nlq, oA, gqA);
                 gin = make_float4((float)G.dtan.x, (float)G.dtan.y, (float)G.dtan.z, (float)G.tau);
                 // material parameters (matProxy2ContactParam's derivatives)
                 const double Es2 = in.Es * in.Es, Gs2 = in.Gs * in.Gs;
@@ -379,8 +547,11 @@ int32_t restore_checkpoint(deme_handle* h, const Checkpoint& c) {
 
 namespace {
 
-// The scenes the adjoint covers: single spheres (relative position 0, isotropic inertia) with plane walls, the
-// built-in model, Extended Taylor integration, contact detection every step, no prescribed sphere families.
+// The scenes the adjoint covers: clumps (any number of member spheres, principal moments of inertia) of free
+// families and analytical walls (planes, cylinders, cones) of families whose motion is prescribed, the built-in
+// model, Extended Taylor integration, contact detection every step.  A clump of a prescribed family counts as
+// driven when both its linear and its rotational motion are prescribed; a partial prescription, or a wall whose
+// owner moves under the contact forces, is outside.
 int32_t check_adjoint_scene(deme_handle* h) {
     if (h->userForce.lib) {
         h->err = "adjoint: only the built-in Hertz-Mindlin model is differentiated";
@@ -394,34 +565,26 @@ int32_t check_adjoint_scene(deme_handle* h) {
         h->err = "adjoint: needs Extended Taylor integration and synchronous contact detection every step";
         return DEME_ERR_INVALID;
     }
-    std::vector<float4> sph(h->nS), moi(h->nO);
-    std::vector<uint32_t> owner(h->nS);
     std::vector<ushort4> loc(h->nO);
     std::vector<AnalRaw> anal(std::max(h->nA, 1u));
     std::vector<Prescription> presc(DEME_NUM_FAMILIES);
-    CUDA_TRY(h, cudaMemcpy(sph.data(), h->sph, h->nS * sizeof(float4), cudaMemcpyDeviceToHost));
-    CUDA_TRY(h, cudaMemcpy(owner.data(), h->sOwner, h->nS * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    CUDA_TRY(h, cudaMemcpy(moi.data(), h->moi, h->nO * sizeof(float4), cudaMemcpyDeviceToHost));
     CUDA_TRY(h, cudaMemcpy(loc.data(), h->loc, h->nO * sizeof(ushort4), cudaMemcpyDeviceToHost));
     if (h->nA) CUDA_TRY(h, cudaMemcpy(anal.data(), h->analRaw, h->nA * sizeof(AnalRaw), cudaMemcpyDeviceToHost));
     CUDA_TRY(h, cudaMemcpy(presc.data(), h->presc, DEME_NUM_FAMILIES * sizeof(Prescription), cudaMemcpyDeviceToHost));
-    for (uint32_t i = 0; i < h->nS; i++) {
-        if (owner[i] != i || sph[i].x != 0.f || sph[i].y != 0.f || sph[i].z != 0.f) {
-            h->err = "adjoint: every owner must be one sphere centred on it";
-            return DEME_ERR_INVALID;
-        }
-        if (moi[i].x != moi[i].y || moi[i].x != moi[i].z) {
-            h->err = "adjoint: sphere moments of inertia must be isotropic";
-            return DEME_ERR_INVALID;
-        }
-        if (presc[loc[i].w].used) {
-            h->err = "adjoint: sphere families must not be prescribed";
+    auto driven = [](const Prescription& p) {
+        return p.used && (p.lin_vel || p.lin_pos) && (p.rot_vel || p.rot_pos);
+    };
+    for (uint32_t o = 0; o < h->nO; o++) {
+        const Prescription& p = presc[loc[o].w];
+        if (o < h->nClumps ? p.used && !driven(p) : !driven(p)) {
+            h->err = o < h->nClumps ? "adjoint: a clump family is only partly prescribed"
+                                    : "adjoint: walls must belong to families with prescribed motion";
             return DEME_ERR_INVALID;
         }
     }
     for (uint32_t a = 0; a < h->nA; a++)
-        if (anal[a].type != DEME_ANAL_PLANE) {
-            h->err = "adjoint: walls must be planes";
+        if (anal[a].type != DEME_ANAL_PLANE && anal[a].type != DEME_ANAL_CYLINDER && anal[a].type != DEME_ANAL_CONE) {
+            h->err = "adjoint: walls must be planes, cylinders or cones";
             return DEME_ERR_INVALID;
         }
     return DEME_OK;
@@ -434,10 +597,10 @@ void adjoint_release(deme_handle* h) {
     AdjointTape* t = h->adj;
     for (Checkpoint& c : t->cps) free_checkpoint(h, c);
     free_checkpoint(h, t->fin);
-    for (void* p : {(void*)t->X, (void*)t->V, (void*)t->W, (void*)t->cA, (void*)t->cB, (void*)t->cT, (void*)t->cH,
-                    (void*)t->cM, (void*)t->lx, (void*)t->lv, (void*)t->lw, (void*)t->nlx, (void*)t->nlv,
-                    (void*)t->nlw, (void*)t->lF, (void*)t->lT, (void*)t->gA, (void*)t->gB, (void*)t->gC,
-                    (void*)t->gmat})
+    for (void* p : {(void*)t->X, (void*)t->V, (void*)t->Q, (void*)t->W, (void*)t->Al, (void*)t->cA, (void*)t->cB,
+                    (void*)t->cT, (void*)t->cH, (void*)t->cM, (void*)t->lx, (void*)t->lv, (void*)t->lw, (void*)t->nlx,
+                    (void*)t->nlv, (void*)t->nlw, (void*)t->lq, (void*)t->nlq, (void*)t->lF, (void*)t->lT,
+                    (void*)t->gA, (void*)t->gB, (void*)t->gC, (void*)t->gmat})
         dfree(h, p);
     delete t;
     h->adj = nullptr;
@@ -498,22 +661,29 @@ int32_t deme_adjoint_backward(deme_handle* h, const deme_adjoint_seed* seed, dem
     if (!t->lx) {
         for (double** p : {&t->lx, &t->lv, &t->lw, &t->nlx, &t->nlv, &t->nlw, &t->lF, &t->lT})
             TRY(dalloc_n(h, p, 3 * (size_t)nO));
+        TRY(dalloc_n(h, &t->lq, 4 * (size_t)nO));
+        TRY(dalloc_n(h, &t->nlq, 4 * (size_t)nO));
         TRY(dalloc_n(h, &t->gmat, 4 * (size_t)nM));
         TRY(dalloc_n(h, &t->X, (size_t)K * nO * 3));
         TRY(dalloc_n(h, &t->V, (size_t)K * nO));
+        TRY(dalloc_n(h, &t->Q, (size_t)K * nO));
         TRY(dalloc_n(h, &t->W, (size_t)K * nO));
+        TRY(dalloc_n(h, &t->Al, (size_t)K * nO));
     }
     CUDA_TRY(h, cudaMemsetAsync(t->gmat, 0, 4 * (size_t)nM * sizeof(double), st));
     {
-        const double* src[3] = {seed ? seed->d_pos : nullptr, seed ? seed->d_vel : nullptr,
-                                seed ? seed->d_angvel : nullptr};
-        double* dst[3] = {t->lx, t->lv, t->lw};
-        for (int a = 0; a < 3; a++) {
+        const double* src[4] = {seed ? seed->d_pos : nullptr, seed ? seed->d_vel : nullptr,
+                                seed ? seed->d_angvel : nullptr, seed ? seed->d_quat : nullptr};
+        double* dst[4] = {t->lx, t->lv, t->lw, t->lq};
+        for (int a = 0; a < 4; a++) {
+            const size_t bytes = (a == 3 ? 4 : 3) * (size_t)nO * sizeof(double);
             if (src[a])
-                CUDA_TRY(h, cudaMemcpy(dst[a], src[a], 3 * (size_t)nO * sizeof(double), cudaMemcpyHostToDevice));
+                CUDA_TRY(h, cudaMemcpy(dst[a], src[a], bytes, cudaMemcpyHostToDevice));
             else
-                CUDA_TRY(h, cudaMemset(dst[a], 0, 3 * (size_t)nO * sizeof(double)));
+                CUDA_TRY(h, cudaMemset(dst[a], 0, bytes));
         }
+        // the seed at the final state, its world-frame angular velocity gradient taken to the owner frame
+        k_adj_seed<<<nblk(nO, 256), 256, 0, st>>>(nO, t->fin.quat, t->fin.omg, t->lq, t->lw);
     }
     uint32_t gCap = t->gCap;
     auto ensure_g = [&](uint32_t n) -> int32_t {
@@ -545,7 +715,8 @@ int32_t deme_adjoint_backward(deme_handle* h, const deme_adjoint_seed* seed, dem
         for (int s = 0; s < len; s++) {
             StateView sv = h->state_view();
             k_adj_record_state<<<nblk(nO, 256), 256, 0, st>>>(k, sv, nO, t->X + (size_t)s * nO * 3,
-                                                               t->V + (size_t)s * nO, t->W + (size_t)s * nO);
+                                                               t->V + (size_t)s * nO, t->Q + (size_t)s * nO,
+                                                               t->W + (size_t)s * nO);
             TRY(deme_detect_contacts(h));
             const uint32_t n = h->nContacts;
             if (base + n > t->poolCap) {  // grow the pool, keeping the steps recorded so far
@@ -592,6 +763,8 @@ int32_t deme_adjoint_backward(deme_handle* h, const deme_adjoint_seed* seed, dem
             t->stepBase[(size_t)s] = base;
             base += n;
             TRY(deme_compute_forces(h));
+            CUDA_TRY(h, cudaMemcpyAsync(t->Al + (size_t)s * nO, h->alpha, nO * sizeof(float4),
+                                        cudaMemcpyDeviceToDevice, st));
             TRY(deme_integrate(h));
         }
         uint32_t need = cp.n;
@@ -613,15 +786,18 @@ int32_t deme_adjoint_backward(deme_handle* h, const deme_adjoint_seed* seed, dem
         for (int s = len - 1; s >= 0; s--) {
             const uint32_t n = t->stepN[(size_t)s], b = t->stepBase[(size_t)s];
             StateView sv = h->state_view();
-            k_adj_integrate<<<nblk(nO, 256), 256, 0, st>>>(sv, nO, h->nClumps, (double)k.h, t->lx, t->lv, t->lw, t->lF, t->lT,
-                                                            t->nlx, t->nlv, t->nlw);
+            const float4 *Qs = t->Q + (size_t)s * nO, *Ws = t->W + (size_t)s * nO;
+            k_adj_integrate<<<nblk(nO, 256), 256, 0, st>>>(sv, nO, h->nClumps, (double)k.h, Qs, Ws,
+                                                            t->Al + (size_t)s * nO, t->lx, t->lv, t->lq, t->lw, t->lF,
+                                                            t->lT, t->nlx, t->nlv, t->nlq, t->nlw);
             if (n)
                 k_adj_contact<<<nblk(n, 256), 256, 4 * nM * sizeof(double), st>>>(
-                    k, sv, n, h->nClumps, nM, t->cA + b, t->cB + b, t->cT + b, t->cH + b, t->X + (size_t)s * nO * 3,
-                    t->V + (size_t)s * nO, t->W + (size_t)s * nO, t->lF, t->lT, gOut, t->gB, t->nlx, t->nlv, t->nlw,
-                    t->gmat, make_double3(t->floors[0], t->floors[1], t->floors[2]));
+                    k, sv, h->analRaw, n, nM, t->cA + b, t->cB + b, t->cT + b, t->cH + b, t->X + (size_t)s * nO * 3,
+                    t->V + (size_t)s * nO, Qs, Ws, t->lF, t->lT, gOut, t->gB, t->nlx, t->nlv, t->nlq, t->nlw, t->gmat,
+                    make_double3(t->floors[0], t->floors[1], t->floors[2]));
             std::swap(t->lx, t->nlx);
             std::swap(t->lv, t->nlv);
+            std::swap(t->lq, t->nlq);
             std::swap(t->lw, t->nlw);
             // incoming-history gradients go to the previous list (the previous step's, or the checkpoint's)
             const uint32_t nPrev = s > 0 ? t->stepN[(size_t)s - 1] : cp.n;
@@ -633,13 +809,17 @@ int32_t deme_adjoint_backward(deme_handle* h, const deme_adjoint_seed* seed, dem
         }
         TRY(check_launch(h, "adjoint"));
     }
-    // ---- results ----
+    // ---- results, in the interface's variables at the window start ----
+    k_adj_result<<<nblk(nO, 256), 256, 0, st>>>(h->state_view(), nO, h->nClumps, t->cps[0].quat, t->cps[0].omg,
+                                                 t->lx, t->lv, t->lq, t->lw);
     CUDA_TRY(h, cudaStreamSynchronize(st));
-    double* dsts[3] = {out->d_pos0, out->d_vel0, out->d_angvel0};
-    const double* srcs[3] = {t->lx, t->lv, t->lw};
-    for (int a = 0; a < 3; a++)
+    TRY(check_launch(h, "adjoint"));
+    double* dsts[4] = {out->d_pos0, out->d_vel0, out->d_angvel0, out->d_quat0};
+    const double* srcs[4] = {t->lx, t->lv, t->lw, t->lq};
+    for (int a = 0; a < 4; a++)
         if (dsts[a])
-            CUDA_TRY(h, cudaMemcpy(dsts[a], srcs[a], 3 * (size_t)nO * sizeof(double), cudaMemcpyDeviceToHost));
+            CUDA_TRY(h, cudaMemcpy(dsts[a], srcs[a], (a == 3 ? 4 : 3) * (size_t)nO * sizeof(double),
+                                   cudaMemcpyDeviceToHost));
     if (out->d_material)
         CUDA_TRY(h, cudaMemcpy(out->d_material, t->gmat, 4 * (size_t)h->nM * sizeof(double), cudaMemcpyDeviceToHost));
     TRY(restore_checkpoint(h, t->fin));

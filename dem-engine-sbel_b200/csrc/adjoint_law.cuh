@@ -1,9 +1,9 @@
 // adjoint_law.cuh -- reverse-mode derivative of one contact of the built-in frictional Hertz-Mindlin model, for the
-// adjoint of a sphere step (adjoint.cu).  The forward part restates force_model_hertz.cuh for single-sphere owners
-// with their angular velocity in the world frame, in double precision; the reverse part propagates the gradients
-// of the contact's force, torque-only force and updated history back to its inputs (relative position, both
-// velocities and angular velocities, the incoming history) and to the pair's material parameters
-// (E*, G*, beta, mu, Crr).  Each reverse step is the derivative of the forward line it follows.
+// adjoint of the step (adjoint.cu).  The forward part restates force_model_hertz.cuh in double precision, taking
+// the rotational velocities of both bodies at the contact point (ARotCP, BRotCP) as inputs; the reverse part
+// propagates the gradients of the contact's force, torque-only force and updated history back to its inputs
+// (normal, overlap, both linear and contact-point rotational velocities, the incoming history) and to the pair's
+// material parameters (E*, G*, beta, mu, Crr).  Each reverse step is the derivative of the forward line it follows.
 #pragma once
 #include "device_common.cuh"
 
@@ -31,9 +31,10 @@ constexpr double kPi2 = 9.869604401089358;
 constexpr double kTiny = 1e-12;
 
 struct LawIn {
-    dv3 n, rAv, rBv;  // unit normal B -> A and lever arms from the owners to the contact point
-    double delta;     // overlap depth
-    dv3 vA, vB, wA, wB;
+    dv3 n;         // unit normal B -> A
+    double delta;  // overlap depth
+    dv3 vA, vB;    // owner velocities
+    dv3 WA, WB;    // rotational velocities at the contact point (w x r of each body)
     dv3 dtan;         // incoming tangential displacement history
     double tau;       // incoming contact duration
     double Es, Gs, be, mu, crr, meff, Rs, h;
@@ -43,9 +44,9 @@ struct LawIn {
 };
 
 struct LawGrad {
-    dv3 n, rAv, rBv;
+    dv3 n;
     double delta;
-    dv3 vA, vB, wA, wB, dtan;
+    dv3 vA, vB, WA, WB, dtan;
     double tau, Es, Gs, be, mu, crr;
 };
 
@@ -55,7 +56,7 @@ __device__ __forceinline__ void law_vjp(const LawIn& in, dv3 g_f, dv3 g_t, dv3 g
                                         dv3& t_out, LawGrad& G) {
     const dv3 n = in.n;
     // ---- forward, keeping what the reverse pass needs ----
-    const dv3 WA = cross(in.wA, in.rAv), WB = cross(in.wB, in.rBv);
+    const dv3 WA = in.WA, WB = in.WB;
     const dv3 vr = in.vA + WA - in.vB - WB;
     const double p = dot(vr, n);
     const dv3 vt = vr - p * n;
@@ -70,7 +71,8 @@ __device__ __forceinline__ void law_vjp(const LawIn& in, dv3 g_f, dv3 g_t, dv3 g
     const double gn = kC5 * in.be * ssm;
     const double fnm = kn * in.delta + gn * p;
     const dv3 fn = fnm * n;
-    const double A = fabs(fnm);
+    const double nn = norm(n);  // 1 but for a wall direction rotated by a quaternion off unit length
+    const double A = fabs(fnm) * nn;  // the length of the normal force, which sets the cap and the rolling torque
     // rolling resistance once the contact is older than the collision time
     const double Reff = sqrt(in.Rs);
     const double kns = (4.0 / 3.0) * in.Es * sqrt(Reff);
@@ -141,8 +143,8 @@ __device__ __forceinline__ void law_vjp(const LawIn& in, dv3 g_f, dv3 g_t, dv3 g
         g_WB += g_vroll;
         g_WA -= g_vroll;
     }
-    const double g_fnm = g_A * (fnm > 0.0 ? 1.0 : (fnm < 0.0 ? -1.0 : 0.0)) + dot(g_fn, n);
-    g_n += fnm * g_fn;
+    const double g_fnm = g_A * nn * (fnm > 0.0 ? 1.0 : (fnm < 0.0 ? -1.0 : 0.0)) + dot(g_fn, n);
+    g_n += fnm * g_fn + (g_A * fabs(fnm) / nn) * n;
     const double g_kn = g_fnm * in.delta;
     double g_delta = g_fnm * kn;
     const double g_gn = g_fnm * p;
@@ -170,10 +172,8 @@ __device__ __forceinline__ void law_vjp(const LawIn& in, dv3 g_f, dv3 g_t, dv3 g
     g_WB -= g_vr;
     G.vA = g_vr;
     G.vB = -g_vr;
-    G.wA = cross(in.rAv, g_WA);
-    G.rAv = cross(g_WA, in.wA);
-    G.wB = cross(in.rBv, g_WB);
-    G.rBv = cross(g_WB, in.wB);
+    G.WA = g_WA;
+    G.WB = g_WB;
     G.n = g_n;
     G.delta = g_delta;
 }

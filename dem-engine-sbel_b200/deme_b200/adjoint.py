@@ -1,8 +1,10 @@
 """Adjoint of the DEM step through the C ABI (deme_adjoint_record / deme_adjoint_backward / deme_set_material), and a
 torch.autograd.Function that makes a window of steps differentiable with respect to the material parameters.
 
-Scope (enforced by the library): single spheres with plane walls, the built-in Hertz-Mindlin model, Extended
-Taylor integration, contact detection every step.
+Scope (enforced by the library): clumps (or single spheres) of free families or of families whose linear and
+rotational motion are both prescribed, analytical walls (planes, cylinders, cones) of prescribed families, the
+built-in Hertz-Mindlin model, Extended Taylor integration, contact detection every step.  Angular velocities are
+in the world frame; quaternion gradients (w, x, y, z) hold the world angular velocity fixed.
 """
 from __future__ import annotations
 
@@ -14,11 +16,12 @@ from . import _capi as capi
 
 
 class AdjointSeed(C.Structure):
-    _fields_ = [("d_pos", C.c_void_p), ("d_vel", C.c_void_p), ("d_angvel", C.c_void_p)]
+    _fields_ = [("d_pos", C.c_void_p), ("d_vel", C.c_void_p), ("d_angvel", C.c_void_p), ("d_quat", C.c_void_p)]
 
 
 class AdjointGrads(C.Structure):
-    _fields_ = [("d_pos0", C.c_void_p), ("d_vel0", C.c_void_p), ("d_angvel0", C.c_void_p), ("d_material", C.c_void_p)]
+    _fields_ = [("d_pos0", C.c_void_p), ("d_vel0", C.c_void_p), ("d_angvel0", C.c_void_p), ("d_material", C.c_void_p),
+                ("d_quat0", C.c_void_p)]
 
 
 def _bind(lib):
@@ -41,26 +44,28 @@ def record(solver, n_steps: int, checkpoint_every: int):
     solver._check(solver.lib.deme_adjoint_record(solver.h, n_steps, checkpoint_every), "adjoint_record")
 
 
-def backward(solver, d_pos=None, d_vel=None, d_angvel=None) -> dict:
-    """Gradients of a loss with respect to the window's initial state (world-frame angular velocity) and to the
-    materials' (E, CoR, mu, Crr), given its gradient with respect to the final state (arrays n_owners x 3)."""
+def backward(solver, d_pos=None, d_vel=None, d_angvel=None, d_quat=None) -> dict:
+    """Gradients of a loss with respect to the window's initial state (world-frame angular velocity; quaternion
+    (w, x, y, z) at fixed world angular velocity) and to the materials' (E, CoR, mu, Crr), given its gradient with
+    respect to the final state (arrays n_owners x 3, quaternions n_owners x 4)."""
     _bind(solver.lib)
     nO = solver.nO
     nM = solver.built.counts["m"]
     keep = []
 
-    def arr(a):
+    def arr(a, w=3):
         if a is None:
             return None
-        a = np.ascontiguousarray(a, np.float64).reshape(nO, 3)
+        a = np.ascontiguousarray(a, np.float64).reshape(nO, w)
         keep.append(a)
         return a.ctypes.data
 
-    seed = AdjointSeed(arr(d_pos), arr(d_vel), arr(d_angvel))
+    seed = AdjointSeed(arr(d_pos), arr(d_vel), arr(d_angvel), arr(d_quat, 4))
     out = {k: np.zeros((nO, 3)) for k in ("d_pos0", "d_vel0", "d_angvel0")}
+    out["d_quat0"] = np.zeros((nO, 4))
     out["d_material"] = np.zeros((max(nM, 1), 4))
     g = AdjointGrads(out["d_pos0"].ctypes.data, out["d_vel0"].ctypes.data, out["d_angvel0"].ctypes.data,
-                     out["d_material"].ctypes.data)
+                     out["d_material"].ctypes.data, out["d_quat0"].ctypes.data)
     solver._check(solver.lib.deme_adjoint_backward(solver.h, C.byref(seed), C.byref(g)), "adjoint_backward")
     out["d_material"] = out["d_material"][:nM]
     return out
@@ -73,6 +78,11 @@ def world_angular_velocity(state: dict) -> np.ndarray:
     u = q[:, 1:]
     t = 2 * np.cross(u, w)
     return w + q[:, :1] * t + np.cross(u, t)
+
+
+def quaternions(state: dict) -> np.ndarray:
+    """Owner quaternions (w, x, y, z) as float64 rows."""
+    return np.stack([state["oriQw"], state["oriQx"], state["oriQy"], state["oriQz"]], 1).astype(np.float64)
 
 
 def final_state(solver):

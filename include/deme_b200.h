@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define DEME_B200_ABI_VERSION 3
+#define DEME_B200_ABI_VERSION 4
 
 /* Status codes (the reference throws std::runtime_error instead: src/DEM/Structs.h:129-141, src/core/utils/GpuError.h:13-27). */
 typedef enum {
@@ -445,17 +445,21 @@ size_t deme_radix_sort_scratch_bytes(uint32_t n);
 int32_t deme_radix_sort_status(const void* scratch, uint32_t n, void* stream, uint32_t* word);
 
 /* ---- Adjoint of the step (no reference counterpart) ----------------------------------------------------------
- * For scenes of single spheres (centred, isotropic inertia) with plane walls, the built-in Hertz-Mindlin model,
- * Extended Taylor integration and contact detection every step.  deme_adjoint_record runs n_steps forward from the
- * current state, keeping a checkpoint every `checkpoint_every` steps; deme_adjoint_backward takes the gradient of
- * a loss with respect to the final state and returns it with respect to the state before the window and to the
- * material parameters, recomputing each window segment from its checkpoint.  The contact set of each step is the
- * one the forward pass found.  Angular velocities are in the world frame.  The model runs on the recorded FP32
- * state; gradients are accumulated in FP64.  The handle ends at the recorded final state. */
+ * For scenes of clumps (or single spheres) with analytical walls (planes, cylinders, cones), the built-in
+ * Hertz-Mindlin model, Extended Taylor integration and contact detection every step.  Clump families are free or
+ * driven (linear and rotational motion both prescribed); wall families are driven.  deme_adjoint_record runs
+ * n_steps forward from the current state, keeping a checkpoint every `checkpoint_every` steps;
+ * deme_adjoint_backward takes the gradient of a loss with respect to the final state and returns it with respect to
+ * the state before the window and to the material parameters, recomputing each window segment from its checkpoint.
+ * The contact set of each step is the one the forward pass found.  Angular velocities are in the world frame
+ * (w_world = R(q) w_owner); quaternion gradients (w, x, y, z) hold the world angular velocity fixed.  Driven owners
+ * get 0.  The model runs on the recorded FP32 state; gradients are accumulated in FP64.  The handle ends at the
+ * recorded final state. */
 typedef struct {
     const double* d_pos;     /* n_owners x 3, dL/d(final position); NULL = 0 */
     const double* d_vel;     /* n_owners x 3, dL/d(final velocity); NULL = 0 */
     const double* d_angvel;  /* n_owners x 3, dL/d(final angular velocity, world frame); NULL = 0 */
+    const double* d_quat;    /* n_owners x 4, dL/d(final quaternion w, x, y, z); NULL = 0 */
 } deme_adjoint_seed;
 
 typedef struct {
@@ -463,6 +467,7 @@ typedef struct {
     double* d_vel0;      /* n_owners x 3 (may be NULL) */
     double* d_angvel0;   /* n_owners x 3 (may be NULL) */
     double* d_material;  /* n_materials x 4: dL/dE, dL/dCoR, dL/dmu, dL/dCrr (may be NULL) */
+    double* d_quat0;     /* n_owners x 4 (may be NULL) */
 } deme_adjoint_grads;
 
 int32_t deme_adjoint_record(deme_handle* h, int32_t n_steps, int32_t checkpoint_every);

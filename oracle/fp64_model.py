@@ -58,16 +58,42 @@ def owner_state(built, st):
     return pos, q, v, w, m, I
 
 
-def sphere_centres(built, pos, q):
+def rot_f32(q, v):
+    """applyOriQToVector3<float, float> as the CUDA path evaluates it: every operation rounded to float32 in the
+    same order (no contraction), the result widened to float64."""
+    f = np.float32
+    w, x, y, z = (q[:, k].astype(f) for k in range(4))
+    ox, oy, oz = (v[:, k].astype(f) for k in range(3))
+    two, one = f(2.0), f(1.0)
+    X = (two * (w * w + x * x) - one) * ox + (two * (x * y - w * z)) * oy + (two * (x * z + w * y)) * oz
+    Y = (two * (x * y + w * z)) * ox + (two * (w * w + y * y) - one) * oy + (two * (y * z - w * x)) * oz
+    Z = (two * (x * z - w * y)) * ox + (two * (y * z + w * x)) * oy + (two * (w * w + z * z) - one) * oz
+    return np.stack([X, Y, Z], 1).astype(np.float64)
+
+
+def _rotate(q, v, f32, q_anchor):
+    if not f32:
+        return rot(q, v)
+    if q_anchor is None:
+        return rot_f32(q, v)
+    # float32 at the anchor, plus the float64 change from it: equal to the float32 rotation at the anchor, and
+    # differentiable there with the exact derivative
+    return rot_f32(q_anchor, v) + (rot(q, v) - rot(q_anchor, v))
+
+
+def sphere_centres(built, pos, q, f32=False, q_anchor=None):
+    """Sphere centres: owner position plus the rotated offset (rotated in float32 as the CUDA path rotates it when
+    ``f32``; with ``q_anchor``, float32 at the anchor quaternions plus the float64 change from them)."""
     a = built.arrays
     o = a["sphere_owner"].astype(np.int64)
     rel = np.stack([a["relX"], a["relY"], a["relZ"]], 1).astype(np.float64)
-    return pos[o] + rot(q[o], rel)
+    return pos[o] + _rotate(q[o], rel, f32, None if q_anchor is None else q_anchor[o])
 
 
-def placed_analytical(built, pos, q):
+def placed_analytical(built, pos, q, f32=False, q_anchor=None):
     """Analytical components in the world frame: reference point, direction (plane normal / axis) and the shape
-    numbers (cylinder radius; cone sin, cos of the half angle and its axial range)."""
+    numbers (cylinder radius; cone sin, cos of the half angle and its axial range).  ``f32``: the reference point's
+    offset and the direction rotated in float32 as the CUDA path places them."""
     a = built.arrays
     nA = built.counts["a"]
     if nA == 0:
@@ -76,7 +102,9 @@ def placed_analytical(built, pos, q):
     rel = np.stack([a["anal_relX"], a["anal_relY"], a["anal_relZ"]], 1).astype(np.float64)
     d = np.stack([a["anal_rotX"], a["anal_rotY"], a["anal_rotZ"]], 1).astype(np.float64)
     half = a["anal_size1"].astype(np.float64)
-    return dict(p=pos[o] + rot(q[o], rel), d=rot(q[o], d), owner=o, type=a["anal_type"].astype(np.int64),
+    qa = None if q_anchor is None else q_anchor[o]
+    return dict(p=pos[o] + _rotate(q[o], rel, f32, qa), d=_rotate(q[o], d, f32, qa), owner=o,
+                type=a["anal_type"].astype(np.int64),
                 normal=a["anal_normal"].astype(np.int64), size1=a["anal_size1"].astype(np.float64),
                 c1=np.sin(half), c2=np.cos(half), umin=a["anal_size2"].astype(np.float64),
                 umax=a["anal_size3"].astype(np.float64), mat=a["anal_material"].astype(np.int64),
@@ -131,20 +159,38 @@ def step(built, st, contacts, h=None):
     Returns per-contact force, torque-only force and local contact points (zero where the contact does not touch),
     the updated history, the owners' accelerations, and the state after integration (positions relative to the
     lower corner, velocities, owner-frame angular velocities, quaternions)."""
+    pos, q, v, w, _, _ = owner_state(built, st)
+    S = dict(pos=pos, q=q, v=v, w=w, family=st["family"].astype(np.int64))
+    return step_state(built, S, contacts, h=h)
+
+
+def step_state(built, S, contacts, hist=None, h=None, mats=None, f32=False, q_anchor=None):
+    """``step`` on a float64 state S (pos, q, v, w in the owner frame, family) with the incoming history ``hist``
+    (rows of 4; default: the list's wildcards) and, optionally, material arrays ``mats`` (E, nu, CoR, mu, Crr)
+    replacing the scene's.  ``f32``: sphere offsets and wall placements rotated in float32 as the CUDA path does
+    (the rest in float64), so that the contact geometry is evaluated where the CUDA path evaluates it; with
+    ``q_anchor`` (owner quaternions), float32 at the anchor plus the float64 change from it, which keeps that
+    geometry differentiable in the quaternions."""
     p = built.params
     a = built.arrays
     h = float(p.h) if h is None else float(h)
-    pos, q, v, w, m, I = owner_state(built, st)
-    Xs = sphere_centres(built, pos, q)
-    an = placed_analytical(built, pos, q)
+    pos, q, v, w = S["pos"], S["q"], S["v"], S["w"]
+    m = a["mass"].astype(np.float64)
+    I = np.stack([a["mmiXX"], a["mmiYY"], a["mmiZZ"]], 1).astype(np.float64)
+    Xs = sphere_centres(built, pos, q, f32, q_anchor)
+    an = placed_analytical(built, pos, q, f32, q_anchor)
     o_s = a["sphere_owner"].astype(np.int64)
     rad = a["radius"].astype(np.float64)
     mat_s = (a["sphere_material_wide"] if "sphere_material_wide" in a else a["sphere_material"]).astype(np.int64)
-    E, nu, CoR, mu, Crr = (a[k].astype(np.float64) for k in ("mat_E", "mat_nu", "mat_CoR", "mat_mu", "mat_Crr"))
+    if mats is None:
+        E, nu, CoR, mu, Crr = (a[k].astype(np.float64) for k in ("mat_E", "mat_nu", "mat_CoR", "mat_mu", "mat_Crr"))
+    else:
+        E, nu, CoR, mu, Crr = (np.asarray(mats[k], np.float64) for k in ("E", "nu", "CoR", "mu", "Crr"))
     A = contacts["idA"].astype(np.int64)
     Bid = contacts["idB"].astype(np.int64)
     typ = contacts["type"].astype(np.int64)
-    hist = contacts["wildcards"].astype(np.float64).T.copy() if contacts["wildcards"].size else np.zeros((len(A), 4))
+    if hist is None:
+        hist = contacts["wildcards"].astype(np.float64).T.copy() if contacts["wildcards"].size else np.zeros((len(A), 4))
     nC = len(A)
     ss = typ == SPHERE_SPHERE
     oA = o_s[A]
@@ -254,7 +300,7 @@ def step(built, st, contacts, h=None):
     np.add.at(alpha, oB[act], np.cross(cpB[act], rot_t(q[oB[act]], -U[act])) / I[oB[act]])
     # Extended Taylor integration with the constant family prescriptions
     G = np.asarray(p.G[:], np.float64)
-    fam = st["family"].astype(np.int64)
+    fam = S["family"]
     vn, wn = v.copy(), w.copy()
     u_lin = (acc + G) * h
     u_rot = alpha * h
@@ -295,3 +341,36 @@ def step(built, st, contacts, h=None):
     qn = np.where(rot_pos[:, None], q, qn)
     return dict(force=F, torque_only_force=TOF, cpA=cpA, cpB=cpB, active=act, hist=hout, acc=acc, alpha=alpha,
                 pos=pos_n, vel=vn, angvel=wn, quat=qn, pos0=pos)
+
+
+def _keys(c):
+    ss = c["type"].astype(np.int64) == SPHERE_SPHERE
+    return (c["idA"].astype(np.int64) << 33) | (ss.astype(np.int64) << 32) | c["idB"].astype(np.int64)
+
+
+def rollout_fixed(built, S0, lists, mats=None, f32=False, q_anchor=None):
+    """Steps of ``step_state`` over the contact lists a run found (one list per step, each with idA, idB, type;
+    the first also with the incoming history wildcards), the lists held fixed: each step's incoming history is the
+    previous step's updated history of the contact with the same (idA, idB, type), 0 for a new contact -- the
+    reference's history map (src/kernel/DEMHistoryMappingKernels.cu).  ``f32`` and ``q_anchor`` (the first step's
+    only) as in ``step_state``.  Returns the final state (pos, q, v, w, family) and the per-step results."""
+    S = dict(S0)
+    prev_keys = prev_hist = None
+    out = []
+    for s, c in enumerate(lists):
+        if s == 0:
+            hist = c["wildcards"].astype(np.float64).T.copy() if c["wildcards"].size else np.zeros((len(c["idA"]), 4))
+        else:
+            k = _keys(c)
+            order = np.argsort(prev_keys, kind="stable")
+            hist = np.zeros((len(k), 4))
+            if len(order):
+                at = np.minimum(np.searchsorted(prev_keys[order], k), len(order) - 1)
+                hit = prev_keys[order][at] == k
+                hist[hit] = prev_hist[order[at[hit]]]
+        r = step_state(built, S, c, hist=hist, mats=mats, f32=f32, q_anchor=q_anchor if s == 0 else None)
+        S = dict(pos=r["pos"], q=r["quat"], v=r["vel"], w=r["angvel"], family=S["family"])
+        prev_keys, prev_hist = _keys(c), r["hist"]
+        out.append(r)
+    return S, out
+

@@ -166,7 +166,7 @@ def test_column_collapse_windows_match_host_adjoint_on_the_gpu_trajectory():
     axis, z0 = init[:, :2].mean(0), float(init[:, 2].min())
     _, gpos = workloads.collapse_loss(pos[:n], axis, z0)
     nO = built.counts["o"]
-    seed = [np.zeros((nO, 3)) for _ in range(3)]
+    seed = [np.zeros((nO, 3)) for _ in range(3)] + [np.zeros((nO, 4))]
     seed[0][:n] = gpos
     worst = np.zeros(4)
     worst_x = 0.0
@@ -178,7 +178,7 @@ def test_column_collapse_windows_match_host_adjoint_on_the_gpu_trajectory():
         if c is not None:
             g.set_contacts({k: c[k] for k in ("idA", "idB", "type", "wildcards")})
         adjoint.record(g, W, W)
-        out = adjoint.backward(g, d_pos=seed[0], d_vel=seed[1], d_angvel=seed[2])
+        out = adjoint.backward(g, d_pos=seed[0], d_vel=seed[1], d_angvel=seed[2], d_quat=seed[3])
         sc, x0, v0, _ = A.from_built(built, state=st)
         w0 = adjoint.world_angular_velocity(st)[:n]
         hc = _host_contacts(c) if c is not None else None
@@ -196,7 +196,7 @@ def test_column_collapse_windows_match_host_adjoint_on_the_gpu_trajectory():
         ex = np.abs(out["d_pos0"][:n] - hx).max() / max(np.abs(hx).max(), 1e-300)
         worst_x = max(worst_x, ex)
         assert ex <= 2e-2, (w, ex)
-        seed = [out["d_pos0"], out["d_vel0"], out["d_angvel0"]]
+        seed = [out["d_pos0"], out["d_vel0"], out["d_angvel0"], out["d_quat0"]]
     r = np.array(ratio_crr)
     assert crr_diff <= 0.5 * crr_host, (crr_diff, crr_host, r)
     print(f"column collapse, 20 windows of 100 steps: largest material-gradient difference (E, CoR, mu, Crr) "
