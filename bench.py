@@ -514,6 +514,9 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint timing on the column collapse")
     ap.add_argument("--adjoint-steps", type=int, default=2000)
     ap.add_argument("--adjoint-checkpoint", type=int, default=100)
+    ap.add_argument("--adjoint-drum-clumps", type=int, default=100_000,
+                    help="clumps of the turning drum whose adjoint is timed beside the column collapse (0: skip)")
+    ap.add_argument("--adjoint-drum-steps", type=int, default=400)
     ap.add_argument("--no-batched", action="store_true", help="skip the packed multi-scene measurement")
     ap.add_argument("--batch-scenes", type=int, default=512)
     ap.add_argument("--batch-steps", type=int, default=1000)
@@ -782,11 +785,51 @@ def adjoint_measure(args, stream):
     t_bwd, out = timed(lambda: adjoint.backward(sa, d_pos=seed))
     nC = sa.num_contacts()
     sa.close()
-    return {"workload": "column collapse: 20,000 spheres r U[2,3] mm released over a floor plane, dt 1e-5, CD every "
-                        "step, contact margin 0", "steps": T, "checkpoint_every": K, "fwd_ms_per_step": t_fwd / T,
-            "record_ms_per_step": t_rec / T, "adjoint_ms_per_step": t_bwd / T, "adjoint_over_forward": t_bwd / t_fwd,
-            "loss": loss, "dL_dE_CoR_mu_Crr": [float(v) for v in out["d_material"][0]], "n_contacts_final": nC,
-            "gradient_precision": "FP64 accumulators, FP32 state"}
+    res = {"workload": "column collapse: 20,000 spheres r U[2,3] mm released over a floor plane, dt 1e-5, CD every "
+                       "step, contact margin 0", "steps": T, "checkpoint_every": K, "fwd_ms_per_step": t_fwd / T,
+           "record_ms_per_step": t_rec / T, "adjoint_ms_per_step": t_bwd / T, "adjoint_over_forward": t_bwd / t_fwd,
+           "loss": loss, "dL_dE_CoR_mu_Crr": [float(v) for v in out["d_material"][0]], "n_contacts_final": nC,
+           "gradient_precision": "FP64 accumulators, FP32 state"}
+    if args.adjoint_drum_clumps > 0:
+        res["drum"] = adjoint_drum_measure(args, stream, timed)
+    return res
+
+
+def adjoint_drum_measure(args, stream, timed):
+    """Adjoint of the turning drum (three-sphere clumps, analytical cylinder and end planes turning at 20 rpm,
+    friction and rolling resistance) from a settled bed: loss = mean clump height after the window; the backward
+    pass (segment recomputation + reverse) against the plain forward window, both timed with CUDA events."""
+    import numpy as np
+    from deme_b200 import Solver, adjoint, workloads
+    built = workloads.drum(n_clumps=args.adjoint_drum_clumps)
+    T, K = args.adjoint_drum_steps, 100
+    s = Solver(built)
+    s.lib.deme_set_streams(s.h, C.c_void_p(stream.cuda_stream), C.c_void_p(stream.cuda_stream))
+    h0 = float(built.params.h)
+    s.set_time_step(2e-5)
+    s.step(15000)
+    s.set_time_step(h0)
+    s.sync()
+    st = {k: v for k, v in s.state().items() if not k.startswith("a")}
+    c = {k: np.array(v, copy=True) for k, v in s.contacts().items() if k in ("idA", "idB", "type", "wildcards")}
+    nC0 = s.num_contacts()
+    adjoint.record(s, 2 * K, K)  # warm-up: allocations and first launches
+    seed = np.zeros((built.counts["o"], 3))
+    seed[:args.adjoint_drum_clumps, 2] = 1.0 / args.adjoint_drum_clumps
+    adjoint.backward(s, d_pos=seed)
+    s.set_state(st)
+    s.set_contacts(c)
+    t_fwd, _ = timed(lambda: s.step(T))
+    s.set_state(st)
+    s.set_contacts(c)
+    t_rec, _ = timed(lambda: adjoint.record(s, T, K))
+    t_bwd, out = timed(lambda: adjoint.backward(s, d_pos=seed))
+    s.close()
+    return {"workload": f"turning drum: {args.adjoint_drum_clumps} three-sphere clumps, analytical cylinder and end "
+                        f"planes at 20 rpm, dt {h0:g}, CD every step, settled 15000 steps at dt 2e-5; loss = mean "
+                        f"clump height", "steps": T, "checkpoint_every": K, "n_contacts": nC0,
+            "fwd_ms_per_step": t_fwd / T, "record_ms_per_step": t_rec / T, "adjoint_ms_per_step": t_bwd / T,
+            "adjoint_over_forward": t_bwd / t_fwd, "dL_dE_CoR_mu_Crr": [float(v) for v in out["d_material"][0]]}
 
 
 def batched_measure(args, stream, rank=0, world=1, dist=None):

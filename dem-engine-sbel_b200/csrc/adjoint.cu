@@ -14,7 +14,7 @@
 //     of its geometry -- sphere centres X + R(q) r of clump members, the wall geometry of planes, cylinders and
 //     cones (adjoint_rigid.cuh), lever arms and their owner-frame images, contact-point velocities R(q) (w x s),
 //     owner-frame torques -- scattered onto both owners' position, velocity, quaternion and angular-velocity
-//     gradients, the gradient of the incoming history, and the
+//     gradients (summed per owner within a warp first), the gradient of the incoming history, and the
 //     material-parameter gradients (FP64 accumulators);
 //   * k_adj_hist_scatter: the history map (src/kernel/DEMHistoryMappingKernels.cu) reversed, so the incoming-history
 //     gradient reaches the previous step's updated history.
@@ -36,6 +36,13 @@
 using namespace deme_b200;
 
 // struct Checkpoint: handle.cuh
+
+// Per material, the terms matProxy2ContactParam (src/kernel/DEMHelperKernels.cu:316-339) combines per pair, in
+// double: E* = 1 / (tE_A + tE_B), G* = 1 / (tG_A + tG_B), the damping ratio beta of a restitution coefficient and
+// its derivative, and the derivatives dE = d tE / d(-E), dG = d tG / d(-E) for the material gradients.
+struct MatAdj {
+    double tE, tG, dE, dG, cor, be, dbe, mu, crr;
+};
 
 struct AdjointTape {
     int K = 0;
@@ -62,7 +69,10 @@ struct AdjointTape {
     uint32_t gCap = 0;
     float4 *gA = nullptr, *gB = nullptr, *gC = nullptr;  // history gradients (current, previous, carried)
     double* gmat = nullptr;                             // nM x 4
+    MatAdj* matAdj = nullptr;                           // nM per-material terms of the pair parameters
     double floors[3] = {1e-4, 1e-4, 1e-6};              // see deme_adjoint_set_floors
+    uint32_t nO = 0;                                    // owners the per-owner buffers are sized for
+    uint32_t maxN = 0;                                  // largest contact count seen at the checkpoints
 };
 
 namespace {
@@ -211,11 +221,63 @@ __device__ __forceinline__ double dbeta_de(double e) {
     return (1.0 / e) * kPi2 / (d * sqrt(d));
 }
 
+__global__ void k_adj_mat_table(MaterialTable m, uint32_t nM, MatAdj* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nM) return;
+    const double E = m.E[i], nu = m.nu[i], cor = m.CoR[i];
+    MatAdj a;
+    a.tE = (1.0 - nu * nu) / E;
+    a.tG = 2.0 * (2.0 - nu) * (1.0 + nu) / E;
+    a.dE = a.tE / E;
+    a.dG = a.tG / E;
+    a.cor = cor;
+    const double le = log(cor > kTiny ? cor : kTiny);
+    a.be = le / sqrt(le * le + kPi2);
+    a.dbe = dbeta_de(cor);
+    a.mu = m.mu[i];
+    a.crr = m.Crr[i];
+    out[i] = a;
+}
+
 // A sphere's offset from its owner as the forward step forms it: rotated in float (rot_f), then added in double.
 __device__ __forceinline__ dv3 sphere_offset(float4 sp, float4 q) {
     float rx = sp.x, ry = sp.y, rz = sp.z;
     rot_f(rx, ry, rz, q.x, q.y, q.z, q.w);
     return mk(rx, ry, rz);
+}
+
+// One side's owner gradients (position 3, velocity 3, owner-frame angular velocity 3, quaternion 4) of every lane of
+// a warp, summed per owner among the lanes that share it (a clump's contacts are adjacent in the list, and its
+// neighbours recur) and added to the accumulators with one set of FP64 atomics per owner.  All 32 lanes call it;
+// `key` is the owner, or kNoOwner for a lane with nothing to add.
+constexpr uint32_t kNoOwner = 0xFFFFFFFFu;
+constexpr int kOwnerGrad = 13;
+__device__ __forceinline__ void warp_owner_add(const double (&v)[kOwnerGrad], uint32_t key, double* sw, double* nlx,
+                                               double* nlv, double* nlw, double* nlq) {
+    const uint32_t lane = threadIdx.x & 31u;
+#pragma unroll
+    for (int c = 0; c < kOwnerGrad; c++) sw[c * 32 + lane] = v[c];
+    __syncwarp();
+    const uint32_t peers = __match_any_sync(0xffffffffu, key);
+    if (key != kNoOwner && lane == (uint32_t)(__ffs(peers) - 1)) {
+        double a[kOwnerGrad];
+#pragma unroll
+        for (int c = 0; c < kOwnerGrad; c++) a[c] = 0.0;
+        for (uint32_t m = peers; m; m &= m - 1u) {
+            const uint32_t b = (uint32_t)(__ffs(m) - 1);
+#pragma unroll
+            for (int c = 0; c < kOwnerGrad; c++) a[c] += sw[c * 32 + b];
+        }
+        add3(nlx, key, mk(a[0], a[1], a[2]));
+        add3(nlv, key, mk(a[3], a[4], a[5]));
+        add3(nlw, key, mk(a[6], a[7], a[8]));
+        add4(nlq, key, dq4{a[9], mk(a[10], a[11], a[12])});
+    }
+    __syncwarp();
+}
+__device__ __forceinline__ void put_owner_grad(double (&v)[kOwnerGrad], dv3 x, dv3 vel, dv3 w, const dq4& q) {
+    v[0] = x.x, v[1] = x.y, v[2] = x.z, v[3] = vel.x, v[4] = vel.y, v[5] = vel.z, v[6] = w.x, v[7] = w.y, v[8] = w.z;
+    v[9] = q.w, v[10] = q.u.x, v[11] = q.u.y, v[12] = q.u.z;
 }
 
 // Per contact of one recorded step: the law's derivative, scattered to both owners and to the material gradients.
@@ -227,17 +289,25 @@ __device__ __forceinline__ dv3 sphere_offset(float4 sp, float4 q) {
 // As the forward step forms them (force_kernel.cuh): the rotational velocity at the contact point is R(q) (w x s)
 // per body, and the owner-frame torques are sA x R(qA)^T (f + t) and sB x R(qB)^T -(f + t) (t: the torque-only
 // force); lT carries the gradients of the owners' summed owner-frame torques.
-__global__ void __launch_bounds__(256) k_adj_contact(SimConsts k, StateView s, const AnalRaw* raw, uint32_t n,
+// 128 threads, 5 blocks per SM: the register cap (102) spills to local memory, which costs less than running one
+// block of 256 per SM at the kernel's natural 255 registers (turning drum, 100k clumps: 0.22 against 0.32 ms per
+// step; 256 x 2 and 256 x 3 gave 0.25 and 0.24).
+constexpr uint32_t kAdjContactThreads = 128;
+__global__ void __launch_bounds__(kAdjContactThreads, 5) k_adj_contact(SimConsts k, StateView s, const MatAdj* matAdj,
+                                                        const AnalRaw* raw, uint32_t n,
                                                      uint32_t nM, const uint32_t* cA, const uint32_t* cB,
                                                      const uint8_t* cT, const float4* cH, const double* X,
                                                      const float4* V, const float4* Q, const float4* W,
                                                      const double* lF, const double* lT, const float4* gHout,
                                                      float4* gHin, double* nlx, double* nlv, double* nlq, double* nlw,
                                                      double* gmat, double3 floors) {
-    extern __shared__ double s_g[];  // nM x (E, CoR, mu, Crr)
+    extern __shared__ double s_g[];  // nM x (E, CoR, mu, Crr), then kOwnerGrad x 32 per warp for warp_owner_add
     for (uint32_t t = threadIdx.x; t < 4u * nM; t += blockDim.x) s_g[t] = 0.0;
+    double* s_w = s_g + 4u * nM + (threadIdx.x >> 5) * (kOwnerGrad * 32);
     __syncthreads();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    double va[kOwnerGrad], vb[kOwnerGrad];
+    uint32_t keyA = kNoOwner, keyB = kNoOwner;
     if (i < n) {
         const uint32_t sA = cA[i], bId = cB[i];
         const bool ss = cT[i] == DEME_SPHERE_SPHERE_CONTACT;
@@ -324,22 +394,16 @@ __global__ void __launch_bounds__(256) k_adj_contact(SimConsts k, StateView s, c
                 in.floor_delta_rel = floors.x;
                 in.floor_roll_speed = floors.y;
                 in.floor_ft = floors.z;
-                const double EA = s.mat.E[matA], EB = s.mat.E[matB], nuA = s.mat.nu[matA], nuB = s.mat.nu[matB];
-                const double invE = (1.0 - nuA * nuA) / EA + (1.0 - nuB * nuB) / EB;
-                in.Es = 1.0 / invE;
-                const double invG = 2.0 * (2.0 - nuA) * (1.0 + nuA) / EA + 2.0 * (2.0 - nuB) * (1.0 + nuB) / EB;
-                in.Gs = 1.0 / invG;
-                const double corA = s.mat.CoR[matA], corB = s.mat.CoR[matB];
-                const double cor = corA < corB ? corA : corB;
-                const uint32_t corSrc = corA < corB ? matA : matB;
-                const double muA = s.mat.mu[matA], muB = s.mat.mu[matB];
-                in.mu = muA > muB ? muA : muB;
-                const uint32_t muSrc = muA > muB ? matA : matB;
-                const double crA = s.mat.Crr[matA], crB = s.mat.Crr[matB];
-                in.crr = crA > crB ? crA : crB;
-                const uint32_t crSrc = crA > crB ? matA : matB;
-                const double le = log(cor > kTiny ? cor : kTiny);
-                in.be = le / sqrt(le * le + kPi2);
+                const MatAdj MA = matAdj[matA], MB = matAdj[matB];
+                in.Es = 1.0 / (MA.tE + MB.tE);
+                in.Gs = 1.0 / (MA.tG + MB.tG);
+                const uint32_t corSrc = MA.cor < MB.cor ? matA : matB;
+                in.be = MA.cor < MB.cor ? MA.be : MB.be;
+                const double dbe = MA.cor < MB.cor ? MA.dbe : MB.dbe;
+                in.mu = MA.mu > MB.mu ? MA.mu : MB.mu;
+                const uint32_t muSrc = MA.mu > MB.mu ? matA : matB;
+                in.crr = MA.crr > MB.crr ? MA.crr : MB.crr;
+                const uint32_t crSrc = MA.crr > MB.crr ? matA : matB;
                 // upstream gradients: forces (world) and owner-frame torques of both owners (driven owners carry 0)
                 const dv3 gFA = ld3(lF, oA), gTA = ld3(lT, oA);
                 const dv3 gFB = ss ? ld3(lF, oB) : mk(0, 0, 0), gTB = ss ? ld3(lT, oB) : mk(0, 0, 0);
@@ -384,36 +448,36 @@ __global__ void __launch_bounds__(256) k_adj_contact(SimConsts k, StateView s, c
                     gcA = g_d;
                     const dv3 gcB = gCP - g_d;
                     // owner B: its position directly and through its sphere centre, its offset's rotation
-                    add3(nlx, oB, gcB - g_rBv);
-                    add3(nlv, oB, G.vB);
-                    add3(nlw, oB, g_wbB);
                     if (spB.x != 0.f || spB.y != 0.f || spB.z != 0.f) gqB += qrot_vjp(qB, mk(spB.x, spB.y, spB.z), gcB);
-                    add4(nlq, oB, gqB);
+                    put_owner_grad(vb, gcB - g_rBv, G.vB, g_wbB, gqB);
+                    keyB = oB;
                 } else {
                     const double g_kk = -dot(gCP, nrm);
                     const dv3 g_n = G.n - kk * gCP;
                     const double g_gap = -0.5 * G.delta + 0.5 * g_kk;
                     gcA = gCP + wall_geom_vjp(wg, g_gap, g_n);
                 }
-                add3(nlx, oA, gcA - g_rAv);
-                add3(nlv, oA, G.vA);
-                add3(nlw, oA, g_wbA);
                 if (spA.x != 0.f || spA.y != 0.f || spA.z != 0.f) gqA += qrot_vjp(qA, mk(spA.x, spA.y, spA.z), gcA);
-                add4(nlq, oA, gqA);
+                put_owner_grad(va, gcA - g_rAv, G.vA, g_wbA, gqA);
+                keyA = oA;
                 gin = make_float4((float)G.dtan.x, (float)G.dtan.y, (float)G.dtan.z, (float)G.tau);
                 // material parameters (matProxy2ContactParam's derivatives)
                 const double Es2 = in.Es * in.Es, Gs2 = in.Gs * in.Gs;
-                atomicAdd(&s_g[4 * matA], G.Es * Es2 * (1.0 - nuA * nuA) / (EA * EA) +
-                                              G.Gs * Gs2 * 2.0 * (2.0 - nuA) * (1.0 + nuA) / (EA * EA));
-                atomicAdd(&s_g[4 * matB], G.Es * Es2 * (1.0 - nuB * nuB) / (EB * EB) +
-                                              G.Gs * Gs2 * 2.0 * (2.0 - nuB) * (1.0 + nuB) / (EB * EB));
-                atomicAdd(&s_g[4 * corSrc + 1], G.be * dbeta_de(cor));
+                atomicAdd(&s_g[4 * matA], G.Es * Es2 * MA.dE + G.Gs * Gs2 * MA.dG);
+                atomicAdd(&s_g[4 * matB], G.Es * Es2 * MB.dE + G.Gs * Gs2 * MB.dG);
+                atomicAdd(&s_g[4 * corSrc + 1], G.be * dbe);
                 atomicAdd(&s_g[4 * muSrc + 2], G.mu);
                 atomicAdd(&s_g[4 * crSrc + 3], G.crr);
             }
         }
         gHin[i] = gin;
     }
+    if (keyA == kNoOwner)
+        for (int c = 0; c < kOwnerGrad; c++) va[c] = 0.0;
+    if (keyB == kNoOwner)
+        for (int c = 0; c < kOwnerGrad; c++) vb[c] = 0.0;
+    warp_owner_add(va, keyA, s_w, nlx, nlv, nlw, nlq);
+    warp_owner_add(vb, keyB, s_w, nlx, nlv, nlw, nlq);
     __syncthreads();
     for (uint32_t t = threadIdx.x; t < 4u * nM; t += blockDim.x)
         if (s_g[t] != 0.0) atomicAdd(&gmat[t], s_g[t]);
@@ -600,7 +664,7 @@ void adjoint_release(deme_handle* h) {
     for (void* p : {(void*)t->X, (void*)t->V, (void*)t->Q, (void*)t->W, (void*)t->Al, (void*)t->cA, (void*)t->cB,
                     (void*)t->cT, (void*)t->cH, (void*)t->cM, (void*)t->lx, (void*)t->lv, (void*)t->lw, (void*)t->nlx,
                     (void*)t->nlv, (void*)t->nlw, (void*)t->lq, (void*)t->nlq, (void*)t->lF, (void*)t->lT,
-                    (void*)t->gA, (void*)t->gB, (void*)t->gC, (void*)t->gmat})
+                    (void*)t->gA, (void*)t->gB, (void*)t->gC, (void*)t->gmat, (void*)t->matAdj})
         dfree(h, p);
     delete t;
     h->adj = nullptr;
@@ -628,20 +692,33 @@ int32_t deme_adjoint_set_floors(deme_handle* h, double overlap_rel, double roll_
 int32_t deme_adjoint_record(deme_handle* h, int32_t n_steps, int32_t checkpoint_every) {
     if (!h || n_steps <= 0 || checkpoint_every <= 0) return DEME_ERR_INVALID;
     TRY(check_adjoint_scene(h));
-    double floors[3] = {1e-4, 1e-4, 1e-6};
-    if (h->adj) std::copy(h->adj->floors, h->adj->floors + 3, floors);
-    adjoint_release(h);
-    h->adj = new AdjointTape();
+    // A tape of the same segment length and owner count is kept with its buffers (the segment records, the pair
+    // pool, the checkpoints): allocating and freeing them at every window would cost more than the window.
+    if (!h->adj || h->adj->K != checkpoint_every || h->adj->nO != h->nO) {
+        double floors[3] = {1e-4, 1e-4, 1e-6};
+        if (h->adj) std::copy(h->adj->floors, h->adj->floors + 3, floors);
+        adjoint_release(h);
+        h->adj = new AdjointTape();
+        std::copy(floors, floors + 3, h->adj->floors);
+        h->adj->K = checkpoint_every;
+        h->adj->nO = h->nO;
+    }
     AdjointTape* t = h->adj;
-    std::copy(floors, floors + 3, t->floors);
-    t->K = checkpoint_every;
     t->nSteps = n_steps;
-    t->cps.resize((size_t)((n_steps + checkpoint_every - 1) / checkpoint_every));
+    const size_t nCp = (size_t)((n_steps + checkpoint_every - 1) / checkpoint_every);
+    for (size_t j = nCp; j < t->cps.size(); j++) free_checkpoint(h, t->cps[j]);
+    t->cps.resize(nCp);
+    t->maxN = 0;
     for (int32_t s = 0; s < n_steps; s++) {
-        if (s % checkpoint_every == 0) TRY(save_checkpoint(h, t->cps[(size_t)(s / checkpoint_every)]));
+        if (s % checkpoint_every == 0) {
+            Checkpoint& c = t->cps[(size_t)(s / checkpoint_every)];
+            TRY(save_checkpoint(h, c));
+            t->maxN = std::max(t->maxN, c.n);
+        }
         TRY(deme_step(h, 1));
     }
     TRY(save_checkpoint(h, t->fin));
+    t->maxN = std::max(t->maxN, t->fin.n);
     CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
     return read_device_errors(h);
 }
@@ -664,6 +741,7 @@ int32_t deme_adjoint_backward(deme_handle* h, const deme_adjoint_seed* seed, dem
         TRY(dalloc_n(h, &t->lq, 4 * (size_t)nO));
         TRY(dalloc_n(h, &t->nlq, 4 * (size_t)nO));
         TRY(dalloc_n(h, &t->gmat, 4 * (size_t)nM));
+        TRY(dalloc_n(h, &t->matAdj, (size_t)nM));
         TRY(dalloc_n(h, &t->X, (size_t)K * nO * 3));
         TRY(dalloc_n(h, &t->V, (size_t)K * nO));
         TRY(dalloc_n(h, &t->Q, (size_t)K * nO));
@@ -671,6 +749,7 @@ int32_t deme_adjoint_backward(deme_handle* h, const deme_adjoint_seed* seed, dem
         TRY(dalloc_n(h, &t->Al, (size_t)K * nO));
     }
     CUDA_TRY(h, cudaMemsetAsync(t->gmat, 0, 4 * (size_t)nM * sizeof(double), st));
+    if (h->nM) k_adj_mat_table<<<nblk(h->nM, 64), 64, 0, st>>>(h->state_view().mat, h->nM, t->matAdj);
     {
         const double* src[4] = {seed ? seed->d_pos : nullptr, seed ? seed->d_vel : nullptr,
                                 seed ? seed->d_angvel : nullptr, seed ? seed->d_quat : nullptr};
@@ -704,6 +783,31 @@ int32_t deme_adjoint_backward(deme_handle* h, const deme_adjoint_seed* seed, dem
         gCap = t->gCap = cap;
         return DEME_OK;
     };
+    {
+        // the pair pool of one segment, sized once from the counts seen at the checkpoints (grown below if a step
+        // holds more)
+        const uint64_t want = std::min<uint64_t>(0xFFFFFFF0ull, (uint64_t)K * t->maxN * 9 / 8 + (uint64_t)K * 1024);
+        if (t->poolCap < want) {
+            dfree(h, t->cA);
+            dfree(h, t->cB);
+            dfree(h, t->cT);
+            dfree(h, t->cH);
+            dfree(h, t->cM);
+            t->cA = t->cB = t->cM = nullptr;
+            t->cT = nullptr;
+            t->cH = nullptr;
+            t->poolCap = 0;
+            TRY(dalloc_n(h, &t->cA, want));
+            TRY(dalloc_n(h, &t->cB, want));
+            TRY(dalloc_n(h, &t->cT, want));
+            TRY(dalloc_n(h, &t->cH, want));
+            TRY(dalloc_n(h, &t->cM, want));
+            t->poolCap = (uint32_t)want;
+        }
+    }
+    const size_t contact_smem = (4 * (size_t)nM + (size_t)kOwnerGrad * kAdjContactThreads) * sizeof(double);
+    if (contact_smem > 48 * 1024)
+        CUDA_TRY(h, cudaFuncSetAttribute(k_adj_contact, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)contact_smem));
     for (int j = nSeg - 1; j >= 0; j--) {
         const Checkpoint& cp = t->cps[(size_t)j];
         const int len = std::min(K, t->nSteps - j * K);
@@ -714,9 +818,12 @@ int32_t deme_adjoint_backward(deme_handle* h, const deme_adjoint_seed* seed, dem
         uint32_t base = 0;
         for (int s = 0; s < len; s++) {
             StateView sv = h->state_view();
-            k_adj_record_state<<<nblk(nO, 256), 256, 0, st>>>(k, sv, nO, t->X + (size_t)s * nO * 3,
+            {
+                ProfScope prof_(KID_ADJ_RECORD, st);
+                k_adj_record_state<<<nblk(nO, 256), 256, 0, st>>>(k, sv, nO, t->X + (size_t)s * nO * 3,
                                                                t->V + (size_t)s * nO, t->Q + (size_t)s * nO,
                                                                t->W + (size_t)s * nO);
+            }
             TRY(deme_detect_contacts(h));
             const uint32_t n = h->nContacts;
             if (base + n > t->poolCap) {  // grow the pool, keeping the steps recorded so far
@@ -752,6 +859,7 @@ int32_t deme_adjoint_backward(deme_handle* h, const deme_adjoint_seed* seed, dem
             }
             const ContactBuf& L = h->lists[h->cur];
             if (n) {
+                ProfScope prof_(KID_ADJ_RECORD, st);
                 CUDA_TRY(h, cudaMemcpyAsync(t->cA + base, L.idA, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
                 CUDA_TRY(h, cudaMemcpyAsync(t->cB + base, L.idB, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
                 CUDA_TRY(h, cudaMemcpyAsync(t->cT + base, L.type, n * sizeof(uint8_t), cudaMemcpyDeviceToDevice, st));
@@ -777,6 +885,7 @@ int32_t deme_adjoint_backward(deme_handle* h, const deme_adjoint_seed* seed, dem
             const Checkpoint& nx = t->cps[(size_t)j + 1];
             const uint32_t n = t->stepN[(size_t)len - 1], b = t->stepBase[(size_t)len - 1];
             if (n) {
+                ProfScope prof_(KID_ADJ_HISTORY, st);
                 k_adj_rekey<<<nblk(n, 256), 256, 0, st>>>(n, t->cA + b, t->cB + b, t->cT + b, nx.off, nx.idB, nx.type,
                                                           nx.n, t->gC, t->gA, h->nS, h->dErr);
                 gOut = t->gA;
@@ -787,14 +896,19 @@ int32_t deme_adjoint_backward(deme_handle* h, const deme_adjoint_seed* seed, dem
             const uint32_t n = t->stepN[(size_t)s], b = t->stepBase[(size_t)s];
             StateView sv = h->state_view();
             const float4 *Qs = t->Q + (size_t)s * nO, *Ws = t->W + (size_t)s * nO;
-            k_adj_integrate<<<nblk(nO, 256), 256, 0, st>>>(sv, nO, h->nClumps, (double)k.h, Qs, Ws,
-                                                            t->Al + (size_t)s * nO, t->lx, t->lv, t->lq, t->lw, t->lF,
-                                                            t->lT, t->nlx, t->nlv, t->nlq, t->nlw);
-            if (n)
-                k_adj_contact<<<nblk(n, 256), 256, 4 * nM * sizeof(double), st>>>(
-                    k, sv, h->analRaw, n, nM, t->cA + b, t->cB + b, t->cT + b, t->cH + b, t->X + (size_t)s * nO * 3,
+            {
+                ProfScope prof_(KID_ADJ_INTEGRATE, st);
+                k_adj_integrate<<<nblk(nO, 256), 256, 0, st>>>(sv, nO, h->nClumps, (double)k.h, Qs, Ws,
+                                                                t->Al + (size_t)s * nO, t->lx, t->lv, t->lq, t->lw,
+                                                                t->lF, t->lT, t->nlx, t->nlv, t->nlq, t->nlw);
+            }
+            if (n) {
+                ProfScope prof_(KID_ADJ_CONTACT, st);
+                k_adj_contact<<<nblk(n, kAdjContactThreads), kAdjContactThreads, contact_smem, st>>>(
+                    k, sv, t->matAdj, h->analRaw, n, nM, t->cA + b, t->cB + b, t->cT + b, t->cH + b, t->X + (size_t)s * nO * 3,
                     t->V + (size_t)s * nO, Qs, Ws, t->lF, t->lT, gOut, t->gB, t->nlx, t->nlv, t->nlq, t->nlw, t->gmat,
                     make_double3(t->floors[0], t->floors[1], t->floors[2]));
+            }
             std::swap(t->lx, t->nlx);
             std::swap(t->lv, t->nlv);
             std::swap(t->lq, t->nlq);
@@ -803,8 +917,10 @@ int32_t deme_adjoint_backward(deme_handle* h, const deme_adjoint_seed* seed, dem
             const uint32_t nPrev = s > 0 ? t->stepN[(size_t)s - 1] : cp.n;
             float4* dst = s > 0 ? t->gA : t->gC;
             if (nPrev) CUDA_TRY(h, cudaMemsetAsync(dst, 0, nPrev * sizeof(float4), st));
-            if (n && nPrev)
+            if (n && nPrev) {
+                ProfScope prof_(KID_ADJ_HISTORY, st);
                 k_adj_hist_scatter<<<nblk(n, 256), 256, 0, st>>>(n, t->cM + b, t->gB, dst, nPrev, h->dErr);
+            }
             gOut = t->gA;
         }
         TRY(check_launch(h, "adjoint"));

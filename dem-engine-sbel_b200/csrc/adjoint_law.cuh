@@ -76,7 +76,7 @@ __device__ __forceinline__ void law_vjp(const LawIn& in, dv3 g_f, dv3 g_t, dv3 g
     // rolling resistance once the contact is older than the collision time
     const double Reff = sqrt(in.Rs);
     const double kns = (4.0 / 3.0) * in.Es * sqrt(Reff);
-    const double gns = -2.0 * sqrt((5.0 / 3.0) * in.meff * in.Es) * in.be * pow(Reff, 0.25);
+    const double gns = -2.0 * sqrt((5.0 / 3.0) * in.meff * in.Es) * in.be * sqrt(sqrt(Reff));  // Reff^(1/4)
     const double dc = gns / (2.0 * sqrt(kns * in.meff));
     bool roll = in.crr > 0.0;
     if (roll && dc < 1.0) {

@@ -215,7 +215,15 @@ __global__ void k_cell_scatter(SimConsts k, StateView s, CDView cd) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= k.n_spheres) return;
     const uint32_t key = cd.cellKey[j];
-    const uint32_t slot = cd.cellStart[key] + atomicSub(&cd.cellCount[key], 1u) - 1u;
+    // one atomic per distinct cell among the warp's spheres (a clump's spheres mostly share a cell); each sphere
+    // then takes its own slot below the value the atomic returned
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t peers = __match_any_sync(__activemask(), key);
+    const uint32_t leader = (uint32_t)(__ffs(peers) - 1);
+    uint32_t top = 0;
+    if (lane == leader) top = atomicSub(&cd.cellCount[key], (uint32_t)__popc(peers));
+    top = __shfl_sync(peers, top, leader);
+    const uint32_t slot = cd.cellStart[key] + top - 1u - (uint32_t)__popc(peers & ((1u << lane) - 1u));
     if (!index_ok(k.err, 1, slot, k.n_spheres)) return;
     write_cell_records(k, s, cd, slot, j);
 }

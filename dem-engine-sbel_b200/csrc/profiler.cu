@@ -18,9 +18,11 @@ std::vector<Pending> g_pending;
 std::vector<cudaEvent_t> g_open;
 double g_ms[KID_COUNT];
 int64_t g_cnt[KID_COUNT];
-const char* g_names[KID_COUNT] = {"place_anal", "sphere_prep", "scan",    "sort_histogram", "sort_onesweep",
-                                  "gather_sorted", "pair_find", "pair_assemble", "pair_overflow", "cell_scatter", "history",        "force",
-                                  "integrate",  "pair_exact", "other"};
+const char* g_names[KID_COUNT] = {"place_anal",    "sphere_prep",   "scan",          "sort_histogram",
+                                  "sort_onesweep", "gather_sorted", "pair_find",     "pair_assemble",
+                                  "pair_overflow", "cell_scatter",  "history",       "force",
+                                  "integrate",     "pair_exact",    "other",         "adj_record",
+                                  "adj_integrate", "adj_contact",   "adj_history"};
 }  // namespace
 
 const char* kernel_name(int id) { return (id >= 0 && id < KID_COUNT) ? g_names[id] : "?"; }

@@ -24,6 +24,10 @@ enum KernelId : int {
     KID_INTEGRATE,
     KID_PAIR_EXACT,
     KID_OTHER,
+    KID_ADJ_RECORD,     // adjoint: per-step records of the recomputed segment (state, accelerations, contact list)
+    KID_ADJ_INTEGRATE,  // adjoint: reverse integration
+    KID_ADJ_CONTACT,    // adjoint: reverse contact law and geometry
+    KID_ADJ_HISTORY,    // adjoint: reverse history map and re-keying at segment boundaries
     KID_COUNT
 };
 
