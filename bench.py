@@ -112,14 +112,11 @@ def algorithmic_bytes(kernel: str, nS: int, nO: int, nC: int, n_cells: int) -> f
         # material (21 B); per owner: voxel, loc, quat, vel+mass, omega, MOI (80 B) + accumulators (32 B)
         return 41.0 * nC + 21.0 * nS + 112.0 * nO
     if kernel == "pair_find":
-        # the candidate scan: per sphere its cell-order float position + id (16 B), its exact record (position,
-        # owner, radius: 32 B) and clump run (8 B); the cell table once; per survivor (about one per contact) its
-        # pool entry (8 B)
-        return 56.0 * nS + 4.0 * n_cells + 8.0 * nC
-    if kernel == "pair_exact":
-        # per sphere its exact record, bin ranges and id (52 B); per pool entry read and rewritten (16 B) and the
-        # count update of a found pair (4 B)
-        return 52.0 * nS + 20.0 * nC
+        # the candidate scan and the exact test of its survivors: per sphere its cell-order float position + id
+        # (16 B), its exact record (position, owner, radius: 32 B), bin ranges + family (16 B), clump run (8 B) and
+        # contact count (4 B); the cell table once; per survivor (about one per contact) its pool entry (8 B) and
+        # the count update of a found pair (4 B)
+        return 76.0 * nS + 4.0 * n_cells + 12.0 * nC
     if kernel == "pair_assemble":
         # scatter: per pair its (A, B) entry (8 B), the count (4 B) and idB written (4 B); assemble: per sphere
         # offsets and analytical count (9 B), per contact idB read and idA, idB, type written (13 B)

@@ -697,7 +697,6 @@ static int32_t cd_search(deme_handle* h, const StateView& s, AnalPlaced* anal, c
     if (retry) launch_cnt_init(k, cd, st);
     launch_pair_find(k, s, cd, h->candCap, h->findShape, st);
     launch_pair_overflow(k, s, cd, h->candCap, st);
-    launch_pair_exact(k, s, cd, h->candCap, h->exactThreads, st);
     TRY(check_launch(h, "contact search"));
     exclusive_scan_u32_onepass(cd.cnt, h->nS + 1, nb.off, nb.dN, h->scratch, h->dErr, st);
     if (hCnt) {
@@ -1326,7 +1325,7 @@ int32_t deme_autotune(deme_handle* h, int32_t steps_per_trial, deme_tuning* out)
     }
     h->forceShape = bestForce;
     const uint32_t threads[] = {128, 512};
-    for (uint32_t* knob : {&h->exactThreads, &h->integrateThreads}) {
+    for (uint32_t* knob : {&h->integrateThreads}) {
         const uint32_t keep = *knob;
         uint32_t pick = keep;
         for (uint32_t t : threads) {

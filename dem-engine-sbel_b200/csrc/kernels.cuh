@@ -62,8 +62,8 @@ struct CDView {
     uint32_t* cellStart;  // nCells + 1
     uint8_t* nAnal;
     uint32_t* cnt;
-    uint2* candTemp;      // pair pool: survivors (cell-order sphere, candidate), then after k_pair_exact the found
-                          // pairs (A, B), A < B by id, or kNoPair; in no particular order
+    uint2* candTemp;      // pair pool: for each survivor of the candidate scan, the exact test's verdict: the
+                          // pair (A, B), A < B by id, or kNoPair; in no particular order
     uint32_t* ovf;        // spheres with more pre-filter survivors than the candidate scan's slots hold
     uint32_t* counters;   // [0] pair-pool entries (survivors) appended, [1] overflow spheres
 };
@@ -107,11 +107,9 @@ int find_shape_count();  // block shapes of the candidate scan
 // warps per block, survivor slots per lane and work-queue (persistent) form of shape v
 void find_shape(int v, uint32_t* warps, uint32_t* slots, bool* persistent);
 void launch_pair_overflow(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, cudaStream_t st);
-void launch_pair_exact(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t tempCap, uint32_t threads,
-                       cudaStream_t st);
 // ranges the wall partials of the force blocks are first summed over (then the range sums, in order)
 constexpr uint32_t kAnalChunks = 32;
-// a pair-pool entry that k_pair_exact rejected
+// a pair-pool entry that the exact test rejected
 constexpr uint32_t kNoPair = 0xFFFFFFFFu;
 void launch_cnt_init(const SimConsts& k, const CDView& cd, cudaStream_t st);
 void launch_pair_scatter(const SimConsts& k, const CDView& cd, const ContactView& c, uint32_t nPairs, uint32_t cap,

@@ -343,8 +343,9 @@ int32_t deme_graph_stats(deme_handle* h, int64_t* replays, int64_t* rollbacks);
 int32_t deme_set_search_shape(deme_handle* h, int32_t shape, float cell_factor);
 int32_t deme_search_shape_count(void);
 /* Block shapes of the other per-step kernels (no reference counterpart): `force_shape` < deme_force_shape_count()
- * (0, the default: 128 threads, 8 blocks per SM; 1: 256 x 4; 2: 64 x 16), and the threads per block of the exact
- * pair test and of the integration (32 to 512, multiples of 32; 256 by default).  They change speed only. */
+ * (0, the default: 128 threads, 8 blocks per SM; 1: 256 x 4; 2: 64 x 16), and the threads per block of the
+ * integration (32 to 512, multiples of 32; 256 by default).  `exact_threads` is checked and kept but no longer used:
+ * the exact pair test runs inside the candidate scan.  They change speed only. */
 int32_t deme_set_kernel_shapes(deme_handle* h, int32_t force_shape, int32_t exact_threads, int32_t integrate_threads);
 int32_t deme_force_shape_count(void);
 
@@ -364,7 +365,7 @@ typedef struct {
 } deme_tuning;
 
 /* Autotuner: times every search shape with cell factors 1, 1.25 and 1.5, then (with the best of those) every force
- * shape, then 128, 256 and 512 threads per block for the exact pair test and for the integration, each trial on
+ * shape, then 128, 256 and 512 threads per block for the integration, each trial on
  * `steps_per_trial` steps (5 when <= 0) from the current state; keeps the fastest, and restores the state and
  * contact history, so the run continues as if it had not been called.  `out` may be NULL. */
 int32_t deme_autotune(deme_handle* h, int32_t steps_per_trial, deme_tuning* out);
