@@ -13,7 +13,7 @@ recorded on the stream the library launches on.  The owner/sphere/contact arrays
 126 MB L2, so no explicit flush is done.  A second short pass brackets every kernel with events to get the
 per-kernel durations that give the roofline of the dominant kernel; an e2e pass goes through the C ABI with a
 pinned host-to-device update of the drum's prescribed rotation and a device-to-host read of the kinetic energy
-every step.
+every step (each step's energy read on the host once the next step is queued).
 
 --impl reference times the reference's CPU path on a bounded sample: its own kernel code compiled for the CPU
 (OpenMP on all host cores) on the shell variant of the drum, since the reference has no analytical cylinder (the C
@@ -665,10 +665,17 @@ def main():
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
+    # every step: its input staged from pinned host memory, and its result (the kinetic energy) copied back and
+    # read on the host; the read of step k waits only for step k, after step k + 1 has been queued
+    prev = None
     for _ in range(args.steps):
         lib.deme_set_family_prescription(s.h, drum_fam, C.byref(presc))
         s.step(1)
-        ke_val = s.kinetic_energy()
+        ticket = s.kinetic_energy_enqueue()
+        if prev is not None:
+            ke_val = s.kinetic_energy_collect(prev)
+        prev = ticket
+    ke_val = s.kinetic_energy_collect(prev)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")

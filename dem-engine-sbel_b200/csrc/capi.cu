@@ -611,6 +611,9 @@ void deme_destroy(deme_handle* h) {
     if (h->hTotal) cudaFreeHost(h->hTotal);
     if (h->hErr) cudaFreeHost(h->hErr);
     if (h->hKE) cudaFreeHost(h->hKE);
+    if (h->hKERing) cudaFreeHost(h->hKERing);
+    for (cudaEvent_t e : h->keDone)
+        if (e) cudaEventDestroy(e);
     if (h->hPresc) cudaFreeHost(h->hPresc);
     for (cudaEvent_t e : h->prescDone)
         if (e) cudaEventDestroy(e);
@@ -1676,6 +1679,42 @@ int32_t deme_kinetic_energy(deme_handle* h, double* ke) {
     CUDA_TRY(h, cudaMemcpyAsync(h->hKE, h->dKE, sizeof(double), cudaMemcpyDeviceToHost, h->st_dt));
     CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
     *ke = *h->hKE;
+    return DEME_OK;
+}
+
+int32_t deme_kinetic_energy_enqueue(deme_handle* h, int64_t* ticket) {
+    if (!h || !ticket) return DEME_ERR_INVALID;
+    if (!h->hKERing) {
+        // the events first: the ring counts as set up (hKERing non-null) only once every slot has its event
+        for (cudaEvent_t& e : h->keDone)
+            if (!e) CUDA_TRY(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        if (!h->dKERing) TRY(dalloc_n(h, &h->dKERing, deme_handle::kKESlots));
+        double* ring = nullptr;
+        CUDA_TRY(h, cudaMallocHost(&ring, deme_handle::kKESlots * sizeof(double)));
+        h->hKERing = ring;
+    }
+    const int64_t t = h->keTickets++;
+    const int slot = (int)(t % deme_handle::kKESlots);
+    // the slot's previous result has landed in host memory before it is reused
+    CUDA_TRY(h, cudaEventSynchronize(h->keDone[slot]));
+    launch_kinetic_energy(h->k, h->state_view(), h->nClumps, h->dKERing + slot, h->st_dt);
+    CUDA_TRY(h, cudaMemcpyAsync(h->hKERing + slot, h->dKERing + slot, sizeof(double), cudaMemcpyDeviceToHost,
+                                h->st_dt));
+    CUDA_TRY(h, cudaEventRecord(h->keDone[slot], h->st_dt));
+    h->keSlotTicket[slot] = t;
+    *ticket = t;
+    return DEME_OK;
+}
+
+int32_t deme_kinetic_energy_collect(deme_handle* h, int64_t ticket, double* ke) {
+    if (!h || !ke || ticket < 0) return DEME_ERR_INVALID;
+    const int slot = (int)(ticket % deme_handle::kKESlots);
+    if (!h->hKERing || h->keSlotTicket[slot] != ticket) {
+        h->err = "deme_kinetic_energy_collect: unknown ticket, or its slot was reused by a later enqueue";
+        return DEME_ERR_STATE;
+    }
+    CUDA_TRY(h, cudaEventSynchronize(h->keDone[slot]));
+    *ke = h->hKERing[slot];
     return DEME_OK;
 }
 

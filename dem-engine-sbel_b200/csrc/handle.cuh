@@ -100,6 +100,13 @@ struct deme_handle {
     uint32_t* hErr = nullptr;
     double* dKE = nullptr;
     double* hKE = nullptr;
+    // ring of kinetic-energy results read without a wait (deme_kinetic_energy_enqueue / _collect)
+    static constexpr int kKESlots = 4;
+    double* dKERing = nullptr;
+    double* hKERing = nullptr;
+    cudaEvent_t keDone[kKESlots] = {};
+    int64_t keSlotTicket[kKESlots] = {-1, -1, -1, -1};
+    int64_t keTickets = 0;
     // pinned staging ring for deme_set_family_prescription: slot i may be rewritten once its copy has run
     static constexpr int kPrescSlots = 8;
     Prescription* hPresc = nullptr;

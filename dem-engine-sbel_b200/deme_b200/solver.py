@@ -256,6 +256,22 @@ class Solver(HandleSolver):
         self._check(self.lib.deme_kinetic_energy(self.h, C.byref(ke)), "kinetic_energy")
         return float(ke.value)
 
+    def kinetic_energy_enqueue(self) -> int:
+        """Queues the kinetic-energy sum after the work queued so far; returns a ticket for kinetic_energy_collect."""
+        t = C.c_int64(0)
+        self.lib.deme_kinetic_energy_enqueue.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+        self.lib.deme_kinetic_energy_enqueue.restype = C.c_int32
+        self._check(self.lib.deme_kinetic_energy_enqueue(self.h, C.byref(t)), "kinetic_energy_enqueue")
+        return int(t.value)
+
+    def kinetic_energy_collect(self, ticket: int) -> float:
+        """Waits for an enqueued kinetic-energy sum and returns it."""
+        ke = C.c_double(0)
+        self.lib.deme_kinetic_energy_collect.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_double)]
+        self.lib.deme_kinetic_energy_collect.restype = C.c_int32
+        self._check(self.lib.deme_kinetic_energy_collect(self.h, int(ticket), C.byref(ke)), "kinetic_energy_collect")
+        return float(ke.value)
+
     def set_time_step(self, h: float):
         self.lib.deme_set_time_step.argtypes = [C.c_void_p, C.c_float]
         self._check(self.lib.deme_set_time_step(self.h, h), "set_time_step")

@@ -420,6 +420,13 @@ int32_t deme_set_time(deme_handle* h, double t, float t_float, int64_t steps);
 /* Sum of 0.5 m v^2 + 0.5 I omega^2 over clump owners (DEMOwnerQueryKernels.cu:10-37 computes the per-owner term;
  * the reference's GetTotalKineticEnergy returns 0, src/DEM/dT.cpp:154-171). */
 int32_t deme_kinetic_energy(deme_handle* h, double* ke);
+/* The same sum without waiting for it (no reference counterpart): _enqueue launches it on the handle's stream after
+ * the work queued so far, copies the result to pinned host memory and returns a ticket; _collect waits for that
+ * copy and returns the value.  Up to 4 results can be outstanding: a fifth enqueue reuses the oldest slot, and
+ * collecting a ticket whose slot was reused returns DEME_ERR_STATE.  A caller that steps and reads the energy every
+ * step can so collect step k's value after queueing step k + 1, keeping the GPU busy while it reads. */
+int32_t deme_kinetic_energy_enqueue(deme_handle* h, int64_t* ticket);
+int32_t deme_kinetic_energy_collect(deme_handle* h, int64_t ticket, double* ke);
 
 /* Bin assignment of the reference (getNumberOfBinsEachSphereTouches / populateBinSphereTouchingPairs, radix sort
  * by bin: src/kernel/DEMBinSphereKernels.cu:12-230, src/algorithms/DEMCubContactDetection.cu:59-129) on the current

@@ -6,6 +6,9 @@
 * Detection every 4 steps: the same, with windows of 4 steps and steps before and after the whole windows.
 * A dense lattice whose first detection finds more pairs than the pair pool holds: the replayed batch is rolled back
   and redone step by step, and the run still equals the plain run.
+* The kinetic energy read without a wait (deme_kinetic_energy_enqueue / _collect), one step behind the stepping
+  as a pipelined caller reads it, equals the blocking read after each step; a ticket whose slot was reused is
+  refused.
 """
 import numpy as np
 import pytest
@@ -88,3 +91,34 @@ def test_pool_overflow_inside_a_window_rolls_back():
     p = run(built, 10, False)
     compare(built, g, p)
     assert g[2][1] >= 1, g[2]
+
+
+def test_kinetic_energy_enqueue_collect_matches_the_blocking_read():
+    from deme_b200 import Solver
+    from deme_b200.solver import DemeError
+    built = workloads.settling_box(n=3000, spacing=2.05, jitter=0.05, seed=4, vel_scale=0.3)
+    ref = Solver(built)
+    want = []
+    for _ in range(6):
+        ref.step(3)
+        want.append(ref.kinetic_energy())
+    ref.close()
+    s = Solver(built)
+    s.set_graph(True)
+    got, prev = [], None
+    for _ in range(6):
+        s.step(3)
+        t = s.kinetic_energy_enqueue()
+        if prev is not None:
+            got.append(s.kinetic_energy_collect(prev))
+        prev = t
+    got.append(s.kinetic_energy_collect(prev))
+    np.testing.assert_allclose(got, want, rtol=1e-6)
+    # five enqueues reuse the first ticket's slot
+    first = s.kinetic_energy_enqueue()
+    for _ in range(4):
+        s.kinetic_energy_enqueue()
+    with pytest.raises(DemeError):
+        s.kinetic_energy_collect(first)
+    s.close()
+
