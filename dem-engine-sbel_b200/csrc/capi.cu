@@ -696,7 +696,8 @@ static int32_t cd_search(deme_handle* h, const StateView& s, AnalPlaced* anal, c
         launch_cell_scatter(k, s, cd, st);  // counting sort and record writes in one pass
     }
     ContactBuf& nb = h->lists[h->cur ^ 1];
-    CUDA_TRY(h, cudaMemsetAsync(cd.counters, 0, 3 * sizeof(uint32_t), st));  // pool, overflow, tile queue
+    // pool, overflow spheres, tile queue, overflow entries
+    CUDA_TRY(h, cudaMemsetAsync(cd.counters, 0, 4 * sizeof(uint32_t), st));
     if (retry) launch_cnt_init(k, cd, st);
     launch_pair_find(k, s, cd, h->candCap, h->findShape, st);
     launch_pair_overflow(k, s, cd, h->candCap, st);

@@ -577,8 +577,10 @@ void launch_pair_find(const SimConsts& k, const StateView& s, const CDView& cd, 
 }
 
 // Spheres whose survivors k_pair_find could not hold: the same forward-half search, one thread per sphere, each
-// survivor tested by the reference predicate and its result appended to the pair pool.  Grid-stride over the
-// device-side overflow count (no host round trip).
+// survivor appended to the pair pool (after every entry of k_pair_find) and counted in counters[3], for
+// k_pair_exact_tail to test one thread per entry.  (Testing them in this kernel, serially per sphere, made a dense
+// start, where many spheres overflow, six times slower.)  Grid-stride over the device-side overflow count (no host
+// round trip).
 template <bool kPacked>
 __global__ void __launch_bounds__(128) k_pair_overflow(SimConsts k, StateView s, CDView cd, uint32_t tempCap) {
     const uint32_t nOvf = *((volatile uint32_t*)&cd.counters[1]);
@@ -597,8 +599,21 @@ __global__ void __launch_bounds__(128) k_pair_overflow(SimConsts k, StateView s,
                                             __ldg(cd.sClump + me.id),
                                    [&](uint32_t j) {
             const uint32_t pos = atomicAdd(&cd.counters[0], 1u);
-            if (pos < tempCap) cd.candTemp[pos] = exact_test(k, s, cd, i, j);
+            atomicAdd(&cd.counters[3], 1u);
+            if (pos < tempCap) cd.candTemp[pos] = make_uint2(i, j);  // tested by k_pair_exact_tail
         });
+    }
+}
+
+// The overflow kernel's entries, the last counters[3] of the pool's counters[0]: the reference predicate, one thread
+// per entry (grid-stride over the device-side counts), each rewritten in place as its verdict.
+__global__ void __launch_bounds__(256) k_pair_exact_tail(SimConsts k, StateView s, CDView cd, uint32_t tempCap) {
+    const uint32_t end = min(*((volatile uint32_t*)&cd.counters[0]), tempCap);
+    const uint32_t nTail = *((volatile uint32_t*)&cd.counters[3]);
+    const uint32_t first = *((volatile uint32_t*)&cd.counters[0]) - nTail;
+    for (uint32_t p = first + blockIdx.x * blockDim.x + threadIdx.x; p < end; p += gridDim.x * blockDim.x) {
+        const uint2 ij = cd.candTemp[p];
+        cd.candTemp[p] = exact_test(k, s, cd, ij.x, ij.y);
     }
 }
 
@@ -609,6 +624,7 @@ void launch_pair_overflow(const SimConsts& k, const StateView& s, const CDView& 
         k_pair_overflow<true><<<148, 128, 0, st>>>(k, s, cd, tempCap);
     else
         k_pair_overflow<false><<<148, 128, 0, st>>>(k, s, cd, tempCap);
+    k_pair_exact_tail<<<4 * (uint32_t)sm_count(), 256, 0, st>>>(k, s, cd, tempCap);
 }
 
 // Presets every sphere's contact count to its number of analytical contacts (k_sphere_prep does the same; this is

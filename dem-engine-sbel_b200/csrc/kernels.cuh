@@ -65,7 +65,8 @@ struct CDView {
     uint2* candTemp;      // pair pool: for each survivor of the candidate scan, the exact test's verdict: the
                           // pair (A, B), A < B by id, or kNoPair; in no particular order
     uint32_t* ovf;        // spheres with more pre-filter survivors than the candidate scan's slots hold
-    uint32_t* counters;   // [0] pair-pool entries (survivors) appended, [1] overflow spheres
+    uint32_t* counters;   // [0] pair-pool entries (survivors) appended, [1] overflow spheres, [2] the candidate
+                          // scan's tile queue, [3] pool entries the overflow search appended (tested last)
 };
 
 // One contact list (kT product) with its history wildcards.

@@ -20,6 +20,8 @@ exact derivatives (floors 0).  Compared: the material gradients (E, CoR, mu, Crr
   different sides within a few steps, so these windows are frictionless: the turning clump drum and a loose clump
   pack.  Central differences at two step sizes are compared where they agree.  Bars: 5e-3 of the largest material
   gradient, 1e-2 of the largest gradient of each state group.
+* Scope: a clump family with only its linear velocity prescribed, and a wall whose family has no prescription (it
+  would move under the contact forces), are refused with DEME_ERR_INVALID and the reason.
 """
 import numpy as np
 import pytest
@@ -149,3 +151,42 @@ def test_frictionless_window_matches_fd_of_fp64_forward(name):
         conv[k] = np.abs(a - b) <= 0.1 * bar * max(np.abs(b).max(), 1e-300)
         assert conv[k].mean() >= 0.75, (k, conv[k].mean())
     _report(name, r, ref, 5e-3, 1e-2, owners=owners, converged=conv)
+
+
+def _pile_with(edit):
+    """A sphere pile scene edited before Initialize (partial prescription, free wall)."""
+    from deme_b200.scene import SceneBuilder, _Prescription
+    rng = np.random.default_rng(1)
+    s = SceneBuilder()
+    s.InstructBoxDomainDimension(0.2, 0.2, 0.2)
+    s.SetCoordSysOrigin("center")
+    m = s.LoadMaterial({"E": 1e7, "nu": 0.3, "CoR": 0.5, "mu": 0.3, "Crr": 0.01})
+    t = s.LoadSphereType(1e-4, 2.5e-3, m)
+    b = s.AddClumps([t] * 27, (rng.uniform(-0.02, 0.02, (27, 3))).astype(np.float32))
+    s.AddBCPlane((0, 0, -0.05), (0, 0, 1), m)
+    edit(s, b, m, _Prescription)
+    s.SetInitTimeStep(1e-5)
+    s.SetCDUpdateFreq(1)
+    return s.Initialize()
+
+
+@pytest.mark.parametrize("case", ["partial_clump_prescription", "free_wall"])
+def test_scope_is_checked(case):
+    from deme_b200 import Solver, adjoint
+    from deme_b200.solver import DemeError
+
+    def partial(s, b, m, P):
+        b.SetFamily(3)
+        s.prescriptions.append(P(3, linVel=["0", "0", "0"], linVelPrescribed=True, rotVelPrescribed=False))
+
+    def free_wall(s, b, m, P):
+        w = s.AddExternalObject()
+        w.AddPlane((0, 0, 0.05), (0, 0, -1), m)
+        w.SetFamily(5)
+
+    built = _pile_with(partial if case == "partial_clump_prescription" else free_wall)
+    g = Solver(built)
+    with pytest.raises(DemeError, match="INVALID.*(partly prescribed|prescribed motion)"):
+        adjoint.record(g, 2, 1)
+    g.close()
+
