@@ -467,6 +467,40 @@ def shell_drum_measure(args, stream):
             "n_spheres": built.n_spheres, "n_contacts": nC, "steps": SHELL_STEPS, "warmup": SHELL_WARMUP}
 
 
+def mesh_drop_measure(args, stream):
+    """Sphere--mesh contacts at scale: a free icosphere of 20,480 facets (radius 0.1 m) driven at 1 m/s into a bed
+    of ``--mesh-spheres`` spheres (r 2 mm, 20 layers) in a box of planes, dt 2e-6, CD every step.  Device time with
+    CUDA events after 200 untimed steps, and the per-kernel split.  The reference detects no sphere--mesh contact,
+    so there is no reference time for this scene."""
+    import numpy as np
+    import torch
+    from deme_b200 import Solver, capi, workloads
+    built = workloads.mesh_ball_drop(n=args.mesh_spheres, ball_radius=0.1, subdivisions=5, layers=20, press=0.5)
+    s = Solver(built)
+    s.lib.deme_set_streams(s.h, C.c_void_p(stream.cuda_stream), C.c_void_p(stream.cuda_stream))
+    s.step(200)
+    s.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    s.step(args.mesh_steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    c = s.contacts()
+    n_mesh = int(np.sum(c["type"] == capi.SPHERE_MESH_CONTACT))
+    split = kernel_breakdown(s, 20)
+    s.close()
+    return {"value": built.n_spheres * args.mesh_steps / (ms / 1e3) / 1e6, "unit": UNIT,
+            "ms_per_step": ms / args.mesh_steps,
+            "workload": f"mesh ball drop: icosphere of {built.info['n_tris']} facets (r 0.1 m, free, 1 m/s) into "
+                        f"{built.n_spheres} spheres (r 2 mm) in a box of 5 planes, dt 2e-6, CD every step",
+            "n_spheres": built.n_spheres, "n_facets": built.info["n_tris"], "n_contacts": len(c["idA"]),
+            "n_sphere_mesh_contacts": n_mesh, "steps": args.mesh_steps, "warmup": 200,
+            "kernel_ms_per_step": {k: round(v, 4) for k, v in sorted(split.items(), key=lambda kv: -kv[1])},
+            "reference": "unavailable: the reference declares the sphere--mesh contact type but detects no such contact"}
+
+
 def cpu_baseline_sample(args):
     from deme_b200 import HandleSolver, capi
     lib_path = os.path.join(ROOT, "oracle", "_build", "libdeme_oracle.so")
@@ -514,6 +548,9 @@ def main():
     ap.add_argument("--adjoint-drum-clumps", type=int, default=100_000,
                     help="clumps of the turning drum whose adjoint is timed beside the column collapse (0: skip)")
     ap.add_argument("--adjoint-drum-steps", type=int, default=400)
+    ap.add_argument("--no-mesh", action="store_true", help="skip the sphere--mesh ball-drop measurement")
+    ap.add_argument("--mesh-spheres", type=int, default=1_000_000)
+    ap.add_argument("--mesh-steps", type=int, default=1000)
     ap.add_argument("--no-batched", action="store_true", help="skip the packed multi-scene measurement")
     ap.add_argument("--batch-scenes", type=int, default=512)
     ap.add_argument("--batch-steps", type=int, default=1000)
@@ -704,6 +741,7 @@ def main():
     wedge = clocked(lambda: hopper_wedge_measure(args, stream)) if (rank == 0 and not args.no_hopper) else None
     ref_wedge = reference_kernels_quick(args, "wedge") if (rank == 0 and not args.no_hopper) else None
     small = clocked(lambda: small_scene_measure(args, stream)) if (rank == 0 and not args.no_small) else None
+    mesh = clocked(lambda: mesh_drop_measure(args, stream)) if (rank == 0 and not args.no_mesh) else None
     # the CPU sample last: its OpenMP threads would otherwise share the host with the GPU sections' host code
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -739,7 +777,7 @@ def main():
                     "d2h_bytes_per_step": 8},
             "gpu_launches": int(launches), "clocks": clocks, "shell_drum": shell, "reference_kernels_shell_drum": ref_shell,
             "hopper": hopper, "hopper_wedge": wedge, "reference_kernels_hopper_wedge": ref_wedge, "small_scene": small,
-            "adjoint": adj, "batched": batched,
+            "adjoint": adj, "batched": batched, "mesh": mesh,
         }
         print(json.dumps(line), flush=True)
     s.close()

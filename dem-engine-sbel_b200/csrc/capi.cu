@@ -157,6 +157,28 @@ static int32_t ensure_cand(deme_handle* h, uint32_t n) {
     return DEME_OK;
 }
 
+// Room for n (cell, facet) entries of the mesh-facet cell lists.
+static int32_t ensure_tri_cells(deme_handle* h, uint32_t n) {
+    if (n <= h->cd.triCellCap && h->cd.triCell) return DEME_OK;
+    const uint32_t cap = std::max<uint32_t>(1024u, (uint32_t)std::min<uint64_t>(0xFFFFFFF0ull, (uint64_t)n * 5 / 4 + 64));
+    dfree(h, h->cd.triCell);
+    h->cd.triCell = nullptr;
+    h->cd.triCellCap = 0;
+    TRY(dalloc_n(h, &h->cd.triCell, cap));
+    h->cd.triCellCap = cap;
+    return DEME_OK;
+}
+
+// A search's counts (total, pool, overflow spheres, -, facet cell entries) fit the buffers it wrote into.
+static bool search_fits(const deme_handle* h, const uint32_t* c) {
+    return c[1] <= h->candCap && (!h->nT || c[4] <= h->cd.triCellCap);
+}
+static int32_t grow_search(deme_handle* h, const uint32_t* c) {
+    TRY(ensure_cand(h, c[1]));
+    if (h->nT) TRY(ensure_tri_cells(h, c[4]));
+    return DEME_OK;
+}
+
 static int32_t ensure_outputs(deme_handle* h, uint32_t n) {
     if (n <= h->outCap) return DEME_OK;
     uint32_t cap = std::max<uint32_t>(1024u, n + n / 4);
@@ -357,6 +379,22 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
             return DEME_ERR_INVALID;
         }
     h->nClumps = nClumps;
+    h->nT = s->n_tris;
+    if (h->nT) {
+        if (s->owner_scene || s->owner_anal_first) {
+            h->err = "mesh facets are not supported together with packed scenes";
+            return DEME_ERR_INVALID;
+        }
+        if (!s->tri_owner || !s->tri_node1 || !s->tri_node2 || !s->tri_node3 || !s->tri_material) {
+            h->err = "n_tris > 0 needs tri_owner, tri_node1..3 and tri_material";
+            return DEME_ERR_INVALID;
+        }
+        for (uint32_t i = 0; i < h->nT; i++)
+            if (s->tri_owner[i] < nClumps || s->tri_owner[i] >= nO || s->tri_material[i] >= std::max(nM, 1u)) {
+                h->err = "mesh facet owner (must follow the clump owners) or material out of range";
+                return DEME_ERR_INVALID;
+            }
+    }
     CUDA_TRY(h, cudaStreamCreateWithFlags(&h->own_dt, cudaStreamNonBlocking));
     CUDA_TRY(h, cudaStreamCreateWithFlags(&h->own_kt, cudaStreamNonBlocking));
     h->st_dt = h->own_dt;
@@ -381,6 +419,7 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
     k.n_spheres = nS;
     k.n_owners = nO;
     k.n_anal = nA;
+    k.n_tris = h->nT;
     float rmax = 0.f;
     for (uint32_t i = 0; i < nS; i++) {
         float r = s->radius[i];
@@ -509,6 +548,24 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
             raw[a] = r;
         }
         CUDA_TRY(h, cudaMemcpy(h->analRaw, raw.data(), raw.size() * sizeof(AnalRaw), cudaMemcpyHostToDevice));
+        if (h->nT) {
+            std::vector<TriRaw> tr(h->nT);
+            for (uint32_t i = 0; i < h->nT; i++) {
+                TriRaw t{};
+                const float *a = s->tri_node1 + 3 * (size_t)i, *b = s->tri_node2 + 3 * (size_t)i,
+                            *c = s->tri_node3 + 3 * (size_t)i;
+                t.n1x = a[0], t.n1y = a[1], t.n1z = a[2];
+                t.n2x = b[0], t.n2y = b[1], t.n2z = b[2];
+                t.n3x = c[0], t.n3y = c[1], t.n3z = c[2];
+                t.owner = s->tri_owner[i];
+                t.mass = s->mass[t.owner];
+                t.material = s->tri_material[i];
+                tr[i] = t;
+            }
+            TRY(dalloc_n(h, &h->triRaw, h->nT));
+            TRY(dalloc_n(h, &h->triPlaced, h->nT));
+            CUDA_TRY(h, cudaMemcpy(h->triRaw, tr.data(), tr.size() * sizeof(TriRaw), cudaMemcpyHostToDevice));
+        }
         std::vector<Prescription> pr(DEME_NUM_FAMILIES);
         for (int f = 0; f < DEME_NUM_FAMILIES; f++) {
             Prescription q{};
@@ -562,8 +619,15 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
     // cnt[nS] stays 0 so the scan over nS + 1 entries leaves the total in off[nS]
     CUDA_TRY(h, cudaMemset(cd.cnt, 0, ((size_t)nS + 1) * sizeof(uint32_t)));
     TRY(dalloc_n(h, &cd.ovf, nS + 1));
-    TRY(dalloc_n(h, &cd.counters, 4));
+    TRY(dalloc_n(h, &cd.counters, 8));
+    CUDA_TRY(h, cudaMemset(cd.counters, 0, 8 * sizeof(uint32_t)));
     TRY(ensure_cand(h, std::max<uint32_t>(1024u, 2u * nS)));
+    if (h->nT) {
+        TRY(dalloc_n(h, &cd.triCellCount, (size_t)h->nCells + 1));
+        TRY(dalloc_n(h, &cd.triCellStart, (size_t)h->nCells + 1));
+        TRY(dalloc_n(h, &cd.nMesh, std::max(nS, 1u)));
+        TRY(ensure_tri_cells(h, std::max<uint32_t>(1024u, 8u * h->nT)));
+    }
     for (int b = 0; b < 2; b++) {
         TRY(dalloc_n(h, &h->lists[b].off, (size_t)nS + 1));
         CUDA_TRY(h, cudaMemset(h->lists[b].off, 0, ((size_t)nS + 1) * sizeof(uint32_t)));
@@ -578,7 +642,7 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
     h->k.err = h->dErr;
     TRY(dalloc_n(h, &h->dKE, 2));
     CUDA_TRY(h, cudaMemset(h->dErr, 0, 4 * sizeof(uint32_t)));
-    CUDA_TRY(h, cudaMallocHost(&h->hTotal, 4 * sizeof(uint32_t)));
+    CUDA_TRY(h, cudaMallocHost(&h->hTotal, 8 * sizeof(uint32_t)));
     CUDA_TRY(h, cudaMallocHost(&h->hErr, 4 * sizeof(uint32_t)));
     CUDA_TRY(h, cudaMallocHost(&h->hKE, 2 * sizeof(double)));
     *h->hErr = 0;
@@ -677,15 +741,25 @@ int32_t deme_keep_contact_forces(deme_handle* h, int32_t enable) {
 
 // ---------------------------------------------------------------------------------------------------- kT ----
 // Contact search up to the per-sphere offsets of the new list (into lists[cur ^ 1].off, its count into .dN), for the
-// poses in `s`, with the analytical components placed into `anal`.  The pair total, the pool count and its overflow
-// counter are copied to `hCnt` (pinned, unless null) at the end, on `st`; nothing here waits for the device.
+// poses in `s`, with the analytical components placed into `anal` (and the mesh facets into s.tri).  The pair total,
+// the pool count, its overflow counter and the facet cell-list total are copied to `hCnt` (pinned, unless null;
+// words 0, 1, 2 and 4) at the end, on `st`; nothing here waits for the device.
 static int32_t cd_search(deme_handle* h, const StateView& s, AnalPlaced* anal, cudaStream_t st, bool retry,
                          uint32_t* hCnt) {
     const SimConsts& k = h->k;
     CDView& cd = h->cd;
     launch_place_anal(k, s, h->analRaw, anal, h->nA, st);
+    launch_place_tri(k, s, h->triRaw, st);
     // the forces of this step, on the same poses, reuse the placement
     if (anal == h->analPlaced) h->analFresh = true;
+    if (h->nT) {
+        // cell lists of the mesh facets: counts, offsets (total in counters[4]), entries
+        CUDA_TRY(h, cudaMemsetAsync(cd.triCellCount, 0, ((size_t)h->nCells + 1) * sizeof(uint32_t), st));
+        launch_tri_bin(k, s, cd, false, st);
+        exclusive_scan_u32_onepass(cd.triCellCount, h->nCells + 1, cd.triCellStart, cd.counters + 4, h->scratch,
+                                   h->dErr, st);
+        launch_tri_bin(k, s, cd, true, st);
+    }
     CUDA_TRY(h, cudaMemsetAsync(cd.cellCount, 0, ((size_t)h->nCells + 1) * sizeof(uint32_t), st));
     launch_sphere_prep(k, s, cd, st);
     exclusive_scan_u32_onepass(cd.cellCount, h->nCells + 1, cd.cellStart, nullptr, h->scratch, h->dErr, st);
@@ -705,6 +779,7 @@ static int32_t cd_search(deme_handle* h, const StateView& s, AnalPlaced* anal, c
     exclusive_scan_u32_onepass(cd.cnt, h->nS + 1, nb.off, nb.dN, h->scratch, h->dErr, st);
     if (hCnt) {
         CUDA_TRY(h, cudaMemcpyAsync(hCnt + 1, cd.counters, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        if (h->nT) CUDA_TRY(h, cudaMemcpyAsync(hCnt + 4, cd.counters + 4, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         CUDA_TRY(h, cudaMemcpyAsync(hCnt, nb.dN, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     }
     return DEME_OK;
@@ -750,11 +825,11 @@ static int32_t cd_sync(deme_handle* h) {
         TRY(cd_search(h, s, h->analPlaced, st, attempt > 0, h->hTotal));
         CUDA_TRY(h, cudaStreamSynchronize(st));
         n = h->hTotal[0];
-        if (h->hTotal[1] <= h->candCap) break;
-        // the pair list outgrew its buffer: grow and search again
-        TRY(ensure_cand(h, h->hTotal[1]));
+        if (search_fits(h, h->hTotal)) break;
+        // the pair list (or a facet cell list) outgrew its buffer: grow and search again
+        TRY(grow_search(h, h->hTotal));
     }
-    if (h->hTotal[1] > h->candCap) {
+    if (!search_fits(h, h->hTotal)) {
         h->err = "contact search: pair list still over capacity after growing";
         return DEME_ERR_OVERFLOW;
     }
@@ -769,7 +844,8 @@ static int32_t ensure_async(deme_handle* h) {
     TRY(dalloc_n(h, &h->kLoc, std::max(h->nO, 1u)));
     TRY(dalloc_n(h, &h->kQuat, std::max(h->nO, 1u)));
     TRY(dalloc_n(h, &h->kAnalPlaced, std::max(h->nA, 1u)));
-    CUDA_TRY(h, cudaMallocHost(&h->hCounts, 4 * sizeof(uint32_t)));
+    if (h->nT) TRY(dalloc_n(h, &h->kTriPlaced, h->nT));
+    CUDA_TRY(h, cudaMallocHost(&h->hCounts, 8 * sizeof(uint32_t)));
     CUDA_TRY(h, cudaEventCreateWithFlags(&h->evPose, cudaEventDisableTiming));
     CUDA_TRY(h, cudaEventCreateWithFlags(&h->evCounts, cudaEventDisableTiming));
     CUDA_TRY(h, cudaEventCreateWithFlags(&h->evListReady, cudaEventDisableTiming));
@@ -805,12 +881,12 @@ static int32_t cd_finish(deme_handle* h) {
     cudaStream_t kt = h->st_kt;
     CUDA_TRY(h, cudaEventSynchronize(h->evCounts));
     const StateView ks = h->kt_view();
-    if (h->hCounts[1] > h->candCap) {
+    if (!search_fits(h, h->hCounts)) {
         // pool overflow: grow and search the same snapshot again (it is untouched until the next detection)
-        TRY(ensure_cand(h, h->hCounts[1]));
+        TRY(grow_search(h, h->hCounts));
         TRY(cd_search(h, ks, h->kAnalPlaced, kt, true, h->hCounts));
         CUDA_TRY(h, cudaStreamSynchronize(kt));
-        if (h->hCounts[1] > h->candCap) {
+        if (!search_fits(h, h->hCounts)) {
             h->err = "contact search: pair list still over capacity after growing";
             return DEME_ERR_OVERFLOW;
         }
@@ -856,7 +932,10 @@ int32_t deme_compute_forces(deme_handle* h) {
     cudaStream_t st = h->st_dt;
     const SimConsts& k = h->k;
     StateView s = h->state_view();
-    if (!h->analFresh) launch_place_anal(k, s, h->analRaw, h->analPlaced, h->nA, st);
+    if (!h->analFresh) {
+        launch_place_anal(k, s, h->analRaw, h->analPlaced, h->nA, st);
+        launch_place_tri(k, s, h->triRaw, st);
+    }
     h->analFresh = false;
     // prepareForceArrays (src/kernel/DEMPrepForceKernels.cu:23-31): accumulators start from zero every step
     CUDA_TRY(h, cudaMemsetAsync(h->acc, 0, h->nO * sizeof(float4), st));
@@ -1377,7 +1456,8 @@ int32_t deme_step(deme_handle* h, int32_t n_steps) {
     // rules and expressions read the time on the device: start it from the host's (a kernel argument, so no
     // staging buffer is read after this call returns)
     if (needs_device_time(h)) launch_set_time(h->dTime, h->tf, h->st_dt);
-    if (h->useGraph && h->cdLag == 0 && !prof_timing()) {
+    // (scenes with mesh facets step without graphs: their cell lists may need to grow inside a window)
+    if (h->useGraph && h->cdLag == 0 && h->nT == 0 && !prof_timing()) {
         TRY(step_graph(h, n_steps));
     } else {
         for (int32_t i = 0; i < n_steps; i++) TRY(step_plain(h));
@@ -1536,17 +1616,22 @@ int32_t deme_upload_contacts(deme_handle* h, const deme_contacts* in) {
     TRY(cd_cancel(h));
     const uint32_t n = in->n_contacts;
     for (uint32_t i = 0; i < n; i++) {
-        const bool ss = in->type[i] == DEME_SPHERE_SPHERE_CONTACT;
-        if (in->idA[i] >= h->nS || (ss && in->idB[i] >= h->nS) || (!ss && in->idB[i] >= h->nA)) {
+        const uint8_t t = in->type[i];
+        const uint32_t limB = t == DEME_SPHERE_SPHERE_CONTACT ? h->nS : (t == DEME_SPHERE_MESH_CONTACT ? h->nT : h->nA);
+        if (t == DEME_NOT_A_CONTACT || t > DEME_SPHERE_CONE_CONTACT) {
+            h->err = "contact type out of range";
+            return DEME_ERR_INVALID;
+        }
+        if (in->idA[i] >= h->nS || in->idB[i] >= limB) {
             h->err = "contact ids out of range";
             return DEME_ERR_INVALID;
         }
     }
-    // canonical order: (idA, group, idB), group 0 = sphere--analytical
+    // canonical order: (idA, group, idB), groups sphere--analytical, sphere--mesh, sphere--sphere
     std::vector<uint32_t> perm(n);
     std::iota(perm.begin(), perm.end(), 0u);
     std::stable_sort(perm.begin(), perm.end(), [&](uint32_t a, uint32_t b) {
-        const uint32_t ga = in->type[a] == DEME_SPHERE_SPHERE_CONTACT, gb = in->type[b] == DEME_SPHERE_SPHERE_CONTACT;
+        const uint32_t ga = contact_group(in->type[a]), gb = contact_group(in->type[b]);
         if (in->idA[a] != in->idA[b]) return in->idA[a] < in->idA[b];
         if (ga != gb) return ga < gb;
         return in->idB[a] < in->idB[b];

@@ -53,6 +53,7 @@ struct SimConsts {
     float G[3];
     int integrator;
     uint32_t n_spheres, n_owners, n_anal;
+    uint32_t n_tris;  // mesh facets (sphere--mesh contacts); 0: none
     // contact-detection search grids: one per scene (several only when independent scenes are packed into one
     // run), each a block of cells in the cell arrays; ownerScene maps an owner to its scene (null: one scene, whose
     // grid is also held here by value, grid0, so that a plain run reads it from the kernel parameters)
@@ -86,6 +87,16 @@ struct AnalPlaced {
     uint16_t material;
     float mass;
     double size1, c1, c2, umin, umax;  // cylinder radius / cone (sin, cos, axial range)
+};
+
+// Mesh facet (triangle) placed in the world for the current state: vertices = owner position (double) + the owner
+// frame vertex rotated in float (as the analytical components are placed).
+struct TriPlaced {
+    double ax, ay, az, bx, by, bz, cx, cy, cz;
+    uint32_t owner;
+    uint16_t material;
+    uint16_t pad;
+    float mass;  // the owner's mass
 };
 
 // ---------------- saturating conversions (cvt.rzi semantics, NaN -> 0) ----------------
@@ -304,6 +315,104 @@ __device__ __forceinline__ int anal_overlap_dt(const AnalPlaced& a, double xA, d
         return a.type == DEME_ANAL_CYLINDER ? DEME_SPHERE_CYLINDER_CONTACT : DEME_SPHERE_CONE_CONTACT;
     }
     return DEME_NOT_A_CONTACT;
+}
+
+// Group of a contact type inside one sphere's segment of the contact list: sphere--analytical (0), sphere--mesh (1),
+// sphere--sphere (2).  Segments are sorted by (group, idB).
+__host__ __device__ __forceinline__ uint32_t contact_group(uint32_t type) {
+    return type == DEME_SPHERE_SPHERE_CONTACT ? 2u : (type == DEME_SPHERE_MESH_CONTACT ? 1u : 0u);
+}
+
+// Sphere--mesh contact geometry (no reference counterpart: the reference declares the sphere--mesh contact type but
+// has no detection for it).  The point of the triangle closest to the sphere centre p, by the region tests of
+// Ericson's closest-point-on-triangle algorithm (Real-Time Collision Detection, 5.1.5), in double: the triangle is
+// two-sided, and each triangle a sphere overlaps is one contact.  Contact-detection form: the distance to that point
+// at most the reach.  Dynamics form, with the plane's conventions (anal_overlap_dt): gap = the distance,
+// half the overlap as the depth, the normal from the closest point to the centre (float, normalised in float as the
+// sphere pair's), the contact point p - n (gap + depth), the contact-detection reach the expanded radius plus the
+// margin beta (as for an analytical component).  A centre exactly on the triangle takes the face normal
+// a->b x a->c.
+__device__ __forceinline__ void tri_closest(const TriPlaced& t, double px, double py, double pz, double& qx, double& qy,
+                                            double& qz) {
+    const double abx = t.bx - t.ax, aby = t.by - t.ay, abz = t.bz - t.az;
+    const double acx = t.cx - t.ax, acy = t.cy - t.ay, acz = t.cz - t.az;
+    const double apx = px - t.ax, apy = py - t.ay, apz = pz - t.az;
+    const double d1 = abx * apx + aby * apy + abz * apz, d2 = acx * apx + acy * apy + acz * apz;
+    if (d1 <= 0.0 && d2 <= 0.0) {
+        qx = t.ax, qy = t.ay, qz = t.az;
+        return;
+    }
+    const double bpx = px - t.bx, bpy = py - t.by, bpz = pz - t.bz;
+    const double d3 = abx * bpx + aby * bpy + abz * bpz, d4 = acx * bpx + acy * bpy + acz * bpz;
+    if (d3 >= 0.0 && d4 <= d3) {
+        qx = t.bx, qy = t.by, qz = t.bz;
+        return;
+    }
+    const double vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) {
+        const double v = d1 / (d1 - d3);
+        qx = t.ax + v * abx, qy = t.ay + v * aby, qz = t.az + v * abz;
+        return;
+    }
+    const double cpx = px - t.cx, cpy = py - t.cy, cpz = pz - t.cz;
+    const double d5 = abx * cpx + aby * cpy + abz * cpz, d6 = acx * cpx + acy * cpy + acz * cpz;
+    if (d6 >= 0.0 && d5 <= d6) {
+        qx = t.cx, qy = t.cy, qz = t.cz;
+        return;
+    }
+    const double vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) {
+        const double w = d2 / (d2 - d6);
+        qx = t.ax + w * acx, qy = t.ay + w * acy, qz = t.az + w * acz;
+        return;
+    }
+    const double va = d3 * d6 - d5 * d4;
+    if (va <= 0.0 && (d4 - d3) >= 0.0 && (d5 - d6) >= 0.0) {
+        const double w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        qx = t.bx + w * (t.cx - t.bx), qy = t.by + w * (t.cy - t.by), qz = t.bz + w * (t.cz - t.bz);
+        return;
+    }
+    const double denom = 1.0 / (va + vb + vc);
+    const double v = vb * denom, w = vc * denom;
+    qx = t.ax + abx * v + acx * w, qy = t.ay + aby * v + acy * w, qz = t.az + abz * v + acz * w;
+}
+__device__ __forceinline__ double tri_dist2(const TriPlaced& t, double px, double py, double pz, double& qx, double& qy,
+                                            double& qz) {
+    tri_closest(t, px, py, pz, qx, qy, qz);
+    return (px - qx) * (px - qx) + (py - qy) * (py - qy) + (pz - qz) * (pz - qz);
+}
+// radA: the sphere's radius + beta; the facet, like an analytical component, adds the margin beta4 once more
+__device__ __forceinline__ bool tri_overlap_cd(const TriPlaced& t, double px, double py, double pz, double radA,
+                                               float beta4) {
+    double qx, qy, qz;
+    const double reach = radA + (double)beta4;
+    return tri_dist2(t, px, py, pz, qx, qy, qz) <= reach * reach;
+}
+__device__ __forceinline__ bool tri_overlap_dt(const TriPlaced& t, double xA, double yA, double zA, double radA,
+                                               double& CPX, double& CPY, double& CPZ, float& nX, float& nY, float& nZ,
+                                               double& depth) {
+    double qx, qy, qz;
+    const double d2 = tri_dist2(t, xA, yA, zA, qx, qy, qz);
+    const double gap = sqrt(d2);
+    const double od = (radA - gap) / 2.0;
+    if (od < 0.0) return false;
+    if (gap > 0.0) {
+        nX = (float)(xA - qx);
+        nY = (float)(yA - qy);
+        nZ = (float)(zA - qz);
+    } else {
+        const double abx = t.bx - t.ax, aby = t.by - t.ay, abz = t.bz - t.az;
+        const double acx = t.cx - t.ax, acy = t.cy - t.ay, acz = t.cz - t.az;
+        nX = (float)(aby * acz - abz * acy);
+        nY = (float)(abz * acx - abx * acz);
+        nZ = (float)(abx * acy - aby * acx);
+    }
+    normalize_f(nX, nY, nZ);
+    depth = od;
+    CPX = xA - (double)nX * (gap + od);
+    CPY = yA - (double)nY * (gap + od);
+    CPZ = zA - (double)nZ * (gap + od);
+    return true;
 }
 
 // Device error word bits (read by the host once per step; kernels never trap).

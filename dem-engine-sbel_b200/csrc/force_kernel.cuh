@@ -45,8 +45,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_force(SimConsts k, Sta
     if (valid) {
         const int ct0 = c.type[i];
         ids_ok = index_ok(k.err, 8, c.idA[i], k.n_spheres) &&
-                 index_ok(k.err, 9, c.idB[i], ct0 == DEME_SPHERE_SPHERE_CONTACT ? k.n_spheres : k.n_anal) &&
-                 index_ok(k.err, 10, ct0 == DEME_SPHERE_SPHERE_CONTACT || ct0 >= 3 ? 0 : 1, 1);
+                 index_ok(k.err, 9, c.idB[i],
+                          ct0 == DEME_SPHERE_SPHERE_CONTACT ? k.n_spheres
+                                                            : (ct0 == DEME_SPHERE_MESH_CONTACT ? k.n_tris : k.n_anal)) &&
+                 index_ok(k.err, 10, ct0 == DEME_NOT_A_CONTACT || ct0 > DEME_SPHERE_CONE_CONTACT ? 1 : 0, 1);
     }
     if (ids_ok) {
         const uint32_t sA = c.idA[i];
@@ -113,6 +115,23 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_force(SimConsts k, Sta
                 CPy = By + (radB - depth / 2.0) * (double)nY;
                 CPz = Bz + (radB - depth / 2.0) * (double)nZ;
             }
+        } else if (ct == DEME_SPHERE_MESH_CONTACT) {
+            // a mesh facet: a wall-like body B (huge radius) on the facet's owner
+            const TriPlaced t = s.tri[bId];
+            oB = t.owner;
+            const ushort4 lB = s.loc[oB];
+            qB = s.quat[oB];
+            const float4 vB = s.vel[oB];
+            const float4 wB = s.omg[oB];
+            voxel_to_pos(k, s.voxel[oB], lB.x, lB.y, lB.z, BOx, BOy, BOz);
+            RB = rot_matrix(qB.x, qB.y, qB.z, qB.w);
+            g.BRadius = (float)kHugeFloat;
+            g.BOwnerMass = t.mass;
+            g.matB = t.material;
+            g.BLinVel = make_float3(vB.x, vB.y, vB.z);
+            g.BRotVel = make_float3(wB.x, wB.y, wB.z);
+            if (!tri_overlap_dt(t, Ax, Ay, Az, (double)g.ARadius, CPx, CPy, CPz, nX, nY, nZ, depth))
+                ct = DEME_NOT_A_CONTACT;
         } else {
             const AnalPlaced a = s.anal[bId];
             oB = a.owner;

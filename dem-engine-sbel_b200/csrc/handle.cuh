@@ -73,6 +73,9 @@ struct deme_handle {
     bool analFresh = false;  // analPlaced holds the placement for the current poses (a detection of this step made it)
     Prescription* presc = nullptr;
     uint2* ownerAnal = nullptr;  // packed scenes: per owner (first, count) of its analytical components
+    uint32_t nT = 0;             // mesh facets
+    TriRaw* triRaw = nullptr;
+    TriPlaced* triPlaced = nullptr;  // placed with analPlaced (analFresh covers both)
     // contact detection
     CDView cd{};
     uint32_t nCells = 0;
@@ -155,7 +158,9 @@ struct deme_handle {
     ushort4* kLoc = nullptr;
     float4* kQuat = nullptr;
     AnalPlaced* kAnalPlaced = nullptr;  // analytical components placed from that snapshot
-    uint32_t* hCounts = nullptr;        // pinned: total, pool count, device error word, copied at the end of kT's part
+    TriPlaced* kTriPlaced = nullptr;    // mesh facets placed from that snapshot
+    uint32_t* hCounts = nullptr;        // pinned: total, pool count, overflow spheres, -, facet cell entries,
+                                        // copied at the end of kT's part (8 words)
     cudaEvent_t evPose = nullptr, evCounts = nullptr, evListReady = nullptr, evListReleased = nullptr;
     StateView kt_view() const {
         StateView s = state_view();
@@ -163,6 +168,7 @@ struct deme_handle {
         s.loc = kLoc;
         s.quat = kQuat;
         s.anal = kAnalPlaced;
+        s.tri = kTriPlaced;
         return s;
     }
 
@@ -186,6 +192,7 @@ struct deme_handle {
         s.nA = nA;
         s.presc = presc;
         s.ownerAnal = ownerAnal;
+        s.tri = triPlaced;
         return s;
     }
 };

@@ -106,11 +106,126 @@ void launch_place_anal(const SimConsts& k, const StateView& s, const AnalRaw* ra
     if (nA) k_place_anal<<<blocks_for(nA, 64), 64, 0, st>>>(k, s, raw, placed, nA);
 }
 
+// Mesh facets placed at the current poses (as k_place_anal places the analytical components): each node rotated
+// by the owner's orientation in float, added to the owner position in double.
+__global__ void k_place_tri(SimConsts k, StateView s, const TriRaw* raw, uint32_t nT) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nT) return;
+    const TriRaw r = raw[i];
+    const uint32_t o = r.owner;
+    const ushort4 l = s.loc[o];
+    const float4 q = s.quat[o];
+    double ox, oy, oz;
+    voxel_to_pos(k, s.voxel[o], l.x, l.y, l.z, ox, oy, oz);
+    float ax = r.n1x, ay = r.n1y, az = r.n1z, bx = r.n2x, by = r.n2y, bz = r.n2z, cx = r.n3x, cy = r.n3y, cz = r.n3z;
+    rot_f(ax, ay, az, q.x, q.y, q.z, q.w);
+    rot_f(bx, by, bz, q.x, q.y, q.z, q.w);
+    rot_f(cx, cy, cz, q.x, q.y, q.z, q.w);
+    TriPlaced t;
+    t.ax = ox + (double)ax;
+    t.ay = oy + (double)ay;
+    t.az = oz + (double)az;
+    t.bx = ox + (double)bx;
+    t.by = oy + (double)by;
+    t.bz = oz + (double)bz;
+    t.cx = ox + (double)cx;
+    t.cy = oy + (double)cy;
+    t.cz = oz + (double)cz;
+    t.owner = o;
+    t.material = r.material;
+    t.pad = 0;
+    t.mass = r.mass;
+    s.tri[i] = t;
+}
+
+void launch_place_tri(const SimConsts& k, const StateView& s, const TriRaw* raw, cudaStream_t st) {
+    if (!(k.n_tris)) return;
+    ProfScope prof_(KID_PLACE_ANAL, st);
+    k_place_tri<<<blocks_for(k.n_tris, 64), 64, 0, st>>>(k, s, raw, k.n_tris);
+}
+
+// Cell lists of the mesh facets, one warp per facet.  A sphere in cell c can touch facet t only if its centre lies
+// within the reach (largest expanded radius + beta) of t, so t is listed in every cell whose box comes that close:
+// the cells of t's reach box, less those whose box (open to the outside at the grid's faces, where cell_of clamps,
+// and cut to the reach box) has its centre farther from t than the reach plus its half diagonal.  Each sphere then
+// tests the facets of its home cell only, so every (sphere, facet) pair is met once.  kEmit false: counts per cell;
+// true: the entries, at start + the count taken down (the order inside a cell is not defined; the assembly sorts
+// by facet id).  Entries past the capacity are dropped and their total, read by the host, makes it grow the list.
+template <bool kEmit>
+__global__ void __launch_bounds__(128) k_tri_bin(SimConsts k, StateView s, CDView cd) {
+    const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (t >= k.n_tris) return;
+    const TriPlaced tp = s.tri[t];
+    const SearchGrid& g = k.grid0;
+    const double cs = 1.0 / g.inv_cell;
+    const double reach = (double)k.r_max_cd + (double)k.beta + 1e-6 * cs;
+    const double lo[3] = {fmin(tp.ax, fmin(tp.bx, tp.cx)) - reach, fmin(tp.ay, fmin(tp.by, tp.cy)) - reach,
+                          fmin(tp.az, fmin(tp.bz, tp.cz)) - reach};
+    const double hi[3] = {fmax(tp.ax, fmax(tp.bx, tp.cx)) + reach, fmax(tp.ay, fmax(tp.by, tp.cy)) + reach,
+                          fmax(tp.az, fmax(tp.bz, tp.cz)) + reach};
+    const uint32_t gdim[3] = {g.gx, g.gy, g.gz};
+    uint32_t c0[3], nc[3];
+    for (int d = 0; d < 3; d++) {
+        c0[d] = cell_of(lo[d], g.inv_cell, gdim[d]);
+        const uint32_t c1 = cell_of(hi[d], g.inv_cell, gdim[d]);
+        if (!(c1 >= c0[d])) return;  // a facet with non-finite nodes is listed nowhere
+        nc[d] = c1 - c0[d] + 1u;
+    }
+    const uint64_t total = (uint64_t)nc[0] * nc[1] * nc[2];
+    for (uint64_t c = lane; c < total; c += 32u) {
+        const uint32_t ci[3] = {c0[0] + (uint32_t)(c % nc[0]), c0[1] + (uint32_t)((c / nc[0]) % nc[1]),
+                                c0[2] + (uint32_t)(c / ((uint64_t)nc[0] * nc[1]))};
+        double ctr[3], hd2 = 0.0;
+        for (int d = 0; d < 3; d++) {
+            const double b0 = ci[d] == 0u ? lo[d] : fmax(lo[d], (double)ci[d] * cs);
+            const double b1 = ci[d] + 1u >= gdim[d] ? hi[d] : fmin(hi[d], (double)(ci[d] + 1u) * cs);
+            ctr[d] = 0.5 * (b0 + b1);
+            hd2 += 0.25 * (b1 - b0) * (b1 - b0);
+        }
+        double qx, qy, qz;
+        const double lim = reach + sqrt(hd2);
+        if (tri_dist2(tp, ctr[0], ctr[1], ctr[2], qx, qy, qz) > lim * lim) continue;
+        const uint32_t key = ci[0] + g.gx * (ci[1] + g.gy * ci[2]);
+        if (!kEmit) {
+            atomicAdd(&cd.triCellCount[key], 1u);
+        } else {
+            const uint32_t slot = cd.triCellStart[key] + atomicSub(&cd.triCellCount[key], 1u) - 1u;
+            if (slot < cd.triCellCap) cd.triCell[slot] = t;
+        }
+    }
+}
+
+void launch_tri_bin(const SimConsts& k, const StateView& s, const CDView& cd, bool emit, cudaStream_t st) {
+    if (!(k.n_tris)) return;
+    ProfScope prof_(KID_MESH_BIN, st);
+    const unsigned blocks = blocks_for((size_t)k.n_tris * 32u, 128);
+    if (emit)
+        k_tri_bin<true><<<blocks, 128, 0, st>>>(k, s, cd);
+    else
+        k_tri_bin<false><<<blocks, 128, 0, st>>>(k, s, cd);
+}
+
+// The facets of home cell `key` that sphere (X, Y, Z, expanded radius rD, family fam) touches: f(t) for each, in
+// the cell list's order.
+template <typename F>
+__device__ __forceinline__ void for_mesh_contacts(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t key,
+                                                  uint32_t fam, double X, double Y, double Z, double rD, F f) {
+    const uint32_t b = cd.triCellStart[key], e = min(cd.triCellStart[key + 1], cd.triCellCap);
+    for (uint32_t p = b; p < e; p++) {
+        const uint32_t t = cd.triCell[p];
+        if (!index_ok(k.err, 19, t, k.n_tris)) continue;
+        const TriPlaced tp = s.tri[t];
+        if (s.masks[mask_index(fam, s.loc[tp.owner].w)] != 0) continue;
+        if (tri_overlap_cd(tp, X, Y, Z, rD, k.beta)) f(t);
+    }
+}
+
 // ------------------------------------------------------------------------------------------------------------
 // Per sphere: home cell and analytical-contact count (getNumberOfBinsEachSphereTouches's analytical loop,
 // DEMBinSphereKernels.cu:72-113).  The exact position is not stored: the cell-order record writer forms it again
 // from the owner pose (the same arithmetic, so the same bits), which costs less than writing and re-reading it.
-template <bool kPacked>
+template <bool kPacked, bool kMesh>
 __global__ void __launch_bounds__(256) k_sphere_prep(SimConsts k, StateView s, CDView cd) {
     const uint32_t sid = blockIdx.x * blockDim.x + threadIdx.x;
     if (sid >= k.n_spheres) return;
@@ -139,16 +254,26 @@ __global__ void __launch_bounds__(256) k_sphere_prep(SimConsts k, StateView s, C
         if (anal_overlap_cd(ap, X, Y, Z, rD, k.beta) != DEME_NOT_A_CONTACT) c++;
     }
     cd.nAnal[sid] = (uint8_t)c;
+    if (kMesh) {
+        // sphere--mesh contacts (the facets listed in the home cell)
+        uint32_t m = 0;
+        for_mesh_contacts(k, s, cd, key, fam, X, Y, Z, rD, [&](uint32_t) { m++; });
+        cd.nMesh[sid] = m;
+        c += m;
+    }
     cd.cnt[sid] = c;  // the pair search adds the sphere partners for which this sphere is A
 }
 
 void launch_sphere_prep(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st) {
     if (!(k.n_spheres)) return;
     ProfScope prof_(KID_SPHERE_PREP, st);
+    // (meshes are not combined with packed scenes)
     if (k.ownerScene)
-        k_sphere_prep<true><<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
+        k_sphere_prep<true, false><<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
+    else if (k.n_tris)
+        k_sphere_prep<false, true><<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
     else
-        k_sphere_prep<false><<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
+        k_sphere_prep<false, false><<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
 }
 
 __device__ __forceinline__ uint4 pack_ranges(const uint32_t lo[3], const uint32_t hi[3]) {
@@ -627,21 +752,23 @@ void launch_pair_overflow(const SimConsts& k, const StateView& s, const CDView& 
     k_pair_exact_tail<<<4 * (uint32_t)sm_count(), 256, 0, st>>>(k, s, cd, tempCap);
 }
 
-// Presets every sphere's contact count to its number of analytical contacts (k_sphere_prep does the same; this is
-// for a repeated search after the temporary list grew).
-__global__ void k_cnt_init(uint32_t n, const uint8_t* __restrict__ nAnal, uint32_t* cnt) {
+// Presets every sphere's contact count to its number of analytical and mesh contacts (k_sphere_prep does the same;
+// this is for a repeated search after the temporary list grew).
+__global__ void k_cnt_init(uint32_t n, const uint8_t* __restrict__ nAnal, const uint32_t* __restrict__ nMesh,
+                           uint32_t* cnt) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) cnt[i] = nAnal[i];
+    if (i < n) cnt[i] = nAnal[i] + (nMesh ? nMesh[i] : 0u);
 }
 
 void launch_cnt_init(const SimConsts& k, const CDView& cd, cudaStream_t st) {
     if (!(k.n_spheres)) return;
     ProfScope prof_(KID_OTHER, st);
-    k_cnt_init<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k.n_spheres, cd.nAnal, cd.cnt);
+    k_cnt_init<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k.n_spheres, cd.nAnal, k.n_tris ? cd.nMesh : nullptr,
+                                                               cd.cnt);
 }
 
 // Places every found pair in A's segment of the new list.  After the scan A's count is no longer needed, so the
-// slots after A's analytical contacts are handed out from the top by decrementing it.
+// slots after A's analytical and mesh contacts are handed out from the top by decrementing it.
 // The pool count is read on the device (counters[0]), so the launch may cover more threads than pairs; a pool that
 // outgrew its buffer (only possible when the host did not see the count first) is flagged.
 __global__ void __launch_bounds__(256) k_pair_scatter(SimConsts k, CDView cd, ContactView c, uint32_t nPairs,
@@ -668,7 +795,8 @@ void launch_pair_scatter(const SimConsts& k, const CDView& cd, const ContactView
 
 // Completes the canonical list: per sphere A (ID order), its sphere--analytical contacts by component id
 // (populateBinSphereTouchingPairs, DEMBinSphereKernels.cu:186-228) in the first slots of its segment, then its
-// sphere partners (placed by k_pair_scatter) sorted by ascending id.
+// sphere--mesh contacts by facet id, then its sphere partners (placed by k_pair_scatter) sorted by ascending id.
+template <bool kMesh>
 __global__ void __launch_bounds__(256) k_pair_assemble(SimConsts k, StateView s, CDView cd, ContactView c,
                                                        uint32_t cap) {
     const uint32_t A = blockIdx.x * blockDim.x + threadIdx.x;
@@ -680,8 +808,10 @@ __global__ void __launch_bounds__(256) k_pair_assemble(SimConsts k, StateView s,
     }
     const uint32_t nAn = cd.nAnal[A];
     const uint32_t anEnd = min(begin + nAn, end);
+    const uint32_t nMe = kMesh ? cd.nMesh[A] : 0u;
+    const uint32_t meEnd = min(anEnd + nMe, end);
     uint32_t w = begin;
-    if (nAn) {
+    if (nAn || nMe) {
         uint32_t owner;
         float4 sp;
         double X, Y, Z;
@@ -702,9 +832,31 @@ __global__ void __launch_bounds__(256) k_pair_assemble(SimConsts k, StateView s,
             }
         }
         if (w != anEnd) atomicOr(k.err, ERR_SEGMENT_TOO_LONG);
+        if (kMesh && nMe) {
+            // sphere--mesh contacts, by facet id
+            w = anEnd;
+            for_mesh_contacts(k, s, cd, cd.cellKey[A], fam, X, Y, Z, rD, [&](uint32_t t) {
+                if (w < meEnd) c.idB[w] = t;
+                w++;
+            });
+            if (w != meEnd) atomicOr(k.err, ERR_SEGMENT_TOO_LONG);
+            for (uint32_t i = anEnd + 1; i < meEnd; i++) {
+                const uint32_t v = c.idB[i];
+                uint32_t j = i;
+                while (j > anEnd && c.idB[j - 1] > v) {
+                    c.idB[j] = c.idB[j - 1];
+                    j--;
+                }
+                c.idB[j] = v;
+            }
+            for (uint32_t i = anEnd; i < meEnd; i++) {
+                c.idA[i] = A;
+                c.type[i] = DEME_SPHERE_MESH_CONTACT;
+            }
+        }
     }
-    uint32_t* seg = c.idB + anEnd;
-    const uint32_t n = end - anEnd;
+    uint32_t* seg = c.idB + meEnd;
+    const uint32_t n = end - meEnd;
     constexpr uint32_t kReg = 8;
     if (n <= kReg) {
         // short segments (nearly all): loaded at once, sorted in registers, stored at once
@@ -735,8 +887,8 @@ __global__ void __launch_bounds__(256) k_pair_assemble(SimConsts k, StateView s,
         }
     }
     for (uint32_t i = 0; i < n; i++) {
-        c.idA[anEnd + i] = A;
-        c.type[anEnd + i] = DEME_SPHERE_SPHERE_CONTACT;
+        c.idA[meEnd + i] = A;
+        c.type[meEnd + i] = DEME_SPHERE_SPHERE_CONTACT;
     }
 }
 
@@ -744,14 +896,18 @@ void launch_pair_assemble(const SimConsts& k, const StateView& s, const CDView& 
                           cudaStream_t st) {
     if (!(k.n_spheres)) return;
     ProfScope prof_(KID_PAIR_EMIT, st);
-    k_pair_assemble<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd, c, cap);
+    if (k.n_tris)
+        k_pair_assemble<true><<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd, c, cap);
+    else
+        k_pair_assemble<false><<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd, c, cap);
 }
 
 // ------------------------------------------------------------------------------------------------------------
 // History map and wildcard remap: for each new contact, find (idB, type) in A's segment of the previous list
 // (buildPersistentMap, src/kernel/DEMHistoryMappingKernels.cu:16-60; rearrangeContactWildcards,
-// src/kernel/DEMPrepForceKernels.cu:93-115).  Segments of both lists are sorted by (group, idB), group 0 being the
-// sphere--analytical contacts, so a binary search finds the unique partner.
+// src/kernel/DEMPrepForceKernels.cu:93-115).  Segments of both lists are sorted by (group, idB), the groups being
+// sphere--analytical, sphere--mesh and sphere--sphere contacts (contact_group), so a binary search finds the unique
+// partner.
 __global__ void __launch_bounds__(256) k_history(uint32_t n, ContactView cur, ContactView prev, bool has_hist,
                                                  uint32_t nS, uint32_t prevN, uint32_t* err) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -762,7 +918,7 @@ __global__ void __launch_bounds__(256) k_history(uint32_t n, ContactView cur, Co
     if (i >= n) return;
     const uint32_t A = cur.idA[i], B = cur.idB[i];
     const uint8_t t = cur.type[i];
-    const uint64_t key = ((uint64_t)(t == DEME_SPHERE_SPHERE_CONTACT ? 1u : 0u) << 32) | B;
+    const uint64_t key = ((uint64_t)contact_group(t) << 32) | B;
     if (!index_ok(err, 5, A, nS)) return;
     uint32_t lo = prev.off[A], hi = prev.off[A + 1];
     if (!index_ok(err, 6, hi, (uint64_t)prevN + 1) || lo > hi) {
@@ -774,7 +930,7 @@ __global__ void __launch_bounds__(256) k_history(uint32_t n, ContactView cur, Co
     while (lo < hi) {
         const uint32_t mid = (lo + hi) >> 1;
         const uint8_t tm = prev.type[mid];
-        const uint64_t km = ((uint64_t)(tm == DEME_SPHERE_SPHERE_CONTACT ? 1u : 0u) << 32) | prev.idB[mid];
+        const uint64_t km = ((uint64_t)contact_group(tm) << 32) | prev.idB[mid];
         if (km < key) {
             lo = mid + 1;
         } else {

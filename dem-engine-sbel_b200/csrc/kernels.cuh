@@ -30,6 +30,7 @@ struct StateView {
     uint32_t nA;
     const Prescription* presc;  // DEME_NUM_FAMILIES entries
     const uint2* ownerAnal;     // per owner (first, count) of the analytical components it meets; null = all
+    TriPlaced* tri;             // mesh facets placed at these poses (n_tris of them)
 };
 
 // Raw analytical component description (scene constants).
@@ -39,6 +40,14 @@ struct AnalRaw {
     uint8_t type, normal;
     uint16_t material;
     double c1, c2;
+};
+
+// Raw mesh facet (scene constants): the nodes in the owner frame (kT's relPosNode1..3), owner, material and the
+// owner's mass.
+struct TriRaw {
+    float n1x, n1y, n1z, n2x, n2y, n2z, n3x, n3y, n3z, mass;
+    uint32_t owner;
+    uint16_t material, pad;
 };
 
 // Cell-order record of one sphere for the exact pair test: 32 bytes, read as two 16-byte loads.
@@ -66,7 +75,15 @@ struct CDView {
                           // pair (A, B), A < B by id, or kNoPair; in no particular order
     uint32_t* ovf;        // spheres with more pre-filter survivors than the candidate scan's slots hold
     uint32_t* counters;   // [0] pair-pool entries (survivors) appended, [1] overflow spheres, [2] the candidate
-                          // scan's tile queue, [3] pool entries the overflow search appended (tested last)
+                          // scan's tile queue, [3] pool entries the overflow search appended (tested last),
+                          // [4] (cell, facet) entries of the mesh-facet cell lists
+    // mesh facets (n_tris > 0 only): per search cell the facets whose reach box meets it, and per sphere the
+    // number of facets it touches
+    uint32_t* triCellCount;  // nCells + 1
+    uint32_t* triCellStart;  // nCells + 1
+    uint32_t* triCell;       // facet ids, by cell
+    uint32_t triCellCap;
+    uint32_t* nMesh;         // per sphere
 };
 
 // One contact list (kT product) with its history wildcards.
@@ -99,6 +116,9 @@ struct ContactOutputs {
 #ifndef __CUDACC_RTC__
 void launch_place_anal(const SimConsts& k, const StateView& s, const AnalRaw* raw, AnalPlaced* placed, uint32_t nA,
                        cudaStream_t st);
+void launch_place_tri(const SimConsts& k, const StateView& s, const TriRaw* raw, cudaStream_t st);
+// the cell lists of the mesh facets: counts (kEmit false), then, after the scan into triCellStart, the entries
+void launch_tri_bin(const SimConsts& k, const StateView& s, const CDView& cd, bool emit, cudaStream_t st);
 void launch_sphere_prep(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
 void launch_cell_scatter(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
 void launch_gather_sorted(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);

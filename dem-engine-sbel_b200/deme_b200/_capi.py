@@ -28,6 +28,7 @@ STATUS_NAMES = {
 
 NOT_A_CONTACT = 0
 SPHERE_SPHERE_CONTACT = 1
+SPHERE_MESH_CONTACT = 2
 SPHERE_PLANE_CONTACT = 3
 SPHERE_CYLINDER_CONTACT = 5
 SPHERE_CONE_CONTACT = 6
@@ -160,10 +161,21 @@ SCENE_EXTENSIONS = [
 ]
 
 
+# mesh facets (n_tris of each; the nodes as n_tris x 3 floats)
+SCENE_TRIS = [
+    ("tri_owner", np.uint32),
+    ("tri_node1", np.float32),
+    ("tri_node2", np.float32),
+    ("tri_node3", np.float32),
+    ("tri_material", np.uint16),
+]
+
+
 class Scene(C.Structure):
     _fields_ = [("n_owners", C.c_uint32), ("n_spheres", C.c_uint32), ("n_anal", C.c_uint32),
                 ("n_materials", C.c_uint32)] + [(name, _P) for name, _, _ in SCENE_ARRAYS] + [
-                    ("prescriptions", _P)] + [(name, _P) for name, _, _ in SCENE_EXTENSIONS]
+                    ("prescriptions", _P)] + [(name, _P) for name, _, _ in SCENE_EXTENSIONS] + [
+                    ("n_tris", C.c_uint32)] + [(name, _P) for name, _ in SCENE_TRIS]
 
 
 STATE_FIELDS = [
@@ -250,6 +262,15 @@ def make_scene_struct(arrays: dict, counts: dict, prescriptions) -> tuple[Scene,
             raise ValueError(f"scene array {name} has {a.shape[0]} entries, expected {counts[key]}")
         keep.append(a)
         setattr(s, name, ptr(a) if a.size > 0 else None)
+    s.n_tris = counts.get("t", 0)
+    for name, dt in SCENE_TRIS:
+        if not s.n_tris:
+            break
+        a = np.ascontiguousarray(arrays[name], dtype=dt)
+        if a.shape[0] != s.n_tris:
+            raise ValueError(f"scene array {name} has {a.shape[0]} entries, expected {s.n_tris}")
+        keep.append(a)
+        setattr(s, name, ptr(a))
     return s, keep
 
 

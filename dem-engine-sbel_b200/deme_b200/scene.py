@@ -5,7 +5,8 @@ reproduces what ``Initialize`` computes on the host before any kernel runs (src/
 
 * the voxel bit split and length unit (figureOutNV, src/DEM/APIPrivate.cpp:222-333),
 * the world origin and optional bounding box (APIPrivate.cpp:647-687),
-* owner ordering: clumps in batch order, then external objects (src/DEM/dT.cpp:522-640),
+* owner ordering: clumps in batch order, then external objects, then mesh objects (src/DEM/dT.cpp:522-640,
+  src/DEM/kT.cpp:603-625),
 * initial position encoding of ``xyz - LBF`` (hostPositionToVoxelID, src/DEM/HostSideHelpers.hpp:328-350),
 * bin size and bin counts (decideBinSize, APIPrivate.cpp:335-369),
 * expand factor (transferSimParams, APIPrivate.cpp:730-758),
@@ -155,6 +156,94 @@ class ExternObj:
                                 float(half_angle), float(u_min), float(u_max), 1 if normal_outward else 0))
 
 
+def load_wavefront(path: str) -> tuple[np.ndarray, np.ndarray]:
+    """Vertices (n x 3) and triangles (m x 3 vertex indices) of a Wavefront OBJ file: ``v`` and ``f`` records
+    (DEMMeshConnected::LoadWavefrontMesh, src/DEM/BdrsAndObjs.h:243); polygons are split into fans, negative
+    indices count from the end, texture and normal indices after ``/`` are ignored."""
+    verts, faces = [], []
+    with open(path) as fh:
+        for line in fh:
+            tok = line.split()
+            if not tok:
+                continue
+            if tok[0] == "v":
+                verts.append([float(x) for x in tok[1:4]])
+            elif tok[0] == "f":
+                idx = []
+                for t in tok[1:]:
+                    i = int(t.split("/")[0])
+                    idx.append(i - 1 if i > 0 else len(verts) + i)
+                for j in range(1, len(idx) - 1):
+                    faces.append([idx[0], idx[j], idx[j + 1]])
+    return np.asarray(verts, f32).reshape(-1, 3), np.asarray(faces, np.int64).reshape(-1, 3)
+
+
+class MeshObj:
+    """DEMMeshConnected (src/DEM/BdrsAndObjs.h:173-300): a body represented by triangle facets, given in its own
+    frame.  Defaults as the reference's: the fixed family, mass 1, principal moments 1, at the origin."""
+
+    def __init__(self, vertices, faces, load_order: int):
+        self.vertices = np.asarray(vertices, f32).reshape(-1, 3).copy()
+        self.faces = np.asarray(faces, np.int64).reshape(-1, 3)
+        if self.faces.size and (self.faces.min() < 0 or self.faces.max() >= len(self.vertices)):
+            raise ValueError("mesh face index out of range")
+        self.load_order = load_order
+        self.family_code = capi.RESERVED_FAMILY
+        self.mass = f32(1.0)
+        self.moi = np.ones(3, f32)
+        self.init_pos = np.zeros(3, f32)
+        self.init_oriQ = np.array([1, 0, 0, 0], f32)  # (w, x, y, z)
+        self.init_vel = np.zeros(3, f32)
+        self.init_angvel = np.zeros(3, f32)
+        self.materials = None
+
+    def GetNumTriangles(self) -> int:
+        return len(self.faces)
+
+    def GetTriangle(self, i: int) -> np.ndarray:
+        return self.vertices[self.faces[i]]
+
+    def SetFamily(self, code: int):
+        if code > 255 or code < 0:
+            raise ValueError(f"family number {code} is larger than the max allowance 255")
+        self.family_code = code
+
+    def SetMass(self, m):
+        self.mass = f32(m)
+
+    def SetMOI(self, moi):
+        self.moi = np.asarray(moi, f32).reshape(3)
+
+    def SetMaterial(self, mat):
+        """One material for every facet, or a list with one per facet."""
+        if isinstance(mat, Material):
+            mat = [mat] * self.GetNumTriangles()
+        if len(mat) != self.GetNumTriangles():
+            raise ValueError(f"SetMaterial input argument must have length {self.GetNumTriangles()} (not "
+                             f"{len(mat)}), same as the number of triangle facets in the mesh.")
+        self.materials = list(mat)
+
+    def SetInitPos(self, pos):
+        self.init_pos = np.asarray(pos, f32).reshape(3)
+
+    def SetInitQuat(self, q):
+        """(w, x, y, z)."""
+        self.init_oriQ = np.asarray(q, f32).reshape(4)
+
+    def SetInitVel(self, v):
+        self.init_vel = np.asarray(v, f32).reshape(3)
+
+    def SetInitAngVel(self, w):
+        self.init_angvel = np.asarray(w, f32).reshape(3)
+
+    def Translate(self, d):
+        """Moves the nodes in the mesh's own frame (DEMMeshConnected::Translate)."""
+        self.vertices += np.asarray(d, f32).reshape(1, 3)
+
+    def Scale(self, s):
+        self.vertices *= np.asarray(s, f32)
+
+
 @dataclass
 class _Prescription:
     family: int
@@ -229,6 +318,7 @@ class SceneBuilder:
         self.templates: list[ClumpTemplate] = []
         self.batches: list[ClumpBatch] = []
         self.extern: list[ExternObj] = []
+        self.meshes: list[MeshObj] = []
         self.box = None
         self.dir_exact = None
         self.origin = "explicit"
@@ -333,6 +423,20 @@ class SceneBuilder:
         o = ExternObj(len(self.extern))
         self.extern.append(o)
         return o
+
+    def AddWavefrontMeshObject(self, mesh, material: Material | None = None) -> MeshObj:
+        """A mesh-represented body: a Wavefront OBJ path, or (vertices, faces) arrays (AddWavefrontMeshObject,
+        src/DEM/API.h:231-238)."""
+        if isinstance(mesh, MeshObj):
+            m = mesh
+            m.load_order = len(self.meshes)
+        else:
+            v, f = load_wavefront(mesh) if isinstance(mesh, str) else mesh
+            m = MeshObj(v, f, len(self.meshes))
+        if material is not None:
+            m.SetMaterial(material)
+        self.meshes.append(m)
+        return m
 
     def AddBCPlane(self, pos, normal, material) -> ExternObj:
         o = self.AddExternalObject()
@@ -469,7 +573,12 @@ class SceneBuilder:
             fams = np.zeros(0, np.uint32)
         nClumps = len(types)
         nExt = len(self.extern)
-        nO = nClumps + nExt
+        nMesh = len(self.meshes)
+        for m in self.meshes:
+            if m.materials is None:
+                raise ValueError("A meshed object is loaded but does not have associated material. Please assign "
+                                 "material to meshes via SetMaterial.")
+        nO = nClumps + nExt + nMesh
         ncomp = tmpl_nc[types] if nClumps else np.zeros(0, np.int64)
         nS = int(ncomp.sum())
         # sphere arrays
@@ -482,7 +591,7 @@ class SceneBuilder:
         rel = all_p[gidx].astype(f32)
         smat_w = all_m[gidx].astype(np.uint16)
         # owner positions relative to LBF in float (input_xyz - LBF, src/DEM/dT.cpp:539)
-        ext_xyz = np.array([o.init_pos for o in self.extern], f32).reshape(-1, 3)
+        ext_xyz = np.array([o.init_pos for o in self.extern] + [m.init_pos for m in self.meshes], f32).reshape(-1, 3)
         pos_f = np.concatenate([xyz, ext_xyz]).astype(f32) - lbf.astype(f32)
         vox, lx, ly, lz = self.host_position_to_voxel(pos_f.astype(np.float64), nv, voxel_size, float(l))
         oriQw = np.ones(nO, f32)
@@ -498,9 +607,23 @@ class SceneBuilder:
         wY = np.zeros(nO, f32)
         wZ = np.zeros(nO, f32)
         wX[:nClumps], wY[:nClumps], wZ[:nClumps] = angv.T
-        family = np.concatenate([fams, [o.family_code for o in self.extern]]).astype(np.uint8)
-        mass = np.concatenate([t_mass[types], [o.mass for o in self.extern]]).astype(f32)
-        moi = np.concatenate([t_moi[types], np.array([o.moi for o in self.extern], f32).reshape(-1, 3)]).astype(f32)
+        m0 = nClumps + nExt  # mesh owners follow the external objects (src/DEM/kT.cpp:603-625)
+        for i, m in enumerate(self.meshes):
+            oriQw[m0 + i], oriQx[m0 + i], oriQy[m0 + i], oriQz[m0 + i] = m.init_oriQ
+            vX[m0 + i], vY[m0 + i], vZ[m0 + i] = m.init_vel
+            wX[m0 + i], wY[m0 + i], wZ[m0 + i] = m.init_angvel
+        family = np.concatenate([fams, [o.family_code for o in self.extern],
+                                 [m.family_code for m in self.meshes]]).astype(np.uint8)
+        mass = np.concatenate([t_mass[types], [o.mass for o in self.extern], [m.mass for m in self.meshes]]).astype(f32)
+        moi = np.concatenate([t_moi[types], np.array([o.moi for o in self.extern], f32).reshape(-1, 3),
+                              np.array([m.moi for m in self.meshes], f32).reshape(-1, 3)]).astype(f32)
+        # ---- mesh facets ----
+        tri = [m.vertices[m.faces].reshape(-1, 9) for m in self.meshes]
+        tri = np.concatenate(tri).astype(f32) if tri else np.zeros((0, 9), f32)
+        nTri = len(tri)
+        tri_owner = np.concatenate([np.full(m.GetNumTriangles(), m0 + i, np.uint32) for i, m in enumerate(self.meshes)]) \
+            if nMesh else np.zeros(0, np.uint32)
+        tri_material = np.array([mt.load_order for m in self.meshes for mt in m.materials], np.uint16)
 
         # ---- analytical components ----
         comps = []
@@ -625,8 +748,12 @@ class SceneBuilder:
                       relY=np.ascontiguousarray(rel[:, 1]), relZ=np.ascontiguousarray(rel[:, 2]), radius=radius,
                       sphere_material=(smat_w & 0xFF).astype(np.uint8), mat_E=matarr("E"), mat_nu=matarr("nu"), mat_CoR=matarr("CoR"),
                       mat_mu=matarr("mu"), mat_Crr=matarr("Crr"), family_masks=masks, **anal, **ext_arrays)
-        counts = dict(o=nO, s=nS, a=nA, m=nM)
-        info = dict(n_clumps=nClumps, n_ext=nExt, n_templates=nT, rmin=rmin, bin_size=bin_size, nb=nb, nv=nv, l=l,
+        if nTri:
+            arrays.update(tri_owner=tri_owner, tri_node1=np.ascontiguousarray(tri[:, 0:3]),
+                          tri_node2=np.ascontiguousarray(tri[:, 3:6]), tri_node3=np.ascontiguousarray(tri[:, 6:9]),
+                          tri_material=tri_material)
+        counts = dict(o=nO, s=nS, a=nA, m=nM, t=nTri)
+        info = dict(n_clumps=nClumps, n_ext=nExt, n_meshes=nMesh, n_templates=nT, rmin=rmin, bin_size=bin_size, nb=nb, nv=nv, l=l,
                     beta=beta, lbf=lbf.copy(), box=self.box.copy(), merged_prescriptions=self.merged_prescriptions,
                     motion_expressions=self.motion_expressions,
                     owner_template=np.asarray(types, np.int64) if nClumps else np.zeros(0, np.int64),

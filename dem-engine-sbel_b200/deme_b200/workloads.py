@@ -473,10 +473,11 @@ def hopper_wedge(n: int = 4_000_000, r_median: float = 1.5e-3, sigma: float = 0.
 
 
 def sphere_pile(n: int = 60, seed: int = 3, h: float = 2e-5, spread: float = 5.2e-3, noise: float = 4e-4,
-                vel_scale: float = 0.05, spin_scale: float = 20.0, lift: float = 2.2e-3):
+                vel_scale: float = 0.05, spin_scale: float = 20.0, lift: float = 2.2e-3, mesh_floor: bool = False):
     """Loose pile of single spheres (radii U[2, 3] mm, two materials) pressed onto a floor plane with random
     velocities and spins: every contact branch of the Hertz-Mindlin model is active within a few dozen steps.
-    Used by the adjoint tests."""
+    Used by the adjoint tests.  ``mesh_floor``: the floor is a mesh body of two facets 0.19 m wide in the same
+    plane instead of an analytical plane."""
     rng = np.random.default_rng(seed)
     r = rng.uniform(2e-3, 3e-3, n).astype(f32)
     rho = 2500.0
@@ -496,13 +497,19 @@ def sphere_pile(n: int = 60, seed: int = 3, h: float = 2e-5, spread: float = 5.2
     b = s.AddClumps(types, x.astype(f32))
     b.SetVel(rng.normal(0, vel_scale, (n, 3)).astype(f32))
     b.SetAngVel(rng.normal(0, spin_scale, (n, 3)).astype(f32))
-    s.AddBCPlane((0, 0, z0), (0, 0, 1), m1)
+    if mesh_floor:
+        w = 0.095
+        v = np.array([[-w, -w, z0], [w, -w, z0], [w, w, z0], [-w, w, z0]], f32)
+        floor = s.AddWavefrontMeshObject((v, np.array([[0, 1, 2], [0, 2, 3]])), m1)
+        floor.SetMass(1e15)  # as an analytical owner's (the mass enters the contacts' effective mass)
+    else:
+        s.AddBCPlane((0, 0, z0), (0, 0, 1), m1)
     s.SetInitTimeStep(h)
     s.SetGravitationalAcceleration((0, 0, -9.81))
     s.SetCDUpdateFreq(1)
     s.SetExpandFactor(0.0)  # contacts are exactly the overlapping pairs (the unset default would shrink them)
     built = s.Initialize()
-    built.info.update(workload="sphere_pile", n=n, seed=seed)
+    built.info.update(workload="sphere_pile", n=n, seed=seed, mesh_floor=mesh_floor)
     return built
 
 
@@ -678,3 +685,170 @@ def single_settling(spec, dt: float = 1e-5, packed=None, index: int = 0):
     s.SetCDUpdateFreq(1)
     s.SetExpandFactor(0.0)
     return s.Initialize()
+
+
+def icosphere(radius: float, subdivisions: int = 2):
+    """Triangulated sphere: an icosahedron whose faces are split in four ``subdivisions`` times, vertices pushed
+    onto the sphere.  Returns (vertices, faces), outward winding."""
+    t = (1.0 + math.sqrt(5.0)) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+         (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10),
+         (8, 6, 7), (9, 8, 1)]
+    verts = [np.array(p, np.float64) / math.sqrt(1 + t * t) for p in v]
+    for _ in range(subdivisions):
+        mid = {}
+
+        def midpoint(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in mid:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                mid[key] = len(verts) - 1
+            return mid[key]
+
+        nf = []
+        for a, b, c in f:
+            ab, bc, ca = midpoint(a, b), midpoint(b, c), midpoint(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        f = nf
+    return (np.array(verts) * radius).astype(f32), np.array(f, np.int64)
+
+
+def _grid_quad(p0, p1, p2, p3, n: int):
+    """The quad p0 p1 p2 p3 (in order around it) as 2 n^2 triangles on an n x n grid."""
+    p0, p1, p2, p3 = (np.asarray(p, np.float64) for p in (p0, p1, p2, p3))
+    tris = []
+    for i in range(n):
+        for j in range(n):
+            def at(u, v):
+                return (1 - v) * ((1 - u) * p0 + u * p1) + v * ((1 - u) * p3 + u * p2)
+            a, b = at(i / n, j / n), at((i + 1) / n, j / n)
+            c, d = at((i + 1) / n, (j + 1) / n), at(i / n, (j + 1) / n)
+            tris += [(a, b, c), (a, c, d)]
+    return tris
+
+
+def _mesh_arrays(tris):
+    v = np.array(tris, np.float64).reshape(-1, 3).astype(f32)
+    return v, np.arange(len(v), dtype=np.int64).reshape(-1, 3)
+
+
+def mesh_funnel(n: int = 2000, r: float = 2e-3, rho: float = 2500.0, seed: int = 11, wall_clearance: float = 0.8,
+                tilt_deg: float = 20.0, grid: int = 4, dt: float = 2e-6, cd_freq: int = 1, margin: float = 0.0,
+                mu: float = 0.4, crr: float = 0.02):
+    """Spheres (radii U[0.8, 1] r) in a square funnel made of triangle facets: four walls leaning ``tilt_deg`` out
+    from the vertical and a floor, each face a ``grid`` x ``grid`` grid of quads split into two triangles (a fixed
+    mesh body, family 1).  Spheres start on a jittered cubic lattice; ``wall_clearance`` below 1 starts the outer
+    ones pressed into the walls and the floor, so sphere--mesh contacts on facet interiors, edges and corners exist
+    from the first step."""
+    rng = np.random.default_rng(seed)
+    th = math.radians(tilt_deg)
+    w0 = 10 * r * max(1.0, (n / 1000.0) ** (1 / 3))  # floor half-width
+    pitch = 2.02 * r
+    # lattice in the funnel: distance to every wall plane and the floor at least clearance x radius
+    H = 4 * w0
+    g = np.arange(-w0 - H * math.tan(th), w0 + H * math.tan(th) + pitch, pitch)
+    zs = np.arange(0.0, H, pitch)
+    X, Y, Z = np.meshgrid(g, g, zs, indexing="ij")
+    P = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
+    P = P[np.lexsort((P[:, 0], P[:, 1], P[:, 2]))]
+    rad = rng.uniform(0.8 * r, r, len(P))
+    c, s_ = math.cos(th), math.sin(th)
+    # inward normals of the walls x = +-(w0 + z tan th), y likewise: (-+c, 0, s)
+    dmin = P[:, 2]
+    for ax in (0, 1):
+        for sg in (1.0, -1.0):
+            d = (w0 - sg * P[:, ax]) * c + P[:, 2] * s_
+            dmin = np.minimum(dmin, d)
+    keep = dmin >= wall_clearance * rad
+    P, rad = P[keep][:n], rad[keep][:n]
+    if len(P) < n:
+        raise ValueError("funnel too small for n")
+    P = P + rng.uniform(-0.005 * r, 0.005 * r, P.shape)
+    zt = float(P[:, 2].max()) + 4 * r
+    wt = w0 + zt * math.tan(th)
+    tris = _grid_quad((-w0, -w0, 0), (w0, -w0, 0), (w0, w0, 0), (-w0, w0, 0), grid)
+    for (a0, a1, b0, b1) in (((-w0, -w0), (w0, -w0), (-wt, -wt), (wt, -wt)), ((w0, -w0), (w0, w0), (wt, -wt), (wt, wt)),
+                             ((w0, w0), (-w0, w0), (wt, wt), (-wt, wt)), ((-w0, w0), (-w0, -w0), (-wt, wt), (-wt, -wt))):
+        tris += _grid_quad((*a0, 0), (*a1, 0), (*b1, zt), (*b0, zt), grid)
+    s = SceneBuilder()
+    box = 2 * wt + 8 * r
+    s.InstructBoxDomainDimension(box, box, box)
+    s.SetCoordSysOrigin("center")
+    shift = np.array([0.0, 0.0, -zt / 2])
+    m_s = s.LoadMaterial({"E": 1e8, "nu": 0.3, "CoR": 0.4, "mu": mu, "Crr": crr})
+    m_w = s.LoadMaterial({"E": 2e8, "nu": 0.25, "CoR": 0.5, "mu": mu, "Crr": crr})
+    types = [s.LoadSphereType(sphere_mass(float(ri), rho), float(ri), m_s) for ri in rad.astype(f32)]
+    b = s.AddClumps(types, (P + shift).astype(f32))
+    b.SetFamily(0)
+    v, f = _mesh_arrays(tris)
+    mesh = s.AddWavefrontMeshObject((v, f), m_w)
+    mesh.SetInitPos(shift)
+    mesh.SetFamily(1)
+    s.SetFamilyFixed(1)
+    s.SetInitTimeStep(dt)
+    s.SetGravitationalAcceleration((0, 0, -9.81))
+    s.SetCDUpdateFreq(cd_freq)
+    s.SetExpandFactor(margin)
+    s.SetInitBinSize(2.0 * float(f32(rad.min())))
+    built = s.Initialize()
+    built.info.update(workload="mesh_funnel", n=n, seed=seed, n_tris=len(f))
+    return built
+
+
+def mesh_ball_drop(n: int = 2000, r: float = 2e-3, rho: float = 2600.0, ball_radius: float = 0.02,
+                   subdivisions: int = 3, ball_rho: float = 7000.0, speed: float = 1.0, seed: int = 12,
+                   dt: float = 2e-6, cd_freq: int = 1, margin: float = 0.0, press: float = 0.2, layers: int = 4):
+    """A mesh ball (icosphere of ``ball_radius``, a free body) driven into a bed of spheres (radii U[0.8, 1] r on a
+    jittered lattice of about ``layers`` layers in a box of analytical planes), as in the reference's BallDrop demo
+    where the projectile is a Wavefront mesh.  The ball starts moving down at ``speed``, pressed ``press`` x r into
+    the bed's top layer."""
+    rng = np.random.default_rng(seed)
+    pitch = 2.02 * r
+    side = max(int(math.ceil(2.5 * ball_radius / pitch)), int(math.ceil(math.sqrt(n / layers))))
+    layers = int(math.ceil(n / side ** 2))
+    idx = np.arange(n)
+    P = np.stack([(idx % side) * pitch, (idx // side % side) * pitch, (idx // side // side) * pitch], 1)
+    P -= np.array([(side - 1) * pitch / 2, (side - 1) * pitch / 2, 0.0])
+    P += rng.uniform(-0.005 * r, 0.005 * r, P.shape)
+    rad = rng.uniform(0.8 * r, r, n)
+    half = side * pitch / 2 + r
+    top = float((layers - 1) * pitch)
+    s = SceneBuilder()
+    box = max(2 * half, top + 4 * ball_radius) + 8 * r
+    s.InstructBoxDomainDimension(box, box, box)
+    s.SetCoordSysOrigin("center")
+    z0 = -box / 2 + 2 * r
+    m_s = s.LoadMaterial({"E": 1e8, "nu": 0.3, "CoR": 0.3, "mu": 0.4, "Crr": 0.01})
+    m_b = s.LoadMaterial({"E": 5e8, "nu": 0.3, "CoR": 0.3, "mu": 0.3, "Crr": 0.0})
+    types = [s.LoadSphereType(sphere_mass(float(ri), rho), float(ri), m_s) for ri in rad.astype(f32)]
+    b = s.AddClumps(types, (P + np.array([0.0, 0.0, z0 + r])).astype(f32))
+    b.SetFamily(0)
+    for ax, sg in ((0, 1), (0, -1), (1, 1), (1, -1)):
+        pos = np.zeros(3)
+        pos[ax] = -sg * half
+        nrm = np.zeros(3)
+        nrm[ax] = sg
+        s.AddBCPlane(pos, nrm, m_s).SetFamily(2)
+    s.AddBCPlane((0, 0, z0), (0, 0, 1), m_s).SetFamily(2)
+    s.SetFamilyFixed(2)
+    # the ball's lowest facet sits `press` x r below the top layer's tops
+    v, f = icosphere(ball_radius, subdivisions)
+    zc = z0 + r + top + r + float(-v[:, 2].min()) - press * r
+    ball = s.AddWavefrontMeshObject((v, f), m_b)
+    ball.SetInitPos((0.0, 0.0, zc))
+    mb = sphere_mass(ball_radius, ball_rho)
+    ball.SetMass(mb)
+    ball.SetMOI([0.4 * mb * ball_radius ** 2] * 3)
+    ball.SetInitVel((0.0, 0.0, -speed))
+    ball.SetFamily(0)
+    s.SetInitTimeStep(dt)
+    s.SetGravitationalAcceleration((0, 0, -9.81))
+    s.SetCDUpdateFreq(cd_freq)
+    s.SetExpandFactor(margin)
+    s.SetInitBinSize(2.0 * float(f32(rad.min())))
+    built = s.Initialize()
+    built.info.update(workload="mesh_ball_drop", n=n, seed=seed, n_tris=len(f))
+    return built

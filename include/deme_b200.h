@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define DEME_B200_ABI_VERSION 4
+#define DEME_B200_ABI_VERSION 5
 
 /* Status codes (the reference throws std::runtime_error instead: src/DEM/Structs.h:129-141, src/core/utils/GpuError.h:13-27). */
 typedef enum {
@@ -177,6 +177,17 @@ typedef struct {
                                               a search grid of its own, sized by its own spheres */
     const float* scene_box;                /* n_scenes x 6: lower and upper corner of each scene's search grid,
                                               relative to the domain's lower corner (NULL: from the initial poses) */
+    /* Mesh facets (triangles) of mesh-represented owners: DEMMeshConnected (src/DEM/BdrsAndObjs.h:173-300), kT's
+     * ownerMesh and relPosNode1..3 (src/DEM/kT.cpp:603-625).  Mesh owners follow the clump owners, like the
+     * analytical owners.  The reference declares the sphere--mesh contact type (src/DEM/Defines.h:66) but detects no
+     * such contact; here every facet a sphere touches is one DEME_SPHERE_MESH_CONTACT with idB = the facet id.
+     * 0 / NULL: no meshes.  Not with the packed-scene extensions above. */
+    uint32_t n_tris;
+    const uint32_t* tri_owner;    /* per facet: its owner (n_clumps <= owner < n_owners) */
+    const float* tri_node1;       /* n_tris x 3 (x, y, z interleaved): the nodes in the owner frame */
+    const float* tri_node2;
+    const float* tri_node3;
+    const uint16_t* tri_material; /* per facet */
 } deme_scene;
 
 /* Mutable owner state (download/upload).  Any pointer may be NULL to skip that array. */
@@ -205,7 +216,8 @@ typedef struct {
 } deme_state;
 
 /* Contact list (kT product, src/DEM/Defines.h:242-245).  Order: sorted by idA; inside one idA, sphere--analytical
- * contacts first (ascending component id), then sphere--sphere contacts (ascending idB).  The reference sorts by idA
+ * contacts first (ascending component id), then sphere--mesh contacts (ascending facet id), then sphere--sphere
+ * contacts (ascending idB).  The reference sorts by idA
  * only, so its in-segment order is a permutation of this one. */
 typedef struct {
     uint32_t capacity;       /* elements available in each caller array (in) */

@@ -2,7 +2,7 @@
  *
  * Keeps the scene-building and stepping API of deme::DEMSolver (src/DEM/API.h:44-887): LoadMaterial,
  * LoadClumpType / LoadSphereType, AddClumps (DEMClumpBatch setters), AddExternalObject / AddBCPlane
- * (DEMExternObj::AddPlane, plus AddCylinder / AddCone), the family controls, DefineContactForceModel with
+ * (DEMExternObj::AddPlane, plus AddCylinder / AddCone), AddWavefrontMeshObject (DEMMeshConnected), the family controls, DefineContactForceModel with
  * SetPerContactWildcards, the world and time-stepping setters, Initialize, DoDynamics / DoDynamicsThenSync /
  * DoStepDynamics and owner-state queries.  Initialize flattens the scene exactly as the reference's host code does
  * before its JIT step (src/DEM/APIPrivate.cpp:222-369, 574-687, 903-1048; src/DEM/dT.cpp:480-640;
@@ -143,6 +143,91 @@ class DEMExternObj {
     std::vector<DEMAnalEntity> entities;
 };
 
+/* DEMMeshConnected (src/DEM/BdrsAndObjs.h:173-300): a body represented by triangle facets given in its own frame.
+ * Defaults as the reference's: the fixed family, mass 1, principal moments 1, at the origin, unit orientation.
+ * Its sphere--mesh contacts (one per facet a sphere touches) are an addition: the reference detects none. */
+class DEMMeshConnected {
+  public:
+    DEMMeshConnected() = default;
+    explicit DEMMeshConnected(const std::string& file) {
+        if (!LoadWavefrontMesh(file)) throw std::runtime_error("cannot read the mesh file " + file);
+    }
+    DEMMeshConnected(const std::string& file, const std::shared_ptr<DEMMaterial>& mat) : DEMMeshConnected(file) {
+        SetMaterial(mat);
+    }
+    /* Wavefront OBJ: `v` and `f` records; polygons split into fans, negative indices from the end, texture and
+     * normal indices after '/' ignored */
+    bool LoadWavefrontMesh(const std::string& file, bool load_normals = true, bool load_uv = false) {
+        std::ifstream in(file);
+        if (!in) return false;
+        vertices.clear();
+        face_v_indices.clear();
+        std::string line;
+        while (std::getline(in, line)) {
+            std::istringstream ls(line);
+            std::string tag;
+            if (!(ls >> tag)) continue;
+            if (tag == "v") {
+                float3 v{0.f, 0.f, 0.f};
+                ls >> v.x >> v.y >> v.z;
+                vertices.push_back(v);
+            } else if (tag == "f") {
+                std::vector<int> idx;
+                std::string tok;
+                while (ls >> tok) {
+                    const int i = std::stoi(tok.substr(0, tok.find('/')));
+                    idx.push_back(i > 0 ? i - 1 : (int)vertices.size() + i);
+                }
+                for (size_t j = 1; j + 1 < idx.size(); j++) face_v_indices.push_back(int3{idx[0], idx[j], idx[j + 1]});
+            }
+        }
+        nTri = face_v_indices.size();
+        return true;
+    }
+    size_t GetNumTriangles() const { return nTri; }
+    void SetFamily(unsigned code) {
+        if (code > 255) throw std::runtime_error("family number is larger than the max allowance 255");
+        family_code = code;
+    }
+    void SetMass(float m) { mass = m; }
+    void SetMOI(float3 moi) { MOI = moi; }
+    void SetMaterial(const std::vector<std::shared_ptr<DEMMaterial>>& input) {
+        if (input.size() != nTri)
+            throw std::runtime_error("SetMaterial input argument must have length " + std::to_string(nTri) + " (not " +
+                                     std::to_string(input.size()) + "), same as the number of triangle facets in the mesh.");
+        materials = input;
+        isMaterialSet = true;
+    }
+    void SetMaterial(const std::shared_ptr<DEMMaterial>& input) {
+        SetMaterial(std::vector<std::shared_ptr<DEMMaterial>>(nTri, input));
+    }
+    void SetInitPos(float3 p) { init_pos = p; }
+    void SetInitQuat(float4 q) { init_oriQ = q; }  // (x, y, z, w)
+    void SetInitVel(float3 v) { init_vel = v; }
+    void SetInitAngVel(float3 w) { init_angvel = w; }
+    /* moves the nodes in the mesh's own frame */
+    void Translate(float3 d) {
+        for (auto& v : vertices) v = float3{v.x + d.x, v.y + d.y, v.z + d.z};
+    }
+    void Scale(float s) {
+        for (auto& v : vertices) v = float3{v.x * s, v.y * s, v.z * s};
+    }
+
+    size_t nTri = 0;
+    std::vector<float3> vertices;
+    std::vector<int3> face_v_indices;
+    std::vector<std::shared_ptr<DEMMaterial>> materials;
+    bool isMaterialSet = false;
+    unsigned family_code = DEME_RESERVED_FAMILY;
+    float mass = 1.f;
+    float3 MOI{1.f, 1.f, 1.f};
+    float3 init_pos{0.f, 0.f, 0.f};
+    float4 init_oriQ{0.f, 0.f, 0.f, 1.f};
+    float3 init_vel{0.f, 0.f, 0.f};
+    float3 init_angvel{0.f, 0.f, 0.f};
+    unsigned load_order = 0;
+};
+
 class DEMForceModel {
   public:
     void DefineCustomModel(const std::string& model) { m_force_model = model; custom = true; }
@@ -179,6 +264,9 @@ struct FlatScene {
     std::vector<float> mat_E, mat_nu, mat_CoR, mat_mu, mat_Crr;
     std::vector<uint8_t> family_masks;
     std::vector<deme_family_prescription> prescriptions;
+    std::vector<uint32_t> tri_owner;
+    std::vector<float> tri_node1, tri_node2, tri_node3;
+    std::vector<uint16_t> tri_material;
     // families whose prescription holds an expression: strings kept here, pointed to by `motion`
     std::vector<std::vector<std::string>> motion_strings;  // per entry: vX vY vZ wX wY wZ X Y Z ("none" = free)
     std::vector<deme_motion_expressions> motion;
@@ -238,6 +326,12 @@ struct FlatScene {
         s.mat_Crr = mat_Crr.data();
         s.family_masks = family_masks.data();
         s.prescriptions = prescriptions.data();
+        s.n_tris = (uint32_t)tri_owner.size();
+        s.tri_owner = s.n_tris ? tri_owner.data() : nullptr;
+        s.tri_node1 = s.n_tris ? tri_node1.data() : nullptr;
+        s.tri_node2 = s.n_tris ? tri_node2.data() : nullptr;
+        s.tri_node3 = s.n_tris ? tri_node3.data() : nullptr;
+        s.tri_material = s.n_tris ? tri_material.data() : nullptr;
     }
 };
 
@@ -459,6 +553,31 @@ class DEMSolver {
         o->AddPlane(pos, normal, mat);
         return o;
     }
+    /* a mesh-represented body (AddWavefrontMeshObject, src/DEM/API.h:231-238) */
+    std::shared_ptr<DEMMeshConnected> AddWavefrontMeshObject(const std::string& filename,
+                                                             const std::shared_ptr<DEMMaterial>& mat,
+                                                             bool load_normals = true, bool load_uv = false) {
+        auto m = std::make_shared<DEMMeshConnected>();
+        if (!m->LoadWavefrontMesh(filename, load_normals, load_uv))
+            throw std::runtime_error("cannot read the mesh file " + filename);
+        m->SetMaterial(mat);
+        return AddWavefrontMeshObject(m);
+    }
+    std::shared_ptr<DEMMeshConnected> AddWavefrontMeshObject(const std::string& filename, bool load_normals = true,
+                                                             bool load_uv = false) {
+        auto m = std::make_shared<DEMMeshConnected>();
+        if (!m->LoadWavefrontMesh(filename, load_normals, load_uv))
+            throw std::runtime_error("cannot read the mesh file " + filename);
+        return AddWavefrontMeshObject(m);
+    }
+    std::shared_ptr<DEMMeshConnected> AddWavefrontMeshObject(DEMMeshConnected& mesh) {
+        return AddWavefrontMeshObject(std::make_shared<DEMMeshConnected>(mesh));
+    }
+    std::shared_ptr<DEMMeshConnected> AddWavefrontMeshObject(const std::shared_ptr<DEMMeshConnected>& mesh) {
+        mesh->load_order = (unsigned)meshes.size();
+        meshes.push_back(mesh);
+        return mesh;
+    }
 
     // ---- families ----
     void DisableContactBetweenFamilies(unsigned a, unsigned b) {
@@ -536,6 +655,7 @@ class DEMSolver {
         // after the flattening, which may add the bounding-box object
         n_clumps_init = n_clumps_system;
         n_ext_init = ext.size();
+        n_mesh_init = meshes.size();
         n_templates_init = templates.size();
         n_materials_init = materials.size();
         n_presc_init = presc.size();
@@ -756,8 +876,8 @@ class DEMSolver {
      * cached before Initialize are added a second time. */
     void UpdateClumps() {
         if (!h) throw std::runtime_error("UpdateClumps: call it only after Initialize");
-        if (ext.size() != n_ext_init)
-            throw std::runtime_error("UpdateClumps cannot be used after loading new analytical objects");
+        if (ext.size() != n_ext_init || meshes.size() != n_mesh_init)
+            throw std::runtime_error("UpdateClumps cannot be used after loading new analytical or mesh objects");
         if (templates.size() != n_templates_init)
             throw std::runtime_error("UpdateClumps cannot be used after loading new clump templates");
         if (materials.size() != n_materials_init || presc.size() != n_presc_init)
@@ -800,8 +920,8 @@ class DEMSolver {
         // the system grows by the cached batches; flatten and create the new handle as Initialize does
         for (const auto& b : batches) system_batches.push_back(b);
         create_handle();
-        // carry the run over: old clumps keep their ids, the external objects move behind the new clumps
-        const size_t nC_new = n_clumps_system, nExt = ext.size();
+        // carry the run over: old clumps keep their ids, the external and mesh objects move behind the new clumps
+        const size_t nC_new = n_clumps_system, nExt = ext.size() + meshes.size();
         FlatScene& f = *flat;
         std::vector<uint64_t> voxel = f.voxel;
         std::vector<uint16_t> lx = f.locX, ly = f.locY, lz = f.locZ;
@@ -961,10 +1081,10 @@ class DEMSolver {
     }
 
     // The handle's index of a reference owner id: the reference numbers the clumps of the first Initialize, then
-    // the external objects, then the clumps of each UpdateClumps; the handle keeps every clump before the
-    // external objects.
+    // the external objects and the mesh objects, then the clumps of each UpdateClumps; the handle keeps every clump
+    // before the external and mesh objects.
     uint32_t handle_owner(uint32_t owner) const {
-        const size_t nExt = n_ext_init;
+        const size_t nExt = n_ext_init + n_mesh_init;
         const uint32_t nO = flat ? flat->scene.n_owners : 0;
         uint32_t o = owner;
         if (owner >= n_clumps_init && owner < n_clumps_init + nExt)
@@ -1096,14 +1216,15 @@ class DEMSolver {
             p.linVelP = p.rotVelP = p.linPosP = p.rotPosP = true;
             all_presc.push_back(p);
         }
-        // ---- owners: clumps in batch order, then external objects (dT.cpp:522-640) ----
+        // ---- owners: clumps in batch order, then external objects, then mesh objects (dT.cpp:522-640,
+        // kT.cpp:603-625) ----
         std::vector<const DEMClumpBatch*> bs;
         size_t nClumps = 0;
         for (const auto& b : batches) {
             bs.push_back(b.get());
             nClumps += b->nClumps;
         }
-        const size_t nExt = ext.size(), nO = nClumps + nExt;
+        const size_t nExt = ext.size(), nMesh = meshes.size(), nO = nClumps + nExt + nMesh;
         auto resize = [nO](auto&... v) { (v.resize(nO), ...); };
         resize(f.voxel, f.locX, f.locY, f.locZ, f.oriQw, f.oriQx, f.oriQy, f.oriQz, f.vX, f.vY, f.vZ, f.omgX, f.omgY,
                f.omgZ, f.family, f.mass, f.mmiXX, f.mmiYY, f.mmiZZ);
@@ -1167,6 +1288,40 @@ class DEMSolver {
                 f.anal_size2.push_back(a.size2);
                 f.anal_size3.push_back(a.size3);
                 f.anal_mass.push_back(x.mass);
+            }
+        }
+        for (size_t e = 0; e < nMesh; e++, o++) {
+            const DEMMeshConnected& x = *meshes[e];
+            if (!x.isMaterialSet)
+                throw std::runtime_error("A meshed object is loaded but does not have associated material. Please "
+                                         "assign material to meshes via SetMaterial.");
+            pos[o] = x.init_pos;
+            f.oriQw[o] = x.init_oriQ.w;
+            f.oriQx[o] = x.init_oriQ.x;
+            f.oriQy[o] = x.init_oriQ.y;
+            f.oriQz[o] = x.init_oriQ.z;
+            f.vX[o] = x.init_vel.x;
+            f.vY[o] = x.init_vel.y;
+            f.vZ[o] = x.init_vel.z;
+            f.omgX[o] = x.init_angvel.x;
+            f.omgY[o] = x.init_angvel.y;
+            f.omgZ[o] = x.init_angvel.z;
+            f.family[o] = (uint8_t)x.family_code;
+            f.mass[o] = x.mass;
+            f.mmiXX[o] = x.MOI.x;
+            f.mmiYY[o] = x.MOI.y;
+            f.mmiZZ[o] = x.MOI.z;
+            for (size_t i = 0; i < x.nTri; i++) {
+                const int3 fv = x.face_v_indices[i];
+                f.tri_owner.push_back((uint32_t)o);
+                for (const auto& pr : {std::make_pair(fv.x, &f.tri_node1), std::make_pair(fv.y, &f.tri_node2),
+                                       std::make_pair(fv.z, &f.tri_node3)}) {
+                    const float3 v = x.vertices.at((size_t)pr.first);
+                    pr.second->push_back(v.x);
+                    pr.second->push_back(v.y);
+                    pr.second->push_back(v.z);
+                }
+                f.tri_material.push_back((uint16_t)x.materials[i]->load_order);
             }
         }
         if (f.anal_type.size() > 255) throw std::runtime_error("at most 255 analytical components");
@@ -1304,6 +1459,7 @@ class DEMSolver {
     std::vector<std::shared_ptr<DEMClumpTemplate>> templates;
     std::vector<std::shared_ptr<DEMClumpBatch>> batches;
     std::vector<std::shared_ptr<DEMExternObj>> ext;
+    std::vector<std::shared_ptr<DEMMeshConnected>> meshes;
     float3 box{0.f, 0.f, 0.f};
     bool has_box = false;
     std::string origin = "explicit";
@@ -1335,8 +1491,8 @@ class DEMSolver {
     std::set<unsigned> no_output;
     // the system's clump batches (flattened into the handle, in order) and what UpdateClumps checks against
     std::vector<std::shared_ptr<DEMClumpBatch>> system_batches;
-    size_t n_clumps_init = 0, n_clumps_system = 0, n_ext_init = 0, n_templates_init = 0, n_materials_init = 0,
-           n_presc_init = 0;
+    size_t n_clumps_init = 0, n_clumps_system = 0, n_ext_init = 0, n_mesh_init = 0, n_templates_init = 0,
+           n_materials_init = 0, n_presc_init = 0;
 };
 
 }  // namespace deme

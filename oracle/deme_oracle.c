@@ -52,6 +52,11 @@ struct oracle_ctx {
     float *aRX, *aRY, *aRZ, *aDX, *aDY, *aDZ, *aS1, *aS2, *aS3, *aMass;
     double *aC1, *aC2; /* cone: sin, cos of the half angle */
     float *E, *nu, *CoR, *mu, *Crr;
+    /* mesh facets: owner, nodes in the owner frame (9 floats), material */
+    uint32_t nT;
+    uint32_t* tOwner;
+    float* tNode;
+    uint16_t* tMat;
     uint8_t* masks;
     deme_family_prescription presc[DEME_NUM_FAMILIES];
     int nW;
@@ -189,6 +194,120 @@ static inline void anal_place(const oracle_ctx* c, uint32_t k, double* X, double
     *dx = ex;
     *dy = ey;
     *dz = ez;
+}
+
+/* ---------- sphere--mesh contacts (no reference counterpart: the reference declares SPHERE_MESH_CONTACT, Defines.h:66,
+ * but detects none).  Facet nodes placed like an analytical component (each node rotated in float, added to the owner
+ * position in double); the closest point of the facet to the sphere centre by the region tests of Ericson's
+ * closest-point-on-triangle algorithm (Real-Time Collision Detection, 5.1.5) in double; contact-detection reach =
+ * expanded radius + margin; dynamics with the plane's conventions (half the overlap as the depth, the normal from the
+ * closest point to the centre normalised in float, the face normal when the centre lies on the facet). ---------- */
+typedef struct {
+    double a[3], b[3], c[3];
+} tri_placed;
+
+static inline void tri_place(const oracle_ctx* c, uint32_t t, tri_placed* out) {
+    uint32_t o = c->tOwner[t];
+    double ox, oy, oz;
+    owner_pos(c, o, &ox, &oy, &oz);
+    const float* n = c->tNode + 9 * (size_t)t;
+    double* dst[3] = {out->a, out->b, out->c};
+    for (int k = 0; k < 3; k++) {
+        float x = n[3 * k], y = n[3 * k + 1], z = n[3 * k + 2];
+        rot_f(&x, &y, &z, c->qw[o], c->qx[o], c->qy[o], c->qz[o]);
+        dst[k][0] = ox + (double)x;
+        dst[k][1] = oy + (double)y;
+        dst[k][2] = oz + (double)z;
+    }
+}
+
+static void tri_closest(const tri_placed* t, double px, double py, double pz, double* q) {
+    const double abx = t->b[0] - t->a[0], aby = t->b[1] - t->a[1], abz = t->b[2] - t->a[2];
+    const double acx = t->c[0] - t->a[0], acy = t->c[1] - t->a[1], acz = t->c[2] - t->a[2];
+    const double apx = px - t->a[0], apy = py - t->a[1], apz = pz - t->a[2];
+    const double d1 = abx * apx + aby * apy + abz * apz, d2 = acx * apx + acy * apy + acz * apz;
+    if (d1 <= 0.0 && d2 <= 0.0) {
+        memcpy(q, t->a, sizeof(t->a));
+        return;
+    }
+    const double bpx = px - t->b[0], bpy = py - t->b[1], bpz = pz - t->b[2];
+    const double d3 = abx * bpx + aby * bpy + abz * bpz, d4 = acx * bpx + acy * bpy + acz * bpz;
+    if (d3 >= 0.0 && d4 <= d3) {
+        memcpy(q, t->b, sizeof(t->b));
+        return;
+    }
+    const double vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) {
+        const double v = d1 / (d1 - d3);
+        q[0] = t->a[0] + v * abx;
+        q[1] = t->a[1] + v * aby;
+        q[2] = t->a[2] + v * abz;
+        return;
+    }
+    const double cpx = px - t->c[0], cpy = py - t->c[1], cpz = pz - t->c[2];
+    const double d5 = abx * cpx + aby * cpy + abz * cpz, d6 = acx * cpx + acy * cpy + acz * cpz;
+    if (d6 >= 0.0 && d5 <= d6) {
+        memcpy(q, t->c, sizeof(t->c));
+        return;
+    }
+    const double vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) {
+        const double w = d2 / (d2 - d6);
+        q[0] = t->a[0] + w * acx;
+        q[1] = t->a[1] + w * acy;
+        q[2] = t->a[2] + w * acz;
+        return;
+    }
+    const double va = d3 * d6 - d5 * d4;
+    if (va <= 0.0 && (d4 - d3) >= 0.0 && (d5 - d6) >= 0.0) {
+        const double w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        q[0] = t->b[0] + w * (t->c[0] - t->b[0]);
+        q[1] = t->b[1] + w * (t->c[1] - t->b[1]);
+        q[2] = t->b[2] + w * (t->c[2] - t->b[2]);
+        return;
+    }
+    const double denom = 1.0 / (va + vb + vc);
+    const double v = vb * denom, w = vc * denom;
+    q[0] = t->a[0] + abx * v + acx * w;
+    q[1] = t->a[1] + aby * v + acy * w;
+    q[2] = t->a[2] + abz * v + acz * w;
+}
+
+static inline double tri_dist2(const tri_placed* t, double px, double py, double pz, double* q) {
+    tri_closest(t, px, py, pz, q);
+    return (px - q[0]) * (px - q[0]) + (py - q[1]) * (py - q[1]) + (pz - q[2]) * (pz - q[2]);
+}
+
+static inline int tri_overlap_cd(const tri_placed* t, double px, double py, double pz, double radA, float beta4) {
+    double q[3];
+    const double reach = radA + (double)beta4;
+    return tri_dist2(t, px, py, pz, q) <= reach * reach;
+}
+
+static int tri_overlap_dt(const tri_placed* t, double xA, double yA, double zA, double radA, double* CPX, double* CPY,
+                          double* CPZ, float* nX, float* nY, float* nZ, double* depth) {
+    double q[3];
+    const double d2 = tri_dist2(t, xA, yA, zA, q);
+    const double gap = sqrt(d2);
+    const double od = (radA - gap) / 2.0;
+    if (od < 0.0) return DEME_NOT_A_CONTACT;
+    if (gap > 0.0) {
+        *nX = (float)(xA - q[0]);
+        *nY = (float)(yA - q[1]);
+        *nZ = (float)(zA - q[2]);
+    } else {
+        const double abx = t->b[0] - t->a[0], aby = t->b[1] - t->a[1], abz = t->b[2] - t->a[2];
+        const double acx = t->c[0] - t->a[0], acy = t->c[1] - t->a[1], acz = t->c[2] - t->a[2];
+        *nX = (float)(aby * acz - abz * acy);
+        *nY = (float)(abz * acx - abx * acz);
+        *nZ = (float)(abx * acy - aby * acx);
+    }
+    normalize_f(nX, nY, nZ);
+    *depth = od;
+    *CPX = xA - (double)*nX * (gap + od);
+    *CPY = yA - (double)*nY * (gap + od);
+    *CPZ = zA - (double)*nZ * (gap + od);
+    return DEME_SPHERE_MESH_CONTACT;
 }
 
 /* Signed gap and outward (wall -> sphere) normal of the new curved shapes.  Returns 0 when undefined. */
@@ -401,6 +520,18 @@ oracle_ctx* orc_create(const deme_sim_params* p, const deme_scene* s) {
     XDUP(c->CoR, s->mat_CoR, nM);
     XDUP(c->mu, s->mat_mu, nM);
     XDUP(c->Crr, s->mat_Crr, nM);
+    c->nT = s->n_tris;
+    if (c->nT) {
+        XDUP(c->tOwner, s->tri_owner, c->nT);
+        XDUP(c->tMat, s->tri_material, c->nT);
+        XALLOC(c->tNode, 9 * (size_t)c->nT);
+        for (uint32_t t = 0; t < c->nT; t++)
+            for (int k = 0; k < 3; k++) {
+                c->tNode[9 * (size_t)t + k] = s->tri_node1[3 * (size_t)t + k];
+                c->tNode[9 * (size_t)t + 3 + k] = s->tri_node2[3 * (size_t)t + k];
+                c->tNode[9 * (size_t)t + 6 + k] = s->tri_node3[3 * (size_t)t + k];
+            }
+    }
     XALLOC(c->masks, DEME_NUM_FAMILY_MASK);
     if (s->family_masks) memcpy(c->masks, s->family_masks, DEME_NUM_FAMILY_MASK);
     if (s->prescriptions) memcpy(c->presc, s->prescriptions, sizeof(c->presc));
@@ -419,7 +550,8 @@ void orc_destroy(oracle_ctx* c) {
                     c->aRY,   c->aRZ,    c->aDX,    c->aDY,    c->aDZ,    c->aS1,    c->aS2,    c->aS3,   c->aMass,
                     c->aC1,   c->aC2,    c->E,      c->nu,     c->CoR,    c->mu,     c->Crr,    c->masks, c->idA,
                     c->idB,   c->map,    c->type,   c->wc,     c->F,      c->TOF,    c->CPA,    c->CPB,   c->pA,
-                    c->pB,    c->pT,     c->nBins,  c->nAnal,  c->pairBin, c->pairSph, c->oAFirst, c->oACount};
+                    c->pB,    c->pT,     c->nBins,  c->nAnal,  c->pairBin, c->pairSph, c->oAFirst, c->oACount,
+                    c->tOwner, c->tNode,  c->tMat};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     free(c);
 }
@@ -454,6 +586,7 @@ int32_t orc_detect_contacts(oracle_ctx* c) {
     double bs = p->bin_size;
     uint32_t* binOff = calloc((size_t)nS + 1, sizeof(uint32_t));
     uint32_t* analOff = calloc((size_t)nS + 1, sizeof(uint32_t));
+    uint32_t* nMeshS = calloc((size_t)nS + 1, sizeof(uint32_t));
     double* PX = malloc((size_t)nS * sizeof(double) * 3);
     /* getNumberOfBinsEachSphereTouches, DEMBinSphereKernels.cu:12-115 */
 #pragma omp parallel for num_threads(g_threads) schedule(static)
@@ -484,11 +617,19 @@ int32_t orc_detect_contacts(oracle_ctx* c) {
             if (anal_overlap_cd(c, k, x, y, z, myRadius, ax, ay, az, dx, dy, dz, p->beta)) cnt++;
         }
         c->nAnal[s] = cnt;
+        uint32_t mcnt = 0;
+        for (uint32_t t = 0; t < c->nT; t++) {
+            if (c->masks[mask_index(sf, c->fam[c->tOwner[t]])] != 0) continue;
+            tri_placed tp;
+            tri_place(c, t, &tp);
+            if (tri_overlap_cd(&tp, x, y, z, myRadius, p->beta)) mcnt++;
+        }
+        nMeshS[s] = mcnt;
     }
     /* ExclusiveScans, DEMCubContactDetection.cu:77-96 */
     for (uint32_t s = 0; s < nS; s++) {
         binOff[s + 1] = binOff[s] + c->nBins[s];
-        analOff[s + 1] = analOff[s] + c->nAnal[s];
+        analOff[s + 1] = analOff[s] + c->nAnal[s] + nMeshS[s];
     }
     uint32_t P = binOff[nS], nGeo = analOff[nS];
     if (P > c->capPairs) {
@@ -530,6 +671,18 @@ int32_t orc_detect_contacts(oracle_ctx* c) {
                 gA[goff] = s;
                 gB[goff] = k;
                 gT[goff] = (uint8_t)ct;
+                goff++;
+            }
+        }
+        /* sphere--mesh contacts after the analytical ones, by facet id */
+        for (uint32_t t = 0; t < c->nT; t++) {
+            if (c->masks[mask_index(sf, c->fam[c->tOwner[t]])] != 0) continue;
+            tri_placed tp;
+            tri_place(c, t, &tp);
+            if (tri_overlap_cd(&tp, x, y, z, myRadius, p->beta)) {
+                gA[goff] = s;
+                gB[goff] = t;
+                gT[goff] = DEME_SPHERE_MESH_CONTACT;
                 goff++;
             }
         }
@@ -687,6 +840,7 @@ int32_t orc_detect_contacts(oracle_ctx* c) {
     free(PX);
     free(binOff);
     free(analOff);
+    free(nMeshS);
     return DEME_OK;
 }
 
@@ -737,6 +891,16 @@ static void contact_force(oracle_ctx* c, uint32_t i) {
             CPy = By + (radB - depth / (double)2) * (double)nY;
             CPz = Bz + (radB - depth / (double)2) * (double)nZ;
         }
+    } else if (ctype == DEME_SPHERE_MESH_CONTACT) {
+        uint32_t t = c->idB[i];
+        oB = c->tOwner[t];
+        matB = c->tMat[t];
+        BOwnerMass = c->mass[oB];
+        BRadius = (float)HUGE_FLOAT;
+        owner_pos(c, oB, &BOx, &BOy, &BOz);
+        tri_placed tp;
+        tri_place(c, t, &tp);
+        ctype = tri_overlap_dt(&tp, Ax, Ay, Az, (double)ARadius, &CPx, &CPy, &CPz, &nX, &nY, &nZ, &depth);
     } else {
         uint32_t k = c->idB[i];
         oB = c->aOwner[k];
@@ -882,6 +1046,7 @@ static void contact_force(oracle_ctx* c, uint32_t i) {
 
 /* ---------- dT: force collection (DEMCubForceCollection.cu:20-158, DEMCollectForceKernels.cu:11-133) ---------- */
 static inline uint32_t owner_of_B(const oracle_ctx* c, uint32_t i) {
+    if (c->type[i] == DEME_SPHERE_MESH_CONTACT) return c->tOwner[c->idB[i]];
     return c->type[i] == DEME_SPHERE_SPHERE_CONTACT ? c->sOwner[c->idB[i]] : c->aOwner[c->idB[i]];
 }
 
@@ -1176,8 +1341,11 @@ int32_t orc_bin_assignment(oracle_ctx* c, uint16_t* n_bins, uint8_t* n_anal, uin
 /* Kinetic energy of clump owners (DEMOwnerQueryKernels.cu:10-37 per-owner term), summed in double. */
 double orc_kinetic_energy(oracle_ctx* c) {
     double ke = 0;
-    for (uint32_t o = 0; o < c->nO; o++) {
-        if (c->mass[o] >= 1e14f) continue; /* analytical owners (mass 1e15, BdrsAndObjs.h:114) */
+    /* clump owners only (they are the owners the spheres reference; external and mesh objects follow them) */
+    uint32_t nClumps = 0;
+    for (uint32_t s = 0; s < c->nS; s++)
+        if (c->sOwner[s] + 1 > nClumps) nClumps = c->sOwner[s] + 1;
+    for (uint32_t o = 0; o < nClumps; o++) {
         double v2 = (double)c->vX[o] * c->vX[o] + (double)c->vY[o] * c->vY[o] + (double)c->vZ[o] * c->vZ[o];
         double r2 = (double)c->mXX[o] * c->wX[o] * c->wX[o] + (double)c->mYY[o] * c->wY[o] * c->wY[o] +
                     (double)c->mZZ[o] * c->wZ[o] * c->wZ[o];

@@ -48,8 +48,10 @@ def reference(built, threads=4):
 
 
 def canonical_order(c: dict) -> np.ndarray:
-    """Permutation putting a contact list in (idA, group, idB) order, group 0 = sphere--analytical."""
-    grp = (c["type"] == capi.SPHERE_SPHERE_CONTACT).astype(np.int64)
+    """Permutation putting a contact list in (idA, group, idB) order, groups sphere--analytical, sphere--mesh,
+    sphere--sphere."""
+    t = c["type"].astype(np.int64)
+    grp = np.where(t == capi.SPHERE_SPHERE_CONTACT, 2, np.where(t == capi.SPHERE_MESH_CONTACT, 1, 0))
     return np.lexsort((c["idB"].astype(np.int64), grp, c["idA"].astype(np.int64)))
 
 

@@ -37,6 +37,11 @@ static void put(std::ofstream& out, const char* name, const std::vector<T>& v) {
     put(out, name, v.data(), v.size());
 }
 
+// the mesh body of the scene (the Python side writes the same text)
+static const char* kMeshObj =
+    "v 0 0 0\nv 0.02 0 0\nv 0.02 0.02 0\nv 0 0.02 0\nv 0.01 0.01 0.015\n"
+    "f 1 2 3 4\nf 1/1 2/1 5/1\nf -4 -3 -1\nf 3 4 5\nf 4 1 5\n";
+
 int main(int argc, char** argv) {
     if (argc < 3 || argc > 5) return 2;
     std::ifstream in(argv[1], std::ios::binary);
@@ -87,6 +92,18 @@ int main(int argc, char** argv) {
     wall->AddCylinder(float3{0.f, 0.f, 0.f}, float3{0.f, 0.f, 1.f}, 0.12f, m0);
     wall->AddCone(float3{0.f, 0.f, -0.2f}, float3{0.f, 0.f, 1.f}, 0.5235988f, 0.03f, 0.15f, m1);
     wall->SetFamily(10);
+    {
+        // a mesh body (Wavefront file, a quad split in two and four triangles, per-facet materials)
+        const std::string obj = std::string(argv[2]) + ".obj";
+        std::ofstream(obj) << kMeshObj;
+        auto mesh = s.AddWavefrontMeshObject(obj, m0);
+        mesh->SetMaterial(std::vector<std::shared_ptr<DEMMaterial>>{m0, m1, m0, m1, m0, m1});
+        mesh->SetInitPos(float3{0.02f, 0.08f, -0.06f});
+        mesh->SetInitQuat(float4{0.f, 0.6f, 0.f, 0.8f});
+        mesh->SetMass(2.5f);
+        mesh->SetMOI(float3{1e-3f, 2e-3f, 3e-3f});
+        mesh->SetFamily(3);
+    }
     s.SetFamilyFixed(3);
     s.SetFamilyPrescribedAngVel(10, "0", "2.0943951", "0");
     s.SetFamilyPrescribedLinVel(4, "0.1", "none", "0");
@@ -145,6 +162,11 @@ int main(int argc, char** argv) {
     put(out, "mat_mu", f.mat_mu);
     put(out, "mat_Crr", f.mat_Crr);
     put(out, "family_masks", f.family_masks);
+    put(out, "tri_owner", f.tri_owner);
+    put(out, "tri_node1", f.tri_node1);
+    put(out, "tri_node2", f.tri_node2);
+    put(out, "tri_node3", f.tri_node3);
+    put(out, "tri_material", f.tri_material);
     put(out, "prescriptions", f.prescriptions);
     {
         // families handed to deme_set_prescribed_motion: family, four flags, nine strings, '|'-separated lines

@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_status_strings():
     lib = solver.load_product_library()
-    assert lib.deme_abi_version() == 4
+    assert lib.deme_abi_version() == 5
     assert lib.deme_status_string(0) == b"DEME_OK"
     assert lib.deme_status_string(6) == b"DEME_ERR_TIMEOUT"
 

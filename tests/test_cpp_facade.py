@@ -3,7 +3,8 @@
 tests/cpp/facade_dump.cpp builds a scene with every kind of input (sphere and clump templates with mixed
 materials, two clump batches with orientations, velocities and families, bounding planes, an extra plane, a
 cylinder and a cone on one family-10 object, fixed and prescribed families, a family mask, contact margin and CD
-frequency) through the C++ API, and writes the flat arrays Initialize would upload.  The same scene is built here
+frequency, a Wavefront mesh body with per-facet materials) through the C++ API, and writes the flat arrays Initialize
+would upload.  The same scene is built here
 with SceneBuilder; every array and the parameter and prescription structs must agree bit for bit.  Compiling and
 running the C++ side needs no GPU.
 """
@@ -11,6 +12,7 @@ import ctypes as C
 import os
 import shutil
 import subprocess
+import tempfile
 
 import numpy as np
 import pytest
@@ -35,6 +37,11 @@ def scene_inputs(seed=5):
     fam1 = rng.integers(0, 6, n1).astype(np.int32)
     xyz2 = rng.uniform(-0.1, 0.1, (n2, 3)).astype(f32)
     return types, xyz1, q1, v1, w1, fam1, xyz2
+
+
+# the mesh body of the scene (tests/cpp/facade_dump.cpp writes the same text)
+MESH_OBJ = ("v 0 0 0\nv 0.02 0 0\nv 0.02 0.02 0\nv 0 0.02 0\nv 0.01 0.01 0.015\n"
+            "f 1 2 3 4\nf 1/1 2/1 5/1\nf -4 -3 -1\nf 3 4 5\nf 4 1 5\n")
 
 
 def python_scene(types, xyz1, q1, v1, w1, fam1, xyz2, extra=None):
@@ -65,6 +72,17 @@ def python_scene(types, xyz1, q1, v1, w1, fam1, xyz2, extra=None):
     wall.AddCylinder((0, 0, 0), (0, 0, 1), 0.12, m0)
     wall.AddCone((0, 0, -0.2), (0, 0, 1), float(f32(0.5235988)), 0.03, 0.15, m1)
     wall.SetFamily(10)
+    with tempfile.TemporaryDirectory() as d:
+        obj = os.path.join(d, "mesh.obj")
+        with open(obj, "w") as fh:
+            fh.write(MESH_OBJ)
+        mesh = s.AddWavefrontMeshObject(obj, m0)
+    mesh.SetMaterial([m0, m1, m0, m1, m0, m1])
+    mesh.SetInitPos((0.02, 0.08, -0.06))
+    mesh.SetInitQuat((0.8, 0.0, 0.6, 0.0))
+    mesh.SetMass(2.5)
+    mesh.SetMOI((1e-3, 2e-3, 3e-3))
+    mesh.SetFamily(3)
     s.SetFamilyFixed(3)
     s.SetFamilyPrescribedAngVel(10, "0", "2.0943951", "0")
     s.SetFamilyPrescribedLinVel(4, "0.1", "none", "0")
@@ -144,7 +162,7 @@ def test_csv_output_agrees_byte_for_byte(dump, tmp_path):
 def test_flat_arrays_agree_bit_for_bit(dump):
     cpp, built = dump
     names = [k for k in cpp if k not in ("params", "prescriptions", "motion") and not k.startswith("csv_")]
-    assert len(names) == 45
+    assert len(names) == 50
     for k in names:
         py = np.ascontiguousarray(built.arrays[k])
         assert cpp[k] == py.tobytes(), f"array {k} differs"

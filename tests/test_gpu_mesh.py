@@ -1,0 +1,138 @@
+"""Sphere--mesh contacts (triangle facets of mesh-represented owners), CUDA path against the C oracle.
+
+The reference loads mesh bodies (DEMMeshConnected) and declares the sphere--mesh contact type but detects no such
+contact, so these scenes are pinned to the oracle's restatement only (closest point on the facet by Ericson's region
+tests; the plane's conventions for depth, normal and contact point).  Bars as in test_gpu_walls: contact lists,
+partners and remapped history bit-exact; per-contact forces within 1e-5 relative; owner accelerations within 1e-5
+of the sum of contribution magnitudes; one-step velocities within 1e-5 relative, positions within 1e-9 m.
+
+* a square funnel of 160 facets (walls and floor on 4 x 4 grids of split quads) with 1500 spheres pressed into it:
+  contacts on facet interiors, edges and corners, a fixed mesh owner;
+* a free icosphere of 1280 facets driven into a bed of 2000 spheres inside analytical planes: a moving, rotating
+  mesh owner whose reactions are collected and integrated;
+* a floor of two large facets against the same floor as an analytical plane: the same contacts, forces equal to
+  float rounding (each facet spans hundreds of search cells, so the facet cell lists outgrow their first buffer
+  and the search grows them and runs again);
+* scope: packed scenes and the adjoint refuse meshes; graph replay falls back to plain steps.
+"""
+import numpy as np
+import pytest
+
+from _util import canonical, contact_key, oracle, workloads, capi
+from test_gpu_parity import gpu_solver
+from test_gpu_walls import lockstep
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def mesh_scenes():
+    return {
+        "funnel_fixed_mesh": lambda: workloads.mesh_funnel(n=1500, seed=31, wall_clearance=0.8),
+        "ball_drop_free_mesh": lambda: workloads.mesh_ball_drop(n=2000, seed=32, press=0.2),
+    }
+
+
+@pytest.mark.parametrize("name", sorted(mesh_scenes()))
+def test_gpu_mesh_contacts_match_oracle_lockstep(name):
+    built = mesh_scenes()[name]()
+    n_type = lockstep(built, 4, name)
+    assert n_type[capi.SPHERE_MESH_CONTACT] > 20, n_type
+
+
+def test_gpu_free_running_ball_drop_matches_oracle():
+    """200 free steps of the ball drop (detection every step): the lists of the first 20 steps stay bit-identical,
+    the ball's velocity and the kinetic energy agree to 1e-4 at the end."""
+    built = workloads.mesh_ball_drop(n=2000, seed=33, press=0.1)
+    g = gpu_solver(built, keep=False)
+    o = oracle(built)
+    for step in range(200):
+        g.step(1)
+        o.step(1)
+        if step < 20:
+            np.testing.assert_array_equal(contact_key(g.contacts()), contact_key(canonical(o.contacts())),
+                                          err_msg=f"step {step}")
+    gs, os_ = g.state(), o.state()
+    vb_g = np.array([gs[k][-1] for k in ("vX", "vY", "vZ")], np.float64)
+    vb_o = np.array([os_[k][-1] for k in ("vX", "vY", "vZ")], np.float64)
+    assert np.abs(vb_g - vb_o).max() <= 1e-4 * np.abs(vb_o).max(), (vb_g, vb_o)
+    ke_g, ke_o = g.kinetic_energy(), o.kinetic_energy()
+    assert abs(ke_g - ke_o) <= 1e-4 * abs(ke_o), (ke_g, ke_o)
+    assert np.any(g.contacts()["type"] == capi.SPHERE_MESH_CONTACT)
+    g.close()
+    o.close()
+
+
+def _pile(mesh_floor: bool):
+    """sphere_pile's 400 spheres on its floor, an analytical plane or two facets 0.19 m wide in the same plane."""
+    return workloads.sphere_pile(n=400, seed=5, mesh_floor=mesh_floor)
+
+
+def test_gpu_mesh_floor_equals_analytical_plane():
+    plane, mesh = _pile(False), _pile(True)
+    gp, gm = gpu_solver(plane), gpu_solver(mesh)
+    ever_double = np.zeros(0, np.int64)
+    for step in range(3):
+        gp.detect_contacts()
+        gm.detect_contacts()
+        cp, cm = gp.contacts(), gm.contacts()
+        wall_p = cp["type"] == capi.SPHERE_PLANE_CONTACT
+        wall_m = cm["type"] == capi.SPHERE_MESH_CONTACT
+        assert wall_p.sum() > 20
+        # a sphere over the shared diagonal touches both facets: compare the spheres that touch one
+        idA_m, cnt = np.unique(cm["idA"][wall_m], return_counts=True)
+        ever_double = np.union1d(ever_double, idA_m[cnt > 1])
+        single = np.setdiff1d(idA_m[cnt == 1], ever_double)
+        assert len(single) > 20
+        np.testing.assert_array_equal(np.unique(cp["idA"][wall_p]), idA_m)
+        np.testing.assert_array_equal(cp["idA"][~wall_p], cm["idA"][~wall_m])
+        np.testing.assert_array_equal(cp["idB"][~wall_p], cm["idB"][~wall_m])
+        gp.compute_forces()
+        gm.compute_forces()
+        fp, fm = gp.contact_forces(), gm.contact_forces()
+        ip = np.nonzero(wall_p & np.isin(cp["idA"], single))[0]
+        im = np.nonzero(wall_m & np.isin(cm["idA"], single))[0]
+        for k in ("force", "torque_only_force", "cpA"):
+            a, b = fm[k][im].astype(np.float64), fp[k][ip].astype(np.float64)
+            scale = np.abs(b).max() + 1e-30
+            assert np.abs(a - b).max() <= 1e-5 * scale, (step, k, np.abs(a - b).max(), scale)
+        gp.integrate()
+        gm.integrate()
+        sm = gm.state()
+        gp.set_state({k: sm[k][:plane.counts["o"]] for k in ("voxel", "locX", "locY", "locZ", "oriQw", "oriQx",
+                                                               "oriQy", "oriQz", "vX", "vY", "vZ", "omgX", "omgY",
+                                                               "omgZ")})
+    gp.close()
+    gm.close()
+
+
+def test_gpu_mesh_scope():
+    from deme_b200 import Solver, adjoint
+    from deme_b200.scene import SceneBuilder
+    from deme_b200.solver import DemeError
+    # packed scenes (per-batch search grids) and meshes do not mix
+    s = SceneBuilder()
+    s.InstructBoxDomainDimension(0.2, 0.2, 0.2)
+    s.SetCoordSysOrigin("center")
+    m = s.LoadMaterial({"E": 1e7, "nu": 0.3, "CoR": 0.5, "mu": 0.3, "Crr": 0.0})
+    t = s.LoadSphereType(1e-4, 2.5e-3, m)
+    s.AddClumps([t] * 8, np.random.default_rng(0).uniform(-0.02, 0.02, (8, 3)).astype(np.float32)).SetSceneBox(
+        (-0.05, -0.05, -0.05), (0.05, 0.05, 0.05))
+    s.AddWavefrontMeshObject((np.eye(3, dtype=np.float32) * 0.01, np.array([[0, 1, 2]])), m)
+    s.SetInitTimeStep(1e-5)
+    with pytest.raises(DemeError, match="mesh facets are not supported together with packed scenes"):
+        Solver(s.Initialize())
+    built = workloads.mesh_funnel(n=300, seed=34, wall_clearance=0.9)
+    g = Solver(built)
+    with pytest.raises(DemeError, match="INVALID.*mesh"):
+        adjoint.record(g, 2, 1)
+    # graph replay is requested but mesh scenes step plainly: the same lists as plain steps
+    h = Solver(built)
+    g.set_graph(True)
+    g.step(10)
+    h.step(10)
+    np.testing.assert_array_equal(contact_key(g.contacts()), contact_key(h.contacts()))
+    assert g.graph_stats()[0] == 0
+    g.close()
+    h.close()

@@ -37,8 +37,12 @@ def owner_scale(built, c, f):
     owner = a["sphere_owner"]
     oA = owner[c["idA"]]
     ss = c["type"] == capi.SPHERE_SPHERE_CONTACT
-    oB = np.where(ss, owner[np.where(ss, c["idB"], 0)], a["anal_owner"][np.where(ss, 0, c["idB"])] if len(
+    me = c["type"] == capi.SPHERE_MESH_CONTACT
+    an = ~ss & ~me
+    oB = np.where(ss, owner[np.where(ss, c["idB"], 0)], a["anal_owner"][np.where(an, c["idB"], 0)] if len(
         a["anal_owner"]) else 0)
+    if me.any():
+        oB = np.where(me, a["tri_owner"][np.where(me, c["idB"], 0)], oB)
     Fm = np.linalg.norm(f["force"].astype(np.float64), axis=1) + np.linalg.norm(
         f["torque_only_force"].astype(np.float64), axis=1)
     lin = np.zeros(nO)

@@ -31,11 +31,12 @@ def wall_scenes():
 
 
 def lockstep(built, steps, name):
-    """Each step: CD, forces, integration on both; compare; then give the GPU the oracle's state and history."""
+    """Each step: CD, forces, integration on both; compare; then give the GPU the oracle's state and history.
+    Returns the contacts seen, counted by type."""
     g = gpu_solver(built)
     o = oracle(built)
     prev = None
-    n_curved = 0
+    n_type = np.zeros(8, np.int64)
     for step in range(steps):
         g.detect_contacts()
         o.detect_contacts()
@@ -44,7 +45,7 @@ def lockstep(built, steps, name):
         gc = g.contacts()
         for k in ("idA", "idB", "type"):
             np.testing.assert_array_equal(gc[k], rc[k], err_msg=f"{name} step {step} {k}")
-        n_curved += int(np.sum(rc["type"] >= 5))
+        n_type += np.bincount(rc["type"], minlength=8)
         if prev is not None:
             np.testing.assert_array_equal(partner_keys(gc, prev), partner_keys(oc, prev_o)[rc["perm"]],
                                           err_msg=f"{name} step {step} partners")
@@ -81,14 +82,14 @@ def lockstep(built, steps, name):
                         "wildcards": oc_post["wildcards"]})
         prev = {k: rc[k] for k in ("idA", "idB", "type")}
         prev_o = {k: oc[k] for k in ("idA", "idB", "type")}
-    return n_curved
+    return n_type
 
 
 @pytest.mark.parametrize("name", sorted(wall_scenes()))
 def test_gpu_curved_walls_match_oracle_lockstep(name):
     built = wall_scenes()[name]()
-    n_curved = lockstep(built, 4, name)
-    assert n_curved > 0, "the scene must exercise cylinder or cone contacts"
+    n_type = lockstep(built, 4, name)
+    assert n_type[5:7].sum() > 0, "the scene must exercise cylinder or cone contacts"
 
 
 def test_gpu_contact_margin_every_5_steps_matches_oracle():
