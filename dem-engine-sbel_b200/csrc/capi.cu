@@ -157,25 +157,25 @@ static int32_t ensure_cand(deme_handle* h, uint32_t n) {
     return DEME_OK;
 }
 
-// Room for n (cell, facet) entries of the mesh-facet cell lists.
-static int32_t ensure_tri_cells(deme_handle* h, uint32_t n) {
-    if (n <= h->cd.triCellCap && h->cd.triCell) return DEME_OK;
+// Room for n (sphere, facet) pairs in the mesh pool.
+static int32_t ensure_mesh_pool(deme_handle* h, uint32_t n) {
+    if (n <= h->cd.meshCap && h->cd.meshPool) return DEME_OK;
     const uint32_t cap = std::max<uint32_t>(1024u, (uint32_t)std::min<uint64_t>(0xFFFFFFF0ull, (uint64_t)n * 5 / 4 + 64));
-    dfree(h, h->cd.triCell);
-    h->cd.triCell = nullptr;
-    h->cd.triCellCap = 0;
-    TRY(dalloc_n(h, &h->cd.triCell, cap));
-    h->cd.triCellCap = cap;
+    dfree(h, h->cd.meshPool);
+    h->cd.meshPool = nullptr;
+    h->cd.meshCap = 0;
+    TRY(dalloc_n(h, &h->cd.meshPool, cap));
+    h->cd.meshCap = cap;
     return DEME_OK;
 }
 
-// A search's counts (total, pool, overflow spheres, -, facet cell entries) fit the buffers it wrote into.
+// A search's counts (total, pool, overflow spheres, -, mesh pairs) fit the buffers it wrote into.
 static bool search_fits(const deme_handle* h, const uint32_t* c) {
-    return c[1] <= h->candCap && (!h->nT || c[4] <= h->cd.triCellCap);
+    return c[1] <= h->candCap && (!h->nT || c[4] <= h->cd.meshCap);
 }
 static int32_t grow_search(deme_handle* h, const uint32_t* c) {
     TRY(ensure_cand(h, c[1]));
-    if (h->nT) TRY(ensure_tri_cells(h, c[4]));
+    if (h->nT) TRY(ensure_mesh_pool(h, c[4]));
     return DEME_OK;
 }
 
@@ -622,12 +622,7 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
     TRY(dalloc_n(h, &cd.counters, 8));
     CUDA_TRY(h, cudaMemset(cd.counters, 0, 8 * sizeof(uint32_t)));
     TRY(ensure_cand(h, std::max<uint32_t>(1024u, 2u * nS)));
-    if (h->nT) {
-        TRY(dalloc_n(h, &cd.triCellCount, (size_t)h->nCells + 1));
-        TRY(dalloc_n(h, &cd.triCellStart, (size_t)h->nCells + 1));
-        TRY(dalloc_n(h, &cd.nMesh, std::max(nS, 1u)));
-        TRY(ensure_tri_cells(h, std::max<uint32_t>(1024u, 8u * h->nT)));
-    }
+    if (h->nT) TRY(ensure_mesh_pool(h, std::max<uint32_t>(1024u, 2u * h->nT)));
     for (int b = 0; b < 2; b++) {
         TRY(dalloc_n(h, &h->lists[b].off, (size_t)nS + 1));
         CUDA_TRY(h, cudaMemset(h->lists[b].off, 0, ((size_t)nS + 1) * sizeof(uint32_t)));
@@ -742,8 +737,8 @@ int32_t deme_keep_contact_forces(deme_handle* h, int32_t enable) {
 // ---------------------------------------------------------------------------------------------------- kT ----
 // Contact search up to the per-sphere offsets of the new list (into lists[cur ^ 1].off, its count into .dN), for the
 // poses in `s`, with the analytical components placed into `anal` (and the mesh facets into s.tri).  The pair total,
-// the pool count, its overflow counter and the facet cell-list total are copied to `hCnt` (pinned, unless null;
-// words 0, 1, 2 and 4) at the end, on `st`; nothing here waits for the device.
+// the pool count, its overflow counter and the mesh-pair count are copied to `hCnt` (pinned, unless null; words 0,
+// 1, 2 and 4) at the end, on `st`; nothing here waits for the device.
 static int32_t cd_search(deme_handle* h, const StateView& s, AnalPlaced* anal, cudaStream_t st, bool retry,
                          uint32_t* hCnt) {
     const SimConsts& k = h->k;
@@ -752,14 +747,6 @@ static int32_t cd_search(deme_handle* h, const StateView& s, AnalPlaced* anal, c
     launch_place_tri(k, s, h->triRaw, st);
     // the forces of this step, on the same poses, reuse the placement
     if (anal == h->analPlaced) h->analFresh = true;
-    if (h->nT) {
-        // cell lists of the mesh facets: counts, offsets (total in counters[4]), entries
-        CUDA_TRY(h, cudaMemsetAsync(cd.triCellCount, 0, ((size_t)h->nCells + 1) * sizeof(uint32_t), st));
-        launch_tri_bin(k, s, cd, false, st);
-        exclusive_scan_u32_onepass(cd.triCellCount, h->nCells + 1, cd.triCellStart, cd.counters + 4, h->scratch,
-                                   h->dErr, st);
-        launch_tri_bin(k, s, cd, true, st);
-    }
     CUDA_TRY(h, cudaMemsetAsync(cd.cellCount, 0, ((size_t)h->nCells + 1) * sizeof(uint32_t), st));
     launch_sphere_prep(k, s, cd, st);
     exclusive_scan_u32_onepass(cd.cellCount, h->nCells + 1, cd.cellStart, nullptr, h->scratch, h->dErr, st);
@@ -770,9 +757,10 @@ static int32_t cd_search(deme_handle* h, const StateView& s, AnalPlaced* anal, c
         launch_cell_scatter(k, s, cd, st);  // counting sort and record writes in one pass
     }
     ContactBuf& nb = h->lists[h->cur ^ 1];
-    // pool, overflow spheres, tile queue, overflow entries
-    CUDA_TRY(h, cudaMemsetAsync(cd.counters, 0, 4 * sizeof(uint32_t), st));
+    // pool, overflow spheres, tile queue, overflow entries, mesh pairs
+    CUDA_TRY(h, cudaMemsetAsync(cd.counters, 0, 5 * sizeof(uint32_t), st));
     if (retry) launch_cnt_init(k, cd, st);
+    launch_mesh_find(k, s, cd, st);
     launch_pair_find(k, s, cd, h->candCap, h->findShape, st);
     launch_pair_overflow(k, s, cd, h->candCap, st);
     TRY(check_launch(h, "contact search"));
@@ -788,10 +776,12 @@ static int32_t cd_search(deme_handle* h, const StateView& s, AnalPlaced* anal, c
 // Writes the new list (n contacts, pool of `pool` pairs) in canonical order into lists[cur ^ 1], on `st`.  While a
 // graph is recorded the counts are unknown: n and pool are the capacities, and the kernels read the counts on the
 // device.
-static int32_t cd_assemble(deme_handle* h, const StateView& s, uint32_t n, uint32_t pool, cudaStream_t st) {
+static int32_t cd_assemble(deme_handle* h, const StateView& s, uint32_t n, uint32_t pool, uint32_t meshPairs,
+                           cudaStream_t st) {
     ContactBuf& nb = h->lists[h->cur ^ 1];
     if (!h->capturing) TRY(ensure_list(h, nb, n));
     launch_pair_scatter(h->k, h->cd, nb.view(), pool, nb.cap, h->candCap, st);
+    launch_mesh_scatter(h->k, h->cd, nb.view(), meshPairs, nb.cap, st);
     launch_pair_assemble(h->k, s, h->cd, nb.view(), nb.cap, st);
     return check_launch(h, "contact assembly");
 }
@@ -816,7 +806,7 @@ static int32_t cd_sync(deme_handle* h) {
     if (h->capturing) {
         // recorded into a graph: no host read; launches cover the capacities, kernels read the counts
         TRY(cd_search(h, s, h->analPlaced, st, false, nullptr));
-        TRY(cd_assemble(h, s, h->lists[h->cur ^ 1].cap, h->candCap, st));
+        TRY(cd_assemble(h, s, h->lists[h->cur ^ 1].cap, h->candCap, h->cd.meshCap, st));
         return cd_adopt(h, h->lists[h->cur ^ 1].cap);
     }
     TRY(refresh_count(h));
@@ -833,7 +823,7 @@ static int32_t cd_sync(deme_handle* h) {
         h->err = "contact search: pair list still over capacity after growing";
         return DEME_ERR_OVERFLOW;
     }
-    TRY(cd_assemble(h, s, n, h->hTotal[1], st));
+    TRY(cd_assemble(h, s, n, h->hTotal[1], h->nT ? h->hTotal[4] : 0u, st));
     TRY(cd_adopt(h, n));
     return read_device_errors(h);
 }
@@ -892,7 +882,7 @@ static int32_t cd_finish(deme_handle* h) {
         }
     }
     const uint32_t n = h->hCounts[0];
-    TRY(cd_assemble(h, ks, n, h->hCounts[1], kt));
+    TRY(cd_assemble(h, ks, n, h->hCounts[1], h->nT ? h->hCounts[4] : 0u, kt));
     CUDA_TRY(h, cudaEventRecord(h->evListReady, kt));
     CUDA_TRY(h, cudaStreamWaitEvent(h->st_dt, h->evListReady, 0));
     TRY(cd_adopt(h, n));

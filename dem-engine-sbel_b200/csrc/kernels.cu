@@ -144,19 +144,20 @@ void launch_place_tri(const SimConsts& k, const StateView& s, const TriRaw* raw,
     k_place_tri<<<blocks_for(k.n_tris, 64), 64, 0, st>>>(k, s, raw, k.n_tris);
 }
 
-// Cell lists of the mesh facets, one warp per facet.  A sphere in cell c can touch facet t only if its centre lies
-// within the reach (largest expanded radius + beta) of t, so t is listed in every cell whose box comes that close:
-// the cells of t's reach box, less those whose box (open to the outside at the grid's faces, where cell_of clamps,
-// and cut to the reach box) has its centre farther from t than the reach plus its half diagonal.  Each sphere then
-// tests the facets of its home cell only, so every (sphere, facet) pair is met once.  kEmit false: counts per cell;
-// true: the entries, at start + the count taken down (the order inside a cell is not defined; the assembly sorts
-// by facet id).  Entries past the capacity are dropped and their total, read by the host, makes it grow the list.
-template <bool kEmit>
-__global__ void __launch_bounds__(128) k_tri_bin(SimConsts k, StateView s, CDView cd) {
+// Sphere--mesh contact search, one warp per facet, once the spheres are in cell order.  A sphere in cell c can touch
+// facet t only if its centre lies within the reach (largest expanded radius + beta) of t, so the facet visits the
+// cells of its reach box, less those whose box (open to the outside at the grid's faces, where cell_of clamps, and
+// cut to the reach box) has its centre farther from t than the reach plus its half diagonal, and tests the spheres
+// of each: family mask, then the exact test at the sphere's exact centre with its expanded radius + beta.  Every
+// sphere lies in one home cell and the facet visits each cell once, so each (sphere, facet) pair is found once.  A
+// pair adds one to the sphere's contact count and is appended to the mesh pool; entries past the pool's capacity
+// are dropped and their total (counters[4]), read by the host, makes it grow the pool and search again.
+__global__ void __launch_bounds__(128) k_mesh_find(SimConsts k, StateView s, CDView cd) {
     const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
     if (t >= k.n_tris) return;
     const TriPlaced tp = s.tri[t];
+    const uint32_t famT = s.loc[tp.owner].w;
     const SearchGrid& g = k.grid0;
     const double cs = 1.0 / g.inv_cell;
     const double reach = (double)k.r_max_cd + (double)k.beta + 1e-6 * cs;
@@ -169,7 +170,7 @@ __global__ void __launch_bounds__(128) k_tri_bin(SimConsts k, StateView s, CDVie
     for (int d = 0; d < 3; d++) {
         c0[d] = cell_of(lo[d], g.inv_cell, gdim[d]);
         const uint32_t c1 = cell_of(hi[d], g.inv_cell, gdim[d]);
-        if (!(c1 >= c0[d])) return;  // a facet with non-finite nodes is listed nowhere
+        if (!(c1 >= c0[d])) return;  // a facet with non-finite nodes meets nothing
         nc[d] = c1 - c0[d] + 1u;
     }
     const uint64_t total = (uint64_t)nc[0] * nc[1] * nc[2];
@@ -187,45 +188,55 @@ __global__ void __launch_bounds__(128) k_tri_bin(SimConsts k, StateView s, CDVie
         const double lim = reach + sqrt(hd2);
         if (tri_dist2(tp, ctr[0], ctr[1], ctr[2], qx, qy, qz) > lim * lim) continue;
         const uint32_t key = ci[0] + g.gx * (ci[1] + g.gy * ci[2]);
-        if (!kEmit) {
-            atomicAdd(&cd.triCellCount[key], 1u);
-        } else {
-            const uint32_t slot = cd.triCellStart[key] + atomicSub(&cd.triCellCount[key], 1u) - 1u;
-            if (slot < cd.triCellCap) cd.triCell[slot] = t;
+        const uint32_t b = cd.cellStart[key], e = min(cd.cellStart[key + 1], k.n_spheres);
+        for (uint32_t p = b; p < e; p++) {
+            if (s.masks[mask_index(cd.rngS[p].w, famT)] != 0) continue;
+            const SphCD r = cd.recS[p];
+            const uint32_t sid = __float_as_uint(cd.posFSorted[p].w) & k.id_mask;
+            if (!index_ok(k.err, 19, sid, k.n_spheres)) continue;
+            double rD = (double)s.sph[sid].w;
+            rD += (double)k.beta;
+            if (!tri_overlap_cd(tp, r.x, r.y, r.z, rD, k.beta)) continue;
+            atomicAdd(&cd.cnt[sid], 1u);
+            const uint32_t q = atomicAdd(&cd.counters[4], 1u);
+            if (q < cd.meshCap) cd.meshPool[q] = make_uint2(sid, t);
         }
     }
 }
 
-void launch_tri_bin(const SimConsts& k, const StateView& s, const CDView& cd, bool emit, cudaStream_t st) {
+void launch_mesh_find(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st) {
     if (!(k.n_tris)) return;
-    ProfScope prof_(KID_MESH_BIN, st);
-    const unsigned blocks = blocks_for((size_t)k.n_tris * 32u, 128);
-    if (emit)
-        k_tri_bin<true><<<blocks, 128, 0, st>>>(k, s, cd);
-    else
-        k_tri_bin<false><<<blocks, 128, 0, st>>>(k, s, cd);
+    ProfScope prof_(KID_MESH_FIND, st);
+    k_mesh_find<<<blocks_for((size_t)k.n_tris * 32u, 128), 128, 0, st>>>(k, s, cd);
 }
 
-// The facets of home cell `key` that sphere (X, Y, Z, expanded radius rD, family fam) touches: f(t) for each, in
-// the cell list's order.
-template <typename F>
-__device__ __forceinline__ void for_mesh_contacts(const SimConsts& k, const StateView& s, const CDView& cd, uint32_t key,
-                                                  uint32_t fam, double X, double Y, double Z, double rD, F f) {
-    const uint32_t b = cd.triCellStart[key], e = min(cd.triCellStart[key + 1], cd.triCellCap);
-    for (uint32_t p = b; p < e; p++) {
-        const uint32_t t = cd.triCell[p];
-        if (!index_ok(k.err, 19, t, k.n_tris)) continue;
-        const TriPlaced tp = s.tri[t];
-        if (s.masks[mask_index(fam, s.loc[tp.owner].w)] != 0) continue;
-        if (tri_overlap_cd(tp, X, Y, Z, rD, k.beta)) f(t);
-    }
+// Places the mesh pool's pairs in their spheres' segments of the new list, from the top like k_pair_scatter (the
+// two share the spheres' counts), each facet id tagged with kMeshTag; k_pair_assemble sorts them ahead of the
+// sphere partners.
+__global__ void __launch_bounds__(256) k_mesh_scatter(SimConsts k, CDView cd, ContactView c, uint32_t nPairs,
+                                                      uint32_t cap) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= min(nPairs, min(cd.counters[4], cd.meshCap))) return;
+    const uint2 st = cd.meshPool[p];
+    if (!index_ok(k.err, 15, st.x, k.n_spheres)) return;
+    const uint32_t slot = atomicSub(&cd.cnt[st.x], 1u) - 1u;
+    const uint32_t pos = c.off[st.x] + slot;
+    if (!index_ok(k.err, 16, pos, cap)) return;
+    c.idB[pos] = kMeshTag | st.y;
+}
+
+void launch_mesh_scatter(const SimConsts& k, const CDView& cd, const ContactView& c, uint32_t nPairs, uint32_t cap,
+                         cudaStream_t st) {
+    if (!(k.n_tris && nPairs)) return;
+    ProfScope prof_(KID_PAIR_EMIT, st);
+    k_mesh_scatter<<<blocks_for(nPairs, 256), 256, 0, st>>>(k, cd, c, nPairs, cap);
 }
 
 // ------------------------------------------------------------------------------------------------------------
 // Per sphere: home cell and analytical-contact count (getNumberOfBinsEachSphereTouches's analytical loop,
 // DEMBinSphereKernels.cu:72-113).  The exact position is not stored: the cell-order record writer forms it again
 // from the owner pose (the same arithmetic, so the same bits), which costs less than writing and re-reading it.
-template <bool kPacked, bool kMesh>
+template <bool kPacked>
 __global__ void __launch_bounds__(256) k_sphere_prep(SimConsts k, StateView s, CDView cd) {
     const uint32_t sid = blockIdx.x * blockDim.x + threadIdx.x;
     if (sid >= k.n_spheres) return;
@@ -254,26 +265,16 @@ __global__ void __launch_bounds__(256) k_sphere_prep(SimConsts k, StateView s, C
         if (anal_overlap_cd(ap, X, Y, Z, rD, k.beta) != DEME_NOT_A_CONTACT) c++;
     }
     cd.nAnal[sid] = (uint8_t)c;
-    if (kMesh) {
-        // sphere--mesh contacts (the facets listed in the home cell)
-        uint32_t m = 0;
-        for_mesh_contacts(k, s, cd, key, fam, X, Y, Z, rD, [&](uint32_t) { m++; });
-        cd.nMesh[sid] = m;
-        c += m;
-    }
-    cd.cnt[sid] = c;  // the pair search adds the sphere partners for which this sphere is A
+    cd.cnt[sid] = c;  // the pair and mesh searches add the sphere partners (this sphere as A) and the facets
 }
 
 void launch_sphere_prep(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st) {
     if (!(k.n_spheres)) return;
     ProfScope prof_(KID_SPHERE_PREP, st);
-    // (meshes are not combined with packed scenes)
     if (k.ownerScene)
-        k_sphere_prep<true, false><<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
-    else if (k.n_tris)
-        k_sphere_prep<false, true><<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
+        k_sphere_prep<true><<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
     else
-        k_sphere_prep<false, false><<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
+        k_sphere_prep<false><<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k, s, cd);
 }
 
 __device__ __forceinline__ uint4 pack_ranges(const uint32_t lo[3], const uint32_t hi[3]) {
@@ -752,23 +753,22 @@ void launch_pair_overflow(const SimConsts& k, const StateView& s, const CDView& 
     k_pair_exact_tail<<<4 * (uint32_t)sm_count(), 256, 0, st>>>(k, s, cd, tempCap);
 }
 
-// Presets every sphere's contact count to its number of analytical and mesh contacts (k_sphere_prep does the same;
-// this is for a repeated search after the temporary list grew).
-__global__ void k_cnt_init(uint32_t n, const uint8_t* __restrict__ nAnal, const uint32_t* __restrict__ nMesh,
-                           uint32_t* cnt) {
+// Presets every sphere's contact count to its number of analytical contacts (k_sphere_prep does the same; this is
+// for a repeated search after the temporary list grew).
+__global__ void k_cnt_init(uint32_t n, const uint8_t* __restrict__ nAnal, uint32_t* cnt) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) cnt[i] = nAnal[i] + (nMesh ? nMesh[i] : 0u);
+    if (i < n) cnt[i] = nAnal[i];
 }
 
 void launch_cnt_init(const SimConsts& k, const CDView& cd, cudaStream_t st) {
     if (!(k.n_spheres)) return;
     ProfScope prof_(KID_OTHER, st);
-    k_cnt_init<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k.n_spheres, cd.nAnal, k.n_tris ? cd.nMesh : nullptr,
-                                                               cd.cnt);
+    k_cnt_init<<<blocks_for(k.n_spheres, 256), 256, 0, st>>>(k.n_spheres, cd.nAnal, cd.cnt);
 }
 
 // Places every found pair in A's segment of the new list.  After the scan A's count is no longer needed, so the
-// slots after A's analytical and mesh contacts are handed out from the top by decrementing it.
+// slots after A's analytical contacts are handed out from the top by decrementing it (shared with the mesh pairs,
+// k_mesh_scatter).
 // The pool count is read on the device (counters[0]), so the launch may cover more threads than pairs; a pool that
 // outgrew its buffer (only possible when the host did not see the count first) is flagged.
 __global__ void __launch_bounds__(256) k_pair_scatter(SimConsts k, CDView cd, ContactView c, uint32_t nPairs,
@@ -795,7 +795,9 @@ void launch_pair_scatter(const SimConsts& k, const CDView& cd, const ContactView
 
 // Completes the canonical list: per sphere A (ID order), its sphere--analytical contacts by component id
 // (populateBinSphereTouchingPairs, DEMBinSphereKernels.cu:186-228) in the first slots of its segment, then its
-// sphere--mesh contacts by facet id, then its sphere partners (placed by k_pair_scatter) sorted by ascending id.
+// sphere--mesh contacts by facet id, then its sphere partners sorted by ascending id.  The scatter kernels left the
+// partners and the facets (tagged with kMeshTag) after the analytical contacts in no order; with meshes the tail is
+// sorted on the ids with the tag bit flipped, which puts the facets first.
 template <bool kMesh>
 __global__ void __launch_bounds__(256) k_pair_assemble(SimConsts k, StateView s, CDView cd, ContactView c,
                                                        uint32_t cap) {
@@ -808,10 +810,8 @@ __global__ void __launch_bounds__(256) k_pair_assemble(SimConsts k, StateView s,
     }
     const uint32_t nAn = cd.nAnal[A];
     const uint32_t anEnd = min(begin + nAn, end);
-    const uint32_t nMe = kMesh ? cd.nMesh[A] : 0u;
-    const uint32_t meEnd = min(anEnd + nMe, end);
     uint32_t w = begin;
-    if (nAn || nMe) {
+    if (nAn) {
         uint32_t owner;
         float4 sp;
         double X, Y, Z;
@@ -832,37 +832,16 @@ __global__ void __launch_bounds__(256) k_pair_assemble(SimConsts k, StateView s,
             }
         }
         if (w != anEnd) atomicOr(k.err, ERR_SEGMENT_TOO_LONG);
-        if (kMesh && nMe) {
-            // sphere--mesh contacts, by facet id
-            w = anEnd;
-            for_mesh_contacts(k, s, cd, cd.cellKey[A], fam, X, Y, Z, rD, [&](uint32_t t) {
-                if (w < meEnd) c.idB[w] = t;
-                w++;
-            });
-            if (w != meEnd) atomicOr(k.err, ERR_SEGMENT_TOO_LONG);
-            for (uint32_t i = anEnd + 1; i < meEnd; i++) {
-                const uint32_t v = c.idB[i];
-                uint32_t j = i;
-                while (j > anEnd && c.idB[j - 1] > v) {
-                    c.idB[j] = c.idB[j - 1];
-                    j--;
-                }
-                c.idB[j] = v;
-            }
-            for (uint32_t i = anEnd; i < meEnd; i++) {
-                c.idA[i] = A;
-                c.type[i] = DEME_SPHERE_MESH_CONTACT;
-            }
-        }
     }
-    uint32_t* seg = c.idB + meEnd;
-    const uint32_t n = end - meEnd;
+    uint32_t* seg = c.idB + anEnd;
+    const uint32_t n = end - anEnd;
+    const uint32_t flip = kMesh ? kMeshTag : 0u;  // sort keys: facets below every sphere
     constexpr uint32_t kReg = 8;
     if (n <= kReg) {
         // short segments (nearly all): loaded at once, sorted in registers, stored at once
         uint32_t v[kReg];
 #pragma unroll
-        for (uint32_t i = 0; i < kReg; i++) v[i] = i < n ? seg[i] : 0xFFFFFFFFu;
+        for (uint32_t i = 0; i < kReg; i++) v[i] = i < n ? seg[i] ^ flip : 0xFFFFFFFFu;
 #pragma unroll
         for (uint32_t i = 1; i < kReg; i++) {
 #pragma unroll
@@ -876,6 +855,8 @@ __global__ void __launch_bounds__(256) k_pair_assemble(SimConsts k, StateView s,
         for (uint32_t i = 0; i < kReg; i++)
             if (i < n) seg[i] = v[i];
     } else {
+        if (kMesh)
+            for (uint32_t i = 0; i < n; i++) seg[i] ^= flip;
         for (uint32_t i = 1; i < n; i++) {
             const uint32_t v = seg[i];
             uint32_t j = i;
@@ -886,9 +867,15 @@ __global__ void __launch_bounds__(256) k_pair_assemble(SimConsts k, StateView s,
             seg[j] = v;
         }
     }
+    // seg now holds sort keys: write the ids back and the types
     for (uint32_t i = 0; i < n; i++) {
-        c.idA[meEnd + i] = A;
-        c.type[meEnd + i] = DEME_SPHERE_SPHERE_CONTACT;
+        c.idA[anEnd + i] = A;
+        if (kMesh && seg[i] < kMeshTag) {
+            c.type[anEnd + i] = DEME_SPHERE_MESH_CONTACT;
+        } else {
+            c.type[anEnd + i] = DEME_SPHERE_SPHERE_CONTACT;
+            if (kMesh) seg[i] ^= flip;
+        }
     }
 }
 

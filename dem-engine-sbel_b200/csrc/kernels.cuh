@@ -76,14 +76,11 @@ struct CDView {
     uint32_t* ovf;        // spheres with more pre-filter survivors than the candidate scan's slots hold
     uint32_t* counters;   // [0] pair-pool entries (survivors) appended, [1] overflow spheres, [2] the candidate
                           // scan's tile queue, [3] pool entries the overflow search appended (tested last),
-                          // [4] (cell, facet) entries of the mesh-facet cell lists
-    // mesh facets (n_tris > 0 only): per search cell the facets whose reach box meets it, and per sphere the
-    // number of facets it touches
-    uint32_t* triCellCount;  // nCells + 1
-    uint32_t* triCellStart;  // nCells + 1
-    uint32_t* triCell;       // facet ids, by cell
-    uint32_t triCellCap;
-    uint32_t* nMesh;         // per sphere
+                          // [4] mesh-pool entries appended
+    // sphere--mesh contacts (n_tris > 0 only): the (sphere, facet) pairs the facet-driven search found, in no
+    // particular order
+    uint2* meshPool;
+    uint32_t meshCap;
 };
 
 // One contact list (kT product) with its history wildcards.
@@ -117,8 +114,13 @@ struct ContactOutputs {
 void launch_place_anal(const SimConsts& k, const StateView& s, const AnalRaw* raw, AnalPlaced* placed, uint32_t nA,
                        cudaStream_t st);
 void launch_place_tri(const SimConsts& k, const StateView& s, const TriRaw* raw, cudaStream_t st);
-// the cell lists of the mesh facets: counts (kEmit false), then, after the scan into triCellStart, the entries
-void launch_tri_bin(const SimConsts& k, const StateView& s, const CDView& cd, bool emit, cudaStream_t st);
+// the sphere--mesh pairs, once the spheres are in cell order (adds to the spheres' contact counts)
+void launch_mesh_find(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
+// the mesh pool's pairs into their spheres' segments (after the contact offsets), tagged with kMeshTag
+void launch_mesh_scatter(const SimConsts& k, const CDView& cd, const ContactView& c, uint32_t nPairs, uint32_t cap,
+                         cudaStream_t st);
+// a facet id placed in a segment before the assembly sorts it (sphere ids stay below it)
+constexpr uint32_t kMeshTag = 0x80000000u;
 void launch_sphere_prep(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
 void launch_cell_scatter(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);
 void launch_gather_sorted(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st);

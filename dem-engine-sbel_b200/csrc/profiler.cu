@@ -22,7 +22,7 @@ const char* g_names[KID_COUNT] = {"place_anal",    "sphere_prep",   "scan",     
                                   "sort_onesweep", "gather_sorted", "pair_find",     "pair_assemble",
                                   "pair_overflow", "cell_scatter",  "history",       "force",
                                   "integrate",     "pair_exact",    "other",         "adj_record",
-                                  "adj_integrate", "adj_contact",   "adj_history",   "mesh_bin"};
+                                  "adj_integrate", "adj_contact",   "adj_history",   "mesh_find"};
 }  // namespace
 
 const char* kernel_name(int id) { return (id >= 0 && id < KID_COUNT) ? g_names[id] : "?"; }

@@ -28,7 +28,7 @@ enum KernelId : int {
     KID_ADJ_INTEGRATE,  // adjoint: reverse integration
     KID_ADJ_CONTACT,    // adjoint: reverse contact law and geometry
     KID_ADJ_HISTORY,    // adjoint: reverse history map and re-keying at segment boundaries
-    KID_MESH_BIN,       // cell lists of the mesh facets
+    KID_MESH_FIND,      // sphere--mesh search (facet-driven)
     KID_COUNT
 };
 

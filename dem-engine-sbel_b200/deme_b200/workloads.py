@@ -800,20 +800,26 @@ def mesh_funnel(n: int = 2000, r: float = 2e-3, rho: float = 2500.0, seed: int =
 
 def mesh_ball_drop(n: int = 2000, r: float = 2e-3, rho: float = 2600.0, ball_radius: float = 0.02,
                    subdivisions: int = 3, ball_rho: float = 7000.0, speed: float = 1.0, seed: int = 12,
-                   dt: float = 2e-6, cd_freq: int = 1, margin: float = 0.0, press: float = 0.2, layers: int = 4):
+                   dt: float = 2e-6, cd_freq: int = 1, margin: float = 0.0, press: float = 0.2, layers: int = 4,
+                   packed: bool = False, ball: bool = True):
     """A mesh ball (icosphere of ``ball_radius``, a free body) driven into a bed of spheres (radii U[0.8, 1] r on a
     jittered lattice of about ``layers`` layers in a box of analytical planes), as in the reference's BallDrop demo
     where the projectile is a Wavefront mesh.  The ball starts moving down at ``speed``, pressed ``press`` x r into
-    the bed's top layer."""
+    the bed's top layer.  ``packed``: spheres of radius r on a simple cubic lattice of pitch 1.998 r, each pressed
+    into its six neighbours (about three contacts per sphere from the first step).  ``ball`` False leaves the ball
+    out (the same bed without a mesh body)."""
     rng = np.random.default_rng(seed)
-    pitch = 2.02 * r
+    pitch = 1.998 * r if packed else 2.02 * r
     side = max(int(math.ceil(2.5 * ball_radius / pitch)), int(math.ceil(math.sqrt(n / layers))))
     layers = int(math.ceil(n / side ** 2))
     idx = np.arange(n)
     P = np.stack([(idx % side) * pitch, (idx // side % side) * pitch, (idx // side // side) * pitch], 1)
     P -= np.array([(side - 1) * pitch / 2, (side - 1) * pitch / 2, 0.0])
-    P += rng.uniform(-0.005 * r, 0.005 * r, P.shape)
-    rad = rng.uniform(0.8 * r, r, n)
+    if packed:
+        rad = np.full(n, r)
+    else:
+        P += rng.uniform(-0.005 * r, 0.005 * r, P.shape)
+        rad = rng.uniform(0.8 * r, r, n)
     half = side * pitch / 2 + r
     top = float((layers - 1) * pitch)
     s = SceneBuilder()
@@ -836,19 +842,20 @@ def mesh_ball_drop(n: int = 2000, r: float = 2e-3, rho: float = 2600.0, ball_rad
     s.SetFamilyFixed(2)
     # the ball's lowest facet sits `press` x r below the top layer's tops
     v, f = icosphere(ball_radius, subdivisions)
-    zc = z0 + r + top + r + float(-v[:, 2].min()) - press * r
-    ball = s.AddWavefrontMeshObject((v, f), m_b)
-    ball.SetInitPos((0.0, 0.0, zc))
-    mb = sphere_mass(ball_radius, ball_rho)
-    ball.SetMass(mb)
-    ball.SetMOI([0.4 * mb * ball_radius ** 2] * 3)
-    ball.SetInitVel((0.0, 0.0, -speed))
-    ball.SetFamily(0)
+    if ball:
+        zc = z0 + r + top + r + float(-v[:, 2].min()) - press * r
+        mesh = s.AddWavefrontMeshObject((v, f), m_b)
+        mesh.SetInitPos((0.0, 0.0, zc))
+        mb = sphere_mass(ball_radius, ball_rho)
+        mesh.SetMass(mb)
+        mesh.SetMOI([0.4 * mb * ball_radius ** 2] * 3)
+        mesh.SetInitVel((0.0, 0.0, -speed))
+        mesh.SetFamily(0)
     s.SetInitTimeStep(dt)
     s.SetGravitationalAcceleration((0, 0, -9.81))
     s.SetCDUpdateFreq(cd_freq)
     s.SetExpandFactor(margin)
     s.SetInitBinSize(2.0 * float(f32(rad.min())))
     built = s.Initialize()
-    built.info.update(workload="mesh_ball_drop", n=n, seed=seed, n_tris=len(f))
+    built.info.update(workload="mesh_ball_drop", n=n, seed=seed, n_tris=len(f) if ball else 0)
     return built

@@ -18,7 +18,8 @@ exact derivatives (floors 0).  Compared: the material gradients (E, CoR, mu, Crr
   adjoint runs on the FP32 trajectory and the differences on the FP64 one.  Coulomb sliding at the cap and
   rolling-resistance directions are non-smooth, and where contacts sit at those points the two trajectories pick
   different sides within a few steps, so these windows are frictionless: the turning clump drum and a loose clump
-  pack.  Central differences at two step sizes are compared where they agree.  Bars: 5e-3 of the largest material
+  pack; the drum is settled on the C oracle (25,500 steps), so the window is the same in every run.  Central
+  differences at two step sizes are compared where they agree.  Bars: 5e-3 of the largest material
   gradient, 1e-2 of the largest gradient of each state group.
 * Scope: a clump family with only its linear velocity prescribed, and a wall whose family has no prescription (it
   would move under the contact forces), are refused with DEME_ERR_INVALID and the reason.
@@ -27,7 +28,7 @@ import numpy as np
 import pytest
 
 import _adjoint_fd as F
-from _util import workloads
+from _util import oracle, workloads
 from oracle import fp64_autograd as AG
 from oracle import fp64_model as M
 
@@ -56,22 +57,32 @@ HOST = {
     "packed_clumps_fresh": (lambda: workloads.packed_clumps(n_clumps=100, seed=7, spacing=1.35), 0),
 }
 T_HOST, K_HOST = 24, 10
+# settled on the C oracle, so that the window is the same in every run (a contact whose overlap passes through zero
+# inside the window makes the damping term's derivative unbounded there, and the FP32 and FP64 trajectories then
+# differ in the derivative they see; a settle on the GPU would give a different window each run)
 WINDOW = {
-    "drum_clumps_cylinder_turning_frictionless": (lambda: _frictionless(_drum()), 25000),
+    "drum_clumps_cylinder_turning_frictionless": (lambda: _frictionless(_drum()), 25500),
     "packed_clumps_frictionless": (lambda: _frictionless(workloads.packed_clumps(
         n_clumps=100, seed=7, spacing=1.45, vel_scale=0.02, ang_scale=2.0)), 0),
 }
 T_WINDOW, K_WINDOW = 15, 6
 
 
-def _run(make, settle, T, K):
-    """Settles, runs the CUDA adjoint over T steps, then the same T steps again keeping each step's contact list
-    and state."""
+def _run(make, settle, T, K, settle_on_oracle=False):
+    """Settles (on the GPU, or on the C oracle and then uploaded), runs the CUDA adjoint over T steps, then the same
+    T steps again keeping each step's contact list and state."""
     from deme_b200 import Solver, adjoint
     built = make()
     g = Solver(built)
     adjoint.set_floors(g, 0.0, 0.0, 0.0)
-    if settle:
+    if settle and settle_on_oracle:
+        o = oracle(built, threads=4)
+        o.step(settle)
+        so, co = o.state(), o.contacts()
+        o.close()
+        g.set_state({k: v for k, v in so.items() if not k.startswith("a")})
+        g.set_contacts({k: co[k] for k in ("idA", "idB", "type", "wildcards")})
+    elif settle:
         g.step(settle)
     st0 = {k: v for k, v in g.state().items() if not k.startswith("a")}
     c0 = {k: np.array(v, copy=True) for k, v in g.contacts().items() if k in ("idA", "idB", "type", "wildcards")}
@@ -130,7 +141,7 @@ def test_matches_fp64_host_adjoint_on_the_recorded_trajectory(name):
 @pytest.mark.parametrize("name", sorted(WINDOW))
 def test_frictionless_window_matches_fd_of_fp64_forward(name):
     make, settle = WINDOW[name]
-    r = _run(make, settle, T_WINDOW, K_WINDOW)
+    r = _run(make, settle, T_WINDOW, K_WINDOW, settle_on_oracle=True)
     built, S0 = r["built"], r["states"][0]
     S, _ = M.rollout_fixed(built, S0, r["lists"])
     d = np.abs(r["states"][-1]["pos"] - S["pos"])[r["free"]].max()

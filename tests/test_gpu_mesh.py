@@ -11,8 +11,9 @@ of the sum of contribution magnitudes; one-step velocities within 1e-5 relative,
 * a free icosphere of 1280 facets driven into a bed of 2000 spheres inside analytical planes: a moving, rotating
   mesh owner whose reactions are collected and integrated;
 * a floor of two large facets against the same floor as an analytical plane: the same contacts, forces equal to
-  float rounding (each facet spans hundreds of search cells, so the facet cell lists outgrow their first buffer
-  and the search grows them and runs again);
+  float rounding;
+* 1,600 spheres in one layer on a two-facet floor: more sphere--mesh pairs than the mesh pool first holds, so the
+  search grows the pool and runs again; the list equals the oracle's;
 * scope: packed scenes and the adjoint refuse meshes; graph replay falls back to plain steps.
 """
 import numpy as np
@@ -105,6 +106,36 @@ def test_gpu_mesh_floor_equals_analytical_plane():
                                                                "omgZ")})
     gp.close()
     gm.close()
+
+
+def test_gpu_mesh_pool_grows():
+    from deme_b200.scene import SceneBuilder
+    r = 2e-3
+    s = SceneBuilder()
+    s.InstructBoxDomainDimension(0.4, 0.4, 0.4)
+    s.SetCoordSysOrigin("center")
+    m = s.LoadMaterial({"E": 1e7, "nu": 0.3, "CoR": 0.5, "mu": 0.3, "Crr": 0.0})
+    t = s.LoadSphereType(1e-4, r, m)
+    g = (np.arange(40) - 19.5) * 2.1 * r
+    X, Y = np.meshgrid(g, g, indexing="ij")
+    z0 = -0.05
+    xyz = np.stack([X.ravel(), Y.ravel(), np.full(X.size, z0 + 0.95 * r)], 1).astype(np.float32)
+    s.AddClumps([t] * len(xyz), xyz)
+    w = 0.15
+    v = np.array([[-w, -w, z0], [w, -w, z0], [w, w, z0], [-w, w, z0]], np.float32)
+    s.AddWavefrontMeshObject((v, np.array([[0, 1, 2], [0, 2, 3]])), m)
+    s.SetInitTimeStep(1e-5)
+    s.SetCDUpdateFreq(1)
+    s.SetExpandFactor(0.0)
+    built = s.Initialize()
+    gs, o = gpu_solver(built, keep=False), oracle(built)
+    gs.detect_contacts()
+    o.detect_contacts()
+    gc = gs.contacts()
+    assert np.sum(gc["type"] == capi.SPHERE_MESH_CONTACT) >= 1600
+    np.testing.assert_array_equal(contact_key(gc), contact_key(canonical(o.contacts())))
+    gs.close()
+    o.close()
 
 
 def test_gpu_mesh_scope():
