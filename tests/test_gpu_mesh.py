@@ -14,6 +14,7 @@ of the sum of contribution magnitudes; one-step velocities within 1e-5 relative,
   float rounding;
 * 1,600 spheres in one layer on a two-facet floor: more sphere--mesh pairs than the mesh pool first holds, so the
   search grows the pool and runs again; the list equals the oracle's;
+* detection on the kT stream (two streams, lag 2): the adopted list is the oracle's detection on the snapshot;
 * scope: packed scenes and the adjoint refuse meshes; graph replay falls back to plain steps.
 """
 import numpy as np
@@ -106,6 +107,35 @@ def test_gpu_mesh_floor_equals_analytical_plane():
                                                                "omgZ")})
     gp.close()
     gm.close()
+
+
+def test_gpu_mesh_detection_on_the_kt_stream_is_the_detection_on_the_snapshot():
+    """kT and dT on two streams (deme_set_async_cd, lag 2, detection every 4 steps, margin 0.1 mm): the list dT
+    adopts is the oracle's detection on the poses of the detection step, mesh facets placed from kT's snapshot."""
+    from deme_b200 import Solver
+    built = workloads.mesh_ball_drop(n=2000, seed=35, press=0.2, cd_freq=4, margin=1e-4)
+    f, lag = 4, 2
+    g = Solver(built)
+    g.set_async_cd(lag)
+    snaps, checked, n_mesh = {}, 0, 0
+    for s in range(3 * f + lag + 1):
+        if s % f == 0:
+            snaps[s] = g.state()
+        g.step(1)
+        src = 0 if s == 0 else (s - lag if s - lag >= f and (s - lag) % f == 0 else None)
+        if src is None:
+            continue
+        o = oracle(built)
+        o.set_state(snaps[src])
+        o.detect_contacts()
+        oc = canonical(o.contacts())
+        gc = g.contacts()
+        np.testing.assert_array_equal(contact_key(gc), contact_key(oc), err_msg=f"step {s} (poses of step {src})")
+        n_mesh += int(np.sum(gc["type"] == capi.SPHERE_MESH_CONTACT))
+        checked += 1
+        o.close()
+    assert checked >= 3 and n_mesh > 0
+    g.close()
 
 
 def test_gpu_mesh_pool_grows():

@@ -10,7 +10,8 @@ pin this part of the oracle to.  Instead:
   relative;
 * order: a sphere touching an analytical plane and several facets lists the plane first, then the facets by id;
 * the Wavefront OBJ reader splits polygons into fans, takes negative indices from the end and ignores texture and
-  normal indices.
+  normal indices;
+* flattening: mesh owners follow the external objects, facets carry owner, material and owner-frame nodes.
 """
 import numpy as np
 import pytest
@@ -128,3 +129,45 @@ def test_wavefront_reader(tmp_path):
     assert obj.GetNumTriangles() == 3
     with pytest.raises(ValueError, match="must have length 3"):
         obj.SetMaterial([m, m])
+
+
+def test_mesh_owners_follow_the_external_objects_when_flattened():
+    """Owners: clumps, external objects, then mesh objects (kT.cpp:603-625); facets carry their owner, per-facet
+    material and their nodes in the owner frame (after Translate / Scale); the owner its pose, mass and moments."""
+    s = SceneBuilder()
+    s.InstructBoxDomainDimension(0.2, 0.2, 0.2)
+    s.SetCoordSysOrigin("center")
+    m0 = s.LoadMaterial({"E": 1e7, "nu": 0.3, "CoR": 0.5, "mu": 0.3, "Crr": 0.0})
+    m1 = s.LoadMaterial({"E": 2e7, "nu": 0.3, "CoR": 0.5, "mu": 0.3, "Crr": 0.0})
+    t = s.LoadSphereType(1e-4, R, m0)
+    s.AddClumps([t] * 3, np.zeros((3, 3), np.float32) + np.arange(3, dtype=np.float32)[:, None] * 0.01)
+    s.AddBCPlane((0, 0, -0.05), (0, 0, 1), m0)
+    a = s.AddWavefrontMeshObject((TRI.astype(np.float32), np.array([[0, 1, 2]])), m1)
+    a.Translate((0.001, 0.0, 0.0))
+    a.Scale(2.0)
+    b = s.AddWavefrontMeshObject((TRI.astype(np.float32), np.array([[0, 1, 2], [2, 1, 0]])))
+    b.SetMaterial([m0, m1])
+    b.SetInitPos((0.01, 0.02, 0.03))
+    b.SetInitQuat((0.8, 0.0, 0.6, 0.0))
+    b.SetMass(3.0)
+    b.SetMOI((1.0, 2.0, 3.0))
+    b.SetFamily(7)
+    built = s.Initialize()
+    arr = built.arrays
+    assert built.counts["o"] == 3 + 1 + 2 and built.counts["t"] == 3
+    np.testing.assert_array_equal(arr["tri_owner"], [4, 5, 5])
+    np.testing.assert_array_equal(arr["tri_material"], [1, 0, 1])
+    np.testing.assert_array_equal(arr["tri_node1"][0], (TRI[0].astype(np.float32) + np.float32([0.001, 0, 0])) * 2)
+    np.testing.assert_array_equal(arr["tri_node1"][2], TRI[2].astype(np.float32))
+    assert arr["family"][5] == 7 and arr["mass"][5] == np.float32(3.0) and arr["mmiZZ"][5] == np.float32(3.0)
+    np.testing.assert_array_equal([arr[k][5] for k in ("oriQw", "oriQx", "oriQy", "oriQz")],
+                                  np.float32([0.8, 0.0, 0.6, 0.0]))
+    pos = built.decode_positions(built.initial_state(), kernel_literals=False) + built.info["lbf"]
+    assert np.abs(pos[5] - [0.01, 0.02, 0.03]).max() < 1e-7
+    assert arr["family"][4] == capi.RESERVED_FAMILY
+    # a mesh without a material is refused at Initialize, as the reference refuses it
+    s2 = SceneBuilder()
+    s2.InstructBoxDomainDimension(0.2, 0.2, 0.2)
+    s2.AddWavefrontMeshObject((TRI.astype(np.float32), np.array([[0, 1, 2]])))
+    with pytest.raises(ValueError, match="does not have associated material"):
+        s2.Initialize()
