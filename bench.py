@@ -512,6 +512,53 @@ def mesh_drop_measure(args, stream):
     return out
 
 
+def mesh_drum_measure(args, stream, settled: dict):
+    """The benchmark drum with its cylinder as a mesh body (`workloads.drum(mesh=True)`: a prism of flat facets
+    touching the radius-R circle, turning with the end planes), started from the analytical drum's settled clumps,
+    against the analytical drum from the same state, both launched step by step (meshes step without CUDA graphs):
+    device time with CUDA events over ``--mesh-steps`` steps after 200 untimed ones (the first detects afresh)."""
+    import numpy as np
+    import torch
+    from deme_b200 import Solver, capi, workloads
+    out = {}
+    for mesh in (True, False):
+        built = workloads.drum(n_clumps=args.clumps, seed=2, mesh=mesh)
+        s = Solver(built)
+        s.lib.deme_set_streams(s.h, C.c_void_p(stream.cuda_stream), C.c_void_p(stream.cuda_stream))
+        nC = built.info["n_clumps"]
+        st = s.state()
+        for k, v in settled.items():
+            if not k.startswith("a"):
+                st[k][:nC] = v[:nC]
+        s.set_state({k: v for k, v in st.items() if not k.startswith("a")})
+        s.step(200)
+        s.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        s.step(args.mesh_steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        c = s.contacts()
+        r = {"value": built.n_spheres * args.mesh_steps / (ms / 1e3) / 1e6, "unit": UNIT,
+             "ms_per_step": ms / args.mesh_steps, "n_contacts": len(c["idA"]),
+             "kernel_ms_per_step": {k: round(v, 4) for k, v in
+                                    sorted(kernel_breakdown(s, 20).items(), key=lambda kv: -kv[1])}}
+        s.close()
+        if mesh:
+            r.update(workload=f"rotating drum, {nC} three-sphere clumps, cylinder as a mesh of {built.info['n_tris']} "
+                              f"facets turning at 20 rpm with the end planes, dt 5e-6, CD every step, from the "
+                              f"settled bed, kernels launched step by step",
+                     n_facets=built.info["n_tris"],
+                     n_sphere_mesh_contacts=int(np.sum(c["type"] == capi.SPHERE_MESH_CONTACT)),
+                     steps=args.mesh_steps, warmup=200)
+            out.update(r)
+        else:
+            out["analytical_cylinder_same_state"] = r
+    return out
+
+
 def cpu_baseline_sample(args):
     from deme_b200 import HandleSolver, capi
     lib_path = os.path.join(ROOT, "oracle", "_build", "libdeme_oracle.so")
@@ -758,6 +805,11 @@ def main():
             mesh = clocked(lambda: mesh_drop_measure(args, stream))
         except Exception as e:  # the headline line is printed whatever happens to this secondary measurement
             mesh = {"unavailable": f"{type(e).__name__}: {e}"}
+        try:
+            settled = s.state()
+            mesh["drum"] = clocked(lambda: mesh_drum_measure(args, stream, settled))
+        except Exception as e:
+            mesh["drum"] = {"unavailable": f"{type(e).__name__}: {e}"}
     # the CPU sample last: its OpenMP threads would otherwise share the host with the GPU sections' host code
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -149,7 +149,7 @@ def triangle_template(rng, r_nom: float, rho: float, n_mc: int = 20000):
 
 def drum(n_clumps: int = 1_000_000, r_nom: float = 2e-3, rho: float = 2500.0, n_templates: int = 64,
          fill: float = 0.30, packing: float = 0.6, rpm: float = 20.0, dt: float = 5e-6, seed: int = 2,
-         shell: bool = False, spacing: float = 1.02, wall_clearance: float = 1.05):
+         shell: bool = False, spacing: float = 1.02, wall_clearance: float = 1.05, mesh: bool = False):
     """Rotating drum of three-sphere clumps (analytical cylinder + two end planes, prescribed rotation).
 
     One million clumps of about 8e-8 m^3 do not fit a 30 % fill of an R = 0.25 m, L = 0.3 m drum, so the drum is
@@ -163,6 +163,11 @@ def drum(n_clumps: int = 1_000_000, r_nom: float = 2e-3, rho: float = 2500.0, n_
     components. The cylinder becomes a shell of fixed spheres of radius ``r_nom``, centred one radius outside R on
     a square lattice of pitch 1.9 ``r_nom``, so that no bed sphere fits through. The shell does not rotate. The two
     end planes and the shell form one fixed family with contacts inside it disabled.
+
+    ``mesh=True`` makes the cylinder a mesh body turning with the end planes: a prism of flat facets whose planes
+    touch the radius-R circle (so the lattice start is the same), enough of them around that a facet's sagitta is
+    at most 0.05 ``r_nom``, split along the axis into near-square quads of two triangles, mass 1e15 as the
+    analytical walls'.
     """
     rng = np.random.default_rng(seed)
     tmpl = [triangle_template(rng, r_nom, rho) for _ in range(n_templates)]
@@ -229,7 +234,27 @@ def drum(n_clumps: int = 1_000_000, r_nom: float = 2e-3, rho: float = 2500.0, n_
                           n_clumps=n_clumps, n_shell=len(S), lattice_spacing=a, clump_reach=reach)
         return built
     d = s.AddExternalObject()
-    d.AddCylinder((0, 0, 0), (0, 1, 0), R, mat)
+    n_tris = 0
+    if mesh:
+        n_around = max(64, int(math.ceil(math.pi / math.sqrt(2 * 0.05 * r_nom / R))))
+        Rv = R / math.cos(math.pi / n_around)  # vertices outside R: the facets' planes touch the circle
+        n_axial = max(1, int(math.ceil(L / (2 * math.pi * Rv / n_around))))
+        th = 2 * math.pi * np.arange(n_around + 1) / n_around
+        ys = -L / 2 + L * np.arange(n_axial + 1) / n_axial
+        tris = []
+        for i in range(n_around):
+            for j in range(n_axial):
+                p = [(Rv * math.cos(th[a]), ys[b], Rv * math.sin(th[a])) for a, b in
+                     ((i, j), (i + 1, j), (i + 1, j + 1), (i, j + 1))]
+                tris += [(p[0], p[1], p[2]), (p[0], p[2], p[3])]
+        v, fc = _mesh_arrays(tris)
+        cyl = s.AddWavefrontMeshObject((v, fc), mat)
+        cyl.SetMass(1e15)
+        cyl.SetMOI((1e15, 1e15, 1e15))
+        cyl.SetFamily(drum_fam)
+        n_tris = len(fc)
+    else:
+        d.AddCylinder((0, 0, 0), (0, 1, 0), R, mat)
     d.AddPlane((0, -L / 2, 0), (0, 1, 0), mat)
     d.AddPlane((0, L / 2, 0), (0, -1, 0), mat)
     d.SetFamily(drum_fam)
@@ -239,8 +264,9 @@ def drum(n_clumps: int = 1_000_000, r_nom: float = 2e-3, rho: float = 2500.0, n_
     s.SetInitTimeStep(dt)
     s.SetGravitationalAcceleration((0, 0, -9.81))
     built = s.Initialize()
-    built.info.update(workload="drum", R=R, L=L, n_templates=n_templates, omega=omega, seed=seed,
-                      vol_clump=vol_clump, n_clumps=n_clumps, lattice_spacing=a, clump_reach=reach)
+    built.info.update(workload="drum_mesh" if mesh else "drum", R=R, L=L, n_templates=n_templates, omega=omega,
+                      seed=seed, vol_clump=vol_clump, n_clumps=n_clumps, lattice_spacing=a, clump_reach=reach,
+                      n_tris=n_tris)
     return built
 
 

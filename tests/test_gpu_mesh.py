@@ -10,6 +10,7 @@ of the sum of contribution magnitudes; one-step velocities within 1e-5 relative,
   contacts on facet interiors, edges and corners, a fixed mesh owner;
 * a free icosphere of 1280 facets driven into a bed of 2000 spheres inside analytical planes: a moving, rotating
   mesh owner whose reactions are collected and integrated;
+* the drum of 700 clumps with its cylinder as 1664 facets turning at 20 rpm: a mesh owner with prescribed rotation;
 * a floor of two large facets against the same floor as an analytical plane: the same contacts, forces equal to
   float rounding;
 * 1,600 spheres in one layer on a two-facet floor: more sphere--mesh pairs than the mesh pool first holds, so the
@@ -33,6 +34,9 @@ def mesh_scenes():
     return {
         "funnel_fixed_mesh": lambda: workloads.mesh_funnel(n=1500, seed=31, wall_clearance=0.8),
         "ball_drop_free_mesh": lambda: workloads.mesh_ball_drop(n=2000, seed=32, press=0.2),
+        # the drum's cylinder as 1664 facets turning with the end planes (prescribed rotation); outer clumps pressed in
+        "drum_turning_mesh_cylinder": lambda: workloads.drum(n_clumps=700, seed=21, wall_clearance=0.7, spacing=0.8,
+                                                             mesh=True),
     }
 
 
