@@ -144,6 +144,18 @@ void launch_place_tri(const SimConsts& k, const StateView& s, const TriRaw* raw,
     k_place_tri<<<blocks_for(k.n_tris, 64), 64, 0, st>>>(k, s, raw, k.n_tris);
 }
 
+// Lane that owns entry p of a warp-wide list made of the lanes' runs in lane order (`pre`: exclusive prefix of the
+// run lengths, 33 entries): the last lane whose prefix is <= p.
+__device__ __forceinline__ uint32_t pool_owner(const uint32_t* pre, uint32_t p) {
+    uint32_t L = 0;
+#pragma unroll
+    for (uint32_t step = 16; step > 0; step >>= 1)
+        if (pre[L + step] <= p) L += step;
+    return L;
+}
+
+constexpr uint32_t kMeshFindWarps = 4;  // k_mesh_find's warps per block
+
 // Sphere--mesh contact search, one warp per facet, once the spheres are in cell order.  A sphere in cell c can touch
 // facet t only if its centre lies within the reach (largest expanded radius + beta) of t, so the facet visits the
 // cells of its reach box, less those whose box (open to the outside at the grid's faces, where cell_of clamps, and
@@ -152,7 +164,7 @@ void launch_place_tri(const SimConsts& k, const StateView& s, const TriRaw* raw,
 // sphere lies in one home cell and the facet visits each cell once, so each (sphere, facet) pair is found once.  A
 // pair adds one to the sphere's contact count and is appended to the mesh pool; entries past the pool's capacity
 // are dropped and their total (counters[4]), read by the host, makes it grow the pool and search again.
-__global__ void __launch_bounds__(128) k_mesh_find(SimConsts k, StateView s, CDView cd) {
+__global__ void __launch_bounds__(kMeshFindWarps * 32) k_mesh_find(SimConsts k, StateView s, CDView cd) {
     const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
     if (t >= k.n_tris) return;
@@ -174,22 +186,46 @@ __global__ void __launch_bounds__(128) k_mesh_find(SimConsts k, StateView s, CDV
         nc[d] = c1 - c0[d] + 1u;
     }
     const uint64_t total = (uint64_t)nc[0] * nc[1] * nc[2];
-    for (uint64_t c = lane; c < total; c += 32u) {
-        const uint32_t ci[3] = {c0[0] + (uint32_t)(c % nc[0]), c0[1] + (uint32_t)((c / nc[0]) % nc[1]),
-                                c0[2] + (uint32_t)(c / ((uint64_t)nc[0] * nc[1]))};
-        double ctr[3], hd2 = 0.0;
-        for (int d = 0; d < 3; d++) {
-            const double b0 = ci[d] == 0u ? lo[d] : fmax(lo[d], (double)ci[d] * cs);
-            const double b1 = ci[d] + 1u >= gdim[d] ? hi[d] : fmin(hi[d], (double)(ci[d] + 1u) * cs);
-            ctr[d] = 0.5 * (b0 + b1);
-            hd2 += 0.25 * (b1 - b0) * (b1 - b0);
+    // the warp's cells 32 at a time, one a lane (reach test, then its sphere range); the batch's spheres are then
+    // spread over the lanes, so that 32 sphere tests run side by side instead of one lane walking its cell's list
+    __shared__ uint32_t s_pre[kMeshFindWarps][33], s_first[kMeshFindWarps][32];
+    const uint32_t w = threadIdx.x >> 5;
+    for (uint64_t cb = 0; cb < total; cb += 32u) {
+        const uint64_t c = cb + lane;
+        uint32_t first = 0, cnt = 0;
+        if (c < total) {
+            const uint32_t ci[3] = {c0[0] + (uint32_t)(c % nc[0]), c0[1] + (uint32_t)((c / nc[0]) % nc[1]),
+                                    c0[2] + (uint32_t)(c / ((uint64_t)nc[0] * nc[1]))};
+            double ctr[3], hd2 = 0.0;
+            for (int d = 0; d < 3; d++) {
+                const double b0 = ci[d] == 0u ? lo[d] : fmax(lo[d], (double)ci[d] * cs);
+                const double b1 = ci[d] + 1u >= gdim[d] ? hi[d] : fmin(hi[d], (double)(ci[d] + 1u) * cs);
+                ctr[d] = 0.5 * (b0 + b1);
+                hd2 += 0.25 * (b1 - b0) * (b1 - b0);
+            }
+            double qx, qy, qz;
+            const double lim = reach + sqrt(hd2);
+            if (tri_dist2(tp, ctr[0], ctr[1], ctr[2], qx, qy, qz) <= lim * lim) {
+                const uint32_t key = ci[0] + g.gx * (ci[1] + g.gy * ci[2]);
+                first = cd.cellStart[key];
+                const uint32_t e = min(cd.cellStart[key + 1], k.n_spheres);
+                cnt = e > first ? e - first : 0u;
+            }
         }
-        double qx, qy, qz;
-        const double lim = reach + sqrt(hd2);
-        if (tri_dist2(tp, ctr[0], ctr[1], ctr[2], qx, qy, qz) > lim * lim) continue;
-        const uint32_t key = ci[0] + g.gx * (ci[1] + g.gy * ci[2]);
-        const uint32_t b = cd.cellStart[key], e = min(cd.cellStart[key + 1], k.n_spheres);
-        for (uint32_t p = b; p < e; p++) {
+        uint32_t incl = cnt;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= (uint32_t)off) incl += y;
+        }
+        const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+        s_pre[w][lane + 1] = incl;
+        if (lane == 0) s_pre[w][0] = 0;
+        s_first[w][lane] = first;
+        __syncwarp();
+        for (uint32_t q = lane; q < tot; q += 32u) {
+            const uint32_t L = pool_owner(s_pre[w], q);
+            const uint32_t p = s_first[w][L] + (q - s_pre[w][L]);
             if (s.masks[mask_index(cd.rngS[p].w, famT)] != 0) continue;
             const SphCD r = cd.recS[p];
             const uint32_t sid = __float_as_uint(cd.posFSorted[p].w) & k.id_mask;
@@ -198,16 +234,17 @@ __global__ void __launch_bounds__(128) k_mesh_find(SimConsts k, StateView s, CDV
             rD += (double)k.beta;
             if (!tri_overlap_cd(tp, r.x, r.y, r.z, rD, k.beta)) continue;
             atomicAdd(&cd.cnt[sid], 1u);
-            const uint32_t q = atomicAdd(&cd.counters[4], 1u);
-            if (q < cd.meshCap) cd.meshPool[q] = make_uint2(sid, t);
+            const uint32_t slot = atomicAdd(&cd.counters[4], 1u);
+            if (slot < cd.meshCap) cd.meshPool[slot] = make_uint2(sid, t);
         }
+        __syncwarp();  // the batch's shared entries are read before the next batch writes them
     }
 }
 
 void launch_mesh_find(const SimConsts& k, const StateView& s, const CDView& cd, cudaStream_t st) {
     if (!(k.n_tris)) return;
     ProfScope prof_(KID_MESH_FIND, st);
-    k_mesh_find<<<blocks_for((size_t)k.n_tris * 32u, 128), 128, 0, st>>>(k, s, cd);
+    k_mesh_find<<<blocks_for((size_t)k.n_tris * 32u, kMeshFindWarps * 32), kMeshFindWarps * 32, 0, st>>>(k, s, cd);
 }
 
 // Places the mesh pool's pairs in their spheres' segments of the new list, from the top like k_pair_scatter (the
@@ -537,14 +574,6 @@ __device__ __forceinline__ float prefilter_lim2(const SimConsts& k, const Search
 // (Testing the pool in a kernel of its own, one thread per entry, read the records back from DRAM: 0.195 + 0.103 ms
 // against 0.282 ms for this form on the 3M-sphere drum.)
 
-// Lane that owns pooled pair p: the last lane whose survivor prefix is <= p.
-__device__ __forceinline__ uint32_t pool_owner(const uint32_t* pre, uint32_t p) {
-    uint32_t L = 0;
-#pragma unroll
-    for (uint32_t step = 16; step > 0; step >>= 1)
-        if (pre[L + step] <= p) L += step;
-    return L;
-}
 
 // The reference's pair predicate on a candidate (cell-order indices i, j): the pair (A, B) with A < B by sphere id,
 // counted on A, or kNoPair.
@@ -836,6 +865,13 @@ __global__ void __launch_bounds__(256) k_pair_assemble(SimConsts k, StateView s,
     uint32_t* seg = c.idB + anEnd;
     const uint32_t n = end - anEnd;
     const uint32_t flip = kMesh ? kMeshTag : 0u;  // sort keys: facets below every sphere
+    // a sorted key back to the contact it stands for
+    auto put = [&](uint32_t i, uint32_t key) {
+        const bool facet = kMesh && key < kMeshTag;
+        seg[i] = facet ? key : key ^ flip;
+        c.idA[anEnd + i] = A;
+        c.type[anEnd + i] = facet ? DEME_SPHERE_MESH_CONTACT : DEME_SPHERE_SPHERE_CONTACT;
+    };
     constexpr uint32_t kReg = 8;
     if (n <= kReg) {
         // short segments (nearly all): loaded at once, sorted in registers, stored at once
@@ -853,7 +889,7 @@ __global__ void __launch_bounds__(256) k_pair_assemble(SimConsts k, StateView s,
         }
 #pragma unroll
         for (uint32_t i = 0; i < kReg; i++)
-            if (i < n) seg[i] = v[i];
+            if (i < n) put(i, v[i]);
     } else {
         if (kMesh)
             for (uint32_t i = 0; i < n; i++) seg[i] ^= flip;
@@ -866,16 +902,7 @@ __global__ void __launch_bounds__(256) k_pair_assemble(SimConsts k, StateView s,
             }
             seg[j] = v;
         }
-    }
-    // seg now holds sort keys: write the ids back and the types
-    for (uint32_t i = 0; i < n; i++) {
-        c.idA[anEnd + i] = A;
-        if (kMesh && seg[i] < kMeshTag) {
-            c.type[anEnd + i] = DEME_SPHERE_MESH_CONTACT;
-        } else {
-            c.type[anEnd + i] = DEME_SPHERE_SPHERE_CONTACT;
-            if (kMesh) seg[i] ^= flip;
-        }
+        for (uint32_t i = 0; i < n; i++) put(i, seg[i]);
     }
 }
 
