@@ -816,7 +816,7 @@ static int32_t cd_sync(deme_handle* h) {
         CUDA_TRY(h, cudaStreamSynchronize(st));
         n = h->hTotal[0];
         if (search_fits(h, h->hTotal)) break;
-        // the pair list (or a facet cell list) outgrew its buffer: grow and search again
+        // the pair pool (or the mesh pool) outgrew its buffer: grow and search again
         TRY(grow_search(h, h->hTotal));
     }
     if (!search_fits(h, h->hTotal)) {

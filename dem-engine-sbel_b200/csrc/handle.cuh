@@ -159,7 +159,7 @@ struct deme_handle {
     float4* kQuat = nullptr;
     AnalPlaced* kAnalPlaced = nullptr;  // analytical components placed from that snapshot
     TriPlaced* kTriPlaced = nullptr;    // mesh facets placed from that snapshot
-    uint32_t* hCounts = nullptr;        // pinned: total, pool count, overflow spheres, -, facet cell entries,
+    uint32_t* hCounts = nullptr;        // pinned: total, pool count, overflow spheres, -, mesh pairs,
                                         // copied at the end of kT's part (8 words)
     cudaEvent_t evPose = nullptr, evCounts = nullptr, evListReady = nullptr, evListReleased = nullptr;
     StateView kt_view() const {
