@@ -356,7 +356,7 @@ def _hopper_top(n, a, r_max, tan_t, cos_t, u_out, wall_clearance):
 def hopper(n: int = 4_000_000, r_median: float = 1.5e-3, sigma: float = 0.25, r_clip=(0.75e-3, 3e-3),
            rho: float = 2500.0, half_angle_deg: float = 30.0, outlet: float = 0.04, n_classes: int = 64,
            seed: int = 4, dt: float = 2e-6, cd_freq: int = 5, margin: float | None = None, closed: bool = True,
-           wall_clearance: float = 1.02, packing_seed_jitter: float = 0.9):
+           wall_clearance: float = 1.02, packing_seed_jitter: float = 0.9, mesh: bool = False):
     """Conical hopper of log-normal polydisperse spheres (analytical cone + outlet gate + catch floor).
 
     Radii are log-normal (median ``r_median``, ``sigma``) clipped to ``r_clip`` and grouped into ``n_classes``
@@ -367,6 +367,9 @@ def hopper(n: int = 4_000_000, r_median: float = 1.5e-3, sigma: float = 0.25, r_
     (deme_change_family / ChangeFamily) opens it.  The floor 0.1 m below catches discharge.
     Contact detection runs every ``cd_freq`` steps with the contact margin ``margin`` (default 0.1 r_median).
     ``wall_clearance`` below 1 starts the outer spheres pressed into the walls (used by parity tests).
+    ``mesh=True`` makes the cone a fixed mesh body: a pyramid frustum of flat facets whose planes touch the cone
+    along their middle lines, enough of them around that a facet's sagitta at the top is at most 0.05 ``r_median``,
+    split along the slant into near-square quads of two triangles.
     """
     rng = np.random.default_rng(seed)
     th = math.radians(half_angle_deg)
@@ -396,9 +399,29 @@ def hopper(n: int = 4_000_000, r_median: float = 1.5e-3, sigma: float = 0.25, r_
     pos = P + np.array([0.0, 0.0, shift])
     b = s.AddClumps([types[c] for c in cls], pos.astype(f32))
     b.SetFamily(0)
-    wall = s.AddExternalObject()
-    wall.AddCone((0.0, 0.0, shift), (0.0, 0.0, 1.0), th, u_out, u_top, mat)
-    wall.SetFamily(1)
+    if mesh:
+        r_top = u_top * tan_t
+        n_around = max(64, int(math.ceil(math.pi / math.sqrt(2 * 0.05 * r_median / r_top))))
+        kv = 1.0 / math.cos(math.pi / n_around)  # vertices outside the cone: the facets' planes touch it
+        slant = (u_top - u_out) / cos_t
+        n_axial = max(1, int(math.ceil(slant / (2 * math.pi * kv * 0.5 * (u_out + u_top) * tan_t / n_around))))
+        ph = 2 * math.pi * np.arange(n_around + 1) / n_around
+        us = u_out + (u_top - u_out) * np.arange(n_axial + 1) / n_axial
+        tris = []
+        for i in range(n_around):
+            for j in range(n_axial):
+                p = [(kv * us[b] * tan_t * math.cos(ph[a]), kv * us[b] * tan_t * math.sin(ph[a]), shift + us[b])
+                     for a, b in ((i, j), (i + 1, j), (i + 1, j + 1), (i, j + 1))]
+                tris += [(p[0], p[1], p[2]), (p[0], p[2], p[3])]
+        v, fc = _mesh_arrays(tris)
+        cone = s.AddWavefrontMeshObject((v, fc), mat)
+        cone.SetMass(1e15)
+        cone.SetMOI((1e15, 1e15, 1e15))
+        cone.SetFamily(1)
+    else:
+        wall = s.AddExternalObject()
+        wall.AddCone((0.0, 0.0, shift), (0.0, 0.0, 1.0), th, u_out, u_top, mat)
+        wall.SetFamily(1)
     floor = s.AddBCPlane((0.0, 0.0, shift + z_floor), (0.0, 0.0, 1.0), mat)
     floor.SetFamily(1)
     if closed:

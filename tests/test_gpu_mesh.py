@@ -11,6 +11,7 @@ of the sum of contribution magnitudes; one-step velocities within 1e-5 relative,
 * a free icosphere of 1280 facets driven into a bed of 2000 spheres inside analytical planes: a moving, rotating
   mesh owner whose reactions are collected and integrated;
 * the drum of 700 clumps with its cylinder as 1664 facets turning at 20 rpm: a mesh owner with prescribed rotation;
+* the conical hopper of 1500 log-normal spheres with its cone as 2304 facets;
 * a floor of two large facets against the same floor as an analytical plane: the same contacts, forces equal to
   float rounding;
 * 1,600 spheres in one layer on a two-facet floor: more sphere--mesh pairs than the mesh pool first holds, so the
@@ -37,6 +38,8 @@ def mesh_scenes():
         # the drum's cylinder as 1664 facets turning with the end planes (prescribed rotation); outer clumps pressed in
         "drum_turning_mesh_cylinder": lambda: workloads.drum(n_clumps=700, seed=21, wall_clearance=0.7, spacing=0.8,
                                                              mesh=True),
+        # the conical hopper's cone as 2304 fixed facets, polydisperse spheres pressed into it
+        "hopper_mesh_cone": lambda: workloads.hopper(n=1500, seed=22, wall_clearance=0.4, mesh=True),
     }
 
 
