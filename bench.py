@@ -800,7 +800,8 @@ def main():
     ref_wedge = reference_kernels_quick(args, "wedge") if (rank == 0 and not args.no_hopper) else None
     small = clocked(lambda: small_scene_measure(args, stream)) if (rank == 0 and not args.no_small) else None
     mesh = None
-    if rank == 0 and not args.no_mesh:
+    # one GPU only: in a multi-GPU run the other ranks would wait at the closing barrier through it
+    if rank == 0 and world == 1 and not args.no_mesh:
         try:
             mesh = clocked(lambda: mesh_drop_measure(args, stream))
         except Exception as e:  # the headline line is printed whatever happens to this secondary measurement
