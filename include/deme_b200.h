@@ -295,7 +295,9 @@ int32_t deme_upload_state_range(deme_handle* h, uint32_t first, uint32_t count, 
 int32_t deme_get_num_contacts(deme_handle* h, uint32_t* n);
 int32_t deme_download_contacts(deme_handle* h, deme_contacts* out);
 /* Replace the current contact list and its wildcards (history); mapping is ignored.  Used to inject identical
- * kT products into dT for parity checks. */
+ * kT products into dT for parity checks.  The list may come in any order (it is put in the canonical order);
+ * idB must be below the count of its kind (spheres, analytical components or mesh facets) and the type one of
+ * the contact types above, else DEME_ERR_INVALID. */
 int32_t deme_upload_contacts(deme_handle* h, const deme_contacts* in);
 int32_t deme_download_contact_forces(deme_handle* h, deme_contact_forces* out);
 /* Keep the per-contact force, torque-only force and local contact points of the next deme_compute_forces calls so
