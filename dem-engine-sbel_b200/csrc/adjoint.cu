@@ -629,6 +629,10 @@ int32_t check_adjoint_scene(deme_handle* h) {
         h->err = "adjoint: sphere--mesh contacts are not differentiated";
         return DEME_ERR_INVALID;
     }
+    if (h->nW == 0) {
+        h->err = "adjoint: the frictionless Hertzian model (no contact wildcards) is not differentiated";
+        return DEME_ERR_INVALID;
+    }
     if (h->params.integrator != DEME_INTEGRATOR_EXTENDED_TAYLOR || h->params.cd_update_freq > 1 || h->cdLag > 0) {
         h->err = "adjoint: needs Extended Taylor integration and synchronous contact detection every step";
         return DEME_ERR_INVALID;

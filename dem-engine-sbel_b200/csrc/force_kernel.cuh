@@ -16,7 +16,9 @@ namespace deme_b200 {
 // autotuner may pick another.  Run-time compiled user models use the default.
 constexpr uint32_t kForceThreads = 128;
 constexpr uint32_t kForceMinBlocks = 8;
-template <bool kStore, uint32_t kThreads = kForceThreads, uint32_t kMinBlocks = kForceMinBlocks>
+// kNormalOnly: the built-in model as the frictionless Hertzian model (a scene with no contact wildcards).
+template <bool kStore, uint32_t kThreads = kForceThreads, uint32_t kMinBlocks = kForceMinBlocks,
+          bool kNormalOnly = false>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) k_force(SimConsts k, StateView s, ContactView c, uint32_t n,
                                                                bool has_hist, ContactOutputs out, AnalAccum aa) {
     // a device error earlier in the step (a list or pool outgrew its capacity inside a replayed graph) voids the
@@ -195,7 +197,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_force(SimConsts k, Sta
                 cpB = locCPB;
             }
 #else
-            hertz_mindlin(g, s.mat, k.h, F, T, hw.x, hw.y, hw.z, hw.w);
+            hertz_mindlin<kNormalOnly>(g, s.mat, k.h, F, T, hw.x, hw.y, hw.z, hw.w);
 #endif
         } else {
             hw = make_float4(0.f, 0.f, 0.f, 0.f);

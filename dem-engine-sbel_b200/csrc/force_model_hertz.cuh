@@ -62,6 +62,12 @@ __device__ __forceinline__ void contact_params(const MaterialTable& m, uint32_t 
     beta = (float)((double)loge / sqrt((double)(loge * loge) + kPiSquared));
 }
 
+// kNormalOnly: the frictionless Hertzian model (FrictionlessHertzianForceModel.cu, the reference's
+// UseFrictionlessHertzianModel): the same normal spring and damper, no rolling resistance, no tangential force and no
+// contact history.  (The reference's file calls a material-proxy helper by a name its helper header does not define,
+// mat2ProxyContactParam for matProxy2ContactParam, so its run-time build of that model fails; this is the model the
+// file states, with the proxy overload for E and CoR, whose formulas are the full one's.)
+template <bool kNormalOnly = false>
 __device__ __forceinline__ void hertz_mindlin(const ContactGeom& g, const MaterialTable& m, float ts, float3& force,
                                               float3& torque_only_force, float& delta_tan_x, float& delta_tan_y,
                                               float& delta_tan_z, float& delta_time) {
@@ -104,6 +110,7 @@ __device__ __forceinline__ void hertz_mindlin(const ContactGeom& g, const Materi
     force.x += scal * nX;
     force.y += scal * nY;
     force.z += scal * nZ;
+    if (kNormalOnly) return;
     // rolling resistance
     if ((double)Crr_cnt > 0.0) {
         bool add_rr = true;

@@ -1020,10 +1020,18 @@ template <uint32_t T, uint32_t B>
 void launch_force_shape(const SimConsts& k, const StateView& s, const ContactView& c, uint32_t n, bool has_hist,
                         const ContactOutputs* out, const AnalAccum& aa, size_t smem, cudaStream_t st) {
     const uint32_t nb = blocks_for(n, T);
-    if (out)
+    // no contact history: the built-in model is the frictionless Hertzian model (the reference's frictionless model
+    // has no contact wildcards; the full one has four)
+    if (!has_hist) {
+        if (out)
+            k_force<true, T, B, true><<<nb, T, smem, st>>>(k, s, c, n, has_hist, *out, aa);
+        else
+            k_force<false, T, B, true><<<nb, T, smem, st>>>(k, s, c, n, has_hist, ContactOutputs{}, aa);
+    } else if (out) {
         k_force<true, T, B><<<nb, T, smem, st>>>(k, s, c, n, has_hist, *out, aa);
-    else
+    } else {
         k_force<false, T, B><<<nb, T, smem, st>>>(k, s, c, n, has_hist, ContactOutputs{}, aa);
+    }
 }
 }  // namespace
 

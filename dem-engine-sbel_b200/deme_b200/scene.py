@@ -384,9 +384,12 @@ class SceneBuilder:
         self.integrator = intg
 
     def UseFrictionlessHertzianModel(self):
+        """The frictionless Hertzian model (the reference's FrictionlessHertzianForceModel.cu): the normal spring and
+        damper only, no rolling resistance, no tangential force and so no contact wildcards (history)."""
         self.n_wildcards = 0
 
     def UseFrictionalHertzianModel(self):
+        """The full Hertz--Mindlin model (the default): four contact wildcards (tangential displacement, time)."""
         self.n_wildcards = 4
 
     # ---- materials / templates / clumps ----

@@ -522,11 +522,13 @@ def hopper_wedge(n: int = 4_000_000, r_median: float = 1.5e-3, sigma: float = 0.
 
 
 def sphere_pile(n: int = 60, seed: int = 3, h: float = 2e-5, spread: float = 5.2e-3, noise: float = 4e-4,
-                vel_scale: float = 0.05, spin_scale: float = 20.0, lift: float = 2.2e-3, mesh_floor: bool = False):
+                vel_scale: float = 0.05, spin_scale: float = 20.0, lift: float = 2.2e-3, mesh_floor: bool = False,
+                frictionless: bool = False):
     """Loose pile of single spheres (radii U[2, 3] mm, two materials) pressed onto a floor plane with random
     velocities and spins: every contact branch of the Hertz-Mindlin model is active within a few dozen steps.
     Used by the adjoint tests.  ``mesh_floor``: the floor is a mesh body of two facets 0.19 m wide in the same
-    plane instead of an analytical plane."""
+    plane instead of an analytical plane.  ``frictionless``: the frictionless Hertzian model
+    (UseFrictionlessHertzianModel) instead of the full one."""
     rng = np.random.default_rng(seed)
     r = rng.uniform(2e-3, 3e-3, n).astype(f32)
     rho = 2500.0
@@ -557,8 +559,10 @@ def sphere_pile(n: int = 60, seed: int = 3, h: float = 2e-5, spread: float = 5.2
     s.SetGravitationalAcceleration((0, 0, -9.81))
     s.SetCDUpdateFreq(1)
     s.SetExpandFactor(0.0)  # contacts are exactly the overlapping pairs (the unset default would shrink them)
+    if frictionless:
+        s.UseFrictionlessHertzianModel()
     built = s.Initialize()
-    built.info.update(workload="sphere_pile", n=n, seed=seed, mesh_floor=mesh_floor)
+    built.info.update(workload="sphere_pile", n=n, seed=seed, mesh_floor=mesh_floor, frictionless=frictionless)
     return built
 
 

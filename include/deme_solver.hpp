@@ -242,6 +242,7 @@ class DEMForceModel {
     void SetPerContactWildcards(const std::set<std::string>& names) { m_contact_wildcards = names; }
 
     bool custom = false;
+    bool frictionless = false;  // UseFrictionlessHertzianModel: normal force only, no contact wildcards
     std::string m_force_model;
     std::set<std::string> m_contact_wildcards{"delta_tan_x", "delta_tan_y", "delta_tan_z", "delta_time"};
 };
@@ -624,6 +625,14 @@ class DEMSolver {
     // ---- force model ----
     std::shared_ptr<DEMForceModel> UseFrictionalHertzianModel() {
         force_model = std::make_shared<DEMForceModel>();
+        return force_model;
+    }
+    /* the frictionless Hertzian model (FrictionlessHertzianForceModel.cu): the built-in model with no contact
+     * wildcards runs its normal part only */
+    std::shared_ptr<DEMForceModel> UseFrictionlessHertzianModel() {
+        force_model = std::make_shared<DEMForceModel>();
+        force_model->frictionless = true;
+        force_model->m_contact_wildcards.clear();
         return force_model;
     }
     std::shared_ptr<DEMForceModel> DefineContactForceModel(const std::string& model) {
@@ -1448,7 +1457,7 @@ class DEMSolver {
         p.integrator = integrator;
         p.cd_update_freq = update_freq;
         p.n_contact_wildcards = force_model && force_model->custom ? (int32_t)force_model->m_contact_wildcards.size()
-                                                                   : 4;
+                                : (force_model && force_model->frictionless ? 0 : 4);
         p.domain[0] = box.x;
         p.domain[1] = box.y;
         p.domain[2] = box.z;

@@ -974,7 +974,9 @@ static void contact_force(oracle_ctx* c, uint32_t i) {
         fx += scal * nX;
         fy += scal * nY;
         fz += scal * nZ;
-        if ((double)Crr_cnt > 0.0) {
+        /* no contact wildcards: the frictionless Hertzian model (FrictionlessHertzianForceModel.cu), normal part only */
+        const int normal_only = c->nW == 0;
+        if (!normal_only && (double)Crr_cnt > 0.0) {
             int add_rr = 1;
             float R_eff = sqrtf((ARadius * BRadius) / (ARadius + BRadius));
             float kn_simple = (float)(FOUR_OVER_THREE * (double)E_cnt * (double)sqrtf(R_eff));
@@ -997,7 +999,7 @@ static void contact_force(oracle_ctx* c, uint32_t i) {
                 }
             }
         }
-        if ((double)mu_cnt > 0.0) {
+        if (!normal_only && (double)mu_cnt > 0.0) {
             float kt = (float)(8. * (double)G_cnt * (double)sqrt_Rd);
             float gt = (float)(-TWO_TIMES_SQRT_FIVE_OVER_SIX * (double)beta * (double)sqrtf(mass_eff * kt));
             float nkt = -kt;
