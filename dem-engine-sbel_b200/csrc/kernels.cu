@@ -930,6 +930,12 @@ __global__ void __launch_bounds__(256) k_history(uint32_t n, ContactView cur, Co
     if (cur.dN) n = min(n, *cur.dN);
     if (prev.dN) prevN = *prev.dN;
     if (i >= n) return;
+    if (!has_hist) {
+        // a model without contact wildcards keeps no history, and the reference builds no map for it
+        // (DEMCubContactDetection.cu:267, isHistoryless)
+        cur.mapping[i] = DEME_NULL_MAPPING_PARTNER;
+        return;
+    }
     const uint32_t A = cur.idA[i], B = cur.idB[i];
     const uint8_t t = cur.type[i];
     const uint64_t key = ((uint64_t)contact_group(t) << 32) | B;
