@@ -1293,6 +1293,23 @@ int32_t deme_change_family(deme_handle* h, uint32_t from, uint32_t to) {
     return check_launch(h, "change_family");
 }
 
+int32_t deme_set_family_contact(deme_handle* h, uint32_t a, uint32_t b, int32_t prevent) {
+    if (!h) return DEME_ERR_INVALID;
+    if (a > 255u || b > 255u) {
+        h->err = "family numbers lie in [0, 255]";
+        return DEME_ERR_INVALID;
+    }
+    const uint32_t lo = a < b ? a : b, hi = a < b ? b : a;
+    const uint32_t index = (1u + hi) * hi / 2u + lo;  // the device's mask_index
+    if (index >= DEME_NUM_FAMILY_MASK) {
+        h->err = "family mask entry out of range";
+        return DEME_ERR_INVALID;
+    }
+    TRY(cd_finish(h));
+    launch_set_mask(h->masks, index, prevent ? 1u : 0u, h->st_dt);
+    return check_launch(h, "set_family_contact");
+}
+
 // ------------------------------------------------------------------------------------------- search shape ----
 int32_t deme_set_search_shape(deme_handle* h, int32_t shape, float cell_factor) {
     if (!h) return DEME_ERR_INVALID;

@@ -1103,6 +1103,13 @@ void launch_change_family(ushort4* loc, uint32_t n, uint32_t from, uint32_t to, 
     k_change_family<<<blocks_for(n, 256), 256, 0, st>>>(loc, n, from, to);
 }
 
+// One entry of the family-mask table, written in stream order (no host buffer has to outlive the call).
+__global__ void k_set_mask(uint8_t* masks, uint32_t index, uint8_t value) { masks[index] = value; }
+void launch_set_mask(uint8_t* masks, uint32_t index, uint8_t value, cudaStream_t st) {
+    ProfScope prof_(KID_OTHER, st);
+    k_set_mask<<<1, 1, 0, st>>>(masks, index, value);
+}
+
 // The simulation time on the device (read by the family-change rules and prescribed-motion expressions): a float
 // advanced by h once per step, as the reference's dT advances timeElapsed (src/DEM/dT.cpp:1585).  A voided step
 // does not advance it.

@@ -151,6 +151,7 @@ int force_shape_count();                 // block shapes of the force kernel
 uint32_t force_shape_threads(int shape);
 void launch_window_done(const uint32_t* err, uint32_t* done, cudaStream_t st);
 void launch_change_family(ushort4* loc, uint32_t n, uint32_t from, uint32_t to, cudaStream_t st);
+void launch_set_mask(uint8_t* masks, uint32_t index, uint8_t value, cudaStream_t st);
 void launch_advance_time(float* time, float h, const uint32_t* err, cudaStream_t st);
 void launch_set_time(float* time, float t, cudaStream_t st);
 // Scenes with at most this many materials keep a table of contact-pair parameters (2 float4 per ordered pair).

@@ -316,6 +316,19 @@ class Solver(HandleSolver):
         self.lib.deme_change_family.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
         self._check(self.lib.deme_change_family(self.h, int(family_from), int(family_to)), "change_family")
 
+    def DisableContactBetweenFamilies(self, a: int, b: int):
+        """Contact between families a and b is off from the next detection (the reference's call on an initialized
+        solver)."""
+        self._set_family_contact(a, b, True)
+
+    def EnableContactBetweenFamilies(self, a: int, b: int):
+        """Contact between families a and b is on again from the next detection."""
+        self._set_family_contact(a, b, False)
+
+    def _set_family_contact(self, a: int, b: int, prevent: bool):
+        self.lib.deme_set_family_contact.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_int32]
+        self._check(self.lib.deme_set_family_contact(self.h, int(a), int(b), int(prevent)), "set_family_contact")
+
     def set_family_change_rules(self, rules):
         """ChangeFamilyWhen rules, a list of (from, to, condition) applied every step (see
         deme_set_family_change_rules); an empty list removes them."""

@@ -331,6 +331,11 @@ int32_t deme_set_async_cd(deme_handle* h, int32_t lag);
  * apply, the last one wins.  n = 0 removes the rules.  A rule that does not compile returns DEME_ERR_NVRTC with the
  * log. */
 int32_t deme_change_family(deme_handle* h, uint32_t from, uint32_t to);
+/* Contact between families a and b (either order) on a created solver: prevent = 1 disables it, 0 enables it
+ * (DisableContactBetweenFamilies / EnableContactBetweenFamilies on an initialized DEMSolver, src/DEM/APIPublic.cpp:
+ * 431-468, which write the workers' family-mask tables directly).  Ordered on the dynamics stream; the next contact
+ * detection uses it. */
+int32_t deme_set_family_contact(deme_handle* h, uint32_t a, uint32_t b, int32_t prevent);
 int32_t deme_set_family_change_rules(deme_handle* h, int32_t n, const uint32_t* from, const uint32_t* to,
                                      const char* const* conditions);
 

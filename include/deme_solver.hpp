@@ -581,11 +581,28 @@ class DEMSolver {
     }
 
     // ---- families ----
+    /* before Initialize: part of the scene; after it: written into the running solver's mask table at once, as the
+     * reference does (APIPublic.cpp:431-449), and kept for a later UpdateClumps */
     void DisableContactBetweenFamilies(unsigned a, unsigned b) {
         const unsigned lo = std::min(a, b), hi = std::max(a, b);
         if ((1u + hi) * hi / 2u + lo >= 255u * 256u / 2u)
             throw std::runtime_error("family mask entry out of range (the mask table holds 32640 entries)");
         no_contact.emplace_back(a, b);
+        if (h) check(deme_set_family_contact(h, a, b, 1));
+    }
+    /* after Initialize only (APIPublic.cpp:451-468): families are in contact unless disabled */
+    void EnableContactBetweenFamilies(unsigned a, unsigned b) {
+        if (!h)
+            throw std::runtime_error("There is no need to call EnableContactBetweenFamilies before system "
+                                     "initialization. All families have contacts with each other by default.");
+        const unsigned lo = std::min(a, b), hi = std::max(a, b);
+        no_contact.erase(std::remove_if(no_contact.begin(), no_contact.end(),
+                                        [&](const std::pair<unsigned, unsigned>& p) {
+                                            return std::min(p.first, p.second) == lo &&
+                                                   std::max(p.first, p.second) == hi;
+                                        }),
+                         no_contact.end());
+        check(deme_set_family_contact(h, a, b, 0));
     }
     void SetFamilyFixed(unsigned fam) {
         Presc p(fam);

@@ -12,7 +12,7 @@ single `return <bool>;` (a second return would overwrite the first decision).
 import numpy as np
 import pytest
 
-from _util import canonical, oracle
+from _util import canonical, capi, oracle, workloads
 from deme_b200 import SceneBuilder
 
 pytestmark = pytest.mark.gpu
@@ -121,4 +121,31 @@ def test_rule_that_does_not_compile_is_refused():
     g = Solver(scene())
     with pytest.raises(DemeError):
         g.set_family_change_rules([(0, 2, "return pos.q < 1;")])
+    g.close()
+
+
+def test_contact_between_families_toggled_on_a_running_solver():
+    """DisableContactBetweenFamilies / EnableContactBetweenFamilies after Initialize (deme_set_family_contact): the
+    next detection drops the pile's floor contacts and keeps its sphere pairs; enabled again, it finds the first
+    list again, bit for bit (the state does not move in between)."""
+    from deme_b200 import Solver
+    built = workloads.sphere_pile(n=400, seed=5)
+    fam_s, fam_w = int(built.arrays["family"][0]), int(built.arrays["family"][-1])
+    g = Solver(built)
+    g.step(3)
+    g.detect_contacts()
+    c0 = g.contacts()
+    floor = c0["type"] == capi.SPHERE_PLANE_CONTACT
+    assert floor.sum() > 20 and (~floor).sum() > 20
+    g.DisableContactBetweenFamilies(fam_w, fam_s)
+    g.detect_contacts()
+    c1 = g.contacts()
+    assert not np.any(c1["type"] == capi.SPHERE_PLANE_CONTACT)
+    for k in ("idA", "idB", "type"):
+        np.testing.assert_array_equal(c1[k], c0[k][~floor], err_msg=k)
+    g.EnableContactBetweenFamilies(fam_s, fam_w)
+    g.detect_contacts()
+    c2 = g.contacts()
+    for k in ("idA", "idB", "type"):
+        np.testing.assert_array_equal(c2[k], c0[k], err_msg=k)
     g.close()
