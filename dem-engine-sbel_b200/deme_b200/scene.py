@@ -345,6 +345,11 @@ class SceneBuilder:
         self.dir_exact = dir_exact
 
     def InstructBoxDomainNumVoxel(self, x, y, z, len_unit=1e-10):
+        """The voxel bit split and length unit given directly (APIPublic.cpp:94-114); the domain is the voxel
+        world."""
+        if int(x) + int(y) + int(z) != 64:
+            raise ValueError("Please give voxel numbers (as powers of 2) along each direction such that they add up "
+                             "to 64.")
         self.explicit_nv = (int(x), int(y), int(z), float(np.float32(len_unit)))
 
     def SetCoordSysOrigin(self, where):

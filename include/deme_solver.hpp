@@ -39,6 +39,9 @@
 namespace deme {
 
 enum class TIME_INTEGRATOR { FORWARD_EULER = 0, CENTERED_DIFFERENCE = 1, EXTENDED_TAYLOR = 2 };
+// src/DEM/Defines.h:104, 114: verbosity levels (accepted, no effect here) and output formats (CSV is written)
+enum VERBOSITY { QUIET = 0, ERROR = 10, WARNING = 20, INFO = 30, STEP_STATS = 32, STEP_METRIC = 35, DEBUG = 40 };
+enum class OUTPUT_FORMAT { CSV, BINARY, CHPF };
 
 class DEMMaterial {
   public:
@@ -480,6 +483,38 @@ class DEMSolver {
 
     // ---- world ----
     void InstructBoxDomainDimension(float x, float y, float z) { box = float3{x, y, z}; has_box = true; }
+    /* the voxel bit split and length unit given directly (APIPublic.cpp:94-114); the domain is then the voxel world */
+    void InstructBoxDomainNumVoxel(unsigned char x, unsigned char y, unsigned char z, float len_unit = 1e-10f) {
+        if ((unsigned)x + y + z != 64u)
+            throw std::runtime_error("Please give voxel numbers (as powers of 2) along each direction such that they "
+                                     "add up to 64.");
+        explicit_nv[0] = x;
+        explicit_nv[1] = y;
+        explicit_nv[2] = z;
+        explicit_l = len_unit;
+        has_explicit_nv = true;
+    }
+    bool GetInitStatus() const { return h != nullptr; }
+    double GetTimeStepSize() const { return h_step; }
+    float GetExpandFactor() const { return flat ? flat->params.beta : expand_factor; }
+    // reference tuning and diagnostics switches with no counterpart here (the contact list is always sorted, kernels
+    // are compiled ahead of time, output is CSV): accepted so that reference programs compile, no effect
+    void SetVerbosity(VERBOSITY) {}
+    /* CSV only (the writers below); the reference's binary and ChPF formats are not written */
+    void SetOutputFormat(OUTPUT_FORMAT f) {
+        if (f != OUTPUT_FORMAT::CSV) throw std::runtime_error("only the CSV output format is written");
+    }
+    void SetContactOutputFormat(OUTPUT_FORMAT f) { SetOutputFormat(f); }
+    void SetSortContactPairs(bool) {}
+    void SetJitifyClumpTemplates(bool = true) {}
+    void SetJitifyMassProperties(bool = true) {}
+    void SetOneBinPerThread(bool = true) {}
+    void UseCompactForceKernel(bool = true) {}
+    void EnsureKernelErrMsgLineNum(bool = true) {}
+    void InstructNumOwners(size_t) {}
+    void ReleaseFlattenedArrays() {}
+    void ShowThreadCollaborationStats() {}
+    void ClearThreadCollaborationStats() {}
     void SetCoordSysOrigin(const std::string& where) { origin = where; }
     void SetCoordSysOrigin(float3 lbf) { LBF = lbf; origin = "explicit"; }
     void InstructBoxDomainBoundingBC(const std::string& inst, const std::shared_ptr<DEMMaterial>& mat) {
@@ -1007,6 +1042,8 @@ class DEMSolver {
         check(deme_kinetic_energy(h, &ke));
         return ke;
     }
+    /* the clumps' kinetic energy (API.h:315): the energy above already sums clump owners only */
+    double GetClumpKineticEnergy() { return GetTotalKineticEnergy(); }
     double GetSimTime() {
         double t = 0;
         int64_t s = 0;
@@ -1210,10 +1247,19 @@ class DEMSolver {
     }
 
     void build_flat(FlatScene& f, const std::vector<std::shared_ptr<DEMClumpBatch>>& batches) {
-        if (!has_box) throw std::runtime_error("InstructBoxDomainDimension must be called before Initialize");
+        if (!has_box && !has_explicit_nv)
+            throw std::runtime_error("InstructBoxDomainDimension must be called before Initialize");
         uint8_t nv[3];
         double l = 0.0;
-        figure_out_nv(nv, l);
+        if (has_explicit_nv) {
+            for (int a = 0; a < 3; a++) nv[a] = explicit_nv[a];
+            l = (double)explicit_l;
+            const double vox = 65536.0 * l;
+            box = float3{(float)(vox * (double)(1ull << nv[0])), (float)(vox * (double)(1ull << nv[1])),
+                         (float)(vox * (double)(1ull << nv[2]))};
+        } else {
+            figure_out_nv(nv, l);
+        }
         const double voxel_size = 65536.0 * l;
         float3 lbf = LBF;
         if (origin == "center")
@@ -1488,6 +1534,9 @@ class DEMSolver {
     std::vector<std::shared_ptr<DEMMeshConnected>> meshes;
     float3 box{0.f, 0.f, 0.f};
     bool has_box = false;
+    bool has_explicit_nv = false;  // InstructBoxDomainNumVoxel
+    uint8_t explicit_nv[3] = {0, 0, 0};
+    float explicit_l = 0.f;
     std::string origin = "explicit";
     float3 LBF{0.f, 0.f, 0.f};
     std::string bounding_bc = "none";

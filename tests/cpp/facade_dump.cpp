@@ -54,7 +54,16 @@ int main(int argc, char** argv) {
     const auto xyz2 = read_vec<float>(in);       // batch 2 positions
 
     DEMSolver s;
-    s.InstructBoxDomainDimension(0.3f, 0.3f, 0.45f);
+    const bool numvoxel = argc >= 4 && std::string(argv[3]) == "nv";
+    if (numvoxel)
+        s.InstructBoxDomainNumVoxel(21, 21, 22, 4e-12f);
+    else
+        s.InstructBoxDomainDimension(0.3f, 0.3f, 0.45f);
+    // switches of the reference that have no effect here must still compile
+    s.SetVerbosity(INFO);
+    s.SetOutputFormat(OUTPUT_FORMAT::CSV);
+    s.SetSortContactPairs(true);
+    s.InstructNumOwners(100);
     s.SetCoordSysOrigin("center");
     auto m0 = s.LoadMaterial({{"E", 1e7f}, {"nu", 0.3f}, {"CoR", 0.5f}, {"mu", 0.5f}, {"Crr", 0.0f}});
     auto m1 = s.LoadMaterial({{"E", 5e7f}, {"nu", 0.25f}, {"CoR", 0.3f}, {"mu", 0.4f}, {"Crr", 0.02f}});
@@ -220,7 +229,7 @@ int main(int argc, char** argv) {
         const std::string c = cnt.str();
         put(out, "csv_contacts", c.data(), c.size());
     }
-    if (argc >= 4) {
+    if (argc >= 4 && !numvoxel) {
         const int steps = std::atoi(argv[3]);
         s.Initialize();  // flattens again: use the new FlatScene from here on
         for (int i = 0; i < steps; i++) s.DoStepDynamics();

@@ -44,10 +44,14 @@ MESH_OBJ = ("v 0 0 0\nv 0.02 0 0\nv 0.02 0.02 0\nv 0 0.02 0\nv 0.01 0.01 0.015\n
             "f 1 2 3 4\nf 1/1 2/1 5/1\nf -4 -3 -1\nf 3 4 5\nf 4 1 5\n")
 
 
-def python_scene(types, xyz1, q1, v1, w1, fam1, xyz2, extra=None):
-    """The scene of tests/cpp/facade_dump.cpp; `extra` = (positions, velocity) of sphere clumps of a third batch."""
+def python_scene(types, xyz1, q1, v1, w1, fam1, xyz2, extra=None, numvoxel=False):
+    """The scene of tests/cpp/facade_dump.cpp; `extra` = (positions, velocity) of sphere clumps of a third batch;
+    `numvoxel`: the voxel split given by InstructBoxDomainNumVoxel instead of the domain's dimensions."""
     s = SceneBuilder()
-    s.InstructBoxDomainDimension(0.3, 0.3, 0.45)
+    if numvoxel:
+        s.InstructBoxDomainNumVoxel(21, 21, 22, 4e-12)
+    else:
+        s.InstructBoxDomainDimension(0.3, 0.3, 0.45)
     s.SetCoordSysOrigin("center")
     m0 = s.LoadMaterial({"E": 1e7, "nu": 0.3, "CoR": 0.5, "mu": 0.5, "Crr": 0.0})
     m1 = s.LoadMaterial({"E": 5e7, "nu": 0.25, "CoR": 0.3, "mu": 0.4, "Crr": 0.02})
@@ -175,6 +179,26 @@ def build_exe(d):
                            CUDA_INC, os.path.join(ROOT, "tests", "cpp", "facade_dump.cpp"), "-o", exe, "-L", libdir,
                            "-ldeme_b200", f"-Wl,-rpath,{libdir}"])
     return exe
+
+
+def test_explicit_voxel_split_agrees(tmp_path):
+    """InstructBoxDomainNumVoxel: the same parameters and owner encoding from both front ends."""
+    if shutil.which("g++") is None or not os.path.exists(os.path.join(CUDA_INC, "vector_types.h")):
+        pytest.skip("g++ or the CUDA headers are missing")
+    solver.load_product_library()
+    exe = build_exe(tmp_path)
+    inputs = scene_inputs()
+    inp = write_inputs(tmp_path, inputs)
+    subprocess.check_call([exe, str(inp), str(tmp_path / "out.bin"), "nv"])
+    cpp = read_dump(tmp_path / "out.bin")
+    built = python_scene(*inputs, numvoxel=True)
+    assert cpp["params"] == bytes(built.params)
+    p = capi.SimParams.from_buffer_copy(cpp["params"])
+    assert (p.nvXp2, p.nvYp2, p.nvZp2) == (21, 21, 22)
+    for k in ("voxel", "locX", "locY", "locZ", "anal_relX", "anal_relZ"):
+        assert cpp[k] == np.ascontiguousarray(built.arrays[k]).tobytes(), k
+    with pytest.raises(ValueError, match="add up to 64"):
+        SceneBuilder().InstructBoxDomainNumVoxel(20, 21, 22)
 
 
 def test_params_and_prescriptions_agree(dump):
