@@ -322,6 +322,21 @@ static int32_t set_scene_boxes(deme_handle* h, const deme_scene* s) {
     return DEME_OK;
 }
 
+// The sphere id in the low bits of a cell-order record's last word and a CD radius bound in the bits above (at
+// least 4 of them; with fewer the bound is r_max_cd for every sphere).
+static void radius_bounds(SimConsts& k, uint32_t nS, float rmax) {
+    uint32_t idBits = 1;
+    while (idBits < 31 && (1ull << idBits) < (uint64_t)nS) idBits++;
+    if (32 - idBits >= 4) {
+        k.q_shift = idBits;
+        k.q_scale = rmax / (float)((1u << (32 - idBits)) - 1u);
+    } else {
+        k.q_shift = 31;
+        k.q_scale = rmax;
+    }
+    k.id_mask = (1u << k.q_shift) - 1u;
+}
+
 static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_scene* s) {
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -437,21 +452,9 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
     }
     TRY(set_scene_boxes(h, s));
     k.prefilter_abs = (float)(4e-7 * wmax + 1e-9);
-    {
-        // sphere id in the low bits of the record's last word, a CD radius bound in the bits above (at least 4 of
-        // them; with fewer the bound is r_max_cd for every sphere)
-        uint32_t idBits = 1;
-        while (idBits < 31 && (1ull << idBits) < (uint64_t)nS) idBits++;
-        if (32 - idBits >= 4) {
-            k.q_shift = idBits;
-            k.q_scale = rmax / (float)((1u << (32 - idBits)) - 1u);
-        } else {
-            k.q_shift = 31;
-            k.q_scale = rmax;
-        }
-        k.id_mask = (1u << k.q_shift) - 1u;
-    }
+    radius_bounds(k, nS, rmax);
     TRY(set_cell_grid(h, 1.0));
+    h->cellCap = h->nCells;  // the cell arrays below are sized for the finest grid (factor 1)
 
     // ---- device arrays ----
     TRY(dalloc_n(h, &h->voxel, nO));
@@ -1308,6 +1311,68 @@ int32_t deme_set_family_contact(deme_handle* h, uint32_t a, uint32_t b, int32_t 
     TRY(cd_finish(h));
     launch_set_mask(h->masks, index, prevent ? 1u : 0u, h->st_dt);
     return check_launch(h, "set_family_contact");
+}
+
+int32_t deme_change_clump_sizes(deme_handle* h, uint32_t n, const uint32_t* owners, const float* factors) {
+    if (!h || (n && (!owners || !factors))) return DEME_ERR_INVALID;
+    if (h->ownerScene) {
+        h->err = "change_clump_sizes: not with packed scenes";
+        return DEME_ERR_INVALID;
+    }
+    std::vector<float> fac(h->nClumps, 1.f);
+    std::vector<uint8_t> mark(h->nClumps, 0);
+    for (uint32_t i = 0; i < n; i++) {
+        if (owners[i] >= h->nClumps || !(factors[i] > 0.f)) {
+            h->err = "change_clump_sizes: owner is not a clump, or factor not positive";
+            return DEME_ERR_INVALID;
+        }
+        mark[owners[i]] = 1;
+        fac[owners[i]] = factors[i];  // a clump listed twice takes its last factor
+    }
+    TRY(cd_finish(h));
+    CUDA_TRY(h, cudaStreamSynchronize(h->st_dt));
+    const uint32_t nS = h->nS;
+    std::vector<float4> sph(nS);
+    std::vector<uint32_t> own(nS);
+    if (nS) {
+        CUDA_TRY(h, cudaMemcpy(sph.data(), h->sph, nS * sizeof(float4), cudaMemcpyDeviceToHost));
+        CUDA_TRY(h, cudaMemcpy(own.data(), h->sOwner, nS * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    }
+    // the components' relative positions and radii times the factor, in float (dTModifyComponents,
+    // src/kernel/DEMMiscKernels.cu:18-33); masses and moments stay
+    float rmax = 0.f;
+    for (uint32_t i = 0; i < nS; i++) {
+        float4& q = sph[i];
+        if (own[i] < h->nClumps && mark[own[i]]) {
+            const float f = fac[own[i]];
+            q.x *= f;
+            q.y *= f;
+            q.z *= f;
+            q.w *= f;
+        }
+        float r = q.w;
+        r += h->params.beta;
+        rmax = std::max(rmax, r);
+    }
+    if (nS) CUDA_TRY(h, cudaMemcpy(h->sph, sph.data(), nS * sizeof(float4), cudaMemcpyHostToDevice));
+    // the search grid follows the largest expanded radius; its arrays grow if the finest grid has more cells now
+    h->k.r_max_cd = rmax;
+    radius_bounds(h->k, nS, rmax);
+    h->sceneRmax.assign(1, rmax);
+    const float factor = h->cellFactor;
+    TRY(set_cell_grid(h, 1.0));
+    if (h->nCells > h->cellCap) {
+        dfree(h, h->cd.cellCount);
+        dfree(h, h->cd.cellStart);
+        h->cd.cellCount = h->cd.cellStart = nullptr;
+        TRY(dalloc_n(h, &h->cd.cellCount, (size_t)h->nCells + 1));
+        TRY(dalloc_n(h, &h->cd.cellStart, (size_t)h->nCells + 1));
+        TRY(ensure_scratch(h, std::max(scan_scratch_bytes(h->nCells + 1), scan_onepass_scratch_bytes(h->nCells + 1))));
+        h->cellCap = h->nCells;
+    }
+    TRY(set_cell_grid(h, factor));
+    h->outsValid = false;
+    return DEME_OK;
 }
 
 // ------------------------------------------------------------------------------------------- search shape ----

@@ -79,6 +79,7 @@ struct deme_handle {
     // contact detection
     CDView cd{};
     uint32_t nCells = 0;
+    uint32_t cellCap = 0;  // cells the cell arrays hold (the finest grid's count when they were sized)
     int cellBits = 0;
     SearchGrid* grids = nullptr;         // per scene (one for a plain run): see set_cell_grid
     uint32_t* ownerScene = nullptr;      // packed scenes: scene of each owner

@@ -92,6 +92,18 @@ class HandleSolver:
         except Exception:
             pass
 
+    def change_clump_sizes(self, owners, factors):
+        """ChangeClumpSizes: the listed clumps' component spheres get their relative positions and radii multiplied by
+        the factors (masses and moments stay); contacts are found anew at the next detection."""
+        o = np.ascontiguousarray(owners, np.uint32)
+        f = np.ascontiguousarray(factors, np.float32)
+        if o.shape != f.shape:
+            raise ValueError("one factor per clump")
+        fn = self._fn("change_clump_sizes")
+        fn.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
+        fn.restype = C.c_int32
+        self._check(fn(self.h, len(o), capi.ptr(o), capi.ptr(f)), "change_clump_sizes")
+
     # --- steps ---
     def detect_contacts(self):
         self._check(self._fn("detect_contacts")(self.h), "detect_contacts")

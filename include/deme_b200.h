@@ -336,6 +336,12 @@ int32_t deme_change_family(deme_handle* h, uint32_t from, uint32_t to);
  * 431-468, which write the workers' family-mask tables directly).  Ordered on the dynamics stream; the next contact
  * detection uses it. */
 int32_t deme_set_family_contact(deme_handle* h, uint32_t a, uint32_t b, int32_t prevent);
+/* ChangeClumpSizes (src/DEM/APIPublic.cpp:844-862; dTModifyComponents / kTModifyComponents,
+ * src/kernel/DEMMiscKernels.cu:18-52): the component spheres of each listed clump owner get their relative positions
+ * and radii multiplied by its factor (float products; a clump listed twice takes its last factor); masses and
+ * moments of inertia stay.  The search grid follows the new largest radius.  Contacts are found anew at the next
+ * detection.  Not with packed scenes. */
+int32_t deme_change_clump_sizes(deme_handle* h, uint32_t n, const uint32_t* owners, const float* factors);
 int32_t deme_set_family_change_rules(deme_handle* h, int32_t n, const uint32_t* from, const uint32_t* to,
                                      const char* const* conditions);
 

@@ -515,6 +515,49 @@ class DEMSolver {
     void ReleaseFlattenedArrays() {}
     void ShowThreadCollaborationStats() {}
     void ClearThreadCollaborationStats() {}
+    // Stubs in the reference itself, kept with its behaviour: SetFamilyPrescribedQuaternion checks the family and
+    // stores nothing (APIPublic.cpp:275-280), and PurgeFamily is empty (:869).
+    void SetFamilyPrescribedQuaternion(unsigned fam, const std::string&) {
+        if (fam > 255) throw std::runtime_error("family number should not be larger than 255");
+    }
+    void PurgeFamily(unsigned) {}
+    /* APIPublic.cpp:844-862: the listed clumps' spheres scaled by the factors (owner ids in the reference's numbering) */
+    void ChangeClumpSizes(const std::vector<uint32_t>& ids, const std::vector<float>& factors) {
+        if (!h) throw std::runtime_error("ChangeClumpSizes operates on the running solver: call it after Initialize");
+        if (ids.size() != factors.size()) throw std::runtime_error("ChangeClumpSizes: one factor per clump");
+        std::vector<uint32_t> o(ids.size());
+        for (size_t i = 0; i < ids.size(); i++) o[i] = handle_owner(ids[i]);
+        check(deme_change_clump_sizes(h, (uint32_t)o.size(), o.data(), factors.data()));
+    }
+    /* Per-kernel device times (deme_kernel_timing / deme_kernel_times) stand in for the reference's kT and dT phase
+     * timers (kT.h:179-181, dT.h:253-255).  Timing brackets every launch with events and keeps whole steps off CUDA
+     * graphs, so it is off until this build's EnableTimingStats turns it on. */
+    void EnableTimingStats(bool on = true) {
+        check(deme_kernel_timing(on ? 1 : 0));
+        timing_on = on;
+    }
+    void ClearTimingStats() {
+        if (timing_on) check(deme_kernel_timing(1));
+    }
+    void ShowTimingStats() {
+        const char* names[64];
+        double ms[64];
+        int64_t cnt[64];
+        int32_t n = 0;
+        check(deme_kernel_times(64, names, ms, cnt, &n));
+        double total = 0.0;
+        for (int i = 0; i < n; i++) total += ms[i];
+        std::printf("\n~~ KERNEL TIMING STATISTICS ~~\n");
+        if (!timing_on || total <= 0.0) {
+            std::printf("no kernel timed (EnableTimingStats turns per-kernel timing on)\n");
+            return;
+        }
+        std::printf("total device time: %.9g seconds\n", total / 1e3);
+        for (int i = 0; i < n; i++)
+            if (cnt[i] > 0)
+                std::printf("%s: %.9g seconds over %lld launches, %.6g%% of the total\n", names[i], ms[i] / 1e3,
+                            (long long)cnt[i], ms[i] / total * 100.);
+    }
     void SetCoordSysOrigin(const std::string& where) { origin = where; }
     void SetCoordSysOrigin(float3 lbf) { LBF = lbf; origin = "explicit"; }
     void InstructBoxDomainBoundingBC(const std::string& inst, const std::shared_ptr<DEMMaterial>& mat) {
@@ -526,6 +569,17 @@ class DEMSolver {
     void UpdateStepSize(double ts) {
         h_step = ts;
         if (h) check(deme_set_time_step(h, (float)ts));
+    }
+    /* after Initialize (APIPublic.cpp:786-790, which transfers the solver and simulation parameters again): the time
+     * step is applied; gravity, the contact margin and the integrator are fixed when the solver is created, so a
+     * change of them since Initialize is refused rather than ignored */
+    void UpdateSimParams() {
+        if (!h) throw std::runtime_error("UpdateSimParams: call it only after Initialize");
+        const deme_sim_params& p = flat->params;
+        if (p.G[0] != G.x || p.G[1] != G.y || p.G[2] != G.z || p.integrator != integrator ||
+            (expand_fixed && p.beta != expand_factor))
+            throw std::runtime_error("UpdateSimParams: only the time step can change after Initialize here");
+        check(deme_set_time_step(h, (float)h_step));
     }
     void SetInitBinSize(double b) { bin_size = b; }
     void SetCDUpdateFreq(int f) { update_freq = f; }
@@ -1535,6 +1589,7 @@ class DEMSolver {
     float3 box{0.f, 0.f, 0.f};
     bool has_box = false;
     bool has_explicit_nv = false;  // InstructBoxDomainNumVoxel
+    bool timing_on = false;        // EnableTimingStats
     uint8_t explicit_nv[3] = {0, 0, 0};
     float explicit_l = 0.f;
     std::string origin = "explicit";

@@ -1358,6 +1358,34 @@ double orc_kinetic_energy(oracle_ctx* c) {
 int32_t orc_max_spheres_in_bin(oracle_ctx* c) { return c->maxInBin; }
 double orc_time(oracle_ctx* c) { return c->t; }
 
+/* ChangeClumpSizes (APIPublic.cpp:844-862): markOwnerToChange, then dTModifyComponents (DEMMiscKernels.cu:4-33):
+ * relative positions and radii of the listed owners' spheres times the owner's factor (the last one given). */
+int32_t orc_change_clump_sizes(oracle_ctx* c, uint32_t n, const uint32_t* owners, const float* factors) {
+    float* fac = calloc((size_t)c->nO + 1, sizeof(float));
+    uint8_t* mark = calloc((size_t)c->nO + 1, 1);
+    for (uint32_t i = 0; i < n; i++) {
+        if (owners[i] >= c->nO) {
+            free(fac);
+            free(mark);
+            return DEME_ERR_INVALID;
+        }
+        mark[owners[i]] = 1;
+        fac[owners[i]] = factors[i];
+    }
+    for (uint32_t s = 0; s < c->nS; s++) {
+        uint32_t o = c->sOwner[s];
+        if (!mark[o]) continue;
+        float f = fac[o];
+        c->rX[s] *= f;
+        c->rY[s] *= f;
+        c->rZ[s] *= f;
+        c->rad[s] *= f;
+    }
+    free(fac);
+    free(mark);
+    return DEME_OK;
+}
+
 int32_t orc_set_family_prescription(oracle_ctx* c, int32_t family, const deme_family_prescription* p) {
     if (!c || !p || family < 0 || family >= DEME_NUM_FAMILIES) return DEME_ERR_INVALID;
     c->presc[family] = *p;

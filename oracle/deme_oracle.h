@@ -42,6 +42,7 @@ double orc_time(oracle_ctx* c);
 /* Replaces one family's constant prescription (deme_set_family_prescription's counterpart); a test that checks
  * prescribed-motion expressions sets, before each step, the values the expressions take at that step's time. */
 int32_t orc_set_family_prescription(oracle_ctx* c, int32_t family, const deme_family_prescription* p);
+int32_t orc_change_clump_sizes(oracle_ctx* c, uint32_t n, const uint32_t* owners, const float* factors);
 
 #ifdef __cplusplus
 }

@@ -64,6 +64,8 @@ int main(int argc, char** argv) {
     s.SetOutputFormat(OUTPUT_FORMAT::CSV);
     s.SetSortContactPairs(true);
     s.InstructNumOwners(100);
+    s.SetFamilyPrescribedQuaternion(4, "none");
+    s.PurgeFamily(4);
     s.SetCoordSysOrigin("center");
     auto m0 = s.LoadMaterial({{"E", 1e7f}, {"nu", 0.3f}, {"CoR", 0.5f}, {"mu", 0.5f}, {"Crr", 0.0f}});
     auto m1 = s.LoadMaterial({{"E", 5e7f}, {"nu", 0.25f}, {"CoR", 0.3f}, {"mu", 0.4f}, {"Crr", 0.02f}});
