@@ -472,6 +472,38 @@ inline void write_contact_csv(std::ostream& os, const FlatScene& f, const OwnerS
     }
 }
 
+class DEMSolver;
+
+/* DEMTracker (src/DEM/AuxClasses.h:76-121, AuxClasses.cpp:166-212): get and set one tracked owner (a clump batch's
+ * first clump plus an offset, an external object or a mesh body) through the solver's per-owner calls.  Owner ids are
+ * the reference's numbering, resolved when first used (after Initialize). */
+class DEMTracker {
+  public:
+    DEMTracker(DEMSolver* sys, const void* obj, int kind) : sys(sys), obj(obj), kind(kind) {}
+    float3 Pos(size_t offset = 0);
+    float3 AngVelLocal(size_t offset = 0);
+    float3 Vel(size_t offset = 0);
+    float4 OriQ(size_t offset = 0);
+    float3 ContactAcc(size_t offset = 0);
+    float3 ContactAngAccLocal(size_t offset = 0);
+    void SetPos(float3 pos, size_t offset = 0);
+    void SetAngVel(float3 angVel, size_t offset = 0);
+    void SetVel(float3 vel, size_t offset = 0);
+    void SetOriQ(float4 oriQ, size_t offset = 0);
+    /* an extra acceleration for the next step only: there is no such input on this build's step (a persistent one
+     * is a family prescription) */
+    void AddAcc(float3, size_t = 0) {
+        throw std::runtime_error("AddAcc is not supported here; prescribe the family's motion instead");
+    }
+    void ChangeClumpSizes(const std::vector<uint32_t>& ids, const std::vector<float>& factors);
+    uint32_t OwnerID();  // the tracked owner's id in the reference's numbering
+
+  private:
+    DEMSolver* sys;
+    const void* obj;
+    int kind;  // 0 clump batch, 1 external object, 2 mesh body
+};
+
 class DEMSolver {
   public:
     DEMSolver() = default;
@@ -634,6 +666,34 @@ class DEMSolver {
                                              const std::vector<float3>& xyz) {
         return AddClumps(std::vector<std::shared_ptr<DEMClumpTemplate>>(xyz.size(), type), xyz);
     }
+    std::shared_ptr<DEMTracker> Track(const std::shared_ptr<DEMClumpBatch>& obj) {
+        return std::make_shared<DEMTracker>(this, obj.get(), 0);
+    }
+    std::shared_ptr<DEMTracker> Track(const std::shared_ptr<DEMExternObj>& obj) {
+        return std::make_shared<DEMTracker>(this, obj.get(), 1);
+    }
+    std::shared_ptr<DEMTracker> Track(const std::shared_ptr<DEMMeshConnected>& obj) {
+        return std::make_shared<DEMTracker>(this, obj.get(), 2);
+    }
+    /* the reference's owner id of a batch's first clump, an external object or a mesh body */
+    uint32_t TrackedOwnerID(const void* obj, int kind) const {
+        if (!h) throw std::runtime_error("a tracker is read or written only after Initialize");
+        size_t id = 0;
+        if (kind == 0) {
+            for (const auto& b : system_batches) {
+                if (b.get() == obj) return (uint32_t)(id < n_clumps_init ? id : id + n_ext_init + n_mesh_init);
+                id += b->nClumps;
+            }
+        } else if (kind == 1) {
+            for (size_t e = 0; e < ext.size(); e++)
+                if (ext[e].get() == obj) return (uint32_t)(n_clumps_init + e);
+        } else {
+            for (size_t m = 0; m < meshes.size(); m++)
+                if (meshes[m].get() == obj) return (uint32_t)(n_clumps_init + n_ext_init + m);
+        }
+        throw std::runtime_error("the tracked object is not part of the initialized system");
+    }
+
     std::shared_ptr<DEMExternObj> AddExternalObject() {
         ext.push_back(std::make_shared<DEMExternObj>((unsigned)ext.size()));
         return ext.back();
@@ -1624,6 +1684,28 @@ class DEMSolver {
     size_t n_clumps_init = 0, n_clumps_system = 0, n_ext_init = 0, n_mesh_init = 0, n_templates_init = 0,
            n_materials_init = 0, n_presc_init = 0;
 };
+
+inline uint32_t DEMTracker::OwnerID() { return sys->TrackedOwnerID(obj, kind); }
+inline float3 DEMTracker::Pos(size_t offset) { return sys->GetOwnerPosition(OwnerID() + (uint32_t)offset); }
+inline float3 DEMTracker::AngVelLocal(size_t offset) { return sys->GetOwnerAngVel(OwnerID() + (uint32_t)offset); }
+inline float3 DEMTracker::Vel(size_t offset) { return sys->GetOwnerVelocity(OwnerID() + (uint32_t)offset); }
+inline float4 DEMTracker::OriQ(size_t offset) { return sys->GetOwnerOriQ(OwnerID() + (uint32_t)offset); }
+inline float3 DEMTracker::ContactAcc(size_t offset) { return sys->GetOwnerAcc(OwnerID() + (uint32_t)offset); }
+inline float3 DEMTracker::ContactAngAccLocal(size_t offset) {
+    return sys->GetOwnerAngAcc(OwnerID() + (uint32_t)offset);
+}
+inline void DEMTracker::SetPos(float3 pos, size_t offset) {
+    sys->SetOwnerPosition(OwnerID() + (uint32_t)offset, pos);
+}
+inline void DEMTracker::SetAngVel(float3 w, size_t offset) { sys->SetOwnerAngVel(OwnerID() + (uint32_t)offset, w); }
+inline void DEMTracker::SetVel(float3 v, size_t offset) { sys->SetOwnerVelocity(OwnerID() + (uint32_t)offset, v); }
+inline void DEMTracker::SetOriQ(float4 q, size_t offset) { sys->SetOwnerOriQ(OwnerID() + (uint32_t)offset, q); }
+inline void DEMTracker::ChangeClumpSizes(const std::vector<uint32_t>& ids, const std::vector<float>& factors) {
+    std::vector<uint32_t> shifted(ids);
+    const uint32_t first = OwnerID();
+    for (auto& x : shifted) x += first;
+    sys->ChangeClumpSizes(shifted, factors);
+}
 
 }  // namespace deme
 

@@ -274,6 +274,13 @@ int main(int argc, char** argv) {
             }
             put(out, "ops_pos", pos);
             put(out, "ops_vel", vel);
+            // trackers of the second batch (its first clump and the next) and of the cylinder-and-cone object
+            auto t2 = s.Track(b2);
+            auto tw = s.Track(wall);
+            const float3 tr[3] = {t2->Pos(0), t2->Vel(1), tw->Pos()};
+            const uint32_t tid[2] = {t2->OwnerID(), tw->OwnerID()};
+            put(out, "trk", tr, 3);
+            put(out, "trk_id", tid, 2);
             // UpdateClumps: forget the cached batches, add three spheres, carry the run over
             const uint32_t nc_before = s.GetNumContacts();
             const double t_before = s.GetSimTime();

@@ -300,6 +300,15 @@ def test_cpp_facade_owner_setters_getters_and_update_clumps(tmp_path):
     pos = built.decode_positions(st, kernel_literals=False) + lbf
     cpos = np.frombuffer(cpp["ops_pos"], f32).reshape(-1, 3).astype(np.float64)
     assert np.abs(cpos - pos).max() <= 1e-7, np.abs(cpos - pos).max()
+    # trackers (DEMTracker): the second batch starts at owner len(types), the cylinder-and-cone object is the second
+    # external object
+    tid = np.frombuffer(cpp["trk_id"], np.uint32)
+    assert list(tid) == [len(inputs[0]), built.info["n_clumps"] + 1]
+    trk = np.frombuffer(cpp["trk"], f32).reshape(3, 3)
+    cvel = np.frombuffer(cpp["ops_vel"], f32).reshape(-1, 3)
+    np.testing.assert_array_equal(trk[0], np.frombuffer(cpp["ops_pos"], f32).reshape(-1, 3)[tid[0]])
+    np.testing.assert_array_equal(trk[1], cvel[tid[0] + 1])
+    np.testing.assert_array_equal(trk[2], np.frombuffer(cpp["ops_pos"], f32).reshape(-1, 3)[tid[1]])
     # UpdateClumps: nothing moves, the counts and the time carry over, owners are numbered as the reference does
     nC = built.info["n_clumps"]
     nExt = nO - nC
