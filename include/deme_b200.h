@@ -39,7 +39,8 @@ typedef enum {
     DEME_ERR_TOO_LARGE = 9    /* input larger than a fixed capacity (nothing was launched) */
 } deme_status;
 
-/* Contact types (src/DEM/Defines.h:63-67).  Cylinder and cone are additions of this build. */
+/* Contact types (src/DEM/Defines.h:63-67).  Cylinder and cone are additions of this build; sphere--mesh contacts
+ * are detected here (the reference declares the type but detects none). */
 #define DEME_NOT_A_CONTACT 0
 #define DEME_SPHERE_SPHERE_CONTACT 1
 #define DEME_SPHERE_MESH_CONTACT 2
