@@ -643,7 +643,6 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     from deme_b200 import Solver, capi
-    from deme_b200 import solver as solver_mod
 
     built = build_drum(args.clumps, seed=2 + rank)
     s = Solver(built)

@@ -19,7 +19,6 @@ Everything is vectorised with numpy so million-clump scenes assemble in seconds.
 """
 from __future__ import annotations
 
-import ctypes as C
 import math
 from dataclasses import dataclass, field
 

@@ -11,7 +11,6 @@ import math
 
 import numpy as np
 
-from . import _capi as capi
 from .scene import SceneBuilder
 
 f32 = np.float32

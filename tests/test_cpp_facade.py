@@ -8,7 +8,6 @@ would upload.  The same scene is built here
 with SceneBuilder; every array and the parameter and prescription structs must agree bit for bit.  Compiling and
 running the C++ side needs no GPU.
 """
-import ctypes as C
 import os
 import shutil
 import subprocess
