@@ -404,11 +404,22 @@ static int32_t create_impl(deme_handle* h, const deme_sim_params* p, const deme_
             h->err = "n_tris > 0 needs tri_owner, tri_node1..3 and tri_material";
             return DEME_ERR_INVALID;
         }
-        for (uint32_t i = 0; i < h->nT; i++)
+        for (uint32_t i = 0; i < h->nT; i++) {
             if (s->tri_owner[i] < nClumps || s->tri_owner[i] >= nO || s->tri_material[i] >= std::max(nM, 1u)) {
                 h->err = "mesh facet owner (must follow the clump owners) or material out of range";
                 return DEME_ERR_INVALID;
             }
+            // a facet of zero area has no closest-point region test that is defined everywhere
+            const float *a = s->tri_node1 + 3 * (size_t)i, *b = s->tri_node2 + 3 * (size_t)i,
+                        *c = s->tri_node3 + 3 * (size_t)i;
+            const double u[3] = {(double)b[0] - a[0], (double)b[1] - a[1], (double)b[2] - a[2]};
+            const double v[3] = {(double)c[0] - a[0], (double)c[1] - a[1], (double)c[2] - a[2]};
+            const double n[3] = {u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]};
+            if (!(n[0] * n[0] + n[1] * n[1] + n[2] * n[2] > 0.0)) {
+                h->err = "mesh facet " + std::to_string(i) + " has zero area (or non-finite nodes)";
+                return DEME_ERR_INVALID;
+            }
+        }
     }
     CUDA_TRY(h, cudaStreamCreateWithFlags(&h->own_dt, cudaStreamNonBlocking));
     CUDA_TRY(h, cudaStreamCreateWithFlags(&h->own_kt, cudaStreamNonBlocking));

@@ -631,6 +631,13 @@ class SceneBuilder:
         tri_owner = np.concatenate([np.full(m.GetNumTriangles(), m0 + i, np.uint32) for i, m in enumerate(self.meshes)]) \
             if nMesh else np.zeros(0, np.uint32)
         tri_material = np.array([mt.load_order for m in self.meshes for mt in m.materials], np.uint16)
+        if nTri:
+            t64 = tri.astype(np.float64)
+            area2 = np.sum(np.cross(t64[:, 3:6] - t64[:, 0:3], t64[:, 6:9] - t64[:, 0:3]) ** 2, axis=1)
+            bad = np.nonzero(~(area2 > 0.0))[0]
+            if len(bad):
+                raise ValueError(f"mesh facet {int(bad[0])} has zero area (or non-finite nodes); "
+                                 f"{len(bad)} such facets in all")
 
         # ---- analytical components ----
         comps = []

@@ -171,3 +171,15 @@ def test_mesh_owners_follow_the_external_objects_when_flattened():
     s2.AddWavefrontMeshObject((TRI.astype(np.float32), np.array([[0, 1, 2]])))
     with pytest.raises(ValueError, match="does not have associated material"):
         s2.Initialize()
+
+
+def test_zero_area_facets_are_refused():
+    """A facet whose nodes are collinear has no closest-point region test that is defined everywhere; Initialize
+    refuses it (the C ABI does too), naming the facet."""
+    s = SceneBuilder()
+    s.InstructBoxDomainDimension(0.2, 0.2, 0.2)
+    m = s.LoadMaterial({"E": 1e7, "nu": 0.3, "CoR": 0.5, "mu": 0.3, "Crr": 0.0})
+    v = np.array([[0, 0, 0], [0.01, 0, 0], [0, 0.01, 0], [0.02, 0, 0]], np.float32)
+    s.AddWavefrontMeshObject((v, np.array([[0, 1, 2], [0, 1, 3]])), m)
+    with pytest.raises(ValueError, match="mesh facet 1 has zero area"):
+        s.Initialize()
