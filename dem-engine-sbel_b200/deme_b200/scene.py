@@ -155,6 +155,53 @@ class ExternObj:
                                 float(half_angle), float(u_min), float(u_max), 1 if normal_outward else 0))
 
 
+def write_wavefront(path: str, meshes) -> None:
+    """DEMMeshConnected::WriteWavefront (src/DEM/MeshUtils.cpp:119-165): the meshes' vertices, then their faces with
+    indices offset into one object, numbers printed as C++'s default stream prints a float (6 significant
+    digits)."""
+    with open(path, "w") as fh:
+        for m in meshes:
+            for v in m.vertices:
+                fh.write("v " + " ".join(f"{float(x):g}" for x in v) + "\n")
+        off = 1
+        for m in meshes:
+            for f in m.faces:
+                fh.write("f " + " ".join(str(int(i) + off) for i in f) + "\n")
+            off += len(m.vertices)
+
+
+def mesh_mass_properties(vertices, faces):
+    """Volume (the mass at unit density), centroid and the principal-axis-aligned moments of inertia about the
+    centroid of the solid a closed, outward-wound triangle mesh bounds, by the divergence theorem over each facet
+    (Eberly's polyhedral mass properties).  In float64."""
+    t = np.asarray(vertices, np.float64)[np.asarray(faces, np.int64)]
+    p0, p1, p2 = t[:, 0], t[:, 1], t[:, 2]
+    d = np.cross(p1 - p0, p2 - p0)
+
+    def sub(w0, w1, w2):
+        t0 = w0 + w1
+        f1 = t0 + w2
+        t1 = w0 * w0
+        t2 = t1 + w1 * t0
+        f2 = t2 + w2 * f1
+        f3 = w0 * t1 + w1 * t2 + w2 * f2
+        return f1, f2, f3, f2 + w0 * (f1 + w0), f2 + w1 * (f1 + w1), f2 + w2 * (f1 + w2)
+
+    fx = sub(p0[:, 0], p1[:, 0], p2[:, 0])
+    fy = sub(p0[:, 1], p1[:, 1], p2[:, 1])
+    fz = sub(p0[:, 2], p1[:, 2], p2[:, 2])
+    mass = np.sum(d[:, 0] * fx[0]) / 6.0
+    cx = np.sum(d[:, 0] * fx[1]) / 24.0 / mass
+    cy = np.sum(d[:, 1] * fy[1]) / 24.0 / mass
+    cz = np.sum(d[:, 2] * fz[1]) / 24.0 / mass
+    xx = np.sum(d[:, 0] * fx[2]) / 60.0
+    yy = np.sum(d[:, 1] * fy[2]) / 60.0
+    zz = np.sum(d[:, 2] * fz[2]) / 60.0
+    inertia = np.array([yy + zz - mass * (cy * cy + cz * cz), zz + xx - mass * (cz * cz + cx * cx),
+                        xx + yy - mass * (cx * cx + cy * cy)])
+    return float(mass), np.array([cx, cy, cz]), inertia
+
+
 def load_wavefront(path: str) -> tuple[np.ndarray, np.ndarray]:
     """Vertices (n x 3) and triangles (m x 3 vertex indices) of a Wavefront OBJ file: ``v`` and ``f`` records
     (DEMMeshConnected::LoadWavefrontMesh, src/DEM/BdrsAndObjs.h:243); polygons are split into fans, negative
@@ -241,6 +288,24 @@ class MeshObj:
 
     def Scale(self, s):
         self.vertices *= np.asarray(s, f32)
+
+    def Rotate(self, q):
+        """Rotates the nodes in the mesh's own frame by the unit quaternion q = (w, x, y, z)."""
+        w, x, y, z = (float(c) for c in np.asarray(q, np.float64).reshape(4))
+        R = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)],
+                      [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
+                      [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
+        self.vertices = (self.vertices.astype(np.float64) @ R.T).astype(f32)
+
+    def ComputeMassProperties(self):
+        """(mass at unit density, centroid, moments of inertia about the centroid) of the closed, outward-wound mesh
+        (DEMMeshConnected::ComputeMassProperties, declared in src/DEM/BdrsAndObjs.h:291; see
+        mesh_mass_properties)."""
+        return mesh_mass_properties(self.vertices, self.faces)
+
+    @staticmethod
+    def WriteWavefront(path: str, meshes):
+        write_wavefront(path, meshes)
 
 
 @dataclass

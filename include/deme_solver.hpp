@@ -215,6 +215,72 @@ class DEMMeshConnected {
     void Scale(float s) {
         for (auto& v : vertices) v = float3{v.x * s, v.y * s, v.z * s};
     }
+    /* rotates the nodes in the mesh's own frame by the unit quaternion q = (x, y, z, w) */
+    void Rotate(float4 q) {
+        const double w = q.w, x = q.x, y = q.y, z = q.z;
+        const double R[3][3] = {{1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)},
+                                {2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)},
+                                {2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)}};
+        for (auto& v : vertices) {
+            const double p[3] = {v.x, v.y, v.z};
+            v = float3{(float)(R[0][0] * p[0] + R[0][1] * p[1] + R[0][2] * p[2]),
+                       (float)(R[1][0] * p[0] + R[1][1] * p[1] + R[1][2] * p[2]),
+                       (float)(R[2][0] * p[0] + R[2][1] * p[1] + R[2][2] * p[2])};
+        }
+    }
+    /* Volume (the mass at unit density), centroid and the moments of inertia about the centroid along the mesh's
+     * axes, of the solid a closed, outward-wound mesh bounds (declared, not defined, in the reference:
+     * BdrsAndObjs.h:291): the divergence theorem over each facet (Eberly's polyhedral mass properties), in double. */
+    void ComputeMassProperties(double& mass, float3& center, float3& inertia) const {
+        double m = 0, sx = 0, sy = 0, sz = 0, xx = 0, yy = 0, zz = 0;
+        auto sub = [](double w0, double w1, double w2, double& f1, double& f2, double& f3) {
+            const double t0 = w0 + w1;
+            f1 = t0 + w2;
+            const double t1 = w0 * w0;
+            const double t2 = t1 + w1 * t0;
+            f2 = t2 + w2 * f1;
+            f3 = w0 * t1 + w1 * t2 + w2 * f2;
+        };
+        for (const int3& f : face_v_indices) {
+            const float3 a = vertices.at((size_t)f.x), b = vertices.at((size_t)f.y), c = vertices.at((size_t)f.z);
+            const double u[3] = {(double)b.x - a.x, (double)b.y - a.y, (double)b.z - a.z};
+            const double v[3] = {(double)c.x - a.x, (double)c.y - a.y, (double)c.z - a.z};
+            const double d[3] = {u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]};
+            double f1x, f2x, f3x, f1y, f2y, f3y, f1z, f2z, f3z;
+            sub(a.x, b.x, c.x, f1x, f2x, f3x);
+            sub(a.y, b.y, c.y, f1y, f2y, f3y);
+            sub(a.z, b.z, c.z, f1z, f2z, f3z);
+            m += d[0] * f1x;
+            sx += d[0] * f2x;
+            sy += d[1] * f2y;
+            sz += d[2] * f2z;
+            xx += d[0] * f3x;
+            yy += d[1] * f3y;
+            zz += d[2] * f3z;
+        }
+        m /= 6.0;
+        const double cx = sx / 24.0 / m, cy = sy / 24.0 / m, cz = sz / 24.0 / m;
+        xx /= 60.0;
+        yy /= 60.0;
+        zz /= 60.0;
+        mass = m;
+        center = float3{(float)cx, (float)cy, (float)cz};
+        inertia = float3{(float)(yy + zz - m * (cy * cy + cz * cz)), (float)(zz + xx - m * (cz * cz + cx * cx)),
+                         (float)(xx + yy - m * (cx * cx + cy * cy))};
+    }
+    /* WriteWavefront (src/DEM/MeshUtils.cpp:119-165): the meshes' vertices, then their faces offset into one
+     * object */
+    static void WriteWavefront(const std::string& filename, std::vector<DEMMeshConnected>& meshes) {
+        std::ofstream mf(filename);
+        for (const auto& m : meshes)
+            for (const auto& v : m.vertices) mf << "v " << v.x << " " << v.y << " " << v.z << "\n";
+        int off = 1;
+        for (const auto& m : meshes) {
+            for (const auto& f : m.face_v_indices)
+                mf << "f " << f.x + off << " " << f.y + off << " " << f.z + off << "\n";
+            off += (int)m.vertices.size();
+        }
+    }
 
     size_t nTri = 0;
     std::vector<float3> vertices;

@@ -54,6 +54,7 @@ int main(int argc, char** argv) {
     const auto xyz2 = read_vec<float>(in);       // batch 2 positions
 
     DEMSolver s;
+    std::vector<float> mesh_props;
     const bool numvoxel = argc >= 4 && std::string(argv[3]) == "nv";
     if (numvoxel)
         s.InstructBoxDomainNumVoxel(21, 21, 22, 4e-12f);
@@ -114,6 +115,15 @@ int main(int argc, char** argv) {
         mesh->SetMass(2.5f);
         mesh->SetMOI(float3{1e-3f, 2e-3f, 3e-3f});
         mesh->SetFamily(3);
+        // mesh utilities: a rotated copy's mass properties, and both written back as one Wavefront file
+        DEMMeshConnected copy(obj);
+        copy.Rotate(float4{0.f, 0.6f, 0.f, 0.8f});
+        double mp_mass = 0.0;
+        float3 mp_c{0.f, 0.f, 0.f}, mp_i{0.f, 0.f, 0.f};
+        copy.ComputeMassProperties(mp_mass, mp_c, mp_i);
+        mesh_props = {(float)mp_mass, mp_c.x, mp_c.y, mp_c.z, mp_i.x, mp_i.y, mp_i.z};
+        std::vector<DEMMeshConnected> both{*mesh, copy};
+        DEMMeshConnected::WriteWavefront(std::string(argv[2]) + ".out.obj", both);
     }
     s.SetFamilyFixed(3);
     s.SetFamilyPrescribedAngVel(10, "0", "2.0943951", "0");
@@ -173,6 +183,7 @@ int main(int argc, char** argv) {
     put(out, "mat_mu", f.mat_mu);
     put(out, "mat_Crr", f.mat_Crr);
     put(out, "family_masks", f.family_masks);
+    put(out, "mesh_props", mesh_props);
     put(out, "tri_owner", f.tri_owner);
     put(out, "tri_node1", f.tri_node1);
     put(out, "tri_node2", f.tri_node2);

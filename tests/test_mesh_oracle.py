@@ -183,3 +183,31 @@ def test_zero_area_facets_are_refused():
     s.AddWavefrontMeshObject((v, np.array([[0, 1, 2], [0, 1, 3]])), m)
     with pytest.raises(ValueError, match="mesh facet 1 has zero area"):
         s.Initialize()
+
+
+def test_mesh_mass_properties_rotation_and_writer(tmp_path):
+    """ComputeMassProperties on a unit cube (volume 1, centroid at its centre, moments 1/6) and an icosphere (the
+    sphere's 4/3 pi R^3 and 2/5 m R^2 within its faceting, 0.3 %); Rotate turns a mesh without changing its volume;
+    WriteWavefront then LoadWavefrontMesh gives the meshes back."""
+    import math
+    from deme_b200 import workloads
+    from deme_b200.scene import MeshObj, write_wavefront
+    V = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], np.float32)
+    F = np.array([[0, 2, 1], [0, 3, 2], [4, 5, 6], [4, 6, 7], [0, 1, 5], [0, 5, 4], [1, 2, 6], [1, 6, 5],
+                  [2, 3, 7], [2, 7, 6], [3, 0, 4], [3, 4, 7]])
+    cube = MeshObj(V, F, 0)
+    m, c, inertia = cube.ComputeMassProperties()
+    assert abs(m - 1.0) < 1e-12 and np.abs(c - 0.5).max() < 1e-12 and np.abs(inertia - 1 / 6).max() < 1e-12
+    v, f = workloads.icosphere(0.1, 4)
+    ball = MeshObj(v, f, 1)
+    m, c, inertia = ball.ComputeMassProperties()
+    assert abs(m / (4 / 3 * math.pi * 1e-3) - 1) < 3e-3 and np.abs(c).max() < 1e-9
+    assert np.abs(inertia / (0.4 * m * 0.01) - 1).max() < 3e-3
+    cube.Rotate((math.cos(0.3), math.sin(0.3), 0.0, 0.0))
+    m2, c2, _ = cube.ComputeMassProperties()
+    assert abs(m2 - 1.0) < 1e-6 and abs(c2[0] - 0.5) < 1e-6
+    write_wavefront(str(tmp_path / "two.obj"), [cube, ball])
+    vv, ff = load_wavefront(str(tmp_path / "two.obj"))
+    assert len(vv) == 8 + len(v) and len(ff) == 12 + len(f)
+    np.testing.assert_array_equal(ff[12:], f + 8)
+    assert np.abs(vv[8:] - v).max() <= 1e-6
