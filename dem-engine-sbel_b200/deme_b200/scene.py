@@ -249,6 +249,15 @@ class MeshObj:
     def GetTriangle(self, i: int) -> np.ndarray:
         return self.vertices[self.faces[i]]
 
+    def Clear(self):
+        self.vertices = np.zeros((0, 3), f32)
+        self.faces = np.zeros((0, 3), np.int64)
+        self.materials = None
+
+    def UseNormals(self, use: bool = True):
+        """Accepted without effect: the reference reorders facet nodes to agree with the file's normals, but facets
+        here are two-sided, so the order does not matter."""
+
     def SetFamily(self, code: int):
         if code > 255 or code < 0:
             raise ValueError(f"family number {code} is larger than the max allowance 255")

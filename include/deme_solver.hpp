@@ -188,6 +188,21 @@ class DEMMeshConnected {
         return true;
     }
     size_t GetNumTriangles() const { return nTri; }
+    /* the i-th facet's nodes (DEMTriangle p1, p2, p3 in the reference) */
+    std::vector<float3> GetTriangle(size_t i) const {
+        const int3 f = face_v_indices.at(i);
+        return {vertices.at((size_t)f.x), vertices.at((size_t)f.y), vertices.at((size_t)f.z)};
+    }
+    void Clear() {
+        vertices.clear();
+        face_v_indices.clear();
+        materials.clear();
+        nTri = 0;
+        isMaterialSet = false;
+    }
+    /* the reference reorders each facet's nodes to agree with the file's vertex normals; facets here are two-sided,
+     * so the order does not matter and this is accepted without effect */
+    void UseNormals(bool = true) {}
     void SetFamily(unsigned code) {
         if (code > 255) throw std::runtime_error("family number is larger than the max allowance 255");
         family_code = code;
