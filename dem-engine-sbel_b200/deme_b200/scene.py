@@ -143,6 +143,12 @@ class ExternObj:
         self.components.append((capi.ANAL_PLANE, material, np.asarray(pos, f32), _normalize_f32(normal), 0.0, 0.0,
                                 0.0, 0))
 
+    def AddPlate(self, pos, normal, xdim: float, ydim: float, material: Material):
+        """DEMExternObj::AddPlate (src/DEM/BdrsAndObjs.h:152-170): kept as a component with its half sizes, and, as
+        in the reference (DEMHelperKernels.cu:385-387, 439-441), it meets no sphere."""
+        self.components.append((capi.ANAL_PLATE, material, np.asarray(pos, f32), _normalize_f32(normal),
+                                float(f32(xdim) / 2.0), float(f32(ydim) / 2.0), 0.0, 0))
+
     def AddCylinder(self, point, axis, radius: float, material: Material, normal_outward: bool = False):
         """Infinite cylinder through ``point`` along ``axis``.  Spheres live inside unless normal_outward."""
         self.components.append((capi.ANAL_CYLINDER, material, np.asarray(point, f32), _normalize_f32(axis),

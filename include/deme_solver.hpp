@@ -121,6 +121,12 @@ class DEMExternObj {
     void AddPlane(float3 pos, float3 normal, const std::shared_ptr<DEMMaterial>& mat) {
         entities.push_back({DEME_ANAL_PLANE, mat, pos, normalize_host(normal), 0.f, 0.f, 0.f, 0});
     }
+    /* AddPlate (BdrsAndObjs.h:152-170): kept with its half sizes; as in the reference (DEMHelperKernels.cu:385-387,
+     * 439-441) it meets no sphere */
+    void AddPlate(float3 pos, float3 normal, float xdim, float ydim, const std::shared_ptr<DEMMaterial>& mat) {
+        entities.push_back({DEME_ANAL_PLATE, mat, pos, normalize_host(normal), (float)(xdim / 2.0),
+                            (float)(ydim / 2.0), 0.f, 0});
+    }
     /* infinite cylinder through `point` along `axis`; spheres live inside unless normal_outward */
     void AddCylinder(float3 point, float3 axis, float radius, const std::shared_ptr<DEMMaterial>& mat,
                      bool normal_outward = false) {

@@ -102,6 +102,7 @@ int main(int argc, char** argv) {
     s.AddBCPlane(float3{0.f, 0.f, -0.1f}, float3{0.1f, 0.f, 1.f}, m1);
     auto wall = s.AddExternalObject();
     wall->AddCylinder(float3{0.f, 0.f, 0.f}, float3{0.f, 0.f, 1.f}, 0.12f, m0);
+    wall->AddPlate(float3{0.f, 0.05f, -0.15f}, float3{0.f, 0.f, 1.f}, 0.04f, 0.03f, m0);
     wall->AddCone(float3{0.f, 0.f, -0.2f}, float3{0.f, 0.f, 1.f}, 0.5235988f, 0.03f, 0.15f, m1);
     wall->SetFamily(10);
     {

@@ -73,6 +73,7 @@ def python_scene(types, xyz1, q1, v1, w1, fam1, xyz2, extra=None, numvoxel=False
     s.AddBCPlane((0, 0, -0.1), (0.1, 0, 1), m1)
     wall = s.AddExternalObject()
     wall.AddCylinder((0, 0, 0), (0, 0, 1), 0.12, m0)
+    wall.AddPlate((0, 0.05, -0.15), (0, 0, 1), 0.04, 0.03, m0)
     wall.AddCone((0, 0, -0.2), (0, 0, 1), float(f32(0.5235988)), 0.03, 0.15, m1)
     wall.SetFamily(10)
     with tempfile.TemporaryDirectory() as d:
