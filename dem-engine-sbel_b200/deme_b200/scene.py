@@ -208,6 +208,25 @@ def mesh_mass_properties(vertices, faces):
     return float(mass), np.array([cx, cy, cz]), inertia
 
 
+def read_clump_components(path: str, x_id="x", y_id="y", z_id="z", r_id="r"):
+    """DEMClumpTemplate::ReadComponentFromFile (src/DEM/Structs.h:419-437): radii and relative positions from a CSV
+    file with a header row naming the columns (any order among others; a missing column reads 0)."""
+    with open(path) as fh:
+        lines = [ln for ln in fh.read().splitlines()]
+    if not lines:
+        return np.zeros(0, f32), np.zeros((0, 3), f32)
+    head = [c.strip() for c in lines[0].split(",")]
+    cols = [head.index(k) if k in head else -1 for k in (x_id, y_id, z_id, r_id)]
+    rows = []
+    for ln in lines[1:]:
+        if not ln.strip():
+            continue
+        cells = [c.strip() for c in ln.split(",")]
+        rows.append([float(np.float32(cells[c])) if 0 <= c < len(cells) else 0.0 for c in cols])
+    a = np.asarray(rows, f32).reshape(-1, 4)
+    return a[:, 3].copy(), a[:, :3].copy()
+
+
 def load_wavefront(path: str) -> tuple[np.ndarray, np.ndarray]:
     """Vertices (n x 3) and triangles (m x 3 vertex indices) of a Wavefront OBJ file: ``v`` and ``f`` records
     (DEMMeshConnected::LoadWavefrontMesh, src/DEM/BdrsAndObjs.h:243); polygons are split into fans, negative
@@ -482,7 +501,12 @@ class SceneBuilder:
         self.materials.append(m)
         return m
 
-    def LoadClumpType(self, mass, moi, radii, rel_pos, materials) -> ClumpTemplate:
+    def LoadClumpType(self, mass, moi, radii, rel_pos, materials=None) -> ClumpTemplate:
+        """Components as arrays (radii, rel_pos, materials), or from a CSV file: LoadClumpType(mass, moi, path,
+        materials) (API.h:175-184; the file's header names the columns x, y, z and r, read as
+        DEMClumpTemplate::ReadComponentFromFile reads them)."""
+        if isinstance(radii, str):
+            radii, rel_pos, materials = (*read_clump_components(radii), rel_pos)
         radii = np.asarray(radii, f32).reshape(-1)
         rel_pos = np.asarray(rel_pos, f32).reshape(-1, 3)
         if not isinstance(materials, (list, tuple)):

@@ -62,6 +62,43 @@ class DEMClumpTemplate {
     std::vector<std::shared_ptr<DEMMaterial>> materials;
     unsigned mark = 0;
     unsigned nComp() const { return (unsigned)radii.size(); }
+    /* ReadComponentFromFile (src/DEM/Structs.h:419-437): sphere components from a CSV file with a header row;
+     * the columns named x_id, y_id, z_id and r_id, in any order among others (a missing one reads 0), are appended.
+     * Returns 0, or 1 if the file cannot be read. */
+    int ReadComponentFromFile(const std::string& filename, const std::string& x_id = "x",
+                              const std::string& y_id = "y", const std::string& z_id = "z",
+                              const std::string& r_id = "r") {
+        std::ifstream in(filename);
+        if (!in) return 1;
+        auto split = [](const std::string& line) {
+            std::vector<std::string> out;
+            std::stringstream ss(line);
+            std::string cell;
+            while (std::getline(ss, cell, ',')) {
+                const size_t b = cell.find_first_not_of(" \t\r"), e = cell.find_last_not_of(" \t\r");
+                out.push_back(b == std::string::npos ? std::string() : cell.substr(b, e - b + 1));
+            }
+            return out;
+        };
+        std::string line;
+        if (!std::getline(in, line)) return 0;
+        const std::vector<std::string> head = split(line);
+        int col[4] = {-1, -1, -1, -1};
+        const std::string* ids[4] = {&x_id, &y_id, &z_id, &r_id};
+        for (int k = 0; k < 4; k++)
+            for (size_t c = 0; c < head.size(); c++)
+                if (head[c] == *ids[k]) col[k] = (int)c;
+        while (std::getline(in, line)) {
+            if (line.find_first_not_of(" \t\r") == std::string::npos) continue;
+            const std::vector<std::string> row = split(line);
+            float v[4] = {0.f, 0.f, 0.f, 0.f};
+            for (int k = 0; k < 4; k++)
+                if (col[k] >= 0 && (size_t)col[k] < row.size()) v[k] = std::strtof(row[col[k]].c_str(), nullptr);
+            relPos.push_back(float3{v[0], v[1], v[2]});
+            radii.push_back(v[3]);
+        }
+        return 0;
+    }
 };
 
 class DEMClumpBatch {
@@ -729,6 +766,24 @@ class DEMSolver {
         t->AssignName(name);
         templates.push_back(t);
         return t;
+    }
+    /* the template built by the caller (API.h:173) */
+    std::shared_ptr<DEMClumpTemplate> LoadClumpType(DEMClumpTemplate& clump) {
+        return LoadClumpType(clump.mass, clump.MOI, clump.radii, clump.relPos, clump.materials);
+    }
+    /* components from a CSV file (API.h:175-184; DEMClumpTemplate::ReadComponentFromFile) */
+    std::shared_ptr<DEMClumpTemplate> LoadClumpType(float mass, float3 moi, const std::string& filename,
+                                                    const std::vector<std::shared_ptr<DEMMaterial>>& mats) {
+        DEMClumpTemplate c;
+        if (c.ReadComponentFromFile(filename)) throw std::runtime_error("cannot read clump file " + filename);
+        return LoadClumpType(mass, moi, c.radii, c.relPos, mats);
+    }
+    std::shared_ptr<DEMClumpTemplate> LoadClumpType(float mass, float3 moi, const std::string& filename,
+                                                    const std::shared_ptr<DEMMaterial>& mat) {
+        DEMClumpTemplate c;
+        if (c.ReadComponentFromFile(filename)) throw std::runtime_error("cannot read clump file " + filename);
+        return LoadClumpType(mass, moi, c.radii, c.relPos,
+                             std::vector<std::shared_ptr<DEMMaterial>>(c.radii.size(), mat));
     }
     std::shared_ptr<DEMClumpTemplate> LoadClumpType(float mass, float3 moi, const std::vector<float>& radii,
                                                     const std::vector<float3>& relPos,

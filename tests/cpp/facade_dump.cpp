@@ -42,6 +42,9 @@ static const char* kMeshObj =
     "v 0 0 0\nv 0.02 0 0\nv 0.02 0.02 0\nv 0 0.02 0\nv 0.01 0.01 0.015\n"
     "f 1 2 3 4\nf 1/1 2/1 5/1\nf -4 -3 -1\nf 3 4 5\nf 4 1 5\n";
 
+// the third clump template's components (the Python side writes the same text)
+static const char* kClumpCsv = "r,note,x,y,z\n0.004,top,0,0,0.0025\n0.004,bottom,0,0,-0.0025\n";
+
 int main(int argc, char** argv) {
     if (argc < 3 || argc > 5) return 2;
     std::ifstream in(argv[1], std::ios::binary);
@@ -76,8 +79,12 @@ int main(int argc, char** argv) {
     T.push_back(s.LoadClumpType(2.5e-3f, float3{1e-7f, 1.2e-7f, 1.5e-7f}, {4e-3f, 5e-3f, 4.5e-3f},
                                 {float3{3e-3f, 0.f, 0.f}, float3{-1.5e-3f, 2.6e-3f, 0.f}, float3{-1.5e-3f, -2.6e-3f, 0.f}},
                                 {m0, m1, m0}));
-    T.push_back(s.LoadClumpType(1.8e-3f, float3{8e-8f, 9e-8f, 9e-8f}, {4e-3f, 4e-3f},
-                                {float3{0.f, 0.f, 2.5e-3f}, float3{0.f, 0.f, -2.5e-3f}}, m1));
+    {
+        // the third template from a clump file (header names the columns; an extra column is ignored)
+        const std::string csv = std::string(argv[2]) + ".clump.csv";
+        std::ofstream(csv) << kClumpCsv;
+        T.push_back(s.LoadClumpType(1.8e-3f, float3{8e-8f, 9e-8f, 9e-8f}, csv, m1));
+    }
     const size_t n1 = types.size(), n2 = xyz2.size() / 3;
     std::vector<std::shared_ptr<DEMClumpTemplate>> tv;
     std::vector<float3> p1, vv, ww, p2;

@@ -43,6 +43,18 @@ MESH_OBJ = ("v 0 0 0\nv 0.02 0 0\nv 0.02 0.02 0\nv 0 0.02 0\nv 0.01 0.01 0.015\n
             "f 1 2 3 4\nf 1/1 2/1 5/1\nf -4 -3 -1\nf 3 4 5\nf 4 1 5\n")
 
 
+# the third clump template's components (tests/cpp/facade_dump.cpp writes the same text)
+CLUMP_CSV = "r,note,x,y,z\n0.004,top,0,0,0.0025\n0.004,bottom,0,0,-0.0025\n"
+
+
+def _clump_from_file(s, mat):
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "clump.csv")
+        with open(path, "w") as fh:
+            fh.write(CLUMP_CSV)
+        return s.LoadClumpType(1.8e-3, (8e-8, 9e-8, 9e-8), path, mat)
+
+
 def python_scene(types, xyz1, q1, v1, w1, fam1, xyz2, extra=None, numvoxel=False):
     """The scene of tests/cpp/facade_dump.cpp; `extra` = (positions, velocity) of sphere clumps of a third batch;
     `numvoxel`: the voxel split given by InstructBoxDomainNumVoxel instead of the domain's dimensions."""
@@ -59,7 +71,7 @@ def python_scene(types, xyz1, q1, v1, w1, fam1, xyz2, extra=None, numvoxel=False
     T = [s.LoadSphereType(mass_s, r_s, m0),
          s.LoadClumpType(2.5e-3, (1e-7, 1.2e-7, 1.5e-7), [4e-3, 5e-3, 4.5e-3],
                          [[3e-3, 0, 0], [-1.5e-3, 2.6e-3, 0], [-1.5e-3, -2.6e-3, 0]], [m0, m1, m0]),
-         s.LoadClumpType(1.8e-3, (8e-8, 9e-8, 9e-8), [4e-3, 4e-3], [[0, 0, 2.5e-3], [0, 0, -2.5e-3]], m1)]
+         _clump_from_file(s, m1)]
     b1 = s.AddClumps([T[t] for t in types], xyz1)
     b1.SetOriQ(q1)
     b1.SetVel(v1)
