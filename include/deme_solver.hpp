@@ -107,8 +107,10 @@ class DEMClumpBatch {
                                        oriQ(n, float4{0, 0, 0, 1}), families(n, 0) {}
     size_t GetNumClumps() const { return nClumps; }
     void SetTypes(const std::vector<std::shared_ptr<DEMClumpTemplate>>& t) { check(t.size(), "SetTypes"); types = t; }
+    void SetTypes(const std::shared_ptr<DEMClumpTemplate>& t) { SetTypes({nClumps, t}); }
     void SetType(const std::shared_ptr<DEMClumpTemplate>& t) { SetTypes({nClumps, t}); }
     void SetPos(const std::vector<float3>& p) { check(p.size(), "SetPos"); xyz = p; }
+    void SetPos(float3 p) { SetPos(std::vector<float3>(nClumps, p)); }
     void SetVel(const std::vector<float3>& v) { check(v.size(), "SetVel"); vel = v; }
     void SetVel(float3 v) { SetVel(std::vector<float3>(nClumps, v)); }
     void SetAngVel(const std::vector<float3>& w) { check(w.size(), "SetAngVel"); angVel = w; }
