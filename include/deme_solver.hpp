@@ -42,6 +42,7 @@ enum class TIME_INTEGRATOR { FORWARD_EULER = 0, CENTERED_DIFFERENCE = 1, EXTENDE
 // src/DEM/Defines.h:104, 114: verbosity levels (accepted, no effect here) and output formats (CSV is written)
 enum VERBOSITY { QUIET = 0, ERROR = 10, WARNING = 20, INFO = 30, STEP_STATS = 32, STEP_METRIC = 35, DEBUG = 40 };
 enum class OUTPUT_FORMAT { CSV, BINARY, CHPF };
+enum class FORCE_MODEL { HERTZIAN, HERTZIAN_FRICTIONLESS, CUSTOM };  // src/DEM/Defines.h:116
 
 class DEMMaterial {
   public:
@@ -369,6 +370,16 @@ class DEMForceModel {
         return 0;
     }
     void SetPerContactWildcards(const std::set<std::string>& names) { m_contact_wildcards = names; }
+    /* DEMForceModel::SetForceModelType (AuxClasses.cpp:218-236): the built-in full or frictionless Hertzian model
+     * with its wildcards, or a custom one (its string comes from DefineCustomModel) */
+    void SetForceModelType(FORCE_MODEL t) {
+        custom = t == FORCE_MODEL::CUSTOM;
+        frictionless = t == FORCE_MODEL::HERTZIAN_FRICTIONLESS;
+        if (t == FORCE_MODEL::HERTZIAN)
+            m_contact_wildcards = {"delta_tan_x", "delta_tan_y", "delta_tan_z", "delta_time"};
+        else if (frictionless)
+            m_contact_wildcards.clear();
+    }
 
     bool custom = false;
     bool frictionless = false;  // UseFrictionlessHertzianModel: normal force only, no contact wildcards
