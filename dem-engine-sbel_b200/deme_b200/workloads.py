@@ -881,8 +881,10 @@ def mesh_ball_drop(n: int = 2000, r: float = 2e-3, rho: float = 2600.0, ball_rad
     z0 = -box / 2 + 2 * r
     m_s = s.LoadMaterial({"E": 1e8, "nu": 0.3, "CoR": 0.3, "mu": 0.4, "Crr": 0.01})
     m_b = s.LoadMaterial({"E": 5e8, "nu": 0.3, "CoR": 0.3, "mu": 0.3, "Crr": 0.0})
-    types = [s.LoadSphereType(sphere_mass(float(ri), rho), float(ri), m_s) for ri in rad.astype(f32)]
-    b = s.AddClumps(types, (P + np.array([0.0, 0.0, z0 + r])).astype(f32))
+    # one sphere type per distinct radius (a packed bed has one)
+    r_u, r_idx = np.unique(rad.astype(f32), return_inverse=True)
+    tmpl = [s.LoadSphereType(sphere_mass(float(ri), rho), float(ri), m_s) for ri in r_u]
+    b = s.AddClumps([tmpl[k] for k in r_idx], (P + np.array([0.0, 0.0, z0 + r])).astype(f32))
     b.SetFamily(0)
     for ax, sg in ((0, 1), (0, -1), (1, 1), (1, -1)):
         pos = np.zeros(3)
