@@ -101,3 +101,55 @@ def heap_angle(built, state, axis_xy, z_floor: float, ring: float) -> float:
         sel = np.ones_like(hs, bool)
     slope = np.polyfit(xs[sel], hs[sel], 1)[0]
     return float(math.degrees(math.atan(-slope)))
+
+
+def _rotate_f32(q, r):
+    """hostApplyOriQToVector3<float> (src/DEM/HostSideHelpers.hpp:384-394) in float32, operation by operation."""
+    f = np.float32
+    w, x, y, z = (np.asarray(c, f) for c in q)
+    rx, ry, rz = (np.asarray(c, f) for c in r)
+    two, one = f(2.0), f(1.0)
+    X = (two * (w * w + x * x) - one) * rx + (two * (x * y - w * z)) * ry + (two * (x * z + w * y)) * rz
+    Y = (two * (x * y + w * z)) * rx + (two * (w * w + y * y) - one) * ry + (two * (y * z - w * x)) * rz
+    Z = (two * (x * z - w * y)) * rx + (two * (y * z + w * x)) * ry + (two * (w * w + z * z) - one) * rz
+    return X, Y, Z
+
+
+def inspect(built, state, quantity: str = "clump_max_z", template_volume=None) -> float:
+    """The reference's inspectors over the whole domain (DEMInspector, src/DEM/AuxClasses.cpp:14-106;
+    inspectSphereProperty, src/kernel/DEMSphereQueryKernels.cu:9-50):
+
+    * "clump_max_z" / "clump_min_z": the largest sphere top / smallest sphere bottom, Z +- r, the sphere centre
+      formed as the kernel forms it (owner position in float64 from the voxel code and the kernel literals, the
+      relative position rotated in float32, the lower corner added, rounded to float32);
+    * "clump_max_absv": the largest speed of a sphere centre, |v + R (omega x relPos)| in float32;
+    * "clump_volume": the sum of the clumps' template volumes (``template_volume[i]`` for template i; 0 if not
+      given).
+    The C++ façade's inspect_quantity computes the same, bit for bit."""
+    a = built.arrays
+    f = np.float32
+    if quantity == "clump_volume":
+        tv = np.asarray(template_volume if template_volume is not None else [], f)
+        marks = np.asarray(built.info["owner_template"], np.int64)
+        vals = np.where(marks < len(tv), tv[np.minimum(marks, max(len(tv) - 1, 0))] if len(tv) else f(0), f(0))
+        out = f(0)
+        for v in np.asarray(vals, f):  # in owner order, as the façade sums
+            out = f(out + v)
+        return float(out)
+    if quantity not in ("clump_max_z", "clump_min_z", "clump_max_absv"):
+        raise ValueError(f"{quantity} is not a known query type.")
+    own = np.asarray(a["sphere_owner"], np.int64)
+    q = [np.asarray(state[k], f)[own] for k in ("oriQw", "oriQx", "oriQy", "oriQz")]
+    rel = [np.asarray(a[k], f) for k in ("relX", "relY", "relZ")]
+    rad = np.asarray(a["radius"], f)
+    if quantity == "clump_max_absv":
+        wx, wy, wz = (np.asarray(state[k], f)[own] for k in ("omgX", "omgY", "omgZ"))
+        rx, ry, rz = rel
+        X, Y, Z = _rotate_f32(q, (wy * rz - wz * ry, wz * rx - wx * rz, wx * ry - wy * rx))
+        vx, vy, vz = (np.asarray(state[k], f)[own] for k in ("vX", "vY", "vZ"))
+        sx, sy, sz = X + vx, Y + vy, Z + vz
+        return float(np.max(np.sqrt(sx * sx + sy * sy + sz * sz)))
+    _, _, dz = _rotate_f32(q, rel)
+    oz = built.decode_positions(state, kernel_literals=True)[own, 2]
+    Zs = (oz + dz.astype(np.float64) + float(f(built.params.lbf[2]))).astype(f)
+    return float(np.max(Zs + rad) if quantity == "clump_max_z" else np.min(Zs - rad))

@@ -62,6 +62,8 @@ class DEMClumpTemplate {
     std::vector<float3> relPos;
     std::vector<std::shared_ptr<DEMMaterial>> materials;
     unsigned mark = 0;
+    float volume = 0.f;  // for the "clump_volume" inspector (DEMClumpTemplate::SetVolume)
+    void SetVolume(float vol) { volume = vol; }
     unsigned nComp() const { return (unsigned)radii.size(); }
     /* ReadComponentFromFile (src/DEM/Structs.h:419-437): sphere components from a CSV file with a header row;
      * the columns named x_id, y_id, z_id and r_id, in any order among others (a missing one reads 0), are appended.
@@ -493,13 +495,14 @@ struct OwnerState {
     std::vector<uint64_t> voxel;
     std::vector<uint16_t> locX, locY, locZ;
     std::vector<float> oriQw, oriQx, oriQy, oriQz, vX, vY, vZ;
+    std::vector<float> omgX, omgY, omgZ;  // angular velocity in the owner's frame
     std::vector<uint8_t> family;
     void resize(size_t n) {
         voxel.resize(n);
         locX.resize(n);
         locY.resize(n);
         locZ.resize(n);
-        for (auto* v : {&oriQw, &oriQx, &oriQy, &oriQz, &vX, &vY, &vZ}) v->resize(n);
+        for (auto* v : {&oriQw, &oriQx, &oriQy, &oriQz, &vX, &vY, &vZ, &omgX, &omgY, &omgZ}) v->resize(n);
         family.resize(n);
     }
 };
@@ -528,6 +531,47 @@ inline float3 rotate(float3 r, float Qw, float Qx, float Qy, float Qz) {
 }
 inline float speed(float x, float y, float z) { return std::sqrt(x * x + y * y + z * z); }
 }  // namespace csv_detail
+
+/* The reference's inspectors (DEMInspector, src/DEM/AuxClasses.cpp:14-106; inspectSphereProperty,
+ * src/kernel/DEMSphereQueryKernels.cu:9-50), on an owner state, over the whole domain:
+ *   "clump_max_z" / "clump_min_z": the largest sphere top / smallest sphere bottom, Z +- r, with the sphere centre
+ *   formed as the kernel forms it (owner position in double from the voxel code and the kernel literals, the
+ *   relative position rotated in float, the lower corner added, rounded to float);
+ *   "clump_max_absv": the largest speed of a sphere centre, |v + R (omega x relPos)| in float;
+ *   "clump_volume": the sum of the clumps' template volumes (DEMClumpTemplate::SetVolume, 0 unless set). */
+inline float inspect_quantity(const FlatScene& f, const OwnerState& st, const std::string& q,
+                              const std::vector<float>& template_volume) {
+    using namespace csv_detail;
+    const deme_sim_params& p = f.params;
+    if (q == "clump_volume") {
+        float sum = 0.f;
+        for (size_t o = 0; o < f.owner_template.size(); o++)
+            sum += f.owner_template[o] < template_volume.size() ? template_volume[f.owner_template[o]] : 0.f;
+        return sum;
+    }
+    const bool top = q == "clump_max_z", bottom = q == "clump_min_z", absv = q == "clump_max_absv";
+    if (!top && !bottom && !absv) throw std::runtime_error(q + " is not a known query type.");
+    float best = bottom ? 3.4e38f : -3.4e38f;
+    for (size_t i = 0; i < f.radius.size(); i++) {
+        const size_t o = f.sphere_owner[i];
+        const float qw = st.oriQw[o], qx = st.oriQx[o], qy = st.oriQy[o], qz = st.oriQz[o];
+        float v;
+        if (absv) {
+            const float rx = f.relX[i], ry = f.relY[i], rz = f.relZ[i];
+            const float wx = st.omgX[o], wy = st.omgY[o], wz = st.omgZ[o];
+            const float3 w = rotate(float3{wy * rz - wz * ry, wz * rx - wx * rz, wx * ry - wy * rx}, qw, qx, qy, qz);
+            v = speed(w.x + st.vX[o], w.y + st.vY[o], w.z + st.vZ[o]);
+        } else {
+            const float3 d = rotate(float3{f.relX[i], f.relY[i], f.relZ[i]}, qw, qx, qy, qz);
+            const double oz = (double)(st.voxel[o] >> (p.nvXp2 + p.nvYp2)) * p.voxel_size_kernel +
+                              (double)st.locZ[o] * p.l_kernel;
+            const float Z = (float)(oz + (double)d.z + (double)p.lbf[2]);
+            v = top ? Z + f.radius[i] : Z - f.radius[i];
+        }
+        best = bottom ? std::min(best, v) : std::max(best, v);
+    }
+    return best;
+}
 
 inline void write_sphere_csv(std::ostream& os, const FlatScene& f, const OwnerState& st, unsigned content,
                              const std::set<unsigned>& no_output = {}) {
@@ -639,6 +683,18 @@ class DEMTracker {
     DEMSolver* sys;
     const void* obj;
     int kind;  // 0 clump batch, 1 external object, 2 mesh body
+};
+
+/* DEMInspector (src/DEM/AuxClasses.h:42-74): one of the reference's reductions over the running solver's state
+ * (inspect_quantity), read back to the host. */
+class DEMInspector {
+  public:
+    DEMInspector(DEMSolver* sys, const std::string& quantity) : sys(sys), quantity(quantity) {}
+    float GetValue();
+
+  private:
+    DEMSolver* sys;
+    std::string quantity;
 };
 
 class DEMSolver {
@@ -820,6 +876,24 @@ class DEMSolver {
     std::shared_ptr<DEMClumpBatch> AddClumps(const std::shared_ptr<DEMClumpTemplate>& type,
                                              const std::vector<float3>& xyz) {
         return AddClumps(std::vector<std::shared_ptr<DEMClumpTemplate>>(xyz.size(), type), xyz);
+    }
+    /* CreateInspector (API.h:248-249): "clump_max_z", "clump_min_z", "clump_max_absv" or "clump_volume" over the
+     * whole domain; a region (a compiled expression of X, Y, Z in the reference) is not supported */
+    std::shared_ptr<DEMInspector> CreateInspector(const std::string& quantity = "clump_max_z") {
+        if (quantity != "clump_max_z" && quantity != "clump_min_z" && quantity != "clump_max_absv" &&
+            quantity != "clump_volume")
+            throw std::runtime_error(quantity + " is not a known query type.");
+        return std::make_shared<DEMInspector>(this, quantity);
+    }
+    std::shared_ptr<DEMInspector> CreateInspector(const std::string&, const std::string&) {
+        throw std::runtime_error("inspectors of a region are not supported here; inspect the whole domain");
+    }
+    float InspectValue(const std::string& quantity) {
+        if (!h) throw std::runtime_error("Inspector should only be used after the simulation system is initialized");
+        const OwnerState st = pull_owner_state();
+        std::vector<float> vols;
+        for (const auto& t : templates) vols.push_back(t->volume);
+        return inspect_quantity(*flat, st, quantity, vols);
     }
     std::shared_ptr<DEMTracker> Track(const std::shared_ptr<DEMClumpBatch>& obj) {
         return std::make_shared<DEMTracker>(this, obj.get(), 0);
@@ -1350,6 +1424,9 @@ class DEMSolver {
         s.vX = st.vX.data();
         s.vY = st.vY.data();
         s.vZ = st.vZ.data();
+        s.omgX = st.omgX.data();
+        s.omgY = st.omgY.data();
+        s.omgZ = st.omgZ.data();
         s.family = st.family.data();
         check(deme_download_state(h, &s));
         return st;
@@ -1840,6 +1917,7 @@ class DEMSolver {
            n_materials_init = 0, n_presc_init = 0;
 };
 
+inline float DEMInspector::GetValue() { return sys->InspectValue(quantity); }
 inline uint32_t DEMTracker::OwnerID() { return sys->TrackedOwnerID(obj, kind); }
 inline float3 DEMTracker::Pos(size_t offset) { return sys->GetOwnerPosition(OwnerID() + (uint32_t)offset); }
 inline float3 DEMTracker::AngVelLocal(size_t offset) { return sys->GetOwnerAngVel(OwnerID() + (uint32_t)offset); }

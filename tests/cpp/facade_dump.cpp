@@ -226,6 +226,17 @@ int main(int argc, char** argv) {
         st.vY = f.vY;
         st.vZ = f.vZ;
         st.family = f.family;
+        st.omgX = f.omgX;
+        st.omgY = f.omgY;
+        st.omgZ = f.omgZ;
+        {
+            // the inspectors' reductions on the initial state (template volumes 1, 2, 3)
+            const float insp[4] = {inspect_quantity(f, st, "clump_max_z", {1.f, 2.f, 3.f}),
+                                   inspect_quantity(f, st, "clump_min_z", {1.f, 2.f, 3.f}),
+                                   inspect_quantity(f, st, "clump_max_absv", {1.f, 2.f, 3.f}),
+                                   inspect_quantity(f, st, "clump_volume", {1.f, 2.f, 3.f})};
+            put(out, "inspect", insp, 4);
+        }
         const unsigned all = OUTPUT_CONTENT::ABSV | OUTPUT_CONTENT::VEL | OUTPUT_CONTENT::FAMILY;
         std::ostringstream sph, clu;
         write_sphere_csv(sph, f, st, all, {3});

@@ -179,7 +179,7 @@ def test_csv_output_agrees_byte_for_byte(dump, tmp_path):
 
 def test_flat_arrays_agree_bit_for_bit(dump):
     cpp, built = dump
-    names = [k for k in cpp if k not in ("params", "prescriptions", "motion", "mesh_props")
+    names = [k for k in cpp if k not in ("params", "prescriptions", "motion", "mesh_props", "inspect")
              and not k.startswith("csv_") and not k.startswith("_")]
     assert len(names) == 50
     for k in names:
@@ -235,6 +235,19 @@ def test_mesh_utilities_agree(dump, tmp_path):
     v_cpp, f_cpp = load_wavefront(cpp["_dir"] + "/out.bin.out.obj")
     np.testing.assert_array_equal(f_py, f_cpp)
     assert np.abs(v_py - v_cpp).max() <= 1e-6
+
+
+def test_inspectors_agree(dump):
+    """The inspectors' reductions (CreateInspector: clump_max_z, clump_min_z, clump_max_absv, clump_volume) on the
+    initial state, from the façade's inspect_quantity and statistics.inspect, bit for bit."""
+    from deme_b200 import statistics
+    cpp, built = dump
+    st = built.initial_state()
+    got = np.frombuffer(cpp["inspect"], f32)
+    want = [statistics.inspect(built, st, q, template_volume=[1.0, 2.0, 3.0])
+            for q in ("clump_max_z", "clump_min_z", "clump_max_absv", "clump_volume")]
+    np.testing.assert_array_equal(got, np.asarray(want, f32))
+    assert got[0] > got[1] and got[2] > 0 and got[3] > 0
 
 
 def test_params_and_prescriptions_agree(dump):
