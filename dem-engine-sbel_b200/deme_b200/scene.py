@@ -162,18 +162,28 @@ class ExternObj:
 
 
 def write_wavefront(path: str, meshes) -> None:
-    """DEMMeshConnected::WriteWavefront (src/DEM/MeshUtils.cpp:119-165): the meshes' vertices, then their faces with
-    indices offset into one object, numbers printed as C++'s default stream prints a float (6 significant
-    digits)."""
+    """DEMMeshConnected::WriteWavefront (src/DEM/MeshUtils.cpp:119-165): every mesh's vertices, then the normals of
+    the meshes that have them, then the faces with indices offset into one object (``f a//n b//n c//n`` for a mesh
+    with normals); numbers printed as C++'s default stream prints a float (6 significant digits)."""
     with open(path, "w") as fh:
         for m in meshes:
             for v in m.vertices:
                 fh.write("v " + " ".join(f"{float(x):g}" for x in v) + "\n")
-        off = 1
         for m in meshes:
-            for f in m.faces:
-                fh.write("f " + " ".join(str(int(i) + off) for i in f) + "\n")
+            for v in m.normals:
+                fh.write("vn " + " ".join(f"{float(x):g}" for x in v) + "\n")
+        off, noff = 1, 1
+        for m in meshes:
+            if len(m.normals):
+                if len(m.face_normals) != len(m.faces):
+                    raise ValueError("a mesh with normals needs one normal triple per facet")
+                for f, n in zip(m.faces, m.face_normals):
+                    fh.write("f " + " ".join(f"{int(i) + off}//{int(j) + noff}" for i, j in zip(f, n)) + "\n")
+            else:
+                for f in m.faces:
+                    fh.write("f " + " ".join(str(int(i) + off) for i in f) + "\n")
             off += len(m.vertices)
+            noff += len(m.normals)
 
 
 def mesh_mass_properties(vertices, faces):
@@ -227,37 +237,89 @@ def read_clump_components(path: str, x_id="x", y_id="y", z_id="z", r_id="r"):
     return a[:, 3].copy(), a[:, :3].copy()
 
 
-def load_wavefront(path: str) -> tuple[np.ndarray, np.ndarray]:
-    """Vertices (n x 3) and triangles (m x 3 vertex indices) of a Wavefront OBJ file: ``v`` and ``f`` records
-    (DEMMeshConnected::LoadWavefrontMesh, src/DEM/BdrsAndObjs.h:243); polygons are split into fans, negative
-    indices count from the end, texture and normal indices after ``/`` are ignored."""
-    verts, faces = [], []
+def read_wavefront(path: str) -> dict:
+    """The records of a Wavefront OBJ file as the reference's parser reads them (OBJ::ParseLine,
+    src/core/utils/WavefrontMeshLoader.hpp:578-647, behind DEMMeshConnected::LoadWavefrontMesh,
+    src/DEM/MeshUtils.cpp:44-112): ``v`` and ``vn`` records with three coordinates (a float rounded from the decimal
+    value), ``f`` records of three or more corners split into fans about the first corner, tags in any letter case.
+    Returns the vertices (n x 3), the facets' vertex indices (m x 3), the normals and the facets' normal indices
+    (the corners' ``a//n`` or ``a/t/n`` normal indices, three at a time).  Where the reference misreads a record,
+    this reads it as the OBJ format defines it: a negative index counts back from the last record read (the
+    reference subtracts one from it, leaving an index outside the mesh), and a vertex or normal record with more
+    numbers (a weight, a colour) or a trailing ``#`` comment is kept with its first three (the reference drops it,
+    shifting every later index)."""
+    verts, norms, faces, flat_n = [], [], [], []
     with open(path) as fh:
         for line in fh:
-            tok = line.split()
+            tok = line.split("#", 1)[0].split()
             if not tok:
                 continue
-            if tok[0] == "v":
-                verts.append([float(x) for x in tok[1:4]])
-            elif tok[0] == "f":
-                idx = []
+            tag = tok[0].lower()
+            if tag in ("v", "vn"):
+                if len(tok) >= 4:
+                    (verts if tag == "v" else norms).append([float(x) for x in tok[1:4]])
+            elif tag == "f" and len(tok) >= 4:
+                vi, ni = [], []
                 for t in tok[1:]:
-                    i = int(t.split("/")[0])
-                    idx.append(i - 1 if i > 0 else len(verts) + i)
-                for j in range(1, len(idx) - 1):
-                    faces.append([idx[0], idx[j], idx[j + 1]])
-    return np.asarray(verts, f32).reshape(-1, 3), np.asarray(faces, np.int64).reshape(-1, 3)
+                    parts = t.split("/")
+                    i = int(parts[0])
+                    vi.append(i - 1 if i > 0 else len(verts) + i)
+                    if len(parts) >= 3 and parts[2]:
+                        k = int(parts[2])
+                        ni.append(k - 1 if k > 0 else len(norms) + k)
+                    else:
+                        ni.append(None)
+                for j in range(1, len(vi) - 1):
+                    faces.append([vi[0], vi[j], vi[j + 1]])
+                    flat_n.extend(ni[c] for c in (0, j, j + 1) if ni[c] is not None)
+    nf = len(flat_n) // 3
+    return {"vertices": np.asarray(verts, f32).reshape(-1, 3), "faces": np.asarray(faces, np.int64).reshape(-1, 3),
+            "normals": np.asarray(norms, f32).reshape(-1, 3),
+            "face_normals": np.asarray(flat_n[:3 * nf], np.int64).reshape(-1, 3)}
+
+
+def load_wavefront(path: str) -> tuple[np.ndarray, np.ndarray]:
+    """Vertices (n x 3) and triangles (m x 3 vertex indices) of a Wavefront OBJ file (read_wavefront)."""
+    r = read_wavefront(path)
+    return r["vertices"], r["faces"]
+
+
+def facet_nodes(vertices, faces, normals=None, face_normals=None) -> np.ndarray:
+    """Each facet's three nodes (m x 9, float32).  Given the file's normals, a facet whose right-hand normal
+    cross(p2 - p1, p3 - p1) points away from the normal of its first corner has nodes 2 and 3 swapped
+    (DEMMeshConnected::UseNormals, applied at initialisation: src/DEM/APIPrivate.cpp:545-560), the products
+    in float as the reference's float3 arithmetic forms them."""
+    t = np.asarray(vertices, f32)[np.asarray(faces, np.int64)]
+    if normals is not None:
+        if len(face_normals) < len(t):
+            raise ValueError("UseNormals needs a normal index for every facet")
+        n = np.asarray(normals, f32)[np.asarray(face_normals, np.int64)[:len(t), 0]]
+        ab, ac = t[:, 1] - t[:, 0], t[:, 2] - t[:, 0]
+        cx = ab[:, 1] * ac[:, 2] - ab[:, 2] * ac[:, 1]
+        cy = ab[:, 2] * ac[:, 0] - ab[:, 0] * ac[:, 2]
+        cz = ab[:, 0] * ac[:, 1] - ab[:, 1] * ac[:, 0]
+        flip = (cx * n[:, 0] + cy * n[:, 1]) + cz * n[:, 2] < 0
+        t = t.copy()
+        t[flip, 1], t[flip, 2] = t[flip, 2], t[flip, 1].copy()
+    return t.reshape(-1, 9)
 
 
 class MeshObj:
     """DEMMeshConnected (src/DEM/BdrsAndObjs.h:173-300): a body represented by triangle facets, given in its own
     frame.  Defaults as the reference's: the fixed family, mass 1, principal moments 1, at the origin."""
 
-    def __init__(self, vertices, faces, load_order: int):
+    def __init__(self, vertices, faces, load_order: int, normals=None, face_normals=None):
         self.vertices = np.asarray(vertices, f32).reshape(-1, 3).copy()
         self.faces = np.asarray(faces, np.int64).reshape(-1, 3)
         if self.faces.size and (self.faces.min() < 0 or self.faces.max() >= len(self.vertices)):
             raise ValueError("mesh face index out of range")
+        # the file's normals and each facet's corner normal indices (kept for UseNormals and WriteWavefront)
+        self.normals = np.zeros((0, 3), f32) if normals is None else np.asarray(normals, f32).reshape(-1, 3).copy()
+        self.face_normals = np.zeros((0, 3), np.int64) if face_normals is None else \
+            np.asarray(face_normals, np.int64).reshape(-1, 3)
+        if self.face_normals.size and (self.face_normals.min() < 0 or self.face_normals.max() >= len(self.normals)):
+            raise ValueError("mesh normal index out of range")
+        self.use_normals = False
         self.load_order = load_order
         self.family_code = capi.RESERVED_FAMILY
         self.mass = f32(1.0)
@@ -277,11 +339,20 @@ class MeshObj:
     def Clear(self):
         self.vertices = np.zeros((0, 3), f32)
         self.faces = np.zeros((0, 3), np.int64)
+        self.normals = np.zeros((0, 3), f32)
+        self.face_normals = np.zeros((0, 3), np.int64)
         self.materials = None
 
     def UseNormals(self, use: bool = True):
-        """Accepted without effect: the reference reorders facet nodes to agree with the file's normals, but facets
-        here are two-sided, so the order does not matter."""
+        """At initialisation, order each facet's nodes so that their right-hand normal agrees with the file's
+        normal at its first corner (facet_nodes)."""
+        self.use_normals = bool(use)
+
+    def facet_nodes(self) -> np.ndarray:
+        """The facets' nodes in the mesh's own frame as initialisation places them (m x 9)."""
+        if self.use_normals:
+            return facet_nodes(self.vertices, self.faces, self.normals, self.face_normals)
+        return facet_nodes(self.vertices, self.faces)
 
     def SetFamily(self, code: int):
         if code > 255 or code < 0:
@@ -321,7 +392,13 @@ class MeshObj:
         self.vertices += np.asarray(d, f32).reshape(1, 3)
 
     def Scale(self, s):
-        self.vertices *= np.asarray(s, f32)
+        """Scales the nodes (one factor, or one per axis); the normals keep their direction on the scaled
+        surface."""
+        s = np.asarray(s, f32)
+        self.vertices *= s
+        if len(self.normals):
+            n = self.normals.astype(np.float64) / np.broadcast_to(s, (3,)).astype(np.float64)
+            self.normals = (n / np.linalg.norm(n, axis=1, keepdims=True)).astype(f32)
 
     def Rotate(self, q):
         """Rotates the nodes in the mesh's own frame by the unit quaternion q = (w, x, y, z)."""
@@ -330,6 +407,7 @@ class MeshObj:
                       [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
                       [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
         self.vertices = (self.vertices.astype(np.float64) @ R.T).astype(f32)
+        self.normals = (self.normals.astype(np.float64) @ R.T).astype(f32)
 
     def ComputeMassProperties(self):
         """(mass at unit density, centroid, moments of inertia about the centroid) of the closed, outward-wound mesh
@@ -340,6 +418,21 @@ class MeshObj:
     @staticmethod
     def WriteWavefront(path: str, meshes):
         write_wavefront(path, meshes)
+
+    @staticmethod
+    def Merge(meshes) -> "MeshObj":
+        """One mesh of the given meshes' nodes, normals and facets (declared in src/DEM/BdrsAndObjs.h:250); the
+        first mesh's body properties, no materials."""
+        vo = np.cumsum([0] + [len(m.vertices) for m in meshes])
+        no = np.cumsum([0] + [len(m.normals) for m in meshes])
+        cat = (lambda xs, shape, dt: np.concatenate(xs) if xs else np.zeros(shape, dt))
+        out = MeshObj(cat([m.vertices for m in meshes], (0, 3), f32),
+                      cat([m.faces + vo[i] for i, m in enumerate(meshes)], (0, 3), np.int64), 0,
+                      cat([m.normals for m in meshes], (0, 3), f32),
+                      cat([m.face_normals + no[i] for i, m in enumerate(meshes)], (0, 3), np.int64))
+        if meshes:
+            out.mass, out.moi, out.family_code = meshes[0].mass, meshes[0].moi.copy(), meshes[0].family_code
+        return out
 
 
 @dataclass
@@ -535,14 +628,18 @@ class SceneBuilder:
         self.extern.append(o)
         return o
 
-    def AddWavefrontMeshObject(self, mesh, material: Material | None = None) -> MeshObj:
-        """A mesh-represented body: a Wavefront OBJ path, or (vertices, faces) arrays (AddWavefrontMeshObject,
-        src/DEM/API.h:231-238)."""
+    def AddWavefrontMeshObject(self, mesh, material: Material | None = None, load_normals: bool = True) -> MeshObj:
+        """A mesh-represented body: a Wavefront OBJ path (its normals kept unless load_normals is False), or
+        (vertices, faces) arrays (AddWavefrontMeshObject, src/DEM/API.h:231-238)."""
         if isinstance(mesh, MeshObj):
             m = mesh
             m.load_order = len(self.meshes)
+        elif isinstance(mesh, str):
+            r = read_wavefront(mesh)
+            m = MeshObj(r["vertices"], r["faces"], len(self.meshes), *((r["normals"], r["face_normals"])
+                                                                       if load_normals else ()))
         else:
-            v, f = load_wavefront(mesh) if isinstance(mesh, str) else mesh
+            v, f = mesh
             m = MeshObj(v, f, len(self.meshes))
         if material is not None:
             m.SetMaterial(material)
@@ -729,7 +826,7 @@ class SceneBuilder:
         moi = np.concatenate([t_moi[types], np.array([o.moi for o in self.extern], f32).reshape(-1, 3),
                               np.array([m.moi for m in self.meshes], f32).reshape(-1, 3)]).astype(f32)
         # ---- mesh facets ----
-        tri = [m.vertices[m.faces].reshape(-1, 9) for m in self.meshes]
+        tri = [m.facet_nodes() for m in self.meshes]
         tri = np.concatenate(tri).astype(f32) if tri else np.zeros((0, 9), f32)
         nTri = len(tri)
         tri_owner = np.concatenate([np.full(m.GetNumTriangles(), m0 + i, np.uint32) for i, m in enumerate(self.meshes)]) \

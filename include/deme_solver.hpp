@@ -17,6 +17,9 @@
 #define DEME_SOLVER_HPP
 
 #include <algorithm>
+#include <array>
+#include <cctype>
+#include <climits>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -206,31 +209,67 @@ class DEMMeshConnected {
     DEMMeshConnected(const std::string& file, const std::shared_ptr<DEMMaterial>& mat) : DEMMeshConnected(file) {
         SetMaterial(mat);
     }
-    /* Wavefront OBJ: `v` and `f` records; polygons split into fans, negative indices from the end, texture and
-     * normal indices after '/' ignored */
+    /* The records of a Wavefront OBJ file as the reference's parser reads them (OBJ::ParseLine,
+     * src/core/utils/WavefrontMeshLoader.hpp:578-647, behind src/DEM/MeshUtils.cpp:44-112): `v` and `vn` records
+     * with three coordinates (a float rounded from the decimal value), `f` records of three or more corners split
+     * into fans about the first corner, with the corners' normal indices (`a//n`, `a/t/n`) kept three at a time;
+     * tags in any letter case.  Where the reference misreads a record, this reads it as the OBJ format defines it:
+     * a negative index counts back from the last record read (the reference subtracts one from it, leaving an index
+     * outside the mesh), and a vertex or normal record with more numbers or a trailing '#' comment is kept with its
+     * first three (the reference drops it, shifting every later index).  Texture coordinates are not kept.  False
+     * when the file cannot be opened or a number cannot be read. */
     bool LoadWavefrontMesh(const std::string& file, bool load_normals = true, bool load_uv = false) {
+        (void)load_uv;
         std::ifstream in(file);
         if (!in) return false;
         vertices.clear();
+        normals.clear();
         face_v_indices.clear();
+        face_n_indices.clear();
+        std::vector<int> flat_n;
         std::string line;
-        while (std::getline(in, line)) {
-            std::istringstream ls(line);
-            std::string tag;
-            if (!(ls >> tag)) continue;
-            if (tag == "v") {
-                float3 v{0.f, 0.f, 0.f};
-                ls >> v.x >> v.y >> v.z;
-                vertices.push_back(v);
-            } else if (tag == "f") {
-                std::vector<int> idx;
-                std::string tok;
-                while (ls >> tok) {
-                    const int i = std::stoi(tok.substr(0, tok.find('/')));
-                    idx.push_back(i > 0 ? i - 1 : (int)vertices.size() + i);
+        try {
+            while (std::getline(in, line)) {
+                const size_t hash = line.find('#');
+                if (hash != std::string::npos) line.resize(hash);
+                std::istringstream ls(line);
+                std::string tag;
+                if (!(ls >> tag)) continue;
+                for (char& c : tag) c = (char)std::tolower((unsigned char)c);
+                if (tag == "v" || tag == "vn") {
+                    std::string x, y, z;
+                    if (!(ls >> x >> y >> z)) continue;
+                    const float3 p{(float)std::stod(x), (float)std::stod(y), (float)std::stod(z)};
+                    (tag == "v" ? vertices : normals).push_back(p);
+                } else if (tag == "f") {
+                    std::vector<int> vi, ni;
+                    std::string tok;
+                    while (ls >> tok) {
+                        const size_t s1 = tok.find('/');
+                        const int i = std::stoi(tok.substr(0, s1));
+                        vi.push_back(i > 0 ? i - 1 : (int)vertices.size() + i);
+                        const size_t s2 = s1 == std::string::npos ? s1 : tok.find('/', s1 + 1);
+                        if (s2 != std::string::npos && s2 + 1 < tok.size()) {
+                            const int k = std::stoi(tok.substr(s2 + 1));
+                            ni.push_back(k > 0 ? k - 1 : (int)normals.size() + k);
+                        } else {
+                            ni.push_back(INT_MIN);
+                        }
+                    }
+                    for (size_t j = 1; j + 1 < vi.size(); j++) {
+                        face_v_indices.push_back(int3{vi[0], vi[j], vi[j + 1]});
+                        for (size_t c : {(size_t)0, j, j + 1})
+                            if (ni[c] != INT_MIN) flat_n.push_back(ni[c]);
+                    }
                 }
-                for (size_t j = 1; j + 1 < idx.size(); j++) face_v_indices.push_back(int3{idx[0], idx[j], idx[j + 1]});
             }
+        } catch (const std::logic_error&) {
+            return false;
+        }
+        for (size_t k = 0; k + 2 < flat_n.size(); k += 3) face_n_indices.push_back(int3{flat_n[k], flat_n[k + 1], flat_n[k + 2]});
+        if (!load_normals) {
+            normals.clear();
+            face_n_indices.clear();
         }
         nTri = face_v_indices.size();
         return true;
@@ -243,14 +282,34 @@ class DEMMeshConnected {
     }
     void Clear() {
         vertices.clear();
+        normals.clear();
         face_v_indices.clear();
+        face_n_indices.clear();
         materials.clear();
         nTri = 0;
         isMaterialSet = false;
     }
-    /* the reference reorders each facet's nodes to agree with the file's vertex normals; facets here are two-sided,
-     * so the order does not matter and this is accepted without effect */
-    void UseNormals(bool = true) {}
+    /* At initialisation, order each facet's nodes so that their right-hand normal agrees with the file's normal
+     * at its first corner (src/DEM/APIPrivate.cpp:545-560; FacetNodes) */
+    void UseNormals(bool use = true) { use_mesh_normals = use; }
+    /* The i-th facet's nodes as initialisation places them: with UseNormals, nodes 2 and 3 swapped where
+     * cross(p2 - p1, p3 - p1) points away from the normal of the first corner (float arithmetic, the reference's
+     * float3 operators) */
+    std::array<float3, 3> FacetNodes(size_t i) const {
+        const int3 fv = face_v_indices.at(i);
+        std::array<float3, 3> t{vertices.at((size_t)fv.x), vertices.at((size_t)fv.y), vertices.at((size_t)fv.z)};
+        if (use_mesh_normals) {
+            if (i >= face_n_indices.size())
+                throw std::runtime_error("UseNormals needs a normal index for every facet of the mesh");
+            const float3 n = normals.at((size_t)face_n_indices[i].x);
+            const float3 ab{t[1].x - t[0].x, t[1].y - t[0].y, t[1].z - t[0].z};
+            const float3 ac{t[2].x - t[0].x, t[2].y - t[0].y, t[2].z - t[0].z};
+            const float cx = ab.y * ac.z - ab.z * ac.y, cy = ab.z * ac.x - ab.x * ac.z, cz = ab.x * ac.y - ab.y * ac.x;
+            const float d = cx * n.x + cy * n.y;
+            if (d + cz * n.z < 0.f) std::swap(t[1], t[2]);
+        }
+        return t;
+    }
     void SetFamily(unsigned code) {
         if (code > 255) throw std::runtime_error("family number is larger than the max allowance 255");
         family_code = code;
@@ -275,8 +334,15 @@ class DEMMeshConnected {
     void Translate(float3 d) {
         for (auto& v : vertices) v = float3{v.x + d.x, v.y + d.y, v.z + d.z};
     }
-    void Scale(float s) {
-        for (auto& v : vertices) v = float3{v.x * s, v.y * s, v.z * s};
+    void Scale(float s) { Scale(float3{s, s, s}); }
+    /* one factor per axis; the normals keep their direction on the scaled surface */
+    void Scale(float3 s) {
+        for (auto& v : vertices) v = float3{v.x * s.x, v.y * s.y, v.z * s.z};
+        for (auto& n : normals) {
+            const double x = (double)n.x / s.x, y = (double)n.y / s.y, z = (double)n.z / s.z;
+            const double l = std::sqrt(x * x + y * y + z * z);
+            n = float3{(float)(x / l), (float)(y / l), (float)(z / l)};
+        }
     }
     /* rotates the nodes in the mesh's own frame by the unit quaternion q = (x, y, z, w) */
     void Rotate(float4 q) {
@@ -284,12 +350,13 @@ class DEMMeshConnected {
         const double R[3][3] = {{1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)},
                                 {2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)},
                                 {2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)}};
-        for (auto& v : vertices) {
-            const double p[3] = {v.x, v.y, v.z};
-            v = float3{(float)(R[0][0] * p[0] + R[0][1] * p[1] + R[0][2] * p[2]),
-                       (float)(R[1][0] * p[0] + R[1][1] * p[1] + R[1][2] * p[2]),
-                       (float)(R[2][0] * p[0] + R[2][1] * p[1] + R[2][2] * p[2])};
-        }
+        for (std::vector<float3>* a : {&vertices, &normals})
+            for (auto& v : *a) {
+                const double p[3] = {v.x, v.y, v.z};
+                v = float3{(float)(R[0][0] * p[0] + R[0][1] * p[1] + R[0][2] * p[2]),
+                           (float)(R[1][0] * p[0] + R[1][1] * p[1] + R[1][2] * p[2]),
+                           (float)(R[2][0] * p[0] + R[2][1] * p[1] + R[2][2] * p[2])};
+            }
     }
     /* Volume (the mass at unit density), centroid and the moments of inertia about the centroid along the mesh's
      * axes, of the solid a closed, outward-wound mesh bounds (declared, not defined, in the reference:
@@ -331,23 +398,58 @@ class DEMMeshConnected {
         inertia = float3{(float)(yy + zz - m * (cy * cy + cz * cz)), (float)(zz + xx - m * (cz * cz + cx * cx)),
                          (float)(xx + yy - m * (cx * cx + cy * cy))};
     }
-    /* WriteWavefront (src/DEM/MeshUtils.cpp:119-165): the meshes' vertices, then their faces offset into one
-     * object */
+    /* WriteWavefront (src/DEM/MeshUtils.cpp:119-165): every mesh's vertices, then the normals of the meshes that have
+     * them, then the faces offset into one object (`f a//n b//n c//n` for a mesh with normals) */
     static void WriteWavefront(const std::string& filename, std::vector<DEMMeshConnected>& meshes) {
         std::ofstream mf(filename);
         for (const auto& m : meshes)
             for (const auto& v : m.vertices) mf << "v " << v.x << " " << v.y << " " << v.z << "\n";
-        int off = 1;
+        for (const auto& m : meshes)
+            for (const auto& v : m.normals) mf << "vn " << v.x << " " << v.y << " " << v.z << "\n";
+        int off = 1, noff = 1;
         for (const auto& m : meshes) {
-            for (const auto& f : m.face_v_indices)
-                mf << "f " << f.x + off << " " << f.y + off << " " << f.z + off << "\n";
+            if (!m.normals.empty()) {
+                if (m.face_n_indices.size() != m.face_v_indices.size())
+                    throw std::runtime_error("a mesh with normals needs one normal triple per facet");
+                for (size_t j = 0; j < m.face_v_indices.size(); j++) {
+                    const int3 f = m.face_v_indices[j], n = m.face_n_indices[j];
+                    mf << "f " << f.x + off << "//" << n.x + noff << " " << f.y + off << "//" << n.y + noff << " "
+                       << f.z + off << "//" << n.z + noff << "\n";
+                }
+            } else {
+                for (const auto& f : m.face_v_indices)
+                    mf << "f " << f.x + off << " " << f.y + off << " " << f.z + off << "\n";
+            }
             off += (int)m.vertices.size();
+            noff += (int)m.normals.size();
         }
+    }
+    /* One mesh of the given meshes' nodes, normals and facets (declared, not defined, in the reference:
+     * BdrsAndObjs.h:250); the first mesh's body properties, no materials */
+    static DEMMeshConnected Merge(std::vector<DEMMeshConnected>& meshes) {
+        DEMMeshConnected out;
+        if (!meshes.empty()) {
+            out.mass = meshes[0].mass;
+            out.MOI = meshes[0].MOI;
+            out.family_code = meshes[0].family_code;
+        }
+        for (const auto& m : meshes) {
+            const int vo = (int)out.vertices.size(), no = (int)out.normals.size();
+            out.vertices.insert(out.vertices.end(), m.vertices.begin(), m.vertices.end());
+            out.normals.insert(out.normals.end(), m.normals.begin(), m.normals.end());
+            for (const int3& f : m.face_v_indices) out.face_v_indices.push_back(int3{f.x + vo, f.y + vo, f.z + vo});
+            for (const int3& f : m.face_n_indices) out.face_n_indices.push_back(int3{f.x + no, f.y + no, f.z + no});
+        }
+        out.nTri = out.face_v_indices.size();
+        return out;
     }
 
     size_t nTri = 0;
     std::vector<float3> vertices;
     std::vector<int3> face_v_indices;
+    std::vector<float3> normals;
+    std::vector<int3> face_n_indices;
+    bool use_mesh_normals = false;
     std::vector<std::shared_ptr<DEMMaterial>> materials;
     bool isMaterialSet = false;
     unsigned family_code = DEME_RESERVED_FAMILY;
@@ -1730,14 +1832,13 @@ class DEMSolver {
             f.mmiYY[o] = x.MOI.y;
             f.mmiZZ[o] = x.MOI.z;
             for (size_t i = 0; i < x.nTri; i++) {
-                const int3 fv = x.face_v_indices[i];
+                const std::array<float3, 3> t = x.FacetNodes(i);
                 f.tri_owner.push_back((uint32_t)o);
-                for (const auto& pr : {std::make_pair(fv.x, &f.tri_node1), std::make_pair(fv.y, &f.tri_node2),
-                                       std::make_pair(fv.z, &f.tri_node3)}) {
-                    const float3 v = x.vertices.at((size_t)pr.first);
-                    pr.second->push_back(v.x);
-                    pr.second->push_back(v.y);
-                    pr.second->push_back(v.z);
+                for (int c = 0; c < 3; c++) {
+                    std::vector<float>* dst = c == 0 ? &f.tri_node1 : c == 1 ? &f.tri_node2 : &f.tri_node3;
+                    dst->push_back(t[c].x);
+                    dst->push_back(t[c].y);
+                    dst->push_back(t[c].z);
                 }
                 f.tri_material.push_back((uint16_t)x.materials[i]->load_order);
             }

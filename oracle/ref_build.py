@@ -287,3 +287,38 @@ def build(built, out_root: str = OUT_ROOT, verbose: bool = False) -> str:
     if out_root == OUT_ROOT:
         _index_put(built, lib)
     return lib
+
+
+MESH_DIR = os.path.join(REF_ROOT, "data", "mesh")
+LOADER_HDR = os.path.join(REF_SRC, "core", "utils", "WavefrontMeshLoader.hpp")
+
+
+def obj_loader_available() -> bool:
+    return os.path.exists(LOADER_HDR)
+
+
+def build_obj_dump(out_root: str = OUT_ROOT) -> str:
+    """Compile oracle/ref_obj_dump.cpp against the reference's Wavefront parser (src/core/utils/
+    WavefrontMeshLoader.hpp, the loader behind DEMMeshConnected::LoadWavefrontMesh) into ``_ref/ref_obj_dump``."""
+    src = os.path.join(HERE, "ref_obj_dump.cpp")
+    exe = os.path.join(out_root, "ref_obj_dump")
+    if os.path.exists(exe) and os.path.getmtime(exe) >= max(os.path.getmtime(src), os.path.getmtime(LOADER_HDR)):
+        return exe
+    os.makedirs(out_root, exist_ok=True)
+    tmp = exe + ".tmp"
+    subprocess.check_call(["g++", "-O1", "-std=c++17", "-w", "-I" + REF_SRC, src, "-o", tmp])
+    os.replace(tmp, exe)
+    return exe
+
+
+def read_obj_dump(path: str) -> dict:
+    """The arrays ``ref_obj_dump`` writes: vertices, facet vertex indices, normals, facet normal indices."""
+    raw = open(path, "rb").read()
+    nv, nf, nn, nfn = np.frombuffer(raw[:16], np.int32)
+    off, out = 16, {}
+    for key, n, dt in (("vertices", nv, np.float32), ("faces", nf, np.int32), ("normals", nn, np.float32),
+                       ("face_normals", nfn, np.int32)):
+        a = np.frombuffer(raw, dt, 3 * int(n), off).reshape(-1, 3)
+        off += a.nbytes
+        out[key] = a
+    return out
