@@ -1097,6 +1097,8 @@ static std::vector<uint8_t> graph_key(const deme_handle* h) {
     put(&h->params.cd_update_freq, sizeof(h->params.cd_update_freq));
     put(&h->findShape, sizeof(h->findShape));
     put(&h->cellFactor, sizeof(h->cellFactor));
+    put(&h->nCells, sizeof(h->nCells));  // recorded as the cell scan's length (deme_change_clump_sizes changes it)
+    put(&h->cellBits, sizeof(h->cellBits));
     put(&h->forceShape, sizeof(h->forceShape));
     put(&h->exactThreads, sizeof(h->exactThreads));
     put(&h->integrateThreads, sizeof(h->integrateThreads));
