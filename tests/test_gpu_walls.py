@@ -10,7 +10,7 @@ contribution magnitudes; one-step velocities within 1e-5 relative, positions wit
 import numpy as np
 import pytest
 
-from _util import canonical, contact_key, oracle, partner_keys, workloads, capi
+from _util import canonical, contact_key, oracle, partner_keys, workloads
 from test_gpu_parity import gpu_solver, owner_scale
 
 pytestmark = pytest.mark.gpu
