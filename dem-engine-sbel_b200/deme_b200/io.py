@@ -180,6 +180,74 @@ def write_contact_file(path: str, built, state, contacts: dict, forces: dict | N
         f.write("\n".join(lines) + "\n")
 
 
+def csv_floats(cells) -> np.ndarray:
+    """float32 values of CSV cells as the reference's CSV reader forms them (io::detail::parse_float<float>,
+    src/core/utils/csv.hpp:936-997, the reader behind DEMClumpTemplate::ReadComponentFromFile and
+    ReadClumpXyzFromCsv / ReadClumpQuatFromCsv).  That reader is not correctly rounded: it accumulates the integer
+    digits in float (x = x * 10 + d), each fraction digit as d * p with p divided by 10 per digit in float, and applies
+    an exponent by repeated squaring of 10 or 0.1 in float, so its values can differ from the nearest float by a few
+    units in the last place; this forms them with the same float32 operations in the same order, for a whole column
+    at once.  Cells are trimmed of spaces and tabs; an empty cell is 0.  One deliberate difference: an exponent
+    written with '+' is read (the reference rejects it).  Anything else that is not a number raises ValueError."""
+    cells = [str(c).strip(" \t") for c in cells]
+    n = len(cells)
+    if n == 0:
+        return np.zeros(0, f32)
+    w = max(1, max(len(c) for c in cells))
+    try:
+        b = np.frombuffer("".join(c.ljust(w, "\0") for c in cells).encode("ascii"), np.uint8).reshape(n, w)
+    except UnicodeEncodeError:
+        raise ValueError("a CSV number cell holds a character that is not ASCII") from None
+    x = np.zeros(n, f32)
+    pos = np.ones(n, f32)
+    neg = b[:, 0] == ord("-")
+    phase = np.zeros(n, np.int8)  # 0 integer digits, 1 fraction digits, 2 exponent sign, 3 exponent digits, 4 done
+    e = np.zeros(n, np.int64)
+    e_neg = np.zeros(n, bool)
+    bad = np.zeros(n, bool)
+    ten = f32(10)
+    for j in range(w):
+        c = b[:, j]
+        if j == 0:
+            c = np.where((c == ord("-")) | (c == ord("+")), np.uint8(0xFF), c)  # a leading sign: nothing more here
+        skip = c == 0xFF
+        digit = (c >= ord("0")) & (c <= ord("9"))
+        d = (c.astype(np.int64) - ord("0"))
+        end = c == 0
+        m = (phase == 0) & digit
+        x[m] = x[m] * ten
+        x[m] = x[m] + d[m].astype(f32)
+        m = (phase == 1) & digit
+        pos[m] = pos[m] / ten
+        x[m] = x[m] + d[m].astype(f32) * pos[m]
+        m = (phase >= 2) & (phase <= 3) & digit
+        e[m] = np.minimum(e[m] * 10 + d[m], 1 << 20)
+        dot = (phase == 0) & ((c == ord(".")) | (c == ord(",")))
+        expo = (phase <= 1) & ((c == ord("e")) | (c == ord("E")))
+        esign = (phase == 2) & ((c == ord("-")) | (c == ord("+")))
+        e_neg |= esign & (c == ord("-"))
+        bad |= ~(skip | digit | end | dot | expo | esign) & (phase < 4)
+        phase = np.where(dot, 1, np.where(expo, 2, np.where(esign | ((phase == 2) & digit), 3, phase))).astype(np.int8)
+        phase[end] = 4
+    if bad.any():
+        raise ValueError(f"not a number in a CSV cell: {cells[int(np.argmax(bad))]!r}")
+    base = np.where(e_neg, f32(0.1), ten).astype(f32)
+    active = e != 0
+    while active.any():
+        step = active & (e != 1)
+        even = step & (e % 2 == 0)
+        odd = step & (e % 2 == 1)
+        base[even] = base[even] * base[even]
+        e[even] >>= 1
+        x[odd] = x[odd] * base[odd]
+        e[odd] -= 1
+        fin = active & (e == 1)
+        x[fin] = x[fin] * base[fin]
+        active &= ~fin
+    x[neg] = -x[neg]
+    return x
+
+
 def _read_columns(path: str, headers):
     with open(path, newline="") as f:
         rows = [r for r in csv.reader(f) if r and any(c.strip() for c in r)]
@@ -190,16 +258,22 @@ def _read_columns(path: str, headers):
 
 def read_clump_xyz_from_csv(path: str, clump_header="clump_type", x_header="X", y_header="Y", z_header="Z") -> dict:
     """Template name -> (n, 3) float32 positions, in file order."""
-    out: dict = {}
-    for name, x, y, z in _read_columns(path, (clump_header, x_header, y_header, z_header)):
-        out.setdefault(name, []).append((float(x), float(y), float(z)))
-    return {k: np.asarray(v, f32) for k, v in out.items()}
+    return _by_name(_read_columns(path, (clump_header, x_header, y_header, z_header)), 3)
 
 
 def read_clump_quat_from_csv(path: str, clump_header="clump_type", qw_header="Qw", qx_header="Qx", qy_header="Qy",
                              qz_header="Qz") -> dict:
     """Template name -> (n, 4) float32 quaternions (w, x, y, z), in file order."""
+    return _by_name(_read_columns(path, (clump_header, qw_header, qx_header, qy_header, qz_header)), 4)
+
+
+def _by_name(rows, k: int) -> dict:
+    """Rows of (name, k numbers) -> name -> (n, k) float32 in file order, the numbers read by csv_floats."""
+    if not rows:
+        return {}
+    vals = csv_floats([r[i] for r in rows for i in range(1, k + 1)]).reshape(-1, k)
+    names = [r[0] for r in rows]
     out: dict = {}
-    for name, w, x, y, z in _read_columns(path, (clump_header, qw_header, qx_header, qy_header, qz_header)):
-        out.setdefault(name, []).append((float(w), float(x), float(y), float(z)))
-    return {k: np.asarray(v, f32) for k, v in out.items()}
+    for i, name in enumerate(names):
+        out.setdefault(name, []).append(i)
+    return {name: vals[idx] for name, idx in out.items()}

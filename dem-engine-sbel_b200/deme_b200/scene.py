@@ -220,20 +220,21 @@ def mesh_mass_properties(vertices, faces):
 
 def read_clump_components(path: str, x_id="x", y_id="y", z_id="z", r_id="r"):
     """DEMClumpTemplate::ReadComponentFromFile (src/DEM/Structs.h:419-437): radii and relative positions from a CSV
-    file with a header row naming the columns (any order among others; a missing column reads 0)."""
+    file with a header row naming the columns (any order among others; a missing column or an empty cell reads 0),
+    the numbers formed as the reference's CSV reader forms them (io.csv_floats)."""
     with open(path) as fh:
-        lines = [ln for ln in fh.read().splitlines()]
+        # the reader's default comment policy: a line starting with '#', and a blank line, are skipped
+        lines = [ln for ln in fh.read().splitlines() if ln.strip(" \t") and not ln.startswith("#")]
     if not lines:
         return np.zeros(0, f32), np.zeros((0, 3), f32)
+    from .io import csv_floats
     head = [c.strip() for c in lines[0].split(",")]
     cols = [head.index(k) if k in head else -1 for k in (x_id, y_id, z_id, r_id)]
-    rows = []
+    cells = []
     for ln in lines[1:]:
-        if not ln.strip():
-            continue
-        cells = [c.strip() for c in ln.split(",")]
-        rows.append([float(np.float32(cells[c])) if 0 <= c < len(cells) else 0.0 for c in cols])
-    a = np.asarray(rows, f32).reshape(-1, 4)
+        row = ln.split(",")
+        cells.extend(row[c] if 0 <= c < len(row) else "" for c in cols)
+    a = csv_floats(cells).reshape(-1, 4)
     return a[:, 3].copy(), a[:, :3].copy()
 
 

@@ -55,6 +55,64 @@ class DEMMaterial {
     unsigned load_order;
 };
 
+/* A CSV cell's float as the reference's CSV reader forms it (io::detail::parse_float<float>,
+ * src/core/utils/csv.hpp:936-997, behind DEMClumpTemplate::ReadComponentFromFile and ReadClumpXyzFromCsv /
+ * ReadClumpQuatFromCsv).  That reader is not correctly rounded: integer digits accumulate in float (x = x * 10 + d),
+ * each fraction digit adds d * p with p divided by 10 per digit in float, and an exponent is applied by repeated
+ * squaring of 10 or 0.1 in float; the same float operations in the same order are done here, each product stored
+ * before it is added so that no compiler fuses them.  Spaces and tabs around the cell are ignored; an empty cell is
+ * 0.  An exponent written with '+' is read (the reference rejects it).  Anything else throws
+ * std::invalid_argument. */
+inline float csv_float(const std::string& cell) {
+    size_t i = cell.find_first_not_of(" \t\r"), end = cell.find_last_not_of(" \t\r");
+    if (i == std::string::npos) return 0.f;
+    end++;
+    auto bad = [&]() { return std::invalid_argument("not a number in a CSV cell: '" + cell + "'"); };
+    const bool neg = cell[i] == '-';
+    if (cell[i] == '-' || cell[i] == '+') i++;
+    volatile float x = 0.f;
+    auto digit = [&](size_t k) { return k < end && cell[k] >= '0' && cell[k] <= '9'; };
+    for (; digit(i); i++) {
+        x = x * 10.f;
+        x = x + (float)(cell[i] - '0');
+    }
+    if (i < end && (cell[i] == '.' || cell[i] == ',')) {
+        i++;
+        float pos = 1.f;
+        for (; digit(i); i++) {
+            pos = pos / 10.f;
+            const volatile float term = (float)(cell[i] - '0') * pos;
+            x = x + term;
+        }
+    }
+    if (i < end && (cell[i] == 'e' || cell[i] == 'E')) {
+        i++;
+        bool eneg = false;
+        if (i < end && (cell[i] == '-' || cell[i] == '+')) eneg = cell[i++] == '-';
+        long e = 0;
+        for (; i < end; i++) {
+            if (!digit(i)) throw bad();
+            e = std::min(e * 10 + (cell[i] - '0'), 1L << 20);
+        }
+        if (e != 0) {
+            float base = eneg ? 0.1f : 10.f;
+            while (e != 1) {
+                if ((e & 1) == 0) {
+                    base = base * base;
+                    e >>= 1;
+                } else {
+                    x = x * base;
+                    --e;
+                }
+            }
+            x = x * base;
+        }
+    } else if (i != end) {
+        throw bad();
+    }
+    return neg ? -x : x;
+}
+
 class DEMClumpTemplate {
   public:
     std::string m_name = "NULL";  // "%04d" of the load count unless assigned (src/DEM/APIPublic.cpp:337-341)
@@ -69,8 +127,10 @@ class DEMClumpTemplate {
     void SetVolume(float vol) { volume = vol; }
     unsigned nComp() const { return (unsigned)radii.size(); }
     /* ReadComponentFromFile (src/DEM/Structs.h:419-437): sphere components from a CSV file with a header row;
-     * the columns named x_id, y_id, z_id and r_id, in any order among others (a missing one reads 0), are appended.
-     * Returns 0, or 1 if the file cannot be read. */
+     * the columns named x_id, y_id, z_id and r_id, in any order among others (a missing one or an empty cell reads
+     * 0), are appended, the numbers formed as the reference's reader forms them (csv_float).  Lines starting with
+     * '#' and blank lines are skipped, as by that reader's default comment policy.  Returns 0, or 1 if the file
+     * cannot be read. */
     int ReadComponentFromFile(const std::string& filename, const std::string& x_id = "x",
                               const std::string& y_id = "y", const std::string& z_id = "z",
                               const std::string& r_id = "r") {
@@ -87,7 +147,12 @@ class DEMClumpTemplate {
             return out;
         };
         std::string line;
-        if (!std::getline(in, line)) return 0;
+        auto skipped = [](const std::string& l) {
+            return l.find_first_not_of(" \t\r") == std::string::npos || (!l.empty() && l[0] == '#');
+        };
+        do {
+            if (!std::getline(in, line)) return 0;
+        } while (skipped(line));
         const std::vector<std::string> head = split(line);
         int col[4] = {-1, -1, -1, -1};
         const std::string* ids[4] = {&x_id, &y_id, &z_id, &r_id};
@@ -95,11 +160,11 @@ class DEMClumpTemplate {
             for (size_t c = 0; c < head.size(); c++)
                 if (head[c] == *ids[k]) col[k] = (int)c;
         while (std::getline(in, line)) {
-            if (line.find_first_not_of(" \t\r") == std::string::npos) continue;
+            if (skipped(line)) continue;
             const std::vector<std::string> row = split(line);
             float v[4] = {0.f, 0.f, 0.f, 0.f};
             for (int k = 0; k < 4; k++)
-                if (col[k] >= 0 && (size_t)col[k] < row.size()) v[k] = std::strtof(row[col[k]].c_str(), nullptr);
+                if (col[k] >= 0 && (size_t)col[k] < row.size()) v[k] = csv_float(row[col[k]]);
             relPos.push_back(float3{v[0], v[1], v[2]});
             radii.push_back(v[3]);
         }
@@ -1274,13 +1339,14 @@ class DEMSolver {
     }
 
     /* ReadClumpXyzFromCsv / ReadClumpQuatFromCsv (src/DEM/API.h:326-371): clump type name -> coordinates or
-     * quaternions (w, x, y, z) from a clump file, in file order. */
+     * quaternions (w, x, y, z) from a clump file, in file order, the numbers formed as the reference's reader
+     * forms them (csv_float). */
     static std::unordered_map<std::string, std::vector<float3>> ReadClumpXyzFromCsv(
         const std::string& path, const std::string& clump_header = "clump_type", const std::string& x_header = "X",
         const std::string& y_header = "Y", const std::string& z_header = "Z") {
         std::unordered_map<std::string, std::vector<float3>> out;
         for (const auto& r : read_csv_columns(path, {clump_header, x_header, y_header, z_header}))
-            out[r[0]].push_back(float3{std::stof(r[1]), std::stof(r[2]), std::stof(r[3])});
+            out[r[0]].push_back(float3{csv_float(r[1]), csv_float(r[2]), csv_float(r[3])});
         return out;
     }
     static std::unordered_map<std::string, std::vector<float4>> ReadClumpQuatFromCsv(
@@ -1289,10 +1355,10 @@ class DEMSolver {
         std::unordered_map<std::string, std::vector<float4>> out;
         for (const auto& r : read_csv_columns(path, {clump_header, qw_header, qx_header, qy_header, qz_header})) {
             float4 q;
-            q.w = std::stof(r[1]);
-            q.x = std::stof(r[2]);
-            q.y = std::stof(r[3]);
-            q.z = std::stof(r[4]);
+            q.w = csv_float(r[1]);
+            q.x = csv_float(r[2]);
+            q.y = csv_float(r[3]);
+            q.z = csv_float(r[4]);
             out[r[0]].push_back(q);
         }
         return out;

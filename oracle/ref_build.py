@@ -322,3 +322,34 @@ def read_obj_dump(path: str) -> dict:
         off += a.nbytes
         out[key] = a
     return out
+
+
+def build_csv_dump(out_root: str = OUT_ROOT) -> str:
+    """Compile oracle/ref_csv_dump.cpp against the reference's CSV reader (src/core/utils/csv.hpp, the reader behind
+    DEMClumpTemplate::ReadComponentFromFile and ReadClumpXyzFromCsv) into ``_ref/ref_csv_dump``."""
+    src = os.path.join(HERE, "ref_csv_dump.cpp")
+    hdr = os.path.join(REF_SRC, "core", "utils", "csv.hpp")
+    exe = os.path.join(out_root, "ref_csv_dump")
+    if os.path.exists(exe) and os.path.getmtime(exe) >= max(os.path.getmtime(src), os.path.getmtime(hdr)):
+        return exe
+    os.makedirs(out_root, exist_ok=True)
+    tmp = exe + ".tmp"
+    subprocess.check_call(["g++", "-O1", "-std=c++17", "-w", "-pthread", "-I" + REF_SRC, src, "-o", tmp])
+    os.replace(tmp, exe)
+    return exe
+
+
+CLUMP_DIR = os.path.join(REF_ROOT, "data", "clumps")
+
+
+def read_csv_dump(path: str) -> tuple[np.ndarray, list]:
+    """The rows (n x 4 float32) and names ``ref_csv_dump`` writes."""
+    raw = open(path, "rb").read()
+    n = int(np.frombuffer(raw, np.int32, 1)[0])
+    vals = np.frombuffer(raw, np.float32, 4 * n, 4).reshape(-1, 4)
+    off, names = 4 + 16 * n, []
+    while off < len(raw):
+        ln = int(np.frombuffer(raw, np.int32, 1, off)[0])
+        names.append(raw[off + 4:off + 4 + ln].decode())
+        off += 4 + ln
+    return vals, names
